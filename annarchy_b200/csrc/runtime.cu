@@ -1,0 +1,650 @@
+// Native runtime of the B200 simulation backend: the C ABI declared in
+// include/annarchy_b200.h.
+//
+// It owns, per network: the device arrays of every population/projection
+// attribute (by name), the NVRTC-compiled module generated for the network,
+// and the per-step launch plan. A step is either the list of plan kernels
+// (grid engine; captured once into a CUDA graph of `graph_steps` steps and
+// replayed, so a run of n steps costs n/graph_steps graph launches and no
+// host round trip per step) or one persistent kernel that advances many
+// steps per launch (local engine).
+//
+// The reference drives its generated CUDA step from the host every step
+// and blocks on a device->host copy of the spike count
+// (ANNarchy/generator/Template/CUDABaseTemplate.py:328-630); here the spike
+// counts and the time counter stay on the device.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/annarchy_b200.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+// Driver-API entry points, fetched through the runtime on first use so that
+// the library itself does not link libcuda (it then loads, and reports "no
+// device", on machines without a GPU driver).
+struct Driver {
+  bool loaded = false;
+  decltype(&cuModuleLoadData) moduleLoadData = nullptr;
+  decltype(&cuModuleUnload) moduleUnload = nullptr;
+  decltype(&cuModuleGetFunction) moduleGetFunction = nullptr;
+  decltype(&cuModuleGetGlobal) moduleGetGlobal = nullptr;
+  decltype(&cuLaunchKernel) launchKernel = nullptr;
+  decltype(&cuFuncSetAttribute) funcSetAttribute = nullptr;
+  decltype(&cuGetErrorString) getErrorString = nullptr;
+};
+Driver g_drv;
+
+template <typename F>
+bool entry(const char* name, F* fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !p)
+    return false;
+  *fn = reinterpret_cast<F>(p);
+  return true;
+}
+
+bool load_driver() {
+  if (g_drv.loaded) return true;
+  bool ok = entry("cuModuleLoadData", &g_drv.moduleLoadData) &&
+            entry("cuModuleUnload", &g_drv.moduleUnload) &&
+            entry("cuModuleGetFunction", &g_drv.moduleGetFunction) &&
+            entry("cuModuleGetGlobal", &g_drv.moduleGetGlobal) &&
+            entry("cuLaunchKernel", &g_drv.launchKernel) &&
+            entry("cuFuncSetAttribute", &g_drv.funcSetAttribute) &&
+            entry("cuGetErrorString", &g_drv.getErrorString);
+  g_drv.loaded = ok;
+  return ok;
+}
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+#define ANB_CUDA(call)                                                                \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(ANB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+  } while (0)
+
+#define ANB_CU(call)                                                \
+  do {                                                              \
+    CUresult r_ = (call);                                           \
+    if (r_ != CUDA_SUCCESS) {                                       \
+      const char* s_ = nullptr;                                     \
+      if (g_drv.getErrorString) g_drv.getErrorString(r_, &s_);      \
+      return fail(ANB_ERR_CUDA, std::string(#call) + ": " + (s_ ? s_ : "?")); \
+    }                                                               \
+  } while (0)
+
+struct Array {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct Launch {
+  std::string name;
+  CUfunction fn = nullptr;
+  unsigned grid = 1, block = 1, smem = 0;
+};
+
+struct TimedLaunch {
+  int kernel;
+  cudaEvent_t start, stop;
+};
+
+struct KernelTime {
+  std::string name;
+  double total_ms = 0.0;
+  int64_t launches = 0;
+};
+
+}  // namespace
+
+struct anb_net {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::map<std::string, Array> arrays;
+  CUmodule module = nullptr;
+  bool bindings_dirty = true;
+  std::vector<Launch> plan;
+  Launch local;
+  bool has_local = false;
+  int graph_steps = 32;
+  cudaGraphExec_t graph = nullptr;
+  double dt = 1.0;
+  int64_t t = 0;
+  bool timing = false;
+  std::vector<TimedLaunch> pending;
+  std::vector<KernelTime> times;
+  std::map<std::string, int> time_index;
+};
+
+namespace {
+
+int ensure_device(anb_net* net) {
+  ANB_CUDA(cudaSetDevice(net->device));
+  return ANB_OK;
+}
+
+Array* find(anb_net* net, const char* name) {
+  if (!name) return nullptr;
+  auto it = net->arrays.find(name);
+  return it == net->arrays.end() ? nullptr : &it->second;
+}
+
+void drop_graph(anb_net* net) {
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+}
+
+// Write the device address of every array into the module's __constant__
+// pointer of the same name (anb_p_<name>), where the module declares one.
+int bind(anb_net* net) {
+  if (!net->module || !net->bindings_dirty) return ANB_OK;
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  for (auto& kv : net->arrays) {
+    std::string sym = "anb_p_" + kv.first;
+    CUdeviceptr dptr = 0;
+    size_t sz = 0;
+    CUresult r = g_drv.moduleGetGlobal(&dptr, &sz, net->module, sym.c_str());
+    if (r == CUDA_ERROR_NOT_FOUND) continue;
+    if (r != CUDA_SUCCESS) return fail(ANB_ERR_CUDA, "cuModuleGetGlobal(" + sym + ") failed");
+    if (sz != sizeof(void*)) return fail(ANB_ERR_ARG, sym + " is not a pointer");
+    void* p = kv.second.ptr;
+    ANB_CUDA(cudaMemcpy((void*)dptr, &p, sizeof(void*), cudaMemcpyHostToDevice));
+  }
+  net->bindings_dirty = false;
+  return ANB_OK;
+}
+
+int launch(anb_net* net, const Launch& l, void** params) {
+  ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem, (CUstream)net->stream,
+                        params, nullptr));
+  return ANB_OK;
+}
+
+int timed_launch(anb_net* net, const Launch& l, void** params) {
+  auto it = net->time_index.find(l.name);
+  int idx;
+  if (it == net->time_index.end()) {
+    idx = (int)net->times.size();
+    net->time_index[l.name] = idx;
+    net->times.push_back(KernelTime{l.name, 0.0, 0});
+  } else {
+    idx = it->second;
+  }
+  TimedLaunch tl{idx, nullptr, nullptr};
+  ANB_CUDA(cudaEventCreate(&tl.start));
+  ANB_CUDA(cudaEventCreate(&tl.stop));
+  ANB_CUDA(cudaEventRecord(tl.start, net->stream));
+  int rc = launch(net, l, params);
+  if (rc != ANB_OK) return rc;
+  ANB_CUDA(cudaEventRecord(tl.stop, net->stream));
+  net->pending.push_back(tl);
+  return ANB_OK;
+}
+
+int collect_times(anb_net* net) {
+  for (auto& tl : net->pending) {
+    float ms = 0.f;
+    ANB_CUDA(cudaEventSynchronize(tl.stop));
+    ANB_CUDA(cudaEventElapsedTime(&ms, tl.start, tl.stop));
+    net->times[tl.kernel].total_ms += ms;
+    net->times[tl.kernel].launches += 1;
+    cudaEventDestroy(tl.start);
+    cudaEventDestroy(tl.stop);
+  }
+  net->pending.clear();
+  return ANB_OK;
+}
+
+int run_plan_once(anb_net* net) {
+  for (auto& l : net->plan) {
+    int rc = net->timing ? timed_launch(net, l, nullptr) : launch(net, l, nullptr);
+    if (rc != ANB_OK) return rc;
+  }
+  return ANB_OK;
+}
+
+int build_graph(anb_net* net) {
+  if (net->graph) return ANB_OK;
+  cudaGraph_t g = nullptr;
+  ANB_CUDA(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = ANB_OK;
+  for (int s = 0; s < net->graph_steps && rc == ANB_OK; ++s) rc = run_plan_once(net);
+  cudaError_t e = cudaStreamEndCapture(net->stream, &g);
+  if (rc != ANB_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(ANB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&net->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(ANB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return ANB_OK;
+}
+
+int write_time(anb_net* net) {
+  Array* a = find(net, "t");
+  if (!a) return fail(ANB_ERR_STATE, "time counter missing");
+  long long t = (long long)net->t;
+  ANB_CUDA(cudaMemcpyAsync(a->ptr, &t, sizeof(t), cudaMemcpyHostToDevice, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  return ANB_OK;
+}
+
+int create_array(anb_net* net, const std::string& name, size_t bytes) {
+  Array* old = find(net, name.c_str());
+  if (old) {
+    if (old->bytes == bytes) {
+      ANB_CUDA(cudaMemsetAsync(old->ptr, 0, bytes ? bytes : 1, net->stream));
+      ANB_CUDA(cudaStreamSynchronize(net->stream));
+      return ANB_OK;
+    }
+    ANB_CUDA(cudaStreamSynchronize(net->stream));
+    cudaFree(old->ptr);
+    net->arrays.erase(name);
+  }
+  Array a;
+  a.bytes = bytes;
+  size_t alloc = bytes ? bytes : 16;
+  cudaError_t e = cudaMalloc(&a.ptr, alloc);
+  if (e != cudaSuccess)
+    return fail(ANB_ERR_ALLOC, "cudaMalloc(" + std::to_string(alloc) + ") for " + name + ": " +
+                                   cudaGetErrorString(e));
+  ANB_CUDA(cudaMemsetAsync(a.ptr, 0, alloc, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  net->arrays[name] = a;
+  net->bindings_dirty = true;
+  return ANB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int anb_abi_version(void) { return 1; }
+
+const char* anb_last_error(void) { return g_error.c_str(); }
+
+int anb_device_count(int* count) {
+  if (!count) return fail(ANB_ERR_ARG, "count is NULL");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  *count = (e == cudaSuccess) ? n : 0;
+  return ANB_OK;
+}
+
+int anb_create(int device, anb_net** out) {
+  if (!out) return fail(ANB_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(ANB_ERR_CUDA, "no CUDA device is available");
+  if (device < 0 || device >= n) return fail(ANB_ERR_ARG, "device index out of range");
+  std::unique_ptr<anb_net> net(new anb_net());
+  net->device = device;
+  ANB_CUDA(cudaSetDevice(device));
+  ANB_CUDA(cudaFree(nullptr));  // create the primary context for the driver-API calls
+  if (!load_driver()) return fail(ANB_ERR_CUDA, "CUDA driver entry points are unavailable");
+  ANB_CUDA(cudaStreamCreateWithFlags(&net->own_stream, cudaStreamNonBlocking));
+  net->stream = net->own_stream;
+  int rc = create_array(net.get(), "t", sizeof(long long));
+  if (rc == ANB_OK) rc = create_array(net.get(), "dt", sizeof(double));
+  if (rc == ANB_OK) rc = create_array(net.get(), "err", 4 * sizeof(int));
+  if (rc != ANB_OK) return rc;
+  *out = net.release();
+  return ANB_OK;
+}
+
+int anb_destroy(anb_net* net) {
+  if (!net) return ANB_OK;
+  cudaSetDevice(net->device);
+  if (net->stream) cudaStreamSynchronize(net->stream);
+  for (auto& tl : net->pending) {
+    cudaEventDestroy(tl.start);
+    cudaEventDestroy(tl.stop);
+  }
+  drop_graph(net);
+  if (net->module) g_drv.moduleUnload(net->module);
+  for (auto& kv : net->arrays) cudaFree(kv.second.ptr);
+  if (net->own_stream) cudaStreamDestroy(net->own_stream);
+  delete net;
+  return ANB_OK;
+}
+
+int anb_initialize(anb_net* net, double dt) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  if (!(dt > 0.0)) return fail(ANB_ERR_ARG, "dt must be positive");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  net->dt = dt;
+  Array* a = find(net, "dt");
+  ANB_CUDA(cudaMemcpyAsync(a->ptr, &dt, sizeof(double), cudaMemcpyHostToDevice, net->stream));
+  net->t = 0;
+  return write_time(net);
+}
+
+int anb_set_time(anb_net* net, int64_t t) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  net->t = t;
+  return write_time(net);
+}
+
+int anb_get_time(anb_net* net, int64_t* t) {
+  if (!net || !t) return fail(ANB_ERR_ARG, "NULL argument");
+  *t = net->t;
+  return ANB_OK;
+}
+
+int anb_set_stream(anb_net* net, void* cuda_stream) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  net->stream = cuda_stream ? (cudaStream_t)cuda_stream : net->own_stream;
+  drop_graph(net);
+  return ANB_OK;
+}
+
+int anb_array_create(anb_net* net, const char* name, size_t bytes) {
+  if (!net || !name || !*name) return fail(ANB_ERR_ARG, "NULL argument");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  return create_array(net, name, bytes);
+}
+
+int anb_array_free(anb_net* net, const char* name) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  Array* a = find(net, name);
+  if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + (name ? name : "(null)"));
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  cudaFree(a->ptr);
+  net->arrays.erase(name);
+  net->bindings_dirty = true;
+  return ANB_OK;
+}
+
+int anb_array_write(anb_net* net, const char* name, size_t offset, const void* src, size_t bytes) {
+  if (!net || (!src && bytes)) return fail(ANB_ERR_ARG, "NULL argument");
+  Array* a = find(net, name);
+  if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + (name ? name : "(null)"));
+  if (offset > a->bytes || bytes > a->bytes - offset)
+    return fail(ANB_ERR_ARG, std::string("write beyond the end of ") + name);
+  if (!bytes) return ANB_OK;
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  ANB_CUDA(cudaMemcpyAsync((char*)a->ptr + offset, src, bytes, cudaMemcpyHostToDevice, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  return ANB_OK;
+}
+
+int anb_array_read(anb_net* net, const char* name, size_t offset, void* dst, size_t bytes) {
+  if (!net || (!dst && bytes)) return fail(ANB_ERR_ARG, "NULL argument");
+  Array* a = find(net, name);
+  if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + (name ? name : "(null)"));
+  if (offset > a->bytes || bytes > a->bytes - offset)
+    return fail(ANB_ERR_ARG, std::string("read beyond the end of ") + name);
+  if (!bytes) return ANB_OK;
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  ANB_CUDA(cudaMemcpyAsync(dst, (const char*)a->ptr + offset, bytes, cudaMemcpyDeviceToHost, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  return ANB_OK;
+}
+
+int anb_array_fill_zero(anb_net* net, const char* name) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  Array* a = find(net, name);
+  if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + (name ? name : "(null)"));
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  if (a->bytes) ANB_CUDA(cudaMemsetAsync(a->ptr, 0, a->bytes, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  return ANB_OK;
+}
+
+int anb_array_info(anb_net* net, const char* name, void** device_ptr, size_t* bytes) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  Array* a = find(net, name);
+  if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + (name ? name : "(null)"));
+  if (device_ptr) *device_ptr = a->ptr;
+  if (bytes) *bytes = a->bytes;
+  return ANB_OK;
+}
+
+int anb_module_load(anb_net* net, const char* source, const char* options) {
+  if (!net || !source) return fail(ANB_ERR_ARG, "NULL argument");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  std::vector<std::string> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device",
+                                   "-lineinfo"};
+  if (options) {
+    std::string s(options), cur;
+    for (char c : s) {
+      if (c == '\n') {
+        if (!cur.empty()) opts.push_back(cur);
+        cur.clear();
+      } else {
+        cur.push_back(c);
+      }
+    }
+    if (!cur.empty()) opts.push_back(cur);
+  }
+  std::vector<const char*> copts;
+  for (auto& o : opts) copts.push_back(o.c_str());
+
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, source, "anb_network.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+    return fail(ANB_ERR_COMPILE, "nvrtcCreateProgram failed");
+  nvrtcResult cr = nvrtcCompileProgram(prog, (int)copts.size(), copts.data());
+  size_t log_size = 0;
+  nvrtcGetProgramLogSize(prog, &log_size);
+  std::string log(log_size, '\0');
+  if (log_size) nvrtcGetProgramLog(prog, &log[0]);
+  if (cr != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    return fail(ANB_ERR_COMPILE, std::string("NVRTC: ") + nvrtcGetErrorString(cr) + "\n" + log);
+  }
+  size_t cubin_size = 0;
+  if (nvrtcGetCUBINSize(prog, &cubin_size) != NVRTC_SUCCESS || cubin_size == 0) {
+    nvrtcDestroyProgram(&prog);
+    return fail(ANB_ERR_COMPILE, "NVRTC produced no cubin");
+  }
+  std::vector<char> cubin(cubin_size);
+  nvrtcGetCUBIN(prog, cubin.data());
+  nvrtcDestroyProgram(&prog);
+
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  drop_graph(net);
+  net->plan.clear();
+  net->has_local = false;
+  if (net->module) {
+    g_drv.moduleUnload(net->module);
+    net->module = nullptr;
+  }
+  ANB_CU(g_drv.moduleLoadData(&net->module, cubin.data()));
+  net->bindings_dirty = true;
+  return bind(net);
+}
+
+int anb_plan_clear(anb_net* net) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  drop_graph(net);
+  net->plan.clear();
+  return ANB_OK;
+}
+
+static int resolve(anb_net* net, const char* kernel, unsigned grid, unsigned block, unsigned smem,
+                   Launch* out) {
+  if (!net || !kernel) return fail(ANB_ERR_ARG, "NULL argument");
+  if (!net->module) return fail(ANB_ERR_STATE, "no module loaded");
+  if (grid == 0 || block == 0 || block > 1024) return fail(ANB_ERR_ARG, "bad launch shape");
+  Launch l;
+  l.name = kernel;
+  l.grid = grid;
+  l.block = block;
+  l.smem = smem;
+  CUresult r = g_drv.moduleGetFunction(&l.fn, net->module, kernel);
+  if (r != CUDA_SUCCESS) return fail(ANB_ERR_ARG, std::string("kernel not found: ") + kernel);
+  if (smem > 48 * 1024)
+    ANB_CU(g_drv.funcSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  *out = l;
+  return ANB_OK;
+}
+
+int anb_plan_add(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                 unsigned shared_bytes) {
+  Launch l;
+  int rc = resolve(net, kernel, grid, block, shared_bytes, &l);
+  if (rc) return rc;
+  drop_graph(net);
+  net->plan.push_back(l);
+  return ANB_OK;
+}
+
+int anb_set_local_kernel(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                         unsigned shared_bytes) {
+  Launch l;
+  int rc = resolve(net, kernel, grid, block, shared_bytes, &l);
+  if (rc) return rc;
+  net->local = l;
+  net->has_local = true;
+  return ANB_OK;
+}
+
+int anb_set_graph_steps(anb_net* net, int steps) {
+  if (!net || steps < 0) return fail(ANB_ERR_ARG, "bad argument");
+  drop_graph(net);
+  net->graph_steps = steps;
+  return ANB_OK;
+}
+
+int anb_run(anb_net* net, int64_t nsteps) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  if (nsteps < 0) return fail(ANB_ERR_ARG, "negative step count");
+  if (nsteps == 0) return ANB_OK;
+  if (!net->module) return fail(ANB_ERR_STATE, "no module loaded");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  rc = bind(net);
+  if (rc) return rc;
+  if (net->has_local) {
+    int64_t done = 0;
+    while (done < nsteps) {
+      long long t0 = (long long)(net->t + done);
+      int n = (int)((nsteps - done) > (1 << 30) ? (1 << 30) : (nsteps - done));
+      void* params[] = {&t0, &n};
+      rc = net->timing ? timed_launch(net, net->local, params) : launch(net, net->local, params);
+      if (rc) return rc;
+      done += n;
+    }
+    net->t += nsteps;
+    return ANB_OK;
+  }
+  int64_t remaining = nsteps;
+  if (!net->timing && net->graph_steps > 1 && nsteps >= net->graph_steps) {
+    rc = build_graph(net);
+    if (rc) return rc;
+    while (remaining >= net->graph_steps) {
+      ANB_CUDA(cudaGraphLaunch(net->graph, net->stream));
+      remaining -= net->graph_steps;
+    }
+  }
+  for (int64_t s = 0; s < remaining; ++s) {
+    rc = run_plan_once(net);
+    if (rc) return rc;
+  }
+  net->t += nsteps;
+  return ANB_OK;
+}
+
+int anb_step(anb_net* net) { return anb_run(net, 1); }
+
+int anb_synchronize(anb_net* net) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  if (net->timing) {
+    rc = collect_times(net);
+    if (rc) return rc;
+  }
+  int code = 0;
+  rc = anb_device_error(net, &code);
+  if (rc) return rc;
+  if (code) return fail(ANB_ERR_TIMEOUT, "device-side error code " + std::to_string(code));
+  return ANB_OK;
+}
+
+int anb_device_error(anb_net* net, int* code) {
+  if (!net || !code) return fail(ANB_ERR_ARG, "NULL argument");
+  Array* a = find(net, "err");
+  int v[4] = {0, 0, 0, 0};
+  ANB_CUDA(cudaMemcpyAsync(v, a->ptr, sizeof(v), cudaMemcpyDeviceToHost, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  *code = v[0];
+  return ANB_OK;
+}
+
+int anb_clear_device_error(anb_net* net) { return anb_array_fill_zero(net, "err"); }
+
+int anb_kernel_timing(anb_net* net, int enable) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  rc = collect_times(net);
+  if (rc) return rc;
+  net->timing = enable != 0;
+  if (enable) {
+    net->times.clear();
+    net->time_index.clear();
+  }
+  return ANB_OK;
+}
+
+int anb_kernel_time_count(anb_net* net, int* count) {
+  if (!net || !count) return fail(ANB_ERR_ARG, "NULL argument");
+  *count = (int)net->times.size();
+  return ANB_OK;
+}
+
+int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len, double* total_ms,
+                        int64_t* launches) {
+  if (!net || index < 0 || index >= (int)net->times.size())
+    return fail(ANB_ERR_ARG, "bad kernel index");
+  const KernelTime& k = net->times[index];
+  if (name && name_len) {
+    std::strncpy(name, k.name.c_str(), name_len - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (total_ms) *total_ms = k.total_ms;
+  if (launches) *launches = k.launches;
+  return ANB_OK;
+}
+
+}  // extern "C"

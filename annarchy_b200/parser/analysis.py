@@ -1,0 +1,395 @@
+"""Neuron and synapse analysis: model definition -> description dict.
+
+The description has the same keys as the reference's
+(ANNarchy/parser/AnalyseNeuron.py:27-392, AnalyseSynapse.py:34-590):
+``parameters``, ``variables`` (each with ``cpp``, ``switch``, ``bounds``,
+``init``, ``locality``, ``method``), ``local``/``semiglobal``/``global``,
+``targets``, ``spike`` (``spike_cond``, ``spike_reset``) and, for synapses,
+``pre_spike``/``post_spike``/``psp``. C strings keep the reference's index
+placeholders (``%(local_index)s`` ...); the code generator fills them.
+
+Not supported by this backend (an error names them): if-then-else
+statements, global operations (``mean(r)``...), random distributions inside
+equations, user functions, coupled implicit/midpoint/rk4 systems.
+"""
+from __future__ import annotations
+
+import re
+
+from .equation import BUILTIN_FUNCTIONS, Statement
+from .text import ParserError, equation_list, lhs_name, parse_flags, split_flags, statements
+
+
+# ---------------------------------------------------------------------------
+# parameters and variables (Extraction.py:251-536)
+# ---------------------------------------------------------------------------
+
+def _flags_to_locality(flags):
+    for f in ("population", "postsynaptic", "projection"):
+        if f in flags:
+            return "semiglobal" if f == "postsynaptic" else "global"
+    return "local"
+
+
+def _typed_init(bounds, flags, equation=""):
+    ctype = "int" if "int" in flags else ("bool" if "bool" in flags else "double")
+    if "init" in bounds:
+        init = bounds["init"]
+        if ctype == "bool":
+            init = init in ("true", "True", "1")
+        else:
+            try:
+                init = int(init) if ctype == "int" else float(init)
+            except ValueError:
+                init = str(init)
+    elif "=" in equation:
+        init = equation.split("=")[1].strip()
+        if init in ("false", "False", "true", "True"):
+            ctype, init = "bool", init in ("true", "True")
+        elif ctype == "int":
+            init = int(eval(init, {}, {}))  # numeric literal, possibly an expression like 2*3
+        else:
+            try:
+                init = float(eval(init, {}, {}))
+            except Exception as exc:
+                raise ParserError("the value of the parameter is not a float: " + equation) from exc
+    else:
+        init = False if ctype == "bool" else (0 if ctype == "int" else 0.0)
+    return ctype, init
+
+
+def extract_parameters(parameters, object_type):
+    out = []
+    if parameters is None:
+        return out
+    if isinstance(parameters, dict):
+        for key, val in parameters.items():
+            locality, ctype, value = "global", "double", val
+            if hasattr(val, "locality") and hasattr(val, "value"):   # Parameter(...) objects
+                locality = {"population": "global", "projection": "global",
+                            "postsynaptic": "semiglobal"}.get(val.locality, val.locality)
+                value = val.value
+                ctype = {float: "double", int: "int", bool: "bool", "float": "double"}.get(
+                    getattr(val, "type", float), str(getattr(val, "type", "double")))
+            if locality == "global":
+                flags = "population" if object_type == "neuron" else "projection"
+            elif locality == "semiglobal":
+                flags = "postsynaptic"
+            else:
+                flags = ""
+            out.append(dict(name=key, locality=locality, eq=f"{key} = {value}", bounds={},
+                            flags=flags, ctype=ctype, init=value))
+        return out
+    lines = statements(parameters) if isinstance(parameters, str) else list(parameters)
+    for definition in lines:
+        equation, tail = split_flags(definition)
+        name = lhs_name(equation)
+        if name in ("_undefined", ""):
+            raise ParserError("definition can not be analysed: " + equation)
+        bounds, flags = parse_flags(tail)
+        ctype, init = _typed_init(bounds, flags, equation)
+        out.append(dict(name=name, locality=_flags_to_locality(flags), eq=equation,
+                        bounds=bounds, flags=flags, ctype=ctype, init=init))
+    return out
+
+
+def extract_variables(equations):
+    out = []
+    for d in equation_list(equations):
+        eq = d["eq"]
+        if eq.count("(") != eq.count(")"):
+            raise ParserError("the number of parentheses does not match: " + eq)
+        bounds, flags = parse_flags(d["constraint"])
+        ctype, init = _typed_init(bounds, flags)
+        out.append(dict(name=d["name"], locality=_flags_to_locality(flags), eq=eq, bounds=bounds,
+                        flags=flags, ctype=ctype, init=init))
+    return out
+
+
+def _method(var, default="explicit"):
+    for f, m in (("implicit", "implicit"), ("semiimplicit", "semiimplicit"),
+                 ("exponential", "exponential"), ("midpoint", "midpoint"),
+                 ("runge-kutta4", "rk4"), ("rk4", "rk4"), ("explicit", "explicit"),
+                 ("exact", "event-driven"), ("event-driven", "event-driven")):
+        if f in var["flags"]:
+            return m
+    return default
+
+
+def _split_locality(items, neuron):
+    attributes, local, global_, semiglobal = [], [], [], []
+    for p in items:
+        attributes.append(p["name"])
+        flags = p["flags"]
+        if "population" in flags:
+            if not neuron:
+                raise ParserError(f"{p['name']}: 'population' is a neuron flag")
+            global_.append(p["name"])
+        elif "projection" in flags:
+            if neuron:
+                raise ParserError(f"{p['name']}: 'projection' is a synapse flag")
+            global_.append(p["name"])
+        elif "postsynaptic" in flags:
+            if neuron:
+                raise ParserError(f"{p['name']}: 'postsynaptic' is a synapse flag")
+            semiglobal.append(p["name"])
+        else:
+            local.append(p["name"])
+    return attributes, local, global_, semiglobal
+
+
+def _targets(variables):
+    found = []
+    for var in variables:
+        for _, t in re.findall(r"(?P<pre>[^\w.])sum\(\s*([^()]+)\s*\)", var["eq"]):
+            found.append(t.strip())
+        if re.findall(r"([^\w.])sum\(\)", var["eq"]):
+            found.append("__all__")
+        for _, t in re.findall(r"([^\w.])g_([\w]+)", var["eq"]):
+            found.append(t.strip())
+    return sorted(set(found))
+
+
+def _unsupported(eq, where):
+    if re.search(r"\bite\(|\bif\b.*\belse\b", eq):
+        raise ParserError(f"{where}: if-then-else statements are not supported by this backend")
+    if re.search(r"\b(mean|min|max|norm1|norm2)\(", eq):
+        raise ParserError(f"{where}: global operations are not supported by this backend")
+    if re.search(r"\b(Uniform|Normal|LogNormal|Exponential|Gamma|Binomial|DiscreteUniform)\(", eq):
+        raise ParserError(f"{where}: random distributions in equations are not supported by "
+                          "this backend")
+
+
+def _bound_code(name, value, desc, untouched):
+    if isinstance(value, str):
+        try:
+            float(value)
+        except ValueError:
+            st = Statement(name, value, desc, untouched=untouched, kind="return")
+            return st.parse().replace(";", "")
+    return value
+
+
+# ---------------------------------------------------------------------------
+# neurons
+# ---------------------------------------------------------------------------
+
+def analyse_neuron(neuron) -> dict:
+    """Description dict of a neuron type (AnalyseNeuron.py:27-392)."""
+    desc = {"object": "neuron", "type": neuron.type, "raw_parameters": neuron.parameters,
+            "raw_equations": neuron.equations}
+    if neuron.type == "spike":
+        desc["raw_reset"] = neuron.reset
+        desc["raw_spike"] = neuron.spike
+        desc["refractory"] = neuron.refractory
+    params = extract_parameters(neuron.parameters, "neuron")
+    variables = extract_variables(neuron.equations)
+    desc["parameters"], desc["variables"] = params, variables
+    names = [v["name"] for v in params + variables]
+    if neuron.type == "rate":
+        if "r" not in names:
+            raise ParserError('rate-coded neurons must define the variable "r"')
+    else:
+        if "r" in names:
+            raise ParserError('spiking neurons use "r" for the mean firing rate; use another name')
+        variables.append(dict(name="r", locality="local", bounds={}, ctype="double", init=0.0,
+                              flags=[], eq="", cpp=""))
+    attributes, local, global_, _ = _split_locality(params + variables, neuron=True)
+    if len(attributes) != len(set(attributes)):
+        raise ParserError("attributes must be declared only once: " + str(attributes))
+    desc.update(attributes=attributes, local=local, semiglobal=[], global_=None)
+    desc["global"] = global_
+    del desc["global_"]
+    targets = _targets(variables)
+    desc["targets"] = targets
+    if neuron.type == "spike":
+        for t in targets:
+            if not any(v["name"] == "g_" + t for v in variables):
+                variables.append(dict(name="g_" + t, locality="local", bounds={}, ctype="double",
+                                      init=0.0, flags=[], eq="g_" + t + " = 0.0"))
+                desc["attributes"].append("g_" + t)
+                desc["local"].append("g_" + t)
+        desc["spike"] = _spike(desc)
+    for var in variables:
+        eq = var.get("transformed_eq", var["eq"])
+        if eq.strip() == "":
+            continue
+        _unsupported(eq, var["name"])
+        untouched = {}
+        for t in targets:
+            eq = re.sub(r"(?P<pre>[^\w.])sum\(\)", r"\1sum(__all__)", eq)
+            eq = re.sub(r"sum\(\s*" + t + r"\s*\)", "__sum_" + t + "__", eq)
+            untouched["__sum_" + t + "__"] = "_sum_" + t + "%(local_index)s"
+        method = _method(var)
+        for b in ("min", "max"):
+            if b in var["bounds"]:
+                var["bounds"][b] = _bound_code(var["name"], var["bounds"][b], desc, untouched)
+        st = Statement(var["name"], eq, desc, untouched=untouched, method=method)
+        code = st.parse()
+        if isinstance(code, str):
+            pre_loop, cpp, switch = {}, code, None
+        else:
+            pre_loop, cpp, switch = code
+        for prev, new in sorted(untouched.items(), key=lambda kv: len(kv[0]), reverse=True):
+            cpp = re.sub(prev, new, cpp)
+            if pre_loop:
+                pre_loop["value"] = re.sub(prev, new, pre_loop["value"])
+            if switch:
+                switch = re.sub(prev, new, switch)
+        var.update(pre_loop=pre_loop, cpp=cpp, switch=switch, transformed_eq=eq,
+                   untouched=untouched, method=method, dependencies=sorted(set(st.dependencies())))
+        if method in ("implicit", "semiimplicit", "midpoint", "rk4") and switch is not None:
+            raise ParserError(f"{var['name']}: method {method!r} is not supported by this backend")
+    return desc
+
+
+def _spike(desc):
+    cond = statements(desc["raw_spike"])
+    if len(cond) != 1:
+        raise ParserError("the spike condition must be a single expression")
+    st = Statement("raw_spike_cond", cond[0].strip(), desc)
+    spike_cond = st.parse()
+    resets = []
+    raw = desc.get("raw_reset")
+    if raw:
+        for var in equation_list(raw):
+            rs = Statement(var["name"], var["eq"], desc)
+            var["cpp"] = rs.parse()
+            var["dependencies"] = rs.dependencies()
+            resets.append(var)
+    return {"spike_cond": spike_cond, "spike_cond_dependencies": st.dependencies(),
+            "spike_reset": resets}
+
+
+# ---------------------------------------------------------------------------
+# synapses
+# ---------------------------------------------------------------------------
+
+def _prepost(eq):
+    """pre.x / post.x -> placeholders (Extraction.py:189-248)."""
+    untouched = {}
+    for var in sorted(set(re.findall(r"pre\.([\w]+)", eq))):
+        if var == "sum":
+            def rep(m):
+                t = m.group(1).strip()
+                untouched["_pre_sum_" + t] = "%(pre_prefix)s_sum_" + t + "%(pre_index)s"
+                return "_pre_sum_" + t
+            eq = re.sub(r"pre\.sum\(([\s\w]+)\)", rep, eq)
+        else:
+            eq = re.sub(r"pre." + var + r"([^_\w]+)", "_pre_" + var + r"__\g<1>", eq + " ")
+            untouched["_pre_" + var + "__"] = "%(pre_prefix)s" + var + "%(pre_index)s"
+    for var in sorted(set(re.findall(r"post\.([\w]+)", eq))):
+        if var == "sum":
+            def rep(m):
+                t = m.group(1).strip()
+                untouched["_post_sum_" + t] = "%(post_prefix)s_sum_" + t + "%(post_index)s"
+                return "_post_sum_" + t
+            eq = re.sub(r"post\.sum\(([\s\w]+)\)", rep, eq)
+        else:
+            eq = re.sub(r"post." + var + r"([^_\w]+)", "_post_" + var + r"__\g<1>", eq + " ")
+            untouched["_post_" + var + "__"] = "%(post_prefix)s" + var + "%(post_index)s"
+    return eq, untouched
+
+
+def _event_statements(raw):
+    out = []
+    if not raw:
+        return out
+    for var in equation_list(raw):
+        bounds, flags = parse_flags(var["constraint"])
+        ctype, init = _typed_init(bounds, flags)
+        out.append(dict(name=var["name"], eq=var["eq"], locality="local", bounds=bounds,
+                        flags=flags, ctype=ctype, init=init))
+    return out
+
+
+def analyse_synapse(synapse) -> dict:
+    """Description dict of a synapse type (AnalyseSynapse.py:34-590)."""
+    desc = {"object": "synapse", "type": synapse.type, "raw_parameters": synapse.parameters,
+            "raw_equations": synapse.equations}
+    if synapse.psp:
+        desc["raw_psp"] = synapse.psp
+    elif synapse.type == "rate":
+        desc["raw_psp"] = "w*pre.r"
+    params = extract_parameters(synapse.parameters, "synapse")
+    variables = extract_variables(synapse.equations)
+    if not any(v["name"] == "w" for v in params + variables):
+        params.append(dict(name="w", bounds={}, ctype="double", init=0.0, flags=[], eq="w=0.0",
+                           locality="local"))
+    desc["plasticity"] = any(v["name"] == "w" for v in variables)
+    attributes, local, global_, semiglobal = _split_locality(params + variables, neuron=False)
+    if len(attributes) != len(set(attributes)):
+        raise ParserError("attributes must be declared only once: " + str(attributes))
+    desc.update(parameters=params, variables=variables, attributes=attributes, local=local,
+                semiglobal=semiglobal)
+    desc["global"] = global_
+    if synapse.type == "spike":
+        desc["pre_spike"] = _event_statements(synapse.pre_spike)
+        desc["post_spike"] = _event_statements(synapse.post_spike)
+        for group, skip in (("pre_spike", ("g_target",)), ("post_spike", ("g_target", "w"))):
+            for var in desc[group]:
+                if var["name"] in skip or any(v["name"] == var["name"] for v in variables):
+                    continue
+                variables.append(dict(name=var["name"], bounds=var["bounds"], ctype=var["ctype"],
+                                      init=var["init"], locality=var["locality"], flags=[],
+                                      transformed_eq="", eq="", cpp="", switch="",
+                                      untouched="", method="explicit"))
+                desc["local"].append(var["name"])
+                desc["attributes"].append(var["name"])
+    untouched_all = {}
+    for var in variables:
+        eq = var.get("transformed_eq", var["eq"])
+        if eq.strip() == "":
+            continue
+        _unsupported(eq, var["name"])
+        eq, untouched = _prepost(eq)
+        for k, v in untouched.items():
+            untouched_all.setdefault(k, v)
+        method = _method(var)
+        for b in ("min", "max"):
+            if b in var["bounds"]:
+                var["bounds"][b] = _bound_code(var["name"], var["bounds"][b], desc,
+                                               list(untouched_all))
+        st = Statement(var["name"], eq, desc, untouched=list(untouched_all), method=method)
+        code = st.parse()
+        if isinstance(code, str):
+            pre_loop, cpp, switch = {}, code, None
+        else:
+            pre_loop, cpp, switch = code
+        for prev, new in sorted(untouched_all.items(), key=lambda kv: len(kv[0]), reverse=True):
+            cpp = cpp.replace(prev, new)
+        var.update(pre_loop=pre_loop, cpp=cpp, switch=switch, transformed_eq=eq,
+                   untouched=dict(untouched_all), method=method,
+                   dependencies=st.dependencies())
+        if method in ("implicit", "semiimplicit", "midpoint", "rk4") and switch is not None:
+            raise ParserError(f"{var['name']}: method {method!r} is not supported by this backend")
+    if "raw_psp" in desc:
+        eq, untouched = _prepost(" " + desc["raw_psp"].strip() + " ")
+        for k, v in untouched.items():
+            untouched_all.setdefault(k, v)
+        st = Statement("psp", eq, desc, untouched=list(untouched_all), kind="return")
+        code = st.parse()
+        for prev, new in sorted(untouched_all.items(), key=lambda kv: len(kv[0]), reverse=True):
+            code = code.replace(prev, new)
+        desc["psp"] = {"eq": desc["raw_psp"].strip(), "cpp": code}
+    if synapse.type == "spike":
+        for var in desc["pre_spike"] + desc["post_spike"]:
+            if var["name"] == "w":
+                desc["plasticity"] = True
+            _unsupported(var["eq"], var["name"])
+            eq, untouched = _prepost(var["eq"])
+            st = Statement(var["name"], eq, desc, untouched=untouched, method="explicit")
+            code = st.parse()
+            if isinstance(code, list):
+                raise ParserError("ODEs are not allowed in pre_spike/post_spike: " + var["eq"])
+            for prev, new in sorted(untouched.items(), key=lambda kv: len(kv[0]), reverse=True):
+                code = code.replace(prev, new)
+            for b in ("min", "max"):
+                if b in var["bounds"]:
+                    var["bounds"][b] = _bound_code(var["name"], var["bounds"][b], desc, untouched)
+            var["cpp"] = code
+            var["dependencies"] = st.dependencies()
+    return desc
+
+
+__all__ = ["analyse_neuron", "analyse_synapse", "ParserError", "BUILTIN_FUNCTIONS"]

@@ -1,0 +1,259 @@
+"""Seeded synthetic networks for the benchmark configurations.
+
+Every random array is drawn here from ``numpy.random.default_rng(seed)`` and
+injected into a network explicitly (connectivity through ``from_sparse``,
+initial states as arrays), because the reference simulator's own
+``Uniform``/``Normal`` draw from an unseeded generator unless given ``rng=``
+(ANNarchy/core/Random.py:88-92) and two runs of one script differ.
+
+Connectivity is returned as ``scipy.sparse.csr_matrix`` of shape
+(post, pre) with column indices ascending in every row: the order in which
+the reference's ``from_sparse`` builds each dendrite
+(ANNarchy/core/ConnectorMethods.py:763-796). ``to_from_sparse`` gives the
+(pre, post) matrix that ``Projection.from_sparse`` takes.
+
+Workloads (sizes and values as in the benchmark configurations):
+
+* ``rate_net``   - constant-rate inputs feeding leaky integrators through a
+  Bernoulli-masked input projection and a recurrent projection (the
+  1000 -> 4000 rate-coded net, 1000 steps at dt = 1 ms).
+* ``coba_net``   - conductance-based LIF network, 80 % excitatory, Bernoulli
+  connectivity p = 0.02, constant weights 0.6 / 6.7, v0 ~ U[-60, -50] mV
+  (the 4000-neuron spiking net, 10,000 steps at dt = 0.1 ms). A constant
+  drive ``I`` is part of the neuron model: without it the network as
+  specified never fires.
+* ``sweep_matrix`` - 100k-row recurrent matrices with the four connectivity
+  structures used for the format study.
+* ``batched_coba`` - uneven-size instances of the spiking net for the
+  batched sweep.
+"""
+from __future__ import annotations
+
+import hashlib
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+
+
+def bernoulli_csr(rng: np.random.Generator, n_post: int, n_pre: int, p: float,
+                  weights) -> sp.csr_matrix:
+    """(post, pre) matrix whose entries exist independently with probability p.
+
+    ``weights`` is either a scalar or a callable ``f(n) -> ndarray`` that gives
+    the values of the n existing entries in row-major order.
+    """
+    mask = rng.random((n_post, n_pre)) < p
+    rows, cols = np.nonzero(mask)
+    nnz = rows.size
+    if callable(weights):
+        data = np.asarray(weights(nnz), dtype=np.float64)
+    else:
+        data = np.full(nnz, float(weights), dtype=np.float64)
+    m = sp.csr_matrix((data, (rows, cols)), shape=(n_post, n_pre))
+    m.sort_indices()
+    return m
+
+
+def to_from_sparse(m: sp.csr_matrix) -> sp.csr_matrix:
+    """(post, pre) -> the (pre, post) layout ``Projection.from_sparse`` expects."""
+    return m.T.tocsr()
+
+
+def csr_digest(m: sp.csr_matrix) -> str:
+    """Short content hash of a CSR matrix (structure and values)."""
+    h = hashlib.sha256()
+    h.update(np.asarray(m.indptr, dtype=np.int64).tobytes())
+    h.update(np.asarray(m.indices, dtype=np.int64).tobytes())
+    h.update(np.asarray(m.data, dtype=np.float64).tobytes())
+    return h.hexdigest()[:16]
+
+
+@dataclass
+class RateNet:
+    n_in: int
+    n_out: int
+    w_in: sp.csr_matrix          # (n_out, n_in)
+    w_rec: sp.csr_matrix         # (n_out, n_out)
+    r_in: np.ndarray             # (n_in,)
+    tau: float = 10.0
+    dt: float = 1.0
+    steps: int = 1000
+
+    @property
+    def nnz(self) -> int:
+        return int(self.w_in.nnz + self.w_rec.nnz)
+
+
+def rate_net(seed: int = 42, n_in: int = 1000, n_out: int = 4000,
+             p_in: float = 0.1, p_rec: float = 0.02,
+             sd_in: float = 0.05, sd_rec: float = 0.02,
+             steps: int = 1000) -> RateNet:
+    rng = np.random.default_rng(seed)
+    w_in = bernoulli_csr(rng, n_out, n_in, p_in, lambda n: rng.normal(0.0, sd_in, n))
+    w_rec = bernoulli_csr(rng, n_out, n_out, p_rec, lambda n: rng.normal(0.0, sd_rec, n))
+    r_in = rng.uniform(0.0, 1.0, n_in)
+    return RateNet(n_in, n_out, w_in, w_rec, r_in, steps=steps)
+
+
+COBA_PARAMS = dict(El=-60.0, Vr=-60.0, Erev_exc=0.0, Erev_inh=-80.0, Vt=-50.0,
+                   tau=20.0, tau_exc=5.0, tau_inh=10.0, I=20.0)
+COBA_EQUATIONS = [
+    "tau * dv/dt = (El - v) + g_exc * (Erev_exc - v) + g_inh * (Erev_inh - v) + I",
+    "tau_exc * dg_exc/dt = - g_exc",
+    "tau_inh * dg_inh/dt = - g_inh",
+]
+COBA_SPIKE = "v > Vt"
+COBA_RESET = "v = Vr"
+COBA_REFRACTORY = 5.0
+
+STDP_PARAMS = dict(tau_plus=16.8, tau_minus=33.7, A_plus=0.005, A_minus=0.00525,
+                   w_min=0.0, w_max=1.0)
+
+
+@dataclass
+class CobaNet:
+    n: int
+    n_exc: int
+    w_exc: sp.csr_matrix         # (n, n_exc): excitatory pre ranks 0..n_exc-1
+    w_inh: sp.csr_matrix         # (n, n - n_exc): inhibitory pre ranks n_exc..n-1
+    v0: np.ndarray
+    params: dict = field(default_factory=lambda: dict(COBA_PARAMS))
+    dt: float = 0.1
+    steps: int = 10000
+    refractory: float = COBA_REFRACTORY
+
+    @property
+    def nnz(self) -> int:
+        return int(self.w_exc.nnz + self.w_inh.nnz)
+
+    def out_degree(self) -> np.ndarray:
+        """Number of efferent synapses of every neuron (over both projections)."""
+        deg = np.zeros(self.n, dtype=np.int64)
+        deg[: self.n_exc] = np.bincount(self.w_exc.indices, minlength=self.n_exc)
+        deg[self.n_exc:] = np.bincount(self.w_inh.indices, minlength=self.n - self.n_exc)
+        return deg
+
+
+def coba_net(seed: int = 42, n: int = 4000, exc_frac: float = 0.8, p: float = 0.02,
+             w_exc: float = 0.6, w_inh: float = 6.7, drive: float = 20.0,
+             steps: int = 10000) -> CobaNet:
+    rng = np.random.default_rng(seed)
+    n_exc = int(round(n * exc_frac))
+    v0 = rng.uniform(-60.0, -50.0, n)
+    we = bernoulli_csr(rng, n, n_exc, p, w_exc)
+    wi = bernoulli_csr(rng, n, n - n_exc, p, w_inh)
+    params = dict(COBA_PARAMS)
+    params["I"] = float(drive)
+    return CobaNet(n, n_exc, we, wi, v0, params=params, steps=steps)
+
+
+# ---------------------------------------------------------------------------
+# 100k-row matrices for the storage-format study
+# ---------------------------------------------------------------------------
+
+def sweep_matrix(kind: str, seed: int = 42, n: int = 100_000, mean_nnz: int = 100,
+                 sd: float = 0.01) -> sp.csr_matrix:
+    """(n, n) recurrent matrices with the four connectivity structures.
+
+    kind: 'uniform' (exactly mean_nnz distinct random columns per row),
+    'powerlaw' (Zipf-like row lengths, exponent 2, clipped to [k_min, 20000]
+    with k_min chosen so the mean is close to mean_nnz), 'local' (Gaussian
+    neighbourhood on a square grid, sigma 5, cutoff 15) or 'blocks' (64x64
+    dense blocks at 2 % block density).
+    """
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        cols = np.empty((n, mean_nnz), dtype=np.int64)
+        for r0 in range(0, n, 4096):
+            r1 = min(n, r0 + 4096)
+            keys = rng.random((r1 - r0, n), dtype=np.float32)
+            cols[r0:r1] = np.argpartition(keys, mean_nnz, axis=1)[:, :mean_nnz]
+        cols.sort(axis=1)
+        indptr = np.arange(0, n * mean_nnz + 1, mean_nnz, dtype=np.int64)
+        data = rng.normal(0.0, sd, n * mean_nnz)
+        return sp.csr_matrix((data, cols.ravel(), indptr), shape=(n, n))
+    if kind == "powerlaw":
+        kmax = 20000
+        # continuous power law p(k) ~ k^-2 on [kmin, kmax]; mean = kmin*kmax*ln(kmax/kmin)/(kmax-kmin)
+        lo, hi = 1.0, float(mean_nnz)
+        for _ in range(60):
+            mid = 0.5 * (lo + hi)
+            m = mid * kmax * np.log(kmax / mid) / (kmax - mid)
+            lo, hi = (mid, hi) if m < mean_nnz else (lo, mid)
+        kmin = 0.5 * (lo + hi)
+        u = rng.random(n)
+        k = kmin * kmax / (kmax - u * (kmax - kmin))      # inverse CDF of k^-2
+        lengths = np.clip(np.rint(k).astype(np.int64), 1, kmax)
+        indptr = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(lengths, out=indptr[1:])
+        cols = np.empty(indptr[-1], dtype=np.int64)
+        for r in range(n):
+            L = lengths[r]
+            if L * 4 < n:
+                c = np.unique(rng.integers(0, n, int(L * 1.2) + 8))
+                while c.size < L:
+                    c = np.unique(np.concatenate([c, rng.integers(0, n, L)]))
+                c = rng.choice(c, L, replace=False)
+            else:
+                c = rng.choice(n, L, replace=False)
+            c.sort()
+            cols[indptr[r]:indptr[r + 1]] = c
+        data = rng.normal(0.0, sd, cols.size)
+        return sp.csr_matrix((data, cols, indptr), shape=(n, n))
+    if kind == "local":
+        side = int(round(np.sqrt(n)))
+        n = side * side
+        sigma, cutoff = 5.0, 15
+        offs = [(dy, dx) for dy in range(-cutoff, cutoff + 1) for dx in range(-cutoff, cutoff + 1)
+                if dy * dy + dx * dx <= cutoff * cutoff]
+        offs = np.array(offs, dtype=np.int64)
+        prob = np.exp(-(offs ** 2).sum(1) / (2 * sigma * sigma))
+        ys, xs = np.divmod(np.arange(n), side)
+        rows_l, cols_l = [], []
+        for r0 in range(0, n, 8192):
+            r1 = min(n, r0 + 8192)
+            ty = ys[r0:r1, None] + offs[None, :, 0]
+            tx = xs[r0:r1, None] + offs[None, :, 1]
+            ok = (ty >= 0) & (ty < side) & (tx >= 0) & (tx < side)
+            ok &= rng.random(ok.shape) < prob[None, :]
+            rr, kk = np.nonzero(ok)
+            rows_l.append(rr + r0)
+            cols_l.append(ty[rr, kk] * side + tx[rr, kk])
+        rows = np.concatenate(rows_l)
+        cols = np.concatenate(cols_l)
+        data = rng.normal(0.0, sd, rows.size)
+        m = sp.csr_matrix((data, (rows, cols)), shape=(n, n))
+        m.sort_indices()
+        return m
+    if kind == "blocks":
+        bs = 64
+        nb = (n + bs - 1) // bs
+        n = nb * bs
+        bmask = rng.random((nb, nb)) < 0.02
+        brow, bcol = np.nonzero(bmask)
+        rr = (brow[:, None] * bs + np.arange(bs)[None, :])          # (nblk, 64)
+        cc = (bcol[:, None] * bs + np.arange(bs)[None, :])
+        rows = np.repeat(rr, bs, axis=1).ravel()
+        cols = np.tile(cc, (1, bs)).ravel()
+        data = rng.normal(0.0, sd, rows.size)
+        m = sp.csr_matrix((data, (rows, cols)), shape=(n, n))
+        m.sort_indices()
+        return m
+    raise ValueError(f"unknown connectivity structure {kind!r}")
+
+
+def batched_coba(n_instances: int = 256, seed: int = 42, n_min: int = 1000,
+                 n_max: int = 8000, steps: int = 5000) -> list[CobaNet]:
+    """Uneven-size spiking networks; excitatory increment swept 0.2-1.0 and
+    inhibitory increment 2-10 over a square grid, one seed per instance."""
+    side = int(np.ceil(np.sqrt(n_instances)))
+    we = np.linspace(0.2, 1.0, side)
+    wi = np.linspace(2.0, 10.0, side)
+    size_rng = np.random.default_rng(seed)
+    sizes = size_rng.integers(n_min, n_max + 1, n_instances)
+    nets = []
+    for i in range(n_instances):
+        nets.append(coba_net(seed=seed + i, n=int(sizes[i]), w_exc=float(we[i % side]),
+                             w_inh=float(wi[i // side]), steps=steps))
+    return nets

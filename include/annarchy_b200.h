@@ -1,0 +1,137 @@
+/*
+ * annarchy_b200 — C ABI of the B200 simulation backend.
+ *
+ * This library replaces the per-network extension module that the reference
+ * simulator generates and loads (ANNarchyWrapper<id>, emitted by
+ * ANNarchy/generator/NanoBind/Generator.py:18-434 from the template
+ * ANNarchy/generator/NanoBind/BaseTemplate.py:1-45). The reference's Python
+ * core drives that module through a small set of calls — create the core,
+ * set the device, initialise with dt, upload connectivity, get/set
+ * attributes, run(n)/step(), set/get time — and this header provides the
+ * same operations with plain pointers, sizes and status codes:
+ *
+ *   - No exception crosses the boundary: every call returns an anb_status;
+ *     anb_last_error() gives the message of the last failure on this thread.
+ *   - Populations and projections are not C types here. Every attribute of
+ *     a population or projection is a named device array ("pop0__v",
+ *     "proj1__w", ...); the host side converts the reference's LIL/CSR
+ *     connectivity into the storage format and writes it with
+ *     anb_array_write. The generated per-network CUDA module declares one
+ *     __constant__ pointer "anb_p_<array name>" per array it uses, and the
+ *     library binds those pointers to the arrays.
+ *   - The per-step work is a list of kernels from that module (grid engine,
+ *     one launch each per step, replayed as a CUDA graph) or one persistent
+ *     kernel that runs many steps per launch (local engine).
+ *
+ * Threading: calls on one network must not overlap. All device work is
+ * ordered on the network's stream.
+ */
+#ifndef ANNARCHY_B200_H
+#define ANNARCHY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum anb_status {
+  ANB_OK = 0,
+  ANB_ERR_ARG = 1,       /* invalid argument or unknown name */
+  ANB_ERR_ALLOC = 2,     /* device or host allocation failed */
+  ANB_ERR_CUDA = 3,      /* a CUDA runtime/driver call failed */
+  ANB_ERR_COMPILE = 4,   /* NVRTC rejected the generated module (log in anb_last_error) */
+  ANB_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up (see anb_device_error) */
+  ANB_ERR_STATE = 6      /* call out of order (e.g. run before a module is loaded) */
+} anb_status;
+
+typedef struct anb_net anb_net;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Version of this ABI (increments on incompatible changes). */
+int anb_abi_version(void);
+
+/* Message of the last failing call on the calling thread ("" if none). */
+const char* anb_last_error(void);
+
+/* Number of visible CUDA devices (0 without a GPU). */
+int anb_device_count(int* count);
+
+/* ---- network lifetime --------------------------------------------------
+ * anb_create replaces pyx_create() plus set_device(int)
+ * (ANNarchy/generator/NanoBind/BaseTemplate.py:1-45,
+ *  ANNarchy/generator/Template/CUDABaseTemplate.py:97-104);
+ * anb_initialize replaces pyx_initialize(double dt)
+ * (ANNarchy/generator/Compiler.py:888-905). */
+int anb_create(int device, anb_net** out);
+int anb_destroy(anb_net* net);
+int anb_initialize(anb_net* net, double dt);
+
+/* set_time(long) / get_time() of the generated module: the integer step
+ * counter t (simulated time is t*dt). */
+int anb_set_time(anb_net* net, int64_t t);
+int anb_get_time(anb_net* net, int64_t* t);
+
+/* Use a caller-provided cudaStream_t (NULL: the library's own stream). */
+int anb_set_stream(anb_net* net, void* cuda_stream);
+
+/* ---- named device arrays ------------------------------------------------
+ * Replace the per-attribute get/set properties of pop<k>_wrapper and the
+ * init_from_lil / get/set_local_attribute_* methods of proj<k>_wrapper
+ * (ANNarchy/generator/NanoBind/Population.py:27-54,
+ *  ANNarchy/generator/NanoBind/Projection.py:20-179). Arrays are zeroed
+ * on creation. Reads and writes are synchronous with the network's stream. */
+int anb_array_create(anb_net* net, const char* name, size_t bytes);
+int anb_array_free(anb_net* net, const char* name);
+int anb_array_write(anb_net* net, const char* name, size_t offset, const void* src, size_t bytes);
+int anb_array_read(anb_net* net, const char* name, size_t offset, void* dst, size_t bytes);
+int anb_array_fill_zero(anb_net* net, const char* name);
+int anb_array_info(anb_net* net, const char* name, void** device_ptr, size_t* bytes);
+
+/* ---- generated module ---------------------------------------------------
+ * Compiles CUDA C++ source with NVRTC for sm_100a, loads it and binds its
+ * __constant__ pointers named "anb_p_<array>" to the arrays of the same
+ * name. `options` is a '\n'-separated list of extra NVRTC options. Replaces
+ * the reference's CMake/nvcc build of the generated network
+ * (ANNarchy/generator/Compiler.py:496-596). */
+int anb_module_load(anb_net* net, const char* source, const char* options);
+
+/* Kernels launched, in order, once per simulation step (grid engine). */
+int anb_plan_clear(anb_net* net);
+int anb_plan_add(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                 unsigned shared_bytes);
+
+/* Local engine: one kernel `kernel(long long t0, int nsteps)` that runs
+ * nsteps steps per launch (grid CTAs, each owning whole network instances). */
+int anb_set_local_kernel(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                         unsigned shared_bytes);
+
+/* Steps per captured CUDA graph in the grid engine (0 = no graph). */
+int anb_set_graph_steps(anb_net* net, int steps);
+
+/* run(int) and step() of the generated module
+ * (ANNarchy/generator/Template/CUDABaseTemplate.py:328-630, called from
+ * ANNarchy/core/Simulate.py:76-87). Returns after the work is queued;
+ * anb_synchronize waits and reports device-side errors. */
+int anb_run(anb_net* net, int64_t nsteps);
+int anb_step(anb_net* net);
+int anb_synchronize(anb_net* net);
+
+/* Device-side error word: 0, or the code a kernel wrote when a bounded wait
+ * gave up or an index check failed; anb_clear_device_error resets it. */
+int anb_device_error(anb_net* net, int* code);
+int anb_clear_device_error(anb_net* net);
+
+/* ---- per-kernel timing (CUDA events around every launch; no graphs) ----- */
+int anb_kernel_timing(anb_net* net, int enable);
+int anb_kernel_time_count(anb_net* net, int* count);
+int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len,
+                        double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ANNARCHY_B200_H */

@@ -1,0 +1,281 @@
+/*
+ * CPU oracle — TEST INFRASTRUCTURE ONLY.
+ *
+ * A C restatement of the reference simulator's CPU step for the model
+ * families of the benchmark configurations, used by the test suite to check
+ * the CUDA backend, by __graft_entry__.smoke() as the checker, and by
+ * bench.py as the timed CPU baseline. Nothing in the backend calls it.
+ *
+ * It restates, in the reference's operation order and with IEEE-754 double
+ * arithmetic (build with -ffp-contract=off so no multiply-add is fused):
+ *
+ *  - the step order of the generated core (ANNarchy/generator/Template/
+ *    OpenMPBaseTemplate.py:131-484): zero rate sums -> compute_psp of every
+ *    projection (spikes of the previous step) -> neuron update -> spike
+ *    gather (ascending ranks) -> post_event of plastic projections -> t++;
+ *  - the rate-coded weighted sum of a CSR projection, one sequential sum per
+ *    row in ascending pre rank, then `_sum[post] += sum`
+ *    (ANNarchy/generator/Projection/OpenMP/CSR.py:177-253);
+ *  - event-driven transmission: for every spiking pre neuron in ascending
+ *    rank, for its synapses in ascending post rank, `g[post] += w`
+ *    (OpenMP/CSR.py:870-902), with the STDP pre-spike statements inlined
+ *    (ANNarchy/generator/Projection/OpenMPGenerator.py:910-1100) and the
+ *    post-spike statements of post_event (OpenMP/CSR.py:903-922);
+ *  - the neuron updates emitted for the leaky integrator
+ *    "tau*dr/dt + r = sum(exc) : min=0.0" and for the conductance-based LIF
+ *    of the spiking configurations, with the refractory mask of
+ *    ANNarchy/generator/Population/OpenMPGenerator.py:870-998 and the spike
+ *    gather of :999-1237; refractory steps are int(refractory_ms / dt)
+ *    (ANNarchy/core/Population.py:659-690).
+ *
+ * Parity pinned against golden fixtures produced by running the reference
+ * itself (tests/golden/make_golden.py).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_CLIP(x, a, b) ((x) < (a) ? (a) : ((x) > (b) ? (b) : (x)))
+
+int orc_version(void) { return 1; }
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* rate-coded: leaky integrators fed by CSR projections                      */
+/* ------------------------------------------------------------------------ */
+
+/* One rate-coded projection into the integrator population.
+ * rows are post ranks 0..n_post-1; col holds pre ranks of population `pre`
+ * (0 = the input population, 1 = the integrator population itself). */
+typedef struct {
+  int pre;
+  const int* row_ptr;
+  const int* col;
+  const double* w;
+} orc_rate_proj;
+
+/* Simulates `steps` steps of: input population (constant r_in) and one
+ * leaky-integrator population of n_out neurons with a single target "exc".
+ * r (n_out) is the state (in/out). If r_trace != NULL it receives r after
+ * every step (steps x n_out). threads > 1 uses OpenMP like the reference's
+ * OpenMP paradigm (rows and neurons split across threads; results are
+ * identical to one thread). */
+int orc_rate_run(int n_in, int n_out, const double* r_in, double* r, int nproj,
+                 const orc_rate_proj* projs, double tau, double dt, double r_min, int steps,
+                 double* r_trace, int threads) {
+  double* sum = (double*)calloc((size_t)n_out, sizeof(double));
+  double* r_prev = (double*)malloc(sizeof(double) * (size_t)n_out);
+  if (!sum || !r_prev) {
+    free(sum);
+    free(r_prev);
+    return 1;
+  }
+#ifdef _OPENMP
+  if (threads < 1) threads = 1;
+#endif
+  for (int t = 0; t < steps; ++t) {
+    /* the reference reads r of the integrators as it is before this step's update */
+    memcpy(r_prev, r, sizeof(double) * (size_t)n_out);
+#pragma omp parallel num_threads(threads)
+    {
+#pragma omp for schedule(static)
+      for (int i = 0; i < n_out; ++i) sum[i] = 0.0;
+      for (int p = 0; p < nproj; ++p) {
+        const orc_rate_proj* pj = &projs[p];
+        const double* pre_r = pj->pre == 0 ? r_in : r_prev;
+#pragma omp for schedule(static)
+        for (int i = 0; i < n_out; ++i) {
+          double s = 0.0;
+          for (int j = pj->row_ptr[i]; j < pj->row_ptr[i + 1]; ++j) s += pre_r[pj->col[j]] * pj->w[j];
+          sum[i] += s;
+        }
+      }
+#pragma omp for schedule(static)
+      for (int i = 0; i < n_out; ++i) {
+        double _r = (sum[i] - r[i]) / tau;
+        r[i] += dt * _r;
+        if (r[i] < r_min) r[i] = r_min;
+      }
+    }
+    if (r_trace) memcpy(r_trace + (size_t)t * n_out, r, sizeof(double) * (size_t)n_out);
+  }
+  free(sum);
+  free(r_prev);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* spiking: conductance-based LIF population with event-driven projections   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  double El, Vr, Erev_exc, Erev_inh, Vt, tau, tau_exc, tau_inh, I;
+} orc_coba_params;
+
+typedef struct {
+  double tau_plus, tau_minus, A_plus, A_minus, w_min, w_max;
+} orc_stdp_params;
+
+/* One spiking projection within a population of n neurons.
+ * CSR part (post-major): rows r = 0..n_rows-1 are post ranks post_rank[r];
+ *   row_ptr/col: col = pre rank (population rank), ascending in each row.
+ * Column view for propagation: for every pre rank p in 0..n-1,
+ *   col_ptr[p]..col_ptr[p+1] lists (row_idx = row, inv_idx = synapse index
+ *   into the CSR arrays) in ascending row order.
+ * target: 0 -> g_exc, 1 -> g_inh. With stdp != NULL the projection is
+ * plastic and x, y, last_event (per synapse, CSR order) are its traces. */
+typedef struct {
+  int n_rows;
+  const int* post_rank;
+  const int* row_ptr;
+  const int* col;
+  double* w;
+  const int* col_ptr;
+  const int* row_idx;
+  const int* inv_idx;
+  int target;
+  const orc_stdp_params* stdp;
+  double* x;
+  double* y;
+  int64_t* last_event;
+} orc_spike_proj;
+
+/* Simulates `steps` steps starting at time step t0. State arrays (length n)
+ * are in/out. Every spike is appended to (spike_t, spike_i) up to
+ * max_spikes entries; *n_spikes receives the total number of spikes (which
+ * may exceed max_spikes). `spiked`/`n_spiked` carry the spike list of the
+ * previous step in and the last step's list out (length n). */
+int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double dt, int64_t t0,
+                 int steps, double* v, double* g_exc, double* g_inh, int* refractory_remaining,
+                 int64_t* last_spike, int nproj, const orc_spike_proj* projs, int* spiked,
+                 int* n_spiked, int32_t* spike_t, int32_t* spike_i, int64_t max_spikes,
+                 int64_t* n_spikes, int threads) {
+  short* in_ref = (short*)malloc(sizeof(short) * (size_t)n);
+  int* row_of = NULL;
+  if (!in_ref) return 1;
+  int64_t total = 0;
+  int ns = *n_spiked;
+#ifdef _OPENMP
+  if (threads < 1) threads = 1;
+#else
+  (void)threads;
+#endif
+  /* post rank -> row index for plastic projections (the reference searches post_rank) */
+  int any_plastic = 0;
+  for (int p = 0; p < nproj; ++p) any_plastic |= projs[p].stdp != NULL;
+  if (any_plastic) {
+    row_of = (int*)malloc(sizeof(int) * (size_t)n * (size_t)nproj);
+    if (!row_of) {
+      free(in_ref);
+      return 1;
+    }
+    for (int p = 0; p < nproj; ++p) {
+      for (int i = 0; i < n; ++i) row_of[(size_t)p * n + i] = -1;
+      for (int r = 0; r < projs[p].n_rows; ++r) row_of[(size_t)p * n + projs[p].post_rank[r]] = r;
+    }
+  }
+  for (int s = 0; s < steps; ++s) {
+    const int64_t t = t0 + s;
+    /* compute_psp: propagate the previous step's spikes, projection by projection */
+    for (int p = 0; p < nproj; ++p) {
+      const orc_spike_proj* pj = &projs[p];
+      double* g = pj->target == 0 ? g_exc : g_inh;
+      for (int k = 0; k < ns; ++k) {
+        const int pre = spiked[k];
+        const int beg = pj->col_ptr[pre], end = pj->col_ptr[pre + 1];
+        if (!pj->stdp) {
+#pragma omp parallel for num_threads(threads) schedule(static) if (end - beg > 4096)
+          for (int syn = beg; syn < end; ++syn) g[pj->post_rank[pj->row_idx[syn]]] += pj->w[pj->inv_idx[syn]];
+        } else {
+          const orc_stdp_params* sp = pj->stdp;
+          for (int syn = beg; syn < end; ++syn) {
+            const int j = pj->inv_idx[syn];
+            pj->x[j] *= exp(dt * (double)(pj->last_event[j] - (t - 1)) / (sp->tau_plus));
+            pj->y[j] *= exp(dt * (double)(pj->last_event[j] - (t - 1)) / (sp->tau_minus));
+            pj->last_event[j] = t;
+            g[pj->post_rank[pj->row_idx[syn]]] += pj->w[j];
+            pj->x[j] += sp->A_plus * sp->w_max;
+            pj->w[j] = ORC_CLIP(pj->w[j] + pj->y[j], sp->w_min, sp->w_max);
+          }
+        }
+      }
+    }
+    /* neuron update */
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int i = 0; i < n; ++i) in_ref[i] = (refractory_remaining[i] > 0) ? 0 : 1;
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      double _v = (prm->El + prm->Erev_exc * g_exc[i] + prm->Erev_inh * g_inh[i] + prm->I -
+                   g_exc[i] * v[i] - g_inh[i] * v[i] - v[i]) / prm->tau;
+      double _g_exc = -g_exc[i] / prm->tau_exc;
+      double _g_inh = -g_inh[i] / prm->tau_inh;
+      v[i] += dt * _v * in_ref[i];
+      g_exc[i] += dt * _g_exc;
+      g_inh[i] += dt * _g_inh;
+      refractory_remaining[i] -= (1 - in_ref[i]);
+    }
+    /* spike gather, ascending ranks */
+    ns = 0;
+    for (int i = 0; i < n; ++i) {
+      if (in_ref[i] == 0) continue;
+      if (v[i] > prm->Vt) {
+        v[i] = prm->Vr;
+        spiked[ns++] = i;
+        last_spike[i] = t;
+        refractory_remaining[i] = refractory_steps;
+        if (total < max_spikes) {
+          spike_t[total] = (int32_t)t;
+          spike_i[total] = i;
+        }
+        ++total;
+      }
+    }
+    /* post_event of plastic projections */
+    for (int p = 0; p < nproj; ++p) {
+      const orc_spike_proj* pj = &projs[p];
+      if (!pj->stdp) continue;
+      const orc_stdp_params* sp = pj->stdp;
+      for (int k = 0; k < ns; ++k) {
+        const int r = row_of[(size_t)p * n + spiked[k]];
+        if (r < 0) continue;
+        for (int j = pj->row_ptr[r]; j < pj->row_ptr[r + 1]; ++j) {
+          pj->x[j] *= exp(dt * (double)(pj->last_event[j] - (t)) / (sp->tau_plus));
+          pj->y[j] *= exp(dt * (double)(pj->last_event[j] - (t)) / (sp->tau_minus));
+          pj->last_event[j] = t;
+          pj->y[j] -= sp->A_minus * sp->w_max;
+          pj->w[j] = ORC_CLIP(pj->w[j] + pj->x[j], sp->w_min, sp->w_max);
+        }
+      }
+    }
+  }
+  *n_spiked = ns;
+  *n_spikes = total;
+  free(in_ref);
+  free(row_of);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* single operations (used by tests of individual kernels)                    */
+/* ------------------------------------------------------------------------ */
+
+/* sum[i] (+)= sequential row sum of w*x over row i of a CSR matrix. */
+void orc_csr_rowsum(int n_rows, const int64_t* row_ptr, const int* col, const double* w,
+                    const double* x, double* sum, int accumulate) {
+  for (int i = 0; i < n_rows; ++i) {
+    double s = 0.0;
+    for (int64_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) s += x[col[j]] * w[j];
+    sum[i] = accumulate ? sum[i] + s : s;
+  }
+}

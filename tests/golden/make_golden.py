@@ -1,0 +1,224 @@
+"""Generate the golden fixtures in this folder by running the reference
+simulator (ANNarchy 5.0.3) itself, in its single-thread CPU build.
+
+Run from the repository root, in a container that has the reference sources
+at /root/reference, g++, cmake and the pybind11 wheel in /opt/wheelhouse:
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py coba_small # one case
+
+Set-up, done once under /tmp/anb_golden (nothing is written to the reference
+tree and no reference source enters this repository):
+
+1. copy the reference sources to /tmp/anb_golden/src and build its Cython
+   extensions there (``setup.py build_ext --inplace``);
+2. install pybind11 from the offline wheelhouse into /tmp/anb_golden/pb;
+3. put ``refshim/`` on PYTHONPATH: an own ``nanobind`` stand-in whose CMake
+   config builds the reference's generated wrapper as a pybind11 module, and
+   empty ``h5py``/``matplotlib`` modules that the reference imports but these
+   cases do not use.
+
+Every network is compiled with ``-march=native -O3 -ffp-contract=off`` so
+that no multiply-add is contracted: the fixtures are the IEEE-754 double
+results of the reference's own operation order. All random arrays come from
+``annarchy_b200.workloads`` (seeded numpy) and are injected through
+``from_sparse`` and attribute arrays, so the same inputs can be rebuilt on any
+machine with the same numpy.
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference"
+WORK = "/tmp/anb_golden"
+SRC = os.path.join(WORK, "src")
+PB = os.path.join(WORK, "pb")
+FLAGS = "-march=native -O3 -ffp-contract=off"
+
+
+def setup_env() -> dict:
+    os.makedirs(WORK, exist_ok=True)
+    if not os.path.isdir(SRC):
+        shutil.copytree(REF, SRC)
+    if not os.path.exists(os.path.join(SRC, ".built")):
+        subprocess.check_call([sys.executable, "setup.py", "build_ext", "--inplace"], cwd=SRC,
+                              stdout=subprocess.DEVNULL)
+        open(os.path.join(SRC, ".built"), "w").close()
+    if not os.path.isdir(os.path.join(PB, "pybind11")):
+        subprocess.check_call([sys.executable, "-m", "pip", "install", "--no-index", "--quiet",
+                               "--find-links", "/opt/wheelhouse", "--target", PB, "pybind11"])
+    env = dict(os.environ)
+    env["PYTHONPATH"] = os.pathsep.join([SRC, os.path.join(HERE, "refshim"), PB, REPO])
+    env["ANB_PYBIND11_INCLUDE"] = os.path.join(PB, "pybind11", "include")
+    return env
+
+
+# ---------------------------------------------------------------------------
+# Cases (executed in a child process with the reference importable)
+# ---------------------------------------------------------------------------
+
+def _spikes_to_arrays(spk: dict):
+    import numpy as np
+    steps, idx = [], []
+    for n, ts in spk.items():
+        steps.extend(ts)
+        idx.extend([n] * len(ts))
+    steps = np.asarray(steps, dtype=np.int64)
+    idx = np.asarray(idx, dtype=np.int64)
+    order = np.lexsort((idx, steps))
+    return steps[order].astype(np.int32), idx[order].astype(np.int32)
+
+
+def _coba_neuron(ann, params):
+    from annarchy_b200 import workloads as wl
+    return ann.Neuron(parameters=dict(params), equations=list(wl.COBA_EQUATIONS),
+                      spike=wl.COBA_SPIKE, reset=wl.COBA_RESET, refractory=wl.COBA_REFRACTORY)
+
+
+def case_rate(name, seed, n_in, n_out, p_in, p_rec, steps, record_steps):
+    import numpy as np
+    import ANNarchy as ann
+    from annarchy_b200 import workloads as wl
+    rn = wl.rate_net(seed=seed, n_in=n_in, n_out=n_out, p_in=p_in, p_rec=p_rec, steps=steps)
+    net = ann.Network(dt=rn.dt, seed=seed)
+    net.config(num_threads=1)
+    inp = net.create(n_in, ann.Neuron(parameters="r=0.0"))
+    li = ann.Neuron(parameters=dict(tau=rn.tau), equations="tau*dr/dt + r = sum(exc) : min=0.0")
+    pop = net.create(n_out, li)
+    p1 = net.connect(inp, pop, "exc")
+    p1.from_sparse(wl.to_from_sparse(rn.w_in), storage_format="csr")
+    p2 = net.connect(pop, pop, "exc")
+    p2.from_sparse(wl.to_from_sparse(rn.w_rec), storage_format="csr")
+    m = net.monitor(pop, "r")
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    inp.r = rn.r_in
+    net.simulate(steps * rn.dt)
+    r = np.asarray(m.get("r"))
+    out = dict(seed=seed, n_in=n_in, n_out=n_out, p_in=p_in, p_rec=p_rec, steps=steps,
+               digest_in=wl.csr_digest(rn.w_in), digest_rec=wl.csr_digest(rn.w_rec),
+               record_steps=np.asarray(record_steps, dtype=np.int64),
+               r_at=r[record_steps], r_sum=r.sum(axis=1), r_final=r[-1])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def case_coba(name, seed, n, p, steps, v_every, stdp=False):
+    import numpy as np
+    import ANNarchy as ann
+    from annarchy_b200 import workloads as wl
+    cn = wl.coba_net(seed=seed, n=n, p=p, steps=steps)
+    net = ann.Network(dt=cn.dt, seed=seed)
+    net.config(num_threads=1)
+    P = net.create(n, _coba_neuron(ann, cn.params))
+    Pe, Pi = P[: cn.n_exc], P[cn.n_exc:]
+    extra = {}
+    if stdp:
+        # plastic E->E (weights U[0, 0.5]), static E->I and I->all
+        rng = np.random.default_rng(seed + 1000)
+        w_ee = wl.bernoulli_csr(rng, cn.n_exc, cn.n_exc, p, lambda k: rng.uniform(0.0, 0.5, k))
+        w_ei = cn.w_exc[cn.n_exc:]
+        syn = ann.STDP(**wl.STDP_PARAMS)
+        ee = net.connect(Pe, Pe, "exc", synapse=syn)
+        ee.from_sparse(wl.to_from_sparse(w_ee), storage_format="csr")
+        ei = net.connect(Pe, Pi, "exc")
+        ei.from_sparse(wl.to_from_sparse(w_ei), storage_format="csr")
+        extra.update(digest_ee=wl.csr_digest(w_ee), digest_ei=wl.csr_digest(w_ei))
+    else:
+        ce = net.connect(Pe, P, "exc")
+        ce.from_sparse(wl.to_from_sparse(cn.w_exc), storage_format="csr")
+    ci = net.connect(Pi, P, "inh")
+    ci.from_sparse(wl.to_from_sparse(cn.w_inh), storage_format="csr")
+    m = net.monitor(P, ["spike"])
+    mv = net.monitor(P, ["v"], period=v_every * cn.dt) if v_every else None
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    P.v = cn.v0
+    net.simulate(steps * cn.dt)
+    s_steps, s_idx = _spikes_to_arrays(m.get("spike"))
+    out = dict(seed=seed, n=n, p=p, steps=steps, digest_exc=wl.csr_digest(cn.w_exc),
+               digest_inh=wl.csr_digest(cn.w_inh), spike_steps=s_steps, spike_idx=s_idx,
+               v_final=np.asarray(P.v), g_exc_final=np.asarray(P.g_exc),
+               g_inh_final=np.asarray(P.g_inh), **extra)
+    if mv is not None:
+        out["v_every"] = v_every
+        out["v_trace"] = np.asarray(mv.get("v"))
+    if stdp:
+        out["w_ee_final"] = np.concatenate([np.asarray(d, dtype=np.float64) for d in ee.w])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def case_parser(name):
+    """Description dicts of the reference parser for a set of models."""
+    import ANNarchy as ann
+    from ANNarchy.parser.AnalyseNeuron import analyse_neuron
+    from ANNarchy.parser.AnalyseSynapse import analyse_synapse
+    from annarchy_b200.parser.models_catalog import NEURONS, SYNAPSES
+    net = ann.Network(dt=0.1)
+    res = {"neurons": {}, "synapses": {}}
+    for key, spec in NEURONS.items():
+        d = analyse_neuron(ann.Neuron(**spec), net.id)
+        res["neurons"][key] = _digest_desc(d)
+    for key, spec in SYNAPSES.items():
+        d = analyse_synapse(ann.Synapse(**spec), net.id)
+        res["synapses"][key] = _digest_desc(d)
+    with open(os.path.join(HERE, name + ".json"), "w") as f:
+        json.dump(res, f, indent=1, sort_keys=True)
+
+
+def _digest_desc(d):
+    keep = {}
+    keep["type"] = d.get("type")
+    keep["local"] = list(d.get("local", []))
+    keep["global"] = list(d.get("global", []))
+    keep["semiglobal"] = list(d.get("semiglobal", []))
+    keep["targets"] = list(d.get("targets", []))
+    keep["variables"] = [dict(name=v["name"], cpp=v.get("cpp"), switch=v.get("switch"),
+                              bounds=v.get("bounds", {}), init=v.get("init"),
+                              locality=v.get("locality"), method=v.get("method"))
+                         for v in d.get("variables", [])]
+    keep["parameters"] = [dict(name=v["name"], init=v.get("init"), locality=v.get("locality"))
+                          for v in d.get("parameters", [])]
+    if d.get("spike"):
+        keep["spike_cond"] = d["spike"]["spike_cond"]
+        keep["spike_reset"] = [r["cpp"] for r in d["spike"]["spike_reset"]]
+    if "refractory" in d:
+        keep["refractory"] = d["refractory"]
+    for k in ("pre_spike", "post_spike"):
+        if d.get(k):
+            keep[k] = [v["cpp"] for v in d[k]]
+    if d.get("psp"):
+        keep["psp"] = d["psp"].get("cpp")
+    return keep
+
+
+CASES = {
+    "parser_strings": (case_parser, dict()),
+    "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
+                                   record_steps=list(range(100)))),
+    "rate_c1": (case_rate, dict(seed=42, n_in=1000, n_out=4000, p_in=0.1, p_rec=0.02, steps=1000,
+                                record_steps=[0, 1, 9, 99, 499, 998, 999])),
+    "coba_small": (case_coba, dict(seed=7, n=400, p=0.05, steps=2000, v_every=50)),
+    "coba_c2": (case_coba, dict(seed=42, n=4000, p=0.02, steps=10000, v_every=0)),
+    "stdp_small": (case_coba, dict(seed=11, n=400, p=0.05, steps=2000, v_every=0, stdp=True)),
+}
+
+
+def main():
+    if len(sys.argv) > 2 and sys.argv[1] == "--run":
+        fn, kw = CASES[sys.argv[2]]
+        fn(sys.argv[2], **kw)
+        return
+    env = setup_env()
+    names = sys.argv[1:] or list(CASES)
+    for nm in names:
+        print("golden:", nm, flush=True)
+        subprocess.check_call([sys.executable, os.path.abspath(__file__), "--run", nm], env=env,
+                              cwd=WORK)
+
+
+if __name__ == "__main__":
+    main()

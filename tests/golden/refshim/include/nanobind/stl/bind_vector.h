@@ -1,0 +1,2 @@
+#pragma once
+// STL casters come from pybind11/stl.h (included by nanobind.h).
