@@ -1,0 +1,355 @@
+"""Compiled state of a network on one GPU.
+
+Creates the device arrays of every population, projection and monitor
+through the C ABI, generates and loads the network's CUDA module, and runs
+steps in chunks whose length is bounded by the monitors' device buffers;
+after every chunk the buffers are copied to the host once.
+
+Array names (the generated module binds a __constant__ pointer to each):
+  pop<k>__<attr>            local attributes (size N) and globals (size 1)
+  pop<k>___sum_<target>     rate-coded weighted sums
+  pop<k>__spk               spike bitmap of the last step (N/32 words)
+  pop<k>__refractory[_remaining], pop<k>__last_spike
+  proj<k>__row_ptr/col/w/post_rank        CSR rows (post-major, pre ascending)
+  proj<k>__col_ptr/post_idx/w_pre/inv_idx pre-major view for spike scatter
+  proj<k>__<format arrays>                ELL/SELL/BSR/HYB (rate-coded)
+  mon<k>__spk / mon<k>__<var>             recording buffers
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from ..generator import formats as F
+from ..generator.codegen import BLOCK, CodeGenerator, grid_for
+from ..runtime.lib import DryNative, NativeNet
+
+BF16 = np.uint16
+MAX_MONITOR_BYTES = 256 << 20
+LOCAL_SMEM_LIMIT = 220 * 1024
+
+
+def to_bf16(x: np.ndarray) -> np.ndarray:
+    """float -> bfloat16 bits, round to nearest even."""
+    f = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    rounding = ((f >> 16) & 1) + 0x7FFF
+    return ((f + rounding) >> 16).astype(np.uint16)
+
+
+def from_bf16(h: np.ndarray) -> np.ndarray:
+    return (np.asarray(h, dtype=np.uint32) << 16).view(np.float32).astype(np.float64)
+
+
+class CompiledNetwork:
+    def __init__(self, net, dry: bool = False):
+        self.net = net
+        cfg = net._config
+        self.exact = cfg["precision"] == "double"
+        self.real = np.float64 if self.exact else np.float32
+        wd = cfg.get("weight_dtype") or ("float64" if self.exact else "float32")
+        if self.exact and wd != "float64":
+            raise ValueError("double precision uses float64 weights")
+        self.wdtype = {"float64": np.float64, "float32": np.float32, "bfloat16": BF16}[wd]
+        self.wctype = {"float64": "double", "float32": "float", "bfloat16": "anb_bf16"}[wd]
+        self.native = DryNative() if dry else NativeNet(cfg.get("device", 0))
+        self.layout: dict[int, dict] = {}
+        self.mon_layout: dict[int, dict] = {}
+        self.local_layout = None
+        self.engine = None
+        self.module = None
+
+    # --------------------------------------------------------------- helpers
+    def _w(self, w: np.ndarray) -> np.ndarray:
+        return to_bf16(w) if self.wdtype is BF16 else np.asarray(w, dtype=self.wdtype)
+
+    def _dtype_of(self, pop, name):
+        return np.int32 if pop._ctype.get(name) in ("int", "bool") else self.real
+
+    # ----------------------------------------------------------------- build
+    def build(self):
+        net = self.net
+        nat = self.native
+        nat.initialize(net.dt)
+        for pop in net.populations:
+            self._create_population(pop)
+        for proj in net.projections:
+            self._create_projection(proj)
+        self.engine = self._choose_engine()
+        for mon in net.monitors:
+            self._create_monitor(mon)
+        gen = CodeGenerator(self)
+        if self.engine == "local":
+            self._local_layout()
+            mod = gen.local_module()
+        else:
+            mod = gen.grid_module()
+        self.module = mod
+        nat.load_module(mod.source, mod.options)
+        if mod.engine == "local":
+            nat.set_local_kernel(*mod.local)
+        else:
+            nat.plan(mod.plan)
+            nat.set_graph_steps(int(net._config.get("graph_steps", 32)))
+
+    def _choose_engine(self) -> str:
+        want = self.net._config.get("engine", "auto")
+        ok, why = self._local_possible()
+        if want == "local":
+            if not ok:
+                raise NotImplementedError("local engine not possible: " + why)
+            return "local"
+        if want == "grid":
+            return "grid"
+        return "local" if ok else "grid"
+
+    def _local_possible(self):
+        net = self.net
+        if any(p.neuron_type.type != "spike" for p in net.populations):
+            return False, "rate-coded populations"
+        if any(p.synapse_type.type != "spike" or p.plastic for p in net.projections):
+            return False, "plastic or rate-coded projections"
+        if any(v != "spike" for m in net.monitors for v in m.variables):
+            return False, "variable monitors"
+        smem = self._local_smem_bytes()
+        if smem > LOCAL_SMEM_LIMIT:
+            return False, f"state needs {smem} bytes of shared memory"
+        return True, ""
+
+    def _local_vars(self, pop):
+        names = []
+        for v in pop.desc["variables"]:
+            if v.get("cpp"):
+                names.append(v["name"])
+        for r in pop.desc["spike"]["spike_reset"]:
+            if r["name"] not in names:
+                names.append(r["name"])
+        for t in pop.targets:
+            if "g_" + t not in names:
+                names.append("g_" + t)
+        return [n for n in names if pop._locality.get(n) == "local"]
+
+    def _local_smem_bytes(self):
+        total = 0
+        rb = np.dtype(self.real).itemsize
+        for pop in self.net.populations:
+            n = pop.size
+            total += len(self._local_vars(pop)) * ((n * rb + 15) // 16 * 16)
+            total += (n * 4 + 15) // 16 * 16                     # refractory_remaining
+            total += (((n + 31) // 32) * 4 + 15) // 16 * 16       # spike bitmap
+        return total
+
+    def _local_layout(self):
+        off = 0
+        pops = {}
+        rb = np.dtype(self.real).itemsize
+        rct = "double" if self.exact else "float"
+        for pop in self.net.populations:
+            d = {}
+            n = pop.size
+            for name in self._local_vars(pop):
+                d[name] = (off, rct)
+                off += (n * rb + 15) // 16 * 16
+            d["refractory_remaining"] = (off, "int")
+            off += (n * 4 + 15) // 16 * 16
+            d["spk"] = (off, "anb_u32")
+            off += (((n + 31) // 32) * 4 + 15) // 16 * 16
+            pops[pop.id] = d
+        self.local_layout = {"pops": pops, "smem": off, "block": 1024}
+
+    def _create_population(self, pop):
+        nat = self.native
+        for name, arr in pop._host.items():
+            dt = np.int32 if arr.dtype == np.int32 else self.real
+            nat.create(f"pop{pop.id}__{name}", np.asarray(arr, dtype=dt).reshape(-1))
+        if pop.neuron_type.type == "spike":
+            n = pop.size
+            nat.create(f"pop{pop.id}__spk", np.zeros((n + 31) // 32, dtype=np.uint32))
+            nat.create(f"pop{pop.id}__refractory", pop.refractory_steps.astype(np.int32))
+            nat.create(f"pop{pop.id}__refractory_remaining", np.zeros(n, dtype=np.int32))
+            nat.create(f"pop{pop.id}__last_spike", np.full(n, -10000, dtype=np.int64))
+
+    def _create_projection(self, proj):
+        nat = self.native
+        k = proj.id
+        if proj._csr is None:
+            raise RuntimeError(f"projection {proj.name} has no connectivity (call a connector)")
+        post_rank, row_ptr, cols, w = proj.csr_population_ranks()
+        rows = int(post_rank.size)
+        nnz = int(cols.size)
+        idx_t = "int" if nnz < 2**31 - 1 else "long long"
+        lay = {"rows": rows, "nnz": nnz, "idx_t": idx_t, "format": "csr"}
+        nat.create(f"proj{k}__post_rank", post_rank)
+        nat.create(f"proj{k}__row_ptr", row_ptr.astype(np.int32 if idx_t == "int" else np.int64))
+        nat.create(f"proj{k}__col", cols)
+        nat.create(f"proj{k}__w", self._w(w))
+        for prm in proj.desc["parameters"] + proj.desc["variables"]:
+            if prm["locality"] == "global":
+                nat.create(f"proj{k}__{prm['name']}", np.array([prm["init"]], dtype=self.real))
+        if proj.synapse_type.type == "rate":
+            fmt = self._rate_format(proj, lay)
+            lay["format"] = fmt
+            if fmt != "csr":
+                F.create_format_arrays(self, proj, fmt, post_rank, row_ptr, cols, w, lay)
+            lay["group"] = F.csr_group(nnz / max(rows, 1))
+            lay["kahan_min"] = 10000
+            lay["grid"] = grid_for(rows * (lay["group"] if not self.exact and fmt == "csr" else 1))
+        else:
+            # pre-major view (the reference's CSRC column view, CSRCMatrix.hpp:164-222)
+            npre = proj.pre_pop.size
+            rows_of = np.repeat(np.arange(rows, dtype=np.int64), np.diff(row_ptr))
+            order = np.lexsort((rows_of, cols))
+            col_ptr = np.zeros(npre + 1, dtype=np.int32)
+            np.cumsum(np.bincount(cols, minlength=npre), out=col_ptr[1:])
+            nat.create(f"proj{k}__col_ptr", col_ptr)
+            nat.create(f"proj{k}__post_idx", post_rank[rows_of[order]].astype(np.int32))
+            nat.create(f"proj{k}__inv_idx", order.astype(np.int32))
+            if not proj.plastic:
+                nat.create(f"proj{k}__w_pre", self._w(w[order]) if not self.exact else w[order])
+            lay["w0"] = int(proj.pre_ranks.min()) // 32
+            lay["w1"] = int(proj.pre_ranks.max()) // 32 + 1
+            if self.exact or proj.plastic:
+                lay["grid"] = grid_for(rows)
+            else:
+                lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
+            if proj.plastic:
+                nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
+                for name, arr in proj._host_attr.items():
+                    nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
+                if self.wdtype is not np.float64 and not self.exact:
+                    # plastic weights stay float32 (they are updated every event)
+                    nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
+                nat.create(f"proj{k}___last_event", np.full(nnz, -10000, dtype=np.int64))
+        self.layout[k] = lay
+
+    def _rate_format(self, proj, lay) -> str:
+        fmt = proj._storage_format
+        if fmt == "auto":
+            fmt = F.select_format(proj, self)
+        return fmt
+
+    def _create_monitor(self, mon):
+        nat = self.native
+        m = mon.id
+        pop = mon.population
+        words = (pop.size + 31) // 32
+        n = pop.size if mon.ranks is None else len(mon.ranks)
+        nvars = sum(1 for v in mon.variables if v != "spike")
+        per_step = (words * 4 if "spike" in mon.variables else 0) + nvars * n * 8 / mon.period_steps
+        cap_steps = int(max(1, min(self.net._config.get("monitor_chunk", 100000),
+                                   MAX_MONITOR_BYTES // max(per_step, 1))))
+        lay = {"words": words, "n": n, "cap_steps": cap_steps,
+               "cap_spike": cap_steps if "spike" in mon.variables else 0,
+               "cap_var": cap_steps // mon.period_steps + 1}
+        nat.create(f"mon{m}__on", np.array([1 if mon._recording else 0], dtype=np.int32))
+        nat.create(f"mon{m}__t0", np.zeros(1, dtype=np.int64))
+        nat.create(f"mon{m}__t0v", np.zeros(1, dtype=np.int64))
+        nat.create(f"mon{m}__start", np.array([mon._start_step], dtype=np.int64))
+        if "spike" in mon.variables:
+            nat.create_empty(f"mon{m}__spk", np.uint32, (cap_steps, words))
+        if mon.ranks is not None:
+            nat.create(f"mon{m}__ranks", np.asarray(mon.ranks, dtype=np.int32))
+        for v in mon.variables:
+            if v != "spike":
+                nat.create_empty(f"mon{m}__{v}", np.float64, (lay["cap_var"], n))
+        self.mon_layout[m] = lay
+
+    # ------------------------------------------------------------------- run
+    def chunk_steps(self) -> int:
+        if not self.mon_layout:
+            return 1 << 30
+        return min(l["cap_steps"] for l in self.mon_layout.values())
+
+    def run(self, nsteps: int):
+        nat = self.native
+        t = nat.get_time()
+        left = int(nsteps)
+        cap = self.chunk_steps()
+        while left > 0:
+            n = min(left, cap)
+            starts = {}
+            for mon in self.net.monitors:
+                first = self._first_record(mon, t)
+                starts[mon.id] = first
+                nat.write(f"mon{mon.id}__t0", np.array([t], dtype=np.int64))
+                nat.write(f"mon{mon.id}__t0v", np.array([first], dtype=np.int64))
+                nat.write(f"mon{mon.id}__on", np.array([1 if mon._recording else 0], dtype=np.int32))
+            nat.run(n)
+            nat.synchronize()
+            for mon in self.net.monitors:
+                self._drain(mon, t, n, starts[mon.id])
+            t += n
+            left -= n
+
+    @staticmethod
+    def _first_record(mon, t):
+        """First step >= t at which the monitor's variables are recorded."""
+        p, off = mon.period_steps, mon.period_offset_steps % mon.period_steps
+        return t + ((off - (t - mon._start_step)) % p)
+
+    def _drain(self, mon, t, n, first):
+        if not mon._recording:
+            return
+        nat = self.native
+        lay = self.mon_layout[mon.id]
+        if "spike" in mon.variables:
+            words = lay["words"]
+            buf = np.empty((n, words), dtype=np.uint32)
+            nat.read_into(f"mon{mon.id}__spk", buf)
+            steps, ranks = bitmap_to_spikes(buf, mon.population.size)
+            mon._append_spikes(steps + t, ranks)
+        nrec = 0 if first >= t + n else (t + n - 1 - first) // mon.period_steps + 1
+        if nrec > 0:
+            rec_steps = first + mon.period_steps * np.arange(nrec)
+            for v in mon.variables:
+                if v == "spike":
+                    continue
+                out = np.empty((nrec, lay["n"]), dtype=np.float64)
+                nat.read_into(f"mon{mon.id}__{v}", out)
+                mon._append_values(v, out, rec_steps)
+
+    # ------------------------------------------------------------ attributes
+    def read_population_attribute(self, pop, name):
+        arr = self.native.read(f"pop{pop.id}__{name}")
+        return arr.astype(np.int32 if arr.dtype == np.int32 else np.float64)
+
+    def write_population_attribute(self, pop, name, arr):
+        dt = np.int32 if pop._host[name].dtype == np.int32 else self.real
+        self.native.write(f"pop{pop.id}__{name}", np.asarray(arr, dtype=dt).reshape(-1))
+
+    def write_refractory(self, pop):
+        self.native.write(f"pop{pop.id}__refractory", pop.refractory_steps.astype(np.int32))
+
+    def read_spiked(self, pop):
+        bits = self.native.read(f"pop{pop.id}__spk")
+        return np.nonzero(np.unpackbits(bits.view(np.uint8), bitorder="little")[: pop.size])[0]
+
+    def read_projection_attribute(self, proj, name):
+        arr = self.native.read(f"proj{proj.id}__{name}")
+        if arr.dtype == np.uint16:
+            return from_bf16(arr)
+        return arr.astype(np.float64)
+
+    def write_projection_attribute(self, proj, name, arr):
+        k = proj.id
+        dtype, _ = self.native.arrays[f"proj{k}__{name}"]
+        data = to_bf16(arr) if dtype == np.uint16 else np.asarray(arr, dtype=dtype)
+        self.native.write(f"proj{k}__{name}", data)
+        if name == "w" and f"proj{k}__w_pre" in self.native.arrays:
+            order = self.native.read(f"proj{k}__inv_idx")
+            dtype, _ = self.native.arrays[f"proj{k}__w_pre"]
+            pre = arr[order]
+            self.native.write(f"proj{k}__w_pre", to_bf16(pre) if dtype == np.uint16
+                              else np.asarray(pre, dtype=dtype))
+        if name == "w" and self.layout[k].get("format", "csr") != "csr":
+            F.refresh_format_weights(self, proj, arr)
+
+
+def bitmap_to_spikes(buf: np.ndarray, n: int):
+    """(steps, words) uint32 bitmaps -> (step offsets, ranks), sorted by step
+    then rank."""
+    if buf.size == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    bits = np.unpackbits(np.ascontiguousarray(buf).view(np.uint8), axis=1, bitorder="little")
+    s, r = np.nonzero(bits[:, :n])
+    return s.astype(np.int64), r.astype(np.int64)

@@ -1,0 +1,190 @@
+"""Network: container of populations, projections and monitors.
+
+Same methods as the reference's Network (ANNarchy/core/Network.py:73-1521):
+create / connect / monitor / compile / simulate / step / get_time ...
+compile() generates and loads the network's CUDA module instead of
+generating C++ and running CMake (Network.py:517, Compiler.py:81-320).
+
+Configuration (``Network.config``):
+  precision    "double" (default): reference operation order, bit-identical
+               results; "float": fast single-precision kernels.
+  weight_dtype "float32" or "bfloat16" storage of static weights (float mode).
+  engine       "auto" | "grid" | "local" (see annarchy_b200.generator.codegen).
+  graph_steps  steps captured per CUDA graph in the grid engine.
+  device       CUDA device index.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from .monitor import Monitor
+from .population import Population
+from .projection import Projection
+
+_NETWORK_IDS = [0]
+
+
+class Network:
+    def __init__(self, dt: float = 1.0, seed: int | None = None):
+        _NETWORK_IDS[0] += 1
+        self.id = _NETWORK_IDS[0]
+        self.dt = float(dt)
+        self.seed = seed
+        self._rng = np.random.default_rng(seed)
+        self.populations: list[Population] = []
+        self.projections: list[Projection] = []
+        self.monitors: list[Monitor] = []
+        self._config = {"precision": "double", "weight_dtype": None, "engine": "auto",
+                        "graph_steps": 32, "device": 0}
+        self._compiled = False
+        self._backend = None
+        self._t_python = 0
+
+    # ----------------------------------------------------------- construction
+    def config(self, **kwargs):
+        for key, val in kwargs.items():
+            if key in ("dtype", "precision"):
+                name = getattr(val, "__name__", str(val))
+                val = {"float": "float", "float32": "float", "single": "float",
+                       "double": "double", "float64": "double"}.get(name, name)
+                key = "precision"
+            if key == "paradigm" and val not in ("b200", "cuda"):
+                raise ValueError("this backend only runs on the GPU (paradigm='b200')")
+            if key in ("num_threads", "paradigm", "seed", "verbose", "sparse_matrix_format",
+                       "method"):
+                if key == "seed" and val is not None:
+                    self.seed = val
+                    self._rng = np.random.default_rng(val)
+                if key == "sparse_matrix_format":
+                    self._config["default_format"] = val
+                continue
+            self._config[key] = val
+        return self
+
+    def create(self, geometry, neuron, name: str | None = None, **kw) -> Population:
+        if self._compiled:
+            raise RuntimeError("the network is already compiled")
+        pop = Population(geometry, neuron, name=name, net=self, pop_id=len(self.populations))
+        self.populations.append(pop)
+        return pop
+
+    def connect(self, pre, post, target: str = "exc", synapse=None, name: str | None = None,
+                **kw) -> Projection:
+        if self._compiled:
+            raise RuntimeError("the network is already compiled")
+        proj = Projection(pre, post, target, synapse=synapse, name=name, net=self,
+                          proj_id=len(self.projections))
+        if "default_format" in self._config:
+            proj._storage_format = self._config["default_format"]
+        self.projections.append(proj)
+        return proj
+
+    def monitor(self, obj, variables=None, period: float | None = None,
+                period_offset: float | None = None, start: bool = True,
+                name: str | None = None) -> Monitor:
+        if self._compiled:
+            raise RuntimeError("monitors must be created before compile() in this backend")
+        mon = Monitor(obj, variables, period=period, period_offset=period_offset, start=start,
+                      name=name, net=self, mon_id=len(self.monitors))
+        self.monitors.append(mon)
+        return mon
+
+    # ------------------------------------------------------------ compilation
+    def compile(self, directory: str | None = None, clean: bool = False, silent: bool = True,
+                **kwargs):
+        """Generate, compile (NVRTC, sm_100a) and load the network's kernels,
+        and copy every population and projection to the device."""
+        from .backend import CompiledNetwork
+        if self._compiled:
+            return
+        if not self.populations:
+            raise RuntimeError("the network has no population")
+        backend = CompiledNetwork(self)
+        backend.build()
+        self._backend = backend
+        self._compiled = True
+
+    def generate_code(self):
+        """Generate the network's CUDA module without a device (for
+        inspection and compile-only checks); returns the codegen Module."""
+        from .backend import CompiledNetwork
+        backend = CompiledNetwork(self, dry=True)
+        backend.build()
+        return backend.module
+
+    @property
+    def compiled(self) -> bool:
+        return self._compiled
+
+    @property
+    def engine(self) -> str | None:
+        return self._backend.engine if self._backend else None
+
+    # ------------------------------------------------------------- simulation
+    def _steps(self, duration: float) -> int:
+        return int(math.ceil(float(duration) / self.dt))
+
+    def simulate(self, duration: float, measure_time: bool = False):
+        if not self._compiled:
+            raise RuntimeError("simulate(): the network is not compiled yet")
+        n = self._steps(duration)
+        t0 = time.time()
+        self._backend.run(n)
+        if measure_time:
+            print(f"Simulating {duration / 1000.0} seconds of the network took "
+                  f"{time.time() - t0} seconds.")
+
+    def simulate_steps(self, nsteps: int):
+        if not self._compiled:
+            raise RuntimeError("the network is not compiled yet")
+        self._backend.run(int(nsteps))
+
+    def step(self):
+        self.simulate_steps(1)
+
+    @property
+    def current_step(self) -> int:
+        return self._backend.native.get_time() if self._compiled else 0
+
+    def get_current_step(self) -> int:
+        return self.current_step
+
+    def get_time(self) -> float:
+        return self.current_step * self.dt
+
+    def set_current_step(self, t: int):
+        self._backend.native.set_time(int(t))
+
+    def set_time(self, t: float):
+        self.set_current_step(int(round(t / self.dt)))
+
+    # ---------------------------------------------------------------- access
+    def get_population(self, name: str) -> Population:
+        for p in self.populations:
+            if p.name == name:
+                return p
+        raise KeyError(name)
+
+    def get_projection(self, name: str) -> Projection:
+        for p in self.projections:
+            if p.name == name:
+                return p
+        raise KeyError(name)
+
+    def get_monitors(self):
+        return list(self.monitors)
+
+    def close(self):
+        if self._backend is not None:
+            self._backend.native.close()
+            self._backend = None
+        self._compiled = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

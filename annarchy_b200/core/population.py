@@ -1,0 +1,207 @@
+"""Populations and population views.
+
+Attribute access follows the reference (ANNarchy/core/Population.py:375-500):
+every parameter and variable of the neuron type is an attribute; local
+ones are arrays of the population's size, global ones scalars. Before
+compile() values live on the host; afterwards the device arrays are the
+state and every get/set copies through the C ABI (like the reference's
+pop<k>_wrapper properties, which also copy).
+
+The refractory period is given in ms and converted to whole steps by
+truncation, int(refractory / dt) (Population.py:659-690).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .random import RandomDistribution, values as draw
+
+_RESERVED = {"size", "geometry", "neuron_type", "name", "id", "ranks", "net", "refractory",
+             "desc", "population", "targets", "attributes"}
+
+
+class Population:
+    def __init__(self, geometry, neuron, name: str | None = None, net=None, pop_id: int = 0,
+                 stop_condition=None, storage_order="post_to_pre", copied=False):
+        if isinstance(geometry, int):
+            geometry = (geometry,)
+        object.__setattr__(self, "_ready", False)
+        self.geometry = tuple(int(g) for g in geometry)
+        self.size = int(np.prod(self.geometry))
+        self.neuron_type = neuron
+        self.net = net
+        self.id = pop_id
+        self.name = name or f"pop{pop_id}"
+        self.desc = neuron.desc
+        self.targets = list(self.desc["targets"])
+        self._host: dict[str, np.ndarray] = {}
+        self._ctype: dict[str, str] = {}
+        self._locality: dict[str, str] = {}
+        for p in self.desc["parameters"] + self.desc["variables"]:
+            self._locality[p["name"]] = p["locality"]
+            self._ctype[p["name"]] = p.get("ctype", "double")
+        for p in self.desc["parameters"] + self.desc["variables"]:
+            self._host[p["name"]] = self._initial(p)
+        if self.neuron_type.type == "rate":
+            for t in self.targets:
+                self._host["_sum_" + t] = np.zeros(self.size)
+                self._locality["_sum_" + t] = "local"
+                self._ctype["_sum_" + t] = "double"
+        refr = self.neuron_type.refractory if self.neuron_type.type == "spike" else None
+        self._refractory_ms = np.full(self.size, float(refr or 0.0))
+        self._has_refractory = bool(refr)
+        object.__setattr__(self, "_ready", True)
+
+    # -- helpers --------------------------------------------------------------
+    def _initial(self, p):
+        init = p["init"]
+        shape = (self.size,) if p["locality"] == "local" else ()
+        dtype = np.int32 if p.get("ctype") in ("int", "bool") else np.float64
+        if isinstance(init, str):
+            ref = [q for q in self.desc["parameters"] if q["name"] == init]
+            if not ref:
+                raise ValueError(f"init value {init!r} of {p['name']} is not a parameter")
+            init = ref[0]["init"]
+        if isinstance(init, RandomDistribution):
+            return draw(init, shape, self._rng(), dtype)
+        return np.full(shape, init, dtype=dtype)
+
+    def _rng(self):
+        return self.net._rng if self.net is not None else np.random.default_rng()
+
+    def _device_name(self, attr: str) -> str:
+        return f"pop{self.id}__{attr}"
+
+    @property
+    def attributes(self):
+        return list(self.desc["attributes"])
+
+    @property
+    def ranks(self):
+        return np.arange(self.size)
+
+    @property
+    def population(self):
+        return self
+
+    def _compiled(self) -> bool:
+        return self.net is not None and self.net._compiled
+
+    # -- attribute access -----------------------------------------------------
+    def __getattr__(self, name):
+        if name.startswith("__") or not object.__getattribute__(self, "_ready"):
+            raise AttributeError(name)
+        host = object.__getattribute__(self, "_host")
+        if name in host:
+            return self.get(name)
+        raise AttributeError(f"population {self.name!r} has no attribute {name!r}")
+
+    def __setattr__(self, name, value):
+        if not self.__dict__.get("_ready", False) or name.startswith("_") and name not in self._host:
+            object.__setattr__(self, name, value)
+            return
+        if name in self._host:
+            self.set({name: value})
+            return
+        if name == "refractory":
+            self.set_refractory(value)
+            return
+        object.__setattr__(self, name, value)
+
+    def get(self, name: str):
+        if self._compiled():
+            arr = self.net._backend.read_population_attribute(self, name)
+        else:
+            arr = self._host[name].copy()
+        if self._locality.get(name) != "local":
+            return arr.reshape(()).item()
+        return arr.reshape(self.geometry) if len(self.geometry) > 1 else arr
+
+    def set(self, values: dict):
+        for name, value in values.items():
+            if name not in self._host:
+                raise AttributeError(f"population {self.name!r} has no attribute {name!r}")
+            cur = self._host[name]
+            shape = cur.shape
+            arr = draw(value, shape, self._rng(), cur.dtype)
+            self._host[name] = arr
+            if self._compiled():
+                self.net._backend.write_population_attribute(self, name, arr)
+
+    def _set_ranks(self, name: str, ranks: np.ndarray, value):
+        if self._locality.get(name) != "local":
+            raise AttributeError(f"{name} is global; set it on the population")
+        cur = self.get(name).reshape(-1).astype(self._host[name].dtype)
+        cur[ranks] = draw(value, (len(ranks),), self._rng(), cur.dtype)
+        self.set({name: cur})
+
+    def set_refractory(self, value):
+        self._refractory_ms = draw(value, (self.size,), self._rng())
+        self._has_refractory = self._has_refractory or bool(np.any(self._refractory_ms > 0))
+        if self._compiled():
+            self.net._backend.write_refractory(self)
+
+    @property
+    def refractory_steps(self) -> np.ndarray:
+        dt = self.net.dt if self.net is not None else 1.0
+        return (self._refractory_ms / dt).astype(np.int32)  # truncation, like int(x/dt)
+
+    # -- views ----------------------------------------------------------------
+    def __getitem__(self, idx):
+        ranks = np.arange(self.size)[idx]
+        return PopulationView(self, np.atleast_1d(ranks))
+
+    def __len__(self):
+        return self.size
+
+    def __repr__(self):
+        return f"Population({self.name!r}, size={self.size}, {self.neuron_type.type})"
+
+    # spikes of the last step (spiking populations)
+    @property
+    def spiked(self):
+        if not self._compiled():
+            return np.array([], dtype=np.int64)
+        return self.net._backend.read_spiked(self)
+
+
+class PopulationView:
+    """A subset of a population's neurons (ANNarchy/core/PopulationView.py)."""
+
+    def __init__(self, population: Population, ranks):
+        object.__setattr__(self, "population", population)
+        object.__setattr__(self, "ranks", np.asarray(ranks, dtype=np.int64))
+        object.__setattr__(self, "size", int(len(ranks)))
+
+    @property
+    def id(self):
+        return self.population.id
+
+    @property
+    def neuron_type(self):
+        return self.population.neuron_type
+
+    @property
+    def net(self):
+        return self.population.net
+
+    def __getattr__(self, name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        pop = object.__getattribute__(self, "population")
+        val = pop.get(name)
+        if np.ndim(val) == 0:
+            return val
+        return np.asarray(val).reshape(-1)[self.ranks]
+
+    def __setattr__(self, name, value):
+        self.population._set_ranks(name, self.ranks, value)
+
+    def __getitem__(self, idx):
+        return PopulationView(self.population, self.ranks[idx])
+
+    def __len__(self):
+        return self.size
+
+    def __repr__(self):
+        return f"PopulationView({self.population.name!r}, size={self.size})"

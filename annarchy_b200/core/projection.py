@@ -1,0 +1,311 @@
+"""Projections and connector methods.
+
+Connectivity is kept as one CSR matrix per projection, rows = post neurons
+of the projection (in ``post_ranks`` order) and columns = pre neurons, with
+each row's pre ranks ascending: the order in which the reference builds its
+LIL dendrites and hence the order of its CSR rows
+(ANNarchy/core/ConnectorMethods.py:763-796, ANNarchy/include/CSRMatrix.hpp:142).
+The storage format the kernels read (CSR, ELL, ELL-R, SELL-C-sigma, BSR,
+HYB) is derived from it at compile time.
+
+Connector methods (ANNarchy/core/ConnectorMethods.py): from_sparse,
+from_matrix, fixed_probability, fixed_number_pre, fixed_number_post,
+all_to_all, one_to_one. Only zero (one-step) transmission delays are
+supported; weights may be scalars, arrays or random distributions drawn from
+the network's seeded generator.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+from .models import Synapse
+from .population import Population, PopulationView
+from .random import values as draw
+
+FORMATS = ("csr", "ell", "ellr", "sell", "bsr", "hyb", "auto")
+
+
+def _ranks(obj):
+    return np.asarray(obj.ranks, dtype=np.int64)
+
+
+def _population(obj):
+    return obj.population if isinstance(obj, PopulationView) else obj
+
+
+class Projection:
+    def __init__(self, pre, post, target: str, synapse: Synapse | None = None,
+                 name: str | None = None, net=None, proj_id: int = 0, disable_omp=True):
+        self.pre = pre
+        self.post = post
+        self.pre_pop: Population = _population(pre)
+        self.post_pop: Population = _population(post)
+        self.target = target
+        self.net = net
+        self.id = proj_id
+        self.name = name or f"proj{proj_id}"
+        pre_type = self.pre_pop.neuron_type.type
+        if synapse is None:
+            synapse = Synapse(pre_spike="g_target += w") if pre_type == "spike" else Synapse()
+        self.synapse_type = synapse
+        self.desc = synapse.desc
+        if synapse.type == "spike" and pre_type != "spike":
+            raise TypeError("a spiking synapse needs a spiking pre-synaptic population")
+        if synapse.type == "rate" and pre_type != "rate":
+            raise TypeError("a rate-coded synapse needs a rate-coded pre-synaptic population")
+        if self.post_pop.neuron_type.type == "spike" and synapse.type == "spike":
+            if target not in self.post_pop.targets:
+                raise ValueError(f"target {target!r} is not used by the post-synaptic neuron")
+        self.pre_ranks = _ranks(pre)
+        self.post_ranks_view = _ranks(post)
+        self._csr: sp.csr_matrix | None = None   # (n_post_view, n_pre_view), view-relative
+        self._storage_format = "csr"
+        self._host_attr: dict[str, np.ndarray] = {}
+        self.connector_name = None
+        self._schedule = None
+
+    # -- properties -------------------------------------------------------------
+    @property
+    def nb_synapses(self) -> int:
+        return 0 if self._csr is None else int(self._csr.nnz)
+
+    def __len__(self):
+        return self.nb_synapses
+
+    @property
+    def size(self) -> int:
+        return 0 if self._csr is None else int((np.diff(self._csr.indptr) > 0).sum())
+
+    @property
+    def plastic(self) -> bool:
+        return bool(self.desc.get("plasticity")) or bool(self.desc.get("post_spike"))
+
+    @property
+    def storage_format(self) -> str:
+        return self._storage_format
+
+    def _rng(self):
+        return self.net._rng if self.net is not None else np.random.default_rng()
+
+    # -- connectors ---------------------------------------------------------------
+    def _store(self, m: sp.csr_matrix, name, storage_format, delays=0.0):
+        if delays not in (0, 0.0, None):
+            if self.net is None or abs(float(delays) - self.net.dt) > 1e-12:
+                raise NotImplementedError("synaptic delays are not supported by this backend")
+        m = sp.csr_matrix(m)
+        m.sum_duplicates()
+        m.sort_indices()
+        self._csr = m
+        self.connector_name = name
+        if storage_format is not None:
+            if storage_format not in FORMATS:
+                raise ValueError(f"unknown storage format {storage_format!r}")
+            self._storage_format = storage_format
+        for v in self.desc["variables"] + self.desc["parameters"]:
+            if v["locality"] == "local" and v["name"] != "w":
+                init = v["init"] if not isinstance(v["init"], str) else 0.0
+                self._host_attr[v["name"]] = np.full(m.nnz, float(init))
+        return self
+
+    def _weights(self, weights, nnz):
+        return draw(weights, (nnz,), self._rng())
+
+    def from_sparse(self, weights, delays=0.0, storage_format=None, storage_order=None):
+        """weights: scipy sparse matrix of shape (pre, post)."""
+        w = sp.csr_matrix(weights)
+        if w.shape != (len(self.pre_ranks), len(self.post_ranks_view)):
+            raise ValueError(f"from_sparse(): expected shape {(len(self.pre_ranks), len(self.post_ranks_view))}, "
+                             f"got {w.shape}")
+        return self._store(w.T.tocsr(), "Sparse connectivity matrix", storage_format, delays)
+
+    connect_from_sparse = from_sparse
+
+    def from_matrix(self, weights, delays=0.0, pre_post=False, storage_format=None,
+                    storage_order=None):
+        """weights: dense (post, pre) array (or (pre, post) with pre_post=True);
+        entries that are None/NaN mean no synapse."""
+        W = np.array(weights, dtype=object if np.asarray(weights).dtype == object else np.float64)
+        if pre_post:
+            W = W.T
+        if W.dtype == object:
+            mask = np.vectorize(lambda x: x is not None)(W)
+            W = np.where(mask, W, 0.0).astype(np.float64)
+        else:
+            mask = ~np.isnan(W)
+            W = np.nan_to_num(W)
+        rows, cols = np.nonzero(mask)
+        m = sp.csr_matrix((W[rows, cols], (rows, cols)), shape=W.shape)
+        return self._store(m, "Connectivity matrix", storage_format, delays)
+
+    def _self_mask(self, rows, cols):
+        if self.pre_pop is not self.post_pop:
+            return np.ones(rows.shape, dtype=bool)
+        return self.post_ranks_view[rows] != self.pre_ranks[cols]
+
+    def all_to_all(self, weights, delays=0.0, allow_self_connections=False,
+                   force_multiple_weights=False, storage_format=None, storage_order=None):
+        npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
+        rows = np.repeat(np.arange(npost), npre)
+        cols = np.tile(np.arange(npre), npost)
+        if not allow_self_connections:
+            keep = self._self_mask(rows, cols)
+            rows, cols = rows[keep], cols[keep]
+        w = self._weights(weights, rows.size)
+        m = sp.csr_matrix((w, (rows, cols)), shape=(npost, npre))
+        return self._store(m, "All-to-All", storage_format, delays)
+
+    def one_to_one(self, weights=1.0, delays=0.0, force_multiple_weights=False,
+                   storage_format=None, storage_order=None):
+        n = min(len(self.post_ranks_view), len(self.pre_ranks))
+        rows = np.arange(n)
+        w = self._weights(weights, n)
+        m = sp.csr_matrix((w, (rows, rows)), shape=(len(self.post_ranks_view), len(self.pre_ranks)))
+        return self._store(m, "One-to-One", storage_format, delays)
+
+    def fixed_probability(self, probability, weights, delays=0.0, allow_self_connections=False,
+                          force_multiple_weights=False, storage_format=None, storage_order=None):
+        """Each (post, pre) pair is connected independently with the given
+        probability (per-post Bernoulli masks, as in the reference's
+        ANNarchy/cython_ext/Connector.pyx:306-345)."""
+        rng = self._rng()
+        npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
+        rows_l, cols_l = [], []
+        for r0 in range(0, npost, 4096):
+            r1 = min(npost, r0 + 4096)
+            mask = rng.random((r1 - r0, npre)) < probability
+            rr, cc = np.nonzero(mask)
+            rows_l.append(rr + r0)
+            cols_l.append(cc)
+        rows = np.concatenate(rows_l) if rows_l else np.zeros(0, np.int64)
+        cols = np.concatenate(cols_l) if cols_l else np.zeros(0, np.int64)
+        if not allow_self_connections:
+            keep = self._self_mask(rows, cols)
+            rows, cols = rows[keep], cols[keep]
+        w = self._weights(weights, rows.size)
+        m = sp.csr_matrix((w, (rows, cols)), shape=(npost, npre))
+        return self._store(m, "Random", storage_format, delays)
+
+    def fixed_number_pre(self, number, weights, delays=0.0, allow_self_connections=False,
+                         force_multiple_weights=False, storage_format=None, storage_order=None):
+        """Every post neuron receives exactly `number` distinct pre neurons."""
+        rng = self._rng()
+        npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
+        avail = npre - (0 if allow_self_connections or self.pre_pop is not self.post_pop else 1)
+        if number > avail:
+            raise ValueError("fixed_number_pre: number exceeds the available pre-synaptic neurons")
+        cols = np.empty((npost, number), dtype=np.int64)
+        for r0 in range(0, npost, 2048):
+            r1 = min(npost, r0 + 2048)
+            keys = rng.random((r1 - r0, npre), dtype=np.float32)
+            if not allow_self_connections and self.pre_pop is self.post_pop:
+                pos = {int(r): k for k, r in enumerate(self.pre_ranks)}
+                for i in range(r0, r1):
+                    k = pos.get(int(self.post_ranks_view[i]))
+                    if k is not None:
+                        keys[i - r0, k] = 2.0
+            cols[r0:r1] = np.argpartition(keys, number - 1, axis=1)[:, :number]
+        cols.sort(axis=1)
+        indptr = np.arange(0, npost * number + 1, number, dtype=np.int64)
+        w = self._weights(weights, npost * number)
+        m = sp.csr_matrix((w, cols.ravel(), indptr), shape=(npost, npre))
+        return self._store(m, "Random Convergent", storage_format, delays)
+
+    def fixed_number_post(self, number, weights, delays=0.0, allow_self_connections=False,
+                          force_multiple_weights=False, storage_format=None, storage_order=None):
+        """Every pre neuron projects onto exactly `number` distinct post neurons."""
+        rng = self._rng()
+        npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
+        keys = rng.random((npre, npost))
+        if not allow_self_connections and self.pre_pop is self.post_pop:
+            for c in range(npre):
+                hit = np.nonzero(self.post_ranks_view == self.pre_ranks[c])[0]
+                keys[c, hit] = 2.0
+        posts = np.argpartition(keys, number - 1, axis=1)[:, :number]
+        cols = np.repeat(np.arange(npre), number)
+        rows = posts.ravel()
+        w = self._weights(weights, rows.size)
+        m = sp.csr_matrix((w, (rows, cols)), shape=(npost, npre))
+        return self._store(m, "Random Divergent", storage_format, delays)
+
+    # -- compiled connectivity (population ranks) ------------------------------------------
+    def csr_population_ranks(self):
+        """(post_ranks, row_ptr, pre_rank_per_synapse, w) with rows that have
+        at least one synapse, like the reference's post_rank list."""
+        m = self._csr
+        lengths = np.diff(m.indptr)
+        rows = np.nonzero(lengths > 0)[0]
+        post_ranks = self.post_ranks_view[rows].astype(np.int32)
+        row_ptr = np.zeros(rows.size + 1, dtype=np.int64)
+        np.cumsum(lengths[rows], out=row_ptr[1:])
+        cols = self.pre_ranks[m.indices].astype(np.int32)
+        return post_ranks, row_ptr, cols, np.asarray(m.data, dtype=np.float64)
+
+    # -- attributes --------------------------------------------------------------------------
+    def _attr_names(self):
+        return ["w"] + list(self._host_attr)
+
+    def get(self, name: str, flat: bool = False):
+        if name not in self._attr_names() and name not in {p["name"] for p in self.desc["parameters"]}:
+            raise AttributeError(f"projection {self.name!r} has no attribute {name!r}")
+        glob = {p["name"]: p for p in self.desc["parameters"] + self.desc["variables"]
+                if p["locality"] == "global"}
+        if name in glob:
+            if self.net is not None and self.net._compiled:
+                return float(self.net._backend.read_projection_attribute(self, name)[0])
+            return float(glob[name]["init"])
+        if self.net is not None and self.net._compiled:
+            flat_v = self.net._backend.read_projection_attribute(self, name)
+        elif name == "w":
+            flat_v = np.asarray(self._csr.data, dtype=np.float64).copy()
+        else:
+            flat_v = self._host_attr[name].copy()
+        if flat:
+            return flat_v
+        lengths = np.diff(self._csr.indptr)
+        lengths = lengths[lengths > 0]
+        return [a for a in np.split(flat_v, np.cumsum(lengths)[:-1])]
+
+    def set(self, values: dict):
+        for name, value in values.items():
+            nnz = self.nb_synapses
+            if isinstance(value, list):
+                value = np.concatenate([np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in value])
+            arr = draw(value, (nnz,), self._rng())
+            if name == "w":
+                self._csr.data[:] = arr
+            elif name in self._host_attr:
+                self._host_attr[name] = arr
+            else:
+                raise AttributeError(f"projection {self.name!r} has no attribute {name!r}")
+            if self.net is not None and self.net._compiled:
+                self.net._backend.write_projection_attribute(self, name, arr)
+
+    def __getattr__(self, name):
+        if name.startswith("_") or name in ("pre", "post", "desc", "net", "synapse_type"):
+            raise AttributeError(name)
+        desc = self.__dict__.get("desc")
+        if desc is not None and (name == "w" or name in self.__dict__.get("_host_attr", {}) or
+                                 name in {p["name"] for p in desc["parameters"]}):
+            return self.get(name)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        desc = self.__dict__.get("desc")
+        if desc is not None and self.__dict__.get("_csr") is not None and (
+                name == "w" or name in self.__dict__.get("_host_attr", {})):
+            self.set({name: value})
+            return
+        object.__setattr__(self, name, value)
+
+    def dendrite_sizes(self):
+        lengths = np.diff(self._csr.indptr)
+        return lengths[lengths > 0]
+
+    @property
+    def post_ranks(self):
+        return self.csr_population_ranks()[0].tolist()
+
+    def __repr__(self):
+        return (f"Projection({self.name!r}, {self.pre_pop.name}->{self.post_pop.name}, "
+                f"target={self.target!r}, {self.nb_synapses} synapses, {self._storage_format})")

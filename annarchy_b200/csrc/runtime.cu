@@ -491,6 +491,46 @@ int anb_module_load(anb_net* net, const char* source, const char* options) {
   return bind(net);
 }
 
+int anb_nvrtc_compile(const char* source, const char* options, char* log, size_t log_len,
+                      size_t* cubin_bytes) {
+  if (!source) return fail(ANB_ERR_ARG, "source is NULL");
+  std::vector<std::string> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device",
+                                   "-lineinfo"};
+  if (options) {
+    std::string s(options), cur;
+    for (char c : s) {
+      if (c == '\n') {
+        if (!cur.empty()) opts.push_back(cur);
+        cur.clear();
+      } else {
+        cur.push_back(c);
+      }
+    }
+    if (!cur.empty()) opts.push_back(cur);
+  }
+  std::vector<const char*> copts;
+  for (auto& o : opts) copts.push_back(o.c_str());
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, source, "anb_network.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+    return fail(ANB_ERR_COMPILE, "nvrtcCreateProgram failed");
+  nvrtcResult cr = nvrtcCompileProgram(prog, (int)copts.size(), copts.data());
+  size_t log_size = 0;
+  nvrtcGetProgramLogSize(prog, &log_size);
+  std::string text(log_size, '\0');
+  if (log_size) nvrtcGetProgramLog(prog, &text[0]);
+  if (log && log_len) {
+    std::strncpy(log, text.c_str(), log_len - 1);
+    log[log_len - 1] = '\0';
+  }
+  size_t sz = 0;
+  if (cr == NVRTC_SUCCESS) nvrtcGetCUBINSize(prog, &sz);
+  nvrtcDestroyProgram(&prog);
+  if (cubin_bytes) *cubin_bytes = sz;
+  if (cr != NVRTC_SUCCESS)
+    return fail(ANB_ERR_COMPILE, std::string("NVRTC: ") + nvrtcGetErrorString(cr) + "\n" + text);
+  return ANB_OK;
+}
+
 int anb_plan_clear(anb_net* net) {
   if (!net) return fail(ANB_ERR_ARG, "net is NULL");
   drop_graph(net);

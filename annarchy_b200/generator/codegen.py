@@ -1,0 +1,674 @@
+"""CUDA source generation for one compiled network.
+
+Lowers the parser's description dicts (C statements with index
+placeholders) into the network's kernels and pairs them with the
+hand-written templates of csrc/device/anb_device.cuh.
+
+Step semantics follow the reference's generated core
+(ANNarchy/generator/Template/OpenMPBaseTemplate.py:131-484):
+
+    compute_psp of every projection (spikes of the previous step)
+    -> update of every population (ODE block: all increments from the old
+       state, then the switches, each followed by its min/max bound;
+       refractory neurons keep v frozen: the switch of every non-g_
+       variable is multiplied by in_ref; ANNarchy/generator/Utils.py:17-265)
+    -> spike gather (threshold, reset, last_spike, refractory counter;
+       Population/OpenMPGenerator.py:999-1237)
+    -> post_event of plastic projections -> record -> t++
+
+Two engines:
+
+* grid  - one kernel per phase over the whole GPU, launched once per step;
+          the runtime captures `graph_steps` steps into one CUDA graph.
+* local - spiking networks whose state fits in one CTA's shared memory:
+          a single kernel keeps the whole state on-chip and loops over the
+          steps itself (no launch per step; barriers are __syncthreads).
+
+Precision modes:
+
+* exact (double) - reference operation order, no contraction
+                   (--fmad=false): bit-identical to the reference's CPU build.
+* fast  (float)  - float state, float or bfloat16 weights, float
+                   accumulation with atomics; checked by tolerance.
+"""
+from __future__ import annotations
+
+import os
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEVICE_HEADER = os.path.join(os.path.dirname(HERE), "csrc", "device", "anb_device.cuh")
+
+BLOCK = 256
+MAX_GRID = 148 * 16
+
+CTYPE_OF = {np.dtype(np.float64): "double", np.dtype(np.float32): "float",
+            np.dtype(np.int32): "int", np.dtype(np.int64): "long long",
+            np.dtype(np.uint32): "anb_u32", np.dtype(np.uint16): "anb_bf16"}
+
+
+def grid_for(n: int, block: int = BLOCK) -> int:
+    return max(1, min(MAX_GRID, (n + block - 1) // block))
+
+
+def float_literals(code: str) -> str:
+    """Suffix floating literals with f (single-precision modules), like the
+    reference's float precision mode (ANNarchy/parser/Equation.py:172-197)."""
+    return re.sub(r"(?<![\w.])(\d+\.\d+(?:[eE][-+]?\d+)?)(?![\w.])", r"\1f", code)
+
+
+@dataclass
+class Module:
+    source: str
+    options: list
+    engine: str
+    plan: list = field(default_factory=list)           # [(kernel, grid, block, smem)]
+    local: tuple | None = None                         # (kernel, grid, block, smem)
+    kernels: list = field(default_factory=list)
+
+
+class CodeGenerator:
+    def __init__(self, compiled):
+        self.c = compiled                  # CompiledNetwork (arrays, precision, layout)
+        self.net = compiled.net
+        self.exact = compiled.exact
+        self.real = "double" if self.exact else "float"
+        self.decls: dict[str, str] = {}
+
+    # ------------------------------------------------------------------ utils
+    def ptr(self, name: str) -> str:
+        """C expression of the device pointer of array `name` (declares it)."""
+        dtype = self.c.native.arrays[name][0]
+        self.decls[name] = CTYPE_OF[np.dtype(dtype)]
+        return "anb_p_" + name
+
+    def typed(self, code: str) -> str:
+        code = code.replace("double ", self.real + " ")
+        return code if self.exact else float_literals(code)
+
+    @staticmethod
+    def fill(code: str, local="", glob="", semi="", pre_prefix="", pre_index="", post_prefix="",
+             post_index="") -> str:
+        return code % {"local_index": local, "global_index": glob, "semiglobal_index": semi,
+                       "pre_prefix": pre_prefix, "pre_index": pre_index,
+                       "post_prefix": post_prefix, "post_index": post_index}
+
+    # --------------------------------------------------------------- neurons
+    def _neuron_body(self, pop, src_of, masked: bool) -> tuple[str, list]:
+        """Statements updating one neuron; locals are C variables named after
+        the attributes. Returns (code, names of modified attributes)."""
+        desc = pop.desc
+        local = set(desc["local"])
+        blocks = []
+        is_ode = False
+        for v in desc["variables"]:
+            if v.get("cpp", "") == "" or v.get("method") == "event-driven":
+                continue
+            if v["name"] not in local:
+                raise NotImplementedError(f"global variable {v['name']!r} with an equation is "
+                                          "not supported by this backend")
+            if v.get("switch"):
+                if is_ode:
+                    blocks[-1][1].append(v)
+                else:
+                    blocks.append(("ode", [v]))
+                    is_ode = True
+            else:
+                if is_ode or not blocks:
+                    blocks.append(("non-ode", [v]))
+                    is_ode = False
+                else:
+                    blocks[-1][1].append(v)
+        lines, modified = [], []
+
+        def bounds(v):
+            out = []
+            for b, val in v.get("bounds", {}).items():
+                if b in ("min", "max"):
+                    op = "<" if b == "min" else ">"
+                    out.append(f"if ({v['name']} {op} {val}) {v['name']} = {val};")
+            return out
+
+        for kind, vs in blocks:
+            if kind == "ode":
+                for v in vs:
+                    lines.append(self.typed(self.fill(v["cpp"])))
+                for v in vs:
+                    sw = self.fill(v["switch"])
+                    if masked and not v["name"].startswith("g_"):
+                        sw = sw.replace(";", "* in_ref;")
+                    lines.append(sw)
+                    lines += [self.typed(b) for b in bounds(v)]
+                    modified.append(v["name"])
+            else:
+                for v in vs:
+                    code = self.typed(self.fill(v["cpp"]))
+                    if masked and not v["name"].startswith("g_"):
+                        code = "if (in_ref) { " + code + " }"
+                    lines.append(code)
+                    lines += [self.typed(b) for b in bounds(v)]
+                    modified.append(v["name"])
+        return "\n".join(lines), modified
+
+    def _globals_preamble(self, pop, src) -> str:
+        out = []
+        for p in pop.desc["parameters"] + pop.desc["variables"]:
+            if p["locality"] == "global":
+                ct = "int" if p.get("ctype") in ("int", "bool") else self.real
+                out.append(f"const {ct} {p['name']} = {src(p['name'])}[0];")
+        for v in pop.desc["variables"]:
+            pl = v.get("pre_loop") or {}
+            if pl:
+                out.append(self.typed(f"const double {pl['name']} = {self.fill(pl['value'])};"))
+        return "\n    ".join(out)
+
+    def _locals(self, pop):
+        return [p["name"] for p in pop.desc["parameters"] + pop.desc["variables"]
+                if p["locality"] == "local"]
+
+    def neuron_update(self, pop, *, local_engine=False, smem=None) -> str:
+        """Update (+ spike gather) of one population for step t."""
+        spiking = pop.neuron_type.type == "spike"
+        masked = spiking and pop._has_refractory
+        body, modified = self._neuron_body(pop, None, masked)
+        names = self._locals(pop)
+        k = pop.id
+
+        def gsrc(name):
+            return self.ptr(f"pop{k}__{name}")
+
+        loads, stores = [], []
+        for name in names:
+            ct = "int" if pop._ctype.get(name) in ("int", "bool") else self.real
+            src = smem[name] if (smem and name in smem) else gsrc(name)
+            loads.append(f"{ct} {name} = {src}[anb_i];")
+            if name in modified or (spiking and any(r["name"] == name for r in
+                                                    pop.desc["spike"]["spike_reset"])):
+                stores.append(f"{src}[anb_i] = {name};")
+        if pop.neuron_type.type == "rate":
+            for t in pop.targets:
+                src = gsrc("_sum_" + t)
+                loads.append(f"const {self.real} _sum_{t} = {src}[anb_i];")
+                stores.append(f"{src}[anb_i] = ({self.real})0;")
+        spike_code = ""
+        if spiking:
+            rr_src = smem["refractory_remaining"] if smem else gsrc("refractory_remaining")
+            cond = self.typed(self.fill(pop.desc["spike"]["spike_cond"]))
+            resets = "\n          ".join(self.typed(self.fill(r["cpp"]))
+                                         for r in pop.desc["spike"]["spike_reset"])
+            if masked:
+                loads.append(f"int refractory_remaining = {rr_src}[anb_i];")
+                loads.append("const int in_ref = (refractory_remaining > 0) ? 0 : 1;")
+                refr_dec = "refractory_remaining -= (1 - in_ref);"
+                guard = f"(in_ref != 0) && ({cond})"
+                refr_set = f"refractory_remaining = {gsrc('refractory')}[anb_i];"
+                stores.append(f"{rr_src}[anb_i] = refractory_remaining;")
+            else:
+                refr_dec, guard, refr_set = "", f"({cond})", ""
+            spike_code = f"""{refr_dec}
+        if ({guard}) {{
+          {resets}
+          anb_spiked = true;
+          {gsrc('last_spike')}[anb_i] = t;
+          {refr_set}
+        }}"""
+        spk_dst = (smem["spk"] if smem else gsrc("spk")) if spiking else None
+        ballot = ""
+        if spiking:
+            ballot = f"""
+      {{
+        const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
+        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {spk_dst}[anb_i >> 5] = anb_m;
+      }}"""
+        if local_engine:
+            loop = "for (int anb_base = 0; anb_base < anb_n; anb_base += blockDim.x)"
+        else:
+            loop = ("for (int anb_base = blockIdx.x * blockDim.x; anb_base < anb_n; "
+                    "anb_base += gridDim.x * blockDim.x)")
+        nl = "\n        "
+        return f"""
+    {{  // population {pop.name}: update{' and spike gather' if spiking else ''}
+      const int anb_n = {pop.size};
+      {loop} {{
+        const int anb_i = anb_base + threadIdx.x;
+        bool anb_spiked = false;
+        if (anb_i < anb_n) {{
+        {nl.join(loads)}
+        {body.replace(chr(10), nl)}
+        {spike_code}
+        {nl.join(stores)}
+        }}{ballot}
+      }}
+    }}"""
+
+    def pop_kernel(self, pop) -> str:
+        preamble = self._globals_preamble(pop, lambda n: self.ptr(f"pop{pop.id}__{n}"))
+        dt_t = "double" if self.exact else "float"
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
+    const long long t = *{self.ptr('t')};
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    {preamble}
+{self.neuron_update(pop)}
+}}
+"""
+
+    def has_update(self, pop) -> bool:
+        if pop.neuron_type.type == "spike":
+            return True
+        return any(v.get("cpp") for v in pop.desc["variables"])
+
+    # ------------------------------------------------------------ projections
+    def rate_kernel(self, proj) -> str:
+        k = proj.id
+        lay = self.c.layout[proj.id]
+        pre_r = self.ptr(f"pop{proj.pre_pop.id}__r")
+        sum_ = self.ptr(f"pop{proj.post_pop.id}___sum_{proj.target}")
+        fmt = lay["format"]
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        W = self.c.wctype
+        if fmt == "csr":
+            if self.exact:
+                call = (f"anb_rate_csr_scalar<double, double, {lay['idx_t']}>({lay['rows']}, "
+                        f"{p('row_ptr')}, {p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_});")
+            else:
+                call = (f"anb_rate_csr_vector<{lay['group']}, {W}, {lay['idx_t']}>({lay['rows']}, "
+                        f"{p('row_ptr')}, {p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_}, "
+                        f"{lay['kahan_min']});")
+        elif fmt in ("ell", "ellr"):
+            rl = p("rl") if fmt == "ellr" else "nullptr"
+            call = (f"anb_rate_ell<{self.real}, {W}>({lay['rows']}, {lay['width']}, {p('ell_col')}, "
+                    f"{p('ell_w')}, {rl}, {pre_r}, {p('post_rank')}, {sum_});")
+        elif fmt == "sell":
+            call = (f"anb_rate_sell<{lay['C']}, {self.real}, {W}>({lay['rows']}, {p('slice_ptr')}, "
+                    f"{p('slice_len')}, {p('sell_col')}, {p('sell_w')}, {p('sell_rl')}, "
+                    f"{p('perm')}, {pre_r}, {p('post_rank')}, {sum_});")
+        elif fmt == "hyb":
+            call = (f"anb_rate_ell<{self.real}, {W}>({lay['rows']}, {lay['width']}, {p('ell_col')}, "
+                    f"{p('ell_w')}, {p('rl')}, {pre_r}, {p('post_rank')}, {sum_});")
+        elif fmt == "bsr":
+            call = (f"anb_rate_bsr<{lay['tile']}, {self.real}, {W}>({lay['block_rows']}, "
+                    f"{p('bsr_row_ptr')}, {p('bsr_col')}, {p('bsr_val')}, {pre_r}, "
+                    f"{p('bsr_post')}, {lay['n_post_pad']}, {sum_});")
+        else:
+            raise NotImplementedError(fmt)
+        out = f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    {call}
+}}
+"""
+        if fmt == "hyb" and lay["coo_nnz"] > 0:
+            out += self._hyb_tail(proj, lay, pre_r, sum_)
+        return out
+
+    def _hyb_tail(self, proj, lay, pre_r, sum_):
+        k = proj.id
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        if self.exact:
+            body = (f"anb_rate_csr_scalar<double, double, int>({lay['coo_rows']}, {p('coo_row_ptr')}, "
+                    f"{p('coo_col')}, {p('coo_w')}, {pre_r}, {p('coo_post')}, {sum_});")
+        else:
+            body = (f"anb_rate_coo_atomic<{self.c.wctype}>({lay['coo_nnz']}, {p('coo_row')}, "
+                    f"{p('coo_col')}, {p('coo_w')}, {pre_r}, {p('post_rank')}, {sum_});")
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp_tail() {{
+    {body}
+}}
+"""
+
+    def spike_kernel(self, proj) -> str:
+        k = proj.id
+        lay = self.c.layout[proj.id]
+        pre_spk = self.ptr(f"pop{proj.pre_pop.id}__spk")
+        g = self.ptr(f"pop{proj.post_pop.id}__g_{proj.target}")
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        if proj.plastic:
+            return self.plastic_psp_kernel(proj, lay, pre_spk, g)
+        if self.exact:
+            call = (f"anb_spike_gather<double, double>({lay['rows']}, {p('row_ptr')}, {p('col')}, "
+                    f"{p('w')}, {pre_spk}, {p('post_rank')}, {g});")
+        else:
+            call = (f"anb_spike_scatter<float, {self.c.wctype}>({lay['w0']}, {lay['w1']}, {pre_spk}, "
+                    f"{p('col_ptr')}, {p('post_idx')}, {p('w_pre')}, {g});")
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    {call}
+}}
+"""
+
+    # plastic synapses: pre_spike statements inlined in the transmission
+    def _syn_globals(self, proj):
+        out = []
+        for prm in proj.desc["parameters"] + proj.desc["variables"]:
+            if prm["locality"] == "global":
+                out.append(f"const {self.real} {prm['name']} = {self.ptr(f'proj{proj.id}__{prm['name']}')}[0];")
+        return "\n    ".join(out)
+
+    def _syn_arrays(self, proj):
+        names = ["w"] + [v["name"] for v in proj.desc["variables"]
+                         if v["locality"] == "local" and v["name"] != "w"]
+        for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
+            if v["name"] not in names and v["name"] != "g_target":
+                names.append(v["name"])
+        decl = []
+        for n in names:
+            decl.append(f"{self.real}* __restrict__ {n} = {self.ptr(f'proj{proj.id}__{n}')};")
+        decl.append(f"long long* __restrict__ _last_event = {self.ptr(f'proj{proj.id}___last_event')};")
+        return "\n    ".join(decl)
+
+    def _event_driven(self, proj, idx, t_expr):
+        out = []
+        for v in proj.desc["variables"]:
+            if v.get("method") == "event-driven":
+                code = self.fill(v["cpp"], local=f"[{idx}]")
+                out.append(self.typed(code.replace("(t))", f"({t_expr}))")))
+        out.append(f"_last_event[{idx}] = t;")
+        return out
+
+    def plastic_psp_kernel(self, proj, lay, pre_spk, g) -> str:
+        k = proj.id
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        stmts = self._event_driven(proj, "j", "t-1")
+        for v in proj.desc["pre_spike"]:
+            code = self.fill(v["cpp"], local="[j]")
+            if v["name"] == "w" and proj.desc["plasticity"]:
+                code = f"if (anb_plastic) {{ {code} }}"
+            stmts.append(self.typed(code))
+        body = "\n          ".join(stmts)
+        if self.exact:
+            # post-centric, ordered: pre spikes of a row in ascending pre rank
+            return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    const long long t = *{self.ptr('t')};
+    const double dt = *{self.ptr('dt')};
+    const int anb_plastic = {p('flags')}[0];
+    {self._syn_globals(proj)}
+    {self._syn_arrays(proj)}
+    for (int anb_row = blockIdx.x * blockDim.x + threadIdx.x; anb_row < {lay['rows']};
+         anb_row += gridDim.x * blockDim.x) {{
+      const int anb_post = {p('post_rank')}[anb_row];
+      double sum = {g}[anb_post];
+      for (int j = {p('row_ptr')}[anb_row]; j < {p('row_ptr')}[anb_row + 1]; ++j) {{
+        if (anb_bit({pre_spk}, {p('col')}[j])) {{
+          {body}
+        }}
+      }}
+      {g}[anb_post] = sum;
+    }}
+}}
+"""
+        # fast: warp per spiking pre neuron, synapse index through inv_idx
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    const long long t = *{self.ptr('t')};
+    const float dt = (float)(*{self.ptr('dt')});
+    const int anb_plastic = {p('flags')}[0];
+    {self._syn_globals(proj)}
+    {self._syn_arrays(proj)}
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int word = {lay['w0']} + warp; word < {lay['w1']}; word += nwarps) {{
+      anb_u32 m = {pre_spk}[word];
+      while (m) {{
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        const int anb_pre = (word << 5) + b;
+        const int anb_beg = {p('col_ptr')}[anb_pre], anb_end = {p('col_ptr')}[anb_pre + 1];
+        for (int anb_k = anb_beg + lane; anb_k < anb_end; anb_k += 32) {{
+          const int j = {p('inv_idx')}[anb_k];
+          float sum = 0.f;
+          {body}
+          atomicAdd(&{g}[{p('post_idx')}[anb_k]], sum);
+        }}
+      }}
+    }}
+}}
+"""
+
+    def post_event_kernel(self, proj) -> str:
+        k = proj.id
+        lay = self.c.layout[proj.id]
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        post_spk = self.ptr(f"pop{proj.post_pop.id}__spk")
+        stmts = self._event_driven(proj, "j", "t")
+        for v in proj.desc["post_spike"]:
+            code = self.fill(v["cpp"], local="[j]")
+            if v["name"] == "w":
+                code = f"if (anb_plastic) {{ {code} }}"
+            stmts.append(self.typed(code))
+        body = "\n        ".join(stmts)
+        dt_t = "double" if self.exact else "float"
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
+    const long long t = *{self.ptr('t')};
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    const int anb_plastic = {p('flags')}[0];
+    {self._syn_globals(proj)}
+    {self._syn_arrays(proj)}
+    for (int anb_row = blockIdx.x * blockDim.x + threadIdx.x; anb_row < {lay['rows']};
+         anb_row += gridDim.x * blockDim.x) {{
+      const int anb_post = {p('post_rank')}[anb_row];
+      if (!anb_bit({post_spk}, anb_post)) continue;
+      for (int j = {p('row_ptr')}[anb_row]; j < {p('row_ptr')}[anb_row + 1]; ++j) {{
+        {body}
+      }}
+    }}
+}}
+"""
+
+    # --------------------------------------------------------------- monitors
+    def monitor_kernel(self, mon) -> str:
+        m = mon.id
+        lay = self.c.mon_layout[m]
+        parts = []
+        if "spike" in mon.variables:
+            spk = self.ptr(f"pop{mon.population.id}__spk")
+            parts.append(f"""
+    if (anb_on) {{
+      const long long anb_slot = t - {self.ptr(f'mon{m}__t0')}[0];
+      if (anb_slot >= 0 && anb_slot < {lay['cap_spike']}) {{
+        anb_u32* anb_dst = {self.ptr(f'mon{m}__spk')} + anb_slot * {lay['words']};
+        for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < {lay['words']}; w += gridDim.x * blockDim.x)
+          anb_dst[w] = {spk}[w];
+      }} else if (blockIdx.x == 0 && threadIdx.x == 0) {{
+        anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+      }}
+    }}""")
+        for var in mon.variables:
+            if var == "spike":
+                continue
+            src = self.ptr(f"pop{mon.population.id}__{var}")
+            ranks = self.ptr(f"mon{m}__ranks") if mon.ranks is not None else "nullptr"
+            parts.append(f"""
+    if (anb_on && ((t - {self.ptr(f'mon{m}__start')}[0]) % {mon.period_steps} == {mon.period_offset_steps % mon.period_steps})) {{
+      const long long anb_slot = (t - {self.ptr(f'mon{m}__t0v')}[0]) / {mon.period_steps};
+      if (anb_slot >= 0 && anb_slot < {lay['cap_var']})
+        anb_record({src}, {ranks}, {lay['n']}, {self.ptr(f'mon{m}__{var}')}, anb_slot);
+      else if (blockIdx.x == 0 && threadIdx.x == 0)
+        anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+    }}""")
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
+    const long long t = *{self.ptr('t')};
+    const int anb_on = {self.ptr(f'mon{m}__on')}[0];
+    {''.join(parts)}
+}}
+"""
+
+    # ------------------------------------------------------------------ engines
+    def grid_module(self) -> Module:
+        net = self.net
+        kernels, plan = [], []
+        for proj in net.projections:
+            lay = self.c.layout[proj.id]
+            if proj.synapse_type.type == "rate":
+                kernels.append(self.rate_kernel(proj))
+                plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0))
+                if lay.get("format") == "hyb" and lay.get("coo_nnz", 0) > 0:
+                    plan.append((f"proj{proj.id}_psp_tail", lay["tail_grid"], BLOCK, 0))
+            else:
+                kernels.append(self.spike_kernel(proj))
+                plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0))
+        for pop in net.populations:
+            if self.has_update(pop):
+                kernels.append(self.pop_kernel(pop))
+                plan.append((f"pop{pop.id}_step", grid_for(pop.size), BLOCK, 0))
+        for proj in net.projections:
+            if proj.synapse_type.type == "spike" and proj.desc.get("post_spike"):
+                kernels.append(self.post_event_kernel(proj))
+                plan.append((f"proj{proj.id}_post_event", grid_for(self.c.layout[proj.id]["rows"]),
+                             BLOCK, 0))
+        for mon in net.monitors:
+            kernels.append(self.monitor_kernel(mon))
+            n = self.c.mon_layout[mon.id]["n"]
+            plan.append((f"mon{mon.id}_record", grid_for(max(n, 32)), BLOCK, 0))
+        kernels.append(f"""
+extern "C" __global__ void anb_tick() {{
+    if (blockIdx.x == 0 && threadIdx.x == 0) *{self.ptr('t')} += 1;
+}}
+""")
+        plan.append(("anb_tick", 1, 32, 0))
+        return Module(self.assemble(kernels), self.options(), "grid", plan=plan,
+                      kernels=[p[0] for p in plan])
+
+    def local_module(self) -> Module:
+        """One CTA holds every population's state in shared memory and runs
+        many steps per launch."""
+        net = self.net
+        layout = self.c.local_layout
+        block = layout["block"]
+        smem_ptrs: dict[int, dict] = {}
+        carve = []
+        for pop in net.populations:
+            d = {}
+            for name, (off, ct) in layout["pops"][pop.id].items():
+                carve.append(f"{ct}* __restrict__ anb_s_pop{pop.id}_{name} = "
+                             f"reinterpret_cast<{ct}*>(anb_smem + {off});")
+                d[name] = f"anb_s_pop{pop.id}_{name}"
+            smem_ptrs[pop.id] = d
+        load, store = [], []
+        for pop in net.populations:
+            for name, (off, ct) in layout["pops"][pop.id].items():
+                n = (pop.size + 31) // 32 if name == "spk" else pop.size
+                g = self.ptr(f"pop{pop.id}__{name}")
+                s = smem_ptrs[pop.id][name]
+                load.append(f"for (int q = threadIdx.x; q < {n}; q += blockDim.x) {s}[q] = {g}[q];")
+                store.append(f"for (int q = threadIdx.x; q < {n}; q += blockDim.x) {g}[q] = {s}[q];")
+        # propagation
+        prop = []
+        for proj in net.projections:
+            lay = self.c.layout[proj.id]
+            spk = smem_ptrs[proj.pre_pop.id]["spk"]
+            gname = "g_" + proj.target
+            g = smem_ptrs[proj.post_pop.id][gname]
+            p = lambda n, k=proj.id: self.ptr(f"proj{k}__{n}")
+            W = "double" if self.exact else self.c.wctype
+            if self.exact:
+                prop.append(f"""
+      // {proj.name}: spikes in ascending pre rank; one barrier per spike keeps
+      // the per-post accumulation order of the reference
+      for (int word = {lay['w0']}; word < {lay['w1']}; ++word) {{
+        anb_u32 m = {spk}[word];
+        while (m) {{
+          const int b = __ffs(m) - 1;
+          m &= m - 1;
+          const int pre = (word << 5) + b;
+          const int beg = {p('col_ptr')}[pre], end = {p('col_ptr')}[pre + 1];
+          if (end > beg) {{
+            for (int q = beg + threadIdx.x; q < end; q += blockDim.x)
+              {g}[{p('post_idx')}[q]] += {p('w_pre')}[q];
+            __syncthreads();
+          }}
+        }}
+      }}""")
+            else:
+                prop.append(f"""
+      // {proj.name}: warp per 32-neuron word, shared-memory atomics
+      for (int word = {lay['w0']} + anb_warp; word < {lay['w1']}; word += anb_nwarps) {{
+        anb_u32 m = {spk}[word];
+        while (m) {{
+          const int b = __ffs(m) - 1;
+          m &= m - 1;
+          const int pre = (word << 5) + b;
+          const int beg = {p('col_ptr')}[pre], end = {p('col_ptr')}[pre + 1];
+          for (int q = beg + anb_lane; q < end; q += 32)
+            atomicAdd(&{g}[{p('post_idx')}[q]], anb_wf({p('w_pre')}[q]));
+        }}
+      }}""")
+        updates = []
+        globals_ = []
+        for pop in net.populations:
+            globals_.append(self._globals_preamble(pop, lambda n, k=pop.id: self.ptr(f"pop{k}__{n}")))
+            updates.append(self.neuron_update(pop, local_engine=True, smem=smem_ptrs[pop.id]))
+        recs = []
+        for mon in net.monitors:
+            lay = self.c.mon_layout[mon.id]
+            m = mon.id
+            spk = smem_ptrs[mon.population.id]["spk"]
+            recs.append(f"""
+      if (anb_mon_on{m}) {{
+        const long long anb_slot = t - anb_mon_t0{m};
+        if (anb_slot >= 0 && anb_slot < {lay['cap_spike']}) {{
+          anb_u32* anb_dst = {self.ptr(f'mon{m}__spk')} + anb_slot * {lay['words']};
+          for (int q = threadIdx.x; q < {lay['words']}; q += blockDim.x) anb_dst[q] = {spk}[q];
+        }} else if (threadIdx.x == 0) {{
+          anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+        }}
+      }}""")
+        mon_pre = "\n    ".join(
+            f"const int anb_mon_on{mon.id} = {self.ptr(f'mon{mon.id}__on')}[0];\n    "
+            f"const long long anb_mon_t0{mon.id} = {self.ptr(f'mon{mon.id}__t0')}[0];"
+            for mon in net.monitors)
+        dt_t = "double" if self.exact else "float"
+        nl = "\n    "
+        src = f"""
+extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long t0, int nsteps) {{
+    extern __shared__ __align__(16) unsigned char anb_smem[];
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    const int anb_lane = threadIdx.x & 31;
+    const int anb_warp = threadIdx.x >> 5;
+    const int anb_nwarps = blockDim.x >> 5;
+    (void)anb_lane; (void)anb_warp; (void)anb_nwarps;
+    {nl.join(carve)}
+    {nl.join(g for g in globals_ if g)}
+    {mon_pre}
+    {nl.join(load)}
+    __syncthreads();
+    for (int anb_s = 0; anb_s < nsteps; ++anb_s) {{
+      const long long t = t0 + anb_s;
+      {''.join(prop)}
+      __syncthreads();
+      {''.join(updates)}
+      __syncthreads();
+      {''.join(recs)}
+    }}
+    __syncthreads();
+    {nl.join(store)}
+    if (threadIdx.x == 0) *{self.ptr('t')} = t0 + nsteps;
+}}
+"""
+        return Module(self.assemble([src]), self.options(), "local",
+                      local=("anb_local_run", 1, block, layout["smem"]), kernels=["anb_local_run"])
+
+    # ------------------------------------------------------------------ output
+    def options(self) -> list:
+        opts = ["-diag-suppress=177"]
+        if self.exact:
+            opts.append("--fmad=false")
+        cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+        if os.path.isdir(cuda_inc):
+            opts.append("-I" + cuda_inc)
+        return opts
+
+    def assemble(self, kernels: list) -> str:
+        header = open(DEVICE_HEADER).read()
+        self.ptr("t")
+        self.ptr("dt")
+        self.ptr("err")
+        decl = "\n".join(f"__constant__ {ct}* anb_p_{name};" for name, ct in sorted(self.decls.items()))
+        return (f"// generated by annarchy_b200 for network {self.net.id}\n{header}\n"
+                f"typedef {self.real} real;\n{decl}\n" + "".join(kernels))

@@ -1,0 +1,198 @@
+"""Storage formats of rate-coded projections and their conversion from CSR.
+
+Containers restated from the reference's headers (ANNarchy/include/*.hpp):
+
+* ELL   (ELLMatrix.hpp:76, init :290-363): rows padded to the longest row,
+        column-major slots (slot k of row r at k*rows + r), empty slots hold
+        -1 (the reference uses the index type's maximum).
+* ELL-R (ELLRMatrix.hpp:73, init :245): ELL plus the length of every row.
+* SELL  (SELLMatrix.hpp:69, init :285): slices of C rows, each padded to its
+        own longest row; the reference uses C = 32 rows and keeps the row
+        order. This backend also sorts rows by length inside windows of
+        sigma rows (SELL-C-sigma) and keeps the permutation.
+* BSR   (BSRMatrix.hpp:41, init :149-260): dense t x t tiles, block-row
+        pointer and block-column indices, column-major tiles.
+* HYB   (HYBMatrix.hpp:68, init :279): an ELL part of width k plus a COO
+        tail holding the rest of every longer row; the reference picks k as
+        the modal row length (HYBMatrix.hpp:84-104).
+
+In double precision every format sums each row in ascending pre rank, so
+its result equals CSR bit for bit, except HYB, which adds the ELL part and
+then the tail of a row (the reference's HYB differs from CSR the same way).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RATE_FORMATS = ("csr", "ell", "ellr", "sell", "bsr", "hyb")
+
+
+def csr_group(mean_row: float) -> int:
+    """Lanes per row of the vector CSR kernel."""
+    for g in (2, 4, 8, 16):
+        if mean_row <= 2 * g:
+            return g
+    return 32
+
+
+def _lengths(row_ptr):
+    return np.diff(np.asarray(row_ptr, dtype=np.int64))
+
+
+def ell_arrays(row_ptr, cols, w, width=None):
+    """(cols, w, rl) column-major with `width` slots per row (default: max)."""
+    rl = _lengths(row_ptr)
+    rows = rl.size
+    width = int(rl.max()) if width is None and rows else int(width or 0)
+    ec = np.full((width, rows), -1, dtype=np.int32)
+    ew = np.zeros((width, rows), dtype=np.float64)
+    r_of = np.repeat(np.arange(rows), rl)
+    k_of = np.arange(cols.size) - np.repeat(np.asarray(row_ptr[:-1], dtype=np.int64), rl)
+    keep = k_of < width
+    ec[k_of[keep], r_of[keep]] = cols[keep]
+    ew[k_of[keep], r_of[keep]] = w[keep]
+    return ec.ravel(), ew.ravel(), np.minimum(rl, width).astype(np.int32), width
+
+
+def sell_arrays(row_ptr, cols, w, C=32, sigma=1):
+    """SELL-C-sigma. Returns dict with slice_ptr, slice_len, cols, w, row_len
+    (in sorted order) and perm (sorted position -> original row)."""
+    rl = _lengths(row_ptr)
+    rows = rl.size
+    perm = np.arange(rows)
+    if sigma > 1:
+        for s0 in range(0, rows, sigma):
+            s1 = min(rows, s0 + sigma)
+            perm[s0:s1] = s0 + np.argsort(-rl[s0:s1], kind="stable")
+    nsl = (rows + C - 1) // C
+    slice_len = np.zeros(nsl, dtype=np.int32)
+    rl_sorted = rl[perm]
+    for s in range(nsl):
+        seg = rl_sorted[s * C:(s + 1) * C]
+        slice_len[s] = seg.max() if seg.size else 0
+    slice_ptr = np.zeros(nsl + 1, dtype=np.int64)
+    np.cumsum(slice_len.astype(np.int64) * C, out=slice_ptr[1:])
+    sc = np.zeros(int(slice_ptr[-1]), dtype=np.int32)
+    sw = np.zeros(int(slice_ptr[-1]), dtype=np.float64)
+    starts = np.asarray(row_ptr[:-1], dtype=np.int64)
+    for pos in range(rows):
+        r = perm[pos]
+        s, lane = divmod(pos, C)
+        L = rl[r]
+        if L:
+            slots = slice_ptr[s] + np.arange(L) * C + lane
+            sc[slots] = cols[starts[r]:starts[r] + L]
+            sw[slots] = w[starts[r]:starts[r] + L]
+    return dict(slice_ptr=slice_ptr[:-1].astype(np.int32), slice_len=slice_len, cols=sc, w=sw,
+                row_len=rl_sorted.astype(np.int32), perm=perm.astype(np.int32), nslices=nsl)
+
+
+def hyb_width(row_ptr) -> int:
+    """ELL width of the HYB split: the modal row length (HYBMatrix.hpp:84-104)."""
+    rl = _lengths(row_ptr)
+    if rl.size == 0:
+        return 0
+    counts = np.bincount(rl)
+    return int(np.argmax(counts))
+
+
+def bsr_arrays(post_rank, row_ptr, cols, w, n_pre, tile):
+    """Dense t x t tiles over (post rank, pre rank). Returns block-row
+    pointers, block columns, tile values (row-major inside a tile), the post
+    rank of every tile row and the padded sizes."""
+    rl = _lengths(row_ptr)
+    rows_of = np.repeat(np.asarray(post_rank, dtype=np.int64), rl)
+    n_post = int(post_rank.max()) + 1 if post_rank.size else 0
+    nbr = (n_post + tile - 1) // tile
+    br, bc = rows_of // tile, np.asarray(cols, dtype=np.int64) // tile
+    key = br * ((n_pre + tile - 1) // tile) + bc
+    ukey, inv = np.unique(key, return_inverse=True)
+    nblk = ukey.size
+    ubr = ukey // ((n_pre + tile - 1) // tile)
+    ubc = ukey % ((n_pre + tile - 1) // tile)
+    vals = np.zeros((nblk, tile, tile), dtype=np.float64)
+    vals[inv, rows_of % tile, np.asarray(cols) % tile] = w
+    brp = np.zeros(nbr + 1, dtype=np.int32)
+    np.cumsum(np.bincount(ubr, minlength=nbr), out=brp[1:])
+    return dict(block_row_ptr=brp, block_col=ubc.astype(np.int32), values=vals.reshape(-1),
+                n_block_rows=nbr, n_blocks=nblk, n_post_pad=nbr * tile)
+
+
+def select_format(proj, compiled) -> str:
+    """Format used for storage_format='auto': the reference's heuristic for
+    rate-coded projections on the GPU (ANNarchy/core/Projection.py:691-789):
+    mean row length <= 128 -> SELL (ELL-R when plastic), else CSR. The learned
+    selector, when trained, overrides it (annarchy_b200.tuning)."""
+    sched = getattr(proj, "_schedule", None)
+    if sched:
+        return sched
+    m = proj._csr
+    mean = m.nnz / max(1, (np.diff(m.indptr) > 0).sum())
+    if mean <= 128:
+        return "ellr" if proj.plastic else "sell"
+    return "csr"
+
+
+def create_format_arrays(compiled, proj, fmt, post_rank, row_ptr, cols, w, lay):
+    nat = compiled.native
+    k = proj.id
+    W = compiled._w
+    if fmt in ("ell", "ellr"):
+        ec, ew, rl, width = ell_arrays(row_ptr, cols, w)
+        nat.create(f"proj{k}__ell_col", ec)
+        nat.create(f"proj{k}__ell_w", W(ew))
+        if fmt == "ellr":
+            nat.create(f"proj{k}__rl", rl)
+        lay["width"] = width
+    elif fmt == "sell":
+        C = 32
+        sigma = int(proj.net._config.get("sell_sigma", 1024)) if not compiled.exact else 1
+        d = sell_arrays(row_ptr, cols, w, C=C, sigma=sigma)
+        nat.create(f"proj{k}__slice_ptr", d["slice_ptr"])
+        nat.create(f"proj{k}__slice_len", d["slice_len"])
+        nat.create(f"proj{k}__sell_col", d["cols"])
+        nat.create(f"proj{k}__sell_w", W(d["w"]))
+        nat.create(f"proj{k}__sell_rl", d["row_len"])
+        nat.create(f"proj{k}__perm", d["perm"])
+        lay["C"] = C
+    elif fmt == "hyb":
+        width = hyb_width(row_ptr)
+        ec, ew, rl, _ = ell_arrays(row_ptr, cols, w, width=width)
+        nat.create(f"proj{k}__ell_col", ec)
+        nat.create(f"proj{k}__ell_w", W(ew))
+        nat.create(f"proj{k}__rl", rl)
+        lay["width"] = width
+        lens = _lengths(row_ptr)
+        tail_len = np.maximum(lens - width, 0)
+        tail_rows = np.nonzero(tail_len)[0]
+        starts = np.asarray(row_ptr[:-1], dtype=np.int64)
+        idx = np.concatenate([np.arange(starts[r] + width, starts[r] + lens[r]) for r in tail_rows]) \
+            if tail_rows.size else np.zeros(0, dtype=np.int64)
+        lay["coo_nnz"] = int(idx.size)
+        lay["coo_rows"] = int(tail_rows.size)
+        if idx.size:
+            trp = np.zeros(tail_rows.size + 1, dtype=np.int32)
+            np.cumsum(tail_len[tail_rows], out=trp[1:])
+            nat.create(f"proj{k}__coo_row_ptr", trp)
+            nat.create(f"proj{k}__coo_post", post_rank[tail_rows].astype(np.int32))
+            nat.create(f"proj{k}__coo_row", np.repeat(tail_rows, tail_len[tail_rows]).astype(np.int32))
+            nat.create(f"proj{k}__coo_col", cols[idx].astype(np.int32))
+            nat.create(f"proj{k}__coo_w", W(w[idx]) if not compiled.exact else w[idx])
+            from .codegen import grid_for
+            lay["tail_grid"] = grid_for(int(idx.size) if not compiled.exact else int(tail_rows.size))
+    elif fmt == "bsr":
+        tile = int(getattr(proj, "_bsr_tile_size", 0) or proj.net._config.get("bsr_tile", 16))
+        d = bsr_arrays(post_rank, row_ptr, cols, w, proj.pre_pop.size, tile)
+        nat.create(f"proj{k}__bsr_row_ptr", d["block_row_ptr"])
+        nat.create(f"proj{k}__bsr_col", d["block_col"])
+        nat.create(f"proj{k}__bsr_val", W(d["values"]))
+        lay.update(tile=tile, block_rows=d["n_block_rows"], n_post_pad=d["n_post_pad"])
+    else:
+        raise ValueError(f"unknown format {fmt!r}")
+
+
+def refresh_format_weights(compiled, proj, w_flat):
+    post_rank, row_ptr, cols, _ = proj.csr_population_ranks()
+    lay = compiled.layout[proj.id]
+    create_format_arrays(compiled, proj, lay["format"], post_rank, row_ptr, cols,
+                         np.asarray(w_flat, dtype=np.float64), dict(lay))

@@ -1,0 +1,278 @@
+"""ctypes binding of the C ABI in include/annarchy_b200.h.
+
+The shared library is built in-tree (``annarchy_b200/_lib``) by
+``annarchy_b200.build.build_all()``. There is no fallback: if the library
+is missing or no GPU is visible, creating a network raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "_lib", "libannarchy_b200.so")
+
+ANB_OK = 0
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_ALLOC", 3: "ERR_CUDA", 4: "ERR_COMPILE",
+          5: "ERR_TIMEOUT", 6: "ERR_STATE"}
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "anb_abi_version": (C.c_int, []),
+    "anb_last_error": (C.c_char_p, []),
+    "anb_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "anb_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "anb_destroy": (C.c_int, [C.c_void_p]),
+    "anb_initialize": (C.c_int, [C.c_void_p, C.c_double]),
+    "anb_set_time": (C.c_int, [C.c_void_p, C.c_int64]),
+    "anb_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "anb_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "anb_array_create": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "anb_array_free": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "anb_array_write": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_void_p, C.c_size_t]),
+    "anb_array_read": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_void_p, C.c_size_t]),
+    "anb_array_fill_zero": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "anb_array_info": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p),
+                                 C.POINTER(C.c_size_t)]),
+    "anb_module_load": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
+    "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
+                                    C.POINTER(C.c_size_t)]),
+    "anb_plan_clear": (C.c_int, [C.c_void_p]),
+    "anb_plan_add": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint]),
+    "anb_set_local_kernel": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint]),
+    "anb_set_graph_steps": (C.c_int, [C.c_void_p, C.c_int]),
+    "anb_run": (C.c_int, [C.c_void_p, C.c_int64]),
+    "anb_step": (C.c_int, [C.c_void_p]),
+    "anb_synchronize": (C.c_int, [C.c_void_p]),
+    "anb_device_error": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "anb_clear_device_error": (C.c_int, [C.c_void_p]),
+    "anb_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "anb_kernel_time_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "anb_kernel_time_get": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+}
+
+_lib = None
+
+# arrays every network has from anb_create on: step counter, dt, error words
+BUILTIN_ARRAYS = {"t": (np.dtype(np.int64), (1,)), "dt": (np.dtype(np.float64), (1,)),
+                  "err": (np.dtype(np.int32), (4,))}
+
+
+class BackendError(RuntimeError):
+    """A call of the native library failed."""
+
+    def __init__(self, fn: str, status: int, message: str):
+        super().__init__(f"{fn} -> {STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def load():
+    """Load libannarchy_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"native library not found at {LIB_PATH}; build it with "
+                           "`python -c 'import annarchy_b200.build as b; b.build_all()'`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(fn: str, status: int):
+    if status != ANB_OK:
+        msg = load().anb_last_error()
+        raise BackendError(fn, status, msg.decode(errors="replace") if msg else "")
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    check("anb_device_count", load().anb_device_count(C.byref(n)))
+    return n.value
+
+
+def nvrtc_compile(source: str, options: list[str]) -> tuple[int, str]:
+    """Compile a generated module for sm_100a without a device; returns
+    (cubin bytes, compiler log). Raises BackendError with the log on errors."""
+    log = C.create_string_buffer(1 << 16)
+    n = C.c_size_t(0)
+    check("anb_nvrtc_compile", load().anb_nvrtc_compile(source.encode(), "\n".join(options).encode(),
+                                                        log, len(log), C.byref(n)))
+    return n.value, log.value.decode(errors="replace")
+
+
+class NativeNet:
+    """One network instance inside the native library."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        check("anb_create", self.lib.anb_create(device, C.byref(h)))
+        self.h = h
+        self.arrays: dict[str, tuple[np.dtype, tuple]] = dict(BUILTIN_ARRAYS)
+
+    def close(self):
+        if self.h:
+            self.lib.anb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- lifetime / time --------------------------------------------------
+    def initialize(self, dt: float):
+        check("anb_initialize", self.lib.anb_initialize(self.h, float(dt)))
+
+    def set_time(self, t: int):
+        check("anb_set_time", self.lib.anb_set_time(self.h, int(t)))
+
+    def get_time(self) -> int:
+        t = C.c_int64()
+        check("anb_get_time", self.lib.anb_get_time(self.h, C.byref(t)))
+        return t.value
+
+    def set_stream(self, stream_ptr: int | None):
+        check("anb_set_stream", self.lib.anb_set_stream(self.h, C.c_void_p(stream_ptr or None)))
+
+    # -- arrays -------------------------------------------------------------
+    def create(self, name: str, data: np.ndarray):
+        """Create (or re-create) array `name` holding a copy of `data`."""
+        data = np.ascontiguousarray(data)
+        check("anb_array_create", self.lib.anb_array_create(self.h, name.encode(), data.nbytes))
+        self.arrays[name] = (data.dtype, data.shape)
+        if data.nbytes:
+            self.write(name, data)
+
+    def create_empty(self, name: str, dtype, shape):
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+        check("anb_array_create", self.lib.anb_array_create(self.h, name.encode(), nbytes))
+        self.arrays[name] = (dtype, tuple(shape) if isinstance(shape, (tuple, list)) else (shape,))
+
+    def write(self, name: str, data: np.ndarray, offset_bytes: int = 0):
+        data = np.ascontiguousarray(data)
+        check("anb_array_write", self.lib.anb_array_write(
+            self.h, name.encode(), offset_bytes, data.ctypes.data_as(C.c_void_p), data.nbytes))
+
+    def read(self, name: str, count: int | None = None, offset: int = 0) -> np.ndarray:
+        dtype, shape = self.arrays[name]
+        if count is None:
+            out = np.empty(shape, dtype=dtype)
+        else:
+            out = np.empty(count, dtype=dtype)
+        check("anb_array_read", self.lib.anb_array_read(
+            self.h, name.encode(), offset * dtype.itemsize, out.ctypes.data_as(C.c_void_p),
+            out.nbytes))
+        return out
+
+    def read_into(self, name: str, out: np.ndarray, offset_bytes: int = 0):
+        check("anb_array_read", self.lib.anb_array_read(
+            self.h, name.encode(), offset_bytes, out.ctypes.data_as(C.c_void_p), out.nbytes))
+
+    def zero(self, name: str):
+        check("anb_array_fill_zero", self.lib.anb_array_fill_zero(self.h, name.encode()))
+
+    def device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        n = C.c_size_t()
+        check("anb_array_info", self.lib.anb_array_info(self.h, name.encode(), C.byref(p),
+                                                       C.byref(n)))
+        return p.value or 0
+
+    def free(self, name: str):
+        check("anb_array_free", self.lib.anb_array_free(self.h, name.encode()))
+        self.arrays.pop(name, None)
+
+    # -- module and plan ------------------------------------------------------
+    def load_module(self, source: str, options: list[str]):
+        check("anb_module_load", self.lib.anb_module_load(self.h, source.encode(),
+                                                         "\n".join(options).encode()))
+
+    def plan(self, launches):
+        check("anb_plan_clear", self.lib.anb_plan_clear(self.h))
+        for name, grid, block, smem in launches:
+            check("anb_plan_add", self.lib.anb_plan_add(self.h, name.encode(), grid, block, smem))
+
+    def set_local_kernel(self, name, grid, block, smem):
+        check("anb_set_local_kernel", self.lib.anb_set_local_kernel(self.h, name.encode(), grid,
+                                                                   block, smem))
+
+    def set_graph_steps(self, steps: int):
+        check("anb_set_graph_steps", self.lib.anb_set_graph_steps(self.h, steps))
+
+    def run(self, steps: int):
+        check("anb_run", self.lib.anb_run(self.h, int(steps)))
+
+    def synchronize(self):
+        check("anb_synchronize", self.lib.anb_synchronize(self.h))
+
+    def device_error(self) -> int:
+        c = C.c_int()
+        check("anb_device_error", self.lib.anb_device_error(self.h, C.byref(c)))
+        return c.value
+
+    # -- timing -----------------------------------------------------------------
+    def kernel_timing(self, enable: bool):
+        check("anb_kernel_timing", self.lib.anb_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_times(self) -> dict[str, tuple[float, int]]:
+        n = C.c_int()
+        check("anb_kernel_time_count", self.lib.anb_kernel_time_count(self.h, C.byref(n)))
+        out = {}
+        buf = C.create_string_buffer(256)
+        for i in range(n.value):
+            ms = C.c_double()
+            cnt = C.c_int64()
+            check("anb_kernel_time_get", self.lib.anb_kernel_time_get(
+                self.h, i, buf, 256, C.byref(ms), C.byref(cnt)))
+            out[buf.value.decode()] = (ms.value, cnt.value)
+        return out
+
+
+class DryNative:
+    """Stand-in for NativeNet that only records array names, types and
+    shapes. It lets the code generator run on a machine without a GPU, so the
+    generated module can be compiled (nvrtc_compile) and inspected there."""
+
+    def __init__(self, device: int = 0):
+        self.arrays: dict[str, tuple[np.dtype, tuple]] = dict(BUILTIN_ARRAYS)
+        self.source = None
+        self.options = None
+
+    def initialize(self, dt):
+        pass
+
+    def create(self, name, data):
+        data = np.asarray(data)
+        self.arrays[name] = (data.dtype, data.shape)
+
+    def create_empty(self, name, dtype, shape):
+        self.arrays[name] = (np.dtype(dtype), tuple(np.atleast_1d(shape)))
+
+    def write(self, *a, **k):
+        pass
+
+    def load_module(self, source, options):
+        self.source, self.options = source, options
+
+    def plan(self, launches):
+        self.launches = list(launches)
+
+    def set_local_kernel(self, *a):
+        self.local = a
+
+    def set_graph_steps(self, steps):
+        pass
+
+    def close(self):
+        pass

@@ -257,3 +257,57 @@ def batched_coba(n_instances: int = 256, seed: int = 42, n_min: int = 1000,
         nets.append(coba_net(seed=seed + i, n=int(sizes[i]), w_exc=float(we[i % side]),
                              w_inh=float(wi[i // side]), steps=steps))
     return nets
+
+
+# ---------------------------------------------------------------------------
+# networks built through the public API
+# ---------------------------------------------------------------------------
+
+def build_rate_network(rn: RateNet, precision: str = "double", record: bool = True,
+                       storage_format: str = "csr", **config):
+    """Input population (constant r) -> leaky integrators, input and
+    recurrent projections on target 'exc'. Returns (net, pop, monitor)."""
+    from . import Network, Neuron
+    net = Network(dt=rn.dt, seed=0)
+    net.config(precision=precision, **config)
+    inp = net.create(rn.n_in, Neuron(parameters="r = 0.0"))
+    li = Neuron(parameters=dict(tau=rn.tau), equations="tau*dr/dt + r = sum(exc) : min=0.0")
+    pop = net.create(rn.n_out, li)
+    net.connect(inp, pop, "exc").from_sparse(to_from_sparse(rn.w_in), storage_format=storage_format)
+    net.connect(pop, pop, "exc").from_sparse(to_from_sparse(rn.w_rec), storage_format=storage_format)
+    mon = net.monitor(pop, "r") if record else None
+    inp.r = rn.r_in
+    return net, pop, mon
+
+
+def coba_neuron(params: dict):
+    from . import Neuron
+    return Neuron(parameters=dict(params), equations=list(COBA_EQUATIONS), spike=COBA_SPIKE,
+                  reset=COBA_RESET, refractory=COBA_REFRACTORY)
+
+
+def build_coba_network(cn: CobaNet, precision: str = "double", engine: str = "auto",
+                       record: bool = True, stdp_w_ee: sp.csr_matrix | None = None, **config):
+    """The spiking net: E->all (exc) and I->all (inh); with a plastic E->E
+    matrix: E->E (STDP, exc), E->I (exc), I->all (inh). Returns (net, pop,
+    monitor); the initial potentials are set after compile()."""
+    from . import STDP, Network
+    net = Network(dt=cn.dt, seed=0)
+    net.config(precision=precision, engine=engine, **config)
+    P = net.create(cn.n, coba_neuron(cn.params))
+    Pe, Pi = P[: cn.n_exc], P[cn.n_exc:]
+    if stdp_w_ee is None:
+        net.connect(Pe, P, "exc").from_sparse(to_from_sparse(cn.w_exc))
+    else:
+        net.connect(Pe, Pe, "exc", synapse=STDP(**STDP_PARAMS)).from_sparse(to_from_sparse(stdp_w_ee))
+        net.connect(Pe, Pi, "exc").from_sparse(to_from_sparse(cn.w_exc[cn.n_exc:]))
+    net.connect(Pi, P, "inh").from_sparse(to_from_sparse(cn.w_inh))
+    mon = net.monitor(P, "spike") if record else None
+    P.v = cn.v0
+    return net, P, mon
+
+
+def stdp_matrix(cn: CobaNet, seed: int, p: float) -> sp.csr_matrix:
+    """Plastic E->E weights U[0, 0.5] of the plastic test network."""
+    rng = np.random.default_rng(seed + 1000)
+    return bernoulli_csr(rng, cn.n_exc, cn.n_exc, p, lambda k: rng.uniform(0.0, 0.5, k))

@@ -98,6 +98,12 @@ int anb_array_info(anb_net* net, const char* name, void** device_ptr, size_t* by
  * (ANNarchy/generator/Compiler.py:496-596). */
 int anb_module_load(anb_net* net, const char* source, const char* options);
 
+/* Compile-only check of a generated module (no device needed): NVRTC for
+ * sm_100a; the compiler log is copied into `log` (may be NULL) and the cubin
+ * size into *cubin_bytes. */
+int anb_nvrtc_compile(const char* source, const char* options, char* log, size_t log_len,
+                      size_t* cubin_bytes);
+
 /* Kernels launched, in order, once per simulation step (grid engine). */
 int anb_plan_clear(anb_net* net);
 int anb_plan_add(anb_net* net, const char* kernel, unsigned grid, unsigned block,

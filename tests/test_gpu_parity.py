@@ -1,0 +1,141 @@
+"""CUDA backend vs the reference: bit-exact in double precision (against the
+golden fixtures produced by the reference itself and against the oracle),
+within stated tolerances in single precision."""
+import numpy as np
+import pytest
+
+from annarchy_b200 import workloads as wl
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def run_rate(rn, steps, **kw):
+    net, pop, mon = wl.build_rate_network(rn, **kw)
+    net.compile()
+    net.simulate_steps(steps)
+    r = mon.get("r")
+    net.close()
+    return r
+
+
+def run_coba(cn, steps, **kw):
+    net, P, mon = wl.build_coba_network(cn, **kw)
+    net.compile()
+    net.simulate_steps(steps)
+    s, i = mon.spike_arrays()
+    out = dict(steps=s, idx=i, v=P.v.copy(), g_exc=P.g_exc.copy(), g_inh=P.g_inh.copy(),
+               engine=net.engine)
+    out["net"] = net
+    return out
+
+
+def test_rate_small_exact(golden):
+    g = golden("rate_small")
+    rn = wl.rate_net(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100)
+    r = run_rate(rn, 100)
+    assert np.array_equal(r, g["r_at"])
+
+
+def test_rate_c1_exact(golden):
+    g = golden("rate_c1")
+    rn = wl.rate_net(seed=42)
+    r = run_rate(rn, 1000)
+    assert np.array_equal(r[g["record_steps"]], g["r_at"])
+    assert np.array_equal(r.sum(axis=1), g["r_sum"])
+
+
+@pytest.mark.parametrize("fmt", ["ell", "ellr", "sell"])
+def test_rate_formats_exact(golden, fmt):
+    """ELL, ELL-R and SELL sum every row in ascending pre rank: bit-identical to CSR."""
+    g = golden("rate_small")
+    rn = wl.rate_net(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100)
+    r = run_rate(rn, 100, storage_format=fmt)
+    assert np.array_equal(r, g["r_at"])
+
+
+def test_rate_hyb_close(golden):
+    """HYB adds the ELL part and the COO tail of a row separately (as the
+    reference's HYB does): equal to CSR up to rounding."""
+    g = golden("rate_small")
+    rn = wl.rate_net(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100)
+    r = run_rate(rn, 100, storage_format="hyb")
+    np.testing.assert_allclose(r, g["r_at"], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("wdt", ["float32", "bfloat16"])
+def test_rate_float(wdt):
+    """Single-precision state and accumulation: norm-wise relative error of r
+    per step <= 1e-5 against the double oracle fed the same (rounded) weights."""
+    rn = wl.rate_net(seed=42, steps=200)
+    if wdt == "bfloat16":
+        from annarchy_b200.core.backend import from_bf16, to_bf16
+        rn.w_in.data = from_bf16(to_bf16(rn.w_in.data))
+        rn.w_rec.data = from_bf16(to_bf16(rn.w_rec.data))
+    _, ref = O.rate_run(rn, trace=True)
+    r = run_rate(rn, 200, precision="float", weight_dtype=wdt)
+    err = np.linalg.norm(r - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert err.max() <= 1e-5, err.max()
+
+
+@pytest.mark.parametrize("engine", ["grid", "local"])
+def test_coba_small_exact(golden, engine):
+    g = golden("coba_small")
+    cn = wl.coba_net(seed=7, n=400, p=0.05, steps=2000)
+    out = run_coba(cn, 2000, engine=engine)
+    assert out["engine"] == engine
+    assert np.array_equal(out["steps"], g["spike_steps"])
+    assert np.array_equal(out["idx"], g["spike_idx"])
+    for k in ("v", "g_exc", "g_inh"):
+        assert np.array_equal(out[k], g[k + "_final"]), k
+    out["net"].close()
+
+
+def test_coba_c2_exact(golden):
+    g = golden("coba_c2")
+    cn = wl.coba_net(seed=42)
+    out = run_coba(cn, 10000)
+    assert np.array_equal(out["steps"], g["spike_steps"])
+    assert np.array_equal(out["idx"], g["spike_idx"])
+    for k in ("v", "g_exc", "g_inh"):
+        assert np.array_equal(out[k], g[k + "_final"]), k
+    out["net"].close()
+
+
+def test_coba_oracle_other_seed_grid_vs_local():
+    cn = wl.coba_net(seed=3, n=1000, p=0.03, steps=1500)
+    ref = O.coba_run(cn)
+    for engine in ("grid", "local"):
+        out = run_coba(cn, 1500, engine=engine)
+        assert np.array_equal(out["idx"], ref["spike_idx"]), engine
+        assert np.array_equal(out["v"], ref["v"]), engine
+        out["net"].close()
+
+
+def test_stdp_small(golden):
+    """Plastic E->E: spikes bit-exact; weights equal up to the last-ulp
+    differences of the device exp() against glibc's."""
+    g = golden("stdp_small")
+    cn = wl.coba_net(seed=11, n=400, p=0.05, steps=2000)
+    w_ee = wl.stdp_matrix(cn, 11, 0.05)
+    out = run_coba(cn, 2000, stdp_w_ee=w_ee)
+    assert np.array_equal(out["steps"], g["spike_steps"])
+    assert np.array_equal(out["idx"], g["spike_idx"])
+    w = out["net"].projections[0].get("w", flat=True)
+    np.testing.assert_allclose(w, g["w_ee_final"], rtol=0, atol=1e-12)
+    out["net"].close()
+
+
+@pytest.mark.parametrize("engine", ["grid", "local"])
+def test_coba_float_rates(engine):
+    """Single precision: identical rasters over the first steps, firing
+    rate within 2 % of the double oracle over 2000 steps."""
+    cn = wl.coba_net(seed=42, n=4000, p=0.02, steps=2000)
+    ref = O.coba_run(cn)
+    out = run_coba(cn, 2000, precision="float", engine=engine)
+    n_ref, n = ref["n_spikes"], out["idx"].size
+    assert abs(n - n_ref) / n_ref < 0.02, (n, n_ref)
+    early = ref["spike_steps"] < 300
+    e2 = out["steps"] < 300
+    assert np.array_equal(out["idx"][e2], ref["spike_idx"][early])
+    out["net"].close()

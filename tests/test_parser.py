@@ -1,0 +1,56 @@
+"""The parser restatement against the reference parser's output for a
+catalogue of models (tests/golden/parser_strings.json)."""
+import json
+import os
+
+import pytest
+
+from annarchy_b200.core.models import Neuron, Synapse
+from annarchy_b200.parser.analysis import analyse_neuron, analyse_synapse
+from annarchy_b200.parser.models_catalog import NEURONS, SYNAPSES
+from annarchy_b200.parser.text import ParserError
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "parser_strings.json")))
+
+
+def _cmp_vars(d, g):
+    assert len(d["variables"]) == len(g["variables"])
+    for v, gv in zip(d["variables"], g["variables"]):
+        for f in ("name", "cpp", "switch", "bounds", "init", "locality", "method"):
+            assert v.get(f) == gv.get(f), (v["name"], f)
+
+
+@pytest.mark.parametrize("key", sorted(NEURONS))
+def test_neuron_strings(key):
+    d = analyse_neuron(Neuron(**NEURONS[key]))
+    g = GOLD["neurons"][key]
+    _cmp_vars(d, g)
+    assert d["local"] == g["local"] and d["global"] == g["global"]
+    assert d["targets"] == g["targets"]
+    if "spike_cond" in g:
+        assert d["spike"]["spike_cond"] == g["spike_cond"]
+        assert [r["cpp"] for r in d["spike"]["spike_reset"]] == g["spike_reset"]
+    for p, gp in zip(d["parameters"], g["parameters"]):
+        assert (p["name"], p["init"], p["locality"]) == (gp["name"], gp["init"], gp["locality"])
+
+
+@pytest.mark.parametrize("key", sorted(SYNAPSES))
+def test_synapse_strings(key):
+    d = analyse_synapse(Synapse(**SYNAPSES[key]))
+    g = GOLD["synapses"][key]
+    _cmp_vars(d, g)
+    for f in ("pre_spike", "post_spike"):
+        if f in g:
+            assert [v["cpp"] for v in d[f]] == g[f]
+
+
+def test_rate_neuron_needs_r():
+    with pytest.raises(ParserError):
+        analyse_neuron(Neuron(parameters="tau = 10.0", equations="tau * dv/dt = -v"))
+
+
+def test_unsupported_constructs_rejected():
+    with pytest.raises(ParserError):
+        analyse_neuron(Neuron(equations="r = ite(v > 0, 1.0, 0.0)\n dv/dt = -v"))
+    with pytest.raises(ParserError):
+        analyse_neuron(Neuron(equations="r = mean(v)\n dv/dt = -v"))
