@@ -122,11 +122,16 @@ class Population:
             if name not in self._host:
                 raise AttributeError(f"population {self.name!r} has no attribute {name!r}")
             cur = self._host[name]
-            shape = cur.shape
-            arr = draw(value, shape, self._rng(), cur.dtype)
-            self._host[name] = arr
+            if self._compiled() and isinstance(value, np.ndarray) and value.size == cur.size:
+                # straight to the device: no host copy when the array already
+                # has the device dtype (e.g. a pinned buffer)
+                self.net._backend.write_population_attribute(self, name, value)
+                continue
+            arr = draw(value, cur.shape, self._rng(), cur.dtype)
             if self._compiled():
                 self.net._backend.write_population_attribute(self, name, arr)
+            else:
+                self._host[name] = arr
 
     def _set_ranks(self, name: str, ranks: np.ndarray, value):
         if self._locality.get(name) != "local":
