@@ -56,6 +56,7 @@ class CompiledNetwork:
         self.layout: dict[int, dict] = {}
         self.mon_layout: dict[int, dict] = {}
         self.local_layout = None
+        self._col_ptr: dict[int, np.ndarray] = {}
         self.engine = None
         self.module = None
 
@@ -78,6 +79,9 @@ class CompiledNetwork:
         self.engine = self._choose_engine()
         for mon in net.monitors:
             self._create_monitor(mon)
+        if self.engine == "local":
+            self._build_cluster()
+            return
         gen = CodeGenerator(self)
         if self.engine == "local":
             self._local_layout()
@@ -86,11 +90,45 @@ class CompiledNetwork:
             mod = gen.grid_module()
         self.module = mod
         nat.load_module(mod.source, mod.options)
-        if mod.engine == "local":
+        if mod.local is not None:
             nat.set_local_kernel(*mod.local)
         else:
             nat.plan(mod.plan)
             nat.set_graph_steps(int(net._config.get("graph_steps", 32)))
+
+    def _build_cluster(self):
+        """Fast spiking engine on one thread-block cluster: the smallest
+        cluster (up to 16 CTAs) whose shared memory holds the state and the
+        synapses; otherwise 8 CTAs with the synapses read from global memory.
+        A cluster the device cannot schedule falls back the same way."""
+        from ..runtime.lib import BackendError
+        want = self.net._config.get("cluster_size")
+        total = max(p.size for p in self.net.populations)
+        cands = [int(want)] if want else [c for c in (1, 2, 4, 8, 16) if (total + c - 1) // c <= 1024]
+        # weights in shared memory with the smallest cluster that holds them,
+        # else weights read from global memory
+        plans = [(c, True) for c in cands] + [(c, False) for c in reversed(cands)]
+        last_err = None
+        for C, in_smem in plans:
+            if self._cluster_layout(C, in_smem) > LOCAL_SMEM_LIMIT:
+                continue
+            for k, arrs in self._cl_arrays.items():
+                for name, arr in arrs.items():
+                    if name in ("cl_w", "cl_pal"):
+                        arr = arr if self.exact else self._w(arr)
+                    self.native.create(f"proj{k}__{name}", arr)
+            gen = CodeGenerator(self)
+            mod = gen.cluster_module()
+            try:
+                self.native.load_module(mod.source, mod.options)
+                self.native.set_local_kernel(*mod.local)
+            except BackendError as exc:
+                last_err = exc
+                continue
+            self.module = mod
+            self.engine = "cluster"
+            return
+        raise RuntimeError(f"no cluster configuration fits this network ({last_err})")
 
     def _choose_engine(self) -> str:
         want = self.net._config.get("engine", "auto")
@@ -157,6 +195,107 @@ class CompiledNetwork:
             pops[pop.id] = d
         self.local_layout = {"pops": pops, "smem": off, "block": 1024}
 
+    def _cluster_size(self) -> int:
+        """CTAs per cluster for the fast local engine: about 512 neurons per
+        CTA, at most 8 (the portable cluster size); the double-precision mode
+        keeps one CTA (its ordered delivery needs a single owner)."""
+        if self.exact:
+            return 1
+        want = self.net._config.get("cluster_size")
+        if want:
+            return int(want)
+        total = max(p.size for p in self.net.populations)
+        return int(max(1, min(8, (total + 511) // 512)))
+
+    def _cluster_layout(self, C: int, weights_in_smem: bool = True):
+        """Shared-memory layout of one CTA of a C-CTA cluster and the
+        per-CTA incoming-synapse arrays (see CodeGenerator.cluster_module).
+        Returns the bytes of shared memory per CTA."""
+        pops, projs = {}, {}
+        off = 0
+        rb = np.dtype(self.real).itemsize
+        rct = "double" if self.exact else "float"
+        a16 = lambda x: (x + 15) // 16 * 16
+        for pop in self.net.populations:
+            chunk = ((pop.size + C - 1) // C + 31) // 32 * 32
+            words = (pop.size + 31) // 32
+            d = {}
+            for name in self._local_vars(pop):
+                d[name] = (off, rct)
+                off += a16(chunk * rb)
+            d["refractory_remaining"] = (off, "int")
+            off += a16(chunk * 4)
+            if pop._has_refractory:
+                d["refractory"] = (off, "int")
+                off += a16(chunk * 4)
+            for par in (0, 1):
+                d[f"spk{par}"] = (off, "anb_u32")
+                off += a16(words * 4)
+            d["nzw"] = (off, "int")              # nonzero words of a bitmap + count
+            off += a16((words + 1) * 4)
+            pops[pop.id] = {"chunk": chunk, "arrays": d}
+        per_cta = np.zeros(C, dtype=np.int64)
+        self._cl_arrays = {}
+        for proj in self.net.projections:
+            lay = self.layout[proj.id]
+            span = (lay["w1"] - lay["w0"]) * 32
+            arrs = self._incoming_slices(proj, C, pops[proj.post_pop.id]["chunk"], lay["w0"] * 32,
+                                         span)
+            self._cl_arrays[proj.id] = arrs
+            per_cta += np.diff(arrs["cl_base"])
+            projs[proj.id] = {"span": span, "w_smem": weights_in_smem}
+            pops[proj.pre_pop.id]["arrays"][f"cp{proj.id}"] = (off, "int")
+            off += a16((span + 1) * 4)
+        pool = int(per_cta.max()) if per_cta.size else 0
+        wb = 8 if self.exact else (2 if self.wdtype is BF16 else 4)
+        wct = "double" if self.exact else ("anb_bf16" if self.wdtype is BF16 else "float")
+        # weight palettes: every projection with at most 256 distinct weights
+        # stores 1-byte indices into a per-projection table
+        pal = {k: np.unique(a["cl_w"]) for k, a in self._cl_arrays.items()}
+        use_pal = bool(pal) and all(v.size <= 256 for v in pal.values()) and wb > 1
+        pool_l = {"post": (off, "unsigned short"), "w": (None, wct), "palette": use_pal,
+                  "w_ct_real": wct}
+        off += a16(pool * 2)
+        if use_pal:
+            for k, v in pal.items():
+                arrs = self._cl_arrays[k]
+                arrs["cl_wi"] = np.searchsorted(v, arrs["cl_w"]).astype(np.uint8)
+                arrs["cl_pal"] = v
+                projs[k]["pal"] = (off, int(v.size))
+                off += a16(v.size * wb)
+            pool_l["w"] = (off, "unsigned char")
+            off += a16(pool)
+            for k in projs:
+                projs[k]["w_smem"] = True
+        elif weights_in_smem:
+            pool_l["w"] = (off, wct)
+            off += a16(pool * wb)
+        block = int(min(1024, max(128, max(l["chunk"] for l in pops.values()))))
+        self.cluster_layout = {"C": C, "block": block, "pops": pops, "proj": projs, "smem": off,
+                               "pool": pool_l}
+        return off
+
+    def _incoming_slices(self, proj, C, chunk_post, lo, span):
+        """Per owner CTA r (post neurons [r*chunk_post, (r+1)*chunk_post)),
+        the synapses of projection `proj` onto its neurons, sorted by pre rank
+        then post rank: cl_base[r] = first synapse of CTA r, cl_ptr[r] = its
+        local column pointers over pre ranks lo..lo+span, cl_post = post index
+        relative to the CTA, cl_w = weights."""
+        post_rank, row_ptr, cols, w = proj.csr_population_ranks()
+        rows_of = np.repeat(np.arange(post_rank.size), np.diff(row_ptr))
+        posts = post_rank[rows_of].astype(np.int64)
+        owner = posts // chunk_post
+        pre_rel = cols.astype(np.int64) - lo
+        order = np.lexsort((posts, pre_rel, owner))
+        counts = np.bincount(owner * span + pre_rel, minlength=C * span).reshape(C, span)
+        cl_ptr = np.zeros((C, span + 1), dtype=np.int32)
+        np.cumsum(counts, axis=1, out=cl_ptr[:, 1:])
+        cl_base = np.zeros(C + 1, dtype=np.int32)
+        np.cumsum(np.bincount(owner, minlength=C), out=cl_base[1:])
+        return {"cl_ptr": cl_ptr.reshape(-1), "cl_base": cl_base,
+                "cl_post": (posts - owner * chunk_post)[order].astype(np.uint16),
+                "cl_w": w[order]}
+
     def _create_population(self, pop):
         nat = self.native
         for name, arr in pop._host.items():
@@ -202,6 +341,7 @@ class CompiledNetwork:
             col_ptr = np.zeros(npre + 1, dtype=np.int32)
             np.cumsum(np.bincount(cols, minlength=npre), out=col_ptr[1:])
             nat.create(f"proj{k}__col_ptr", col_ptr)
+            self._col_ptr[k] = col_ptr
             nat.create(f"proj{k}__post_idx", post_rank[rows_of[order]].astype(np.int32))
             nat.create(f"proj{k}__inv_idx", order.astype(np.int32))
             if not proj.plastic:
@@ -350,6 +490,16 @@ def bitmap_to_spikes(buf: np.ndarray, n: int):
     then rank."""
     if buf.size == 0:
         return np.zeros(0, np.int64), np.zeros(0, np.int64)
-    bits = np.unpackbits(np.ascontiguousarray(buf).view(np.uint8), axis=1, bitorder="little")
-    s, r = np.nonzero(bits[:, :n])
-    return s.astype(np.int64), r.astype(np.int64)
+    from ..runtime.lib import bitmap_decode
+    return bitmap_decode(buf, n)
+
+
+def bitmap_to_spikes_numpy(buf: np.ndarray, n: int):
+    """Pure numpy version of bitmap_to_spikes (no native library needed)."""
+    step, word = np.nonzero(buf)                   # only words holding a spike
+    vals = np.ascontiguousarray(buf[step, word])
+    bits = np.unpackbits(vals.view(np.uint8).reshape(-1, 4), axis=1, bitorder="little")
+    k, b = np.nonzero(bits)
+    ranks = word[k].astype(np.int64) * 32 + b
+    keep = ranks < n
+    return step[k][keep].astype(np.int64), ranks[keep]

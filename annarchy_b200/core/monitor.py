@@ -89,8 +89,11 @@ class Monitor:
             return np.zeros(0, np.int64), np.zeros(0, np.int64)
         s = np.concatenate(self._spike_steps)
         r = np.concatenate(self._spike_ranks)
-        order = np.lexsort((r, s))
-        return s[order], r[order]
+        # chunks arrive in time order, each sorted by (step, rank)
+        if s.size > 1 and (np.any(np.diff(s) < 0)):
+            order = np.lexsort((r, s))
+            s, r = s[order], r[order]
+        return s, r
 
     def get(self, variables=None, keep: bool = False, reshape: bool = False,
             force_dict: bool = False):
@@ -103,16 +106,14 @@ class Monitor:
         for v in variables:
             if v == "spike":
                 s, r = self.spike_arrays()
-                ranks = self.ranks if self.ranks is not None else np.arange(self.population.size)
-                d = {int(k): [] for k in ranks}
-                if s.size:
-                    sel = np.isin(r, ranks)
-                    s, r = s[sel], r[sel]
-                    order = np.argsort(r, kind="stable")
-                    s, r = s[order], r[order]
-                    bounds = np.flatnonzero(np.diff(r)) + 1
-                    for ss, rr in zip(np.split(s, bounds), np.split(r, bounds)):
-                        d[int(rr[0])] = ss.astype(np.int64).tolist()
+                size = self.population.size
+                order = np.argsort(r, kind="stable")       # by rank, steps stay ascending
+                counts = np.bincount(r, minlength=size)
+                chunks = np.split(s[order], np.cumsum(counts)[:-1])
+                if self.ranks is None:
+                    d = dict(zip(range(size), (c.tolist() for c in chunks)))
+                else:
+                    d = {int(k): chunks[int(k)].tolist() for k in self.ranks}
                 out[v] = d
                 if not keep:
                     self._spike_steps, self._spike_ranks = [], []

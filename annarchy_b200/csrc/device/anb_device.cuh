@@ -229,6 +229,43 @@ __device__ __forceinline__ void anb_spike_scatter(int w0, int w1, const anb_u32*
   }
 }
 
+// ---- thread-block clusters (distributed shared memory) ----------------------------------
+// The cluster engine splits a network's neurons over the CTAs of one
+// cluster; spikes are delivered into the owning CTA's shared memory with
+// DSMEM reductions and the CTAs meet at one hardware cluster barrier per
+// step (no spin loop).
+
+__device__ __forceinline__ unsigned anb_cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ unsigned anb_smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// Address of the same shared-memory offset in CTA `rank` of the cluster.
+__device__ __forceinline__ unsigned anb_cluster_map(unsigned addr, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void anb_cluster_red_add(unsigned addr, float v) {
+  asm volatile("red.relaxed.cluster.shared::cluster.add.f32 [%0], %1;" ::"r"(addr), "f"(v)
+               : "memory");
+}
+
+__device__ __forceinline__ void anb_cluster_st_u32(unsigned addr, anb_u32 v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void anb_cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+
 // ---- monitors ---------------------------------------------------------------------------
 
 // Copy n values (converted to double) into slot `slot` of a ring of `cap` slots.

@@ -43,6 +43,8 @@ struct Driver {
   decltype(&cuLaunchKernel) launchKernel = nullptr;
   decltype(&cuFuncSetAttribute) funcSetAttribute = nullptr;
   decltype(&cuGetErrorString) getErrorString = nullptr;
+  decltype(&cuLaunchKernelEx) launchKernelEx = nullptr;
+  decltype(&cuOccupancyMaxActiveClusters) maxActiveClusters = nullptr;
 };
 Driver g_drv;
 
@@ -65,7 +67,9 @@ bool load_driver() {
             entry("cuModuleGetGlobal", &g_drv.moduleGetGlobal) &&
             entry("cuLaunchKernel", &g_drv.launchKernel) &&
             entry("cuFuncSetAttribute", &g_drv.funcSetAttribute) &&
-            entry("cuGetErrorString", &g_drv.getErrorString);
+            entry("cuGetErrorString", &g_drv.getErrorString) &&
+            entry("cuLaunchKernelEx", &g_drv.launchKernelEx) &&
+            entry("cuOccupancyMaxActiveClusters", &g_drv.maxActiveClusters);
   g_drv.loaded = ok;
   return ok;
 }
@@ -101,6 +105,7 @@ struct Launch {
   std::string name;
   CUfunction fn = nullptr;
   unsigned grid = 1, block = 1, smem = 0;
+  unsigned cluster = 1;  // CTAs per thread-block cluster (launch attribute)
 };
 
 struct TimedLaunch {
@@ -177,8 +182,30 @@ int bind(anb_net* net) {
 }
 
 int launch(anb_net* net, const Launch& l, void** params) {
-  ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem, (CUstream)net->stream,
-                        params, nullptr));
+  if (l.cluster <= 1) {
+    ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem, (CUstream)net->stream,
+                              params, nullptr));
+    return ANB_OK;
+  }
+  CUlaunchAttribute attr;
+  std::memset(&attr, 0, sizeof(attr));
+  attr.id = CU_LAUNCH_ATTRIBUTE_CLUSTER_DIMENSION;
+  attr.value.clusterDim.x = l.cluster;
+  attr.value.clusterDim.y = 1;
+  attr.value.clusterDim.z = 1;
+  CUlaunchConfig cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDimX = l.grid;
+  cfg.gridDimY = 1;
+  cfg.gridDimZ = 1;
+  cfg.blockDimX = l.block;
+  cfg.blockDimY = 1;
+  cfg.blockDimZ = 1;
+  cfg.sharedMemBytes = l.smem;
+  cfg.hStream = (CUstream)net->stream;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  ANB_CU(g_drv.launchKernelEx(&cfg, l.fn, params, nullptr));
   return ANB_OK;
 }
 
@@ -531,6 +558,29 @@ int anb_nvrtc_compile(const char* source, const char* options, char* log, size_t
   return ANB_OK;
 }
 
+int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
+                          int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity) {
+  int64_t k = 0;
+  for (int64_t s = 0; s < steps; ++s) {
+    const uint32_t* row = words + s * words_per_step;
+    for (int64_t w = 0; w < words_per_step; ++w) {
+      uint32_t m = row[w];
+      while (m) {
+        const int b = __builtin_ctz(m);
+        m &= m - 1;
+        const int64_t rank = w * 32 + b;
+        if (rank >= n) continue;
+        if (k < capacity) {
+          out_steps[k] = s;
+          out_ranks[k] = rank;
+        }
+        ++k;
+      }
+    }
+  }
+  return k;
+}
+
 int anb_plan_clear(anb_net* net) {
   if (!net) return fail(ANB_ERR_ARG, "net is NULL");
   drop_graph(net);
@@ -571,6 +621,46 @@ int anb_set_local_kernel(anb_net* net, const char* kernel, unsigned grid, unsign
   Launch l;
   int rc = resolve(net, kernel, grid, block, shared_bytes, &l);
   if (rc) return rc;
+  net->local = l;
+  net->has_local = true;
+  return ANB_OK;
+}
+
+int anb_set_local_kernel_ex(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                            unsigned shared_bytes, unsigned cluster) {
+  if (cluster == 0 || cluster > 16 || grid % cluster != 0)
+    return fail(ANB_ERR_ARG, "cluster size must divide the grid and be at most 16");
+  Launch l;
+  int rc = resolve(net, kernel, grid, block, shared_bytes, &l);
+  if (rc) return rc;
+  l.cluster = cluster;
+  if (cluster > 1) {
+    if (cluster > 8)
+      ANB_CU(g_drv.funcSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_NON_PORTABLE_CLUSTER_SIZE_ALLOWED, 1));
+    CUlaunchAttribute attr;
+    std::memset(&attr, 0, sizeof(attr));
+    attr.id = CU_LAUNCH_ATTRIBUTE_CLUSTER_DIMENSION;
+    attr.value.clusterDim.x = cluster;
+    attr.value.clusterDim.y = 1;
+    attr.value.clusterDim.z = 1;
+    CUlaunchConfig cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDimX = grid;
+    cfg.gridDimY = 1;
+    cfg.gridDimZ = 1;
+    cfg.blockDimX = block;
+    cfg.blockDimY = 1;
+    cfg.blockDimZ = 1;
+    cfg.sharedMemBytes = shared_bytes;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    ANB_CU(g_drv.maxActiveClusters(&clusters, l.fn, &cfg));
+    if (clusters < 1)
+      return fail(ANB_ERR_ARG, "a cluster of " + std::to_string(cluster) + " CTAs with " +
+                                   std::to_string(shared_bytes) +
+                                   " bytes of shared memory each cannot be scheduled");
+  }
   net->local = l;
   net->has_local = true;
   return ANB_OK;

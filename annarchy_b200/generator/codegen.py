@@ -47,7 +47,8 @@ MAX_GRID = 148 * 16
 
 CTYPE_OF = {np.dtype(np.float64): "double", np.dtype(np.float32): "float",
             np.dtype(np.int32): "int", np.dtype(np.int64): "long long",
-            np.dtype(np.uint32): "anb_u32", np.dtype(np.uint16): "anb_bf16"}
+            np.dtype(np.uint32): "anb_u32", np.dtype(np.uint16): "anb_bf16",
+            np.dtype(np.uint8): "unsigned char"}
 
 
 def grid_for(n: int, block: int = BLOCK) -> int:
@@ -153,12 +154,29 @@ class CodeGenerator:
                     modified.append(v["name"])
         return "\n".join(lines), modified
 
+    def _reciprocals(self, pop):
+        """Global real parameters used as divisors: in fast mode their
+        reciprocal is computed once and the division becomes a multiply."""
+        if self.exact:
+            return []
+        names = [p["name"] for p in pop.desc["parameters"]
+                 if p["locality"] == "global" and p.get("ctype") not in ("int", "bool")]
+        code = " ".join(v.get("cpp", "") or "" for v in pop.desc["variables"])
+        return [n for n in names if re.search(r"/" + re.escape(n) + r"(?![\w\[])", code)]
+
+    def _use_reciprocals(self, pop, code: str) -> str:
+        for n in self._reciprocals(pop):
+            code = re.sub(r"/" + re.escape(n) + r"(?![\w\[])", "*anb_inv_" + n, code)
+        return code
+
     def _globals_preamble(self, pop, src) -> str:
         out = []
         for p in pop.desc["parameters"] + pop.desc["variables"]:
             if p["locality"] == "global":
                 ct = "int" if p.get("ctype") in ("int", "bool") else self.real
                 out.append(f"const {ct} {p['name']} = {src(p['name'])}[0];")
+        for n in self._reciprocals(pop):
+            out.append(f"const {self.real} anb_inv_{n} = ({self.real})1 / {n};")
         for v in pop.desc["variables"]:
             pl = v.get("pre_loop") or {}
             if pl:
@@ -169,11 +187,18 @@ class CodeGenerator:
         return [p["name"] for p in pop.desc["parameters"] + pop.desc["variables"]
                 if p["locality"] == "local"]
 
-    def neuron_update(self, pop, *, local_engine=False, smem=None) -> str:
-        """Update (+ spike gather) of one population for step t."""
+    def neuron_update(self, pop, *, local_engine=False, smem=None, cluster=None) -> str:
+        """Update (+ spike gather) of one population for step t.
+
+        grid: grid-stride over all neurons, state in global memory; local:
+        one CTA over all neurons, state in shared memory (`smem`); cluster:
+        this CTA's slice [anb_base, anb_base + anb_cnt), shared-memory state
+        indexed by the local index anb_q and the conductance increments of
+        the step (`cluster` = {target: increment buffer}) added first."""
         spiking = pop.neuron_type.type == "spike"
         masked = spiking and pop._has_refractory
         body, modified = self._neuron_body(pop, None, masked)
+        body = self._use_reciprocals(pop, body)
         names = self._locals(pop)
         k = pop.id
 
@@ -181,13 +206,19 @@ class CodeGenerator:
             return self.ptr(f"pop{k}__{name}")
 
         loads, stores = [], []
+        sidx = "anb_q" if cluster is not None else "anb_i"
         for name in names:
             ct = "int" if pop._ctype.get(name) in ("int", "bool") else self.real
-            src = smem[name] if (smem and name in smem) else gsrc(name)
-            loads.append(f"{ct} {name} = {src}[anb_i];")
+            on_chip = bool(smem and name in smem)
+            src = smem[name] if on_chip else gsrc(name)
+            idx = sidx if on_chip else "anb_i"
+            loads.append(f"{ct} {name} = {src}[{idx}];")
             if name in modified or (spiking and any(r["name"] == name for r in
                                                     pop.desc["spike"]["spike_reset"])):
-                stores.append(f"{src}[anb_i] = {name};")
+                stores.append(f"{src}[{idx}] = {name};")
+        if cluster is not None:
+            for target, dg in cluster.items():
+                loads.append(f"g_{target} += {dg}[anb_q]; {dg}[anb_q] = 0.f;")
         if pop.neuron_type.type == "rate":
             for t in pop.targets:
                 src = gsrc("_sum_" + t)
@@ -196,16 +227,20 @@ class CodeGenerator:
         spike_code = ""
         if spiking:
             rr_src = smem["refractory_remaining"] if smem else gsrc("refractory_remaining")
+            rr_idx = sidx if smem else "anb_i"
             cond = self.typed(self.fill(pop.desc["spike"]["spike_cond"]))
             resets = "\n          ".join(self.typed(self.fill(r["cpp"]))
                                          for r in pop.desc["spike"]["spike_reset"])
             if masked:
-                loads.append(f"int refractory_remaining = {rr_src}[anb_i];")
+                loads.append(f"int refractory_remaining = {rr_src}[{rr_idx}];")
                 loads.append("const int in_ref = (refractory_remaining > 0) ? 0 : 1;")
                 refr_dec = "refractory_remaining -= (1 - in_ref);"
                 guard = f"(in_ref != 0) && ({cond})"
-                refr_set = f"refractory_remaining = {gsrc('refractory')}[anb_i];"
-                stores.append(f"{rr_src}[anb_i] = refractory_remaining;")
+                if smem and "refractory" in smem:
+                    refr_set = f"refractory_remaining = {smem['refractory']}[{rr_idx}];"
+                else:
+                    refr_set = f"refractory_remaining = {gsrc('refractory')}[anb_i];"
+                stores.append(f"{rr_src}[{rr_idx}] = refractory_remaining;")
             else:
                 refr_dec, guard, refr_set = "", f"({cond})", ""
             spike_code = f"""{refr_dec}
@@ -218,17 +253,36 @@ class CodeGenerator:
         spk_dst = (smem["spk"] if smem else gsrc("spk")) if spiking else None
         ballot = ""
         if spiking:
+            widx, lim = ("anb_q", "anb_cnt") if cluster is not None else ("anb_i", "anb_n")
             ballot = f"""
       {{
         const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
-        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {spk_dst}[anb_i >> 5] = anb_m;
+        if ((threadIdx.x & 31) == 0 && {widx} < {lim}) {spk_dst}[{widx} >> 5] = anb_m;
       }}"""
+        nl = "\n        "
+        if cluster is not None:
+            k = pop.id
+            return f"""
+    {{  // population {pop.name}: this CTA's slice
+      const int anb_n = {pop.size};
+      const int anb_base = anb_base{k}, anb_cnt = anb_cnt{k};
+      for (int anb_q0 = 0; anb_q0 < anb_cnt; anb_q0 += blockDim.x) {{
+        const int anb_q = anb_q0 + threadIdx.x;
+        const int anb_i = anb_base + anb_q;
+        bool anb_spiked = false;
+        if (anb_q < anb_cnt) {{
+        {nl.join(loads)}
+        {body.replace(chr(10), nl)}
+        {spike_code}
+        {nl.join(stores)}
+        }}{ballot}
+      }}
+    }}"""
         if local_engine:
             loop = "for (int anb_base = 0; anb_base < anb_n; anb_base += blockDim.x)"
         else:
             loop = ("for (int anb_base = blockIdx.x * blockDim.x; anb_base < anb_n; "
                     "anb_base += gridDim.x * blockDim.x)")
-        nl = "\n        "
         return f"""
     {{  // population {pop.name}: update{' and spike gather' if spiking else ''}
       const int anb_n = {pop.size};
@@ -653,6 +707,238 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
 """
         return Module(self.assemble([src]), self.options(), "local",
                       local=("anb_local_run", 1, block, layout["smem"]), kernels=["anb_local_run"])
+
+    def cluster_module(self) -> Module:
+        """Spiking networks on the CTAs of one thread-block cluster.
+
+        CTA r owns the neurons [r*chunk, (r+1)*chunk) of every population
+        (chunk a multiple of 32) with their state in its shared memory, and
+        the incoming synapses of those neurons (pre-major, per projection).
+        Every CTA keeps a replica of each population's spike bitmap, double
+        buffered by step parity. A step s:
+
+          1. deliver the spikes of step s-1 (replica of parity (s-1)&1) into
+             the own neurons' conductances: fast mode with shared-memory
+             atomics, exact mode spike by spike in ascending pre rank with a
+             CTA barrier after each, which is the reference's per-post order;
+          2. update the own neurons and write the own bitmap words into the
+             local replica of parity s&1 and into every other CTA's (DSMEM
+             stores);
+          3. one cluster barrier.
+
+        Step s+1 writes the other replica, so the barrier of step s is the
+        only one: nobody still reads a replica when it is overwritten."""
+        net = self.net
+        lay = self.c.cluster_layout
+        C, block = lay["C"], lay["block"]
+        carve, load, store = [], [], []
+        smem_ptrs: dict[int, dict] = {}
+        ranges = []
+        for pop in net.populations:
+            pl = lay["pops"][pop.id]
+            chunk = pl["chunk"]
+            k = pop.id
+            d = {}
+            for name, (off, ct) in pl["arrays"].items():
+                carve.append(f"{ct}* __restrict__ anb_s_pop{k}_{name} = "
+                             f"reinterpret_cast<{ct}*>(anb_smem + {off});")
+                d[name] = f"anb_s_pop{k}_{name}"
+            smem_ptrs[k] = d
+            words = (pop.size + 31) // 32
+            ranges.append(f"const int anb_base{k} = (int)anb_rank * {chunk};")
+            ranges.append(f"const int anb_cnt{k} = max(0, min({pop.size}, anb_base{k} + {chunk}) - anb_base{k});")
+            ranges.append(f"const int anb_words{k} = (anb_cnt{k} + 31) >> 5;")
+            for name in pl["arrays"]:
+                s_ = d[name]
+                if name.startswith(("spk", "cp", "nzw")):
+                    continue
+                g = self.ptr(f"pop{k}__{name}")
+                load.append(f"for (int q = threadIdx.x; q < anb_cnt{k}; q += blockDim.x) {s_}[q] = {g}[anb_base{k} + q];")
+                if name != "refractory":
+                    store.append(f"for (int q = threadIdx.x; q < anb_cnt{k}; q += blockDim.x) {g}[anb_base{k} + q] = {s_}[q];")
+            gspk = self.ptr(f"pop{k}__spk")
+            # spikes of the step before the launch go to the replica of parity 1
+            load.append(f"for (int q = threadIdx.x; q < {words}; q += blockDim.x) {{ {d['spk1']}[q] = {gspk}[q]; {d['spk0']}[q] = 0u; }}")
+            store.append(f"for (int q = threadIdx.x; q < anb_words{k}; q += blockDim.x) "
+                         f"{gspk}[(anb_base{k} >> 5) + q] = (nsteps & 1 ? {d['spk0']} : {d['spk1']})[(anb_base{k} >> 5) + q];")
+        prop = []
+        scans = []
+        for pop in net.populations:
+            if not any(pr.pre_pop is pop for pr in net.projections):
+                continue
+            k = pop.id
+            d = smem_ptrs[k]
+            words = (pop.size + 31) // 32
+            # warp 0 lists the nonzero words of the previous step's bitmap, in order
+            scans.append(f"""
+      if (anb_warp == 0) {{
+        const anb_u32* __restrict__ anb_spk = (anb_par ? {d['spk0']} : {d['spk1']});
+        int anb_cnt = 0;
+        for (int c = 0; c < {words}; c += 32) {{
+          const anb_u32 w = (c + anb_lane < {words}) ? anb_spk[c + anb_lane] : 0u;
+          const anb_u32 nz = __ballot_sync(0xffffffffu, w != 0u);
+          if (w != 0u) {d['nzw']}[anb_cnt + __popc(nz & ((1u << anb_lane) - 1u))] = c + anb_lane;
+          anb_cnt += __popc(nz);
+        }}
+        if (anb_lane == 0) {d['nzw']}[{words}] = anb_cnt;
+      }}""")
+        for proj in net.projections:
+            a, b = proj.pre_pop.id, proj.post_pop.id
+            play = self.c.layout[proj.id]
+            cl = lay["proj"][proj.id]
+            k = proj.id
+            p = lambda n, kk=k: self.ptr(f"proj{kk}__{n}")
+            lo = play["w0"] * 32
+            cp = smem_ptrs[a][f"cp{k}"]
+            g = smem_ptrs[b]["g_" + proj.target]
+            # this CTA's incoming synapses of projection k, appended to the pool
+            palette = lay["pool"].get("palette")
+            w_src = "anb_s_pool_w" if cl["w_smem"] else p("cl_w")
+            w_idx = "q" if cl["w_smem"] else "anb_gbase{k} + q - anb_poff{k}".format(k=k)
+            pool_w_src = p("cl_wi") if palette else p("cl_w")
+            if palette:
+                poff, npal = cl["pal"]
+                wct = lay["pool"]["w_ct_real"]
+                carve.append(f"{wct}* __restrict__ anb_s_pal{k} = reinterpret_cast<{wct}*>(anb_smem + {poff});")
+                load.append(f"for (int q = threadIdx.x; q < {npal}; q += blockDim.x) anb_s_pal{k}[q] = {p('cl_pal')}[q];")
+                w_src, w_idx = f"anb_s_pal{k}", "anb_s_pool_w[q]"
+            load.append(f"""const int anb_gbase{k} = {p('cl_base')}[anb_rank];
+    const int anb_poff{k} = anb_pool_off;
+    {{
+      const int anb_n = {p('cl_base')}[anb_rank + 1] - anb_gbase{k};
+      for (int q = threadIdx.x; q <= {cl['span']}; q += blockDim.x)
+        {cp}[q] = anb_pool_off + {p('cl_ptr')}[anb_rank * {cl['span'] + 1} + q];
+      for (int q = threadIdx.x; q < anb_n; q += blockDim.x) {{
+        anb_s_pool_post[anb_pool_off + q] = {p('cl_post')}[anb_gbase{k} + q];
+        {"anb_s_pool_w[anb_pool_off + q] = " + pool_w_src + "[anb_gbase" + str(k) + " + q];" if cl["w_smem"] else ""}
+      }}
+      anb_pool_off += anb_n;
+    }}""")
+            spk = f"(anb_par ? {smem_ptrs[a]['spk0']} : {smem_ptrs[a]['spk1']})"
+            nzw = smem_ptrs[a]["nzw"]
+            nwords = (proj.pre_pop.size + 31) // 32
+            if self.exact:
+                prop.append(f"""
+      {{  // {proj.name}: spikes in ascending pre rank, one CTA barrier per spike
+        const anb_u32* __restrict__ anb_spk = {spk};
+        const int anb_nz = {nzw}[{nwords}];
+        for (int i = 0; i < anb_nz; ++i) {{
+          const int word = {nzw}[i];
+          if (word < {play['w0']} || word >= {play['w1']}) continue;
+          anb_u32 m = anb_spk[word];
+          while (m) {{
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int pre = (word << 5) + b - {lo};
+            const int beg = {cp}[pre], end = {cp}[pre + 1];
+            if (end > beg) {{
+              for (int q = beg + threadIdx.x; q < end; q += blockDim.x)
+                {g}[anb_s_pool_post[q]] += {w_src}[{w_idx}];
+              __syncthreads();
+            }}
+          }}
+        }}
+      }}""")
+            else:
+                prop.append(f"""
+      {{  // {proj.name}: warp per nonzero bitmap word, shared-memory atomics
+        const anb_u32* __restrict__ anb_spk = {spk};
+        const int anb_nz = {nzw}[{nwords}];
+        for (int i = anb_warp; i < anb_nz; i += anb_nwarps) {{
+          const int word = {nzw}[i];
+          if (word < {play['w0']} || word >= {play['w1']}) continue;
+          anb_u32 m = anb_spk[word];
+          while (m) {{
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int pre = (word << 5) + b - {lo};
+            const int beg = {cp}[pre], end = {cp}[pre + 1];
+            for (int q = beg + anb_lane; q < end; q += 32)
+              atomicAdd(&{g}[anb_s_pool_post[q]], anb_wf({w_src}[{w_idx}]));
+          }}
+        }}
+      }}""")
+        updates, globals_, bcast = [], [], []
+        for pop in net.populations:
+            k = pop.id
+            globals_.append(self._globals_preamble(pop, lambda n, kk=k: self.ptr(f"pop{kk}__{n}")))
+            d = dict(smem_ptrs[k])
+            d["spk"] = f"((anb_par ? {d['spk1']} : {d['spk0']}) + (anb_base{k} >> 5))"
+            updates.append(self.neuron_update(pop, local_engine=True, smem=d, cluster={}))
+            bcast.append(f"""
+      {{  // own bitmap words of {pop.name} -> the other CTAs' replicas
+        anb_u32* __restrict__ anb_own = (anb_par ? {d['spk1']} : {d['spk0']}) + (anb_base{k} >> 5);
+        const unsigned anb_addr = anb_smem_addr(anb_own);
+        for (int q = threadIdx.x; q < {C} * anb_words{k}; q += blockDim.x) {{
+          const unsigned r = (unsigned)(q / anb_words{k});
+          const int w = q - (int)r * anb_words{k};
+          if (r != anb_rank) anb_cluster_st_u32(anb_cluster_map(anb_addr + 4u * w, r), anb_own[w]);
+        }}
+      }}""")
+        recs = []
+        for mon in net.monitors:
+            ml = self.c.mon_layout[mon.id]
+            m, k = mon.id, mon.population.id
+            d = smem_ptrs[k]
+            recs.append(f"""
+      if (anb_mon_on{m}) {{
+        const long long anb_slot = t - anb_mon_t0{m};
+        const anb_u32* __restrict__ anb_own = (anb_par ? {d['spk1']} : {d['spk0']}) + (anb_base{k} >> 5);
+        if (anb_slot >= 0 && anb_slot < {ml['cap_spike']}) {{
+          anb_u32* anb_dst = {self.ptr(f'mon{m}__spk')} + anb_slot * {ml['words']} + (anb_base{k} >> 5);
+          for (int q = threadIdx.x; q < anb_words{k}; q += blockDim.x) anb_dst[q] = anb_own[q];
+        }} else if (threadIdx.x == 0) {{
+          anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+        }}
+      }}""")
+        mon_pre = "\n    ".join(
+            f"const int anb_mon_on{mon.id} = {self.ptr(f'mon{mon.id}__on')}[0];\n    "
+            f"const long long anb_mon_t0{mon.id} = {self.ptr(f'mon{mon.id}__t0')}[0];"
+            for mon in net.monitors)
+        (poff, pct), (woff, wct) = lay["pool"]["post"], lay["pool"]["w"]
+        pool_carve = f"{pct}* __restrict__ anb_s_pool_post = reinterpret_cast<{pct}*>(anb_smem + {poff});"
+        if woff is not None:
+            pool_carve += f"\n    {wct}* __restrict__ anb_s_pool_w = reinterpret_cast<{wct}*>(anb_smem + {woff});"
+        dt_t = "double" if self.exact else "float"
+        nl = "\n    "
+        src = f"""
+extern "C" __global__ void __launch_bounds__({block}, 1)
+anb_cluster_run(long long t0, int nsteps) {{
+    extern __shared__ __align__(16) unsigned char anb_smem[];
+    const unsigned anb_rank = anb_cluster_rank();
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    const int anb_lane = threadIdx.x & 31;
+    const int anb_warp = threadIdx.x >> 5;
+    const int anb_nwarps = blockDim.x >> 5;
+    (void)anb_lane; (void)anb_warp; (void)anb_nwarps;
+    {nl.join(carve)}
+    {pool_carve}
+    {nl.join(ranges)}
+    {nl.join(g for g in globals_ if g)}
+    {mon_pre}
+    int anb_pool_off = 0;
+    {nl.join(load)}
+    (void)anb_pool_off;
+    anb_cluster_sync();
+    for (int anb_s = 0; anb_s < nsteps; ++anb_s) {{
+      const long long t = t0 + anb_s;
+      const int anb_par = anb_s & 1;
+      {''.join(scans)}
+      __syncthreads();
+      {''.join(prop)}
+      __syncthreads();
+      {''.join(updates)}
+      __syncthreads();
+      {''.join(bcast)}
+      {''.join(recs)}
+      anb_cluster_sync();
+    }}
+    {nl.join(store)}
+    if (anb_rank == 0 && threadIdx.x == 0) *{self.ptr('t')} = t0 + nsteps;
+}}
+"""
+        return Module(self.assemble([src]), self.options(), "cluster",
+                      local=("anb_cluster_run", C, block, lay["smem"], C), kernels=["anb_cluster_run"])
 
     # ------------------------------------------------------------------ output
     def options(self) -> list:

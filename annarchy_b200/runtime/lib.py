@@ -39,9 +39,13 @@ SIGNATURES = {
     "anb_module_load": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
+    "anb_bitmap_decode": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p,
+                                      C.c_void_p, C.c_int64]),
     "anb_plan_clear": (C.c_int, [C.c_void_p]),
     "anb_plan_add": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint]),
     "anb_set_local_kernel": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint]),
+    "anb_set_local_kernel_ex": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint,
+                                          C.c_uint]),
     "anb_set_graph_steps": (C.c_int, [C.c_void_p, C.c_int]),
     "anb_run": (C.c_int, [C.c_void_p, C.c_int64]),
     "anb_step": (C.c_int, [C.c_void_p]),
@@ -106,6 +110,22 @@ def nvrtc_compile(source: str, options: list[str]) -> tuple[int, str]:
     check("anb_nvrtc_compile", load().anb_nvrtc_compile(source.encode(), "\n".join(options).encode(),
                                                         log, len(log), C.byref(n)))
     return n.value, log.value.decode(errors="replace")
+
+
+def bitmap_decode(buf: np.ndarray, n: int):
+    """(steps, words) uint32 spike bitmaps -> (step, rank) int64 arrays."""
+    buf = np.ascontiguousarray(buf, dtype=np.uint32)
+    steps, words = buf.shape
+    lib = load()
+    cap = int(min(buf.size * 32, max(1024, np.count_nonzero(buf) * 4)))
+    while True:
+        s = np.empty(cap, dtype=np.int64)
+        r = np.empty(cap, dtype=np.int64)
+        k = lib.anb_bitmap_decode(buf.ctypes.data_as(C.c_void_p), steps, words, n,
+                                  s.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p), cap)
+        if k <= cap:
+            return s[:k], r[:k]
+        cap = int(k)
 
 
 class NativeNet:
@@ -203,9 +223,13 @@ class NativeNet:
         for name, grid, block, smem in launches:
             check("anb_plan_add", self.lib.anb_plan_add(self.h, name.encode(), grid, block, smem))
 
-    def set_local_kernel(self, name, grid, block, smem):
-        check("anb_set_local_kernel", self.lib.anb_set_local_kernel(self.h, name.encode(), grid,
-                                                                   block, smem))
+    def set_local_kernel(self, name, grid, block, smem, cluster: int = 1):
+        if cluster > 1:
+            check("anb_set_local_kernel_ex", self.lib.anb_set_local_kernel_ex(
+                self.h, name.encode(), grid, block, smem, cluster))
+        else:
+            check("anb_set_local_kernel", self.lib.anb_set_local_kernel(self.h, name.encode(),
+                                                                       grid, block, smem))
 
     def set_graph_steps(self, steps: int):
         check("anb_set_graph_steps", self.lib.anb_set_graph_steps(self.h, steps))

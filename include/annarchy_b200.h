@@ -114,6 +114,12 @@ int anb_plan_add(anb_net* net, const char* kernel, unsigned grid, unsigned block
 int anb_set_local_kernel(anb_net* net, const char* kernel, unsigned grid, unsigned block,
                          unsigned shared_bytes);
 
+/* Same, launched as thread-block clusters of `cluster` CTAs (1..16; sizes
+ * above 8 are non-portable). Fails with ANB_ERR_ARG if such a cluster with
+ * this much shared memory cannot be scheduled on the device. */
+int anb_set_local_kernel_ex(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                            unsigned shared_bytes, unsigned cluster);
+
 /* Steps per captured CUDA graph in the grid engine (0 = no graph). */
 int anb_set_graph_steps(anb_net* net, int steps);
 
@@ -129,6 +135,15 @@ int anb_synchronize(anb_net* net);
  * gave up or an index check failed; anb_clear_device_error resets it. */
 int anb_device_error(anb_net* net, int* code);
 int anb_clear_device_error(anb_net* net);
+
+/* ---- monitors ------------------------------------------------------------
+ * Decode recorded spike bitmaps (steps x words_per_step words, bit b of word
+ * w = neuron 32*w+b) into (step, rank) pairs sorted by step then rank; the
+ * host side of the reference's spike recorder (recording_spike_tpl in
+ * ANNarchy/generator/Monitor/BaseTemplates.py). Writes at most `capacity`
+ * pairs and returns the total number of spikes. Host memory only. */
+int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
+                          int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity);
 
 /* ---- per-kernel timing (CUDA events around every launch; no graphs) ----- */
 int anb_kernel_timing(anb_net* net, int enable);

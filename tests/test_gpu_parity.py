@@ -83,7 +83,7 @@ def test_coba_small_exact(golden, engine):
     g = golden("coba_small")
     cn = wl.coba_net(seed=7, n=400, p=0.05, steps=2000)
     out = run_coba(cn, 2000, engine=engine)
-    assert out["engine"] == engine
+    assert out["engine"] == {"grid": "grid", "local": "cluster"}[engine]
     assert np.array_equal(out["steps"], g["spike_steps"])
     assert np.array_equal(out["idx"], g["spike_idx"])
     for k in ("v", "g_exc", "g_inh"):
