@@ -98,9 +98,20 @@ class CodeGenerator:
                        "post_prefix": post_prefix, "post_index": post_index}
 
     # --------------------------------------------------------------- neurons
+    def compensated(self, pop) -> list:
+        """ODE variables whose explicit-Euler switch is Kahan-compensated
+        (single precision only): the rounding error of every `x += dt*_x`
+        is carried in anb_kc_x and added back at the next step."""
+        if self.exact or not self.c.net._config.get("compensate", True):
+            return []
+        return [v["name"] for v in pop.desc["variables"]
+                if v.get("switch") and v.get("method") != "event-driven"
+                and v["name"] in pop.desc["local"]]
+
     def _neuron_body(self, pop, src_of, masked: bool) -> tuple[str, list]:
         """Statements updating one neuron; locals are C variables named after
         the attributes. Returns (code, names of modified attributes)."""
+        comp = set(self.compensated(pop))
         desc = pop.desc
         local = set(desc["local"])
         blocks = []
@@ -141,6 +152,12 @@ class CodeGenerator:
                     sw = self.fill(v["switch"])
                     if masked and not v["name"].startswith("g_"):
                         sw = sw.replace(";", "* in_ref;")
+                    if v["name"] in comp:
+                        x = v["name"]
+                        inc = sw.split("+=", 1)[1].strip().rstrip(";")
+                        sw = (f"{{ const {self.real} anb_y = ({inc}) - anb_kc_{x}; "
+                              f"const {self.real} anb_tx = {x} + anb_y; "
+                              f"anb_kc_{x} = (anb_tx - {x}) - anb_y; {x} = anb_tx; }}")
                     lines.append(sw)
                     lines += [self.typed(b) for b in bounds(v)]
                     modified.append(v["name"])
@@ -187,7 +204,8 @@ class CodeGenerator:
         return [p["name"] for p in pop.desc["parameters"] + pop.desc["variables"]
                 if p["locality"] == "local"]
 
-    def neuron_update(self, pop, *, local_engine=False, smem=None, cluster=None) -> str:
+    def neuron_update(self, pop, *, local_engine=False, smem=None, cluster=None,
+                      ballot_hook=None) -> str:
         """Update (+ spike gather) of one population for step t.
 
         grid: grid-stride over all neurons, state in global memory; local:
@@ -219,6 +237,13 @@ class CodeGenerator:
         if cluster is not None:
             for target, dg in cluster.items():
                 loads.append(f"g_{target} += {dg}[anb_q]; {dg}[anb_q] = 0.f;")
+        comp = self.compensated(pop)
+        for x in comp:
+            on_chip = bool(smem and ("kc_" + x) in smem)
+            src = smem["kc_" + x] if on_chip else gsrc("kc_" + x)
+            idx = sidx if on_chip else "anb_i"
+            loads.append(f"{self.real} anb_kc_{x} = {src}[{idx}];")
+            stores.append(f"{src}[{idx}] = anb_kc_{x};")
         if pop.neuron_type.type == "rate":
             for t in pop.targets:
                 src = gsrc("_sum_" + t)
@@ -231,6 +256,9 @@ class CodeGenerator:
             cond = self.typed(self.fill(pop.desc["spike"]["spike_cond"]))
             resets = "\n          ".join(self.typed(self.fill(r["cpp"]))
                                          for r in pop.desc["spike"]["spike_reset"])
+            for r in pop.desc["spike"]["spike_reset"]:
+                if r["name"] in comp:
+                    resets += f"\n          anb_kc_{r['name']} = ({self.real})0;"
             if masked:
                 loads.append(f"int refractory_remaining = {rr_src}[{rr_idx}];")
                 loads.append("const int in_ref = (refractory_remaining > 0) ? 0 : 1;")
@@ -250,9 +278,12 @@ class CodeGenerator:
           {gsrc('last_spike')}[anb_i] = t;
           {refr_set}
         }}"""
-        spk_dst = (smem["spk"] if smem else gsrc("spk")) if spiking else None
+        spk_dst = ((smem.get("spk") if smem else gsrc("spk")) if spiking and ballot_hook is None
+                   else None)
         ballot = ""
-        if spiking:
+        if spiking and cluster is not None and ballot_hook is not None:
+            ballot = ballot_hook
+        elif spiking:
             widx, lim = ("anb_q", "anb_cnt") if cluster is not None else ("anb_i", "anb_n")
             ballot = f"""
       {{
@@ -750,7 +781,10 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
             ranges.append(f"const int anb_words{k} = (anb_cnt{k} + 31) >> 5;")
             for name in pl["arrays"]:
                 s_ = d[name]
-                if name.startswith(("spk", "cp", "nzw")):
+                if name.startswith(("spk", "cp", "spl", "spn")):
+                    continue
+                if name.startswith("kc_"):
+                    load.append(f"for (int q = threadIdx.x; q < anb_cnt{k}; q += blockDim.x) {s_}[q] = 0.f;")
                     continue
                 g = self.ptr(f"pop{k}__{name}")
                 load.append(f"for (int q = threadIdx.x; q < anb_cnt{k}; q += blockDim.x) {s_}[q] = {g}[anb_base{k} + q];")
@@ -762,33 +796,14 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
             store.append(f"for (int q = threadIdx.x; q < anb_words{k}; q += blockDim.x) "
                          f"{gspk}[(anb_base{k} >> 5) + q] = (nsteps & 1 ? {d['spk0']} : {d['spk1']})[(anb_base{k} >> 5) + q];")
         prop = []
-        scans = []
-        for pop in net.populations:
-            if not any(pr.pre_pop is pop for pr in net.projections):
-                continue
-            k = pop.id
-            d = smem_ptrs[k]
-            words = (pop.size + 31) // 32
-            # warp 0 lists the nonzero words of the previous step's bitmap, in order
-            scans.append(f"""
-      if (anb_warp == 0) {{
-        const anb_u32* __restrict__ anb_spk = (anb_par ? {d['spk0']} : {d['spk1']});
-        int anb_cnt = 0;
-        for (int c = 0; c < {words}; c += 32) {{
-          const anb_u32 w = (c + anb_lane < {words}) ? anb_spk[c + anb_lane] : 0u;
-          const anb_u32 nz = __ballot_sync(0xffffffffu, w != 0u);
-          if (w != 0u) {d['nzw']}[anb_cnt + __popc(nz & ((1u << anb_lane) - 1u))] = c + anb_lane;
-          anb_cnt += __popc(nz);
-        }}
-        if (anb_lane == 0) {d['nzw']}[{words}] = anb_cnt;
-      }}""")
+        fast_groups: dict[int, list] = {}
         for proj in net.projections:
             a, b = proj.pre_pop.id, proj.post_pop.id
             play = self.c.layout[proj.id]
             cl = lay["proj"][proj.id]
             k = proj.id
             p = lambda n, kk=k: self.ptr(f"proj{kk}__{n}")
-            lo = play["w0"] * 32
+            lo, hi = play["w0"] * 32, play["w1"] * 32
             cp = smem_ptrs[a][f"cp{k}"]
             g = smem_ptrs[b]["g_" + proj.target]
             # this CTA's incoming synapses of projection k, appended to the pool
@@ -814,83 +829,99 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
       }}
       anb_pool_off += anb_n;
     }}""")
+            deliver = (f"const int beg = {cp}[pre - {lo}], end = {cp}[pre - {lo} + 1];")
             spk = f"(anb_par ? {smem_ptrs[a]['spk0']} : {smem_ptrs[a]['spk1']})"
-            nzw = smem_ptrs[a]["nzw"]
-            nwords = (proj.pre_pop.size + 31) // 32
             if self.exact:
+                # every warp walks all nonzero words of the projection's range in
+                # ascending order (warp-uniform), one CTA barrier per spike
                 prop.append(f"""
       {{  // {proj.name}: spikes in ascending pre rank, one CTA barrier per spike
         const anb_u32* __restrict__ anb_spk = {spk};
-        const int anb_nz = {nzw}[{nwords}];
-        for (int i = 0; i < anb_nz; ++i) {{
-          const int word = {nzw}[i];
-          if (word < {play['w0']} || word >= {play['w1']}) continue;
-          anb_u32 m = anb_spk[word];
-          while (m) {{
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            const int pre = (word << 5) + b - {lo};
-            const int beg = {cp}[pre], end = {cp}[pre + 1];
-            if (end > beg) {{
-              for (int q = beg + threadIdx.x; q < end; q += blockDim.x)
-                {g}[anb_s_pool_post[q]] += {w_src}[{w_idx}];
-              __syncthreads();
+        for (int c = {play['w0']}; c < {play['w1']}; c += 32) {{
+          const anb_u32 anb_wv = (c + anb_lane < {play['w1']}) ? anb_spk[c + anb_lane] : 0u;
+          anb_u32 anb_nz = __ballot_sync(0xffffffffu, anb_wv != 0u);
+          while (anb_nz) {{
+            const int j = __ffs(anb_nz) - 1;
+            anb_nz &= anb_nz - 1;
+            anb_u32 m = __shfl_sync(0xffffffffu, anb_wv, j);
+            while (m) {{
+              const int b = __ffs(m) - 1;
+              m &= m - 1;
+              const int pre = ((c + j) << 5) + b;
+              {deliver}
+              if (end > beg) {{
+                for (int q = beg + threadIdx.x; q < end; q += blockDim.x)
+                  {g}[anb_s_pool_post[q]] += {w_src}[{w_idx}];
+                __syncthreads();
+              }}
             }}
           }}
         }}
       }}""")
             else:
-                prop.append(f"""
-      {{  // {proj.name}: warp per nonzero bitmap word, shared-memory atomics
-        const anb_u32* __restrict__ anb_spk = {spk};
-        const int anb_nz = {nzw}[{nwords}];
-        for (int i = anb_warp; i < anb_nz; i += anb_nwarps) {{
-          const int word = {nzw}[i];
-          if (word < {play['w0']} || word >= {play['w1']}) continue;
-          anb_u32 m = anb_spk[word];
-          while (m) {{
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            const int pre = (word << 5) + b - {lo};
-            const int beg = {cp}[pre], end = {cp}[pre + 1];
+                fast_groups.setdefault(a, []).append(f"""
+          if (pre >= {lo} && pre < {hi}) {{  // {proj.name}
+            {deliver}
             for (int q = beg + anb_lane; q < end; q += 32)
               atomicAdd(&{g}[anb_s_pool_post[q]], anb_wf({w_src}[{w_idx}]));
+          }}""")
+        for a, blocks in fast_groups.items():
+            pop_a = next(pp for pp in net.populations if pp.id == a)
+            W = (pop_a.size + 31) // 32
+            ch = max(1, min(32, -(-W // (lay["block"] // 32))))
+            spk = f"(anb_par ? {smem_ptrs[a]['spk0']} : {smem_ptrs[a]['spk1']})"
+            prop.append(f"""
+      {{  // population {a}: warp w scans its own {ch} bitmap words and delivers their
+          // spikes with shared-memory atomics (lanes over the synapses)
+        const anb_u32* __restrict__ anb_spk = {spk};
+        for (int c0 = anb_warp * {ch}; c0 < {W}; c0 += anb_nwarps * {ch}) {{
+          const anb_u32 anb_wv = (anb_lane < {ch} && c0 + anb_lane < {W}) ? anb_spk[c0 + anb_lane] : 0u;
+          anb_u32 anb_nz = __ballot_sync(0xffffffffu, anb_wv != 0u);
+          while (anb_nz) {{
+            const int j = __ffs(anb_nz) - 1;
+            anb_nz &= anb_nz - 1;
+            anb_u32 m = __shfl_sync(0xffffffffu, anb_wv, j);
+            while (m) {{
+              const int b = __ffs(m) - 1;
+              m &= m - 1;
+              const int pre = ((c0 + j) << 5) + b;{''.join(blocks)}
+            }}
           }}
         }}
       }}""")
-        updates, globals_, bcast = [], [], []
+        updates, globals_, bcast, recs = [], [], [], []
         for pop in net.populations:
             k = pop.id
             globals_.append(self._globals_preamble(pop, lambda n, kk=k: self.ptr(f"pop{kk}__{n}")))
             d = dict(smem_ptrs[k])
-            d["spk"] = f"((anb_par ? {d['spk1']} : {d['spk0']}) + (anb_base{k} >> 5))"
-            updates.append(self.neuron_update(pop, local_engine=True, smem=d, cluster={}))
-            bcast.append(f"""
-      {{  // own bitmap words of {pop.name} -> the other CTAs' replicas
-        anb_u32* __restrict__ anb_own = (anb_par ? {d['spk1']} : {d['spk0']}) + (anb_base{k} >> 5);
-        const unsigned anb_addr = anb_smem_addr(anb_own);
-        for (int q = threadIdx.x; q < {C} * anb_words{k}; q += blockDim.x) {{
-          const unsigned r = (unsigned)(q / anb_words{k});
-          const int w = q - (int)r * anb_words{k};
-          if (r != anb_rank) anb_cluster_st_u32(anb_cluster_map(anb_addr + 4u * w, r), anb_own[w]);
+            # right after its ballot, a warp stores its bitmap word into every
+            # CTA's replica (lane r -> CTA r) and one lane records it
+            rec = ""
+            for mon in net.monitors:
+                if mon.population is not pop or "spike" not in mon.variables:
+                    continue
+                ml = self.c.mon_layout[mon.id]
+                m = mon.id
+                rec += f"""
+          if (anb_lane == 31 && anb_mon_on{m}) {{
+            const long long anb_slot = t - anb_mon_t0{m};
+            if (anb_slot >= 0 && anb_slot < {ml['cap_spike']})
+              {self.ptr(f'mon{m}__spk')}[anb_slot * {ml['words']} + anb_gw] = anb_m;
+            else
+              anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+          }}"""
+            hook = f"""
+      {{
+        const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
+        if (anb_q - anb_lane < anb_cnt) {{
+          const int anb_gw = (anb_base >> 5) + (anb_q >> 5);
+          anb_u32* anb_dstw = (anb_par ? {d['spk1']} : {d['spk0']}) + anb_gw;
+          if (anb_lane == (int)anb_rank) *anb_dstw = anb_m;
+          else if (anb_lane < {C}) anb_cluster_st_u32(anb_cluster_map(anb_smem_addr(anb_dstw), (unsigned)anb_lane), anb_m);{rec}
         }}
-      }}""")
-        recs = []
-        for mon in net.monitors:
-            ml = self.c.mon_layout[mon.id]
-            m, k = mon.id, mon.population.id
-            d = smem_ptrs[k]
-            recs.append(f"""
-      if (anb_mon_on{m}) {{
-        const long long anb_slot = t - anb_mon_t0{m};
-        const anb_u32* __restrict__ anb_own = (anb_par ? {d['spk1']} : {d['spk0']}) + (anb_base{k} >> 5);
-        if (anb_slot >= 0 && anb_slot < {ml['cap_spike']}) {{
-          anb_u32* anb_dst = {self.ptr(f'mon{m}__spk')} + anb_slot * {ml['words']} + (anb_base{k} >> 5);
-          for (int q = threadIdx.x; q < anb_words{k}; q += blockDim.x) anb_dst[q] = anb_own[q];
-        }} else if (threadIdx.x == 0) {{
-          anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
-        }}
-      }}""")
+      }}"""
+            updates.append(self.neuron_update(pop, local_engine=True, smem=d, cluster={},
+                                              ballot_hook=hook))
         mon_pre = "\n    ".join(
             f"const int anb_mon_on{mon.id} = {self.ptr(f'mon{mon.id}__on')}[0];\n    "
             f"const long long anb_mon_t0{mon.id} = {self.ptr(f'mon{mon.id}__t0')}[0];"
@@ -923,14 +954,9 @@ anb_cluster_run(long long t0, int nsteps) {{
     for (int anb_s = 0; anb_s < nsteps; ++anb_s) {{
       const long long t = t0 + anb_s;
       const int anb_par = anb_s & 1;
-      {''.join(scans)}
-      __syncthreads();
       {''.join(prop)}
       __syncthreads();
       {''.join(updates)}
-      __syncthreads();
-      {''.join(bcast)}
-      {''.join(recs)}
       anb_cluster_sync();
     }}
     {nl.join(store)}

@@ -228,6 +228,34 @@ def accuracy(cn):
             "first_divergence_step": first, "v_rel_err_before_divergence": v_err}
 
 
+def accuracy_study(seeds=range(42, 50)):
+    """Firing-rate error of the fast path against the double path over
+    several seeds, next to the spread between two double runs whose initial
+    potentials differ by 1e-9 mV (the network is chaotic: any perturbation
+    eventually changes the raster, so this is the floor of the metric)."""
+    from annarchy_b200 import workloads as wl
+    rows = []
+    for seed in seeds:
+        cn = wl.coba_net(seed=seed)
+        counts = {}
+        for tag, prec, v0 in (("fp64", "double", cn.v0), ("fast", "float", cn.v0),
+                              ("fp64_perturbed", "double", cn.v0 + 1e-9)):
+            cn2 = wl.CobaNet(cn.n, cn.n_exc, cn.w_exc, cn.w_inh, v0, params=cn.params)
+            net, P, mon = build_net(cn2, prec, "local", "float32" if prec == "float" else None)
+            net.simulate_steps(MODEL_STEPS)
+            counts[tag] = mon.spike_arrays()[1].size
+            net.close()
+        rows.append((seed, counts["fp64"], counts["fast"], counts["fp64_perturbed"]))
+    d_fast = np.array([(f - e) / e for _, e, f, _ in rows])
+    d_pert = np.array([(q - e) / e for _, e, _, q in rows])
+    return {"seeds": [r[0] for r in rows], "spikes": [r[1:] for r in rows],
+            "rate_err_fast_mean_abs": float(np.abs(d_fast).mean()),
+            "rate_err_fast_mean_signed": float(d_fast.mean()),
+            "rate_err_perturbed_fp64_mean_abs": float(np.abs(d_pert).mean()),
+            "rate_err_fast_of_seed_mean": float(abs(sum(r[2] for r in rows) - sum(r[1] for r in rows))
+                                                / sum(r[1] for r in rows))}
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -279,9 +307,29 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fast-only", action="store_true",
+                    help="time only the fast path (used for profiler captures)")
+    ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.accuracy:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(accuracy_study()))
+        return
+    if args.fast_only:
+        import torch
+        torch.cuda.set_device(0)
+        from annarchy_b200 import workloads as wl
+        cn = wl.coba_net(seed=42)
+        net, P, mon = build_net(cn, "float", "local", "float32")
+        dev = time_device(net, P, mon, cn, args.steps, args.warmup)
+        print(json.dumps({"ms_per_step": sum(dev["ms"]) / len(dev["ms"]),
+                          "events_per_step": sum(dev["events"]) / len(dev["events"]),
+                          "engine": net.engine}))
+        net.close()
         return
     rank, world, local = dist_env()
     import torch
