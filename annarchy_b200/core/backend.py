@@ -338,8 +338,18 @@ class CompiledNetwork:
             if fmt != "csr":
                 F.create_format_arrays(self, proj, fmt, post_rank, row_ptr, cols, w, lay)
             lay["group"] = F.csr_group(nnz / max(rows, 1))
+            lay["split"] = int(self.net._config.get("ell_split", 4))
             lay["kahan_min"] = 10000
             lay["grid"] = grid_for(rows * (lay["group"] if not self.exact and fmt == "csr" else 1))
+            if fmt == "csr" and not self.exact:
+                light, heavy = F.csr_bins(row_ptr)
+                lay["heavy"] = int(heavy.size)
+                lengths = np.diff(row_ptr)
+                lay["vgroup"] = F.vec_group(float(lengths[light].mean()) if light.size else 1.0)
+                if heavy.size:
+                    nat.create(f"proj{k}__rows_light", light)
+                    nat.create(f"proj{k}__rows_heavy", heavy)
+                lay["light"] = int(light.size)
         else:
             # pre-major view (the reference's CSRC column view, CSRCMatrix.hpp:164-222)
             npre = proj.pre_pop.size

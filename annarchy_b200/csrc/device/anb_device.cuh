@@ -110,6 +110,168 @@ __device__ __forceinline__ void anb_rate_csr_vector(int n_rows, const I* __restr
   }
 }
 
+// Streaming loads of matrix data that is read once per step: not allocated
+// in L1, so L1 keeps the gathered pre-synaptic vector.
+__device__ __forceinline__ int4 anb_ls_i4(const int4* p) {
+  int4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float4 anb_ls_f4(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint2 anb_ls_u2(const uint2* p) {
+  uint2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ int anb_ls_i(const int* p) {
+  int v;
+  asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float anb_ls_f(const float* p) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ unsigned short anb_ls_h(const unsigned short* p) {
+  unsigned short v;
+  asm volatile("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
+}
+
+// Four consecutive weights widened to float (16-byte or 8-byte load).
+__device__ __forceinline__ float4 anb_w4(const float* w) { return anb_ls_f4(reinterpret_cast<const float4*>(w)); }
+__device__ __forceinline__ float4 anb_w4(const anb_bf16* w) {
+  const uint2 u = anb_ls_u2(reinterpret_cast<const uint2*>(w));
+  return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
+                     __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
+}
+__device__ __forceinline__ float anb_w1(const float* w) { return anb_ls_f(w); }
+__device__ __forceinline__ float anb_w1(const anb_bf16* w) { return anb_bf16_to_f32(anb_ls_h(w)); }
+
+// Sub-warp per row with 16-byte vector loads of the column indices and
+// weights (streaming, evict-first) over the 4-aligned body of every row and
+// scalar loads at its ends. `rows` (optional) lists the rows to process
+// (row-length binning); `n_rows` is its length.
+template <int G, typename W>
+__device__ __forceinline__ void anb_rate_csr_vec(int n_rows, const int* __restrict__ rows,
+                                                 const int* __restrict__ row_ptr,
+                                                 const int* __restrict__ col,
+                                                 const W* __restrict__ w,
+                                                 const float* __restrict__ x,
+                                                 const int* __restrict__ post_rank,
+                                                 float* __restrict__ sum) {
+  const int lane = threadIdx.x % G;
+  const int groups = (gridDim.x * blockDim.x) / G;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) / G; r < n_rows; r += groups) {
+    const int row = rows ? rows[r] : r;
+    const int beg = row_ptr[row], end = row_ptr[row + 1];
+    int j0 = (beg + 3) & ~3;
+    if (j0 > end) j0 = end;
+    float s = 0.f;
+    for (int j = beg + lane; j < j0; j += G) s += __ldg(&x[anb_ls_i(&col[j])]) * anb_w1(&w[j]);
+    const int nv = (end - j0) >> 2;
+    const int4* __restrict__ c4 = reinterpret_cast<const int4*>(col + j0);
+    float s1 = 0.f;
+    int v = lane;
+    for (; v + G < nv; v += 2 * G) {          // two vectors in flight per lane
+      const int4 ca = anb_ls_i4(c4 + v), cb = anb_ls_i4(c4 + v + G);
+      const float4 wa = anb_w4(w + j0 + 4 * v), wb = anb_w4(w + j0 + 4 * (v + G));
+      s += __ldg(&x[ca.x]) * wa.x + __ldg(&x[ca.y]) * wa.y + __ldg(&x[ca.z]) * wa.z +
+           __ldg(&x[ca.w]) * wa.w;
+      s1 += __ldg(&x[cb.x]) * wb.x + __ldg(&x[cb.y]) * wb.y + __ldg(&x[cb.z]) * wb.z +
+            __ldg(&x[cb.w]) * wb.w;
+    }
+    if (v < nv) {
+      const int4 c = anb_ls_i4(c4 + v);
+      const float4 ww = anb_w4(w + j0 + 4 * v);
+      s += __ldg(&x[c.x]) * ww.x + __ldg(&x[c.y]) * ww.y + __ldg(&x[c.z]) * ww.z +
+           __ldg(&x[c.w]) * ww.w;
+    }
+    s += s1;
+    for (int j = j0 + 4 * nv + lane; j < end; j += G) s += __ldg(&x[anb_ls_i(&col[j])]) * anb_w1(&w[j]);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
+    if (lane == 0) sum[post_rank ? post_rank[row] : row] += s;
+  }
+}
+
+// One CTA per (long) row, Kahan-compensated per thread, block reduction.
+template <typename W>
+__device__ __forceinline__ void anb_rate_csr_cta(int n_rows, const int* __restrict__ rows,
+                                                 const int* __restrict__ row_ptr,
+                                                 const int* __restrict__ col,
+                                                 const W* __restrict__ w,
+                                                 const float* __restrict__ x,
+                                                 const int* __restrict__ post_rank,
+                                                 float* __restrict__ sum) {
+  __shared__ float red[32];
+  for (int r = blockIdx.x; r < n_rows; r += gridDim.x) {
+    const int row = rows ? rows[r] : r;
+    const int beg = row_ptr[row], end = row_ptr[row + 1];
+    float s = 0.f, c = 0.f;
+    for (int j = beg + threadIdx.x; j < end; j += blockDim.x) {
+      const float y = __fmul_rn(__ldg(&x[anb_ls_i(&col[j])]), anb_w1(&w[j])) - c;
+      const float t = s + y;
+      c = (t - s) - y;
+      s = t;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      float v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (threadIdx.x == 0) sum[post_rank ? post_rank[row] : row] += v;
+    }
+    __syncthreads();
+  }
+}
+
+// Blocked CSR with T x T tiles stored column-major (val[tile][c][r]): one
+// CTA per block row; thread (r, part) sums tile row r over its share of the
+// tile columns, then the parts are added in shared memory. Exact mode keeps
+// one part per row (ascending columns = ascending pre rank).
+template <int T, int PARTS, typename R, typename W>
+__device__ __forceinline__ void anb_rate_bsr_rows(int n_block_rows, const int* __restrict__ brow_ptr,
+                                                  const int* __restrict__ bcol,
+                                                  const W* __restrict__ val,
+                                                  const R* __restrict__ x, int n_pre, int n_post,
+                                                  R* __restrict__ sum) {
+  __shared__ R part[PARTS][T];
+  const int r = threadIdx.x % T, pidx = threadIdx.x / T;
+  constexpr int CW = T / PARTS;
+  for (int br = blockIdx.x; br < n_block_rows; br += gridDim.x) {
+    R s = R(0);
+    if (pidx < PARTS) {
+      for (int b = brow_ptr[br]; b < brow_ptr[br + 1]; ++b) {
+        const W* __restrict__ tile = val + (size_t)b * T * T;
+        const int c0 = bcol[b] * T;
+        const R* __restrict__ xs = x + c0;
+        const int cend = min((pidx + 1) * CW, n_pre - c0);   // partial last tile column
+        for (int c = pidx * CW; c < cend; ++c) s += xs[c] * (R)anb_wf(tile[c * T + r]);
+      }
+      part[pidx][r] = s;
+    }
+    __syncthreads();
+    if (pidx == 0) {
+      R tot = part[0][r];
+      for (int q = 1; q < PARTS; ++q) tot += part[q][r];
+      const int post = br * T + r;
+      if (post < n_post) sum[post] += tot;
+    }
+    __syncthreads();
+  }
+}
+
 // ELLPACK / ELLPACK-R: column-major slots, thread per row.
 // cols[k*n_rows + row], w likewise; rl = row lengths (ELL-R) or nullptr
 // (ELL: stop at the first slot holding -1).
@@ -123,13 +285,98 @@ __device__ __forceinline__ void anb_rate_ell(int n_rows, int width, const int* _
        row += gridDim.x * blockDim.x) {
     const int len = rl ? rl[row] : width;
     R s = R(0);
-    for (int k = 0; k < len; ++k) {
-      const int c = cols[(size_t)k * n_rows + row];
-      if (!rl && c < 0) break;
-      s += pre_r[c] * (R)anb_wf(w[(size_t)k * n_rows + row]);
+    if (sizeof(R) == 8 || !rl) {
+      // exact order (double) or ELL with -1 padding: one chain
+      for (int k = 0; k < len; ++k) {
+        const int c = cols[(size_t)k * n_rows + row];
+        if (!rl && c < 0) break;
+        s += pre_r[c] * (R)anb_wf(w[(size_t)k * n_rows + row]);
+      }
+    } else {
+      // four independent chains keep four gathers in flight per thread
+      R s1 = R(0), s2 = R(0), s3 = R(0);
+      int k = 0;
+      for (; k + 4 <= len; k += 4) {
+        const size_t o = (size_t)k * n_rows + row;
+        const int c0 = __ldcs(&cols[o]), c1 = __ldcs(&cols[o + n_rows]);
+        const int c2 = __ldcs(&cols[o + 2 * (size_t)n_rows]), c3 = __ldcs(&cols[o + 3 * (size_t)n_rows]);
+        const R w0 = (R)anb_wf(w[o]), w1 = (R)anb_wf(w[o + n_rows]);
+        const R w2 = (R)anb_wf(w[o + 2 * (size_t)n_rows]), w3 = (R)anb_wf(w[o + 3 * (size_t)n_rows]);
+        s += __ldg(&pre_r[c0]) * w0;
+        s1 += __ldg(&pre_r[c1]) * w1;
+        s2 += __ldg(&pre_r[c2]) * w2;
+        s3 += __ldg(&pre_r[c3]) * w3;
+      }
+      for (; k < len; ++k) {
+        const size_t o = (size_t)k * n_rows + row;
+        s += __ldg(&pre_r[__ldcs(&cols[o])]) * (R)anb_wf(w[o]);
+      }
+      s = (s + s1) + (s2 + s3);
     }
     const int post = post_rank ? post_rank[row] : row;
     sum[post] += s;
+  }
+}
+
+// ELL / ELL-R / SELL in single precision with G threads per row: a CTA of
+// R*G threads covers R consecutive rows (consecutive lanes = consecutive rows,
+// so every load instruction is one contiguous run); thread part g takes slots
+// g, g+G, ...; the G partial sums are added in shared memory.
+// SELL passes its slice layout (slot of (row, k) = slice_ptr[row/C] + k*C + row%C);
+// ELL passes slice_ptr = nullptr (slot = k*n_rows + row).
+template <int G, int C, typename W>
+__device__ __forceinline__ void anb_rate_slots_split(int n_rows, int width,
+                                                     const int* __restrict__ slice_ptr,
+                                                     const int* __restrict__ cols,
+                                                     const W* __restrict__ w,
+                                                     const int* __restrict__ rl,
+                                                     const int* __restrict__ perm,
+                                                     const float* __restrict__ x,
+                                                     const int* __restrict__ post_rank,
+                                                     float* __restrict__ sum) {
+  __shared__ float part[1024];
+  const int R = blockDim.x / G;
+  const int lr = threadIdx.x % R, g = threadIdx.x / R;
+  for (int base = blockIdx.x * R; base < n_rows; base += gridDim.x * R) {
+    const int r = base + lr;
+    float s = 0.f, s1 = 0.f;
+    if (r < n_rows) {
+      const int len = rl ? rl[r] : width;
+      size_t slot0, stride;
+      if (slice_ptr) {
+        slot0 = (size_t)slice_ptr[r / C] + (r % C);
+        stride = C;
+      } else {
+        slot0 = r;
+        stride = (size_t)n_rows;
+      }
+      int k = g;
+      for (; k + G < len; k += 2 * G) {
+        const size_t o0 = slot0 + (size_t)k * stride, o1 = o0 + (size_t)G * stride;
+        const int c0 = anb_ls_i(&cols[o0]), c1 = anb_ls_i(&cols[o1]);
+        if (!rl && c1 < 0) {
+          if (c0 >= 0) s += __ldg(&x[c0]) * anb_w1(&w[o0]);
+          k = len;
+          break;
+        }
+        s += __ldg(&x[c0]) * anb_w1(&w[o0]);
+        s1 += __ldg(&x[c1]) * anb_w1(&w[o1]);
+      }
+      if (k < len) {
+        const size_t o0 = slot0 + (size_t)k * stride;
+        const int c0 = anb_ls_i(&cols[o0]);
+        if (rl || c0 >= 0) s += __ldg(&x[c0]) * anb_w1(&w[o0]);
+      }
+    }
+    part[threadIdx.x] = s + s1;
+    __syncthreads();
+    if (g == 0 && r < n_rows) {
+      float tot = part[lr];
+      for (int q = 1; q < G; ++q) tot += part[lr + q * R];
+      const int row = perm ? perm[r] : r;
+      sum[post_rank ? post_rank[row] : row] += tot;
+    }
+    __syncthreads();
   }
 }
 
@@ -151,9 +398,30 @@ __device__ __forceinline__ void anb_rate_sell(int n_rows, const int* __restrict_
     const int base = slice_ptr[sl];
     const int len = row_len[r];
     R s = R(0);
-    for (int k = 0; k < len; ++k) {
-      const int slot = base + k * C + lane;
-      s += pre_r[cols[slot]] * (R)anb_wf(w[slot]);
+    if (sizeof(R) == 8) {
+      for (int k = 0; k < len; ++k) {
+        const int slot = base + k * C + lane;
+        s += pre_r[cols[slot]] * (R)anb_wf(w[slot]);
+      }
+    } else {
+      R s1 = R(0), s2 = R(0), s3 = R(0);
+      int k = 0;
+      for (; k + 4 <= len; k += 4) {
+        const int o = base + k * C + lane;
+        const int c0 = __ldcs(&cols[o]), c1 = __ldcs(&cols[o + C]);
+        const int c2 = __ldcs(&cols[o + 2 * C]), c3 = __ldcs(&cols[o + 3 * C]);
+        const R w0 = (R)anb_wf(w[o]), w1 = (R)anb_wf(w[o + C]);
+        const R w2 = (R)anb_wf(w[o + 2 * C]), w3 = (R)anb_wf(w[o + 3 * C]);
+        s += __ldg(&pre_r[c0]) * w0;
+        s1 += __ldg(&pre_r[c1]) * w1;
+        s2 += __ldg(&pre_r[c2]) * w2;
+        s3 += __ldg(&pre_r[c3]) * w3;
+      }
+      for (; k < len; ++k) {
+        const int o = base + k * C + lane;
+        s += __ldg(&pre_r[__ldcs(&cols[o])]) * (R)anb_wf(w[o]);
+      }
+      s = (s + s1) + (s2 + s3);
     }
     const int row = perm ? perm[r] : r;
     const int post = post_rank ? post_rank[row] : row;

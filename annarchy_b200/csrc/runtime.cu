@@ -139,6 +139,8 @@ struct anb_net {
   std::vector<TimedLaunch> pending;
   std::vector<KernelTime> times;
   std::map<std::string, int> time_index;
+  void* flush_buf = nullptr;
+  size_t flush_bytes = 0;
 };
 
 namespace {
@@ -352,6 +354,7 @@ int anb_destroy(anb_net* net) {
     cudaEventDestroy(tl.stop);
   }
   drop_graph(net);
+  if (net->flush_buf) cudaFree(net->flush_buf);
   if (net->module) g_drv.moduleUnload(net->module);
   for (auto& kv : net->arrays) cudaFree(kv.second.ptr);
   if (net->own_stream) cudaStreamDestroy(net->own_stream);
@@ -741,6 +744,25 @@ int anb_device_error(anb_net* net, int* code) {
 }
 
 int anb_clear_device_error(anb_net* net) { return anb_array_fill_zero(net, "err"); }
+
+int anb_flush_l2(anb_net* net) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  if (!net->flush_buf) {
+    int dev = 0, l2 = 0;
+    ANB_CUDA(cudaGetDevice(&dev));
+    ANB_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+    net->flush_bytes = (size_t)(l2 > 0 ? l2 : (128 << 20)) * 2;
+    cudaError_t e = cudaMalloc(&net->flush_buf, net->flush_bytes);
+    if (e != cudaSuccess) {
+      net->flush_buf = nullptr;
+      return fail(ANB_ERR_ALLOC, "L2 flush buffer");
+    }
+  }
+  ANB_CUDA(cudaMemsetAsync(net->flush_buf, 0x5a, net->flush_bytes, net->stream));
+  return ANB_OK;
+}
 
 int anb_kernel_timing(anb_net* net, int enable) {
   if (!net) return fail(ANB_ERR_ARG, "net is NULL");

@@ -347,7 +347,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
         return any(v.get("cpp") for v in pop.desc["variables"])
 
     # ------------------------------------------------------------ projections
-    def rate_kernel(self, proj) -> str:
+    def rate_kernel(self, proj):
+        """Weighted-sum kernel(s) of a rate-coded projection in its storage
+        format. Returns (source, [(kernel, grid, block, smem)])."""
         k = proj.id
         lay = self.c.layout[proj.id]
         pre_r = self.ptr(f"pop{proj.pre_pop.id}__r")
@@ -355,39 +357,67 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
         fmt = lay["format"]
         p = lambda n: self.ptr(f"proj{k}__{n}")
         W = self.c.wctype
+        name = f"proj{k}_psp"
+
+        def kern(nm, body, block=BLOCK):
+            return f"""
+extern "C" __global__ void __launch_bounds__({block}) {nm}() {{
+    {body}
+}}
+"""
         if fmt == "csr":
             if self.exact:
                 call = (f"anb_rate_csr_scalar<double, double, {lay['idx_t']}>({lay['rows']}, "
                         f"{p('row_ptr')}, {p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_});")
+                return kern(name, call), [(name, lay["grid"], BLOCK, 0)]
+            G = lay["vgroup"]
+            if lay.get("heavy", 0):
+                light = (f"anb_rate_csr_vec<{G}, {W}>({lay['light']}, {p('rows_light')}, {p('row_ptr')}, "
+                         f"{p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_});")
+                heavy = (f"anb_rate_csr_cta<{W}>({lay['heavy']}, {p('rows_heavy')}, {p('row_ptr')}, "
+                         f"{p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_});")
+                return (kern(name, light) + kern(name + "_heavy", heavy),
+                        [(name, grid_for(lay["light"] * G), BLOCK, 0),
+                         (name + "_heavy", min(lay["heavy"], MAX_GRID), BLOCK, 0)])
+            call = (f"anb_rate_csr_vec<{G}, {W}>({lay['rows']}, nullptr, {p('row_ptr')}, {p('col')}, "
+                    f"{p('w')}, {pre_r}, {p('post_rank')}, {sum_});")
+            return kern(name, call), [(name, grid_for(lay["rows"] * G), BLOCK, 0)]
+        if fmt in ("ell", "ellr", "hyb"):
+            rl = p("rl") if fmt in ("ellr", "hyb") else "nullptr"
+            if self.exact:
+                call = (f"anb_rate_ell<{self.real}, {W}>({lay['rows']}, {lay['width']}, {p('ell_col')}, "
+                        f"{p('ell_w')}, {rl}, {pre_r}, {p('post_rank')}, {sum_});")
+                src, plan = kern(name, call), [(name, lay["grid"], BLOCK, 0)]
             else:
-                call = (f"anb_rate_csr_vector<{lay['group']}, {W}, {lay['idx_t']}>({lay['rows']}, "
-                        f"{p('row_ptr')}, {p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_}, "
-                        f"{lay['kahan_min']});")
-        elif fmt in ("ell", "ellr"):
-            rl = p("rl") if fmt == "ellr" else "nullptr"
-            call = (f"anb_rate_ell<{self.real}, {W}>({lay['rows']}, {lay['width']}, {p('ell_col')}, "
-                    f"{p('ell_w')}, {rl}, {pre_r}, {p('post_rank')}, {sum_});")
-        elif fmt == "sell":
-            call = (f"anb_rate_sell<{lay['C']}, {self.real}, {W}>({lay['rows']}, {p('slice_ptr')}, "
-                    f"{p('slice_len')}, {p('sell_col')}, {p('sell_w')}, {p('sell_rl')}, "
-                    f"{p('perm')}, {pre_r}, {p('post_rank')}, {sum_});")
-        elif fmt == "hyb":
-            call = (f"anb_rate_ell<{self.real}, {W}>({lay['rows']}, {lay['width']}, {p('ell_col')}, "
-                    f"{p('ell_w')}, {p('rl')}, {pre_r}, {p('post_rank')}, {sum_});")
-        elif fmt == "bsr":
-            call = (f"anb_rate_bsr<{lay['tile']}, {self.real}, {W}>({lay['block_rows']}, "
+                G = lay["split"]
+                call = (f"anb_rate_slots_split<{G}, 1, {W}>({lay['rows']}, {lay['width']}, nullptr, "
+                        f"{p('ell_col')}, {p('ell_w')}, {rl}, nullptr, {pre_r}, {p('post_rank')}, {sum_});")
+                src = kern(name, call)
+                plan = [(name, grid_for(lay["rows"] * G), BLOCK, 0)]
+            if fmt == "hyb" and lay["coo_nnz"] > 0:
+                src += self._hyb_tail(proj, lay, pre_r, sum_)
+                plan.append((name + "_tail", lay["tail_grid"], BLOCK, 0))
+            return src, plan
+        if fmt == "sell":
+            if self.exact:
+                call = (f"anb_rate_sell<{lay['C']}, {self.real}, {W}>({lay['rows']}, {p('slice_ptr')}, "
+                        f"{p('slice_len')}, {p('sell_col')}, {p('sell_w')}, {p('sell_rl')}, "
+                        f"{p('perm')}, {pre_r}, {p('post_rank')}, {sum_});")
+                return kern(name, call), [(name, lay["grid"], BLOCK, 0)]
+            G = lay["split"]
+            call = (f"anb_rate_slots_split<{G}, {lay['C']}, {W}>({lay['rows']}, 0, {p('slice_ptr')}, "
+                    f"{p('sell_col')}, {p('sell_w')}, {p('sell_rl')}, {p('perm')}, {pre_r}, "
+                    f"{p('post_rank')}, {sum_});")
+            return kern(name, call), [(name, grid_for(lay["rows"] * G), BLOCK, 0)]
+        if fmt == "bsr":
+            T = lay["tile"]
+            parts = 1 if self.exact else max(1, min(T, 256 // T))
+            block = T * parts
+            call = (f"anb_rate_bsr_rows<{T}, {parts}, {self.real}, {W}>({lay['block_rows']}, "
                     f"{p('bsr_row_ptr')}, {p('bsr_col')}, {p('bsr_val')}, {pre_r}, "
-                    f"{p('bsr_post')}, {lay['n_post_pad']}, {sum_});")
-        else:
-            raise NotImplementedError(fmt)
-        out = f"""
-extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
-    {call}
-}}
-"""
-        if fmt == "hyb" and lay["coo_nnz"] > 0:
-            out += self._hyb_tail(proj, lay, pre_r, sum_)
-        return out
+                    f"{proj.pre_pop.size}, {proj.post_pop.size}, {sum_});")
+            return kern(name, call, block), [(name, min(lay["block_rows"], MAX_GRID * 4), block, 0)]
+        raise NotImplementedError(fmt)
 
     def _hyb_tail(self, proj, lay, pre_r, sum_):
         k = proj.id
@@ -591,10 +621,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
         for proj in net.projections:
             lay = self.c.layout[proj.id]
             if proj.synapse_type.type == "rate":
-                kernels.append(self.rate_kernel(proj))
-                plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0))
-                if lay.get("format") == "hyb" and lay.get("coo_nnz", 0) > 0:
-                    plan.append((f"proj{proj.id}_psp_tail", lay["tail_grid"], BLOCK, 0))
+                src, launches = self.rate_kernel(proj)
+                kernels.append(src)
+                plan.extend(launches)
             else:
                 kernels.append(self.spike_kernel(proj))
                 plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0))

@@ -35,6 +35,27 @@ def csr_group(mean_row: float) -> int:
     return 32
 
 
+def csr_bins(row_ptr, heavy_min: int = 0):
+    """Rows split by length: (light rows, heavy rows) with heavy rows longer
+    than max(1024, 16 x the mean); heavy rows get a CTA each."""
+    rl = _lengths(row_ptr)
+    if rl.size == 0:
+        return np.zeros(0, np.int32), np.zeros(0, np.int32)
+    cut = heavy_min or max(1024, int(16 * rl.mean()))
+    heavy = np.nonzero(rl > cut)[0].astype(np.int32)
+    light = np.nonzero(rl <= cut)[0].astype(np.int32)
+    return light, heavy
+
+
+def vec_group(mean_row: float) -> int:
+    """Lanes per row of the vector-load CSR kernel (each lane takes 4
+    entries per iteration)."""
+    for g in (2, 4, 8, 16):
+        if mean_row <= 8 * g:
+            return g
+    return 32
+
+
 def _lengths(row_ptr):
     return np.diff(np.asarray(row_ptr, dtype=np.int64))
 
@@ -110,8 +131,8 @@ def bsr_arrays(post_rank, row_ptr, cols, w, n_pre, tile):
     nblk = ukey.size
     ubr = ukey // ((n_pre + tile - 1) // tile)
     ubc = ukey % ((n_pre + tile - 1) // tile)
-    vals = np.zeros((nblk, tile, tile), dtype=np.float64)
-    vals[inv, rows_of % tile, np.asarray(cols) % tile] = w
+    vals = np.zeros((nblk, tile, tile), dtype=np.float64)       # column-major tiles
+    vals[inv, np.asarray(cols) % tile, rows_of % tile] = w
     brp = np.zeros(nbr + 1, dtype=np.int32)
     np.cumsum(np.bincount(ubr, minlength=nbr), out=brp[1:])
     return dict(block_row_ptr=brp, block_col=ubc.astype(np.int32), values=vals.reshape(-1),

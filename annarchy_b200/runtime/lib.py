@@ -52,6 +52,7 @@ SIGNATURES = {
     "anb_synchronize": (C.c_int, [C.c_void_p]),
     "anb_device_error": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "anb_clear_device_error": (C.c_int, [C.c_void_p]),
+    "anb_flush_l2": (C.c_int, [C.c_void_p]),
     "anb_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "anb_kernel_time_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "anb_kernel_time_get": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t,
@@ -246,6 +247,9 @@ class NativeNet:
         return c.value
 
     # -- timing -----------------------------------------------------------------
+    def flush_l2(self):
+        check("anb_flush_l2", self.lib.anb_flush_l2(self.h))
+
     def kernel_timing(self, enable: bool):
         check("anb_kernel_timing", self.lib.anb_kernel_timing(self.h, 1 if enable else 0))
 

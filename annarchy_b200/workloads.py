@@ -164,11 +164,19 @@ def sweep_matrix(kind: str, seed: int = 42, n: int = 100_000, mean_nnz: int = 10
     """
     rng = np.random.default_rng(seed)
     if kind == "uniform":
-        cols = np.empty((n, mean_nnz), dtype=np.int64)
-        for r0 in range(0, n, 4096):
-            r1 = min(n, r0 + 4096)
-            keys = rng.random((r1 - r0, n), dtype=np.float32)
-            cols[r0:r1] = np.argpartition(keys, mean_nnz, axis=1)[:, :mean_nnz]
+        # exactly mean_nnz distinct columns per row: draw a few more than
+        # needed, drop repeats, keep a uniformly random subset of the rest
+        k = mean_nnz + 16
+        draws = np.sort(rng.integers(0, n, (n, k)), axis=1)
+        keys = rng.random((n, k))
+        dup = np.zeros_like(draws, dtype=bool)
+        dup[:, 1:] = draws[:, 1:] == draws[:, :-1]
+        keys[dup] = 2.0
+        short = np.nonzero((~dup).sum(axis=1) < mean_nnz)[0]
+        pick = np.argpartition(keys, mean_nnz - 1, axis=1)[:, :mean_nnz]
+        cols = np.take_along_axis(draws, pick, axis=1)
+        for r in short:                       # rare: too many repeats in the draw
+            cols[r] = rng.choice(n, mean_nnz, replace=False)
         cols.sort(axis=1)
         indptr = np.arange(0, n * mean_nnz + 1, mean_nnz, dtype=np.int64)
         data = rng.normal(0.0, sd, n * mean_nnz)

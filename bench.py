@@ -256,6 +256,33 @@ def accuracy_study(seeds=range(42, 50)):
                                                 / sum(r[1] for r in rows))}
 
 
+def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
+    """Rate-coded weighted sums of the 100k-neuron recurrent matrices in every
+    feasible storage format: cold-L2 kernel time and achieved algorithmic
+    bandwidth as a fraction of the measured HBM peak."""
+    from annarchy_b200 import tuning, workloads as wl
+    peak, kind = peaks()
+    out = {"peak_gbs": peak, "peak_source": kind, "results": {}}
+    for st in structures:
+        m = wl.sweep_matrix(st)
+        rl = np.diff(m.indptr)
+        scheds = tuning.SCHEDULES if m.nnz < 50_000_000 else [
+            {"format": "csr"}, {"format": "sell", "sell_sigma": 1024}, {"format": "bsr", "bsr_tile": 64}]
+        for dt in dtypes:
+            wb = 4 if dt == "float32" else 2
+            ab = tuning.algorithmic_bytes(m, wb)
+            tuner = tuning.Autotuner()
+            best, table = tuner.tune(m, "float", dt, reps, scheds, tag=st)
+            out["results"][f"{st}/{dt}"] = {
+                "nnz": int(m.nnz), "mean_row": float(rl.mean()), "max_row": int(rl.max()),
+                "algorithmic_mb": ab / 1e6, "best": best,
+                "heuristic": tuning.heuristic(m),
+                "schedules": {k: {"ms": v, "gbs": ab / (v * 1e-3) / 1e9,
+                                  "frac": ab / (v * 1e-3) / 1e9 / peak} for k, v in table.items()}}
+            print(json.dumps({f"{st}/{dt}": out["results"][f"{st}/{dt}"]}), flush=True)
+    return out
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -310,7 +337,15 @@ def main():
     ap.add_argument("--fast-only", action="store_true",
                     help="time only the fast path (used for profiler captures)")
     ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
+    ap.add_argument("--formats", default="",
+                    help="storage-format study on these 100k structures (comma separated: "
+                         "uniform,powerlaw,local,blocks)")
     args = ap.parse_args()
+    if args.formats:
+        import torch
+        torch.cuda.set_device(0)
+        format_study(args.formats.split(","))
+        return
     if args.impl == "reference":
         run_reference(args)
         return

@@ -145,7 +145,11 @@ int anb_clear_device_error(anb_net* net);
 int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
                           int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity);
 
-/* ---- per-kernel timing (CUDA events around every launch; no graphs) ----- */
+/* ---- per-kernel timing (CUDA events around every launch; no graphs) -----
+ * anb_flush_l2 overwrites a buffer twice the size of the L2 cache (allocated
+ * on first use) on the network's stream, so that the next kernel starts cold;
+ * used between timed repetitions. */
+int anb_flush_l2(anb_net* net);
 int anb_kernel_timing(anb_net* net, int enable);
 int anb_kernel_time_count(anb_net* net, int* count);
 int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len,

@@ -45,9 +45,10 @@ def test_rate_c1_exact(golden):
     assert np.array_equal(r.sum(axis=1), g["r_sum"])
 
 
-@pytest.mark.parametrize("fmt", ["ell", "ellr", "sell"])
+@pytest.mark.parametrize("fmt", ["ell", "ellr", "sell", "bsr"])
 def test_rate_formats_exact(golden, fmt):
-    """ELL, ELL-R and SELL sum every row in ascending pre rank: bit-identical to CSR."""
+    """ELL, ELL-R, SELL and BSR sum every row in ascending pre rank:
+    bit-identical to CSR."""
     g = golden("rate_small")
     rn = wl.rate_net(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100)
     r = run_rate(rn, 100, storage_format=fmt)
@@ -139,3 +140,40 @@ def test_coba_float_rates(engine):
     e2 = out["steps"] < 300
     assert np.array_equal(out["idx"][e2], ref["spike_idx"][early])
     out["net"].close()
+
+
+@pytest.mark.parametrize("fmt", ["csr", "ell", "ellr", "sell", "hyb", "bsr"])
+@pytest.mark.parametrize("wdt", ["float32", "bfloat16"])
+def test_rate_formats_float(fmt, wdt):
+    """Every storage format in single precision: norm-wise relative error of
+    r per step <= 1e-5 against the double oracle fed the same weights."""
+    rn = wl.rate_net(seed=5, n_in=300, n_out=700, p_in=0.1, p_rec=0.05, steps=50)
+    if wdt == "bfloat16":
+        from annarchy_b200.core.backend import from_bf16, to_bf16
+        rn.w_in.data = from_bf16(to_bf16(rn.w_in.data))
+        rn.w_rec.data = from_bf16(to_bf16(rn.w_rec.data))
+    _, ref = O.rate_run(rn, trace=True)
+    r = run_rate(rn, 50, precision="float", weight_dtype=wdt, storage_format=fmt, bsr_tile=32)
+    err = np.linalg.norm(r - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-30)
+    assert err.max() <= 1e-5, err.max()
+
+
+def test_rate_powerlaw_binned_csr():
+    """Power-law row lengths: heavy rows (CTA per row, compensated) and light
+    rows (vector loads) together match the double oracle."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(3)
+    n = 3000
+    lengths = np.minimum((rng.pareto(1.0, n) * 20 + 5).astype(int), n)
+    lengths[:3] = [2500, 2800, 3000]
+    rows = np.repeat(np.arange(n), lengths)
+    cols = np.concatenate([rng.choice(n, L, replace=False) for L in lengths])
+    w = rng.normal(0, 0.01, rows.size)
+    m = sp.csr_matrix((w, (rows, cols)), shape=(n, n))
+    m.sort_indices()
+    rn = wl.RateNet(n_in=n, n_out=n, w_in=m, w_rec=sp.csr_matrix((n, n)),
+                    r_in=rng.uniform(0, 1, n), steps=20)
+    _, ref = O.rate_run(rn, trace=True)
+    r = run_rate(rn, 20, precision="float", weight_dtype="float32")
+    err = np.linalg.norm(r - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-30)
+    assert err.max() <= 1e-5, err.max()
