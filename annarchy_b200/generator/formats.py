@@ -96,14 +96,14 @@ def sell_arrays(row_ptr, cols, w, C=32, sigma=1):
     sc = np.zeros(int(slice_ptr[-1]), dtype=np.int32)
     sw = np.zeros(int(slice_ptr[-1]), dtype=np.float64)
     starts = np.asarray(row_ptr[:-1], dtype=np.int64)
-    for pos in range(rows):
-        r = perm[pos]
-        s, lane = divmod(pos, C)
-        L = rl[r]
-        if L:
-            slots = slice_ptr[s] + np.arange(L) * C + lane
-            sc[slots] = cols[starts[r]:starts[r] + L]
-            sw[slots] = w[starts[r]:starts[r] + L]
+    pos = np.repeat(np.arange(rows, dtype=np.int64), rl_sorted)          # sorted position
+    first = np.zeros(rows + 1, dtype=np.int64)
+    np.cumsum(rl_sorted, out=first[1:])
+    k = np.arange(pos.size, dtype=np.int64) - np.repeat(first[:-1], rl_sorted)
+    slot = slice_ptr[pos // C] + k * C + pos % C
+    src = np.repeat(starts[perm], rl_sorted) + k
+    sc[slot] = cols[src]
+    sw[slot] = w[src]
     return dict(slice_ptr=slice_ptr[:-1].astype(np.int32), slice_len=slice_len, cols=sc, w=sw,
                 row_len=rl_sorted.astype(np.int32), perm=perm.astype(np.int32), nslices=nsl)
 
@@ -140,14 +140,27 @@ def bsr_arrays(post_rank, row_ptr, cols, w, n_pre, tile):
 
 
 def select_format(proj, compiled) -> str:
-    """Format used for storage_format='auto': the reference's heuristic for
-    rate-coded projections on the GPU (ANNarchy/core/Projection.py:691-789):
-    mean row length <= 128 -> SELL (ELL-R when plastic), else CSR. The learned
-    selector, when trained, overrides it (annarchy_b200.tuning)."""
+    """Format used for storage_format='auto'. Single precision: the learned
+    selector (annarchy_b200.selector, trained on the simulator's own timings)
+    picks the schedule and sets its parameter (SELL window, BSR tile) in the
+    projection's layout. Otherwise, or without a trained model, the
+    reference's rule for rate-coded projections on the GPU
+    (ANNarchy/core/Projection.py:691-789): mean row length <= 128 -> SELL
+    (ELL-R when plastic), else CSR."""
     sched = getattr(proj, "_schedule", None)
     if sched:
         return sched
     m = proj._csr
+    if not compiled.exact and not proj.plastic and not compiled.net._config.get("no_selector"):
+        from .. import selector
+        model = selector.default_model()
+        if model is not None:
+            s = model.choose(m)
+            if "sell_sigma" in s:
+                proj._sell_sigma = s["sell_sigma"]
+            if "bsr_tile" in s:
+                proj._bsr_tile_size = s["bsr_tile"]
+            return s["format"]
     mean = m.nnz / max(1, (np.diff(m.indptr) > 0).sum())
     if mean <= 128:
         return "ellr" if proj.plastic else "sell"
@@ -167,7 +180,8 @@ def create_format_arrays(compiled, proj, fmt, post_rank, row_ptr, cols, w, lay):
         lay["width"] = width
     elif fmt == "sell":
         C = 32
-        sigma = int(proj.net._config.get("sell_sigma", 1024)) if not compiled.exact else 1
+        sigma = int(getattr(proj, "_sell_sigma", 0) or proj.net._config.get("sell_sigma", 1024))
+        sigma = 1 if compiled.exact else sigma
         d = sell_arrays(row_ptr, cols, w, C=C, sigma=sigma)
         nat.create(f"proj{k}__slice_ptr", d["slice_ptr"])
         nat.create(f"proj{k}__slice_len", d["slice_len"])

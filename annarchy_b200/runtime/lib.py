@@ -57,6 +57,14 @@ SIGNATURES = {
     "anb_kernel_time_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "anb_kernel_time_get": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t,
                                       C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "anb_selector_last_error": (C.c_char_p, []),
+    "anb_mlp_param_count": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    "anb_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "anb_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]),
+    "anb_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_void_p]),
 }
 
 _lib = None
@@ -94,6 +102,12 @@ def load():
 def check(fn: str, status: int):
     if status != ANB_OK:
         msg = load().anb_last_error()
+        raise BackendError(fn, status, msg.decode(errors="replace") if msg else "")
+
+
+def check_selector(fn: str, status: int):
+    if status != ANB_OK:
+        msg = load().anb_selector_last_error()
         raise BackendError(fn, status, msg.decode(errors="replace") if msg else "")
 
 

@@ -153,13 +153,19 @@ class Autotuner:
                 self.records = json.load(f)
 
     def tune(self, m: sp.csr_matrix, precision="float", weight_dtype="float32", reps=5,
-             schedules=None, tag: str = ""):
+             schedules=None, tag: str = "", extra=()):
+        """Time every feasible schedule (and every schedule in `extra` whose
+        storage stays within 64x the synapse count); returns (best, {name: ms})."""
         wb = {"float32": 4, "bfloat16": 2, "float64": 8}[weight_dtype if precision == "float"
                                                          else "float64"]
         feat = features(m, wb)
         table = {}
-        for s in schedules or SCHEDULES:
-            if not feasible(m, s):
+        cands = list(schedules or SCHEDULES)
+        for e in extra:
+            if e not in cands and feasible(m, e, 64.0):
+                cands.append(e)
+        for s in cands:
+            if not (feasible(m, s) or s in extra):
                 continue
             ms = measure(m, s, precision, weight_dtype, reps)
             table[schedule_name(s)] = ms

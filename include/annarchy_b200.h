@@ -155,6 +155,26 @@ int anb_kernel_time_count(anb_net* net, int* count);
 int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len,
                         double* total_ms, int64_t* launches);
 
+/* ---- learned storage-format selector -----------------------------------
+ * No counterpart in the reference (it uses a fixed rule,
+ * ANNarchy/core/Projection.py:691-789). A multilayer perceptron
+ * in -> hidden (ReLU) -> hidden (ReLU) -> out maps matrix features to the
+ * predicted log10 time of every candidate schedule. Parameters are one float
+ * vector W1[hidden][in], b1, W2[hidden][hidden], b2, W3[out][hidden], b3
+ * (anb_mlp_param_count floats). All pointers are host pointers; the
+ * functions allocate their device buffers themselves. mask[n][out] is 1 for
+ * measured targets and 0 otherwise; the loss is the masked mean squared
+ * error. Errors: anb_selector_last_error(). */
+const char* anb_selector_last_error(void);
+size_t anb_mlp_param_count(int in, int hidden, int out);
+int anb_mlp_loss_grad(const float* params, const float* x, const float* target, const float* mask,
+                      int n, int in, int hidden, int out, float* loss, float* grad);
+int anb_mlp_train(float* params, const float* x, const float* target, const float* mask, int n,
+                  int in, int hidden, int out, int epochs, float lr, float weight_decay,
+                  float* final_loss);
+int anb_mlp_predict(const float* params, const float* x, int n, int in, int hidden, int out,
+                    float* y);
+
 #ifdef __cplusplus
 }
 #endif
