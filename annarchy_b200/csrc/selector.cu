@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -299,6 +300,88 @@ int anb_mlp_predict(const float* params, const float* x, int n, int in, int hidd
   forward(D, p, s, n, 0);
   SEL_CUDA(cudaGetLastError());
   SEL_CUDA(cudaMemcpy(y, s.y, (size_t)n * out * sizeof(float), cudaMemcpyDeviceToHost));
+  return ANB_OK;
+}
+
+}  // extern "C"
+
+// ---- forward pass without allocation ------------------------------------
+//
+// anb_mlp_predict above allocates device buffers on every call. Some callers
+// cannot do that: a simulation loop with real-time deadlines, where the
+// implicit device synchronisation of cudaMalloc/cudaFree would stall it, and
+// host programs whose device memory is owned by another allocator (a memory
+// pool or a framework's caching allocator) that forbids allocations outside
+// it. They pass device buffers they already own for the parameters, the
+// inputs and the outputs; the two hidden-layer activations go to the fixed
+// array below instead of freshly allocated memory.
+//
+// The array is part of this library's device image: every GPU that loads the
+// library holds it (2 MiB) until the process exits. All calls share it and it
+// keeps the last call's contents; the forward pass overwrites every element
+// it reads, so nothing needs clearing. Calls whose work overlaps on the GPU
+// (different streams, or different host threads on one device) race on it.
+
+constexpr size_t kNoAllocScratchFloats = (size_t)1 << 19;  // 2 MiB of float
+static __device__ __align__(256) float anb_mlp_noalloc_scratch[kNoAllocScratchFloats];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device. In host code
+// the array's name only stands for the symbol; the address must come from
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch(float** out) {
+  int dev = 0;
+  SEL_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return sel_fail(ANB_ERR_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, anb_mlp_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return sel_fail(ANB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
+                                        cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return ANB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t anb_mlp_noalloc_max_floats(void) { return kNoAllocScratchFloats; }
+
+int anb_mlp_predict_noalloc(const float* params, const float* x, int n, int in, int hidden, int out,
+                            float* y, void* stream) {
+  int rc = check_dims(n, in, hidden, out);
+  if (rc) return rc;
+  if (!params || !x || !y) return sel_fail(ANB_ERR_ARG, "NULL argument");
+  const size_t need = 2 * (size_t)n * (size_t)hidden;
+  if (need > kNoAllocScratchFloats)
+    return sel_fail(ANB_ERR_ARG, "anb_mlp_predict_noalloc: n * hidden = " +
+                                     std::to_string((size_t)n * hidden) + " exceeds the limit of " +
+                                     std::to_string(kNoAllocScratchFloats / 2) +
+                                     " activations per layer");
+  float* scratch = nullptr;
+  rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  Dims D{in, hidden, out};
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float* h1 = scratch;
+  float* h2 = scratch + (size_t)n * hidden;
+  linear_fwd<<<blocks((size_t)n * D.hidden), 256, 0, st>>>(x, params + D.w1(), params + D.b1(), h1,
+                                                           n, D.in, D.hidden, 1);
+  linear_fwd<<<blocks((size_t)n * D.hidden), 256, 0, st>>>(h1, params + D.w2(), params + D.b2(),
+                                                           h2, n, D.hidden, D.hidden, 1);
+  linear_fwd<<<blocks((size_t)n * D.out), 256, 0, st>>>(h2, params + D.w3(), params + D.b3(), y, n,
+                                                        D.hidden, D.out, 0);
+  SEL_CUDA(cudaGetLastError());
   return ANB_OK;
 }
 

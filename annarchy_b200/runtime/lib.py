@@ -65,6 +65,9 @@ SIGNATURES = {
                                 C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]),
     "anb_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_void_p]),
+    "anb_mlp_noalloc_max_floats": (C.c_size_t, []),
+    "anb_mlp_predict_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -175,6 +175,23 @@ int anb_mlp_train(float* params, const float* x, const float* target, const floa
 int anb_mlp_predict(const float* params, const float* x, int n, int in, int hidden, int out,
                     float* y);
 
+/* Forward pass of the selector network that allocates no memory; it has no
+ * counterpart in the reference. For callers that cannot call cudaMalloc: a
+ * simulation loop with real-time deadlines, where the implicit device
+ * synchronisation of an allocation would stall it, or a host program whose
+ * device memory belongs to another allocator (a pool or a framework's caching
+ * allocator). params, x and y are DEVICE pointers owned by the caller;
+ * `stream` is a cudaStream_t (NULL: the default stream); the call only
+ * queues work. The hidden activations live in a fixed array inside this
+ * library (2 MiB on every GPU that loads it, held until exit), so
+ * n * hidden must not exceed anb_mlp_noalloc_max_floats() / 2 (ANB_ERR_ARG
+ * otherwise). The first call on a device looks up that array's device
+ * address; make it before any stream capture. All calls share the array:
+ * calls whose work overlaps on the GPU race. */
+size_t anb_mlp_noalloc_max_floats(void);
+int anb_mlp_predict_noalloc(const float* params, const float* x, int n, int in, int hidden, int out,
+                            float* y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
