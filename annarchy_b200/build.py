@@ -47,7 +47,7 @@ def _sources(*rel):
 def build_runtime(force=False, verbose=False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     out = os.path.join(LIB_DIR, "libannarchy_b200.so")
-    srcs = _sources("runtime.cu", "selector.cu") + [
+    srcs = _sources("runtime.cu", "selector.cu", "connect.cuh") + [
         os.path.join(os.path.dirname(HERE), "include", "annarchy_b200.h")]
     srcs = [s for s in srcs if os.path.exists(s)]
     if force or _newer(out, srcs):

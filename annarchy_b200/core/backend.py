@@ -56,6 +56,7 @@ class CompiledNetwork:
         self.layout: dict[int, dict] = {}
         self.mon_layout: dict[int, dict] = {}
         self.local_layout = None
+        self.spike_lists = False
         self._col_ptr: dict[int, np.ndarray] = {}
         self.engine = None
         self.module = None
@@ -72,11 +73,13 @@ class CompiledNetwork:
         net = self.net
         nat = self.native
         nat.initialize(net.dt)
+        self.engine = self._choose_engine()
+        # fast grid engine: per-step spike lists drive the event kernels
+        self.spike_lists = (not self.exact and self.engine == "grid")
         for pop in net.populations:
             self._create_population(pop)
         for proj in net.projections:
             self._create_projection(proj)
-        self.engine = self._choose_engine()
         for mon in net.monitors:
             self._create_monitor(mon)
         if self.engine == "local":
@@ -147,6 +150,8 @@ class CompiledNetwork:
             return False, "rate-coded populations"
         if any(p.synapse_type.type != "spike" or p.plastic for p in net.projections):
             return False, "plastic or rate-coded projections"
+        if any(getattr(p, "_device_conn", None) for p in net.projections):
+            return False, "device-generated connectivity"
         if any(v != "spike" for m in net.monitors for v in m.variables):
             return False, "variable monitors"
         smem = self._local_smem_bytes()
@@ -311,13 +316,68 @@ class CompiledNetwork:
         if pop.neuron_type.type == "spike":
             n = pop.size
             nat.create(f"pop{pop.id}__spk", np.zeros((n + 31) // 32, dtype=np.uint32))
+            if self.spike_lists:
+                nat.create_empty(f"pop{pop.id}__spl", np.int32, (2 * n,))
+                nat.create(f"pop{pop.id}__spn", np.zeros(2, dtype=np.int32))
             nat.create(f"pop{pop.id}__refractory", pop.refractory_steps.astype(np.int32))
             nat.create(f"pop{pop.id}__refractory_remaining", np.zeros(n, dtype=np.int32))
             nat.create(f"pop{pop.id}__last_spike", np.full(n, -10000, dtype=np.int64))
 
+    def _syn_local_names(self, proj):
+        names = [v["name"] for v in proj.desc["variables"]
+                 if v["locality"] == "local" and v["name"] != "w"]
+        for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
+            if v["name"] not in names and v["name"] not in ("w", "g_target"):
+                names.append(v["name"])
+        return names
+
+    def _create_device_projection(self, proj):
+        """Fixed in-degree projection generated on the device."""
+        nat = self.native
+        k = proj.id
+        d = proj._device_conn
+        if proj.synapse_type.type != "spike":
+            raise NotImplementedError("device connectors are implemented for spiking projections")
+        npost = len(proj.post_ranks_view)
+        pre_lo, pre_hi = int(proj.pre_ranks[0]), int(proj.pre_ranks[-1]) + 1
+        plastic = proj.plastic
+        wdt = np.float64 if self.exact else (np.float32 if plastic else self.wdtype)
+        nat.connect_fixed_number_pre(f"proj{k}", npost, int(proj.post_ranks_view[0]), pre_lo, pre_hi,
+                                     d["number"], d["seed"], d["wkind"], d["a"], d["b"], wdt,
+                                     d["exclude_self"])
+        nnz = npost * d["number"]
+        lay = {"rows": npost, "nnz": nnz, "idx_t": "int", "format": "csr", "device": True,
+               "w0": pre_lo // 32, "w1": (pre_hi - 1) // 32 + 1}
+        for prm in proj.desc["parameters"] + proj.desc["variables"]:
+            if prm["locality"] == "global":
+                nat.create(f"proj{k}__{prm['name']}", np.array([prm["init"]], dtype=self.real))
+        if not self.exact:
+            nat.csr_to_csc(f"proj{k}", proj.pre_pop.size, with_weights=not plastic)
+        mean_fan = nnz / max(1, pre_hi - pre_lo)
+        lay["chunks"] = max(1, -(-int(1.25 * mean_fan) // 32))
+        lay["post_chunks"] = max(1, -(-d["number"] // 32))
+        if plastic and self.spike_lists:
+            row_of = np.full(proj.post_pop.size, -1, dtype=np.int32)
+            base = int(proj.post_ranks_view[0])
+            row_of[base:base + npost] = np.arange(npost, dtype=np.int32)
+            nat.create(f"proj{k}__row_of", row_of)
+        if self.exact or plastic:
+            lay["grid"] = grid_for(npost * 32)
+        else:
+            lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
+        if plastic:
+            nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
+            for name in self._syn_local_names(proj):
+                nat.create_empty(f"proj{k}__{name}", self.real, (nnz,))
+            nat.create_empty(f"proj{k}___last_event", np.int64, (nnz,))
+            nat.fill(f"proj{k}___last_event", np.int64(-10000))
+        self.layout[k] = lay
+
     def _create_projection(self, proj):
         nat = self.native
         k = proj.id
+        if getattr(proj, "_device_conn", None):
+            return self._create_device_projection(proj)
         if proj._csr is None:
             raise RuntimeError(f"projection {proj.name} has no connectivity (call a connector)")
         post_rank, row_ptr, cols, w = proj.csr_population_ranks()
@@ -365,8 +425,15 @@ class CompiledNetwork:
                 nat.create(f"proj{k}__w_pre", self._w(w[order]) if not self.exact else w[order])
             lay["w0"] = int(proj.pre_ranks.min()) // 32
             lay["w1"] = int(proj.pre_ranks.max()) // 32 + 1
+            fan = np.diff(col_ptr)
+            lay["chunks"] = max(1, -(-int(fan.max() if fan.size else 1) // 32))
+            lay["post_chunks"] = max(1, -(-int(np.diff(row_ptr).max() if rows else 1) // 32))
+            if proj.plastic and self.spike_lists:
+                row_of = np.full(proj.post_pop.size, -1, dtype=np.int32)
+                row_of[post_rank] = np.arange(rows, dtype=np.int32)
+                nat.create(f"proj{k}__row_of", row_of)
             if self.exact or proj.plastic:
-                lay["grid"] = grid_for(rows)
+                lay["grid"] = grid_for(rows * (32 if self.exact else 1))
             else:
                 lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
             if proj.plastic:

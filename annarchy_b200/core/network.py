@@ -156,7 +156,12 @@ class Network:
         return self.current_step * self.dt
 
     def set_current_step(self, t: int):
-        self._backend.native.set_time(int(t))
+        nat = self._backend.native
+        nat.set_time(int(t))
+        # the spike lists are indexed by step parity: a new time starts them empty
+        for pop in self.populations:
+            if f"pop{pop.id}__spn" in nat.arrays:
+                nat.zero(f"pop{pop.id}__spn")
 
     def set_time(self, t: float):
         self.set_current_step(int(round(t / self.dt)))

@@ -61,6 +61,8 @@ class Projection:
         self.post_ranks_view = _ranks(post)
         self._csr: sp.csr_matrix | None = None   # (n_post_view, n_pre_view), view-relative
         self._storage_format = "csr"
+        self._device_conn = None
+        self._nnz = 0
         self._host_attr: dict[str, np.ndarray] = {}
         self.connector_name = None
         self._schedule = None
@@ -68,6 +70,8 @@ class Projection:
     # -- properties -------------------------------------------------------------
     @property
     def nb_synapses(self) -> int:
+        if getattr(self, "_device_conn", None):
+            return int(self._nnz)
         return 0 if self._csr is None else int(self._csr.nnz)
 
     def __len__(self):
@@ -186,11 +190,45 @@ class Projection:
         m = sp.csr_matrix((w, (rows, cols)), shape=(npost, npre))
         return self._store(m, "Random", storage_format, delays)
 
+    def _device_ok(self, nnz: int) -> bool:
+        mode = self.net._config.get("device_connectors", "auto") if self.net is not None else False
+        contiguous = (np.all(np.diff(self.pre_ranks) == 1) and np.all(np.diff(self.post_ranks_view) == 1))
+        if mode is True or mode == "always":
+            if not contiguous:
+                raise NotImplementedError("device connectors need contiguous pre and post ranks")
+            return True
+        return mode == "auto" and nnz > 20_000_000 and contiguous
+
     def fixed_number_pre(self, number, weights, delays=0.0, allow_self_connections=False,
                          force_multiple_weights=False, storage_format=None, storage_order=None):
-        """Every post neuron receives exactly `number` distinct pre neurons."""
+        """Every post neuron receives exactly `number` distinct pre neurons.
+
+        Large projections (more than 2e7 synapses, or device_connectors=True)
+        are generated on the device at compile(): one pre neuron per equal
+        stratum of the pre range (anb_connect_fixed_number_pre)."""
         rng = self._rng()
         npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
+        if self._device_ok(npost * int(number)):
+            from .random import Normal, Uniform
+            if np.ndim(weights) == 0 and not hasattr(weights, "get_values"):
+                wk, a, b = 0, float(weights), 0.0
+            elif isinstance(weights, Uniform):
+                wk, a, b = 1, weights.min, weights.max
+            elif isinstance(weights, Normal) and weights.min is None and weights.max is None:
+                wk, a, b = 2, weights.mu, weights.sigma
+            else:
+                raise NotImplementedError("device connectors take constant, Uniform or Normal weights")
+            if delays not in (0, 0.0, None):
+                raise NotImplementedError("synaptic delays are not supported by this backend")
+            self._device_conn = dict(kind="fixed_number_pre", number=int(number), wkind=wk, a=a, b=b,
+                                     seed=int(rng.integers(0, 2**63 - 1)),
+                                     exclude_self=(not allow_self_connections
+                                                   and self.pre_pop is self.post_pop))
+            self._nnz = npost * int(number)
+            self.connector_name = "Random Convergent (device)"
+            if storage_format is not None:
+                self._storage_format = storage_format
+            return self
         avail = npre - (0 if allow_self_connections or self.pre_pop is not self.post_pop else 1)
         if number > avail:
             raise ValueError("fixed_number_pre: number exceeds the available pre-synaptic neurons")
@@ -262,6 +300,8 @@ class Projection:
             flat_v = self._host_attr[name].copy()
         if flat:
             return flat_v
+        if getattr(self, "_device_conn", None):
+            return np.split(flat_v, len(self.post_ranks_view))
         lengths = np.diff(self._csr.indptr)
         lengths = lengths[lengths > 0]
         return [a for a in np.split(flat_v, np.cumsum(lengths)[:-1])]
@@ -292,7 +332,8 @@ class Projection:
 
     def __setattr__(self, name, value):
         desc = self.__dict__.get("desc")
-        if desc is not None and self.__dict__.get("_csr") is not None and (
+        if desc is not None and (self.__dict__.get("_csr") is not None or
+                                 self.__dict__.get("_device_conn")) and (
                 name == "w" or name in self.__dict__.get("_host_attr", {})):
             self.set({name: value})
             return

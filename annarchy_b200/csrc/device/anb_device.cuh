@@ -472,6 +472,40 @@ __device__ __forceinline__ void anb_spike_gather(int n_rows, const int* __restri
   }
 }
 
+// Exact gather, warp per post row: lanes test 32 synapses at a time; the
+// spiking ones are added in ascending pre rank (set bits of the ballot in
+// order), which is the reference's per-post order.
+template <typename R, typename W>
+__device__ __forceinline__ void anb_spike_gather_warp(int n_rows, const int* __restrict__ row_ptr,
+                                                      const int* __restrict__ col,
+                                                      const W* __restrict__ w,
+                                                      const anb_u32* __restrict__ spk,
+                                                      const int* __restrict__ post_rank,
+                                                      R* __restrict__ g) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int row = warp; row < n_rows; row += nwarps) {
+    const int beg = row_ptr[row], end = row_ptr[row + 1];
+    const int post = post_rank ? post_rank[row] : row;
+    R acc = g[post];
+    bool any = false;
+    for (int base = beg; base < end; base += 32) {
+      const int j = base + lane;
+      const bool sp = j < end && anb_bit(spk, col[j]);
+      anb_u32 m = __ballot_sync(0xffffffffu, sp);
+      any |= m != 0u;
+      const R wj = sp ? (R)w[j] : R(0);
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        acc += __shfl_sync(0xffffffffu, wj, b);
+      }
+    }
+    if (any && lane == 0) g[post] = acc;
+  }
+}
+
 // Fast scatter: a warp per 32-neuron bitmap word of the pre population
 // (words [w0, w1)); for every set bit the warp walks that neuron's outgoing
 // synapses (pre-major: col_ptr / post_idx / w_pre) and adds w to g[post]
@@ -532,6 +566,29 @@ __device__ __forceinline__ void anb_cluster_st_u32(unsigned addr, anb_u32 v) {
 __device__ __forceinline__ void anb_cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
                    : "memory");
+}
+
+// Fast scatter from a spike list: work item = (spike, 32-synapse chunk of its
+// fan-out), so a warp does one pass per item whatever the fan-out; spikes
+// outside [lo, hi) (not pre neurons of this projection) are skipped.
+template <typename R, typename W>
+__device__ __forceinline__ void anb_spike_scatter_list(int lo, int hi, const int* __restrict__ list,
+                                                       int count, int chunks,
+                                                       const int* __restrict__ col_ptr,
+                                                       const int* __restrict__ post_idx,
+                                                       const W* __restrict__ w_pre,
+                                                       R* __restrict__ g) {
+  const int lane = threadIdx.x & 31;
+  const long long items = (long long)count * chunks;
+  for (long long it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items;
+       it += (gridDim.x * blockDim.x) >> 5) {
+    const int pre = list[it / chunks];
+    if (pre < lo || pre >= hi) continue;
+    const int c = (int)(it % chunks);
+    const int end = col_ptr[pre + 1];
+    for (int q = col_ptr[pre] + c * 32 + lane; q < end; q += 32 * chunks)
+      atomicAdd(&g[post_idx[q]], (R)anb_wf(w_pre[q]));
+  }
 }
 
 // ---- monitors ---------------------------------------------------------------------------

@@ -800,3 +800,6 @@ int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len, do
 }
 
 }  // extern "C"
+
+// device-side connectivity construction (uses the helpers above)
+#include "connect.cuh"

@@ -281,7 +281,23 @@ class CodeGenerator:
         spk_dst = ((smem.get("spk") if smem else gsrc("spk")) if spiking and ballot_hook is None
                    else None)
         ballot = ""
-        if spiking and cluster is not None and ballot_hook is not None:
+        listed = (spiking and cluster is None and not local_engine and not self.exact
+                  and self.c.spike_lists)
+        if listed:
+            spl, spn = gsrc("spl"), gsrc("spn")
+            ballot = f"""
+      {{
+        const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
+        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {spk_dst}[anb_i >> 5] = anb_m;
+        if (anb_m) {{   // append to this step's spike list (warp-aggregated)
+          int anb_pos = 0;
+          if ((threadIdx.x & 31) == 0) anb_pos = atomicAdd(&{spn}[t & 1], __popc(anb_m));
+          anb_pos = __shfl_sync(0xffffffffu, anb_pos, 0);
+          if (anb_spiked)
+            {spl}[(t & 1) * (long long)anb_n + anb_pos + __popc(anb_m & ((1u << (threadIdx.x & 31)) - 1u))] = anb_i;
+        }}
+      }}"""
+        elif spiking and cluster is not None and ballot_hook is not None:
             ballot = ballot_hook
         elif spiking:
             widx, lim = ("anb_q", "anb_cnt") if cluster is not None else ("anb_i", "anb_n")
@@ -443,8 +459,20 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp_tail() {{
         if proj.plastic:
             return self.plastic_psp_kernel(proj, lay, pre_spk, g)
         if self.exact:
-            call = (f"anb_spike_gather<double, double>({lay['rows']}, {p('row_ptr')}, {p('col')}, "
+            call = (f"anb_spike_gather_warp<double, double>({lay['rows']}, {p('row_ptr')}, {p('col')}, "
                     f"{p('w')}, {pre_spk}, {p('post_rank')}, {g});")
+        elif self.c.spike_lists:
+            a = proj.pre_pop.id
+            call = (f"anb_spike_scatter_list<float, {self.c.wctype}>({lay['w0'] * 32}, {lay['w1'] * 32}, "
+                    f"{self.ptr(f'pop{a}__spl')} + ((t - 1) & 1) * (long long){proj.pre_pop.size}, "
+                    f"{self.ptr(f'pop{a}__spn')}[(t - 1) & 1], {lay['chunks']}, {p('col_ptr')}, "
+                    f"{p('post_idx')}, {p('w_pre')}, {g});")
+            return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    const long long t = *{self.ptr('t')};
+    {call}
+}}
+"""
         else:
             call = (f"anb_spike_scatter<float, {self.c.wctype}>({lay['w0']}, {lay['w1']}, {pre_spk}, "
                     f"{p('col_ptr')}, {p('post_idx')}, {p('w_pre')}, {g});")
@@ -494,7 +522,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
             stmts.append(self.typed(code))
         body = "\n          ".join(stmts)
         if self.exact:
-            # post-centric, ordered: pre spikes of a row in ascending pre rank
+            # warp per post row; the spiking synapses of a row are processed in
+            # ascending pre rank, one at a time, by the lane that holds them
+            # (the running conductance `sum` is passed along with a shuffle)
             return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     const long long t = *{self.ptr('t')};
@@ -502,20 +532,34 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     const int anb_plastic = {p('flags')}[0];
     {self._syn_globals(proj)}
     {self._syn_arrays(proj)}
-    for (int anb_row = blockIdx.x * blockDim.x + threadIdx.x; anb_row < {lay['rows']};
-         anb_row += gridDim.x * blockDim.x) {{
+    const int anb_lane = threadIdx.x & 31;
+    for (int anb_row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_row < {lay['rows']};
+         anb_row += (gridDim.x * blockDim.x) >> 5) {{
       const int anb_post = {p('post_rank')}[anb_row];
+      const int anb_beg = {p('row_ptr')}[anb_row], anb_end = {p('row_ptr')}[anb_row + 1];
       double sum = {g}[anb_post];
-      for (int j = {p('row_ptr')}[anb_row]; j < {p('row_ptr')}[anb_row + 1]; ++j) {{
-        if (anb_bit({pre_spk}, {p('col')}[j])) {{
-          {body}
+      bool anb_any = false;
+      for (int anb_b0 = anb_beg; anb_b0 < anb_end; anb_b0 += 32) {{
+        const int j = anb_b0 + anb_lane;
+        const bool anb_sp = j < anb_end && anb_bit({pre_spk}, {p('col')}[j]);
+        anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_sp);
+        anb_any |= anb_m != 0u;
+        while (anb_m) {{
+          const int anb_b = __ffs(anb_m) - 1;
+          anb_m &= anb_m - 1;
+          if (anb_lane == anb_b) {{
+            {body}
+          }}
+          sum = __shfl_sync(0xffffffffu, sum, anb_b);
         }}
       }}
-      {g}[anb_post] = sum;
+      if (anb_any && anb_lane == 0) {g}[anb_post] = sum;
     }}
 }}
 """
-        # fast: warp per spiking pre neuron, synapse index through inv_idx
+        # fast: work items (spike of the previous step, 32-synapse chunk of its
+        # fan-out); the synapse state is reached through inv_idx
+        a = proj.pre_pop.id
         return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     const long long t = *{self.ptr('t')};
@@ -526,19 +570,19 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int word = {lay['w0']} + warp; word < {lay['w1']}; word += nwarps) {{
-      anb_u32 m = {pre_spk}[word];
-      while (m) {{
-        const int b = __ffs(m) - 1;
-        m &= m - 1;
-        const int anb_pre = (word << 5) + b;
-        const int anb_beg = {p('col_ptr')}[anb_pre], anb_end = {p('col_ptr')}[anb_pre + 1];
-        for (int anb_k = anb_beg + lane; anb_k < anb_end; anb_k += 32) {{
-          const int j = {p('inv_idx')}[anb_k];
-          float sum = 0.f;
-          {body}
-          atomicAdd(&{g}[{p('post_idx')}[anb_k]], sum);
-        }}
+    const int* __restrict__ anb_list = {self.ptr(f'pop{a}__spl')} + ((t - 1) & 1) * (long long){proj.pre_pop.size};
+    const long long anb_items = (long long){self.ptr(f'pop{a}__spn')}[(t - 1) & 1] * {lay['chunks']};
+    for (long long anb_it = warp; anb_it < anb_items; anb_it += nwarps) {{
+      const int anb_pre = anb_list[anb_it / {lay['chunks']}];
+      if (anb_pre < {lay['w0'] * 32} || anb_pre >= {lay['w1'] * 32}) continue;
+      const int anb_c = (int)(anb_it % {lay['chunks']});
+      const int anb_end = {p('col_ptr')}[anb_pre + 1];
+      for (int anb_k = {p('col_ptr')}[anb_pre] + anb_c * 32 + lane; anb_k < anb_end;
+           anb_k += 32 * {lay['chunks']}) {{
+        const int j = {p('inv_idx')}[anb_k];
+        float sum = 0.f;
+        {body}
+        atomicAdd(&{g}[{p('post_idx')}[anb_k]], sum);
       }}
     }}
 }}
@@ -557,6 +601,31 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
             stmts.append(self.typed(code))
         body = "\n        ".join(stmts)
         dt_t = "double" if self.exact else "float"
+        if not self.exact and self.c.spike_lists:
+            b = proj.post_pop.id
+            ch = lay["post_chunks"]
+            return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
+    const long long t = *{self.ptr('t')};
+    const float dt = (float)(*{self.ptr('dt')});
+    const int anb_plastic = {p('flags')}[0];
+    {self._syn_globals(proj)}
+    {self._syn_arrays(proj)}
+    const int anb_lane = threadIdx.x & 31;
+    const int* __restrict__ anb_list = {self.ptr(f'pop{b}__spl')} + (t & 1) * (long long){proj.post_pop.size};
+    const long long anb_items = (long long){self.ptr(f'pop{b}__spn')}[t & 1] * {ch};
+    for (long long anb_it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_it < anb_items;
+         anb_it += (gridDim.x * blockDim.x) >> 5) {{
+      const int anb_row = {p('row_of')}[anb_list[anb_it / {ch}]];
+      if (anb_row < 0) continue;
+      const int anb_c = (int)(anb_it % {ch});
+      const int anb_end = {p('row_ptr')}[anb_row + 1];
+      for (int j = {p('row_ptr')}[anb_row] + anb_c * 32 + anb_lane; j < anb_end; j += 32 * {ch}) {{
+        {body}
+      }}
+    }}
+}}
+"""
         return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
     const long long t = *{self.ptr('t')};
@@ -564,11 +633,12 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
     const int anb_plastic = {p('flags')}[0];
     {self._syn_globals(proj)}
     {self._syn_arrays(proj)}
-    for (int anb_row = blockIdx.x * blockDim.x + threadIdx.x; anb_row < {lay['rows']};
-         anb_row += gridDim.x * blockDim.x) {{
+    const int anb_lane = threadIdx.x & 31;
+    for (int anb_row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_row < {lay['rows']};
+         anb_row += (gridDim.x * blockDim.x) >> 5) {{
       const int anb_post = {p('post_rank')}[anb_row];
-      if (!anb_bit({post_spk}, anb_post)) continue;
-      for (int j = {p('row_ptr')}[anb_row]; j < {p('row_ptr')}[anb_row + 1]; ++j) {{
+      if (!anb_bit({post_spk}, anb_post)) continue;           // warp-uniform
+      for (int j = {p('row_ptr')}[anb_row] + anb_lane; j < {p('row_ptr')}[anb_row + 1]; j += 32) {{
         {body}
       }}
     }}
@@ -634,15 +704,23 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
         for proj in net.projections:
             if proj.synapse_type.type == "spike" and proj.desc.get("post_spike"):
                 kernels.append(self.post_event_kernel(proj))
-                plan.append((f"proj{proj.id}_post_event", grid_for(self.c.layout[proj.id]["rows"]),
-                             BLOCK, 0))
+                plan.append((f"proj{proj.id}_post_event",
+                             grid_for(self.c.layout[proj.id]["rows"] * 32), BLOCK, 0))
         for mon in net.monitors:
             kernels.append(self.monitor_kernel(mon))
             n = self.c.mon_layout[mon.id]["n"]
             plan.append((f"mon{mon.id}_record", grid_for(max(n, 32)), BLOCK, 0))
+        resets = ""
+        if self.c.spike_lists:
+            for pop in net.populations:
+                if pop.neuron_type.type == "spike":
+                    resets += f" {self.ptr(f'pop{pop.id}__spn')}[(t + 1) & 1] = 0;"
         kernels.append(f"""
 extern "C" __global__ void anb_tick() {{
-    if (blockIdx.x == 0 && threadIdx.x == 0) *{self.ptr('t')} += 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {{
+      const long long t = *{self.ptr('t')};{resets}
+      *{self.ptr('t')} = t + 1;
+    }}
 }}
 """)
         plan.append(("anb_tick", 1, 32, 0))

@@ -37,6 +37,11 @@ SIGNATURES = {
     "anb_array_info": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p),
                                  C.POINTER(C.c_size_t)]),
     "anb_module_load": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
+    "anb_array_fill": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),
+    "anb_connect_fixed_number_pre": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int,
+                                               C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_double,
+                                               C.c_double, C.c_int, C.c_int]),
+    "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
     "anb_bitmap_decode": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p,
@@ -231,6 +236,34 @@ class NativeNet:
         check("anb_array_free", self.lib.anb_array_free(self.h, name.encode()))
         self.arrays.pop(name, None)
 
+    def fill(self, name: str, value):
+        v = np.asarray(value)
+        check("anb_array_fill", self.lib.anb_array_fill(self.h, name.encode(),
+                                                       v.ctypes.data_as(C.c_void_p), v.nbytes))
+
+    def connect_fixed_number_pre(self, prefix, n_post, post_base, pre_lo, pre_hi, number, seed,
+                                 weight_kind, a, b, weight_dtype, exclude_self):
+        wb = {np.dtype(np.float64): 8, np.dtype(np.float32): 4, np.dtype(np.uint16): 2}[
+            np.dtype(weight_dtype)]
+        check("anb_connect_fixed_number_pre", self.lib.anb_connect_fixed_number_pre(
+            self.h, prefix.encode(), n_post, post_base, pre_lo, pre_hi, number, seed, weight_kind,
+            float(a), float(b), wb, 1 if exclude_self else 0))
+        nnz = n_post * number
+        self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n_post,))
+        self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))
+        self.arrays[prefix + "__col"] = (np.dtype(np.int32), (nnz,))
+        self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (nnz,))
+
+    def csr_to_csc(self, prefix, n_pre, with_weights):
+        check("anb_csr_to_csc", self.lib.anb_csr_to_csc(self.h, prefix.encode(), n_pre,
+                                                       1 if with_weights else 0))
+        nnz = self.arrays[prefix + "__col"][1][0]
+        self.arrays[prefix + "__col_ptr"] = (np.dtype(np.int32), (n_pre + 1,))
+        self.arrays[prefix + "__post_idx"] = (np.dtype(np.int32), (nnz,))
+        self.arrays[prefix + "__inv_idx"] = (np.dtype(np.int32), (nnz,))
+        if with_weights:
+            self.arrays[prefix + "__w_pre"] = (self.arrays[prefix + "__w"][0], (nnz,))
+
     # -- module and plan ------------------------------------------------------
     def load_module(self, source: str, options: list[str]):
         check("anb_module_load", self.lib.anb_module_load(self.h, source.encode(),
@@ -306,6 +339,25 @@ class DryNative:
 
     def write(self, *a, **k):
         pass
+
+    def fill(self, name, value):
+        pass
+
+    def connect_fixed_number_pre(self, prefix, n_post, post_base, pre_lo, pre_hi, number, seed,
+                                 weight_kind, a, b, weight_dtype, exclude_self):
+        nnz = n_post * number
+        self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n_post,))
+        self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))
+        self.arrays[prefix + "__col"] = (np.dtype(np.int32), (nnz,))
+        self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (nnz,))
+
+    def csr_to_csc(self, prefix, n_pre, with_weights):
+        nnz = self.arrays[prefix + "__col"][1][0]
+        self.arrays[prefix + "__col_ptr"] = (np.dtype(np.int32), (n_pre + 1,))
+        self.arrays[prefix + "__post_idx"] = (np.dtype(np.int32), (nnz,))
+        self.arrays[prefix + "__inv_idx"] = (np.dtype(np.int32), (nnz,))
+        if with_weights:
+            self.arrays[prefix + "__w_pre"] = (self.arrays[prefix + "__w"][0], (nnz,))
 
     def load_module(self, source, options):
         self.source, self.options = source, options

@@ -319,3 +319,53 @@ def stdp_matrix(cn: CobaNet, seed: int, p: float) -> sp.csr_matrix:
     """Plastic E->E weights U[0, 0.5] of the plastic test network."""
     rng = np.random.default_rng(seed + 1000)
     return bernoulli_csr(rng, cn.n_exc, cn.n_exc, p, lambda k: rng.uniform(0.0, 0.5, k))
+
+
+# ---------------------------------------------------------------------------
+# large plastic spiking network (device-generated connectivity)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class LargeNet:
+    """1M conductance-based LIF neurons (80 % excitatory), every neuron
+    receiving 800 excitatory and 200 inhibitory synapses (1e9 in total);
+    E->E is plastic (pair-based STDP, float weights), the other projections
+    are static. Weights scale the 4000-neuron net's total input to the larger
+    in-degree (0.6 x 64/800 and 6.7 x 16/200)."""
+    n: int = 1_000_000
+    fan_e: int = 800
+    fan_i: int = 200
+    w_exc: float = 0.048
+    w_inh: float = 0.536
+    drive: float = 20.0
+    seed: int = 42
+    steps: int = 1000
+    dt: float = 0.1
+
+    @property
+    def n_exc(self) -> int:
+        return int(round(self.n * 0.8))
+
+    @property
+    def nnz(self) -> int:
+        return self.n * (self.fan_e + self.fan_i)
+
+
+def build_large_network(ln: LargeNet, precision: str = "double", stdp: bool = True,
+                        record: bool = True, **config):
+    """Returns (net, pop, monitor, projections); connectivity is generated on
+    the device at compile()."""
+    from . import STDP, Network, Uniform
+    net = Network(dt=ln.dt, seed=ln.seed)
+    net.config(precision=precision, engine="grid", device_connectors=True, **config)
+    params = dict(COBA_PARAMS)
+    params["I"] = float(ln.drive)
+    P = net.create(ln.n, coba_neuron(params))
+    Pe, Pi = P[: ln.n_exc], P[ln.n_exc:]
+    syn = STDP(**STDP_PARAMS) if stdp else None
+    ee = net.connect(Pe, Pe, "exc", synapse=syn).fixed_number_pre(ln.fan_e, ln.w_exc)
+    ei = net.connect(Pe, Pi, "exc").fixed_number_pre(ln.fan_e, ln.w_exc)
+    ie = net.connect(Pi, P, "inh").fixed_number_pre(ln.fan_i, ln.w_inh)
+    mon = net.monitor(P, "spike") if record else None
+    P.v = np.random.default_rng(ln.seed).uniform(-60.0, -50.0, ln.n)
+    return net, P, mon, (ee, ei, ie)

@@ -283,6 +283,100 @@ def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
     return out
 
 
+def large_study(n=1_000_000, steps=1000):
+    """The 1e9-synapse plastic network: fast path (float state, float plastic
+    weights, bfloat16 static weights) and double path, 1000 steps each with
+    device-generated connectivity. Reports device time, synaptic events per
+    second, per-kernel time and algorithmic bandwidth, firing rates and the
+    E->E weight histograms."""
+    import torch
+    from annarchy_b200 import workloads as wl
+    peak, kind = peaks()
+    ln = wl.LargeNet(n=n, steps=steps)
+    ne = ln.n_exc
+    out = {"config": {"neurons": n, "synapses": ln.nnz, "steps": steps, "dt": ln.dt},
+           "peak_gbs": peak, "peak_source": kind}
+    for prec, kw in (("float", {"weight_dtype": "bfloat16"}), ("double", {})):
+        t0 = time.time()
+        net, P, mon, (ee, ei, ie) = wl.build_large_network(ln, prec, graph_steps=50, **kw)
+        net.compile()
+        build_s = time.time() - t0
+        nat = net._backend.native
+        stream = torch.cuda.Stream()
+        nat.set_stream(stream.cuda_stream)
+        net.simulate_steps(20)                               # warm-up, spikes recorded
+        mon.get("spike")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        net.simulate_steps(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        s_steps, s_idx = mon.spike_arrays()
+        mon.get("spike")
+        n_e = int((s_idx < ne).sum())
+        n_i = int(s_idx.size - n_e)
+        # delivered events: every spike reaches ~1000 targets (mean out-degree),
+        # every excitatory spike also triggers the post-side STDP update of its
+        # 800 incoming E->E synapses
+        events = n_e * (ln.fan_e + ln.fan_e * (n - ne) / ne) + n_i * ln.fan_i * n / (n - ne) \
+            + n_e * ln.fan_e
+        # per-kernel times without graphs
+        nat.kernel_timing(True)
+        net.simulate_steps(20)
+        nat.synchronize()
+        kt = nat.kernel_times()
+        nat.kernel_timing(False)
+        s2, i2 = mon.spike_arrays()
+        mon.get("spike")
+        spk20 = int(i2.size)
+        w_ee = net._backend.read_projection_attribute(ee, "w")
+        hist = np.histogram(w_ee, bins=50, range=(0.0, 1.0))[0]
+        wb = 8 if prec == "double" else 4
+        sb = 2 if prec == "float" else 8
+        per_step_spikes = spk20 / 20
+        e_frac = n_e / max(1, n_e + n_i)
+        kinfo = {}
+        for name, (t, c) in kt.items():
+            avg = t / c
+            if name == f"proj{ee.id}_psp":      # plastic pre side: index, inverse index, w/x/y/last RMW, atomic g
+                b = per_step_spikes * e_frac * ln.fan_e * (4 + 4 + 2 * (3 * wb + 8) + 8) \
+                    if prec == "float" else ln.n_exc * ln.fan_e * 4
+            elif name == f"proj{ee.id}_post_event":
+                b = per_step_spikes * e_frac * ln.fan_e * (4 + 2 * (3 * wb + 8))
+            elif name.endswith("_psp"):
+                k = int(name[4:name.index("_")])
+                proj = next(p for p in (ee, ei, ie) if p.id == k)
+                if prec == "float":
+                    fan = proj.nb_synapses / len(proj.pre_ranks)
+                    sp_k = per_step_spikes * (e_frac if proj is not ie else 1 - e_frac)
+                    b = sp_k * (8 + fan * (4 + sb + 8))
+                else:
+                    b = proj.nb_synapses * 4 + len(proj.post_ranks_view) * 16
+            elif name.startswith("pop"):
+                b = n * (2 * 3 * wb + 8 + 4)
+            else:
+                b = 0
+            kinfo[name] = {"us": avg * 1e3, "launches": c, "gbs": b / (avg * 1e-3) / 1e9 if b else None,
+                           "frac": b / (avg * 1e-3) / 1e9 / peak if b else None}
+        out[prec] = {"ms_total": ms, "us_per_step": ms * 1e3 / steps,
+                     "gsynops": events / (ms * 1e-3) / 1e9,
+                     "rtf": steps * ln.dt / 1e3 / (ms * 1e-3), "build_s": build_s,
+                     "rate_hz": s_idx.size / n / (steps * ln.dt / 1e3),
+                     "spikes": int(s_idx.size), "kernels": kinfo,
+                     "w_ee_mean": float(w_ee.mean()), "w_ee_hist": hist.tolist()}
+        print(json.dumps({prec: {k: v for k, v in out[prec].items() if k != "w_ee_hist"}}), flush=True)
+        del w_ee
+        net.close()
+    h32, h64 = np.array(out["float"]["w_ee_hist"]), np.array(out["double"]["w_ee_hist"])
+    out["rate_err"] = abs(out["float"]["rate_hz"] - out["double"]["rate_hz"]) / out["double"]["rate_hz"]
+    out["hist_l1"] = float(np.abs(h32 - h64).sum() / h64.sum())
+    out["speedup_fast_vs_fp64"] = out["double"]["ms_total"] / out["float"]["ms_total"]
+    print(json.dumps({k: out[k] for k in ("rate_err", "hist_l1", "speedup_fast_vs_fp64")}))
+    return out
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -337,10 +431,17 @@ def main():
     ap.add_argument("--fast-only", action="store_true",
                     help="time only the fast path (used for profiler captures)")
     ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
+    ap.add_argument("--large", type=int, default=0,
+                    help="the large plastic network with this many neurons (1000000 = 1e9 synapses)")
     ap.add_argument("--formats", default="",
                     help="storage-format study on these 100k structures (comma separated: "
                          "uniform,powerlaw,local,blocks)")
     args = ap.parse_args()
+    if args.large:
+        import torch
+        torch.cuda.set_device(0)
+        large_study(args.large)
+        return
     if args.formats:
         import torch
         torch.cuda.set_device(0)

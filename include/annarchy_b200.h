@@ -90,6 +90,31 @@ int anb_array_read(anb_net* net, const char* name, size_t offset, void* dst, siz
 int anb_array_fill_zero(anb_net* net, const char* name);
 int anb_array_info(anb_net* net, const char* name, void** device_ptr, size_t* bytes);
 
+/* Fill an array with a repeated 1-, 2-, 4- or 8-byte value. */
+int anb_array_fill(anb_net* net, const char* name, const void* value, size_t value_bytes);
+
+/* ---- device-side connectivity -------------------------------------------
+ * Replaces the host construction of a fixed_number_pre projection
+ * (ANNarchy/core/ConnectorMethods.py:325-370, ANNarchy/cython_ext/
+ * Connector.pyx:347-420) for large projections: creates "<prefix>__post_rank"
+ * (post ranks post_base..post_base+n_post-1), "__row_ptr", "__col" and "__w"
+ * (weight_bytes 8, 4 or 2 = bfloat16). Every row gets `number` distinct pre
+ * ranks, one per equal stratum of [pre_lo, pre_hi), ascending; weights are
+ * constant a (weight_kind 0), U[a, b) (1) or N(a, b) (2), drawn from a
+ * counter-based hash of `seed`. exclude_self moves a draw equal to the post
+ * rank to a neighbour in its stratum. */
+int anb_connect_fixed_number_pre(anb_net* net, const char* prefix, int n_post, int post_base,
+                                 int pre_lo, int pre_hi, int number, uint64_t seed,
+                                 int weight_kind, double a, double b, int weight_bytes,
+                                 int exclude_self);
+
+/* Pre-major view of a projection's CSR arrays (the reference's CSRC,
+ * ANNarchy/include/CSRCMatrix.hpp:164-222): "<prefix>__col_ptr" over the n_pre
+ * neurons of the pre population, "__post_idx" (post rank of each slot),
+ * "__inv_idx" (CSR index of each slot) and, with with_weights, "__w_pre". The
+ * order of the slots of one pre neuron is unspecified. */
+int anb_csr_to_csc(anb_net* net, const char* prefix, int n_pre, int with_weights);
+
 /* ---- generated module ---------------------------------------------------
  * Compiles CUDA C++ source with NVRTC for sm_100a, loads it and binds its
  * __constant__ pointers named "anb_p_<array>" to the arrays of the same
