@@ -90,6 +90,7 @@ class CompiledNetwork:
             self._local_layout()
             mod = gen.local_module()
         else:
+            nat.create("tickc", np.zeros(1, dtype=np.uint32))
             mod = gen.grid_module()
         self.module = mod
         nat.load_module(mod.source, mod.options)
@@ -491,19 +492,31 @@ class CompiledNetwork:
         cap = self.chunk_steps()
         while left > 0:
             n = min(left, cap)
-            starts = {}
-            for mon in self.net.monitors:
-                first = self._first_record(mon, t)
-                starts[mon.id] = first
-                nat.write(f"mon{mon.id}__t0", np.array([t], dtype=np.int64))
-                nat.write(f"mon{mon.id}__t0v", np.array([first], dtype=np.int64))
-                nat.write(f"mon{mon.id}__on", np.array([1 if mon._recording else 0], dtype=np.int32))
+            starts = self.begin_chunk(t)
             nat.run(n)
             nat.synchronize()
-            for mon in self.net.monitors:
-                self._drain(mon, t, n, starts[mon.id])
+            self.end_chunk(t, n, starts)
             t += n
             left -= n
+
+    def begin_chunk(self, t):
+        """Point every monitor's device ring at step t (a chunk of at most
+        chunk_steps() steps starts there); returns the first variable-record
+        step of each monitor."""
+        starts = {}
+        for mon in self.net.monitors:
+            first = self._first_record(mon, t)
+            starts[mon.id] = first
+            self.native.write(f"mon{mon.id}__t0", np.array([t], dtype=np.int64))
+            self.native.write(f"mon{mon.id}__t0v", np.array([first], dtype=np.int64))
+            self.native.write(f"mon{mon.id}__on", np.array([1 if mon._recording else 0],
+                                                           dtype=np.int32))
+        return starts
+
+    def end_chunk(self, t, n, starts):
+        """Copy the records of the n steps from t into the host monitors."""
+        for mon in self.net.monitors:
+            self._drain(mon, t, n, starts[mon.id])
 
     @staticmethod
     def _first_record(mon, t):

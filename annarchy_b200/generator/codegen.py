@@ -204,6 +204,34 @@ class CodeGenerator:
         return [p["name"] for p in pop.desc["parameters"] + pop.desc["variables"]
                 if p["locality"] == "local"]
 
+    def _fused_spike_records(self, pop) -> str:
+        """Grid engine: lane 0 of every warp also writes its bitmap word into
+        the ring of each spike monitor of the population (no record kernel)."""
+        out = ""
+        for mon in self.net.monitors:
+            if mon.population is not pop or "spike" not in mon.variables:
+                continue
+            ml = self.c.mon_layout[mon.id]
+            m = mon.id
+            out += f"""
+          if (anb_mon_on{m}) {{
+            const long long anb_slot = t - anb_mon_t0{m};
+            if (anb_slot >= 0 && anb_slot < {ml['cap_spike']})
+              {self.ptr(f'mon{m}__spk')}[anb_slot * {ml['words']} + (anb_i >> 5)] = anb_m;
+            else
+              anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+          }}"""
+        return out
+
+    def _fused_record_preamble(self, pop) -> str:
+        out = []
+        for mon in self.net.monitors:
+            if mon.population is pop and "spike" in mon.variables:
+                m = mon.id
+                out.append(f"const int anb_mon_on{m} = {self.ptr(f'mon{m}__on')}[0];")
+                out.append(f"const long long anb_mon_t0{m} = {self.ptr(f'mon{m}__t0')}[0];")
+        return "\n    ".join(out)
+
     def neuron_update(self, pop, *, local_engine=False, smem=None, cluster=None,
                       ballot_hook=None) -> str:
         """Update (+ spike gather) of one population for step t.
@@ -283,12 +311,17 @@ class CodeGenerator:
         ballot = ""
         listed = (spiking and cluster is None and not local_engine and not self.exact
                   and self.c.spike_lists)
+        recs = "" if (local_engine or cluster is not None) else self._fused_spike_records(pop)
+        if recs:
+            recs = f"""
+        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {{{recs}
+        }}"""
         if listed:
             spl, spn = gsrc("spl"), gsrc("spn")
             ballot = f"""
       {{
         const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
-        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {spk_dst}[anb_i >> 5] = anb_m;
+        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {spk_dst}[anb_i >> 5] = anb_m;{recs}
         if (anb_m) {{   // append to this step's spike list (warp-aggregated)
           int anb_pos = 0;
           if ((threadIdx.x & 31) == 0) anb_pos = atomicAdd(&{spn}[t & 1], __popc(anb_m));
@@ -304,7 +337,7 @@ class CodeGenerator:
             ballot = f"""
       {{
         const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
-        if ((threadIdx.x & 31) == 0 && {widx} < {lim}) {spk_dst}[{widx} >> 5] = anb_m;
+        if ((threadIdx.x & 31) == 0 && {widx} < {lim}) {spk_dst}[{widx} >> 5] = anb_m;{recs}
       }}"""
         nl = "\n        "
         if cluster is not None:
@@ -347,6 +380,9 @@ class CodeGenerator:
 
     def pop_kernel(self, pop) -> str:
         preamble = self._globals_preamble(pop, lambda n: self.ptr(f"pop{pop.id}__{n}"))
+        rp = self._fused_record_preamble(pop)
+        if rp:
+            preamble += "\n    " + rp
         dt_t = "double" if self.exact else "float"
         return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
@@ -647,22 +683,11 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
 
     # --------------------------------------------------------------- monitors
     def monitor_kernel(self, mon) -> str:
+        """Variable recording of one monitor (grid engine). Spike bitmaps are
+        written by the update kernel of the population."""
         m = mon.id
         lay = self.c.mon_layout[m]
         parts = []
-        if "spike" in mon.variables:
-            spk = self.ptr(f"pop{mon.population.id}__spk")
-            parts.append(f"""
-    if (anb_on) {{
-      const long long anb_slot = t - {self.ptr(f'mon{m}__t0')}[0];
-      if (anb_slot >= 0 && anb_slot < {lay['cap_spike']}) {{
-        anb_u32* anb_dst = {self.ptr(f'mon{m}__spk')} + anb_slot * {lay['words']};
-        for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < {lay['words']}; w += gridDim.x * blockDim.x)
-          anb_dst[w] = {spk}[w];
-      }} else if (blockIdx.x == 0 && threadIdx.x == 0) {{
-        anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
-      }}
-    }}""")
         for var in mon.variables:
             if var == "spike":
                 continue
@@ -707,25 +732,63 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
                 plan.append((f"proj{proj.id}_post_event",
                              grid_for(self.c.layout[proj.id]["rows"] * 32), BLOCK, 0))
         for mon in net.monitors:
-            kernels.append(self.monitor_kernel(mon))
-            n = self.c.mon_layout[mon.id]["n"]
-            plan.append((f"mon{mon.id}_record", grid_for(max(n, 32)), BLOCK, 0))
+            if any(v != "spike" for v in mon.variables):
+                # spikes are written by the update kernel of the population
+                kernels.append(self.monitor_kernel(mon))
+                n = self.c.mon_layout[mon.id]["n"]
+                plan.append((f"mon{mon.id}_record", grid_for(max(n, 32)), BLOCK, 0))
         resets = ""
         if self.c.spike_lists:
             for pop in net.populations:
                 if pop.neuron_type.type == "spike":
-                    resets += f" {self.ptr(f'pop{pop.id}__spn')}[(t + 1) & 1] = 0;"
-        kernels.append(f"""
-extern "C" __global__ void anb_tick() {{
-    if (blockIdx.x == 0 && threadIdx.x == 0) {{
-      const long long t = *{self.ptr('t')};{resets}
-      *{self.ptr('t')} = t + 1;
+                    resets += f" {self.ptr(f'pop{pop.id}__spn')}[(anb_tt + 1) & 1] = 0;"
+        # the step counter advances at the end of the step's last kernel, by the
+        # last of its CTAs to finish (every CTA has read t by then)
+        epilogue = f"""
+    __syncthreads();
+    if (threadIdx.x == 0) {{
+      __threadfence();
+      const unsigned anb_prev = atomicAdd({self.ptr('tickc')}, 1u);
+      if (anb_prev == gridDim.x - 1) {{
+        *{self.ptr('tickc')} = 0u;
+        const long long anb_tt = *{self.ptr('t')};{resets}
+        *{self.ptr('t')} = anb_tt + 1;
+      }}
     }}
-}}
+"""
+        if not plan or [p[0] for p in plan].count(plan[-1][0]) > 1:
+            kernels.append("""
+extern "C" __global__ void anb_tick() {
+}
 """)
-        plan.append(("anb_tick", 1, 32, 0))
+            plan.append(("anb_tick", 1, 32, 0))
+        kernels = self._append_epilogue(kernels, plan[-1][0], epilogue)
         return Module(self.assemble(kernels), self.options(), "grid", plan=plan,
                       kernels=[p[0] for p in plan])
+
+    @staticmethod
+    def _append_epilogue(kernels: list, name: str, code: str) -> list:
+        """Insert `code` before the closing brace of kernel `name`."""
+        out = []
+        found = False
+        for src in kernels:
+            i = src.find(f" {name}(")
+            if i >= 0 and not found:
+                j = src.index("{", i)
+                depth = 0
+                for k in range(j, len(src)):
+                    if src[k] == "{":
+                        depth += 1
+                    elif src[k] == "}":
+                        depth -= 1
+                        if depth == 0:
+                            src = src[:k] + code + src[k:]
+                            found = True
+                            break
+            out.append(src)
+        if not found:
+            raise RuntimeError(f"kernel {name} not found for the step epilogue")
+        return out
 
     def local_module(self) -> Module:
         """One CTA holds every population's state in shared memory and runs
