@@ -22,7 +22,7 @@ import math
 import numpy as np
 
 from ..generator import formats as F
-from ..generator.codegen import BLOCK, CodeGenerator, grid_for
+from ..generator.codegen import BLOCK, CodeGenerator, compensated_vars, grid_for
 from ..runtime.lib import DryNative, NativeNet
 
 BF16 = np.uint16
@@ -237,11 +237,9 @@ class CompiledNetwork:
             for par in (0, 1):
                 d[f"spk{par}"] = (off, "anb_u32")
                 off += a16(words * 4)
-            if not self.exact and self.net._config.get("compensate", True):
-                for v in pop.desc["variables"]:
-                    if v.get("switch") and v["name"] in pop.desc["local"]:
-                        d["kc_" + v["name"]] = (off, rct)
-                        off += a16(chunk * rb)
+            for name in compensated_vars(pop, self.exact, self.net._config):
+                d["kc_" + name] = (off, rct)
+                off += a16(chunk * rb)
             pops[pop.id] = {"chunk": chunk, "arrays": d}
         per_cta = np.zeros(C, dtype=np.int64)
         self._cl_arrays = {}
@@ -310,10 +308,8 @@ class CompiledNetwork:
         for name, arr in pop._host.items():
             dt = np.int32 if arr.dtype == np.int32 else self.real
             nat.create(f"pop{pop.id}__{name}", np.asarray(arr, dtype=dt).reshape(-1))
-        if not self.exact and self.net._config.get("compensate", True):
-            for v in pop.desc["variables"]:
-                if v.get("switch") and v["name"] in pop.desc["local"]:
-                    nat.create(f"pop{pop.id}__kc_{v['name']}", np.zeros(pop.size, dtype=self.real))
+        for name in compensated_vars(pop, self.exact, self.net._config):
+            nat.create(f"pop{pop.id}__kc_{name}", np.zeros(pop.size, dtype=self.real))
         if pop.neuron_type.type == "spike":
             n = pop.size
             nat.create(f"pop{pop.id}__spk", np.zeros((n + 31) // 32, dtype=np.uint32))

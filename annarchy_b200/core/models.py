@@ -9,6 +9,19 @@ condition; a synapse is spiking when it has ``pre_spike`` or ``post_spike``.
 """
 from __future__ import annotations
 
+import copy
+
+# analysed descriptions by defining strings: the equations of identical
+# models (e.g. the copies of a parameter sweep) are parsed once
+_DESC_CACHE: dict = {}
+
+
+def _cached(kind, key, analyse, model):
+    key = (kind, repr(key))
+    if key not in _DESC_CACHE:
+        _DESC_CACHE[key] = analyse(model)
+    return copy.deepcopy(_DESC_CACHE[key])
+
 
 class Neuron:
     def __init__(self, parameters="", equations="", spike=None, axon_spike=None, reset=None,
@@ -32,7 +45,9 @@ class Neuron:
     def desc(self):
         if self._desc is None:
             from ..parser.analysis import analyse_neuron
-            self._desc = analyse_neuron(self)
+            self._desc = _cached("neuron", (self.parameters, self.equations, self.spike,
+                                            self.reset, self.refractory, self.type),
+                                 analyse_neuron, self)
         return self._desc
 
     def __repr__(self):
@@ -63,7 +78,9 @@ class Synapse:
     def desc(self):
         if self._desc is None:
             from ..parser.analysis import analyse_synapse
-            self._desc = analyse_synapse(self)
+            self._desc = _cached("synapse", (self.parameters, self.equations, self.psp,
+                                             self.pre_spike, self.post_spike, self.type),
+                                 analyse_synapse, self)
         return self._desc
 
     def __repr__(self):

@@ -144,6 +144,17 @@ __device__ __forceinline__ unsigned short anb_ls_h(const unsigned short* p) {
   asm volatile("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
   return v;
 }
+__device__ __forceinline__ uint4 anb_ls_u4(const uint4* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ anb_u32 anb_ls_u(const anb_u32* p) {
+  anb_u32 v;
+  asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
 
 // Four consecutive weights widened to float (16-byte or 8-byte load).
 __device__ __forceinline__ float4 anb_w4(const float* w) { return anb_ls_f4(reinterpret_cast<const float4*>(w)); }
@@ -600,4 +611,31 @@ __device__ __forceinline__ void anb_record(const T* __restrict__ src, const int*
   double* dst = buf + slot * (long long)n;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
     dst[k] = (double)src[ranks ? ranks[k] : k];
+}
+
+
+// Exclusive prefix sum of x over the CTA (blockDim.x a multiple of 32, at
+// most 1024). `warp_sums` is 32 ints of shared memory; two CTA barriers.
+__device__ __forceinline__ int anb_block_exclusive_scan(int x, int* warp_sums, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int s = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += v;
+    }
+    if (lane < nw) warp_sums[lane] = s;
+  }
+  __syncthreads();
+  *total = warp_sums[nw - 1];
+  return (warp ? warp_sums[warp - 1] : 0) + incl - x;
 }

@@ -323,6 +323,13 @@ int anb_device_count(int* count) {
   return ANB_OK;
 }
 
+int anb_device_sm_count(int device, int* count) {
+  if (!count) return fail(ANB_ERR_ARG, "count is NULL");
+  *count = 0;
+  ANB_CUDA(cudaDeviceGetAttribute(count, cudaDevAttrMultiProcessorCount, device));
+  return ANB_OK;
+}
+
 int anb_create(int device, anb_net** out) {
   if (!out) return fail(ANB_ERR_ARG, "out is NULL");
   *out = nullptr;

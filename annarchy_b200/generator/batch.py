@@ -1,0 +1,363 @@
+"""CUDA source of the batched-instance engine.
+
+Many independent spiking networks of one structure (the same neuron and
+synapse equations, populations and projections; sizes, parameter values,
+connectivity and weights free per instance) run in ONE persistent launch.
+Every CTA owns a set of whole instances whose state sits in its shared
+memory for the whole launch; the instances of a CTA are packed so that the
+CTAs of the launch carry about the same number of neurons and synapses.
+Instances never exchange data, so the only barriers are the CTA's own:
+
+    for every step:
+        deliver the spikes of the previous step of every own instance
+        (fast: shared-memory atomics; exact: spike by spike in ascending pre
+        rank with one CTA barrier per spike, the reference's per-post order)
+        __syncthreads
+        update every own instance's neurons, spike bitmap words by ballot
+        (and into the spike monitor ring)
+        __syncthreads
+
+Per-instance quantities come from small tables indexed by the instance's
+slot (its position in the packed order): population sizes, offsets into the
+concatenated global arrays, the shared-memory offset of every state array,
+global parameter values and the word range of each projection's pre ranks.
+
+The per-step semantics are the single-network ones of the reference's
+generated core (ANNarchy/generator/Template/OpenMPBaseTemplate.py:131-484),
+repeated per instance; the reference runs such sweeps as separate processes
+(Network.parallel_run, ANNarchy/core/Network.py:751-900).
+"""
+from __future__ import annotations
+
+from .codegen import CodeGenerator, Module
+
+BATCH_BLOCK = 1024
+
+
+class BatchGenerator(CodeGenerator):
+    """`batch` provides .net (the template network, instance 0), .exact,
+    .native (the device arrays), .smem_arrays ({pop id: [(name, ctype)]}),
+    .n_arrays, .array_index ({(pop id, name): column of the offset table}),
+    .n_cta, .smem, .idx_t and .packed (projection id -> packed synapse
+    words)."""
+
+    def __init__(self, batch):
+        super().__init__(batch)
+        self.b = batch
+
+    def compensated(self, pop) -> list:
+        from .codegen import compensated_vars
+        return compensated_vars(pop, self.exact, self.b.comp_config(pop))
+
+    def _pop_gsrc(self, k):
+        return lambda name: f"({self.ptr(f'pop{k}__{name}')} + anb_goff{k})"
+
+    def _smem_ptrs(self, pop) -> tuple[list, dict]:
+        k = pop.id
+        lines, d = [], {}
+        for name, ct in self.b.smem_arrays[k]:
+            col = self.b.array_index[(k, name)]
+            var = f"anb_s{k}_{name}"
+            lines.append(f"{ct}* __restrict__ {var} = reinterpret_cast<{ct}*>(anb_smem + anb_so[{col}]);")
+            d[name] = var
+        return lines, d
+
+    def _instance_header(self, pops) -> str:
+        out = [f"const int* __restrict__ anb_so = {self.ptr('bt__soff')} + anb_si * {self.b.n_arrays};"]
+        for pop in pops:
+            k = pop.id
+            out.append(f"const int anb_n{k} = {self.ptr(f'pop{k}__bn')}[anb_si];")
+            out.append(f"const long long anb_goff{k} = {self.ptr(f'pop{k}__bgoff')}[anb_si];")
+            out.append(f"const long long anb_woff{k} = {self.ptr(f'pop{k}__bwoff')}[anb_si];")
+            out.append(f"(void)anb_n{k}; (void)anb_goff{k}; (void)anb_woff{k};")
+        return "\n      ".join(out)
+
+    def _copy(self, pop, to_smem: bool) -> str:
+        k = pop.id
+        lines, d = self._smem_ptrs(pop)
+        body = []
+        for name, ct in self.b.smem_arrays[k]:
+            if name == "spk":
+                g = f"{self.ptr(f'pop{k}__spk')}[anb_woff{k} + q]"
+                n = f"((anb_n{k} + 31) >> 5)"
+            else:
+                g = f"{self.ptr(f'pop{k}__{name}')}[anb_goff{k} + q]"
+                n = f"anb_n{k}"
+            if to_smem:
+                body.append(f"for (int q = threadIdx.x; q < {n}; q += blockDim.x) {d[name]}[q] = {g};")
+            else:
+                body.append(f"for (int q = threadIdx.x; q < {n}; q += blockDim.x) {g} = {d[name]}[q];")
+        nl = "\n        "
+        return f"""
+      {{  // population {pop.name}
+        {nl.join(lines)}
+        {nl.join(body)}
+      }}"""
+
+    def _delivery_exact(self, proj) -> str:
+        """Exact mode: the spikes of the projection in ascending pre rank, one
+        CTA barrier after each, so every post neuron adds its inputs in the
+        reference's order (ANNarchy/generator/Projection/OpenMP/CSR.py:870-902)."""
+        k = proj.id
+        a, b = proj.pre_pop.id, proj.post_pop.id
+        spk_col = self.b.array_index[(a, "spk")]
+        g_col = self.b.array_index[(b, "g_" + proj.target)]
+        it = self.b.idx_t
+        cp = self.ptr(f"proj{k}__col_ptr")
+        post, w = self.ptr(f"proj{k}__post"), self.ptr(f"proj{k}__w")
+        return f"""
+      {{  // {proj.name}: spikes in ascending pre rank, one CTA barrier per spike
+        const anb_u32* __restrict__ anb_spk = reinterpret_cast<const anb_u32*>(anb_smem + anb_so[{spk_col}]);
+        real* __restrict__ anb_g = reinterpret_cast<real*>(anb_smem + anb_so[{g_col}]);
+        const int anb_w0 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si];
+        const int anb_w1 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si + 1];
+        const {it}* __restrict__ anb_cp = {cp} + {self.ptr(f'proj{k}__bcpoff')}[anb_si];
+        for (int word = anb_w0; word < anb_w1; ++word) {{
+          anb_u32 m = anb_spk[word];
+          while (m) {{
+            const int pre = (word << 5) + __ffs(m) - 1;
+            m &= m - 1;
+            const {it} beg = anb_cp[pre], end = anb_cp[pre + 1];
+            if (end > beg) {{
+              for ({it} q = beg + threadIdx.x; q < end; q += blockDim.x)
+                anb_g[{post}[q]] += {w}[q];
+              __syncthreads();
+            }}
+          }}
+        }}
+      }}"""
+
+    def _delivery_list(self, spk_pops) -> str:
+        """Fast mode. The spikes of the previous step of every instance of the
+        CTA are gathered into one list in shared memory (each thread holds one
+        bitmap word; a CTA prefix sum of the popcounts gives every spike its
+        slot), LIST_CAP entries per round. Warp w then delivers entries
+        4w..4w+3 (+128 per pass): the four spikes' synapse ranges are read as
+        aligned 4-synapse groups (16-byte loads), lane l taking group l of
+        each, all four loads in flight before the shared-memory atomics. A
+        burst of spikes in one instance is spread over all warps of the CTA."""
+        P = len(spk_pops)
+        it = self.b.idx_t
+        cap = self.b.list_cap
+        NA = self.b.n_arrays
+        so_tab = self.ptr("bt__soff")
+        find = []
+        for pi, pop in enumerate(spk_pops):
+            k = pop.id
+            col = self.b.array_index[(k, "spk")]
+            find.append(f"""
+          {{
+            const int anb_W = ({self.ptr(f'pop{k}__bn')}[anb_si] + 31) >> 5;
+            const int anb_r = (int)threadIdx.x - anb_base;
+            if (anb_r >= 0 && anb_r < anb_W) {{
+              anb_lw = reinterpret_cast<const anb_u32*>(anb_smem + {so_tab}[anb_si * {NA} + {col}])[anb_r];
+              anb_lpair = (anb_si - anb_sb) * {P} + {pi};
+              anb_lword = anb_r;
+            }}
+            anb_base += anb_W;
+          }}""")
+        projs = []
+        for proj in self.net.projections:
+            pi = spk_pops.index(proj.pre_pop)
+            k = proj.id
+            g_col = self.b.array_index[(proj.post_pop.id, "g_" + proj.target)]
+            U = 4 if self.b.packed.get(k) else 2
+            if self.b.packed.get(k):
+                syn = self.ptr(f"proj{k}__syn")
+                load = f"anb_v[u] = anb_ls_u4(reinterpret_cast<const uint4*>({syn}) + anb_g);"
+                regs = "uint4 anb_v[4];"
+                add = ("ANB_ADD(anb_v[u].x, 0) ANB_ADD(anb_v[u].y, 1) "
+                       "ANB_ADD(anb_v[u].z, 2) ANB_ADD(anb_v[u].w, 3)")
+                macro = ("#define ANB_ADD(sw, c) if (anb_g * 4 + c >= anb_bq[u] && anb_g * 4 + c < anb_eq[u]) "
+                         "atomicAdd(reinterpret_cast<real*>(anb_smem + anb_go[u]) + ((sw) >> 16), __uint_as_float((sw) << 16));")
+            else:
+                post, w = self.ptr(f"proj{k}__post"), self.ptr(f"proj{k}__w")
+                load = (f"anb_p4[u] = anb_ls_i4(reinterpret_cast<const int4*>({post}) + anb_g); "
+                        f"anb_w4v[u] = anb_w4({w} + anb_g * 4);")
+                regs = "int4 anb_p4[2]; float4 anb_w4v[2];"
+                add = ("ANB_ADD(anb_p4[u].x, anb_w4v[u].x, 0) ANB_ADD(anb_p4[u].y, anb_w4v[u].y, 1) "
+                       "ANB_ADD(anb_p4[u].z, anb_w4v[u].z, 2) ANB_ADD(anb_p4[u].w, anb_w4v[u].w, 3)")
+                macro = ("#define ANB_ADD(po, wv, c) if (anb_g * 4 + c >= anb_bq[u] && anb_g * 4 + c < anb_eq[u]) "
+                         "atomicAdd(reinterpret_cast<real*>(anb_smem + anb_go[u]) + (po), wv);")
+            projs.append(f"""
+          {{  // {proj.name}
+           {it} anb_bq1 = 0, anb_eq1 = 0;
+           int anb_go1 = 0;
+           if (anb_ent >= 0 && anb_epop == {pi}) {{
+             const {it}* __restrict__ anb_cp = {self.ptr(f'proj{k}__col_ptr')} + {self.ptr(f'proj{k}__bcpoff')}[anb_eslot];
+             anb_bq1 = anb_cp[anb_rank];
+             anb_eq1 = anb_cp[anb_rank + 1];
+             anb_go1 = {so_tab}[anb_eslot * {NA} + {g_col}];
+           }}
+           for (int anb_sub = 0; anb_sub < 4; anb_sub += {U}) {{
+            {it} anb_bq[{U}], anb_eq[{U}];
+            int anb_go[{U}];
+            {it} anb_ng = 0;
+            #pragma unroll
+            for (int u = 0; u < {U}; ++u) {{
+              anb_bq[u] = __shfl_sync(0xffffffffu, anb_bq1, anb_sub + u);
+              anb_eq[u] = __shfl_sync(0xffffffffu, anb_eq1, anb_sub + u);
+              anb_go[u] = __shfl_sync(0xffffffffu, anb_go1, anb_sub + u);
+              const {it} n = anb_eq[u] > anb_bq[u] ? ((anb_eq[u] + 3) >> 2) - (anb_bq[u] >> 2) : 0;
+              anb_ng = n > anb_ng ? n : anb_ng;
+            }}
+            for ({it} anb_p = anb_lane; anb_p - anb_lane < anb_ng; anb_p += 32) {{
+              {regs}
+              #pragma unroll
+              for (int u = 0; u < {U}; ++u) {{
+                const {it} anb_g = (anb_bq[u] >> 2) + anb_p;
+                if (anb_eq[u] > anb_bq[u] && anb_g < ((anb_eq[u] + 3) >> 2)) {{ {load} }}
+              }}
+              #pragma unroll
+              for (int u = 0; u < {U}; ++u) {{
+                const {it} anb_g = (anb_bq[u] >> 2) + anb_p;
+                if (anb_eq[u] > anb_bq[u] && anb_g < ((anb_eq[u] + 3) >> 2)) {{
+{macro}
+                  {add}
+#undef ANB_ADD
+                }}
+              }}
+            }}
+           }}
+          }}""")
+        return f"""
+      {{  // delivery: CTA-wide list of the previous step's spikes
+        anb_u32 anb_lw = 0u;
+        int anb_lpair = 0, anb_lword = 0;
+        {{
+          int anb_base = 0;
+          for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{{''.join(find)}
+          }}
+        }}
+        int anb_total;
+        const int anb_excl = anb_block_exclusive_scan(__popc(anb_lw), anb_scan, &anb_total);
+        for (int anb_r0 = 0; anb_r0 < anb_total; anb_r0 += {cap}) {{
+          {{
+            int k = anb_excl;
+            anb_u32 m = anb_lw;
+            while (m) {{
+              const int b = __ffs(m) - 1;
+              m &= m - 1;
+              if (k >= anb_r0 && k < anb_r0 + {cap})
+                anb_list[k - anb_r0] = (anb_lpair << 16) | ((anb_lword << 5) + b);
+              ++k;
+            }}
+          }}
+          __syncthreads();
+          const int anb_nl = min({cap}, anb_total - anb_r0);
+          for (int anb_e0 = anb_warp * 4; anb_e0 < anb_nl; anb_e0 += anb_nwarps * 4) {{
+            const int anb_ent = (anb_lane < 4 && anb_e0 + anb_lane < anb_nl) ? anb_list[anb_e0 + anb_lane] : -1;
+            const int anb_pair = anb_ent >> 16;
+            const int anb_rank = anb_ent & 0xffff;
+            const int anb_eslot = anb_sb + (anb_ent >= 0 ? anb_pair / {P} : 0);
+            const int anb_epop = anb_ent >= 0 ? anb_pair % {P} : -1;
+            (void)anb_rank; (void)anb_eslot;{''.join(projs)}
+          }}
+          __syncthreads();
+        }}
+      }}"""
+
+    def _update(self, pop) -> str:
+        k = pop.id
+        lines, d = self._smem_ptrs(pop)
+        recs = ""
+        for mon in self.net.monitors:
+            if mon.population is not pop or "spike" not in mon.variables:
+                continue
+            m = mon.id
+            recs += f"""
+          if (anb_mon_on{m}) {{
+            const long long anb_slot = t - anb_mon_t0{m};
+            if (anb_slot >= 0 && anb_slot < {self.b.mon_cap[m]})
+              {self.ptr(f'mon{m}__spk')}[anb_slot * {self.b.total_words[k]}LL + anb_woff{k} + (anb_i >> 5)] = anb_m;
+            else
+              anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+          }}"""
+        hook = f"""
+      {{
+        const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
+        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {{
+          {d['spk']}[anb_i >> 5] = anb_m;{recs}
+        }}
+      }}"""
+        globals_ = self._globals_preamble(pop, lambda n: f"({self.ptr(f'pop{k}__{n}')} + anb_si)")
+        globals_ += f"\n    const int anb_refr{k} = {self.ptr(f'pop{k}__brefr')}[anb_si];"
+        # a refractory period shared by all neurons of the instance comes from
+        # the slot table (no global load in the spike branch)
+        refr = (f"(anb_refr{k} >= 0 ? anb_refr{k} : "
+                f"({self.ptr(f'pop{k}__refractory')} + anb_goff{k})[anb_i])")
+        upd = self.neuron_update(pop, local_engine=True, smem=d, ballot_hook=hook,
+                                 size=f"anb_n{k}", gsrc=self._pop_gsrc(k), refractory=refr)
+        nl = "\n        "
+        return f"""
+      {{
+        {nl.join(lines)}
+        {globals_}
+        {upd}
+      }}"""
+
+    def module(self) -> Module:
+        net = self.net
+        pops = net.populations
+        for pop in pops:
+            if pop.neuron_type.type != "spike":
+                raise NotImplementedError("batched instances hold spiking populations only")
+        mon_pre = "\n    ".join(
+            f"const int anb_mon_on{mon.id} = {self.ptr(f'mon{mon.id}__on')}[0];\n    "
+            f"const long long anb_mon_t0{mon.id} = {self.ptr(f'mon{mon.id}__t0')}[0];\n    "
+            f"(void)anb_mon_on{mon.id}; (void)anb_mon_t0{mon.id};"
+            for mon in net.monitors)
+        header = self._instance_header(pops)
+        load = "".join(self._copy(p, True) for p in pops)
+        store = "".join(self._copy(p, False) for p in pops)
+        spk_pops = [p for p in pops if any(pr.pre_pop is p for pr in net.projections)]
+        if self.exact:
+            deliver = (f"for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{\n        {header}"
+                       + "".join(self._delivery_exact(pr) for pr in net.projections) + "\n      }")
+        elif spk_pops:
+            deliver = self._delivery_list(spk_pops)
+        else:
+            deliver = ""
+        update = "".join(self._update(p) for p in pops)
+        dt_t = "double" if self.exact else "float"
+        scratch = "" if self.exact else f"""// scratch after the instances' state: 32 warp sums, then the spike list
+    int* __restrict__ anb_scan = reinterpret_cast<int*>(anb_smem + {self.b.smem_state});
+    int* __restrict__ anb_list = anb_scan + 32;"""
+        src = f"""
+extern "C" __global__ void __launch_bounds__({BATCH_BLOCK}, 1)
+anb_batch_run(long long t0, int nsteps) {{
+    extern __shared__ __align__(16) unsigned char anb_smem[];
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    const int anb_lane = threadIdx.x & 31;
+    const int anb_warp = threadIdx.x >> 5;
+    const int anb_nwarps = blockDim.x >> 5;
+    (void)anb_lane; (void)anb_warp; (void)anb_nwarps;
+    const int anb_sb = {self.ptr('bt__cta')}[blockIdx.x];
+    const int anb_se = {self.ptr('bt__cta')}[blockIdx.x + 1];
+    {scratch}
+    {mon_pre}
+    for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{
+      {header}
+      {load}
+    }}
+    __syncthreads();
+    for (int anb_s = 0; anb_s < nsteps; ++anb_s) {{
+      const long long t = t0 + anb_s;
+      {deliver}
+      __syncthreads();
+      for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{
+        {header}
+        {update}
+      }}
+      __syncthreads();
+    }}
+    for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{
+      {header}
+      {store}
+    }}
+    if (blockIdx.x == 0 && threadIdx.x == 0) *{self.ptr('t')} = t0 + nsteps;
+}}
+"""
+        return Module(self.assemble([src]), self.options(), "batch",
+                      local=("anb_batch_run", self.b.n_cta, BATCH_BLOCK, self.b.smem),
+                      kernels=["anb_batch_run"])

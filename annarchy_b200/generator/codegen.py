@@ -51,6 +51,21 @@ CTYPE_OF = {np.dtype(np.float64): "double", np.dtype(np.float32): "float",
             np.dtype(np.uint8): "unsigned char"}
 
 
+def compensated_vars(pop, exact: bool, config: dict) -> list:
+    """ODE variables whose explicit-Euler switch is Kahan-compensated
+    (single precision only): the rounding error of every `x += dt*_x` is
+    carried in anb_kc_x and added back at the next step. config
+    "compensate": True (every local ODE variable), False, or a list of
+    variable names."""
+    comp = config.get("compensate", True)
+    if exact or not comp:
+        return []
+    names = [v["name"] for v in pop.desc["variables"]
+             if v.get("switch") and v.get("method") != "event-driven"
+             and v["name"] in pop.desc["local"]]
+    return names if comp is True else [n for n in names if n in comp]
+
+
 def grid_for(n: int, block: int = BLOCK) -> int:
     return max(1, min(MAX_GRID, (n + block - 1) // block))
 
@@ -99,14 +114,7 @@ class CodeGenerator:
 
     # --------------------------------------------------------------- neurons
     def compensated(self, pop) -> list:
-        """ODE variables whose explicit-Euler switch is Kahan-compensated
-        (single precision only): the rounding error of every `x += dt*_x`
-        is carried in anb_kc_x and added back at the next step."""
-        if self.exact or not self.c.net._config.get("compensate", True):
-            return []
-        return [v["name"] for v in pop.desc["variables"]
-                if v.get("switch") and v.get("method") != "event-driven"
-                and v["name"] in pop.desc["local"]]
+        return compensated_vars(pop, self.exact, self.c.net._config)
 
     def _neuron_body(self, pop, src_of, masked: bool) -> tuple[str, list]:
         """Statements updating one neuron; locals are C variables named after
@@ -233,14 +241,19 @@ class CodeGenerator:
         return "\n    ".join(out)
 
     def neuron_update(self, pop, *, local_engine=False, smem=None, cluster=None,
-                      ballot_hook=None) -> str:
+                      ballot_hook=None, size=None, gsrc=None, refractory=None) -> str:
         """Update (+ spike gather) of one population for step t.
 
         grid: grid-stride over all neurons, state in global memory; local:
         one CTA over all neurons, state in shared memory (`smem`); cluster:
         this CTA's slice [anb_base, anb_base + anb_cnt), shared-memory state
         indexed by the local index anb_q and the conductance increments of
-        the step (`cluster` = {target: increment buffer}) added first."""
+        the step (`cluster` = {target: increment buffer}) added first.
+        `size` (a C expression) and `gsrc` (attribute name -> C pointer
+        expression) override the population's size and global arrays; a
+        `ballot_hook` replaces the bitmap store of the local engine;
+        `refractory` is a C expression of the refractory period (in steps)
+        that replaces the per-neuron array."""
         spiking = pop.neuron_type.type == "spike"
         masked = spiking and pop._has_refractory
         body, modified = self._neuron_body(pop, None, masked)
@@ -248,8 +261,9 @@ class CodeGenerator:
         names = self._locals(pop)
         k = pop.id
 
-        def gsrc(name):
-            return self.ptr(f"pop{k}__{name}")
+        if gsrc is None:
+            def gsrc(name):
+                return self.ptr(f"pop{k}__{name}")
 
         loads, stores = [], []
         sidx = "anb_q" if cluster is not None else "anb_i"
@@ -292,7 +306,9 @@ class CodeGenerator:
                 loads.append("const int in_ref = (refractory_remaining > 0) ? 0 : 1;")
                 refr_dec = "refractory_remaining -= (1 - in_ref);"
                 guard = f"(in_ref != 0) && ({cond})"
-                if smem and "refractory" in smem:
+                if refractory is not None:
+                    refr_set = f"refractory_remaining = {refractory};"
+                elif smem and "refractory" in smem:
                     refr_set = f"refractory_remaining = {smem['refractory']}[{rr_idx}];"
                 else:
                     refr_set = f"refractory_remaining = {gsrc('refractory')}[anb_i];"
@@ -330,7 +346,7 @@ class CodeGenerator:
             {spl}[(t & 1) * (long long)anb_n + anb_pos + __popc(anb_m & ((1u << (threadIdx.x & 31)) - 1u))] = anb_i;
         }}
       }}"""
-        elif spiking and cluster is not None and ballot_hook is not None:
+        elif spiking and ballot_hook is not None:
             ballot = ballot_hook
         elif spiking:
             widx, lim = ("anb_q", "anb_cnt") if cluster is not None else ("anb_i", "anb_n")
@@ -365,7 +381,7 @@ class CodeGenerator:
                     "anb_base += gridDim.x * blockDim.x)")
         return f"""
     {{  // population {pop.name}: update{' and spike gather' if spiking else ''}
-      const int anb_n = {pop.size};
+      const int anb_n = {size if size is not None else pop.size};
       {loop} {{
         const int anb_i = anb_base + threadIdx.x;
         bool anb_spiked = false;

@@ -23,6 +23,7 @@ SIGNATURES = {
     "anb_abi_version": (C.c_int, []),
     "anb_last_error": (C.c_char_p, []),
     "anb_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "anb_device_sm_count": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "anb_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "anb_destroy": (C.c_int, [C.c_void_p]),
     "anb_initialize": (C.c_int, [C.c_void_p, C.c_double]),
@@ -122,6 +123,12 @@ def check_selector(fn: str, status: int):
 def device_count() -> int:
     n = C.c_int(0)
     check("anb_device_count", load().anb_device_count(C.byref(n)))
+    return n.value
+
+
+def device_sm_count(device: int = 0) -> int:
+    n = C.c_int(0)
+    check("anb_device_sm_count", load().anb_device_sm_count(int(device), C.byref(n)))
     return n.value
 
 

@@ -55,6 +55,35 @@ def bernoulli_csr(rng: np.random.Generator, n_post: int, n_pre: int, p: float,
     return m
 
 
+def bernoulli_csr_skip(rng: np.random.Generator, n_post: int, n_pre: int, p: float,
+                       weights) -> sp.csr_matrix:
+    """Same distribution as bernoulli_csr (every entry independently with
+    probability p) drawn in O(nnz): the gaps between consecutive entries of
+    the row-major sequence are geometric(p). Row-major order, sorted."""
+    total = n_post * n_pre
+    pos = np.zeros(0, dtype=np.int64)
+    last = -1
+    while True:
+        k = int(max(1024, (total - last) * p * 1.05 + 64))
+        gaps = rng.geometric(p, size=k).astype(np.int64)
+        nxt = last + np.cumsum(gaps)
+        inside = nxt < total
+        pos = np.concatenate([pos, nxt[inside]])
+        if not inside.all():
+            break
+        last = int(nxt[-1])
+    rows = pos // n_pre
+    cols = (pos % n_pre).astype(np.int32)
+    nnz = pos.size
+    if callable(weights):
+        data = np.asarray(weights(nnz), dtype=np.float64)
+    else:
+        data = np.full(nnz, float(weights), dtype=np.float64)
+    indptr = np.zeros(n_post + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n_post), out=indptr[1:])
+    return sp.csr_matrix((data, cols, indptr), shape=(n_post, n_pre))
+
+
 def to_from_sparse(m: sp.csr_matrix) -> sp.csr_matrix:
     """(post, pre) -> the (pre, post) layout ``Projection.from_sparse`` expects."""
     return m.T.tocsr()
@@ -137,12 +166,15 @@ class CobaNet:
 
 def coba_net(seed: int = 42, n: int = 4000, exc_frac: float = 0.8, p: float = 0.02,
              w_exc: float = 0.6, w_inh: float = 6.7, drive: float = 20.0,
-             steps: int = 10000) -> CobaNet:
+             steps: int = 10000, skip: bool = False) -> CobaNet:
+    """skip=True draws the connectivity with bernoulli_csr_skip (same
+    distribution, O(nnz) time and memory; a different sample)."""
     rng = np.random.default_rng(seed)
     n_exc = int(round(n * exc_frac))
     v0 = rng.uniform(-60.0, -50.0, n)
-    we = bernoulli_csr(rng, n, n_exc, p, w_exc)
-    wi = bernoulli_csr(rng, n, n - n_exc, p, w_inh)
+    gen = bernoulli_csr_skip if skip else bernoulli_csr
+    we = gen(rng, n, n_exc, p, w_exc)
+    wi = gen(rng, n, n - n_exc, p, w_inh)
     params = dict(COBA_PARAMS)
     params["I"] = float(drive)
     return CobaNet(n, n_exc, we, wi, v0, params=params, steps=steps)
@@ -263,7 +295,7 @@ def batched_coba(n_instances: int = 256, seed: int = 42, n_min: int = 1000,
     nets = []
     for i in range(n_instances):
         nets.append(coba_net(seed=seed + i, n=int(sizes[i]), w_exc=float(we[i % side]),
-                             w_inh=float(wi[i // side]), steps=steps))
+                             w_inh=float(wi[i // side]), steps=steps, skip=True))
     return nets
 
 
@@ -324,6 +356,16 @@ def stdp_matrix(cn: CobaNet, seed: int, p: float) -> sp.csr_matrix:
 # ---------------------------------------------------------------------------
 # large plastic spiking network (device-generated connectivity)
 # ---------------------------------------------------------------------------
+
+def build_batch(cns: list[CobaNet], precision: str = "float", weight_dtype: str | None = None,
+                record: bool = True, **kw):
+    """The spiking nets of `cns` as instances of one Batch (not compiled).
+    Returns (batch, [(net, pop, monitor)])."""
+    from .core.batch import Batch
+    members = [build_coba_network(cn, "double", "grid", record=record) for cn in cns]
+    batch = Batch([m[0] for m in members], precision=precision, weight_dtype=weight_dtype, **kw)
+    return batch, members
+
 
 @dataclass
 class LargeNet:

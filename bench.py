@@ -382,6 +382,127 @@ def large_study(n=1_000_000, steps=1000):
     return out
 
 
+def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracle_check=4):
+    """Batched instances: uneven-size copies of the spiking net (N ~ U{1000..8000},
+    increments swept 0.2-1.0 / 2-10 over a 16x16 grid, one seed each) in one
+    persistent launch, fast (float state, bfloat16 weights) and exact (double).
+    Reports GSynOps/s and instance-seconds simulated per second of device time,
+    the plain FP64 single-instance GPU path on a sample of the instances,
+    per-instance firing-rate error of the fast batch against the exact batch
+    and a bit-exact check of the exact batch against the oracle on a sample."""
+    import torch
+    from annarchy_b200 import workloads as wl
+    t0 = time.time()
+    cns = wl.batched_coba(n_inst, steps=steps)
+    gen_s = time.time() - t0
+    dt = cns[0].dt
+    out = {"config": {"instances": n_inst, "steps": steps, "dt": dt,
+                      "neurons": int(sum(c.n for c in cns)), "synapses": int(sum(c.nnz for c in cns)),
+                      "sizes": [int(min(c.n for c in cns)), int(max(c.n for c in cns))]},
+           "generate_s": gen_s}
+    peak, peak_kind = peaks()
+    counts = {}
+    for prec, wd in (("float", "bfloat16"), ("float", "float32"), ("double", None)):
+        key = prec if prec == "double" else f"float_{wd}"
+        t0 = time.time()
+        b, members = wl.build_batch(cns, prec, wd)
+        b.compile()
+        build_s = time.time() - t0
+        nat = b.native
+        stream = torch.cuda.Stream()
+        nat.set_stream(stream.cuda_stream)
+        b.simulate_steps(20)                           # warm-up
+        b.reset()
+        for _, _, mon in members:
+            mon.get("spike")
+        ms, t, left = 0.0, 0, steps
+        cap = b.chunk_steps()
+        launches = 0
+        with ClockSampler(0) as clk:
+            while left > 0:
+                n = min(left, cap)
+                b.begin_chunk(t)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                nat.run(n)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+                launches += 1
+                b.end_chunk(t, n)
+                t += n
+                left -= n
+        per = []
+        for i, (_, _, mon) in enumerate(members):
+            s_, r_ = mon.spike_arrays()
+            per.append(r_)
+        counts[key] = np.array([r.size for r in per])
+        events = b.delivered_events([[(0, r)] for r in per])
+        spikes = int(counts[key].sum())
+        words = sum(b.total_words.values())
+        abytes = (events * (4 if b.packed.get(0) else 2 + 4) + spikes * (8 + 8)
+                  + steps * words * 4 + 2 * out["config"]["neurons"] * 28)
+        res = {"ms": ms, "us_per_step": ms * 1e3 / steps, "gsynops": events / (ms * 1e-3) / 1e9,
+               "instance_rtf": steps * dt / 1e3 / (ms * 1e-3),
+               "aggregate_rtf": n_inst * steps * dt / 1e3 / (ms * 1e-3),
+               "events": events, "spikes": spikes, "build_s": build_s, "ctas": b.n_cta,
+               "smem_per_cta": b.smem, "launches": launches,
+               "cta_load_max_over_mean": float(b.cta_load.max() / b.cta_load.mean()),
+               "roofline": {"bound": "hbm", "achieved": abytes / (ms * 1e-3) / 1e9, "peak": peak,
+                            "unit": "GB/s", "frac": abytes / (ms * 1e-3) / 1e9 / peak,
+                            "peak_source": peak_kind, "algorithmic_bytes": abytes},
+               "clocks": clk.summary()}
+        if prec == "double" and oracle_check:
+            from oracle import oracle as O
+            pick = np.linspace(0, n_inst - 1, oracle_check).astype(int)
+            ok = True
+            for i in pick:
+                ref = O.coba_run(cns[i])
+                s_, r_ = members[i][2].spike_arrays()
+                ok &= bool(np.array_equal(s_, ref["spike_steps"]) and np.array_equal(r_, ref["spike_idx"])
+                           and np.array_equal(members[i][1].v, ref["v"]))
+            res["oracle_bit_exact"] = {"instances": pick.tolist(), "ok": ok}
+        out[key] = res
+        print(json.dumps({key: res}), flush=True)
+        b.close()
+    ref = counts["double"]
+    for key in ("float_bfloat16", "float_float32"):
+        err = np.abs(counts[key] - ref) / np.maximum(ref, 1)
+        worst = np.argsort(-err)[:5]
+        out[key]["rate_err_per_instance"] = {
+            "mean": float(err.mean()), "median": float(np.median(err)), "max": float(err.max()),
+            "p95": float(np.percentile(err, 95)),
+            "worst": [{"instance": int(i), "n": int(cns[i].n), "w_exc": float(cns[i].w_exc.data[0]),
+                       "w_inh": float(cns[i].w_inh.data[0]), "spikes": int(counts[key][i]),
+                       "spikes_fp64": int(ref[i])} for i in worst]}
+        out[key]["rate_err_total"] = float(abs(counts[key].sum() - ref.sum()) / ref.sum())
+    # plain FP64 single-instance GPU path (grid engine, one launch per phase,
+    # no graph) on a sample of the instances, one after the other
+    order = np.argsort([c.n for c in cns])
+    pick = order[np.linspace(0, n_inst - 1, plain_sample).astype(int)]
+    tt, ev = 0.0, 0
+    for i in pick:
+        cn = cns[i]
+        net, P, mon = build_net(cn, "double", "grid", graph_steps=0)
+        net.simulate_steps(5)
+        mon.get("spike")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        net.simulate_steps(plain_steps)
+        net._backend.native.synchronize()
+        tt += time.perf_counter() - t0
+        _, r_ = mon.spike_arrays()
+        ev += int(cn.out_degree()[r_].sum())
+        net.close()
+    out["plain_fp64"] = {"gsynops": ev / tt / 1e9, "instances": [int(i) for i in pick],
+                         "steps": plain_steps}
+    out["fast_vs_plain_fp64"] = out["float_bfloat16"]["gsynops"] / out["plain_fp64"]["gsynops"]
+    out["exact_batch_vs_plain_fp64"] = out["double"]["gsynops"] / out["plain_fp64"]["gsynops"]
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -438,6 +559,10 @@ def main():
     ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
     ap.add_argument("--large", type=int, default=0,
                     help="the large plastic network with this many neurons (1000000 = 1e9 synapses)")
+    ap.add_argument("--batched", type=int, default=0,
+                    help="batched-instance study with this many instances (256 = the sweep)")
+    ap.add_argument("--batched-steps", type=int, default=5000,
+                    help="time steps of the batched-instance study")
     ap.add_argument("--formats", default="",
                     help="storage-format study on these 100k structures (comma separated: "
                          "uniform,powerlaw,local,blocks)")
@@ -446,6 +571,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         large_study(args.large)
+        return
+    if args.batched:
+        import torch
+        torch.cuda.set_device(0)
+        batched_study(args.batched, steps=args.batched_steps)
         return
     if args.formats:
         import torch

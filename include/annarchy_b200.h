@@ -59,6 +59,10 @@ const char* anb_last_error(void);
 /* Number of visible CUDA devices (0 without a GPU). */
 int anb_device_count(int* count);
 
+/* Number of streaming multiprocessors of `device` (sizes the persistent
+ * launches of batched instances). No counterpart in the reference. */
+int anb_device_sm_count(int device, int* count);
+
 /* ---- network lifetime --------------------------------------------------
  * anb_create replaces pyx_create() plus set_device(int)
  * (ANNarchy/generator/NanoBind/BaseTemplate.py:1-45,
