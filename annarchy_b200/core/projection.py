@@ -23,7 +23,7 @@ from .models import Synapse
 from .population import Population, PopulationView
 from .random import values as draw
 
-FORMATS = ("csr", "ell", "ellr", "sell", "bsr", "hyb", "auto")
+FORMATS = ("csr", "ell", "ellr", "sell", "bsr", "hyb", "pcsr", "auto")
 
 
 def _ranks(obj):

@@ -456,6 +456,161 @@ __device__ __forceinline__ void anb_rate_coo_atomic(int nnz, const int* __restri
   }
 }
 
+// ---- panelled CSR (fast mode) -------------------------------------------------------
+// The pre-synaptic columns are cut into panels of at most `panel_width`
+// neurons; each panel is a CSR over all rows with 16-bit column indices
+// relative to the panel. One CTA owns rows [r0, r1) of one panel: it copies
+// the panel's rates into shared memory with bulk (TMA) copies, then streams
+// the contiguous synapse range of its rows in aligned 8-synapse chunks (one
+// 16-byte index load and 32 or 16 bytes of weights per thread and chunk), so
+// the gathers hit shared memory and every load of the matrix is a full
+// 16-byte vector. The first row of every chunk comes from a per-chunk table;
+// row boundaries inside a chunk from the CTA's row pointers staged in shared
+// memory. Partial row sums are added in shared memory, then into the global
+// sums (atomically when the projection has several panels).
+
+// Issue bulk copies of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global memory into this CTA's shared memory, completing on
+// the mbarrier `mbar` (phase 0). Called by one thread; the barrier must be
+// published (CTA barrier) before other threads wait on it.
+__device__ __forceinline__ void anb_bulk_issue(void* dst, const void* src, unsigned bytes,
+                                               unsigned long long* mbar) {
+  const unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }"
+               ::"r"(mb), "r"(bytes) : "memory");
+  const unsigned chunk = 32768u;
+  for (unsigned off = 0; off < bytes; off += chunk) {
+    const unsigned n = bytes - off < chunk ? bytes - off : chunk;
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(d + off), "l"(reinterpret_cast<const char*>(src) + off), "r"(n), "r"(mb)
+        : "memory");
+  }
+}
+
+// Wait for phase 0 of `mbar`, at most ANB_BULK_WAIT_TRIES polls; a timeout is
+// reported in `err` (the copied data is then incomplete; the kernel still
+// finishes).
+#define ANB_BULK_WAIT_TRIES (1 << 22)
+__device__ __forceinline__ void anb_bulk_wait(unsigned long long* mbar, int* err) {
+  const unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+  unsigned done = 0;
+  for (int it = 0; it < ANB_BULK_WAIT_TRIES && !done; ++it) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done) : "r"(mb) : "memory");
+  }
+  if (!done) anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+}
+
+// Eight consecutive weights (aligned) widened to float.
+__device__ __forceinline__ void anb_w8(const float* w, float* o) {
+  const float4 a = anb_ls_f4(reinterpret_cast<const float4*>(w));
+  const float4 b = anb_ls_f4(reinterpret_cast<const float4*>(w) + 1);
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+__device__ __forceinline__ void anb_w8(const anb_bf16* w, float* o) {
+  const uint4 u = anb_ls_u4(reinterpret_cast<const uint4*>(w));
+  const anb_u32 q[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    o[2 * i] = __uint_as_float(q[i] << 16);
+    o[2 * i + 1] = __uint_as_float(q[i] & 0xffff0000u);
+  }
+}
+
+// cta_tab[4 * blockIdx.x ...] = (panel, r0, r1, first entry of the CTA in
+// crow); row_ptr: n_panels x (n_rows + 1) absolute offsets into col/w (both
+// padded by at least 8 entries past the last synapse); crow: for each chunk
+// of the CTA, the row (relative to r0) of its first synapse in the CTA's
+// range. Dynamic shared memory: panel_width floats, then max_rows + 1 ints of
+// row pointers and max_rows floats of row sums.
+template <typename W>
+__device__ __forceinline__ void anb_rate_pcsr(const int* __restrict__ cta_tab,
+                                              const int* __restrict__ row_ptr, int n_rows,
+                                              const unsigned short* __restrict__ crow,
+                                              const unsigned short* __restrict__ col,
+                                              const W* __restrict__ w,
+                                              const float* __restrict__ x, int n_pre,
+                                              int panel_width, int max_rows,
+                                              const int* __restrict__ post_rank,
+                                              float* __restrict__ sum, int atomic, int* err) {
+  extern __shared__ __align__(16) unsigned char anb_pc_smem[];
+  __shared__ __align__(8) unsigned long long anb_pc_mbar;
+  float* xs = reinterpret_cast<float*>(anb_pc_smem);
+  int* rps = reinterpret_cast<int*>(anb_pc_smem + 4 * panel_width);
+  float* acc = reinterpret_cast<float*>(rps + max_rows + 1);
+  const int* tab = cta_tab + 4 * blockIdx.x;
+  const int p = tab[0], r0 = tab[1], r1 = tab[2], cr0 = tab[3];
+  const int nr = r1 - r0;
+  const int c0 = p * panel_width;
+  const int cw = min(panel_width, n_pre - c0);
+  const int cw4 = cw & ~3;
+  const int* __restrict__ rp = row_ptr + (long long)p * (n_rows + 1) + r0;
+  const int beg = rp[0], end = rp[nr];
+  if (threadIdx.x == 0 && cw4 > 0) anb_bulk_issue(xs, x + c0, 4u * (unsigned)cw4, &anb_pc_mbar);
+  for (int q = threadIdx.x; q <= nr; q += blockDim.x) rps[q] = rp[q];
+  for (int q = threadIdx.x; q < nr; q += blockDim.x) acc[q] = 0.f;
+  for (int q = cw4 + threadIdx.x; q < cw; q += blockDim.x) xs[q] = x[c0 + q];
+  const int a0 = beg & ~7;
+  // first chunk of this thread, loaded while the panel copy is in flight
+  int j0 = a0 + 8 * (int)threadIdx.x;
+  uint4 cv = make_uint4(0u, 0u, 0u, 0u);
+  float wv[8];
+  int row = 0;
+  if (j0 < end) {
+    cv = anb_ls_u4(reinterpret_cast<const uint4*>(col + j0));
+    anb_w8(w + j0, wv);
+    row = crow[cr0 + (j0 - a0) / 8];
+  }
+  __syncthreads();                                   // mbarrier, rps, acc published
+  if (cw4 > 0) anb_bulk_wait(&anb_pc_mbar, err);
+  while (j0 < end) {
+    // next chunk of this thread in flight while this one is summed
+    const int jn = j0 + 8 * (int)blockDim.x;
+    uint4 cn = make_uint4(0u, 0u, 0u, 0u);
+    float wn[8];
+    int rown = 0;
+    if (jn < end) {
+      cn = anb_ls_u4(reinterpret_cast<const uint4*>(col + jn));
+      anb_w8(w + jn, wn);
+      rown = crow[cr0 + (jn - a0) / 8];
+    }
+    const anb_u32 cq[4] = {cv.x, cv.y, cv.z, cv.w};
+    int nxt = rps[row + 1];                          // start of the next row
+    float s = 0.f;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int j = j0 + e;
+      if (j < beg || j >= end) continue;
+      if (j >= nxt) {                                // the chunk enters the next row(s)
+        atomicAdd(&acc[row], s);
+        s = 0.f;
+        do { ++row; nxt = rps[row + 1]; } while (j >= nxt);
+      }
+      const unsigned c = (e & 1) ? (cq[e >> 1] >> 16) : (cq[e >> 1] & 0xffffu);
+      s += xs[c] * wv[e];
+    }
+    atomicAdd(&acc[row], s);
+    j0 = jn;
+    cv = cn;
+    row = rown;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) wv[e] = wn[e];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nr; q += blockDim.x) {
+    if (rps[q + 1] > rps[q]) {
+      const int post = post_rank ? post_rank[r0 + q] : r0 + q;
+      if (atomic) atomicAdd(&sum[post], acc[q]);
+      else sum[post] += acc[q];
+    }
+  }
+}
+
 // ---- event-driven transmission -----------------------------------------------------
 
 // Exact gather: thread per post row; g[post] += w[j] for every synapse whose

@@ -427,13 +427,23 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
         W = self.c.wctype
         name = f"proj{k}_psp"
 
-        def kern(nm, body, block=BLOCK):
+        def kern(nm, body, block=BLOCK, min_blocks=None):
+            bounds = f"{block}, {min_blocks}" if min_blocks else f"{block}"
             return f"""
-extern "C" __global__ void __launch_bounds__({block}) {nm}() {{
+extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
     {body}
 }}
 """
-        if fmt == "csr":
+        if fmt == "pcsr" and not self.exact:
+            pw, mr = lay["panel_width"], lay["pc_max_rows"]
+            smem = 4 * pw + 4 * (mr + 1) + 4 * mr
+            call = (f"anb_rate_pcsr<{W}>({p('pc_cta')}, {p('pc_row_ptr')}, {lay['rows']}, "
+                    f"{p('pc_crow')}, {p('pc_col')}, {p('pc_w')}, {pre_r}, {proj.pre_pop.size}, {pw}, {mr}, "
+                    f"{p('post_rank')}, {sum_}, {1 if lay['n_panels'] > 1 else 0}, {self.ptr('err')});")
+            B = lay["pc_block"]
+            return (kern(name, call, B, lay["pc_resident"]),
+                    [(name, lay["pc_ctas"], B, smem)])
+        if fmt in ("csr", "pcsr"):       # pcsr in double precision: CSR order
             if self.exact:
                 call = (f"anb_rate_csr_scalar<double, double, {lay['idx_t']}>({lay['rows']}, "
                         f"{p('row_ptr')}, {p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_});")

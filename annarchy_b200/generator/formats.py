@@ -19,12 +19,21 @@ Containers restated from the reference's headers (ANNarchy/include/*.hpp):
 In double precision every format sums each row in ascending pre rank, so
 its result equals CSR bit for bit, except HYB, which adds the ELL part and
 then the tail of a row (the reference's HYB differs from CSR the same way).
+
+This backend adds one schedule of its own, without a counterpart among the
+reference's containers:
+
+* PCSR  (panelled CSR, single precision only): the pre-synaptic columns cut
+        into panels that fit in one CTA's shared memory, one CSR per panel
+        with 16-bit column indices, and a table assigning each CTA a row
+        range of one panel with about the same number of synapses. In double
+        precision a PCSR projection is summed as CSR (ascending pre rank).
 """
 from __future__ import annotations
 
 import numpy as np
 
-RATE_FORMATS = ("csr", "ell", "ellr", "sell", "bsr", "hyb")
+RATE_FORMATS = ("csr", "ell", "ellr", "sell", "bsr", "hyb", "pcsr")
 
 
 def csr_group(mean_row: float) -> int:
@@ -115,6 +124,80 @@ def hyb_width(row_ptr) -> int:
         return 0
     counts = np.bincount(rl)
     return int(np.argmax(counts))
+
+
+PCSR_MAX_ROWS = 4096
+
+
+def pcsr_arrays(row_ptr, cols, w, n_pre, panel_width=16384, ctas=296, max_rows=PCSR_MAX_ROWS):
+    """Panelled CSR. Returns dict(row_ptr (n_panels x (rows+1), int32,
+    absolute offsets), col (uint16, relative to the panel), w (float64,
+    reordered), cta_tab ((n_cta, 4) int32: panel, first row, end row, first
+    entry in crow), crow (uint16: for each aligned 8-synapse chunk
+    overlapping a CTA's synapse range, the row of its first synapse in the
+    range, relative to the CTA's first row), n_panels, panel_width).
+    Synapse arrays are padded by 8 zero entries past a multiple of 8. Each
+    panel gets CTAs in proportion to its synapses, and a CTA's rows are cut
+    where the cumulative synapse count crosses the panel's per-CTA share
+    (and after max_rows rows, at most 65535)."""
+    row_ptr = np.asarray(row_ptr, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    n_rows = row_ptr.size - 1
+    panel_width = int(max(32, min(panel_width, 65536)) // 32 * 32)
+    max_rows = int(min(max_rows, 65535))
+    n_panels = max(1, -(-int(n_pre) // panel_width))
+    rows_of = np.repeat(np.arange(n_rows, dtype=np.int64), np.diff(row_ptr))
+    panel = (cols // panel_width).astype(np.uint16)
+    # CSR order is row-major with ascending columns: a stable sort by panel
+    # gives panel, then row, then column
+    order = np.argsort(panel, kind="stable")
+    counts = np.bincount(panel.astype(np.int64) * n_rows + rows_of,
+                         minlength=n_panels * n_rows).reshape(n_panels, n_rows)
+    rp = np.zeros((n_panels, n_rows + 1), dtype=np.int64)
+    flat = np.cumsum(counts.reshape(-1))
+    starts = np.concatenate([[0], flat])            # start of (panel, row) segments
+    for p_ in range(n_panels):
+        rp[p_] = starts[p_ * n_rows: (p_ + 1) * n_rows + 1]
+    nnz = cols.size
+    pad = (-nnz) % 8 + 8
+    col16 = np.zeros(nnz + pad, dtype=np.uint16)
+    col16[:nnz] = (cols[order] - panel[order].astype(np.int64) * panel_width).astype(np.uint16)
+    wv = np.zeros(nnz + pad, dtype=np.float64)
+    wv[:nnz] = np.asarray(w, dtype=np.float64)[order]
+    per_panel = counts.sum(axis=1)
+    tab = []
+    for p_ in range(n_panels):
+        if per_panel[p_] == 0:
+            continue
+        share = max(1, int(round(ctas * per_panel[p_] / max(nnz, 1))))
+        target = per_panel[p_] / share
+        cum = np.cumsum(counts[p_])
+        r0 = 0
+        while r0 < n_rows:
+            # next cut: where the panel's cumulative count reaches the next share
+            done = cum[r0 - 1] if r0 else 0
+            r1 = int(np.searchsorted(cum, done + target, side="left")) + 1
+            r1 = max(r0 + 1, min(r1, r0 + max_rows, n_rows))
+            if cum[r1 - 1] > done:
+                tab.append((p_, r0, r1))
+            r0 = r1
+    # per CTA: the row (relative to its first row) of the first synapse of
+    # each aligned 8-synapse chunk that overlaps its synapse range
+    full, crow = [], []
+    base = 0
+    for p_, r0, r1 in tab:
+        seg = rp[p_, r0:r1 + 1]
+        beg, end = int(seg[0]), int(seg[-1])
+        a0 = beg & ~7
+        first = np.maximum(np.arange(a0, end, 8, dtype=np.int64), beg)
+        crow.append((np.searchsorted(seg, first, side="right") - 1).astype(np.uint16))
+        full.append((p_, r0, r1, base))
+        base += first.size
+    cta_tab = np.asarray(full, dtype=np.int64).reshape(-1, 4).astype(np.int32)
+    crow = np.concatenate(crow) if crow else np.zeros(0, np.uint16)
+    return {"row_ptr": rp.astype(np.int32).reshape(-1), "col": col16, "w": wv, "cta_tab": cta_tab,
+            "crow": np.concatenate([crow, np.zeros(8, np.uint16)]),
+            "n_panels": n_panels, "panel_width": panel_width}
 
 
 def bsr_arrays(post_rank, row_ptr, cols, w, n_pre, tile):
@@ -222,6 +305,26 @@ def create_format_arrays(compiled, proj, fmt, post_rank, row_ptr, cols, w, lay):
         nat.create(f"proj{k}__bsr_col", d["block_col"])
         nat.create(f"proj{k}__bsr_val", W(d["values"]))
         lay.update(tile=tile, block_rows=d["n_block_rows"], n_post_pad=d["n_post_pad"])
+    elif fmt == "pcsr":
+        if compiled.exact:          # summed as CSR in double precision
+            return
+        cfg = proj.net._config
+        pw = int(cfg.get("pcsr_panel", 16384))
+        mr = int(cfg.get("pcsr_rows", PCSR_MAX_ROWS))
+        sms = int(cfg.get("sm_count", 148))
+        d = pcsr_arrays(row_ptr, cols, w, proj.pre_pop.size, panel_width=pw,
+                        ctas=int(cfg.get("pcsr_ctas", 2 * sms)), max_rows=mr)
+        nat.create(f"proj{k}__pc_row_ptr", d["row_ptr"])
+        nat.create(f"proj{k}__pc_col", d["col"])
+        nat.create(f"proj{k}__pc_w", W(d["w"]))
+        nat.create(f"proj{k}__pc_cta", d["cta_tab"].reshape(-1))
+        nat.create(f"proj{k}__pc_crow", d["crow"])
+        block = int(cfg.get("pcsr_block", 1024))
+        smem = 4 * d["panel_width"] + 8 * mr + 4
+        resident = max(1, min(2048 // block, (228 * 1024) // (smem + 1024)))
+        lay.update(n_panels=d["n_panels"], panel_width=d["panel_width"],
+                   pc_ctas=int(d["cta_tab"].shape[0]), pc_max_rows=mr, pc_block=block,
+                   pc_resident=resident)
     else:
         raise ValueError(f"unknown format {fmt!r}")
 

@@ -31,6 +31,15 @@ SCHEDULES = [
 ]
 
 
+# schedules of this backend without a counterpart among the reference's
+# formats (the learned selector predicts over SCHEDULES; the exhaustive
+# autotuner tries ALL_SCHEDULES)
+SCHEDULES_B200 = [
+    {"format": "pcsr"},
+]
+ALL_SCHEDULES = SCHEDULES + SCHEDULES_B200
+
+
 def schedule_name(s: dict) -> str:
     extra = "".join(f"_{v}" for k, v in sorted(s.items()) if k != "format")
     return s["format"] + extra
@@ -160,7 +169,7 @@ class Autotuner:
                                                          else "float64"]
         feat = features(m, wb)
         table = {}
-        cands = list(schedules or SCHEDULES)
+        cands = list(schedules or ALL_SCHEDULES)
         for e in extra:
             if e not in cands and feasible(m, e, 64.0):
                 cands.append(e)

@@ -175,9 +175,10 @@ int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_pe
                           int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity);
 
 /* ---- per-kernel timing (CUDA events around every launch; no graphs) -----
- * anb_flush_l2 overwrites a buffer twice the size of the L2 cache (allocated
- * on first use) on the network's stream, so that the next kernel starts cold;
- * used between timed repetitions. */
+ * anb_flush_l2 reads a buffer twice the size of the L2 cache (allocated and
+ * filled on first use) on the network's stream, so that the next kernel
+ * starts with a cold cache holding no dirty lines; used between timed
+ * repetitions. */
 int anb_flush_l2(anb_net* net);
 int anb_kernel_timing(anb_net* net, int enable);
 int anb_kernel_time_count(anb_net* net, int* count);

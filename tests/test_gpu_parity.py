@@ -45,7 +45,7 @@ def test_rate_c1_exact(golden):
     assert np.array_equal(r.sum(axis=1), g["r_sum"])
 
 
-@pytest.mark.parametrize("fmt", ["ell", "ellr", "sell", "bsr"])
+@pytest.mark.parametrize("fmt", ["ell", "ellr", "sell", "bsr", "pcsr"])
 def test_rate_formats_exact(golden, fmt):
     """ELL, ELL-R, SELL and BSR sum every row in ascending pre rank:
     bit-identical to CSR."""
@@ -142,7 +142,7 @@ def test_coba_float_rates(engine):
     out["net"].close()
 
 
-@pytest.mark.parametrize("fmt", ["csr", "ell", "ellr", "sell", "hyb", "bsr"])
+@pytest.mark.parametrize("fmt", ["csr", "ell", "ellr", "sell", "hyb", "bsr", "pcsr"])
 @pytest.mark.parametrize("wdt", ["float32", "bfloat16"])
 def test_rate_formats_float(fmt, wdt):
     """Every storage format in single precision: norm-wise relative error of
@@ -154,6 +154,22 @@ def test_rate_formats_float(fmt, wdt):
         rn.w_rec.data = from_bf16(to_bf16(rn.w_rec.data))
     _, ref = O.rate_run(rn, trace=True)
     r = run_rate(rn, 50, precision="float", weight_dtype=wdt, storage_format=fmt, bsr_tile=32)
+    err = np.linalg.norm(r - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-30)
+    assert err.max() <= 1e-5, err.max()
+
+
+@pytest.mark.parametrize("wdt", ["float32", "bfloat16"])
+def test_rate_pcsr_many_panels(wdt):
+    """Panelled CSR with panels of 64 columns (5 panels, atomics between
+    panels, CTAs of a few rows) against the double oracle fed the same
+    weights: norm-wise relative error <= 1e-5 per step."""
+    rn = wl.rate_net(seed=11, n_in=300, n_out=700, p_in=0.1, p_rec=0.05, steps=30)
+    if wdt == "bfloat16":
+        from annarchy_b200.core.backend import from_bf16, to_bf16
+        rn.w_in.data = from_bf16(to_bf16(rn.w_in.data))
+        rn.w_rec.data = from_bf16(to_bf16(rn.w_rec.data))
+    _, ref = O.rate_run(rn, trace=True)
+    r = run_rate(rn, 30, precision="float", weight_dtype=wdt, storage_format="pcsr", pcsr_panel=64)
     err = np.linalg.norm(r - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-30)
     assert err.max() <= 1e-5, err.max()
 

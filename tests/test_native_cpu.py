@@ -43,7 +43,7 @@ def _modules():
     yield "rate-double", wl.build_rate_network(rn, "double")[0]
     yield "rate-float", wl.build_rate_network(rn, "float")[0]
     yield "rate-bf16", wl.build_rate_network(rn, "float", weight_dtype="bfloat16")[0]
-    for fmt in ("ell", "ellr", "sell", "hyb"):
+    for fmt in ("ell", "ellr", "sell", "hyb", "pcsr"):
         yield "rate-" + fmt, wl.build_rate_network(rn, "double", storage_format=fmt)[0]
         yield "rate-float-" + fmt, wl.build_rate_network(rn, "float", storage_format=fmt)[0]
     for prec in ("double", "float"):
