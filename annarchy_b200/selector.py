@@ -131,6 +131,10 @@ class Selector:
 
     # -- training / inference ----------------------------------------------------
     def fit(self, X, Y, M, epochs: int = 3000, lr: float = 3e-3, weight_decay: float = 1e-4):
+        X, Y, M = np.atleast_2d(X), np.atleast_2d(Y), np.atleast_2d(M)
+        if X.shape[1] != self.n_in or Y.shape != (X.shape[0], self.n_out) or M.shape != Y.shape:
+            raise ValueError(f"fit(): expected X (n, {self.n_in}), Y and M (n, {self.n_out}); got "
+                             f"{X.shape}, {Y.shape}, {M.shape}")
         self.mu = X.mean(0)
         self.sd = X.std(0) + 1e-6
         lib = L.load()
@@ -147,6 +151,8 @@ class Selector:
 
     def predict(self, X):
         lib = L.load()
+        if np.atleast_2d(X).shape[1] != self.n_in:
+            raise ValueError(f"predict(): expected {self.n_in} features per row")
         x = np.ascontiguousarray(self._norm(np.atleast_2d(X)))
         y = np.zeros((x.shape[0], self.n_out), np.float32)
         p = np.ascontiguousarray(self.params, np.float32)
@@ -174,8 +180,12 @@ class Selector:
 
     @classmethod
     def load(cls, path):
+        """The model saved at `path`; ValueError if it was trained for another
+        list of schedules or features."""
         with open(path) as f:
             d = json.load(f)
+        if d.get("schedules") != SCHEDULE_NAMES or d.get("features") != tuning.FEATURE_NAMES:
+            raise ValueError(f"{path}: trained for other schedules or features")
         s = cls(hidden=d["hidden"])
         s.params = np.array(d["params"], np.float32)
         s.mu, s.sd = np.array(d["mu"]), np.array(d["sd"])

@@ -28,16 +28,9 @@ SCHEDULES = [
     {"format": "bsr", "bsr_tile": 16},
     {"format": "bsr", "bsr_tile": 32},
     {"format": "bsr", "bsr_tile": 64},
-]
-
-
-# schedules of this backend without a counterpart among the reference's
-# formats (the learned selector predicts over SCHEDULES; the exhaustive
-# autotuner tries ALL_SCHEDULES)
-SCHEDULES_B200 = [
+    # this backend's own schedule (no counterpart among the reference's formats)
     {"format": "pcsr"},
 ]
-ALL_SCHEDULES = SCHEDULES + SCHEDULES_B200
 
 
 def schedule_name(s: dict) -> str:
@@ -169,7 +162,7 @@ class Autotuner:
                                                          else "float64"]
         feat = features(m, wb)
         table = {}
-        cands = list(schedules or ALL_SCHEDULES)
+        cands = list(schedules or SCHEDULES)
         for e in extra:
             if e not in cands and feasible(m, e, 64.0):
                 cands.append(e)

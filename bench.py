@@ -266,7 +266,7 @@ def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
     for st in structures:
         m = wl.sweep_matrix(st)
         rl = np.diff(m.indptr)
-        scheds = tuning.ALL_SCHEDULES if m.nnz < 50_000_000 else [
+        scheds = tuning.SCHEDULES if m.nnz < 50_000_000 else [
             {"format": "csr"}, {"format": "sell", "sell_sigma": 1024}, {"format": "bsr", "bsr_tile": 64},
             {"format": "pcsr"}]
         for dt in dtypes:

@@ -36,6 +36,13 @@ def test_reference_gradient_matches_finite_differences():
         assert abs((lp - lm) / (2 * eps) - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
 
 
+def test_fit_rejects_wrong_shapes():
+    sel = S.Selector(hidden=8, seed=0)
+    X = np.zeros((5, sel.n_in))
+    with pytest.raises(ValueError):
+        sel.fit(X, np.zeros((5, sel.n_out - 1)), np.ones((5, sel.n_out - 1)))
+
+
 def test_features_and_feasibility():
     import scipy.sparse as sp
     rng = np.random.default_rng(0)
@@ -69,11 +76,11 @@ def test_gpu_gradient_matches_reference():
 @pytest.mark.gpu
 def test_gpu_training_fits():
     rng = np.random.default_rng(1)
-    X = rng.normal(size=(200, 13))
-    W = rng.normal(size=(13, 9))
+    sel = S.Selector(hidden=32, seed=3)
+    X = rng.normal(size=(200, sel.n_in))
+    W = rng.normal(size=(sel.n_in, sel.n_out))
     Y = np.tanh(X @ W) * 0.5
     M = np.ones_like(Y)
-    sel = S.Selector(hidden=32, seed=3)
     loss0 = float(((Y - Y.mean(0)) ** 2).mean())
     loss = sel.fit(X, Y, M, epochs=1500, lr=3e-3)
     assert loss < 0.1 * loss0
