@@ -256,6 +256,27 @@ def accuracy_study(seeds=range(42, 50)):
                                                 / sum(r[1] for r in rows))}
 
 
+def stream_read_us(nbytes, reps=5):
+    """Device time of a plain read of `nbytes` (torch sum of a float tensor)
+    after a clean L2 flush (reading 384 MB): the floor any kernel that must
+    read that many cold bytes meets, kernel launch and DRAM ramp included."""
+    import torch
+    x = torch.ones(max(1, int(nbytes) // 4), device="cuda")
+    flush = torch.ones((384 << 20) // 4, device="cuda")
+    ts = []
+    for _ in range(reps):
+        flush.sum()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        x.sum()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) * 1e3)
+    del x, flush
+    return float(sorted(ts)[len(ts) // 2])
+
+
 def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
     """Rate-coded weighted sums of the 100k-neuron recurrent matrices in every
     feasible storage format: cold-L2 kernel time and achieved algorithmic
@@ -274,12 +295,22 @@ def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
             ab = tuning.algorithmic_bytes(m, wb)
             tuner = tuning.Autotuner()
             best, table = tuner.tune(m, "float", dt, reps, scheds, tag=st)
+            floor_us = stream_read_us(ab)
+            sel = None
+            try:
+                from annarchy_b200 import selector as S
+                sel = S.default_model().choose(m) if S.default_model() else None
+            except Exception:       # selector unavailable: reported as None
+                sel = None
             out["results"][f"{st}/{dt}"] = {
                 "nnz": int(m.nnz), "mean_row": float(rl.mean()), "max_row": int(rl.max()),
                 "algorithmic_mb": ab / 1e6, "best": best,
-                "heuristic": tuning.heuristic(m),
+                "heuristic": tuning.heuristic(m), "selector": sel,
+                "stream_floor_us": floor_us,
                 "schedules": {k: {"ms": v, "gbs": ab / (v * 1e-3) / 1e9,
-                                  "frac": ab / (v * 1e-3) / 1e9 / peak} for k, v in table.items()}}
+                                  "frac": ab / (v * 1e-3) / 1e9 / peak,
+                                  "frac_of_stream_floor": floor_us / (v * 1e3)}
+                              for k, v in table.items()}}
             print(json.dumps({f"{st}/{dt}": out["results"][f"{st}/{dt}"]}), flush=True)
     return out
 
@@ -383,7 +414,11 @@ def large_study(n=1_000_000, steps=1000):
     return out
 
 
-def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracle_check=4):
+BATCH_VARIANTS = (("float", "bfloat16"), ("float", "float32"), ("double", None))
+
+
+def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracle_check=4,
+                  variants=BATCH_VARIANTS, verbose=True):
     """Batched instances: uneven-size copies of the spiking net (N ~ U{1000..8000},
     increments swept 0.2-1.0 / 2-10 over a 16x16 grid, one seed each) in one
     persistent launch, fast (float state, bfloat16 weights) and exact (double).
@@ -403,7 +438,7 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
            "generate_s": gen_s}
     peak, peak_kind = peaks()
     counts = {}
-    for prec, wd in (("float", "bfloat16"), ("float", "float32"), ("double", None)):
+    for prec, wd in variants:
         key = prec if prec == "double" else f"float_{wd}"
         t0 = time.time()
         b, members = wl.build_batch(cns, prec, wd)
@@ -465,10 +500,13 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
                            and np.array_equal(members[i][1].v, ref["v"]))
             res["oracle_bit_exact"] = {"instances": pick.tolist(), "ok": ok}
         out[key] = res
-        print(json.dumps({key: res}), flush=True)
+        if verbose:
+            print(json.dumps({key: res}), flush=True)
         b.close()
-    ref = counts["double"]
+    ref = counts.get("double")
     for key in ("float_bfloat16", "float_float32"):
+        if ref is None or key not in counts:
+            continue
         err = np.abs(counts[key] - ref) / np.maximum(ref, 1)
         worst = np.argsort(-err)[:5]
         out[key]["rate_err_per_instance"] = {
@@ -499,8 +537,10 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
     out["plain_fp64"] = {"gsynops": ev / tt / 1e9, "instances": [int(i) for i in pick],
                          "steps": plain_steps}
     out["fast_vs_plain_fp64"] = out["float_bfloat16"]["gsynops"] / out["plain_fp64"]["gsynops"]
-    out["exact_batch_vs_plain_fp64"] = out["double"]["gsynops"] / out["plain_fp64"]["gsynops"]
-    print(json.dumps(out), flush=True)
+    if "double" in out:
+        out["exact_batch_vs_plain_fp64"] = out["double"]["gsynops"] / out["plain_fp64"]["gsynops"]
+    if verbose:
+        print(json.dumps(out), flush=True)
     return out
 
 
@@ -555,6 +595,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-instance summary in the default line")
     ap.add_argument("--fast-only", action="store_true",
                     help="time only the fast path (used for profiler captures)")
     ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
@@ -562,6 +604,8 @@ def main():
                     help="the large plastic network with this many neurons (1000000 = 1e9 synapses)")
     ap.add_argument("--batched", type=int, default=0,
                     help="batched-instance study with this many instances (256 = the sweep)")
+    ap.add_argument("--spmv", default="",
+                    help="one weighted sum: STRUCTURE:FORMAT[:DTYPE] on a 100k matrix (profiling)")
     ap.add_argument("--batched-steps", type=int, default=5000,
                     help="time steps of the batched-instance study")
     ap.add_argument("--formats", default="",
@@ -572,6 +616,20 @@ def main():
         import torch
         torch.cuda.set_device(0)
         large_study(args.large)
+        return
+    if args.spmv:
+        import torch
+        torch.cuda.set_device(0)
+        from annarchy_b200 import tuning, workloads as wl
+        parts = args.spmv.split(":")
+        st, fmt = parts[0], parts[1]
+        dt = parts[2] if len(parts) > 2 else "float32"
+        m = wl.sweep_matrix(st)
+        ms = tuning.measure(m, {"format": fmt}, "float", dt, reps=max(2, args.steps))
+        ab = tuning.algorithmic_bytes(m, 4 if dt == "float32" else 2)
+        peak, kind = peaks()
+        print(json.dumps({"matrix": st, "format": fmt, "dtype": dt, "us": ms * 1e3,
+                          "frac": ab / (ms * 1e-3) / 1e9 / peak, "peak_source": kind}))
         return
     if args.batched:
         import torch
@@ -686,6 +744,20 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
+    # the batched parameter sweep (256 uneven instances in one persistent
+    # launch): fast path only, plain FP64 single-instance path on a sample
+    batched = None
+    if not args.no_batched:
+        bs = batched_study(256, steps=5000, plain_sample=4, plain_steps=300, oracle_check=0,
+                           variants=(("float", "bfloat16"),), verbose=False)
+        f = bs["float_bfloat16"]
+        batched = {"workload": "256 COBA instances, N~U{1000..8000}, p=0.02, 5000 steps, "
+                               "float state / bfloat16 weights",
+                   "gsynops": f["gsynops"], "us_per_step": f["us_per_step"],
+                   "instance_rtf": f["instance_rtf"], "ctas": f["ctas"],
+                   "plain_fp64_gsynops": bs["plain_fp64"]["gsynops"],
+                   "speedup_vs_plain_fp64": bs["fast_vs_plain_fp64"],
+                   "roofline_frac": f["roofline"]["frac"], "clocks": f["clocks"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -708,6 +780,7 @@ def main():
                 "d2h_bytes_per_step": MODEL_STEPS * words * 4},
         "gpu_launches": dev["launches"],
         "clocks": clk.summary(),
+        "batched_sweep": batched,
     }
     print(json.dumps(line))
 
