@@ -107,13 +107,19 @@ class Monitor:
             if v == "spike":
                 s, r = self.spike_arrays()
                 size = self.population.size
-                order = np.argsort(r, kind="stable")       # by rank, steps stay ascending
+                # by rank, steps stay ascending (radix sort for 16-bit ranks)
+                key = r.astype(np.uint16) if size <= 65536 else r
+                order = np.argsort(key, kind="stable")
                 counts = np.bincount(r, minlength=size)
-                chunks = np.split(s[order], np.cumsum(counts)[:-1])
+                offs = np.zeros(size + 1, dtype=np.int64)
+                np.cumsum(counts, out=offs[1:])
+                # one conversion to Python ints, then list slices per neuron
+                steps = s[order].tolist()
+                lo, hi = offs[:-1].tolist(), offs[1:].tolist()
                 if self.ranks is None:
-                    d = dict(zip(range(size), (c.tolist() for c in chunks)))
+                    d = {k: steps[a:b] for k, (a, b) in enumerate(zip(lo, hi))}
                 else:
-                    d = {int(k): chunks[int(k)].tolist() for k in self.ranks}
+                    d = {int(k): steps[lo[int(k)]:hi[int(k)]] for k in self.ranks}
                 out[v] = d
                 if not keep:
                     self._spike_steps, self._spike_ranks = [], []

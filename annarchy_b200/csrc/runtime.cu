@@ -573,7 +573,23 @@ int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_pe
   int64_t k = 0;
   for (int64_t s = 0; s < steps; ++s) {
     const uint32_t* row = words + s * words_per_step;
-    for (int64_t w = 0; w < words_per_step; ++w) {
+    int64_t w = 0;
+    // two words at a time: most words of a raster are zero
+    for (; w + 1 < words_per_step; w += 2) {
+      uint64_t m = (uint64_t)row[w] | ((uint64_t)row[w + 1] << 32);
+      while (m) {
+        const int b = __builtin_ctzll(m);
+        m &= m - 1;
+        const int64_t rank = w * 32 + b;
+        if (rank >= n) continue;
+        if (k < capacity) {
+          out_steps[k] = s;
+          out_ranks[k] = rank;
+        }
+        ++k;
+      }
+    }
+    if (w < words_per_step) {
       uint32_t m = row[w];
       while (m) {
         const int b = __builtin_ctz(m);

@@ -147,7 +147,9 @@ def bitmap_decode(buf: np.ndarray, n: int):
     buf = np.ascontiguousarray(buf, dtype=np.uint32)
     steps, words = buf.shape
     lib = load()
-    cap = int(min(buf.size * 32, max(1024, np.count_nonzero(buf) * 4)))
+    # first guess: one spike per word (np.empty does not touch the pages);
+    # the decoder returns the true count and a second pass follows if needed
+    cap = int(max(1024, buf.size))
     while True:
         s = np.empty(cap, dtype=np.int64)
         r = np.empty(cap, dtype=np.int64)

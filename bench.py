@@ -41,6 +41,9 @@ METRIC = "GSynOps/s (spiking COBA net, 4000 neurons, 1 s model time per step)"
 UNIT = "GSynOps/s"
 WORKLOAD = "coba_lif_4000_p0.02_dt0.1_10000steps_seed42"
 MODEL_STEPS = 10000
+# DRAM bytes (read + write) per launch of the bench's dominant kernel, from one
+# ncu capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum)
+NCU_TRAFFIC = {"anb_cluster_run": 1.193472e6}
 
 
 def dist_env():
@@ -696,7 +699,7 @@ def main():
     peak, peak_kind = peaks()
     achieved = abytes / (k_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+            "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(kname), "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": abytes, "launch_ms": k_ms}
 
     # end to end through the public API (pinned host inputs, raster read back)
