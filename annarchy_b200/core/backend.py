@@ -526,10 +526,9 @@ class CompiledNetwork:
         nat = self.native
         lay = self.mon_layout[mon.id]
         if "spike" in mon.variables:
-            words = lay["words"]
-            buf = np.empty((n, words), dtype=np.uint32)
-            nat.read_into(f"mon{mon.id}__spk", buf)
-            steps, ranks = bitmap_to_spikes(buf, mon.population.size)
+            # decoded on the device: only the (step, rank) pairs are copied back
+            steps, ranks = nat.monitor_decode(f"mon{mon.id}__spk", n, lay["words"],
+                                              mon.population.size)
             mon._append_spikes(steps + t, ranks)
         nrec = 0 if first >= t + n else (t + n - 1 - first) // mon.period_steps + 1
         if nrec > 0:

@@ -23,7 +23,7 @@ import re
 
 import numpy as np
 
-from ..runtime.lib import NativeNet, DryNative, bitmap_decode, device_sm_count
+from ..runtime.lib import NativeNet, DryNative, device_sm_count
 from ..generator.codegen import compensated_vars
 from .backend import BF16, MAX_MONITOR_BYTES, to_bf16, from_bf16
 
@@ -449,9 +449,7 @@ class Batch:
             if not any(net.monitors[j]._recording for net in self.networks):
                 continue
             tw = self.total_words[k]
-            buf = np.empty((n, tw), dtype=np.uint32)
-            self.native.read_into(f"mon{m}__spk", buf)
-            steps, bits = bitmap_decode(buf, tw * 32)
+            steps, bits = self.native.monitor_decode(f"mon{m}__spk", n, tw, tw * 32)
             woff = self.woff[k]
             slot = np.searchsorted(woff * 32, bits, side="right") - 1
             rank = bits - woff[slot] * 32

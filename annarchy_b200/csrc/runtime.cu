@@ -141,6 +141,11 @@ struct anb_net {
   std::map<std::string, int> time_index;
   void* flush_buf = nullptr;
   size_t flush_bytes = 0;
+  // device scratch of anb_monitor_decode (grown on demand)
+  long long* dec_rows = nullptr;
+  int64_t dec_rows_cap = 0;
+  int* dec_out = nullptr;
+  int64_t dec_out_cap = 0;
 };
 
 namespace {
@@ -362,6 +367,8 @@ int anb_destroy(anb_net* net) {
   }
   drop_graph(net);
   if (net->flush_buf) cudaFree(net->flush_buf);
+  if (net->dec_rows) cudaFree(net->dec_rows);
+  if (net->dec_out) cudaFree(net->dec_out);
   if (net->module) g_drv.moduleUnload(net->module);
   for (auto& kv : net->arrays) cudaFree(kv.second.ptr);
   if (net->own_stream) cudaStreamDestroy(net->own_stream);
@@ -565,6 +572,160 @@ int anb_nvrtc_compile(const char* source, const char* options, char* log, size_t
   if (cubin_bytes) *cubin_bytes = sz;
   if (cr != NVRTC_SUCCESS)
     return fail(ANB_ERR_COMPILE, std::string("NVRTC: ") + nvrtcGetErrorString(cr) + "\n" + text);
+  return ANB_OK;
+}
+
+namespace {
+// Spike-ring decoding on the device: one warp per row.
+__device__ __forceinline__ unsigned anb_dec_word(const uint32_t* row, int64_t w, int64_t n) {
+  const int64_t valid = n - 32 * w;                 // bits of this word that are neurons
+  unsigned m = row[w];
+  if (valid <= 0) return 0u;
+  if (valid < 32) m &= (1u << valid) - 1u;
+  return m;
+}
+
+__global__ void anb_dec_count(const uint32_t* __restrict__ ring, int64_t steps, int64_t words,
+                              int64_t n, long long* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < steps; r += nw) {
+    const uint32_t* row = ring + r * words;
+    int c = 0;
+    for (int64_t w = lane; w < words; w += 32) c += __popc(anb_dec_word(row, w, n));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) counts[r] = c;
+  }
+}
+
+// Exclusive prefix sum of counts[0..steps) in place, total in counts[steps]
+// (one CTA of 1024 threads, chunk by chunk with a carry).
+__global__ void anb_dec_scan(long long* __restrict__ counts, int64_t steps) {
+  __shared__ long long sums[32];
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t base = 0; base < steps; base += blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    const long long x = i < steps ? counts[i] : 0;
+    long long incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      long long s = lane < (int)(blockDim.x >> 5) ? sums[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += v;
+      }
+      sums[lane] = s;
+    }
+    __syncthreads();
+    const long long before = carry + (warp ? sums[warp - 1] : 0);
+    if (i < steps) counts[i] = before + incl - x;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = before + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) counts[steps] = carry;
+}
+
+// Pairs in order: out[2k] = step, out[2k+1] = rank.
+__global__ void anb_dec_emit(const uint32_t* __restrict__ ring, int64_t steps, int64_t words,
+                             int64_t n, const long long* __restrict__ offsets, int* __restrict__ out,
+                             int64_t capacity) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < steps; r += nw) {
+    const uint32_t* row = ring + r * words;
+    int64_t base = offsets[r];
+    for (int64_t w0 = 0; w0 < words; w0 += 32) {
+      const int64_t w = w0 + lane;
+      unsigned m = w < words ? anb_dec_word(row, w, n) : 0u;
+      const int c = __popc(m);
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int64_t k = base + incl - c;
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        if (k < capacity) {
+          out[2 * k] = (int)r;
+          out[2 * k + 1] = (int)(w * 32 + b);
+        }
+        ++k;
+      }
+      base += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+}
+}  // namespace
+
+int anb_monitor_decode(anb_net* net, const char* array, int64_t steps, int64_t words_per_step,
+                       int64_t n, int32_t* out_steps, int32_t* out_ranks, int64_t capacity,
+                       int64_t* count) {
+  if (!net || !array || !count || steps < 0 || words_per_step < 0 || capacity < 0)
+    return fail(ANB_ERR_ARG, "bad argument");
+  if (capacity > 0 && (!out_steps || !out_ranks)) return fail(ANB_ERR_ARG, "output is NULL");
+  Array* a = find(net, array);
+  if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + array);
+  if ((size_t)(steps * words_per_step) * 4 > a->bytes)
+    return fail(ANB_ERR_ARG, "more rows requested than the array holds");
+  if (steps >= ((int64_t)1 << 31) || words_per_step * 32 >= ((int64_t)1 << 31))
+    return fail(ANB_ERR_ARG, "ring too large for 32-bit steps and ranks");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  *count = 0;
+  if (steps == 0) return ANB_OK;
+  if (net->dec_rows_cap < steps + 1) {
+    if (net->dec_rows) cudaFree(net->dec_rows);
+    net->dec_rows = nullptr;
+    net->dec_rows_cap = 0;
+    ANB_CUDA(cudaMalloc(&net->dec_rows, (size_t)(steps + 1) * sizeof(long long)));
+    net->dec_rows_cap = steps + 1;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  const uint32_t* ring = static_cast<const uint32_t*>(a->ptr);
+  anb_dec_count<<<sms * 4, 256, 0, net->stream>>>(ring, steps, words_per_step, n, net->dec_rows);
+  anb_dec_scan<<<1, 1024, 0, net->stream>>>(net->dec_rows, steps);
+  ANB_CUDA(cudaGetLastError());
+  long long total = 0;
+  ANB_CUDA(cudaMemcpyAsync(&total, net->dec_rows + steps, sizeof(long long), cudaMemcpyDeviceToHost,
+                           net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  *count = total;
+  const int64_t k = total < capacity ? total : capacity;
+  if (k == 0) return ANB_OK;
+  if (net->dec_out_cap < k) {
+    if (net->dec_out) cudaFree(net->dec_out);
+    net->dec_out = nullptr;
+    net->dec_out_cap = 0;
+    ANB_CUDA(cudaMalloc(&net->dec_out, (size_t)k * 2 * sizeof(int)));
+    net->dec_out_cap = k;
+  }
+  anb_dec_emit<<<sms * 4, 256, 0, net->stream>>>(ring, steps, words_per_step, n, net->dec_rows,
+                                                 net->dec_out, k);
+  ANB_CUDA(cudaGetLastError());
+  std::vector<int> pairs((size_t)k * 2);
+  ANB_CUDA(cudaMemcpyAsync(pairs.data(), net->dec_out, (size_t)k * 2 * sizeof(int),
+                           cudaMemcpyDeviceToHost, net->stream));
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  for (int64_t i = 0; i < k; ++i) {
+    out_steps[i] = pairs[2 * i];
+    out_ranks[i] = pairs[2 * i + 1];
+  }
   return ANB_OK;
 }
 

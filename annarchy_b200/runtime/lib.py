@@ -45,6 +45,8 @@ SIGNATURES = {
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
+    "anb_monitor_decode": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_int64, C.c_int64,
+                                     C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     "anb_bitmap_decode": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p,
                                       C.c_void_p, C.c_int64]),
     "anb_plan_clear": (C.c_int, [C.c_void_p]),
@@ -230,6 +232,22 @@ class NativeNet:
     def read_into(self, name: str, out: np.ndarray, offset_bytes: int = 0):
         check("anb_array_read", self.lib.anb_array_read(
             self.h, name.encode(), offset_bytes, out.ctypes.data_as(C.c_void_p), out.nbytes))
+
+    def monitor_decode(self, name: str, steps: int, words: int, n: int):
+        """(step, rank) int64 arrays of the spikes in the first `steps` rows of
+        the spike ring `name`, decoded on the device (sorted by step, rank)."""
+        cap = int(max(1024, steps * words))
+        for _ in range(2):
+            s = np.empty(cap, dtype=np.int32)
+            r = np.empty(cap, dtype=np.int32)
+            k = C.c_int64(0)
+            check("anb_monitor_decode", self.lib.anb_monitor_decode(
+                self.h, name.encode(), int(steps), int(words), int(n),
+                s.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p), cap, C.byref(k)))
+            if k.value <= cap:
+                return s[:k.value].astype(np.int64), r[:k.value].astype(np.int64)
+            cap = int(k.value)
+        raise RuntimeError("monitor_decode: spike count changed between calls")
 
     def zero(self, name: str):
         check("anb_array_fill_zero", self.lib.anb_array_fill_zero(self.h, name.encode()))

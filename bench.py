@@ -11,8 +11,10 @@ the spike raster recorded on the device.
              state resident in the shared memory of one thread-block cluster),
              device time (CUDA events)
   e2e        the same through the public API: per step the initial state is
-             copied from pinned host memory, the simulation runs and the
-             spike raster is read back and decoded on the host (wall clock)
+             copied from pinned host memory, the simulation runs, the spike
+             raster is decoded on the device and read back as (step, rank)
+             pairs, and Monitor.get() builds the per-neuron spike lists
+             (wall clock)
   fp64_path  the plain double-precision GPU path (bit-identical to the
              reference; one kernel per phase, launched every step)
 GSynOps = delivered synaptic events (sum over spikes of the out-degree of
@@ -173,17 +175,21 @@ def time_device(net, P, mon, cn, steps, warmup):
 def time_graph_free(net, P, mon, cn, steps):
     """Wall time of a run (used for the multi-kernel FP64 path, whose kernels
     are too many to wrap in events one by one): device synchronised on both
-    sides, so it is the device time plus launch gaps."""
+    sides, so it is the device time plus launch gaps; the monitor drain after
+    the run is not timed."""
     import torch
     out_deg = cn.out_degree()
     res = []
+    be = net._backend
     for _ in range(steps):
         reset_state(net, P, cn)
+        starts = be.begin_chunk(0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        net.simulate_steps(MODEL_STEPS)
-        net._backend.native.synchronize()
+        be.native.run(MODEL_STEPS)
+        be.native.synchronize()
         t1 = time.perf_counter()
+        be.end_chunk(0, MODEL_STEPS, starts)          # monitor drain, untimed
         e, _ = events_of(mon, out_deg)
         mon.get("spike")
         res.append(((t1 - t0) * 1e3, e))
@@ -537,8 +543,16 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
         _, r_ = mon.spike_arrays()
         ev += int(cn.out_degree()[r_].sum())
         net.close()
-    out["plain_fp64"] = {"gsynops": ev / tt / 1e9, "instances": [int(i) for i in pick],
-                         "steps": plain_steps}
+    # the plain path's step time hardly depends on the activity (one launch
+    # per phase), its events do: its GSynOps/s over the whole sweep is the
+    # sweep's events (as delivered by the batch) over n_inst x steps x the
+    # sampled time per instance-step
+    us_inst_step = tt * 1e6 / (plain_steps * len(pick))
+    first = out[next(k for k in out if k.startswith("float") or k == "double")]
+    est = first["events"] / (n_inst * steps * us_inst_step * 1e-6) / 1e9
+    out["plain_fp64"] = {"gsynops": est, "us_per_instance_step": us_inst_step,
+                         "sampled_gsynops": ev / tt / 1e9,
+                         "instances": [int(i) for i in pick], "steps": plain_steps}
     out["fast_vs_plain_fp64"] = out["float_bfloat16"]["gsynops"] / out["plain_fp64"]["gsynops"]
     if "double" in out:
         out["exact_batch_vs_plain_fp64"] = out["double"]["gsynops"] / out["plain_fp64"]["gsynops"]
@@ -706,7 +720,7 @@ def main():
     out_deg = cn.out_degree()
     v0_pin = torch.from_numpy(cn.v0.astype(np.float32)).pin_memory()
     zeros_pin = torch.zeros(cn.n, dtype=torch.float32).pin_memory()
-    e2e_t, e2e_ev = [], []
+    e2e_t, e2e_ev, e2e_sp = [], [], []
     for it in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -719,6 +733,7 @@ def main():
         if it >= args.warmup:
             e2e_t.append(t1 - t0)
             e2e_ev.append(sum(out_deg[k] * len(v) for k, v in spikes.items()))
+            e2e_sp.append(sum(len(v) for v in spikes.values()))
     e2e_val = world * (sum(e2e_ev) / len(e2e_ev)) / (sum(e2e_t) / len(e2e_t)) / 1e9
     words = (cn.n + 31) // 32
     net_engine = net.engine
@@ -759,6 +774,7 @@ def main():
                    "gsynops": f["gsynops"], "us_per_step": f["us_per_step"],
                    "instance_rtf": f["instance_rtf"], "ctas": f["ctas"],
                    "plain_fp64_gsynops": bs["plain_fp64"]["gsynops"],
+                   "plain_fp64_us_per_instance_step": bs["plain_fp64"]["us_per_instance_step"],
                    "speedup_vs_plain_fp64": bs["fast_vs_plain_fp64"],
                    "roofline_frac": f["roofline"]["frac"], "clocks": f["clocks"]}
     line = {
@@ -780,7 +796,9 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": UNIT,
                 "h2d_bytes_per_step": 3 * cn.n * 4 + cn.n * 4 + 8,
-                "d2h_bytes_per_step": MODEL_STEPS * words * 4},
+                # the raster is decoded on the device: (step, rank) int32 pairs and
+                # the spike count cross the bus
+                "d2h_bytes_per_step": int(8 * sum(e2e_sp) / len(e2e_sp) + 8)},
         "gpu_launches": dev["launches"],
         "clocks": clk.summary(),
         "batched_sweep": batched,

@@ -171,6 +171,17 @@ int anb_clear_device_error(anb_net* net);
  * host side of the reference's spike recorder (recording_spike_tpl in
  * ANNarchy/generator/Monitor/BaseTemplates.py). Writes at most `capacity`
  * pairs and returns the total number of spikes. Host memory only. */
+/* The same decoding on the device, for the first `steps` rows of the spike
+ * ring `array` of `net` (words_per_step words per row, bit b of word w =
+ * neuron 32*w+b, bits >= n ignored): writes at most `capacity` (step, rank)
+ * pairs, sorted by step then rank, into the host arrays and the total number
+ * of spikes into *count. Only the pairs cross the bus, not the bitmaps
+ * (the reference copies the recorded spikes to the host every step,
+ * ANNarchy/generator/Monitor/CUDATemplates.py:83). */
+int anb_monitor_decode(anb_net* net, const char* array, int64_t steps, int64_t words_per_step,
+                       int64_t n, int32_t* out_steps, int32_t* out_ranks, int64_t capacity,
+                       int64_t* count);
+
 int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
                           int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity);
 
