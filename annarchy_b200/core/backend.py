@@ -17,12 +17,11 @@ Array names (the generated module binds a __constant__ pointer to each):
 """
 from __future__ import annotations
 
-import math
 
 import numpy as np
 
 from ..generator import formats as F
-from ..generator.codegen import BLOCK, CodeGenerator, compensated_vars, grid_for
+from ..generator.codegen import CodeGenerator, compensated_vars, grid_for
 from ..runtime.lib import DryNative, NativeNet
 
 BF16 = np.uint16

@@ -25,7 +25,7 @@ import numpy as np
 
 from ..runtime.lib import NativeNet, DryNative, device_sm_count
 from ..generator.codegen import compensated_vars
-from .backend import BF16, MAX_MONITOR_BYTES, to_bf16, from_bf16
+from .backend import BF16, MAX_MONITOR_BYTES, to_bf16
 
 # opt-in dynamic shared memory of one CTA on sm_100 (227 KB)
 SMEM_LIMIT = 232448

@@ -735,7 +735,6 @@ def main():
             e2e_ev.append(sum(out_deg[k] * len(v) for k, v in spikes.items()))
             e2e_sp.append(sum(len(v) for v in spikes.values()))
     e2e_val = world * (sum(e2e_ev) / len(e2e_ev)) / (sum(e2e_t) / len(e2e_t)) / 1e9
-    words = (cn.n + 31) // 32
     net_engine = net.engine
     net.close()
 
