@@ -17,7 +17,6 @@ Array names (the generated module binds a __constant__ pointer to each):
 """
 from __future__ import annotations
 
-
 import numpy as np
 
 from ..generator import formats as F
