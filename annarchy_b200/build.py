@@ -47,13 +47,16 @@ def _sources(*rel):
 def build_runtime(force=False, verbose=False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     out = os.path.join(LIB_DIR, "libannarchy_b200.so")
-    srcs = _sources("runtime.cu", "selector.cu", "connect.cuh") + [
+    srcs = _sources("runtime.cu", "selector.cu", "bsr_tc.cu", "connect.cuh",
+                    "device/anb_device.cuh") + [
         os.path.join(os.path.dirname(HERE), "include", "annarchy_b200.h")]
     srcs = [s for s in srcs if os.path.exists(s)]
     if force or _newer(out, srcs):
         cu = [s for s in srcs if s.endswith(".cu")]
-        _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-              "-o", out, *cu, "-lnvrtc"], verbose)
+        log = _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xptxas", "-v", "-shared",
+                    "-Xcompiler", "-fPIC", "-I", CSRC, "-o", out, *cu, "-lnvrtc"], verbose)
+        with open(os.path.join(LIB_DIR, "runtime.ptxas.txt"), "w") as f:
+            f.write(log)
     return out
 
 

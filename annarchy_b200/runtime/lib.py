@@ -45,6 +45,11 @@ SIGNATURES = {
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
+    "anb_bsr_tc_pack_x": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "anb_bsr_spmm_tc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                  C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "anb_bsr_spmm_simt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "anb_monitor_decode": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_int64, C.c_int64,
                                      C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     "anb_bitmap_decode": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p,

@@ -561,6 +561,67 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
     return out
 
 
+def spmm_study(batches=(64, 128, 256), reps=5):
+    """Batched weighted sums over the 100k-neuron block matrix (64x64 blocks,
+    2 % block density, bfloat16): tcgen05 tensor cores vs CUDA cores. Device
+    time per product with the weights cold (clean L2 flush before each
+    repetition; the packed rates, 100k x batch bfloat16, are read from L2),
+    TFLOP/s (2 x stored block entries x batch) and HBM fraction of the
+    weight bytes."""
+    import torch
+    from annarchy_b200 import spmm, workloads as wl
+    peak, kind = peaks()
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            tpk = float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        tpk = 1590.0
+    m = wl.sweep_matrix("blocks")
+    flush = torch.ones((384 << 20) // 4, device="cuda")
+    out = {"matrix": "100k blocks 64x64, 2 %", "nnz": int(m.nnz), "hbm_peak_gbs": peak,
+           "bf16_tflops_peak": tpk, "results": {}}
+    for batch in batches:
+        bsb = spmm.BlockSparseBatch(m, batch)
+        x = np.random.default_rng(batch).uniform(0, 1, (batch, m.shape[1])).astype(np.float32)
+        # correctness on a sample of rows
+        y = bsb(x, "tc")
+        rows = np.random.default_rng(1).choice(m.shape[0], 64, replace=False)
+        from annarchy_b200.core.backend import from_bf16, to_bf16
+        wq = m[rows].toarray()
+        wq = from_bf16(to_bf16(wq.astype(np.float32)))
+        ref = (wq @ from_bf16(to_bf16(x)).T).T
+        rel = float(np.linalg.norm(y[:, rows] - ref) / np.linalg.norm(ref))
+        res = {"rel_err_sample": rel}
+        for eng in ("tc", "simt") if batch in (64, 128, 256) else ("tc",):
+            ts = []
+            for _ in range(reps):
+                bsb.load(x)
+                bsb.run(eng)                      # warm + pack
+                flush.sum()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                bsb.run(eng)
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            bsb.result()
+            ms = sorted(ts)[len(ts) // 2]
+            stored = bsb.n_blocks * 64 * 64
+            flops = 2.0 * stored * batch
+            wbytes = stored * 2
+            res[eng] = {"us": ms * 1e3, "tflops": flops / (ms * 1e-3) / 1e12,
+                        "tensor_frac": flops / (ms * 1e-3) / 1e12 / tpk,
+                        "weight_gbs": wbytes / (ms * 1e-3) / 1e9,
+                        "hbm_frac": wbytes / (ms * 1e-3) / 1e9 / peak}
+        if "simt" in res:
+            res["tc_speedup"] = res["simt"]["us"] / res["tc"]["us"]
+        out["results"][batch] = res
+        print(json.dumps({batch: res}), flush=True)
+        bsb.close()
+    return out
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -623,6 +684,9 @@ def main():
                     help="batched-instance study with this many instances (256 = the sweep)")
     ap.add_argument("--spmv", default="",
                     help="one weighted sum: STRUCTURE:FORMAT[:DTYPE] on a 100k matrix (profiling)")
+    ap.add_argument("--spmm", default="",
+                    help="batched block-sparse products on the tensor cores for these batch "
+                         "sizes (comma separated, e.g. 64,128,256)")
     ap.add_argument("--batched-steps", type=int, default=5000,
                     help="time steps of the batched-instance study")
     ap.add_argument("--formats", default="",
@@ -633,6 +697,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         large_study(args.large)
+        return
+    if args.spmm:
+        import torch
+        torch.cuda.set_device(0)
+        spmm_study(tuple(int(b) for b in args.spmm.split(",")))
         return
     if args.spmv:
         import torch

@@ -185,6 +185,34 @@ int anb_monitor_decode(anb_net* net, const char* array, int64_t steps, int64_t w
 int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
                           int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity);
 
+/* ---- batched weighted sums on the tensor cores --------------------------
+ * Y[b][post] += sum_pre W[post][pre] * X[b][pre] for `batch` instances that
+ * share a block-sparse weight matrix of dense 64 x 64 bfloat16 tiles (the
+ * reference's BSR container, ANNarchy/include/BSRMatrix.hpp:41, whose CUDA
+ * weighted sum, ANNarchy/generator/Projection/CUDA/BSR.py:296, handles one
+ * instance per launch). All pointers are device pointers; `stream` is a
+ * cudaStream_t (NULL: the default stream).
+ *   a_tiles   n_blocks tiles of 4096 bfloat16 in the tcgen05 canonical
+ *             K-major layout (element (r, k) of a tile at
+ *             ((r/8)*8 + k/8)*64 + (r%8)*8 + k%8)
+ *   x_tiles   ceil(n_pre/64) tiles of batch*64 bfloat16, same layout with
+ *             the instance as row: written by anb_bsr_tc_pack_x from
+ *             X (batch x n_pre float, row-major)
+ *   y         batch x n_post float, row-major, accumulated into
+ * batch: a multiple of 16, at most 256 (64, 128 or 256 for
+ * anb_bsr_spmm_simt). anb_bsr_spmm_tc runs on the tensor
+ * cores (tcgen05.mma, accumulators in tensor memory; bounded waits report
+ * ANB_DEVERR_BARRIER_TIMEOUT in *err); anb_bsr_spmm_simt computes the same on
+ * the CUDA cores (the comparison baseline). Return 0, 2 (bad argument) or 4
+ * (CUDA error). No counterpart in the reference for the batched form. */
+int anb_bsr_tc_pack_x(const float* x, int batch, int n_pre, uint16_t* x_tiles, void* stream);
+int anb_bsr_spmm_tc(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
+                    int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
+                    int* err, void* stream);
+int anb_bsr_spmm_simt(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
+                      int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
+                      void* stream);
+
 /* ---- per-kernel timing (CUDA events around every launch; no graphs) -----
  * anb_flush_l2 reads a buffer twice the size of the L2 cache (allocated and
  * filled on first use) on the network's stream, so that the next kernel
