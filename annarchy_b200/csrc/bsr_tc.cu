@@ -10,9 +10,9 @@
 // matrix product, which belongs on the tensor cores.
 //
 // Kernel bsr_spmm_tc_kernel: one CTA (one warpgroup, 128 threads) per block row.
-// Thread 0 streams the row's blocks through a STAGES-deep ring of shared-
+// One thread streams the row's blocks through a STAGES-deep ring of shared-
 // memory stages with bulk copies (cp.async.bulk, completing on an mbarrier
-// per stage; no multicast), and issues per block four tcgen05.mma of
+// per stage; no multicast); another thread issues per block four tcgen05.mma of
 // M=64, N=batch, K=16 (kind::f16, bf16 x bf16 -> f32) that accumulate in
 // tensor memory; tcgen05.commit releases each stage when its products are
 // done. The four warps then read the accumulator with tcgen05.ld (warp w owns
@@ -38,6 +38,7 @@ constexpr int kTile = 64;                 // block rows / columns
 constexpr int kStages = 4;
 constexpr unsigned kTileBytes = kTile * kTile * 2;   // 8 KB of bf16
 constexpr int kWaitTries = 1 << 22;
+constexpr int kColCache = 512;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -116,7 +117,8 @@ bsr_spmm_tc_kernel(const int* __restrict__ brow_ptr, const int* __restrict__ bco
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
   __shared__ uint32_t tmem_base;
-  __shared__ int abort_flag;
+  __shared__ int abort_flag, issued_n, consumed_n;
+  __shared__ int bcol_s[kColCache];        // the row's block columns (first kColCache)
   const unsigned x_bytes = (unsigned)batch * kTile * 2;
   const unsigned stage_bytes = kTileBytes + x_bytes;
   const int br = blockIdx.x;
@@ -136,51 +138,59 @@ bsr_spmm_tc_kernel(const int* __restrict__ brow_ptr, const int* __restrict__ bco
     mbar_init(&done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
+    issued_n = 0;
+    consumed_n = 0;
   }
+  for (int q = threadIdx.x; q < nblk && q < kColCache; q += blockDim.x) bcol_s[q] = bcol[beg + q];
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t taddr = tmem_base;
 
-  if (threadIdx.x == 0 && nblk > 0) {
+  // warp 0 lane 0 streams the blocks into the stage ring, warp 1 lane 0
+  // issues the products as stages fill: neither waits on the other's latency
+  if (nblk > 0 && threadIdx.x == 0) {
+    int k = 0;
+    for (; k < nblk; ++k) {
+      const int s = k % kStages, u = k / kStages;
+      if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1)) {
+        anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+        abort_flag = 1;
+        break;
+      }
+      unsigned char* st = smem + s * stage_bytes;
+      mbar_expect_tx(&full[s], stage_bytes);
+      bulk_load(st, a_tiles + (size_t)(beg + k) * (kTile * kTile), kTileBytes, &full[s]);
+      const int bc = k < kColCache ? bcol_s[k] : bcol[beg + k];
+      bulk_load(st + kTileBytes, x_tiles + (size_t)bc * batch * kTile, x_bytes, &full[s]);
+    }
+    issued_n = k;
+  } else if (nblk > 0 && threadIdx.x == 32) {
     const uint32_t idesc = instr_desc(kTile, batch);
-    int issued = 0, consumed = 0;
-    bool ok = true;
-    for (int k = 0; ok && k < nblk + kStages - 1; ++k) {
-      if (k < nblk) {                         // copy block k into stage k % kStages
-        const int s = k % kStages, u = k / kStages;
-        if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1)) { ok = false; break; }
-        unsigned char* st = smem + s * stage_bytes;
-        mbar_expect_tx(&full[s], stage_bytes);
-        bulk_load(st, a_tiles + (size_t)(beg + k) * (kTile * kTile), kTileBytes, &full[s]);
-        bulk_load(st + kTileBytes, x_tiles + (size_t)bcol[beg + k] * batch * kTile, x_bytes, &full[s]);
-        ++issued;
+    int k = 0;
+    for (; k < nblk; ++k) {
+      const int s = k % kStages, u = k / kStages;
+      if (!mbar_wait(&full[s], u & 1)) {
+        anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+        abort_flag = 1;
+        break;
       }
-      const int kk = k - (kStages - 1);
-      if (kk >= 0) {                          // products of block kk
-        const int s = kk % kStages, u = kk / kStages;
-        if (!mbar_wait(&full[s], u & 1)) { ok = false; break; }
-        ++consumed;
-        const unsigned a0 = smem_u32(smem + s * stage_bytes);
-        const unsigned b0 = a0 + kTileBytes;
+      const unsigned a0 = smem_u32(smem + s * stage_bytes);
+      const unsigned b0 = a0 + kTileBytes;
 #pragma unroll
-        for (int q = 0; q < kTile / 16; ++q) {
-          umma_f16(taddr, smem_desc(a0 + q * 256, 128, 1024), smem_desc(b0 + q * 256, 128, 1024),
-                   idesc, (kk > 0 || q > 0) ? 1u : 0u);
-        }
-        umma_commit(&empty[s]);
+      for (int q = 0; q < kTile / 16; ++q) {
+        umma_f16(taddr, smem_desc(a0 + q * 256, 128, 1024), smem_desc(b0 + q * 256, 128, 1024),
+                 idesc, (k > 0 || q > 0) ? 1u : 0u);
       }
+      umma_commit(&empty[s]);
     }
+    consumed_n = k;
     umma_commit(&done);                       // after every issued product
-    if (!ok) {
-      anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
-      abort_flag = 1;
-      // copies issued but not consumed: wait for them (bounded) before leaving
-      for (int k = consumed; k < issued; ++k) {
-        const int s = k % kStages, u = k / kStages;
-        mbar_wait(&full[s], u & 1);
-      }
-    }
+  }
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) {
+    // copies issued but never consumed: wait for them (bounded) before leaving
+    for (int k = consumed_n; k < issued_n; ++k) mbar_wait(&full[k % kStages], (k / kStages) & 1);
   }
   __syncthreads();
   if (nblk > 0) {
@@ -192,12 +202,20 @@ bsr_spmm_tc_kernel(const int* __restrict__ brow_ptr, const int* __restrict__ bco
     if (all_ok) {
       // warp w reads TMEM lanes 32w..32w+31; lanes 0-15 hold rows 16w..16w+15
       const int row = br * kTile + 16 * warp + lane;
+      const bool mine = lane < 16 && row < n_post;
       for (int c0 = 0; c0 < batch; c0 += 16) {
+        // the 16 loads of Y go out together (written before any store, so
+        // they need not wait for one another) and overlap the tensor-memory read
+        float old[16];
         uint32_t r[16];
-        tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, r);
-        if (lane < 16 && row < n_post) {
+        if (mine) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) y[(size_t)(c0 + j) * n_post + row] += __uint_as_float(r[j]);
+          for (int j = 0; j < 16; ++j) old[j] = y[(size_t)(c0 + j) * n_post + row];
+        }
+        tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, r);
+        if (mine) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) y[(size_t)(c0 + j) * n_post + row] = old[j] + __uint_as_float(r[j]);
         }
       }
     }
@@ -260,20 +278,43 @@ bsr_spmm_simt_kernel(const int* __restrict__ brow_ptr, const int* __restrict__ b
 }
 
 // fp32 X[b][pre] -> bf16 tiles in the canonical layout (zero past n_pre).
+// One thread per (instance, 8 consecutive neurons): a coalesced 32-byte read
+// of X, one 16-byte row of a core matrix written.
+__device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
+  const uint32_t a = __float_as_uint(lo), b = __float_as_uint(hi);
+  const uint32_t ra = (a + 0x7FFFu + ((a >> 16) & 1u)) >> 16;   // round to nearest even
+  const uint32_t rb = (b + 0x7FFFu + ((b >> 16) & 1u)) >> 16;
+  return ra | (rb << 16);
+}
+
 __global__ void bsr_pack_x_kernel(const float* __restrict__ x, int batch, int n_pre, int n_bcols,
-                               uint16_t* __restrict__ xt) {
-  const long long total = (long long)n_bcols * batch * kTile;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long tile = e / (batch * kTile);
-    const int in_tile = (int)(e % (batch * kTile));
-    const int core = in_tile >> 6, in = in_tile & 63;
-    const int b = (core >> 3) * 8 + (in >> 3), k = (core & 7) * 8 + (in & 7);
-    const long long pre = tile * kTile + k;
-    const float v = pre < n_pre ? x[(size_t)b * n_pre + pre] : 0.f;
-    // round to nearest even
-    const uint32_t u = __float_as_uint(v);
-    xt[e] = (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+                                  uint16_t* __restrict__ xt) {
+  const long long chunks = (long long)n_bcols * 8;             // 8-neuron chunks per instance
+  const long long total = chunks * batch;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / chunks);
+    const long long c = t - (long long)b * chunks;
+    const long long pre0 = c * 8;
+    float v[8];
+    const float* src = x + (size_t)b * n_pre + pre0;
+    if (pre0 + 8 <= n_pre && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+      const float4 lo = *reinterpret_cast<const float4*>(src);
+      const float4 hi = *reinterpret_cast<const float4*>(src + 4);
+      v[0] = lo.x; v[1] = lo.y; v[2] = lo.z; v[3] = lo.w; v[4] = hi.x; v[5] = hi.y; v[6] = hi.z; v[7] = hi.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] = pre0 + e < n_pre ? src[e] : 0.f;
+    }
+    const long long tile = c >> 3;
+    const int kc = (int)(c & 7);                                 // group of 8 along K
+    uint16_t* dst = xt + tile * (long long)batch * kTile + ((b >> 3) * 8 + kc) * 64 + (b & 7) * 8;
+    uint4 o;
+    o.x = bf16_pair(v[0], v[1]);
+    o.y = bf16_pair(v[2], v[3]);
+    o.z = bf16_pair(v[4], v[5]);
+    o.w = bf16_pair(v[6], v[7]);
+    *reinterpret_cast<uint4*>(dst) = o;
   }
 }
 
@@ -284,7 +325,7 @@ extern "C" {
 int anb_bsr_tc_pack_x(const float* x, int batch, int n_pre, uint16_t* x_tiles, void* stream) {
   if (!x || !x_tiles || batch <= 0 || batch % 16 != 0 || batch > 256 || n_pre <= 0) return 2;
   const int n_bcols = (n_pre + kTile - 1) / kTile;
-  bsr_pack_x_kernel<<<296, 256, 0, (cudaStream_t)stream>>>(x, batch, n_pre, n_bcols, x_tiles);
+  bsr_pack_x_kernel<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(x, batch, n_pre, n_bcols, x_tiles);
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 

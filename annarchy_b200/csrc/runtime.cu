@@ -412,6 +412,14 @@ int anb_set_stream(anb_net* net, void* cuda_stream) {
   return ANB_OK;
 }
 
+int anb_get_stream(anb_net* net, void** cuda_stream) {
+  if (!net || !cuda_stream) return fail(ANB_ERR_ARG, "NULL argument");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  *cuda_stream = (void*)net->stream;
+  return ANB_OK;
+}
+
 int anb_array_create(anb_net* net, const char* name, size_t bytes) {
   if (!net || !name || !*name) return fail(ANB_ERR_ARG, "NULL argument");
   int rc = ensure_device(net);

@@ -45,6 +45,7 @@ SIGNATURES = {
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
+    "anb_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "anb_bsr_tc_pack_x": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "anb_bsr_spmm_tc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                   C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
@@ -237,6 +238,12 @@ class NativeNet:
     def read_into(self, name: str, out: np.ndarray, offset_bytes: int = 0):
         check("anb_array_read", self.lib.anb_array_read(
             self.h, name.encode(), offset_bytes, out.ctypes.data_as(C.c_void_p), out.nbytes))
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) the network's work runs on."""
+        out = C.c_void_p()
+        check("anb_get_stream", self.lib.anb_get_stream(self.h, C.byref(out)))
+        return out.value or 0
 
     def monitor_decode(self, name: str, steps: int, words: int, n: int):
         """(step, rank) int64 arrays of the spikes in the first `steps` rows of

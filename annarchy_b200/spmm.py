@@ -76,6 +76,8 @@ class BlockSparseBatch:
         nat.create("y", np.zeros((batch, self.n_post), np.float32))
         nat.create("kerr", np.zeros(1, np.int32))
         self._p = {n: nat.device_ptr(n) for n in ("brow", "bcol", "tiles", "x", "xt", "y", "kerr")}
+        # the products run on the stream of the arrays' copies
+        self._stream = C.c_void_p(nat.stream())
 
     def _check(self, name, rc):
         if rc != 0:
@@ -92,17 +94,17 @@ class BlockSparseBatch:
         """Pack the loaded rates and add W x into y on the device (no sync)."""
         lib, p = L.load(), self._p
         self._check("anb_bsr_tc_pack_x", lib.anb_bsr_tc_pack_x(
-            C.c_void_p(p["x"]), self.batch, self.n_pre, C.c_void_p(p["xt"]), None))
+            C.c_void_p(p["x"]), self.batch, self.n_pre, C.c_void_p(p["xt"]), self._stream))
         if engine == "tc":
             self._check("anb_bsr_spmm_tc", lib.anb_bsr_spmm_tc(
                 C.c_void_p(p["brow"]), C.c_void_p(p["bcol"]), C.c_void_p(p["tiles"]),
                 self.n_block_rows, C.c_void_p(p["xt"]), self.batch, C.c_void_p(p["y"]),
-                self.n_post, C.c_void_p(p["kerr"]), None))
+                self.n_post, C.c_void_p(p["kerr"]), self._stream))
         elif engine == "simt":
             self._check("anb_bsr_spmm_simt", lib.anb_bsr_spmm_simt(
                 C.c_void_p(p["brow"]), C.c_void_p(p["bcol"]), C.c_void_p(p["tiles"]),
                 self.n_block_rows, C.c_void_p(p["xt"]), self.batch, C.c_void_p(p["y"]),
-                self.n_post, None))
+                self.n_post, self._stream))
         else:
             raise ValueError(engine)
 

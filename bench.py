@@ -592,6 +592,7 @@ def spmm_study(batches=(64, 128, 256), reps=5):
         ref = (wq @ from_bf16(to_bf16(x)).T).T
         rel = float(np.linalg.norm(y[:, rows] - ref) / np.linalg.norm(ref))
         res = {"rel_err_sample": rel}
+        stream = torch.cuda.ExternalStream(bsb.nat.stream())   # where the products run
         for eng in ("tc", "simt") if batch in (64, 128, 256) else ("tc",):
             ts = []
             for _ in range(reps):
@@ -600,9 +601,9 @@ def spmm_study(batches=(64, 128, 256), reps=5):
                 flush.sum()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 torch.cuda.synchronize()
-                e0.record()
+                e0.record(stream)
                 bsb.run(eng)
-                e1.record()
+                e1.record(stream)
                 torch.cuda.synchronize()
                 ts.append(e0.elapsed_time(e1))
             bsb.result()

@@ -81,6 +81,10 @@ int anb_get_time(anb_net* net, int64_t* t);
 /* Use a caller-provided cudaStream_t (NULL: the library's own stream). */
 int anb_set_stream(anb_net* net, void* cuda_stream);
 
+/* The stream the network's kernels and copies run on (a cudaStream_t), so
+ * that other work can be ordered with them. No counterpart in the reference. */
+int anb_get_stream(anb_net* net, void** cuda_stream);
+
 /* ---- named device arrays ------------------------------------------------
  * Replace the per-attribute get/set properties of pop<k>_wrapper and the
  * init_from_lil / get/set_local_attribute_* methods of proj<k>_wrapper

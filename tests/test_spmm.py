@@ -76,3 +76,16 @@ def test_tc_empty_block_rows_and_accumulation():
     y = bsb.result()
     assert np.allclose(y[:, 70], 1.0) and np.count_nonzero(y) == 64
     bsb.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("batch,n_pre", [(16, 100), (64, 200), (256, 131)])
+def test_pack_x_device_matches_host(batch, n_pre):
+    w = _blocks(64, n_pre, 1.0, 0)
+    bsb = spmm.BlockSparseBatch(w, batch)
+    x = np.random.default_rng(batch).normal(size=(batch, n_pre)).astype(np.float32)
+    bsb.load(x)
+    bsb.run("tc")
+    bsb.result()
+    assert np.array_equal(bsb.nat.read("xt"), spmm.pack_x_reference(x))
+    bsb.close()
