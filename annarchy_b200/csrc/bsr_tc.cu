@@ -9,17 +9,29 @@
 // (parameter sweeps of a rate-coded network) every block becomes a 64 x 64 x B
 // matrix product, which belongs on the tensor cores.
 //
-// Kernel bsr_spmm_tc_kernel: one CTA (one warpgroup, 128 threads) per block row.
-// One thread streams the row's blocks through a STAGES-deep ring of shared-
-// memory stages with bulk copies (cp.async.bulk, completing on an mbarrier
-// per stage; no multicast); another thread issues per block four tcgen05.mma of
-// M=64, N=batch, K=16 (kind::f16, bf16 x bf16 -> f32) that accumulate in
-// tensor memory; tcgen05.commit releases each stage when its products are
-// done. The four warps then read the accumulator with tcgen05.ld (warp w owns
-// rows 16w..16w+15 of the 64-row tile: lanes 0-15 of TMEM sub-partition w)
-// and add it into Y. Every mbarrier wait is bounded: a timeout sets the error
-// word, the CTA waits (bounded) for its outstanding copies and products, frees
-// its tensor memory and returns.
+// Kernel bsr_spmm_tc_kernel (persistent: up to three CTAs per SM, each taking
+// block rows blockIdx.x, blockIdx.x + gridDim.x, ...), six warps with fixed
+// roles:
+//   warp 4 streams the CTA's rows through a ring of shared-memory stages of
+//     GROUP consecutive blocks of one row: lane 0 copies the group's weight
+//     tiles (contiguous, 8 KB each) in one bulk copy, lane i the batch x 64
+//     rate tile of the group's i-th block column (cp.async.bulk completing on
+//     the stage's mbarrier; no multicast);
+//   warp 5 (one thread) issues the products of a stage (4 per block, K = 16
+//     each) into one of two accumulators in tensor memory (rows alternate
+//     between them), releases the stage with tcgen05.commit and, after a
+//     row's last stage, commits the accumulator to the epilogue;
+//   warps 0-3 read the accumulator with tcgen05.ld (warp w reads TMEM lanes
+//     32w..32w+31), release it and add it into Y, while the products of the
+//     next row run in the other accumulator.
+// Two orientations of the product:
+//   batch a multiple of 128: D (batch x 64) = X_tile (A, M = 128 per product)
+//     x W_tile^T (B, N = 64), accumulator lane = instance, column = post row;
+//   otherwise: D (64 x batch) = W_tile (A, M = 64) x X_tile^T (B, N = batch),
+//     lane (m % 16) + 32 (m / 16) = post row m, column = instance.
+// Every mbarrier wait is bounded and also gives up once another role has
+// reported a timeout; the CTA then waits (bounded) for its outstanding copies
+// and products, frees its tensor memory and returns.
 //
 // Operand layout in memory is the tcgen05 canonical K-major layout without
 // swizzle: 8 x 8 "core matrices" of 16-byte rows, core (i, j) of a tile at
@@ -35,10 +47,11 @@
 namespace {
 
 constexpr int kTile = 64;                 // block rows / columns
-constexpr int kStages = 4;
+constexpr int kMaxStages = 12;
 constexpr unsigned kTileBytes = kTile * kTile * 2;   // 8 KB of bf16
 constexpr int kWaitTries = 1 << 22;
-constexpr int kColCache = 512;
+constexpr int kThreads = 192;             // warps 0-3 epilogue, 4 copies, 5 products
+constexpr int kRowCache = 512;            // block-row ranges held in shared memory
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -53,14 +66,21 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
                ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the phase of parity `parity`; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// Bounded wait for the phase of parity `parity`; false on timeout or when
+// *abort is set (checked every 64 polls).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, const volatile int* abort) {
   const unsigned b = smem_u32(bar);
   unsigned done = 0;
   for (int it = 0; it < kWaitTries && !done; ++it) {
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
         : "=r"(done) : "r"(b), "r"(parity) : "memory");
+    if (!done && (it & 63) == 63 && abort && *abort) return false;
   }
   return done != 0;
 }
@@ -110,120 +130,273 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(128, 1)
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// y[0..15] += r[0..15] for 16 consecutive floats (vector access when aligned);
+// all loads are issued before the tensor-memory read completes.
+__device__ __forceinline__ void add16_contiguous(float* y, uint32_t taddr, bool vec, int valid) {
+  float old[16];
+  uint32_t r[16];
+  if (vec) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 o = reinterpret_cast<const float4*>(y)[q];
+      old[4 * q] = o.x; old[4 * q + 1] = o.y; old[4 * q + 2] = o.z; old[4 * q + 3] = o.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) old[j] = j < valid ? y[j] : 0.f;
+  }
+  tmem_ld16(taddr, r);
+  if (vec) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      reinterpret_cast<float4*>(y)[q] =
+          make_float4(old[4 * q] + __uint_as_float(r[4 * q]), old[4 * q + 1] + __uint_as_float(r[4 * q + 1]),
+                      old[4 * q + 2] + __uint_as_float(r[4 * q + 2]),
+                      old[4 * q + 3] + __uint_as_float(r[4 * q + 3]));
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (j < valid) y[j] = old[j] + __uint_as_float(r[j]);
+  }
+}
+
+// Block range of the CTA's i-th block row br (from shared memory when cached).
+__device__ __forceinline__ int2 tc_row(const int2* rows_s, const int* brow_ptr, int i, int br) {
+  return i < kRowCache ? rows_s[i] : make_int2(brow_ptr[br], brow_ptr[br + 1]);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
 bsr_spmm_tc_kernel(const int* __restrict__ brow_ptr, const int* __restrict__ bcol,
-                const uint16_t* __restrict__ a_tiles, const uint16_t* __restrict__ x_tiles,
-                int batch, float* __restrict__ y, int n_post, int tmem_cols, int* err) {
+                   const uint16_t* __restrict__ a_tiles, const uint16_t* __restrict__ x_tiles,
+                   int n_block_rows, int batch, float* __restrict__ y, int n_post, int stages,
+                   int group, int xmajor, int acc_cols, int tmem_cols, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], acc_full[2], acc_empty[2], done;
   __shared__ uint32_t tmem_base;
-  __shared__ int abort_flag, issued_n, consumed_n;
-  __shared__ int bcol_s[kColCache];        // the row's block columns (first kColCache)
+  __shared__ volatile int abort_flag;
+  __shared__ int issued_n, consumed_n, mma_any;
+  __shared__ int2 rows_s[kRowCache];       // [beg, end) of the CTA's block rows i = 0, 1, ...
   const unsigned x_bytes = (unsigned)batch * kTile * 2;
-  const unsigned stage_bytes = kTileBytes + x_bytes;
-  const int br = blockIdx.x;
-  const int beg = brow_ptr[br], nblk = brow_ptr[br + 1] - beg;
+  // a stage: `group` weight tiles (consecutive blocks of one row), then their
+  // `group` rate tiles
+  const unsigned stage_bytes = (unsigned)group * (kTileBytes + x_bytes);
+  const unsigned x_off = (unsigned)group * kTileBytes;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  if (warp == 0) {
+  if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  ::"r"(smem_u32(&tmem_base)), "r"(tmem_cols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < stages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 4);          // one arrival per epilogue warp
     }
     mbar_init(&done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
     issued_n = 0;
     consumed_n = 0;
+    mma_any = 0;
   }
-  for (int q = threadIdx.x; q < nblk && q < kColCache; q += blockDim.x) bcol_s[q] = bcol[beg + q];
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  for (int i = threadIdx.x; i < kRowCache; i += kThreads) {
+    const int br = blockIdx.x + i * gridDim.x;
+    if (br < n_block_rows) rows_s[i] = make_int2(brow_ptr[br], brow_ptr[br + 1]);
+  }
+  tc_fence_before();
   __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t taddr = tmem_base;
+  tc_fence_after();
+  const uint32_t tbase = tmem_base;
 
-  // warp 0 lane 0 streams the blocks into the stage ring, warp 1 lane 0
-  // issues the products as stages fill: neither waits on the other's latency
-  if (nblk > 0 && threadIdx.x == 0) {
-    int k = 0;
-    for (; k < nblk; ++k) {
-      const int s = k % kStages, u = k / kStages;
-      if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1)) {
-        anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
-        abort_flag = 1;
-        break;
+  if (warp == 4) {
+    // the whole warp: lane i fetches the block column of the stage's i-th
+    // block (while the stage is still being released) and copies its rate
+    // tile; lane 0 copies the stage's weight tiles in one piece
+    int s = 0, k = 0;                         // stage, stages filled
+    unsigned ph = 0;                          // parity of the stage's current use
+    bool ok = true;
+    for (int i = 0, br = blockIdx.x; br < n_block_rows && ok; ++i, br += gridDim.x) {
+      const int2 rr = tc_row(rows_s, brow_ptr, i, br);
+      for (int g0 = rr.x; g0 < rr.y; g0 += group) {
+        const int gn = rr.y - g0 < group ? rr.y - g0 : group;
+        const int bc = lane < gn ? bcol[g0 + lane] : 0;
+        if (k >= stages) {
+          const bool w = __all_sync(0xffffffffu, mbar_wait(&empty[s], ph ^ 1u, &abort_flag));
+          if (!w) {
+            if (lane == 0) {
+              anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+              abort_flag = 1;
+            }
+            ok = false;
+            break;
+          }
+        }
+        unsigned char* st = smem + s * stage_bytes;
+        if (lane == 0) mbar_expect_tx(&full[s], (unsigned)gn * (kTileBytes + x_bytes));
+        __syncwarp();
+        if (lane == 0) bulk_load(st, a_tiles + (size_t)g0 * (kTile * kTile), (unsigned)gn * kTileBytes, &full[s]);
+        if (lane < gn) bulk_load(st + x_off + lane * x_bytes, x_tiles + (size_t)bc * batch * kTile, x_bytes, &full[s]);
+        ++k;
+        if (++s == stages) {
+          s = 0;
+          ph ^= 1u;
+        }
       }
-      unsigned char* st = smem + s * stage_bytes;
-      mbar_expect_tx(&full[s], stage_bytes);
-      bulk_load(st, a_tiles + (size_t)(beg + k) * (kTile * kTile), kTileBytes, &full[s]);
-      const int bc = k < kColCache ? bcol_s[k] : bcol[beg + k];
-      bulk_load(st + kTileBytes, x_tiles + (size_t)bc * batch * kTile, x_bytes, &full[s]);
     }
-    issued_n = k;
-  } else if (nblk > 0 && threadIdx.x == 32) {
-    const uint32_t idesc = instr_desc(kTile, batch);
-    int k = 0;
-    for (; k < nblk; ++k) {
-      const int s = k % kStages, u = k / kStages;
-      if (!mbar_wait(&full[s], u & 1)) {
-        anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
-        abort_flag = 1;
-        break;
+    if (lane == 0) {
+      issued_n = k;
+      // every stage released by its products before the CTA leaves: the last
+      // use of each stage, in fill order
+      for (int q = 0; ok && q < (k < stages ? k : stages); ++q) {
+        const int kq = k - 1 - q;               // a stage filled kq-th, use kq / stages
+        if (!mbar_wait(&empty[kq % stages], (unsigned)(kq / stages) & 1u, &abort_flag)) {
+          anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+          abort_flag = 1;
+          ok = false;
+        }
       }
-      const unsigned a0 = smem_u32(smem + s * stage_bytes);
-      const unsigned b0 = a0 + kTileBytes;
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      const uint32_t idesc = xmajor ? instr_desc(128, kTile) : instr_desc(kTile, batch);
+      const int halves = xmajor ? batch / 128 : 1;
+      // descriptors of the start of shared memory; offsets added in 16-byte units
+      const uint64_t d0 = smem_desc(smem_u32(smem), 128, 1024);
+      int s = 0, k = 0, t = 0;                // stage, stages consumed, non-empty rows done
+      unsigned ph = 0;
+      bool ok = true;
+      for (int i = 0, br = blockIdx.x; br < n_block_rows && ok; ++i, br += gridDim.x) {
+        const int2 rr = tc_row(rows_s, brow_ptr, i, br);
+        if (rr.y == rr.x) continue;
+        const int a = t & 1, v = t >> 1;
+        if (v > 0 && !mbar_wait(&acc_empty[a], (v - 1) & 1, &abort_flag)) {
+          anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+          abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tbase + (uint32_t)(a * acc_cols);
+        for (int g0 = rr.x; g0 < rr.y; g0 += group) {
+          const int gn = rr.y - g0 < group ? rr.y - g0 : group;
+          if (!mbar_wait(&full[s], ph, &abort_flag)) {
+            anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+            abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t ws = d0 + ((s * stage_bytes) >> 4);
+          const uint64_t xs = ws + (x_off >> 4);
+          for (int b = 0; b < gn; ++b) {
+            const uint64_t wb = ws + ((b * kTileBytes) >> 4), xb = xs + ((b * x_bytes) >> 4);
+            const uint32_t acc0 = (g0 > rr.x || b > 0) ? 1u : 0u;
+            if (xmajor) {
+              for (int h = 0; h < halves; ++h) {
 #pragma unroll
-      for (int q = 0; q < kTile / 16; ++q) {
-        umma_f16(taddr, smem_desc(a0 + q * 256, 128, 1024), smem_desc(b0 + q * 256, 128, 1024),
-                 idesc, (k > 0 || q > 0) ? 1u : 0u);
+                for (int q = 0; q < kTile / 16; ++q)
+                  umma_f16(d + (uint32_t)(h * kTile), xb + h * (16384 >> 4) + q * (256 >> 4), wb + q * (256 >> 4),
+                           idesc, (acc0 | q) ? 1u : 0u);
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < kTile / 16; ++q)
+                umma_f16(d, wb + q * (256 >> 4), xb + q * (256 >> 4), idesc, (acc0 | q) ? 1u : 0u);
+            }
+          }
+          mma_any = 1;
+          umma_commit(&empty[s]);
+          ++k;
+          if (++s == stages) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+        if (!ok) break;
+        umma_commit(&acc_full[a]);
+        ++t;
       }
-      umma_commit(&empty[s]);
+      consumed_n = k;
+      if (mma_any) umma_commit(&done);        // after every issued product
     }
-    consumed_n = k;
-    umma_commit(&done);                       // after every issued product
+  } else {
+    // epilogue warps 0-3
+    const bool vec = (n_post & 3) == 0 && (reinterpret_cast<uintptr_t>(y) & 15) == 0;
+    int t = 0;
+    for (int i = 0, br = blockIdx.x; br < n_block_rows; ++i, br += gridDim.x) {
+      const int2 rr = tc_row(rows_s, brow_ptr, i, br);
+      if (rr.y == rr.x) continue;
+      const int a = t & 1, v = t >> 1;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[a], v & 1, &abort_flag));
+      if (!ok) {
+        if (lane == 0) {
+          anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+          abort_flag = 1;
+        }
+        break;
+      }
+      tc_fence_after();
+      const uint32_t tw = tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(a * acc_cols);
+      if (xmajor) {
+        // lane = instance 32 w + lane (+128 per half); 64 consecutive post rows
+        const int r0 = br * kTile;
+        const int valid_rows = n_post - r0 < kTile ? n_post - r0 : kTile;
+        for (int h = 0; h < batch / 128; ++h) {
+          float* yb = y + (size_t)(h * 128 + 32 * warp + lane) * n_post + r0;
+#pragma unroll 1
+          for (int c0 = 0; c0 < kTile; c0 += 16) {
+            const int valid = valid_rows - c0 < 16 ? (valid_rows - c0 > 0 ? valid_rows - c0 : 0) : 16;
+            add16_contiguous(yb + c0, tw + (uint32_t)(h * kTile + c0), vec && valid == 16, valid);
+          }
+        }
+      } else {
+        // lanes 0-15 of warp w hold post rows 16 w .. 16 w + 15; columns = instances
+        const int row = br * kTile + 16 * warp + lane;
+        const bool mine = lane < 16 && row < n_post;
+        for (int c0 = 0; c0 < batch; c0 += 16) {
+          float old[16];
+          uint32_t r[16];
+          if (mine) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) old[j] = y[(size_t)(c0 + j) * n_post + row];
+          }
+          tmem_ld16(tw + (uint32_t)c0, r);
+          if (mine) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) y[(size_t)(c0 + j) * n_post + row] = old[j] + __uint_as_float(r[j]);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
+      ++t;
+    }
   }
   __syncthreads();
   if (abort_flag && threadIdx.x == 0) {
     // copies issued but never consumed: wait for them (bounded) before leaving
-    for (int k = consumed_n; k < issued_n; ++k) mbar_wait(&full[k % kStages], (k / kStages) & 1);
+    for (int k = consumed_n; k < issued_n; ++k) mbar_wait(&full[k % stages], (unsigned)(k / stages) & 1u, nullptr);
   }
+  if (mma_any && threadIdx.x == 0 && !mbar_wait(&done, 0, nullptr))
+    anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
+  tc_fence_before();
   __syncthreads();
-  if (nblk > 0) {
-    const bool ok = mbar_wait(&done, 0);
-    if (!ok) anb_report(err, ANB_DEVERR_BARRIER_TIMEOUT);
-    // uniform over the CTA: tcgen05.ld is executed by whole warps
-    const int all_ok = __syncthreads_and(ok && !abort_flag ? 1 : 0);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (all_ok) {
-      // warp w reads TMEM lanes 32w..32w+31; lanes 0-15 hold rows 16w..16w+15
-      const int row = br * kTile + 16 * warp + lane;
-      const bool mine = lane < 16 && row < n_post;
-      for (int c0 = 0; c0 < batch; c0 += 16) {
-        // the 16 loads of Y go out together (written before any store, so
-        // they need not wait for one another) and overlap the tensor-memory read
-        float old[16];
-        uint32_t r[16];
-        if (mine) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) old[j] = y[(size_t)(c0 + j) * n_post + row];
-        }
-        tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, r);
-        if (mine) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) y[(size_t)(c0 + j) * n_post + row] = old[j] + __uint_as_float(r[j]);
-        }
-      }
-    }
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(tmem_cols)
+  tc_fence_after();
+  if (warp == 5) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(tmem_cols)
                  : "memory");
   }
 }
@@ -318,6 +491,11 @@ __global__ void bsr_pack_x_kernel(const float* __restrict__ x, int batch, int n_
   }
 }
 
+// launch-shape overrides of anb_bsr_spmm_tc (0 = automatic)
+int g_tc_per_sm = 0;
+int g_tc_stages = 0;
+int g_tc_group = 0;
+
 }  // namespace
 
 extern "C" {
@@ -329,20 +507,70 @@ int anb_bsr_tc_pack_x(const float* x, int batch, int n_pre, uint16_t* x_tiles, v
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
+int anb_bsr_spmm_tc_shape(int ctas_per_sm, int stages, int group) {
+  if (ctas_per_sm < 0 || ctas_per_sm > 4 || stages < 0 || stages == 1 || stages > kMaxStages ||
+      group < 0 || group > 8)
+    return 2;
+  g_tc_per_sm = ctas_per_sm;
+  g_tc_stages = stages;
+  g_tc_group = group;
+  return 0;
+}
+
 int anb_bsr_spmm_tc(const int* brow_ptr, const int* bcol, const uint16_t* a_tiles,
                     int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
                     int* err, void* stream) {
   if (!brow_ptr || !bcol || !a_tiles || !x_tiles || !y || n_block_rows < 0) return 2;
   if (batch < 16 || batch > 256 || batch % 16 != 0) return 2;
   if (n_block_rows == 0) return 0;
-  int cols = 32;
-  while (cols < batch) cols <<= 1;
-  const size_t smem = (size_t)kStages * (kTileBytes + (size_t)batch * kTile * 2);
+  static int sm_count = 0;
+  if (sm_count == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return 4;
+  }
+  // accumulators: two per CTA, a power of two of columns each
+  const int xmajor = batch % 128 == 0 ? 1 : 0;
+  const int need = xmajor ? kTile * (batch / 128) : batch;
+  int acc_cols = 32;
+  while (acc_cols < need) acc_cols <<= 1;
+  const int tmem_cols = 2 * acc_cols;
+  // shape: `group` blocks per stage, `stages` stages, `per_sm` CTAs per SM.
+  // Each CTA's copy and product threads spend a few hundred cycles of their
+  // own per stage, so several CTAs per SM and two blocks per stage keep HBM
+  // busy better than deep rings: two stages, as many CTAs (up to three) as
+  // shared and tensor memory allow, else one CTA with up to four stages of
+  // two blocks. anb_bsr_spmm_tc_shape overrides the choice.
+  const size_t block_bytes = kTileBytes + (size_t)batch * kTile * 2;
+  const int tm_limit = 512 / tmem_cols;
+  int per_sm = 1, group = 2, stages = 2;
+  if (tm_limit >= 2) {
+    group = 4 * block_bytes <= (104u << 10) ? 2 : 1;
+    per_sm = (int)((222u << 10) / ((size_t)stages * group * block_bytes + (6u << 10)));
+    if (per_sm > 3) per_sm = 3;
+    if (per_sm > tm_limit) per_sm = tm_limit;
+  }
+  if (per_sm < 2) {
+    per_sm = 1;
+    group = 2;
+    stages = (int)((200u << 10) / (group * block_bytes));
+    if (stages > 4) stages = 4;
+  }
+  if (g_tc_per_sm > 0) per_sm = g_tc_per_sm;
+  if (g_tc_stages > 0) stages = g_tc_stages;
+  if (g_tc_group > 0) group = g_tc_group;
+  const size_t smem = (size_t)stages * group * block_bytes;
+  if (stages < 2 || stages > kMaxStages || group < 1 || group > 8 || smem > (200u << 10) ||
+      per_sm * tmem_cols > 512)
+    return 2;
   if (cudaFuncSetAttribute(bsr_spmm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return 4;
-  bsr_spmm_tc_kernel<<<n_block_rows, 128, smem, (cudaStream_t)stream>>>(
-      brow_ptr, bcol, a_tiles, x_tiles, batch, y, n_post, cols, err);
+  const int grid = n_block_rows < per_sm * sm_count ? n_block_rows : per_sm * sm_count;
+  bsr_spmm_tc_kernel<<<grid, kThreads, smem, (cudaStream_t)stream>>>(
+      brow_ptr, bcol, a_tiles, x_tiles, n_block_rows, batch, y, n_post, stages, group, xmajor,
+      acc_cols, tmem_cols, err);
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 

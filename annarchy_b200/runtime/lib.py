@@ -47,6 +47,7 @@ SIGNATURES = {
                                     C.POINTER(C.c_size_t)]),
     "anb_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "anb_bsr_tc_pack_x": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "anb_bsr_spmm_tc_shape": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "anb_bsr_spmm_tc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                   C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "anb_bsr_spmm_simt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,

@@ -48,6 +48,14 @@ def pack_x_reference(x: np.ndarray) -> np.ndarray:
     return to_bf16(canonical_tiles(tiles))
 
 
+def tc_shape(ctas_per_sm: int = 0, stages: int = 0, group: int = 0):
+    """Launch shape of the tensor-core product for this process (0 = the
+    automatic choice); see anb_bsr_spmm_tc_shape."""
+    rc = L.load().anb_bsr_spmm_tc_shape(int(ctas_per_sm), int(stages), int(group))
+    if rc != 0:
+        raise ValueError(f"launch shape ({ctas_per_sm}, {stages}, {group}) out of range")
+
+
 class BlockSparseBatch:
     """Weights w (scipy sparse, n_post x n_pre) as 64 x 64 bfloat16 blocks on
     device `device`; calls compute y[b] = w @ x[b] for `batch` rate vectors
@@ -90,11 +98,15 @@ class BlockSparseBatch:
         self.nat.write("x", x)
         self.nat.zero("y")
 
-    def run(self, engine: str = "tc"):
-        """Pack the loaded rates and add W x into y on the device (no sync)."""
+    def pack(self):
+        """Convert the loaded rates to bfloat16 tiles on the device (no sync)."""
         lib, p = L.load(), self._p
         self._check("anb_bsr_tc_pack_x", lib.anb_bsr_tc_pack_x(
             C.c_void_p(p["x"]), self.batch, self.n_pre, C.c_void_p(p["xt"]), self._stream))
+
+    def product(self, engine: str = "tc"):
+        """Add W x of the packed rates into y on the device (no sync)."""
+        lib, p = L.load(), self._p
         if engine == "tc":
             self._check("anb_bsr_spmm_tc", lib.anb_bsr_spmm_tc(
                 C.c_void_p(p["brow"]), C.c_void_p(p["bcol"]), C.c_void_p(p["tiles"]),
@@ -107,6 +119,13 @@ class BlockSparseBatch:
                 self.n_post, self._stream))
         else:
             raise ValueError(engine)
+
+    def run(self, engine: str = "tc"):
+        """Pack the loaded rates and add W x into y on the device (no sync)."""
+        if engine not in ("tc", "simt"):
+            raise ValueError(engine)
+        self.pack()
+        self.product(engine)
 
     def result(self) -> np.ndarray:
         self.nat.synchronize()

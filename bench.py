@@ -561,13 +561,20 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
     return out
 
 
+def wl_blocks_stored(m):
+    """Stored entries of m in 64 x 64 blocks (every block with a nonzero)."""
+    import scipy.sparse as sp
+    c = sp.csr_matrix(m).tocoo()
+    return 4096 * np.unique((c.row // 64).astype(np.int64) * (1 << 32) + c.col // 64).size
+
+
 def spmm_study(batches=(64, 128, 256), reps=5):
     """Batched weighted sums over the 100k-neuron block matrix (64x64 blocks,
     2 % block density, bfloat16): tcgen05 tensor cores vs CUDA cores. Device
-    time per product with the weights cold (clean L2 flush before each
-    repetition; the packed rates, 100k x batch bfloat16, are read from L2),
-    TFLOP/s (2 x stored block entries x batch) and HBM fraction of the
-    weight bytes."""
+    time of the product (and, apart, of packing the rates into bfloat16
+    tiles) with the weights cold (clean L2 flush before each repetition; the
+    packed rates, 100k x batch bfloat16, are read from L2), TFLOP/s
+    (2 x stored block entries x batch) and HBM fraction of the weight bytes."""
     import torch
     from annarchy_b200 import spmm, workloads as wl
     peak, kind = peaks()
@@ -580,6 +587,8 @@ def spmm_study(batches=(64, 128, 256), reps=5):
     flush = torch.ones((384 << 20) // 4, device="cuda")
     out = {"matrix": "100k blocks 64x64, 2 %", "nnz": int(m.nnz), "hbm_peak_gbs": peak,
            "bf16_tflops_peak": tpk, "results": {}}
+    # plain cold read of the weight bytes (the floor of any kernel reading them)
+    out["stream_floor_us"] = stream_read_us(2 * wl_blocks_stored(m))
     for batch in batches:
         bsb = spmm.BlockSparseBatch(m, batch)
         x = np.random.default_rng(batch).uniform(0, 1, (batch, m.shape[1])).astype(np.float32)
@@ -594,24 +603,31 @@ def spmm_study(batches=(64, 128, 256), reps=5):
         res = {"rel_err_sample": rel}
         stream = torch.cuda.ExternalStream(bsb.nat.stream())   # where the products run
         for eng in ("tc", "simt") if batch in (64, 128, 256) else ("tc",):
-            ts = []
+            ts, tp = [], []
             for _ in range(reps):
                 bsb.load(x)
-                bsb.run(eng)                      # warm + pack
+                bsb.run(eng)                      # warm
                 flush.sum()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
                 torch.cuda.synchronize()
-                e0.record(stream)
-                bsb.run(eng)
-                e1.record(stream)
+                with torch.cuda.stream(stream):
+                    torch.cuda._sleep(1 << 20)    # device busy while the host enqueues
+                ev[0].record(stream)
+                bsb.pack()
+                ev[1].record(stream)
+                bsb.product(eng)
+                ev[2].record(stream)
                 torch.cuda.synchronize()
-                ts.append(e0.elapsed_time(e1))
+                tp.append(ev[0].elapsed_time(ev[1]))
+                ts.append(ev[1].elapsed_time(ev[2]))
             bsb.result()
             ms = sorted(ts)[len(ts) // 2]
             stored = bsb.n_blocks * 64 * 64
             flops = 2.0 * stored * batch
             wbytes = stored * 2
-            res[eng] = {"us": ms * 1e3, "tflops": flops / (ms * 1e-3) / 1e12,
+            res[eng] = {"us": ms * 1e3, "pack_us": sorted(tp)[len(tp) // 2] * 1e3,
+                        "of_floor": out["stream_floor_us"] / (ms * 1e3),
+                        "tflops": flops / (ms * 1e-3) / 1e12,
                         "tensor_frac": flops / (ms * 1e-3) / 1e12 / tpk,
                         "weight_gbs": wbytes / (ms * 1e-3) / 1e9,
                         "hbm_frac": wbytes / (ms * 1e-3) / 1e9 / peak}

@@ -213,6 +213,16 @@ int anb_bsr_tc_pack_x(const float* x, int batch, int n_pre, uint16_t* x_tiles, v
 int anb_bsr_spmm_tc(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
                     int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
                     int* err, void* stream);
+/* Launch shape of anb_bsr_spmm_tc for this process: resident CTAs per SM
+ * (1-4), shared-memory stages per CTA (2-12) and consecutive blocks of a row
+ * per stage (1-8); 0 keeps the automatic choice (two stages; two blocks per
+ * stage up to batch 128, one above; up to three CTAs per SM as shared and
+ * tensor memory allow; one CTA with up to four stages of two blocks when two
+ * do not fit). A later anb_bsr_spmm_tc returns 2 when the shape does not fit
+ * its batch (stages above 200 KB in all, or more than 512 tensor-memory
+ * columns per SM). Returns 0 or 2. For tuning; no counterpart in the
+ * reference. */
+int anb_bsr_spmm_tc_shape(int ctas_per_sm, int stages, int group);
 int anb_bsr_spmm_simt(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
                       int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
                       void* stream);

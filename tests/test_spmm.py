@@ -36,7 +36,7 @@ def test_pack_x_reference_layout():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("batch", [16, 64, 128, 256])
+@pytest.mark.parametrize("batch", [16, 64, 128, 144, 256])
 def test_tc_matches_reference(batch):
     w = _blocks(300, 200, 0.35, batch)                  # partial last block row and column
     bsb = spmm.BlockSparseBatch(w, batch)
@@ -47,6 +47,38 @@ def test_tc_matches_reference(batch):
         y = bsb(x, "tc")
         err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
         assert err <= 1e-5, err
+    bsb.close()
+
+
+def _blocks_sparse(n_post, n_pre, density, seed):
+    """Dense 64 x 64 blocks at `density` without forming the dense matrix."""
+    rng = np.random.default_rng(seed)
+    nbr, nbc = -(-n_post // 64), -(-n_pre // 64)
+    br, bc = np.nonzero(rng.random((nbr, nbc)) < density)
+    r = (br[:, None, None] * 64 + np.arange(64)[None, :, None]).repeat(64, axis=2).ravel()
+    c = (bc[:, None, None] * 64 + np.arange(64)[None, None, :]).repeat(64, axis=1).ravel()
+    keep = (r < n_post) & (c < n_pre)
+    v = rng.normal(0, 0.05, r.size)
+    return sp.csr_matrix((v[keep], (r[keep], c[keep])), shape=(n_post, n_pre))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("batch", [48, 64, 128, 192, 256])
+def test_tc_many_block_rows(batch):
+    """More block rows than resident CTAs (each CTA takes several rows and
+    alternates its two accumulators), empty block rows, an odd n_post."""
+    from annarchy_b200.core.backend import from_bf16, to_bf16
+    w = _blocks_sparse(60001, 2000, 0.04, batch)
+    bsb = spmm.BlockSparseBatch(w, batch)
+    assert bsb.n_block_rows > 2 * 148
+    x = np.random.default_rng(batch).uniform(0, 1, (batch, 2000)).astype(np.float32)
+    wq = sp.csr_matrix((from_bf16(to_bf16(w.data.astype(np.float32))), w.indices, w.indptr), shape=w.shape)
+    ref = np.asarray(wq @ from_bf16(to_bf16(x)).T.astype(np.float64)).T
+    for _ in range(2):
+        y = bsb(x, "tc")
+        err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+        assert err <= 1e-5, err
+    assert np.all(y[:, np.diff(w.indptr) == 0] == 0)
     bsb.close()
 
 
