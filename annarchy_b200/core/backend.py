@@ -58,6 +58,7 @@ class CompiledNetwork:
         self._col_ptr: dict[int, np.ndarray] = {}
         self.engine = None
         self.module = None
+        self.slots: dict[int, int] = {}    # history ring length (steps) per population
 
     # --------------------------------------------------------------- helpers
     def _w(self, w: np.ndarray) -> np.ndarray:
@@ -71,6 +72,10 @@ class CompiledNetwork:
         net = self.net
         nat = self.native
         nat.initialize(net.dt)
+        # history kept per population: its outgoing projections' largest delay
+        for pop in net.populations:
+            self.slots[pop.id] = max([1] + [int(p.max_delay) for p in net.projections
+                                           if p.pre_pop is pop])
         self.engine = self._choose_engine()
         # fast grid engine: per-step spike lists drive the event kernels
         self.spike_lists = (not self.exact and self.engine == "grid")
@@ -80,6 +85,8 @@ class CompiledNetwork:
             self._create_projection(proj)
         for mon in net.monitors:
             self._create_monitor(mon)
+        for pop in net.populations:
+            pop._init_state = {k: v.copy() for k, v in pop._host.items()}
         if self.engine == "local":
             self._build_cluster()
             return
@@ -145,6 +152,8 @@ class CompiledNetwork:
 
     def _local_possible(self):
         net = self.net
+        if any(p.max_delay > 1 for p in net.projections):
+            return False, "synaptic delays"
         if any(p.neuron_type.type != "spike" for p in net.populations):
             return False, "rate-coded populations"
         if any(p.synapse_type.type != "spike" or p.plastic for p in net.projections):
@@ -308,9 +317,15 @@ class CompiledNetwork:
             nat.create(f"pop{pop.id}__{name}", np.asarray(arr, dtype=dt).reshape(-1))
         for name in compensated_vars(pop, self.exact, self.net._config):
             nat.create(f"pop{pop.id}__kc_{name}", np.zeros(pop.size, dtype=self.real))
+        R = self.slots.get(pop.id, 1)
+        if pop.neuron_type.type == "rate" and R > 1:
+            # rates of the last R steps (slot t % R holds step t), filled with
+            # the current rates like the reference's queue at compile and reset
+            nat.create(f"pop{pop.id}___delayed_r", self._ring_of(pop, pop._host["r"]))
         if pop.neuron_type.type == "spike":
             n = pop.size
-            nat.create(f"pop{pop.id}__spk", np.zeros((n + 31) // 32, dtype=np.uint32))
+            # spike bitmaps of the last R steps (slot t % R holds step t)
+            nat.create(f"pop{pop.id}__spk", np.zeros(R * ((n + 31) // 32), dtype=np.uint32))
             if self.spike_lists:
                 nat.create_empty(f"pop{pop.id}__spl", np.int32, (2 * n,))
                 nat.create(f"pop{pop.id}__spn", np.zeros(2, dtype=np.int32))
@@ -368,11 +383,48 @@ class CompiledNetwork:
             nat.fill(f"proj{k}___last_event", np.int64(-10000))
         self.layout[k] = lay
 
+    def _create_delays(self, proj):
+        k = proj.id
+        if proj._delay_steps is not None:
+            if proj.synapse_type.type == "rate" and proj._storage_format not in ("csr", "auto"):
+                raise NotImplementedError("non-uniform delays of rate-coded projections use the csr "
+                                          "format (the reference supports them in LIL only)")
+            self.native.create(f"proj{k}__dly", np.asarray(proj._delay_steps, dtype=np.int32))
+        elif proj.max_delay > 1:
+            self.native.create(f"proj{k}__delay", np.array([proj.uniform_delay], dtype=np.int32))
+
+    @staticmethod
+    def ring_stride(pop) -> int:
+        """Elements per slot of a rate history ring (a multiple of 4, so every
+        slot starts 16-byte aligned)."""
+        return -(-pop.size // 4) * 4
+
+    def _ring_of(self, pop, r) -> np.ndarray:
+        R, S = self.slots[pop.id], self.ring_stride(pop)
+        ring = np.zeros((R, S), dtype=self.real)
+        ring[:, :pop.size] = np.asarray(r, dtype=self.real).reshape(-1)
+        return ring.reshape(-1)
+
+    def delay_capacity(self, proj) -> int:
+        """Largest delay (steps) the pre-synaptic history kept since compile()
+        can serve."""
+        if proj.max_delay <= 1:
+            return 1
+        return self.slots[proj.pre_pop.id]
+
+    def read_delays(self, proj) -> np.ndarray:
+        return self.native.read(f"proj{proj.id}__dly").astype(np.int32)
+
+    def write_delays(self, proj, steps: np.ndarray):
+        name = f"proj{proj.id}__dly" if proj._delay_steps is not None else f"proj{proj.id}__delay"
+        self.native.write(name, np.asarray(steps, dtype=np.int32))
+
     def _create_projection(self, proj):
         nat = self.native
         k = proj.id
         if getattr(proj, "_device_conn", None):
             return self._create_device_projection(proj)
+        self._create_delays(proj)
         if proj._csr is None:
             raise RuntimeError(f"projection {proj.name} has no connectivity (call a connector)")
         post_rank, row_ptr, cols, w = proj.csr_population_ranks()
@@ -388,7 +440,7 @@ class CompiledNetwork:
             if prm["locality"] == "global":
                 nat.create(f"proj{k}__{prm['name']}", np.array([prm["init"]], dtype=self.real))
         if proj.synapse_type.type == "rate":
-            fmt = self._rate_format(proj, lay)
+            fmt = "csr" if proj._delay_steps is not None else self._rate_format(proj, lay)
             lay["format"] = fmt
             if fmt != "csr":
                 F.create_format_arrays(self, proj, fmt, post_rank, row_ptr, cols, w, lay)
@@ -427,8 +479,13 @@ class CompiledNetwork:
                 row_of = np.full(proj.post_pop.size, -1, dtype=np.int32)
                 row_of[post_rank] = np.arange(rows, dtype=np.int32)
                 nat.create(f"proj{k}__row_of", row_of)
-            if self.exact or proj.plastic:
-                lay["grid"] = grid_for(rows * (32 if self.exact else 1))
+            # warp per post row: exact order, per-synapse delays, and plastic
+            # delayed projections (the spike lists hold only the last step)
+            gather = self.exact or proj._delay_steps is not None or (proj.plastic and proj.max_delay > 1)
+            if gather:
+                lay["grid"] = grid_for(rows * 32)
+            elif proj.plastic:
+                lay["grid"] = grid_for(rows)
             else:
                 lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
             if proj.plastic:
@@ -552,7 +609,54 @@ class CompiledNetwork:
 
     def read_spiked(self, pop):
         bits = self.native.read(f"pop{pop.id}__spk")
+        R = self.slots.get(pop.id, 1)
+        if R > 1:                               # the slot of the last step
+            words = (pop.size + 31) // 32
+            slot = (self.native.get_time() - 1) % R
+            bits = np.ascontiguousarray(bits[slot * words:(slot + 1) * words])
         return np.nonzero(np.unpackbits(bits.view(np.uint8), bitorder="little")[: pop.size])[0]
+
+    # ----------------------------------------------------------------- reset
+    def reset_population(self, pop, attributes=None):
+        """Initial values back into the device arrays (all attributes, or
+        the given ones) and the reference's PopStruct::reset(): no spikes
+        emitted, refractory counters cleared, the delay queues refilled with
+        the current rates (ANNarchy/generator/Population/
+        SingleThreadTemplates.py:182-212)."""
+        nat = self.native
+        k = pop.id
+        names = list(pop._init_state) if attributes is None else list(attributes)
+        for name in names:
+            if name.startswith("_sum_"):
+                continue
+            self.write_population_attribute(pop, name, pop._init_state[name])
+        for name in compensated_vars(pop, self.exact, self.net._config):
+            nat.fill(f"pop{k}__kc_{name}", self.real(0))
+        for t in pop.targets if pop.neuron_type.type == "rate" else []:
+            nat.fill(f"pop{k}___sum_{t}", self.real(0))
+        R = self.slots.get(k, 1)
+        if pop.neuron_type.type == "rate" and R > 1:
+            nat.write(f"pop{k}___delayed_r", self._ring_of(pop, self.read_population_attribute(pop, "r")))
+        if pop.neuron_type.type == "spike":
+            nat.fill(f"pop{k}__spk", np.uint32(0))
+            nat.fill(f"pop{k}__refractory_remaining", np.int32(0))
+            nat.fill(f"pop{k}__last_spike", np.int64(-10000))
+            if f"pop{k}__spn" in nat.arrays:
+                nat.fill(f"pop{k}__spn", np.int32(0))
+
+    def reset_projection(self, proj):
+        """Synaptic variables (not the weights) back to their initial values."""
+        nat = self.native
+        k = proj.id
+        for v in proj.desc["variables"]:
+            if v["name"] == "w":
+                continue
+            name = f"proj{k}__{v['name']}"
+            if name in nat.arrays and not isinstance(v["init"], str):
+                dtype, _ = nat.arrays[name]
+                nat.fill(name, np.dtype(dtype).type(v["init"]))
+        if f"proj{k}___last_event" in nat.arrays:
+            nat.fill(f"proj{k}___last_event", np.int64(-10000))
 
     def read_projection_attribute(self, proj, name):
         arr = self.native.read(f"proj{proj.id}__{name}")

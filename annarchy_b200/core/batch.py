@@ -160,6 +160,8 @@ class Batch:
         for pr in self.net.projections:
             if pr.synapse_type.type != "spike" or pr.plastic:
                 raise NotImplementedError("batched instances support static spiking projections")
+            if pr.max_delay > 1:
+                raise NotImplementedError("batched instances transmit without synaptic delays")
             if any((v["name"], v.get("eq", "").replace(" ", "")) != ("g_target", "g_target+=w")
                    for v in pr.desc.get("pre_spike", [])) or pr.desc.get("post_spike"):
                 raise NotImplementedError("batched projections add w to the target conductance only")

@@ -72,6 +72,13 @@ class Monitor:
     def stop(self):
         self._recording = False
 
+    def reset(self):
+        """Empty the recordings (ANNarchy/core/Monitor.py reset)."""
+        self._data = {v: [] for v in self.variables if v != "spike"}
+        self._spike_steps, self._spike_ranks = [], []
+        self._record_steps = []
+        self._start_step = 0
+
     # -- results -------------------------------------------------------------------
     def _append_spikes(self, steps: np.ndarray, ranks: np.ndarray):
         if steps.size:

@@ -34,6 +34,7 @@ class Network:
         self.dt = float(dt)
         self.seed = seed
         self._rng = np.random.default_rng(seed)
+        self._rng_state = self._rng.bit_generator.state
         self.populations: list[Population] = []
         self.projections: list[Projection] = []
         self.monitors: list[Monitor] = []
@@ -58,6 +59,7 @@ class Network:
                 if key == "seed" and val is not None:
                     self.seed = val
                     self._rng = np.random.default_rng(val)
+                    self._rng_state = self._rng.bit_generator.state
                 if key == "sparse_matrix_format":
                     self._config["default_format"] = val
                 continue
@@ -165,6 +167,31 @@ class Network:
 
     def set_time(self, t: float):
         self.set_current_step(int(round(t / self.dt)))
+
+    def reset(self, populations: bool = True, projections: bool = False, synapses: bool = False,
+              monitors: bool = True, reseed_rng: bool = True):
+        """Back to the state after compile() (ANNarchy/core/Network.py:628-675):
+        time 0; with `populations`, every neural attribute at its initial
+        value, no spikes in flight, the delay queues refilled with the
+        initial rates; with `projections`, the synaptic variables (not the
+        weights) at their initial values; with `monitors`, the recordings
+        emptied; with `reseed_rng`, the network's generator back to its seed."""
+        if synapses:
+            raise NotImplementedError("reset(synapses=True): recreating the connectivity is not "
+                                      "supported by this backend")
+        if self._compiled:
+            self.set_current_step(0)
+            if populations:
+                for pop in self.populations:
+                    pop.reset()
+            if projections:
+                for proj in self.projections:
+                    self._backend.reset_projection(proj)
+        if monitors:
+            for mon in self.monitors:
+                mon.reset()
+        if reseed_rng:
+            self._rng.bit_generator.state = self._rng_state
 
     # ---------------------------------------------------------------- access
     def get_population(self, name: str) -> Population:

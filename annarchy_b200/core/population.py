@@ -140,6 +140,21 @@ class Population:
         cur[ranks] = draw(value, (len(ranks),), self._rng(), cur.dtype)
         self.set({name: cur})
 
+    def reset(self, attributes=None):
+        """Attributes (all, or the listed ones) back to the values they had at
+        compile() (ANNarchy/core/Population.py:309-353), spikes and delay
+        queues cleared as by the reference's PopStruct::reset()."""
+        if attributes is not None:
+            for a in attributes:
+                if a not in self._host:
+                    raise AttributeError(f"population {self.name!r} has no attribute {a!r}")
+        if self._compiled():
+            self.net._backend.reset_population(self, attributes)
+        else:
+            for p in self.desc["parameters"] + self.desc["variables"]:
+                if attributes is None or p["name"] in attributes:
+                    self._host[p["name"]] = self._initial(p)
+
     def set_refractory(self, value):
         self._refractory_ms = draw(value, (self.size,), self._rng())
         self._has_refractory = self._has_refractory or bool(np.any(self._refractory_ms > 0))

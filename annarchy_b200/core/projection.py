@@ -10,9 +10,14 @@ HYB) is derived from it at compile time.
 
 Connector methods (ANNarchy/core/ConnectorMethods.py): from_sparse,
 from_matrix, fixed_probability, fixed_number_pre, fixed_number_post,
-all_to_all, one_to_one. Only zero (one-step) transmission delays are
-supported; weights may be scalars, arrays or random distributions drawn from
-the network's seeded generator.
+all_to_all, one_to_one. Weights may be scalars, arrays or random
+distributions drawn from the network's seeded generator. Synaptic delays
+follow the reference (ANNarchy/core/Projection.py:651-690, 1283-1416): a
+delay in ms becomes round(delay / dt) steps; one step (or less) is the
+ordinary transmission of the previous step's output; a scalar gives a
+uniform delay, a random distribution or a per-synapse array a non-uniform
+one. A rate-coded projection with delay d reads the pre-synaptic rates of
+step t - d; a spiking one delivers the spikes of step t - d.
 """
 from __future__ import annotations
 
@@ -66,6 +71,9 @@ class Projection:
         self._host_attr: dict[str, np.ndarray] = {}
         self.connector_name = None
         self._schedule = None
+        self.uniform_delay = 1          # steps; -1 when the delays are per synapse
+        self.max_delay = 1              # steps
+        self._delay_steps = None        # per synapse (CSR order) for non-uniform delays
 
     # -- properties -------------------------------------------------------------
     @property
@@ -93,14 +101,50 @@ class Projection:
         return self.net._rng if self.net is not None else np.random.default_rng()
 
     # -- connectors ---------------------------------------------------------------
-    def _store(self, m: sp.csr_matrix, name, storage_format, delays=0.0):
-        if delays not in (0, 0.0, None):
-            if self.net is None or abs(float(delays) - self.net.dt) > 1e-12:
-                raise NotImplementedError("synaptic delays are not supported by this backend")
+    def _dt(self) -> float:
+        return self.net.dt if self.net is not None else 1.0
+
+    def _steps(self, ms) -> np.ndarray:
+        # Python's round(), as the reference uses; at least one step
+        return np.maximum(1, np.array([round(float(v) / self._dt()) for v in np.ravel(ms)],
+                                      dtype=np.int64)).astype(np.int32)
+
+    def _set_delays(self, delays, m: sp.csr_matrix, delay_matrix=None):
+        """delays: ms as a scalar (uniform), a RandomDistribution (one draw
+        per synapse, bounded below by dt) or None; delay_matrix: per-synapse
+        delays in ms with the structure of `m` (rows post, columns pre)."""
+        from .random import RandomDistribution
+        if delay_matrix is not None:
+            rows = np.repeat(np.arange(m.shape[0]), np.diff(m.indptr))
+            vals = np.asarray(delay_matrix[rows, m.indices]).ravel()
+            steps = self._steps(vals)
+        elif isinstance(delays, RandomDistribution):
+            if getattr(delays, "max", None) is None:
+                raise ValueError("a random distribution of delays needs a max value")
+            vals = np.maximum(draw(delays, (m.nnz,), self._rng()), self._dt())
+            steps = self._steps(vals)
+            # history for the distribution's whole range (Projection.py:667)
+            dist_max = int(round(float(delays.max) / self._dt()))
+        else:
+            d = 0.0 if delays is None else float(delays)
+            self.uniform_delay = max(1, int(round(d / self._dt())))
+            self.max_delay = self.uniform_delay
+            self._delay_steps = None
+            return
+        if self.plastic and self.synapse_type.type == "spike":
+            raise NotImplementedError("non-uniform delays of plastic spiking projections "
+                                      "are not supported by this backend")
+        self.uniform_delay = -1
+        self._delay_steps = steps
+        self.max_delay = max(int(steps.max()) if steps.size else 1,
+                             dist_max if delay_matrix is None else 1)
+
+    def _store(self, m: sp.csr_matrix, name, storage_format, delays=0.0, delay_matrix=None):
         m = sp.csr_matrix(m)
         m.sum_duplicates()
         m.sort_indices()
         self._csr = m
+        self._set_delays(delays, m, delay_matrix)
         self.connector_name = name
         if storage_format is not None:
             if storage_format not in FORMATS:
@@ -116,11 +160,15 @@ class Projection:
         return draw(weights, (nnz,), self._rng())
 
     def from_sparse(self, weights, delays=0.0, storage_format=None, storage_order=None):
-        """weights: scipy sparse matrix of shape (pre, post)."""
+        """weights: scipy sparse matrix of shape (pre, post); delays: ms, a
+        scalar or a sparse matrix of the same shape."""
         w = sp.csr_matrix(weights)
         if w.shape != (len(self.pre_ranks), len(self.post_ranks_view)):
             raise ValueError(f"from_sparse(): expected shape {(len(self.pre_ranks), len(self.post_ranks_view))}, "
                              f"got {w.shape}")
+        if sp.issparse(delays):
+            return self._store(w.T.tocsr(), "Sparse connectivity matrix", storage_format, None,
+                               sp.csr_matrix(delays).T.tocsr())
         return self._store(w.T.tocsr(), "Sparse connectivity matrix", storage_format, delays)
 
     connect_from_sparse = from_sparse
@@ -140,6 +188,9 @@ class Projection:
             W = np.nan_to_num(W)
         rows, cols = np.nonzero(mask)
         m = sp.csr_matrix((W[rows, cols], (rows, cols)), shape=W.shape)
+        if np.ndim(delays) == 2:
+            D = np.asarray(delays, dtype=np.float64)
+            return self._store(m, "Connectivity matrix", storage_format, None, D.T if pre_post else D)
         return self._store(m, "Connectivity matrix", storage_format, delays)
 
     def _self_mask(self, rows, cols):
@@ -218,8 +269,9 @@ class Projection:
                 wk, a, b = 2, weights.mu, weights.sigma
             else:
                 raise NotImplementedError("device connectors take constant, Uniform or Normal weights")
-            if delays not in (0, 0.0, None):
-                raise NotImplementedError("synaptic delays are not supported by this backend")
+            if not (np.ndim(delays) == 0 and not hasattr(delays, "get_values")
+                    and round(float(delays or 0.0) / self._dt()) <= 1):
+                raise NotImplementedError("device connectors take no synaptic delays")
             self._device_conn = dict(kind="fixed_number_pre", number=int(number), wkind=wk, a=a, b=b,
                                      seed=int(rng.integers(0, 2**63 - 1)),
                                      exclude_self=(not allow_self_connections
@@ -338,6 +390,50 @@ class Projection:
             self.set({name: value})
             return
         object.__setattr__(self, name, value)
+
+    # -- delays (ANNarchy/core/Projection.py:1283-1416) ------------------------------------
+    @property
+    def delay(self):
+        """Uniform delay in ms, or per dendrite the delays (ms) of its synapses."""
+        dt = self._dt()
+        if self._delay_steps is None:
+            return float(self.uniform_delay * dt)
+        steps = self._delay_steps
+        if self.net is not None and self.net._compiled:
+            steps = self.net._backend.read_delays(self)
+        return [[float(x) * dt for x in a] for a in np.split(steps, np.cumsum(self.dendrite_sizes())[:-1])]
+
+    @delay.setter
+    def delay(self, value):
+        compiled = self.net is not None and self.net._compiled
+        cap = self.net._backend.delay_capacity(self) if compiled else None
+        if self._delay_steps is None:
+            if np.ndim(value) > 0:
+                raise ValueError("the projection was created with a uniform delay; "
+                                 "non-uniform values cannot be loaded")
+            d = int(self._steps([value])[0])
+            if cap is not None and d > cap:
+                raise ValueError(f"delay of {d} steps exceeds the {cap} steps of history kept since "
+                                 f"compile(); give the largest delay before compile()")
+            self.uniform_delay = d
+            self.max_delay = max(self.max_delay, d) if not compiled else self.max_delay
+            if compiled:
+                self.net._backend.write_delays(self, np.array([d], dtype=np.int32))
+            return
+        if not isinstance(value, (list, np.ndarray)):
+            raise ValueError("non-uniform delays are set as one list of delays per dendrite")
+        sizes = self.dendrite_sizes()
+        if len(value) != sizes.size or any(len(v) != n for v, n in zip(value, sizes)):
+            raise ValueError("the delays must match the synapses of every dendrite")
+        steps = self._steps(np.concatenate([np.ravel(np.asarray(v, dtype=np.float64)) for v in value]))
+        if cap is not None and int(steps.max()) > cap:
+            raise ValueError(f"delay of {int(steps.max())} steps exceeds the {cap} steps of history "
+                             f"kept since compile(); give the largest delay before compile()")
+        self._delay_steps = steps
+        if not compiled:
+            self.max_delay = int(steps.max())
+        else:
+            self.net._backend.write_delays(self, steps)
 
     def dendrite_sizes(self):
         lengths = np.diff(self._csr.indptr)

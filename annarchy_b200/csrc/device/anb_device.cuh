@@ -75,6 +75,38 @@ __device__ __forceinline__ void anb_rate_csr_scalar(int n_rows, const I* __restr
   }
 }
 
+// Slot of time step s (possibly negative) in a ring of `slots` entries.
+__device__ __forceinline__ int anb_ring_slot(long long s, int slots) {
+  const long long m = s % slots;
+  return (int)(m < 0 ? m + slots : m);
+}
+
+// Rate-coded weighted sum with one transmission delay per synapse (steps,
+// >= 1): thread per row, sequential in stored order like anb_rate_csr_scalar,
+// each rate read from the pre population's history ring (slot of step
+// t - delay; slots x n_pre values). The reference's non-uniform delays read
+// pre.r from its queue entry delay - 1 (ANNarchy/generator/Projection/
+// SingleThreadGenerator.py, _computesum_rate with max_delay > 1).
+template <typename R, typename W, typename I>
+__device__ __forceinline__ void anb_rate_csr_delayed(int n_rows, const I* __restrict__ row_ptr,
+                                                     const int* __restrict__ col,
+                                                     const W* __restrict__ w,
+                                                     const int* __restrict__ dly,
+                                                     const R* __restrict__ ring, int n_pre,
+                                                     int slots, long long t,
+                                                     const int* __restrict__ post_rank,
+                                                     R* __restrict__ sum) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n_rows;
+       row += gridDim.x * blockDim.x) {
+    R s = R(0);
+    const I beg = row_ptr[row], end = row_ptr[row + 1];
+    for (I j = beg; j < end; ++j)
+      s += ring[(size_t)anb_ring_slot(t - dly[j], slots) * n_pre + col[j]] * (R)w[j];
+    const int post = post_rank ? post_rank[row] : row;
+    sum[post] += s;
+  }
+}
+
 // Sub-warp per row (G lanes, G in {2,4,8,16,32}), fp32 accumulation with a
 // butterfly reduction. Rows longer than `kahan_min` use compensated
 // (Kahan) summation per lane.
@@ -666,6 +698,49 @@ __device__ __forceinline__ void anb_spike_gather_warp(int n_rows, const int* __r
         const int b = __ffs(m) - 1;
         m &= m - 1;
         acc += __shfl_sync(0xffffffffu, wj, b);
+      }
+    }
+    if (any && lane == 0) g[post] = acc;
+  }
+}
+
+// Spike transmission with one delay per synapse (steps, 1..dmax): warp per
+// post row; a spike emitted at step s reaches the synapses of delay t - s at
+// step t. Contributions are added one at a time in the reference's order:
+// emission step ascending, then pre rank ascending (the push order of its
+// ring of delayed spikes, ANNarchy/generator/Projection/SingleThread/
+// LIL.py:915-969). `ring` holds one spike bitmap of `words` words per step,
+// `slots` steps.
+template <typename R, typename W>
+__device__ __forceinline__ void anb_spike_gather_delayed(int n_rows, const int* __restrict__ row_ptr,
+                                                         const int* __restrict__ col,
+                                                         const W* __restrict__ w,
+                                                         const int* __restrict__ dly,
+                                                         const anb_u32* __restrict__ ring, int words,
+                                                         int slots, long long t, int dmax,
+                                                         const int* __restrict__ post_rank,
+                                                         R* __restrict__ g) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int row = warp; row < n_rows; row += nwarps) {
+    const int beg = row_ptr[row], end = row_ptr[row + 1];
+    const int post = post_rank ? post_rank[row] : row;
+    R acc = g[post];
+    bool any = false;
+    for (int d = dmax; d >= 1; --d) {
+      const anb_u32* spk = ring + (size_t)anb_ring_slot(t - d, slots) * words;
+      for (int base = beg; base < end; base += 32) {
+        const int j = base + lane;
+        const bool sp = j < end && dly[j] == d && anb_bit(spk, col[j]);
+        anb_u32 m = __ballot_sync(0xffffffffu, sp);
+        any |= m != 0u;
+        const R wj = sp ? (R)w[j] : R(0);
+        while (m) {
+          const int b = __ffs(m) - 1;
+          m &= m - 1;
+          acc += __shfl_sync(0xffffffffu, wj, b);
+        }
       }
     }
     if (any && lane == 0) g[post] = acc;

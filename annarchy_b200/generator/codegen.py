@@ -101,6 +101,36 @@ class CodeGenerator:
         self.decls[name] = CTYPE_OF[np.dtype(dtype)]
         return "anb_p_" + name
 
+    # history rings (synaptic delays)
+    def slots(self, pop) -> int:
+        return self.c.slots.get(pop.id, 1)
+
+    def spk_at(self, pop, step: str) -> str:
+        """Spike bitmap of the population at time step `step` (a C
+        expression); the slot of that step when the population keeps a ring."""
+        spk = self.ptr(f"pop{pop.id}__spk")
+        R = self.slots(pop)
+        if R == 1:
+            return spk
+        return f"({spk} + (size_t)anb_ring_slot({step}, {R}) * {(pop.size + 31) // 32})"
+
+    def delayed(self, proj) -> bool:
+        """The projection reads its pre-synaptic output through a delay ring."""
+        return proj.max_delay > 1
+
+    def pre_spk(self, proj) -> str:
+        if self.delayed(proj) and proj._delay_steps is None:
+            return self.spk_at(proj.pre_pop, f"t - {self.ptr(f'proj{proj.id}__delay')}[0]")
+        return self.spk_at(proj.pre_pop, "t - 1")
+
+    def pre_rate(self, proj) -> str:
+        k = proj.pre_pop.id
+        if self.delayed(proj) and proj._delay_steps is None:
+            R, S = self.slots(proj.pre_pop), self.c.ring_stride(proj.pre_pop)
+            return (f"({self.ptr(f'pop{k}___delayed_r')} + (size_t)anb_ring_slot(t - "
+                    f"{self.ptr(f'proj{proj.id}__delay')}[0], {R}) * {S})")
+        return self.ptr(f"pop{k}__r")
+
     def typed(self, code: str) -> str:
         code = code.replace("double ", self.real + " ")
         return code if self.exact else float_literals(code)
@@ -322,8 +352,16 @@ class CodeGenerator:
           {gsrc('last_spike')}[anb_i] = t;
           {refr_set}
         }}"""
-        spk_dst = ((smem.get("spk") if smem else gsrc("spk")) if spiking and ballot_hook is None
-                   else None)
+        grid_path = not smem and cluster is None and not local_engine
+        if spiking and ballot_hook is None:
+            spk_dst = smem.get("spk") if smem else (self.spk_at(pop, "t") if grid_path else gsrc("spk"))
+        else:
+            spk_dst = None
+        if grid_path and pop.neuron_type.type == "rate" and self.slots(pop) > 1:
+            # this step's rate into the history ring (the reference's update_delay)
+            rv = "r" if "r" in names else f"{gsrc('r')}[anb_i]"
+            stores.append(f"{self.ptr(f'pop{k}___delayed_r')}[(size_t)anb_ring_slot(t, {self.slots(pop)}) * "
+                          f"{self.c.ring_stride(pop)} + anb_i] = {rv};")
         ballot = ""
         listed = (spiking and cluster is None and not local_engine and not self.exact
                   and self.c.spike_lists)
@@ -409,6 +447,20 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
 }}
 """
 
+    def delay_kernel(self, pop) -> str:
+        """This step's rates into the history ring of a population without
+        an update of its own (the reference's update_delay)."""
+        k = pop.id
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_delay() {{
+    const long long t = *{self.ptr('t')};
+    for (int anb_i = blockIdx.x * blockDim.x + threadIdx.x; anb_i < {pop.size};
+         anb_i += gridDim.x * blockDim.x)
+      {self.ptr(f'pop{k}___delayed_r')}[(size_t)anb_ring_slot(t, {self.slots(pop)}) * {self.c.ring_stride(pop)} + anb_i] =
+          {self.ptr(f'pop{k}__r')}[anb_i];
+}}
+"""
+
     def has_update(self, pop) -> bool:
         if pop.neuron_type.type == "spike":
             return True
@@ -420,20 +472,29 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
         format. Returns (source, [(kernel, grid, block, smem)])."""
         k = proj.id
         lay = self.c.layout[proj.id]
-        pre_r = self.ptr(f"pop{proj.pre_pop.id}__r")
+        pre_r = self.pre_rate(proj)
         sum_ = self.ptr(f"pop{proj.post_pop.id}___sum_{proj.target}")
         fmt = lay["format"]
         p = lambda n: self.ptr(f"proj{k}__{n}")
         W = self.c.wctype
         name = f"proj{k}_psp"
+        tdecl = f"const long long t = *{self.ptr('t')};\n    " if self.delayed(proj) else ""
 
         def kern(nm, body, block=BLOCK, min_blocks=None):
             bounds = f"{block}, {min_blocks}" if min_blocks else f"{block}"
             return f"""
 extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
-    {body}
+    {tdecl}{body}
 }}
 """
+        if proj._delay_steps is not None:
+            # one delay per synapse: CSR rows read the rate ring per synapse
+            a = proj.pre_pop
+            call = (f"anb_rate_csr_delayed<{self.real}, {W}, {lay['idx_t']}>({lay['rows']}, "
+                    f"{p('row_ptr')}, {p('col')}, {p('w')}, {p('dly')}, "
+                    f"{self.ptr(f'pop{a.id}___delayed_r')}, {self.c.ring_stride(a)}, {self.slots(a)}, t, "
+                    f"{p('post_rank')}, {sum_});")
+            return kern(name, call), [(name, grid_for(lay["rows"]), BLOCK, 0)]
         if fmt == "pcsr" and not self.exact:
             pw, mr = lay["panel_width"], lay["pc_max_rows"]
             smem = 4 * pw + 4 * (mr + 1) + 4 * mr
@@ -506,24 +567,38 @@ extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
         else:
             body = (f"anb_rate_coo_atomic<{self.c.wctype}>({lay['coo_nnz']}, {p('coo_row')}, "
                     f"{p('coo_col')}, {p('coo_w')}, {pre_r}, {p('post_rank')}, {sum_});")
+        tdecl = f"const long long t = *{self.ptr('t')};\n    " if self.delayed(proj) else ""
         return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp_tail() {{
-    {body}
+    {tdecl}{body}
 }}
 """
 
     def spike_kernel(self, proj) -> str:
         k = proj.id
         lay = self.c.layout[proj.id]
-        pre_spk = self.ptr(f"pop{proj.pre_pop.id}__spk")
+        pre_spk = self.pre_spk(proj)
         g = self.ptr(f"pop{proj.post_pop.id}__g_{proj.target}")
         p = lambda n: self.ptr(f"proj{k}__{n}")
         if proj.plastic:
             return self.plastic_psp_kernel(proj, lay, pre_spk, g)
+        tdecl = f"const long long t = *{self.ptr('t')};"
+        if proj._delay_steps is not None:
+            a = proj.pre_pop
+            call = (f"anb_spike_gather_delayed<{self.real}, {self.c.wctype if not self.exact else 'double'}>("
+                    f"{lay['rows']}, {p('row_ptr')}, {p('col')}, {p('w')}, {p('dly')}, "
+                    f"{self.ptr(f'pop{a.id}__spk')}, {(a.size + 31) // 32}, {self.slots(a)}, t, "
+                    f"{self.slots(a)}, {p('post_rank')}, {g});")
+            return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    {tdecl}
+    {call}
+}}
+"""
         if self.exact:
             call = (f"anb_spike_gather_warp<double, double>({lay['rows']}, {p('row_ptr')}, {p('col')}, "
                     f"{p('w')}, {pre_spk}, {p('post_rank')}, {g});")
-        elif self.c.spike_lists:
+        elif self.c.spike_lists and not self.delayed(proj):
             a = proj.pre_pop.id
             call = (f"anb_spike_scatter_list<float, {self.c.wctype}>({lay['w0'] * 32}, {lay['w1'] * 32}, "
                     f"{self.ptr(f'pop{a}__spl')} + ((t - 1) & 1) * (long long){proj.pre_pop.size}, "
@@ -540,6 +615,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
                     f"{p('col_ptr')}, {p('post_idx')}, {p('w_pre')}, {g});")
         return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    {tdecl}
     {call}
 }}
 """
@@ -583,14 +659,16 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
                 code = f"if (anb_plastic) {{ {code} }}"
             stmts.append(self.typed(code))
         body = "\n          ".join(stmts)
-        if self.exact:
+        if self.exact or self.delayed(proj) or not self.c.spike_lists:
             # warp per post row; the spiking synapses of a row are processed in
             # ascending pre rank, one at a time, by the lane that holds them
-            # (the running conductance `sum` is passed along with a shuffle)
+            # (the running conductance `sum` is passed along with a shuffle);
+            # also the fast form of a delayed projection (spike lists hold
+            # only the previous step)
             return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     const long long t = *{self.ptr('t')};
-    const double dt = *{self.ptr('dt')};
+    const {self.real} dt = ({self.real})(*{self.ptr('dt')});
     const int anb_plastic = {p('flags')}[0];
     {self._syn_globals(proj)}
     {self._syn_arrays(proj)}
@@ -599,7 +677,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
          anb_row += (gridDim.x * blockDim.x) >> 5) {{
       const int anb_post = {p('post_rank')}[anb_row];
       const int anb_beg = {p('row_ptr')}[anb_row], anb_end = {p('row_ptr')}[anb_row + 1];
-      double sum = {g}[anb_post];
+      {self.real} sum = {g}[anb_post];
       bool anb_any = false;
       for (int anb_b0 = anb_beg; anb_b0 < anb_end; anb_b0 += 32) {{
         const int j = anb_b0 + anb_lane;
@@ -654,7 +732,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
         k = proj.id
         lay = self.c.layout[proj.id]
         p = lambda n: self.ptr(f"proj{k}__{n}")
-        post_spk = self.ptr(f"pop{proj.post_pop.id}__spk")
+        post_spk = self.spk_at(proj.post_pop, "t")
         stmts = self._event_driven(proj, "j", "t")
         for v in proj.desc["post_spike"]:
             code = self.fill(v["cpp"], local="[j]")
@@ -752,6 +830,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
             if self.has_update(pop):
                 kernels.append(self.pop_kernel(pop))
                 plan.append((f"pop{pop.id}_step", grid_for(pop.size), BLOCK, 0))
+            elif pop.neuron_type.type == "rate" and self.slots(pop) > 1:
+                kernels.append(self.delay_kernel(pop))
+                plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))
         for proj in net.projections:
             if proj.synapse_type.type == "spike" and proj.desc.get("post_spike"):
                 kernels.append(self.post_event_kernel(proj))

@@ -303,18 +303,34 @@ def batched_coba(n_instances: int = 256, seed: int = 42, n_min: int = 1000,
 # networks built through the public API
 # ---------------------------------------------------------------------------
 
+def delay_arg(m: sp.csr_matrix, d, dt: float):
+    """Connector `delays` argument for the (post, pre) matrix m: None -> no
+    delay, a number -> uniform delay of that many steps, an array -> one
+    delay (steps) per synapse in m's CSR order, as a sparse (pre, post)
+    matrix of delays in ms."""
+    if d is None:
+        return 0.0
+    if np.ndim(d) == 0:
+        return float(d) * dt
+    dm = sp.csr_matrix((np.asarray(d, dtype=np.float64) * dt, m.indices, m.indptr), shape=m.shape)
+    return to_from_sparse(dm)
+
+
 def build_rate_network(rn: RateNet, precision: str = "double", record: bool = True,
-                       storage_format: str = "csr", **config):
+                       storage_format: str = "csr", delays=(None, None), **config):
     """Input population (constant r) -> leaky integrators, input and
-    recurrent projections on target 'exc'. Returns (net, pop, monitor)."""
+    recurrent projections on target 'exc'; `delays` (input, recurrent) as in
+    delay_arg. Returns (net, pop, monitor)."""
     from . import Network, Neuron
     net = Network(dt=rn.dt, seed=0)
     net.config(precision=precision, **config)
     inp = net.create(rn.n_in, Neuron(parameters="r = 0.0"))
     li = Neuron(parameters=dict(tau=rn.tau), equations="tau*dr/dt + r = sum(exc) : min=0.0")
     pop = net.create(rn.n_out, li)
-    net.connect(inp, pop, "exc").from_sparse(to_from_sparse(rn.w_in), storage_format=storage_format)
-    net.connect(pop, pop, "exc").from_sparse(to_from_sparse(rn.w_rec), storage_format=storage_format)
+    net.connect(inp, pop, "exc").from_sparse(to_from_sparse(rn.w_in), delay_arg(rn.w_in, delays[0], rn.dt),
+                                             storage_format=storage_format)
+    net.connect(pop, pop, "exc").from_sparse(to_from_sparse(rn.w_rec), delay_arg(rn.w_rec, delays[1], rn.dt),
+                                             storage_format=storage_format)
     mon = net.monitor(pop, "r") if record else None
     inp.r = rn.r_in
     return net, pop, mon
@@ -327,21 +343,24 @@ def coba_neuron(params: dict):
 
 
 def build_coba_network(cn: CobaNet, precision: str = "double", engine: str = "auto",
-                       record: bool = True, stdp_w_ee: sp.csr_matrix | None = None, **config):
+                       record: bool = True, stdp_w_ee: sp.csr_matrix | None = None,
+                       delays=(None, None), **config):
     """The spiking net: E->all (exc) and I->all (inh); with a plastic E->E
-    matrix: E->E (STDP, exc), E->I (exc), I->all (inh). Returns (net, pop,
-    monitor); the initial potentials are set after compile()."""
+    matrix: E->E (STDP, exc), E->I (exc), I->all (inh). `delays` (exc, inh)
+    of E->all / I->all as in delay_arg. Returns (net, pop, monitor); the
+    initial potentials are set after compile()."""
     from . import STDP, Network
     net = Network(dt=cn.dt, seed=0)
     net.config(precision=precision, engine=engine, **config)
     P = net.create(cn.n, coba_neuron(cn.params))
     Pe, Pi = P[: cn.n_exc], P[cn.n_exc:]
     if stdp_w_ee is None:
-        net.connect(Pe, P, "exc").from_sparse(to_from_sparse(cn.w_exc))
+        net.connect(Pe, P, "exc").from_sparse(to_from_sparse(cn.w_exc),
+                                              delay_arg(cn.w_exc, delays[0], cn.dt))
     else:
         net.connect(Pe, Pe, "exc", synapse=STDP(**STDP_PARAMS)).from_sparse(to_from_sparse(stdp_w_ee))
         net.connect(Pe, Pi, "exc").from_sparse(to_from_sparse(cn.w_exc[cn.n_exc:]))
-    net.connect(Pi, P, "inh").from_sparse(to_from_sparse(cn.w_inh))
+    net.connect(Pi, P, "inh").from_sparse(to_from_sparse(cn.w_inh), delay_arg(cn.w_inh, delays[1], cn.dt))
     mon = net.monitor(P, "spike") if record else None
     P.v = cn.v0
     return net, P, mon

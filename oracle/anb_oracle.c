@@ -26,7 +26,16 @@
  *    of the spiking configurations, with the refractory mask of
  *    ANNarchy/generator/Population/OpenMPGenerator.py:870-998 and the spike
  *    gather of :999-1237; refractory steps are int(refractory_ms / dt)
- *    (ANNarchy/core/Population.py:659-690).
+ *    (ANNarchy/core/Population.py:659-690);
+ *  - synaptic delays (ANNarchy/generator/Population/SingleThreadGenerator.py
+ *    :370-445, SingleThreadTemplates.py:182-212; Projection/
+ *    SingleThreadGenerator.py:1186-1195; SingleThread/LIL.py:915-969): a
+ *    population keeps the outputs of its last max_delay steps; a rate-coded
+ *    projection with delay d reads the rates of step t - d (the history
+ *    starts filled with the initial rates); a spiking projection with
+ *    uniform delay d propagates the spike list of step t - d; with one delay
+ *    per synapse a post neuron receives the spikes by emission step
+ *    ascending, then pre rank ascending.
  *
  * Parity pinned against golden fixtures produced by running the reference
  * itself (tests/golden/make_golden.py).
@@ -41,7 +50,7 @@
 
 #define ORC_CLIP(x, a, b) ((x) < (a) ? (a) : ((x) > (b) ? (b) : (x)))
 
-int orc_version(void) { return 1; }
+int orc_version(void) { return 2; }
 
 int orc_max_threads(void) {
 #ifdef _OPENMP
@@ -63,7 +72,14 @@ typedef struct {
   const int* row_ptr;
   const int* col;
   const double* w;
+  int delay;            /* uniform delay in steps (<= 1: the previous step) */
+  const int* syn_delay; /* per-synapse delays in steps (CSR order) or NULL */
 } orc_rate_proj;
+
+static int orc_slot(int64_t s, int slots) {
+  int64_t m = s % slots;
+  return (int)(m < 0 ? m + slots : m);
+}
 
 /* Simulates `steps` steps of: input population (constant r_in) and one
  * leaky-integrator population of n_out neurons with a single target "exc".
@@ -76,11 +92,23 @@ int orc_rate_run(int n_in, int n_out, const double* r_in, double* r, int nproj,
                  double* r_trace, int threads) {
   double* sum = (double*)calloc((size_t)n_out, sizeof(double));
   double* r_prev = (double*)malloc(sizeof(double) * (size_t)n_out);
-  if (!sum || !r_prev) {
+  /* history of the integrators' rates: slot t % slots holds step t, every
+   * slot starting at the initial rates (the input population is constant) */
+  int slots = 1;
+  for (int p = 0; p < nproj; ++p) {
+    if (projs[p].delay > slots) slots = projs[p].delay;
+    if (projs[p].syn_delay)
+      for (int j = 0; j < projs[p].row_ptr[n_out]; ++j)
+        if (projs[p].syn_delay[j] > slots) slots = projs[p].syn_delay[j];
+  }
+  double* hist = (double*)malloc(sizeof(double) * (size_t)n_out * (size_t)slots);
+  if (!sum || !r_prev || !hist) {
     free(sum);
     free(r_prev);
+    free(hist);
     return 1;
   }
+  for (int q = 0; q < slots; ++q) memcpy(hist + (size_t)q * n_out, r, sizeof(double) * (size_t)n_out);
 #ifdef _OPENMP
   if (threads < 1) threads = 1;
 #endif
@@ -93,11 +121,18 @@ int orc_rate_run(int n_in, int n_out, const double* r_in, double* r, int nproj,
       for (int i = 0; i < n_out; ++i) sum[i] = 0.0;
       for (int p = 0; p < nproj; ++p) {
         const orc_rate_proj* pj = &projs[p];
-        const double* pre_r = pj->pre == 0 ? r_in : r_prev;
+        const int d = pj->delay > 1 ? pj->delay : 1;
+        const double* pre_r = pj->pre == 0 ? r_in
+                              : (d > 1 ? hist + (size_t)orc_slot(t - d, slots) * n_out : r_prev);
 #pragma omp for schedule(static)
         for (int i = 0; i < n_out; ++i) {
           double s = 0.0;
-          for (int j = pj->row_ptr[i]; j < pj->row_ptr[i + 1]; ++j) s += pre_r[pj->col[j]] * pj->w[j];
+          if (pj->syn_delay && pj->pre != 0) {
+            for (int j = pj->row_ptr[i]; j < pj->row_ptr[i + 1]; ++j)
+              s += hist[(size_t)orc_slot(t - pj->syn_delay[j], slots) * n_out + pj->col[j]] * pj->w[j];
+          } else {
+            for (int j = pj->row_ptr[i]; j < pj->row_ptr[i + 1]; ++j) s += pre_r[pj->col[j]] * pj->w[j];
+          }
           sum[i] += s;
         }
       }
@@ -108,10 +143,12 @@ int orc_rate_run(int n_in, int n_out, const double* r_in, double* r, int nproj,
         if (r[i] < r_min) r[i] = r_min;
       }
     }
+    memcpy(hist + (size_t)orc_slot(t, slots) * n_out, r, sizeof(double) * (size_t)n_out);
     if (r_trace) memcpy(r_trace + (size_t)t * n_out, r, sizeof(double) * (size_t)n_out);
   }
   free(sum);
   free(r_prev);
+  free(hist);
   return 0;
 }
 
@@ -149,6 +186,8 @@ typedef struct {
   double* x;
   double* y;
   int64_t* last_event;
+  int delay;            /* uniform delay in steps (<= 1: the previous step) */
+  const int* syn_delay; /* per-synapse delays in steps (CSR order) or NULL */
 } orc_spike_proj;
 
 /* Simulates `steps` steps starting at time step t0. State arrays (length n)
@@ -163,7 +202,28 @@ int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double
                  int64_t* n_spikes, int threads) {
   short* in_ref = (short*)malloc(sizeof(short) * (size_t)n);
   int* row_of = NULL;
-  if (!in_ref) return 1;
+  /* spike lists of the last `slots` steps (slot s % slots holds step s);
+   * the step before t0 is the list passed in, older steps had no spikes */
+  int slots = 1;
+  for (int p = 0; p < nproj; ++p) {
+    if (projs[p].delay > slots) slots = projs[p].delay;
+    if (projs[p].syn_delay)
+      for (int j = 0; j < projs[p].row_ptr[projs[p].n_rows]; ++j)
+        if (projs[p].syn_delay[j] > slots) slots = projs[p].syn_delay[j];
+  }
+  int* hist = (int*)malloc(sizeof(int) * (size_t)n * (size_t)slots);
+  int* hist_n = (int*)calloc((size_t)slots, sizeof(int));
+  if (!in_ref || !hist || !hist_n) {
+    free(in_ref);
+    free(hist);
+    free(hist_n);
+    return 1;
+  }
+  {
+    const int q = orc_slot(t0 - 1, slots);
+    hist_n[q] = *n_spiked;
+    memcpy(hist + (size_t)q * n, spiked, sizeof(int) * (size_t)(*n_spiked));
+  }
   int64_t total = 0;
   int ns = *n_spiked;
 #ifdef _OPENMP
@@ -178,6 +238,8 @@ int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double
     row_of = (int*)malloc(sizeof(int) * (size_t)n * (size_t)nproj);
     if (!row_of) {
       free(in_ref);
+      free(hist);
+      free(hist_n);
       return 1;
     }
     for (int p = 0; p < nproj; ++p) {
@@ -187,12 +249,30 @@ int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double
   }
   for (int s = 0; s < steps; ++s) {
     const int64_t t = t0 + s;
-    /* compute_psp: propagate the previous step's spikes, projection by projection */
+    /* compute_psp: propagate the (delayed) spikes, projection by projection */
     for (int p = 0; p < nproj; ++p) {
       const orc_spike_proj* pj = &projs[p];
       double* g = pj->target == 0 ? g_exc : g_inh;
-      for (int k = 0; k < ns; ++k) {
-        const int pre = spiked[k];
+      if (pj->syn_delay) {
+        /* emission step ascending, spikes ascending, synapses whose delay
+         * brings that step's spike to this step */
+        for (int64_t s0 = t - slots; s0 < t; ++s0) {
+          const int q = orc_slot(s0, slots);
+          const int* lst = hist + (size_t)q * n;
+          for (int k = 0; k < hist_n[q]; ++k) {
+            const int pre = lst[k];
+            for (int syn = pj->col_ptr[pre]; syn < pj->col_ptr[pre + 1]; ++syn) {
+              const int j = pj->inv_idx[syn];
+              if ((int64_t)pj->syn_delay[j] == t - s0) g[pj->post_rank[pj->row_idx[syn]]] += pj->w[j];
+            }
+          }
+        }
+        continue;
+      }
+      const int dq = orc_slot(t - (pj->delay > 1 ? pj->delay : 1), slots);
+      const int* lst = hist + (size_t)dq * n;
+      for (int k = 0; k < hist_n[dq]; ++k) {
+        const int pre = lst[k];
         const int beg = pj->col_ptr[pre], end = pj->col_ptr[pre + 1];
         if (!pj->stdp) {
 #pragma omp parallel for num_threads(threads) schedule(static) if (end - beg > 4096)
@@ -225,13 +305,14 @@ int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double
       g_inh[i] += dt * _g_inh;
       refractory_remaining[i] -= (1 - in_ref[i]);
     }
-    /* spike gather, ascending ranks */
+    /* spike gather, ascending ranks, into this step's slot */
     ns = 0;
+    int* cur = hist + (size_t)orc_slot(t, slots) * n;
     for (int i = 0; i < n; ++i) {
       if (in_ref[i] == 0) continue;
       if (v[i] > prm->Vt) {
         v[i] = prm->Vr;
-        spiked[ns++] = i;
+        cur[ns++] = i;
         last_spike[i] = t;
         refractory_remaining[i] = refractory_steps;
         if (total < max_spikes) {
@@ -241,13 +322,14 @@ int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double
         ++total;
       }
     }
+    hist_n[orc_slot(t, slots)] = ns;
     /* post_event of plastic projections */
     for (int p = 0; p < nproj; ++p) {
       const orc_spike_proj* pj = &projs[p];
       if (!pj->stdp) continue;
       const orc_stdp_params* sp = pj->stdp;
       for (int k = 0; k < ns; ++k) {
-        const int r = row_of[(size_t)p * n + spiked[k]];
+        const int r = row_of[(size_t)p * n + cur[k]];
         if (r < 0) continue;
         for (int j = pj->row_ptr[r]; j < pj->row_ptr[r + 1]; ++j) {
           pj->x[j] *= exp(dt * (double)(pj->last_event[j] - (t)) / (sp->tau_plus));
@@ -259,10 +341,17 @@ int orc_coba_run(int n, const orc_coba_params* prm, int refractory_steps, double
       }
     }
   }
-  *n_spiked = ns;
+  {
+    const int q = orc_slot(t0 + steps - 1, slots);
+    *n_spiked = steps > 0 ? hist_n[q] : *n_spiked;
+    if (steps > 0) memcpy(spiked, hist + (size_t)q * n, sizeof(int) * (size_t)hist_n[q]);
+  }
+  (void)ns;
   *n_spikes = total;
   free(in_ref);
   free(row_of);
+  free(hist);
+  free(hist_n);
   return 0;
 }
 

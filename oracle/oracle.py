@@ -48,7 +48,8 @@ def max_threads() -> int:
 
 
 class _RateProj(C.Structure):
-    _fields_ = [("pre", C.c_int), ("row_ptr", C.c_void_p), ("col", C.c_void_p), ("w", C.c_void_p)]
+    _fields_ = [("pre", C.c_int), ("row_ptr", C.c_void_p), ("col", C.c_void_p), ("w", C.c_void_p),
+                ("delay", C.c_int), ("syn_delay", C.c_void_p)]
 
 
 class _CobaParams(C.Structure):
@@ -66,16 +67,29 @@ class _SpikeProj(C.Structure):
                 ("col", C.c_void_p), ("w", C.c_void_p), ("col_ptr", C.c_void_p),
                 ("row_idx", C.c_void_p), ("inv_idx", C.c_void_p), ("target", C.c_int),
                 ("stdp", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p),
-                ("last_event", C.c_void_p)]
+                ("last_event", C.c_void_p), ("delay", C.c_int), ("syn_delay", C.c_void_p)]
 
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def rate_run(rn, steps: int | None = None, threads: int = 1, trace: bool = False):
+def _delay_args(d, keep):
+    """(uniform steps, per-synapse steps pointer) of a delay spec: an int
+    (steps) or an array of steps per synapse in CSR order."""
+    if d is None or np.ndim(d) == 0:
+        return int(d or 1), None
+    a = np.ascontiguousarray(d, dtype=np.int32)
+    keep.append(a)
+    return 1, _p(a).value
+
+
+def rate_run(rn, steps: int | None = None, threads: int = 1, trace: bool = False,
+             delays=(None, None)):
     """Runs the rate-coded network ``rn`` (workloads.RateNet) for ``steps``
-    steps. Returns (r_final, r_trace or None)."""
+    steps. ``delays``: (input projection, recurrent projection), each None,
+    a uniform delay in steps or per-synapse steps in CSR order. Returns
+    (r_final, r_trace or None)."""
     steps = rn.steps if steps is None else steps
     keep = []
     projs = (_RateProj * 2)()
@@ -84,7 +98,8 @@ def rate_run(rn, steps: int | None = None, threads: int = 1, trace: bool = False
         col = np.ascontiguousarray(m.indices, dtype=np.int32)
         w = np.ascontiguousarray(m.data, dtype=np.float64)
         keep += [rp, col, w]
-        projs[k] = _RateProj(pre, _p(rp).value, _p(col).value, _p(w).value)
+        d, sd = _delay_args(delays[k], keep)
+        projs[k] = _RateProj(pre, _p(rp).value, _p(col).value, _p(w).value, d, sd)
     r_in = np.ascontiguousarray(rn.r_in, dtype=np.float64)
     r = np.zeros(rn.n_out, dtype=np.float64)
     tr = np.zeros((steps, rn.n_out), dtype=np.float64) if trace else None
@@ -103,7 +118,7 @@ class SpikeProjection:
     columns are pre ranks pre_ranks[c] of the same population."""
 
     def __init__(self, n: int, w_post_pre: sp.csr_matrix, post_ranks, pre_ranks, target: int,
-                 stdp: dict | None = None):
+                 stdp: dict | None = None, delay=None):
         m = w_post_pre.tocsr()
         m.sort_indices()
         pre_ranks = np.asarray(pre_ranks, dtype=np.int32)
@@ -119,6 +134,8 @@ class SpikeProjection:
         self.col_ptr = np.zeros(n + 1, dtype=np.int32)
         np.cumsum(np.bincount(self.col, minlength=n), out=self.col_ptr[1:])
         self.target = target
+        self._keep = []
+        self.delay, self.syn_delay = _delay_args(delay, self._keep)
         self.stdp = None
         self.x = self.y = self.last_event = None
         if stdp is not None:
@@ -135,16 +152,20 @@ class SpikeProjection:
             C.cast(C.pointer(self.stdp), C.c_void_p).value if self.stdp is not None else None,
             _p(self.x).value if self.x is not None else None,
             _p(self.y).value if self.y is not None else None,
-            _p(self.last_event).value if self.last_event is not None else None)
+            _p(self.last_event).value if self.last_event is not None else None,
+            int(self.delay), self.syn_delay)
 
 
-def coba_projections(cn, stdp_w_ee: sp.csr_matrix | None = None, stdp: dict | None = None):
+def coba_projections(cn, stdp_w_ee: sp.csr_matrix | None = None, stdp: dict | None = None,
+                     delays=(None, None)):
     """Projections of a workloads.CobaNet: E->all (exc) and I->all (inh), or,
-    with a plastic E->E matrix, E->E (STDP, exc), E->I (exc), I->all (inh)."""
+    with a plastic E->E matrix, E->E (STDP, exc), E->I (exc), I->all (inh).
+    ``delays`` (exc, inh) of the E->all / I->all projections: None, uniform
+    steps or per-synapse steps in CSR order."""
     n, ne = cn.n, cn.n_exc
     if stdp_w_ee is None:
-        return [SpikeProjection(n, cn.w_exc, np.arange(n), np.arange(ne), 0),
-                SpikeProjection(n, cn.w_inh, np.arange(n), np.arange(ne, n), 1)]
+        return [SpikeProjection(n, cn.w_exc, np.arange(n), np.arange(ne), 0, delay=delays[0]),
+                SpikeProjection(n, cn.w_inh, np.arange(n), np.arange(ne, n), 1, delay=delays[1])]
     return [SpikeProjection(n, stdp_w_ee, np.arange(ne), np.arange(ne), 0, stdp=stdp),
             SpikeProjection(n, cn.w_exc[ne:], np.arange(ne, n), np.arange(ne), 0),
             SpikeProjection(n, cn.w_inh, np.arange(n), np.arange(ne, n), 1)]
