@@ -134,6 +134,8 @@ class Projection:
         if self.plastic and self.synapse_type.type == "spike":
             raise NotImplementedError("non-uniform delays of plastic spiking projections "
                                       "are not supported by this backend")
+        if steps.size and int(steps.max()) > 63:
+            raise NotImplementedError("per-synapse delays are limited to 63 steps by this backend")
         self.uniform_delay = -1
         self._delay_steps = steps
         self.max_delay = max(int(steps.max()) if steps.size else 1,
@@ -426,6 +428,8 @@ class Projection:
         if len(value) != sizes.size or any(len(v) != n for v, n in zip(value, sizes)):
             raise ValueError("the delays must match the synapses of every dendrite")
         steps = self._steps(np.concatenate([np.ravel(np.asarray(v, dtype=np.float64)) for v in value]))
+        if int(steps.max()) > 63:
+            raise ValueError("per-synapse delays are limited to 63 steps by this backend")
         if cap is not None and int(steps.max()) > cap:
             raise ValueError(f"delay of {int(steps.max())} steps exceeds the {cap} steps of history "
                              f"kept since compile(); give the largest delay before compile()")

@@ -706,18 +706,20 @@ __device__ __forceinline__ void anb_spike_gather_warp(int n_rows, const int* __r
 
 // Spike transmission with one delay per synapse (steps, 1..dmax): warp per
 // post row; a spike emitted at step s reaches the synapses of delay t - s at
-// step t. Contributions are added one at a time in the reference's order:
-// emission step ascending, then pre rank ascending (the push order of its
-// ring of delayed spikes, ANNarchy/generator/Projection/SingleThread/
-// LIL.py:915-969). `ring` holds one spike bitmap of `words` words per step,
-// `slots` steps.
-template <typename R, typename W>
+// step t. `ring` holds one spike bitmap of `words` words per step, `slots`
+// steps. ORDERED adds the contributions one at a time in the reference's
+// order: emission step ascending, then pre rank ascending (the push order of
+// its ring of delayed spikes, ANNarchy/generator/Projection/SingleThread/
+// LIL.py:915-969): a first pass over the row collects the delays that
+// deliver a spike this step (a bit mask), then one pass per such delay, the
+// largest first. Without ORDERED one pass adds them in pre-rank order.
+template <typename R, typename W, bool ORDERED>
 __device__ __forceinline__ void anb_spike_gather_delayed(int n_rows, const int* __restrict__ row_ptr,
                                                          const int* __restrict__ col,
                                                          const W* __restrict__ w,
                                                          const int* __restrict__ dly,
                                                          const anb_u32* __restrict__ ring, int words,
-                                                         int slots, long long t, int dmax,
+                                                         int slots, long long t,
                                                          const int* __restrict__ post_rank,
                                                          R* __restrict__ g) {
   const int lane = threadIdx.x & 31;
@@ -726,15 +728,24 @@ __device__ __forceinline__ void anb_spike_gather_delayed(int n_rows, const int* 
   for (int row = warp; row < n_rows; row += nwarps) {
     const int beg = row_ptr[row], end = row_ptr[row + 1];
     const int post = post_rank ? post_rank[row] : row;
+    // delays (bit d) that deliver a spike to this row at step t
+    unsigned long long dmask = 0ull;
     R acc = g[post];
-    bool any = false;
-    for (int d = dmax; d >= 1; --d) {
-      const anb_u32* spk = ring + (size_t)anb_ring_slot(t - d, slots) * words;
-      for (int base = beg; base < end; base += 32) {
-        const int j = base + lane;
-        const bool sp = j < end && dly[j] == d && anb_bit(spk, col[j]);
+    for (int base = beg; base < end; base += 32) {
+      const int j = base + lane;
+      bool sp = false;
+      int d = 0;
+      if (j < end) {
+        d = dly[j];
+        sp = anb_bit(ring + (size_t)anb_ring_slot(t - d, slots) * words, col[j]);
+      }
+      if (ORDERED) {
+        unsigned long long m = sp ? (1ull << d) : 0ull;
+        for (int o = 16; o > 0; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
+        dmask |= m;
+      } else {
         anb_u32 m = __ballot_sync(0xffffffffu, sp);
-        any |= m != 0u;
+        dmask |= m;
         const R wj = sp ? (R)w[j] : R(0);
         while (m) {
           const int b = __ffs(m) - 1;
@@ -743,7 +754,25 @@ __device__ __forceinline__ void anb_spike_gather_delayed(int n_rows, const int* 
         }
       }
     }
-    if (any && lane == 0) g[post] = acc;
+    if (ORDERED) {
+      for (unsigned long long rest = dmask; rest; ) {
+        const int d = 63 - __clzll(rest);              // largest delay first: oldest spikes
+        rest &= ~(1ull << d);
+        const anb_u32* spk = ring + (size_t)anb_ring_slot(t - d, slots) * words;
+        for (int base = beg; base < end; base += 32) {
+          const int j = base + lane;
+          const bool sp = j < end && dly[j] == d && anb_bit(spk, col[j]);
+          anb_u32 m = __ballot_sync(0xffffffffu, sp);
+          const R wj = sp ? (R)w[j] : R(0);
+          while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            acc += __shfl_sync(0xffffffffu, wj, b);
+          }
+        }
+      }
+    }
+    if (dmask != 0ull && lane == 0) g[post] = acc;
   }
 }
 

@@ -585,10 +585,11 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp_tail() {{
         tdecl = f"const long long t = *{self.ptr('t')};"
         if proj._delay_steps is not None:
             a = proj.pre_pop
-            call = (f"anb_spike_gather_delayed<{self.real}, {self.c.wctype if not self.exact else 'double'}>("
+            call = (f"anb_spike_gather_delayed<{self.real}, {self.c.wctype if not self.exact else 'double'}, "
+                    f"{'true' if self.exact else 'false'}>("
                     f"{lay['rows']}, {p('row_ptr')}, {p('col')}, {p('w')}, {p('dly')}, "
                     f"{self.ptr(f'pop{a.id}__spk')}, {(a.size + 31) // 32}, {self.slots(a)}, t, "
-                    f"{self.slots(a)}, {p('post_rank')}, {g});")
+                    f"{p('post_rank')}, {g});")
             return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     {tdecl}

@@ -639,6 +639,56 @@ def spmm_study(batches=(64, 128, 256), reps=5):
     return out
 
 
+def delays_study(reps=3):
+    """The 4000-neuron COBA network (1 s of model time) without delays, with
+    uniform delays (1.5 ms excitatory, 0.8 ms inhibitory) and with one delay
+    per synapse drawn from U{0.1..2.0 ms}: grid engine in float and double,
+    run time per step (device synchronised on both sides, CUDA graphs of 32
+    steps), delivered events per second, spike count against the oracle (the
+    double run must equal it bit for bit) and the oracle's own time on one
+    host core."""
+    import torch
+    from annarchy_b200 import workloads as wl
+    from oracle import oracle as O
+    cn = wl.coba_net()
+    rng = np.random.default_rng(7)
+    cases = [("none", (None, None)), ("uniform 1.5 / 0.8 ms", (15, 8)),
+             ("per synapse U{0.1..2 ms}", (rng.integers(1, 21, cn.w_exc.nnz),
+                                           rng.integers(1, 21, cn.w_inh.nnz)))]
+    out_deg = cn.out_degree()
+    rows = []
+    for name, d in cases:
+        t0 = time.perf_counter()
+        ref = O.coba_run(cn, O.coba_projections(cn, delays=d))
+        cpu_s = time.perf_counter() - t0
+        ref_events = int(out_deg[ref["spike_idx"]].sum())
+        for prec in ("float", "double"):
+            net, P, mon = wl.build_coba_network(cn, prec, engine="grid", delays=d)
+            net.compile()
+            res = time_graph_free(net, P, mon, cn, reps + 1)[1:]
+            ms = sorted(r[0] for r in res)[len(res) // 2]
+            events = res[-1][1]
+            reset_state(net, P, cn)
+            net.simulate_steps(MODEL_STEPS)
+            s, i = mon.spike_arrays()
+            mon.get("spike")
+            row = {"delays": name, "precision": prec, "engine": net.engine,
+                   "us_per_step": ms * 1e3 / MODEL_STEPS, "gsynops": events / (ms * 1e-3) / 1e9,
+                   "spikes": int(s.size), "oracle_spikes": int(ref["n_spikes"]),
+                   "rate_err": abs(s.size - ref["n_spikes"]) / max(1, ref["n_spikes"]),
+                   "oracle_us_per_step_1core": cpu_s * 1e6 / MODEL_STEPS,
+                   "oracle_gsynops_1core": ref_events / cpu_s / 1e9}
+            if prec == "double":
+                row["bit_exact"] = bool(np.array_equal(s, ref["spike_steps"]) and
+                                        np.array_equal(i, ref["spike_idx"]) and
+                                        np.array_equal(P.v, ref["v"]))
+            rows.append(row)
+            print(json.dumps(row), flush=True)
+            net.close()
+            torch.cuda.synchronize()
+    return rows
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -706,6 +756,8 @@ def main():
                          "sizes (comma separated, e.g. 64,128,256)")
     ap.add_argument("--batched-steps", type=int, default=5000,
                     help="time steps of the batched-instance study")
+    ap.add_argument("--delays", action="store_true",
+                    help="synaptic-delay study on the 4000-neuron network")
     ap.add_argument("--formats", default="",
                     help="storage-format study on these 100k structures (comma separated: "
                          "uniform,powerlaw,local,blocks)")
@@ -719,6 +771,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         spmm_study(tuple(int(b) for b in args.spmm.split(",")))
+        return
+    if args.delays:
+        import torch
+        torch.cuda.set_device(0)
+        delays_study()
         return
     if args.spmv:
         import torch
