@@ -20,7 +20,7 @@ from __future__ import annotations
 import numpy as np
 
 from ..generator import formats as F
-from ..generator.codegen import CodeGenerator, compensated_vars, grid_for
+from ..generator.codegen import CodeGenerator, compensated_vars, grid_for, trace_layout
 from ..runtime.lib import DryNative, NativeNet
 
 BF16 = np.uint16
@@ -66,6 +66,30 @@ class CompiledNetwork:
 
     def _dtype_of(self, pop, name):
         return np.int32 if pop._ctype.get(name) in ("int", "bool") else self.real
+
+    # ------------------------------------------------------- packed traces
+    def _trace_dtype(self, proj):
+        lay = trace_layout(proj, self.exact)
+        if lay is None:
+            return None
+        names, nbytes = lay
+        return np.dtype({"names": names + ["_last_event"],
+                         "formats": ["<f4"] * len(names) + ["<i4"],
+                         "offsets": [4 * i for i in range(len(names) + 1)], "itemsize": nbytes})
+
+    def _trace_init(self, proj, nnz, host=None):
+        """Records of the packed traces: the initial values (or `host` arrays)
+        and last event -10000, as uint32 words."""
+        dt = self._trace_dtype(proj)
+        rec = np.zeros(nnz if host is not None else 1, dtype=dt)
+        for n in dt.names[:-1]:
+            if host is not None and n in host:
+                rec[n] = host[n]
+            else:
+                init = next((v["init"] for v in proj.desc["variables"] if v["name"] == n), 0.0)
+                rec[n] = float(init) if not isinstance(init, str) else 0.0
+        rec["_last_event"] = -10000
+        return rec.view(np.uint32).reshape(-1)
 
     # ----------------------------------------------------------------- build
     def build(self):
@@ -377,10 +401,18 @@ class CompiledNetwork:
             lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
         if plastic:
             nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
-            for name in self._syn_local_names(proj):
-                nat.create_empty(f"proj{k}__{name}", self.real, (nnz,))
-            nat.create_empty(f"proj{k}___last_event", np.int64, (nnz,))
-            nat.fill(f"proj{k}___last_event", np.int64(-10000))
+            if self._trace_dtype(proj) is not None:
+                dt = self._trace_dtype(proj)
+                nat.create_empty(f"proj{k}__tr", np.uint32, (nnz * dt.itemsize // 4,))
+                nat.fill(f"proj{k}__tr", self._trace_init(proj, nnz))
+                # the generated weights into the records' first field
+                nat.copy_strided(f"proj{k}__tr", 0, dt.itemsize, f"proj{k}__w", 0, 4, nnz)
+                nat.free(f"proj{k}__w")
+            else:
+                for name in self._syn_local_names(proj):
+                    nat.create_empty(f"proj{k}__{name}", self.real, (nnz,))
+                nat.create_empty(f"proj{k}___last_event", np.int64, (nnz,))
+                nat.fill(f"proj{k}___last_event", np.int64(-10000))
         self.layout[k] = lay
 
     def _create_delays(self, proj):
@@ -490,12 +522,17 @@ class CompiledNetwork:
                 lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
             if proj.plastic:
                 nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
-                for name, arr in proj._host_attr.items():
-                    nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
-                if self.wdtype is not np.float64 and not self.exact:
-                    # plastic weights stay float32 (they are updated every event)
-                    nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
-                nat.create(f"proj{k}___last_event", np.full(nnz, -10000, dtype=np.int64))
+                if self._trace_dtype(proj) is not None:
+                    # w and the traces in one record per synapse (float32)
+                    nat.free(f"proj{k}__w")
+                    nat.create(f"proj{k}__tr", self._trace_init(proj, nnz, {**proj._host_attr, "w": w}))
+                else:
+                    if self.wdtype is not np.float64 and not self.exact:
+                        # plastic weights stay float32 (they are updated every event)
+                        nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
+                    for name, arr in proj._host_attr.items():
+                        nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
+                    nat.create(f"proj{k}___last_event", np.full(nnz, -10000, dtype=np.int64))
         self.layout[k] = lay
 
     def _rate_format(self, proj, lay) -> str:
@@ -648,6 +685,15 @@ class CompiledNetwork:
         """Synaptic variables (not the weights) back to their initial values."""
         nat = self.native
         k = proj.id
+        if f"proj{k}__tr" in nat.arrays:
+            # every field but the weights back to its initial value
+            dt = self._trace_dtype(proj)
+            init = self._trace_init(proj, 0).view(dt)[0]
+            st, nnz = self._stage(proj), self.layout[k]["nnz"]
+            for name in dt.names[1:]:
+                nat.fill(st, np.asarray(init[name]).view(np.uint32))
+                nat.copy_strided(f"proj{k}__tr", dt.fields[name][1], dt.itemsize, st, 0, 4, nnz)
+            return
         for v in proj.desc["variables"]:
             if v["name"] == "w":
                 continue
@@ -658,7 +704,30 @@ class CompiledNetwork:
         if f"proj{k}___last_event" in nat.arrays:
             nat.fill(f"proj{k}___last_event", np.int64(-10000))
 
+    def _stage(self, proj) -> str:
+        """A float32 array of the projection's size for packing and
+        unpacking one record field on the device."""
+        name = f"proj{proj.id}__stage"
+        if name not in self.native.arrays:
+            self.native.create_empty(name, np.float32, (self.layout[proj.id]["nnz"],))
+        return name
+
+    def _field_io(self, proj, name, arr=None):
+        """Read (arr None) or write one field of the packed records."""
+        dt = self._trace_dtype(proj)
+        k, nnz = proj.id, self.layout[proj.id]["nnz"]
+        off = dt.fields[name][1]
+        st = self._stage(proj)
+        if arr is None:
+            self.native.copy_strided(st, 0, 4, f"proj{k}__tr", off, dt.itemsize, nnz)
+            return self.native.read(st).astype(np.float64)
+        self.native.write(st, np.asarray(arr, dtype=dt.fields[name][0]).view(np.float32))
+        self.native.copy_strided(f"proj{k}__tr", off, dt.itemsize, st, 0, 4, nnz)
+
     def read_projection_attribute(self, proj, name):
+        dt = self._trace_dtype(proj)
+        if dt is not None and name in dt.names[:-1]:
+            return self._field_io(proj, name)
         arr = self.native.read(f"proj{proj.id}__{name}")
         if arr.dtype == np.uint16:
             return from_bf16(arr)
@@ -666,6 +735,10 @@ class CompiledNetwork:
 
     def write_projection_attribute(self, proj, name, arr):
         k = proj.id
+        tdt = self._trace_dtype(proj)
+        if tdt is not None and name in tdt.names[:-1]:
+            self._field_io(proj, name, arr)
+            return
         dtype, _ = self.native.arrays[f"proj{k}__{name}"]
         data = to_bf16(arr) if dtype == np.uint16 else np.asarray(arr, dtype=dtype)
         self.native.write(f"proj{k}__{name}", data)

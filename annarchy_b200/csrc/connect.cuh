@@ -125,15 +125,27 @@ __global__ void anb_scatter_cols(int n_rows, const int* __restrict__ row_ptr,
 }
 
 __global__ void anb_fill_kernel(unsigned char* __restrict__ dst, size_t bytes,
-                                const unsigned long long pattern, int pattern_bytes) {
+                                const unsigned long long pattern, const unsigned long long pattern_hi,
+                                int pattern_bytes) {
   const size_t n = bytes / pattern_bytes;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    if (pattern_bytes == 8) reinterpret_cast<unsigned long long*>(dst)[i] = pattern;
+    if (pattern_bytes == 16) reinterpret_cast<ulonglong2*>(dst)[i] = make_ulonglong2(pattern, pattern_hi);
+    else if (pattern_bytes == 8) reinterpret_cast<unsigned long long*>(dst)[i] = pattern;
     else if (pattern_bytes == 4) reinterpret_cast<unsigned int*>(dst)[i] = (unsigned int)pattern;
     else if (pattern_bytes == 2) reinterpret_cast<unsigned short*>(dst)[i] = (unsigned short)pattern;
     else dst[i] = (unsigned char)pattern;
   }
+}
+
+// dst[i * dst_stride + dst_off] = src[i * src_stride + src_off] for 4-byte
+// elements (strides and offsets in 4-byte words).
+__global__ void anb_copy_strided_kernel(unsigned* __restrict__ dst, long long dst_stride, long long dst_off,
+                                        const unsigned* __restrict__ src, long long src_stride,
+                                        long long src_off, long long count) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i * dst_stride + dst_off] = src[i * src_stride + src_off];
 }
 
 unsigned grid_of(long long n) {
@@ -147,20 +159,42 @@ extern "C" {
 
 int anb_array_fill(anb_net* net, const char* name, const void* value, size_t value_bytes) {
   if (!net || !value) return fail(ANB_ERR_ARG, "NULL argument");
-  if (value_bytes != 1 && value_bytes != 2 && value_bytes != 4 && value_bytes != 8)
-    return fail(ANB_ERR_ARG, "fill value must be 1, 2, 4 or 8 bytes");
+  if (value_bytes != 1 && value_bytes != 2 && value_bytes != 4 && value_bytes != 8 && value_bytes != 16)
+    return fail(ANB_ERR_ARG, "fill value must be 1, 2, 4, 8 or 16 bytes");
   Array* a = find(net, name);
   if (!a) return fail(ANB_ERR_ARG, std::string("unknown array ") + (name ? name : "(null)"));
   if (a->bytes % value_bytes) return fail(ANB_ERR_ARG, "array size is not a multiple of the value");
   int rc = ensure_device(net);
   if (rc) return rc;
-  unsigned long long pattern = 0;
-  std::memcpy(&pattern, value, value_bytes);
+  unsigned long long pattern[2] = {0, 0};
+  std::memcpy(pattern, value, value_bytes);
   if (a->bytes) {
     anb_fill_kernel<<<grid_of((long long)(a->bytes / value_bytes)), 256, 0, net->stream>>>(
-        (unsigned char*)a->ptr, a->bytes, pattern, (int)value_bytes);
+        (unsigned char*)a->ptr, a->bytes, pattern[0], pattern[1], (int)value_bytes);
     ANB_CUDA(cudaGetLastError());
   }
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  return ANB_OK;
+}
+
+int anb_array_copy_strided(anb_net* net, const char* dst, size_t dst_offset, size_t dst_stride,
+                           const char* src, size_t src_offset, size_t src_stride, size_t count) {
+  if (!net || !dst || !src) return fail(ANB_ERR_ARG, "NULL argument");
+  Array* d = find(net, dst);
+  Array* a = find(net, src);
+  if (!d || !a) return fail(ANB_ERR_ARG, "unknown array");
+  if ((dst_offset | dst_stride | src_offset | src_stride) % 4 || dst_stride == 0 || src_stride == 0)
+    return fail(ANB_ERR_ARG, "offsets and strides must be multiples of 4 bytes");
+  if (count == 0) return ANB_OK;
+  if (dst_offset + (count - 1) * dst_stride + 4 > d->bytes ||
+      src_offset + (count - 1) * src_stride + 4 > a->bytes)
+    return fail(ANB_ERR_ARG, "strided copy outside an array");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  anb_copy_strided_kernel<<<grid_of((long long)count), 256, 0, net->stream>>>(
+      (unsigned*)d->ptr, (long long)(dst_stride / 4), (long long)(dst_offset / 4), (const unsigned*)a->ptr,
+      (long long)(src_stride / 4), (long long)(src_offset / 4), (long long)count);
+  ANB_CUDA(cudaGetLastError());
   ANB_CUDA(cudaStreamSynchronize(net->stream));
   return ANB_OK;
 }

@@ -106,6 +106,7 @@ struct Launch {
   CUfunction fn = nullptr;
   unsigned grid = 1, block = 1, smem = 0;
   unsigned cluster = 1;  // CTAs per thread-block cluster (launch attribute)
+  int group = 0;         // consecutive launches of one nonzero group may run concurrently
 };
 
 struct TimedLaunch {
@@ -141,6 +142,10 @@ struct anb_net {
   std::map<std::string, int> time_index;
   void* flush_buf = nullptr;
   size_t flush_bytes = 0;
+  // side streams and fork/join events of concurrent plan groups
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
   // device scratch of anb_monitor_decode (grown on demand)
   long long* dec_rows = nullptr;
   int64_t dec_rows_cap = 0;
@@ -188,10 +193,10 @@ int bind(anb_net* net) {
   return ANB_OK;
 }
 
-int launch(anb_net* net, const Launch& l, void** params) {
+int launch(anb_net* net, const Launch& l, void** params, cudaStream_t on = nullptr) {
   if (l.cluster <= 1) {
-    ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem, (CUstream)net->stream,
-                              params, nullptr));
+    ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem,
+                              (CUstream)(on ? on : net->stream), params, nullptr));
     return ANB_OK;
   }
   CUlaunchAttribute attr;
@@ -251,10 +256,52 @@ int collect_times(anb_net* net) {
   return ANB_OK;
 }
 
+// k - 1 side streams and their join events (created once per network)
+int ensure_side(anb_net* net, size_t k) {
+  if (!net->fork_ev) ANB_CUDA(cudaEventCreateWithFlags(&net->fork_ev, cudaEventDisableTiming));
+  while (net->side.size() < k) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    ANB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    ANB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    net->side.push_back(st);
+    net->side_ev.push_back(ev);
+  }
+  return ANB_OK;
+}
+
+// One step of the plan. A run of consecutive launches sharing a nonzero
+// group forks from the network's stream: the first stays on it, the others
+// go to side streams that wait for the fork event, and the network's stream
+// waits for all of them before the next launch (captured as parallel
+// branches when a graph is recorded). Timed runs stay sequential.
 int run_plan_once(anb_net* net) {
-  for (auto& l : net->plan) {
-    int rc = net->timing ? timed_launch(net, l, nullptr) : launch(net, l, nullptr);
+  const size_t n = net->plan.size();
+  for (size_t i = 0; i < n;) {
+    const Launch& l = net->plan[i];
+    size_t j = i + 1;
+    if (l.group != 0 && !net->timing)
+      while (j < n && net->plan[j].group == l.group) ++j;
+    if (j - i == 1) {
+      int rc = net->timing ? timed_launch(net, l, nullptr) : launch(net, l, nullptr);
+      if (rc != ANB_OK) return rc;
+      i = j;
+      continue;
+    }
+    int rc = ensure_side(net, j - i - 1);
     if (rc != ANB_OK) return rc;
+    ANB_CUDA(cudaEventRecord(net->fork_ev, net->stream));
+    for (size_t q = i + 1; q < j; ++q) {
+      cudaStream_t st = net->side[q - i - 1];
+      ANB_CUDA(cudaStreamWaitEvent(st, net->fork_ev, 0));
+      rc = launch(net, net->plan[q], nullptr, st);
+      if (rc != ANB_OK) return rc;
+      ANB_CUDA(cudaEventRecord(net->side_ev[q - i - 1], st));
+    }
+    rc = launch(net, l, nullptr);
+    if (rc != ANB_OK) return rc;
+    for (size_t q = i + 1; q < j; ++q) ANB_CUDA(cudaStreamWaitEvent(net->stream, net->side_ev[q - i - 1], 0));
+    i = j;
   }
   return ANB_OK;
 }
@@ -366,6 +413,9 @@ int anb_destroy(anb_net* net) {
     cudaEventDestroy(tl.stop);
   }
   drop_graph(net);
+  for (auto st : net->side) cudaStreamDestroy(st);
+  for (auto ev : net->side_ev) cudaEventDestroy(ev);
+  if (net->fork_ev) cudaEventDestroy(net->fork_ev);
   if (net->flush_buf) cudaFree(net->flush_buf);
   if (net->dec_rows) cudaFree(net->dec_rows);
   if (net->dec_out) cudaFree(net->dec_out);
@@ -803,9 +853,16 @@ static int resolve(anb_net* net, const char* kernel, unsigned grid, unsigned blo
 
 int anb_plan_add(anb_net* net, const char* kernel, unsigned grid, unsigned block,
                  unsigned shared_bytes) {
+  return anb_plan_add_concurrent(net, kernel, grid, block, shared_bytes, 0);
+}
+
+int anb_plan_add_concurrent(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                            unsigned shared_bytes, int group) {
   Launch l;
   int rc = resolve(net, kernel, grid, block, shared_bytes, &l);
   if (rc) return rc;
+  if (group < 0) return fail(ANB_ERR_ARG, "group must be >= 0");
+  l.group = group;
   drop_graph(net);
   net->plan.push_back(l);
   return ANB_OK;

@@ -55,7 +55,8 @@ def compensated_vars(pop, exact: bool, config: dict) -> list:
     """ODE variables whose explicit-Euler switch is Kahan-compensated
     (single precision only): the rounding error of every `x += dt*_x` is
     carried in anb_kc_x and added back at the next step. config
-    "compensate": True (every local ODE variable), False, or a list of
+    "compensate": True (every local ODE variable), False, "auto" (all but the
+    conductances g_*, whose increments only decay them) or a list of
     variable names."""
     comp = config.get("compensate", True)
     if exact or not comp:
@@ -63,7 +64,27 @@ def compensated_vars(pop, exact: bool, config: dict) -> list:
     names = [v["name"] for v in pop.desc["variables"]
              if v.get("switch") and v.get("method") != "event-driven"
              and v["name"] in pop.desc["local"]]
+    if comp == "auto":
+        return [n for n in names if not n.startswith("g_")]
     return names if comp is True else [n for n in names if n in comp]
+
+
+def trace_layout(proj, exact: bool):
+    """Fast-mode plastic spiking projections keep their per-synapse state
+    (w, the other local variables, the last event step) packed in one record
+    per synapse, so a synapse reached through the inverse index costs one
+    scattered sector instead of one per variable. Returns (field names,
+    record bytes) or None when the variables stay separate arrays."""
+    if exact or not proj.plastic or proj.synapse_type.type != "spike":
+        return None
+    names = ["w"] + [v["name"] for v in proj.desc["variables"]
+                     if v["locality"] == "local" and v["name"] != "w"]
+    for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
+        if v["name"] not in names and v["name"] not in ("w", "g_target"):
+            names.append(v["name"])
+    nbytes = 4 * (len(names) + 1)
+    nbytes = 8 if nbytes <= 8 else -(-nbytes // 16) * 16
+    return names, nbytes
 
 
 def grid_for(n: int, block: int = BLOCK) -> int:
@@ -93,6 +114,7 @@ class CodeGenerator:
         self.exact = compiled.exact
         self.real = "double" if self.exact else "float"
         self.decls: dict[str, str] = {}
+        self.types: dict[str, str] = {}
 
     # ------------------------------------------------------------------ utils
     def ptr(self, name: str) -> str:
@@ -117,6 +139,18 @@ class CodeGenerator:
     def delayed(self, proj) -> bool:
         """The projection reads its pre-synaptic output through a delay ring."""
         return proj.max_delay > 1
+
+    def atomic_psp(self, proj) -> bool:
+        """The projection's transmission kernel only adds into g with atomics
+        (and touches its own synapses): fast mode, spike lists or the bitmap
+        scatter; not the warp-per-row gathers."""
+        if self.exact or proj.synapse_type.type != "spike":
+            return False
+        if proj._delay_steps is not None:
+            return False
+        if proj.plastic:
+            return self.c.spike_lists and not self.delayed(proj)
+        return True
 
     def pre_spk(self, proj) -> str:
         if self.delayed(proj) and proj._delay_steps is None:
@@ -288,7 +322,12 @@ class CodeGenerator:
         masked = spiking and pop._has_refractory
         body, modified = self._neuron_body(pop, None, masked)
         body = self._use_reciprocals(pop, body)
-        names = self._locals(pop)
+        # only the local attributes the update reads or writes are loaded
+        used = body
+        if spiking:
+            used += " " + pop.desc["spike"]["spike_cond"] + " " + " ".join(
+                r["cpp"] for r in pop.desc["spike"]["spike_reset"])
+        names = [n for n in self._locals(pop) if re.search(rf"\b{re.escape(n)}\b", used)]
         k = pop.id
 
         if gsrc is None:
@@ -629,7 +668,33 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
                 out.append(f"const {self.real} {prm['name']} = {self.ptr(f'proj{proj.id}__{prm['name']}')}[0];")
         return "\n    ".join(out)
 
+    def _packed(self, proj):
+        return trace_layout(proj, self.exact)
+
+    def _pack_body(self, proj, body: str, idx: str = "j") -> str:
+        """Per-synapse statements on the packed record: load it once, use
+        its fields, store it back."""
+        lay = self._packed(proj)
+        if lay is None:
+            return body
+        names, _ = lay
+        body = body.replace(f"_last_event[{idx}] = t;", "anb_s._last_event = (int)t;")
+        for n in names + ["_last_event"]:
+            body = re.sub(rf"\b{re.escape(n)}\[{idx}\]", f"anb_s.{n}", body)
+        return (f"anb_tr{proj.id} anb_s = anb_tr[{idx}];\n          {body}\n"
+                f"          anb_tr[{idx}] = anb_s;")
+
     def _syn_arrays(self, proj):
+        lay = self._packed(proj)
+        if lay is not None:
+            names, nbytes = lay
+            fields = " ".join(f"float {n};" for n in names) + " int _last_event;"
+            pad = nbytes // 4 - len(names) - 1
+            fields += "".join(f" int anb_pad{i};" for i in range(pad))
+            self.types[f"anb_tr{proj.id}"] = (f"struct __align__({min(nbytes, 16)}) anb_tr{proj.id} "
+                                              f"{{ {fields} }};\n")
+            return (f"anb_tr{proj.id}* __restrict__ anb_tr = "
+                    f"reinterpret_cast<anb_tr{proj.id}*>({self.ptr(f'proj{proj.id}__tr')});")
         names = ["w"] + [v["name"] for v in proj.desc["variables"]
                          if v["locality"] == "local" and v["name"] != "w"]
         for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
@@ -659,7 +724,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
             if v["name"] == "w" and proj.desc["plasticity"]:
                 code = f"if (anb_plastic) {{ {code} }}"
             stmts.append(self.typed(code))
-        body = "\n          ".join(stmts)
+        body = self._pack_body(proj, "\n          ".join(stmts))
         if self.exact or self.delayed(proj) or not self.c.spike_lists:
             # warp per post row; the spiking synapses of a row are processed in
             # ascending pre rank, one at a time, by the lane that holds them
@@ -740,7 +805,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
             if v["name"] == "w":
                 code = f"if (anb_plastic) {{ {code} }}"
             stmts.append(self.typed(code))
-        body = "\n        ".join(stmts)
+        body = self._pack_body(proj, "\n        ".join(stmts))
         dt_t = "double" if self.exact else "float"
         if not self.exact and self.c.spike_lists:
             b = proj.post_pop.id
@@ -826,7 +891,10 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
                 plan.extend(launches)
             else:
                 kernels.append(self.spike_kernel(proj))
-                plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0))
+                # fast transmissions that add with atomics run concurrently
+                # (one graph branch each); the gathers write g[post] in place
+                group = 1 if self.atomic_psp(proj) else 0
+                plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0, group))
         for pop in net.populations:
             if self.has_update(pop):
                 kernels.append(self.pop_kernel(pop))
@@ -864,7 +932,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
       }}
     }}
 """
-        if not plan or [p[0] for p in plan].count(plan[-1][0]) > 1:
+        if not plan or [p[0] for p in plan].count(plan[-1][0]) > 1 or (len(plan[-1]) > 4 and plan[-1][4]):
             kernels.append("""
 extern "C" __global__ void anb_tick() {
 }
@@ -1260,5 +1328,6 @@ anb_cluster_run(long long t0, int nsteps) {{
         self.ptr("dt")
         self.ptr("err")
         decl = "\n".join(f"__constant__ {ct}* anb_p_{name};" for name, ct in sorted(self.decls.items()))
+        types = "".join(self.types[k] for k in sorted(self.types))
         return (f"// generated by annarchy_b200 for network {self.net.id}\n{header}\n"
-                f"typedef {self.real} real;\n{decl}\n" + "".join(kernels))
+                f"typedef {self.real} real;\n{types}{decl}\n" + "".join(kernels))

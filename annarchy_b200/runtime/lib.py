@@ -48,6 +48,9 @@ SIGNATURES = {
     "anb_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "anb_bsr_tc_pack_x": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "anb_bsr_spmm_tc_shape": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "anb_array_copy_strided": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_size_t, C.c_char_p,
+                                         C.c_size_t, C.c_size_t, C.c_size_t]),
+    "anb_plan_add_concurrent": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint, C.c_int]),
     "anb_bsr_spmm_tc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                   C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "anb_bsr_spmm_simt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
@@ -276,6 +279,12 @@ class NativeNet:
         check("anb_array_free", self.lib.anb_array_free(self.h, name.encode()))
         self.arrays.pop(name, None)
 
+    def copy_strided(self, dst, dst_offset, dst_stride, src, src_offset, src_stride, count):
+        """Device copy of `count` 4-byte elements between arrays (byte offsets
+        and strides)."""
+        check("anb_array_copy_strided", self.lib.anb_array_copy_strided(
+            self.h, dst.encode(), dst_offset, dst_stride, src.encode(), src_offset, src_stride, count))
+
     def fill(self, name: str, value):
         v = np.asarray(value)
         check("anb_array_fill", self.lib.anb_array_fill(self.h, name.encode(),
@@ -310,9 +319,13 @@ class NativeNet:
                                                          "\n".join(options).encode()))
 
     def plan(self, launches):
+        """launches: (kernel, grid, block, shared bytes[, concurrency group])."""
         check("anb_plan_clear", self.lib.anb_plan_clear(self.h))
-        for name, grid, block, smem in launches:
-            check("anb_plan_add", self.lib.anb_plan_add(self.h, name.encode(), grid, block, smem))
+        for entry in launches:
+            name, grid, block, smem = entry[:4]
+            group = entry[4] if len(entry) > 4 else 0
+            check("anb_plan_add_concurrent", self.lib.anb_plan_add_concurrent(
+                self.h, name.encode(), grid, block, smem, group))
 
     def set_local_kernel(self, name, grid, block, smem, cluster: int = 1):
         if cluster > 1:
@@ -381,6 +394,12 @@ class DryNative:
         pass
 
     def fill(self, name, value):
+        pass
+
+    def free(self, name):
+        self.arrays.pop(name, None)
+
+    def copy_strided(self, *a):
         pass
 
     def connect_fixed_number_pre(self, prefix, n_post, post_base, pre_lo, pre_hi, number, seed,

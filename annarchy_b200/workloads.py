@@ -418,6 +418,8 @@ def build_large_network(ln: LargeNet, precision: str = "double", stdp: bool = Tr
     the device at compile()."""
     from . import STDP, Network, Uniform
     net = Network(dt=ln.dt, seed=ln.seed)
+    # float: Kahan compensation of v only (the conductances only decay)
+    config.setdefault("compensate", "auto")
     net.config(precision=precision, engine="grid", device_connectors=True, **config)
     params = dict(COBA_PARAMS)
     params["I"] = float(ln.drive)

@@ -98,8 +98,16 @@ int anb_array_read(anb_net* net, const char* name, size_t offset, void* dst, siz
 int anb_array_fill_zero(anb_net* net, const char* name);
 int anb_array_info(anb_net* net, const char* name, void** device_ptr, size_t* bytes);
 
-/* Fill an array with a repeated 1-, 2-, 4- or 8-byte value. */
+/* Fill an array with a repeated 1-, 2-, 4-, 8- or 16-byte value. */
 int anb_array_fill(anb_net* net, const char* name, const void* value, size_t value_bytes);
+
+/* Strided copy of `count` 4-byte elements between two arrays on the device:
+ * element i goes from byte src_offset + i * src_stride of `src` to byte
+ * dst_offset + i * dst_stride of `dst` (offsets and strides multiples of 4;
+ * bounds checked). Packs and unpacks one field of per-synapse records. No
+ * counterpart in the reference. */
+int anb_array_copy_strided(anb_net* net, const char* dst, size_t dst_offset, size_t dst_stride,
+                           const char* src, size_t src_offset, size_t src_stride, size_t count);
 
 /* ---- device-side connectivity -------------------------------------------
  * Replaces the host construction of a fixed_number_pre projection
@@ -141,6 +149,14 @@ int anb_nvrtc_compile(const char* source, const char* options, char* log, size_t
 int anb_plan_clear(anb_net* net);
 int anb_plan_add(anb_net* net, const char* kernel, unsigned grid, unsigned block,
                  unsigned shared_bytes);
+/* As anb_plan_add; consecutive plan entries with the same nonzero `group`
+ * may run concurrently (forked onto side streams, joined before the next
+ * entry; parallel branches of the step's CUDA graph). For kernels that only
+ * touch disjoint data or combine their results with atomics (the reference
+ * runs its projections one after another, ANNarchy/generator/Template/
+ * OpenMPBaseTemplate.py:225-232). */
+int anb_plan_add_concurrent(anb_net* net, const char* kernel, unsigned grid, unsigned block,
+                            unsigned shared_bytes, int group);
 
 /* Local engine: one kernel `kernel(long long t0, int nsteps)` that runs
  * nsteps steps per launch (grid CTAs, each owning whole network instances). */
