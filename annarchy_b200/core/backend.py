@@ -96,6 +96,13 @@ class CompiledNetwork:
         net = self.net
         nat = self.native
         nat.initialize(net.dt)
+        # key of the random draws in equations (drawn from the network's seed,
+        # only when some equation draws)
+        if any(p.desc.get("random_distributions") for p in net.populations):
+            key = net._rng.integers(0, 2**32, 2, dtype=np.uint64).astype(np.uint32)
+        else:
+            key = np.zeros(2, dtype=np.uint32)
+        nat.create("rng_seed", key)
         # history kept per population: its outgoing projections' largest delay
         for pop in net.populations:
             self.slots[pop.id] = max([1] + [int(p.max_delay) for p in net.projections

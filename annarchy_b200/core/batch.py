@@ -168,6 +168,9 @@ class Batch:
         for m in self.net.monitors:
             if any(v != "spike" for v in m.variables):
                 raise NotImplementedError("batched monitors record spikes only")
+        for p in self.net.populations:
+            if p.desc.get("random_distributions"):
+                raise NotImplementedError("batched instances draw no random numbers in equations")
 
     # -------------------------------------------------------------- layout
     def _smem_arrays(self, pop):

@@ -66,10 +66,24 @@ class Network:
             self._config[key] = val
         return self
 
-    def create(self, geometry, neuron, name: str | None = None, **kw) -> Population:
+    def create(self, geometry, neuron=None, name: str | None = None, **kw) -> Population:
+        """A population of `neuron`, or (as the reference's
+        net.create(PoissonPopulation(...))) a population object built outside
+        the network, which then joins it."""
         if self._compiled:
             raise RuntimeError("the network is already compiled")
-        pop = Population(geometry, neuron, name=name, net=self, pop_id=len(self.populations))
+        if isinstance(geometry, Population):
+            pop = geometry
+            if pop.net is not None and pop.net is not self:
+                raise ValueError("the population belongs to another network")
+            object.__setattr__(pop, "net", self)
+            object.__setattr__(pop, "id", len(self.populations))
+            if name is not None or pop.__dict__.get("_auto_name", False):
+                object.__setattr__(pop, "name", name or f"pop{pop.id}")
+        else:
+            if neuron is None:
+                raise TypeError("create() needs a neuron type")
+            pop = Population(geometry, neuron, name=name, net=self, pop_id=len(self.populations))
         self.populations.append(pop)
         return pop
 

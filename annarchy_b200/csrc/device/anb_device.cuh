@@ -21,6 +21,9 @@ typedef long long anb_i64;
 #define ANB_WARP 32
 
 // Error codes a kernel writes into the network's error word.
+#ifndef M_PI
+#define M_PI 3.14159265358979323846   // pi in equations (the reference's sympy output)
+#endif
 #define ANB_DEVERR_BARRIER_TIMEOUT 1
 #define ANB_DEVERR_INDEX 2
 #define ANB_DEVERR_MONITOR_OVERFLOW 3
@@ -73,6 +76,85 @@ __device__ __forceinline__ void anb_rate_csr_scalar(int n_rows, const I* __restr
     const int post = post_rank ? post_rank[row] : row;
     sum[post] += s;
   }
+}
+
+// ---- random numbers in equations --------------------------------------------------------
+// Counter-based generator Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror,
+// D. E. Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11): ten
+// rounds of two 32x32->64 multiplications with the published multipliers
+// and Weyl key increments. A draw is a pure function of (seed, stream,
+// step, neuron), so no generator state is stored or advanced, and every
+// neuron of every step draws independently in any launch order.
+struct anb_u4 {
+  unsigned x, y, z, w;
+};
+
+__device__ __forceinline__ anb_u4 anb_philox4x32_10(anb_u4 c, unsigned k0, unsigned k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned long long p0 = (unsigned long long)0xD2511F53u * c.x;
+    const unsigned long long p1 = (unsigned long long)0xCD9E8D57u * c.z;
+    const unsigned hi0 = (unsigned)(p0 >> 32), lo0 = (unsigned)p0;
+    const unsigned hi1 = (unsigned)(p1 >> 32), lo1 = (unsigned)p1;
+    c = anb_u4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// The four 32-bit words of draw (seed, stream, step t, index i).
+__device__ __forceinline__ anb_u4 anb_rand_words(const unsigned* seed, unsigned stream, long long t,
+                                                 unsigned i) {
+  return anb_philox4x32_10(anb_u4{i, (unsigned)t, (unsigned)((unsigned long long)t >> 32), stream},
+                           seed[0], seed[1]);
+}
+
+// Uniform on [0, 1): 24 bits (float) or 53 bits (double) of the first words.
+template <typename R>
+__device__ __forceinline__ R anb_unit(const anb_u4& w);
+template <>
+__device__ __forceinline__ float anb_unit<float>(const anb_u4& w) {
+  return (float)(w.x >> 8) * (1.0f / 16777216.0f);
+}
+template <>
+__device__ __forceinline__ double anb_unit<double>(const anb_u4& w) {
+  return (double)(((unsigned long long)(w.x >> 6) << 27) | (w.y >> 5)) * (1.0 / 9007199254740992.0);
+}
+
+// Standard normal by the Box-Muller transform of two uniforms (the second
+// pair of words); u1 in (0, 1] keeps the logarithm finite.
+template <typename R>
+__device__ __forceinline__ R anb_std_normal(const anb_u4& w) {
+  const anb_u4 v{w.z, w.w, w.x, w.y};
+  const R u1 = R(1) - anb_unit<R>(w), u2 = anb_unit<R>(v);
+  return sqrt(R(-2) * log(u1)) * cos(R(6.283185307179586) * u2);
+}
+
+template <typename R>
+__device__ __forceinline__ R anb_draw_uniform(const unsigned* seed, unsigned stream, long long t,
+                                              unsigned i, R lo, R hi) {
+  return lo + (hi - lo) * anb_unit<R>(anb_rand_words(seed, stream, t, i));
+}
+template <typename R>
+__device__ __forceinline__ R anb_draw_normal(const unsigned* seed, unsigned stream, long long t,
+                                             unsigned i, R mu, R sigma) {
+  return mu + sigma * anb_std_normal<R>(anb_rand_words(seed, stream, t, i));
+}
+template <typename R>
+__device__ __forceinline__ R anb_draw_lognormal(const unsigned* seed, unsigned stream, long long t,
+                                                unsigned i, R mu, R sigma) {
+  return exp(mu + sigma * anb_std_normal<R>(anb_rand_words(seed, stream, t, i)));
+}
+template <typename R>
+__device__ __forceinline__ R anb_draw_exponential(const unsigned* seed, unsigned stream, long long t,
+                                                  unsigned i, R lambda) {
+  return -log(R(1) - anb_unit<R>(anb_rand_words(seed, stream, t, i))) / lambda;
+}
+template <typename R>
+__device__ __forceinline__ R anb_draw_discrete_uniform(const unsigned* seed, unsigned stream, long long t,
+                                                       unsigned i, R lo, R hi) {
+  return lo + floor(anb_unit<R>(anb_rand_words(seed, stream, t, i)) * (hi - lo + R(1)));
 }
 
 // Slot of time step s (possibly negative) in a ring of `slots` entries.

@@ -272,6 +272,23 @@ class CodeGenerator:
                 out.append(self.typed(f"const double {pl['name']} = {self.fill(pl['value'])};"))
         return "\n    ".join(out)
 
+    _DRAW_FN = {"Uniform": "anb_draw_uniform", "Normal": "anb_draw_normal",
+                "LogNormal": "anb_draw_lognormal", "Exponential": "anb_draw_exponential",
+                "DiscreteUniform": "anb_draw_discrete_uniform"}
+
+    def _random_draws(self, pop) -> str:
+        """This step's draws of the random distributions in the neuron's
+        equations: Philox4x32-10 keyed by the network's seed, counter (neuron,
+        step, population and distribution); one draw per neuron, or one per
+        population (same counter in every thread) for a global variable."""
+        out = []
+        for k, rd in enumerate(pop.desc.get("random_distributions", [])):
+            idx = "(unsigned)anb_i" if rd["locality"] == "local" else "0xFFFFFFFFu"
+            args = ", ".join(f"({self.real})({self.typed(a)})" for a in rd["args"])
+            out.append(f"const {self.real} {rd['name']} = {self._DRAW_FN[rd['dist']]}<{self.real}>("
+                       f"{self.ptr('rng_seed')}, {(pop.id << 8) | k}u, t, {idx}, {args});")
+        return "\n".join(out)
+
     def _locals(self, pop):
         return [p["name"] for p in pop.desc["parameters"] + pop.desc["variables"]
                 if p["locality"] == "local"]
@@ -322,6 +339,9 @@ class CodeGenerator:
         masked = spiking and pop._has_refractory
         body, modified = self._neuron_body(pop, None, masked)
         body = self._use_reciprocals(pop, body)
+        draws = self._random_draws(pop)
+        if draws:
+            body = draws + "\n" + body
         # only the local attributes the update reads or writes are loaded
         used = body
         if spiking:

@@ -8,9 +8,14 @@ The description has the same keys as the reference's
 ``pre_spike``/``post_spike``/``psp``. C strings keep the reference's index
 placeholders (``%(local_index)s`` ...); the code generator fills them.
 
+Random distributions inside neuron equations (``p = Uniform(0.0, 1.0)``)
+become per-step draws ``rand_<k>`` listed in ``random_distributions``, as the
+reference's parser extracts them (ANNarchy/parser/Extraction.py,
+extract_randomdist); the code generator draws them on the device.
+
 Not supported by this backend (an error names them): if-then-else
 statements, global operations (``mean(r)``...), random distributions inside
-equations, user functions, coupled implicit/midpoint/rk4 systems.
+synapse equations, user functions, coupled implicit/midpoint/rk4 systems.
 """
 from __future__ import annotations
 
@@ -150,6 +155,31 @@ def _targets(variables):
     return sorted(set(found))
 
 
+RANDOM_DISTRIBUTIONS = {"Uniform": 2, "Normal": 2, "LogNormal": 2, "Exponential": 1,
+                        "DiscreteUniform": 2}
+_RANDOM_RE = re.compile(r"\b(Uniform|Normal|LogNormal|Exponential|DiscreteUniform|Gamma|Binomial)"
+                        r"\(([^()]*)\)")
+
+
+def _extract_random(eq, var, found, untouched):
+    """Replace every random distribution of `eq` by a placeholder of a
+    per-step draw rand_<k> (one draw per neuron, or per population for a
+    global variable) recorded in `found`."""
+    def repl(m):
+        dist, args = m.group(1), [a.strip() for a in m.group(2).split(",") if a.strip()]
+        if dist not in RANDOM_DISTRIBUTIONS:
+            raise ParserError(f"{var['name']}: the {dist} distribution is not supported in equations "
+                              "by this backend")
+        if len(args) != RANDOM_DISTRIBUTIONS[dist]:
+            raise ParserError(f"{var['name']}: {dist} takes {RANDOM_DISTRIBUTIONS[dist]} arguments")
+        k = len(found)
+        found.append({"name": f"rand_{k}", "dist": dist, "args": args,
+                      "locality": var.get("locality", "local")})
+        untouched[f"__rand_{k}__"] = f"rand_{k}"
+        return f" __rand_{k}__ "
+    return _RANDOM_RE.sub(repl, eq)
+
+
 def _unsupported(eq, where):
     if re.search(r"\bite\(|\bif\b.*\belse\b", eq):
         raise ParserError(f"{where}: if-then-else statements are not supported by this backend")
@@ -210,12 +240,15 @@ def analyse_neuron(neuron) -> dict:
                 desc["attributes"].append("g_" + t)
                 desc["local"].append("g_" + t)
         desc["spike"] = _spike(desc)
+    randoms = []
+    desc["random_distributions"] = randoms
     for var in variables:
         eq = var.get("transformed_eq", var["eq"])
         if eq.strip() == "":
             continue
-        _unsupported(eq, var["name"])
         untouched = {}
+        eq = _extract_random(eq, var, randoms, untouched)
+        _unsupported(eq, var["name"])
         for t in targets:
             eq = re.sub(r"(?P<pre>[^\w.])sum\(\)", r"\1sum(__all__)", eq)
             eq = re.sub(r"sum\(\s*" + t + r"\s*\)", "__sum_" + t + "__", eq)

@@ -1,0 +1,132 @@
+"""Random distributions in neuron equations and PoissonPopulation
+(ANNarchy/inputs/PoissonPopulation.py). The device's Philox4x32-10 draws are
+pinned against the generator's published known-answer vectors and a host
+restatement (bit for bit); the Poisson statistics against their binomial
+expectations."""
+import numpy as np
+import pytest
+
+import annarchy_b200 as ann
+from annarchy_b200.parser.text import ParserError
+from oracle import philox
+
+
+# ---------------------------------------------------------------- host
+def test_philox_known_answers():
+    """Published known-answer vectors of Philox4x32-10 (Salmon et al., SC'11)."""
+    def hexs(v):
+        return [format(int(x), "08x") for x in v]
+    assert hexs(philox.philox4x32_10(0, 0, 0, 0, 0, 0)) == ["6627e8d5", "e169c58d", "bc57ac4c", "9b00dbd8"]
+    f = 0xFFFFFFFF
+    assert hexs(philox.philox4x32_10(f, f, f, f, f, f)) == ["408f276d", "41c83b0e", "a20bc7c6", "6d5451fd"]
+    assert hexs(philox.philox4x32_10(0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344,
+                                     0xA4093822, 0x299F31D0)) == ["d16cfe09", "94fdcceb", "5001e420",
+                                                                  "24126ea1"]
+
+
+def test_random_distributions_extracted():
+    n = ann.Neuron(parameters="sigma = 2.0",
+                   equations="p = Uniform(0.0, 1.0) * 1000.0 / dt\nq = Normal(0.0, sigma) + Exponential(2.0)",
+                   spike="p < 1.0")
+    rd = n.desc["random_distributions"]
+    assert [(r["name"], r["dist"], r["args"]) for r in rd] == [
+        ("rand_0", "Uniform", ["0.0", "1.0"]), ("rand_1", "Normal", ["0.0", "sigma"]),
+        ("rand_2", "Exponential", ["2.0"])]
+    p = next(v for v in n.desc["variables"] if v["name"] == "p")
+    assert "rand_0" in p["cpp"]
+    with pytest.raises(ParserError):
+        ann.Neuron(equations="r = Gamma(1.0, 2.0)").desc
+    with pytest.raises(ParserError):
+        ann.Neuron(equations="r = Uniform(1.0)").desc
+
+
+def test_poisson_population_forms():
+    net = ann.Network(dt=0.1, seed=1)
+    a = net.create(ann.PoissonPopulation(100, rates=20.0))
+    b = net.create(ann.PoissonPopulation((10, 10), rates=np.arange(100.0)))
+    c = net.create(ann.PoissonPopulation(5, rates="amp * (1.0 + sin(2*pi*t/1000.0))/2.0",
+                                         parameters={"amp": 50.0}))
+    assert (a.name, b.name, c.name) == ("pop0", "pop1", "pop2")
+    assert a.rates[0] == 20.0 and b.rates[3, 4] == 34.0
+    assert c.neuron_type.type == "spike"
+    with pytest.raises(ValueError):
+        ann.PoissonPopulation(10)
+    with pytest.raises(NotImplementedError):
+        ann.PoissonPopulation(10, target="exc")
+
+
+# ---------------------------------------------------------------- GPU
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["double", "float"])
+def test_device_draws_match_host_philox(precision):
+    """r = Uniform(0, 1) drawn on the device equals the host restatement bit
+    for bit at every step checked; a normal draw agrees to rounding."""
+    net = ann.Network(dt=1.0, seed=5)
+    net.config(precision=precision)
+    pop = net.create(1000, ann.Neuron(equations="r = Uniform(0.0, 1.0)\nz = Normal(1.0, 2.0)"))
+    net.compile()
+    seed = net._backend.native.read("rng_seed")
+    for t in range(3):
+        net.step()
+        want = philox.uniform(seed, (pop.id << 8) | 0, t, np.arange(1000), precision == "double")
+        assert np.array_equal(pop.r.astype(want.dtype), want)
+        w = philox.words(seed, (pop.id << 8) | 1, t, np.arange(1000))
+        u1 = 1.0 - philox.uniform(seed, (pop.id << 8) | 1, t, np.arange(1000), True)
+        v = [w[2], w[3], w[0], w[1]]
+        hi = (v[0] >> np.uint32(6)).astype(np.uint64) << np.uint64(27)
+        u2 = (hi | (v[1] >> np.uint32(5)).astype(np.uint64)).astype(np.float64) / 9007199254740992.0
+        if precision == "float":
+            u1 = 1.0 - philox.uniform(seed, (pop.id << 8) | 1, t, np.arange(1000), False).astype(np.float64)
+            u2 = (v[0] >> np.uint32(8)).astype(np.float64) / 16777216.0
+        z = 1.0 + 2.0 * np.sqrt(-2.0 * np.log(u1)) * np.cos(2 * np.pi * u2)
+        np.testing.assert_allclose(pop.z, z, rtol=1e-4 if precision == "float" else 1e-12, atol=1e-5)
+    net.close()
+
+
+def _poisson_run(engine="auto", seed=11, steps=10000, precision="float"):
+    net = ann.Network(dt=0.1, seed=seed)
+    net.config(engine=engine, precision=precision)
+    flat = net.create(ann.PoissonPopulation(10000, rates=20.0))
+    ramp = net.create(ann.PoissonPopulation(1000, rates=np.repeat([5.0, 50.0], 500)))
+    mf, mr = net.monitor(flat, "spike"), net.monitor(ramp, "spike")
+    net.compile()
+    net.simulate_steps(steps)
+    out = mf.spike_arrays(), mr.spike_arrays(), net.engine
+    net.close()
+    return out
+
+
+@pytest.mark.gpu
+def test_poisson_statistics():
+    """Spike counts within 5 binomial standard deviations of rate * dt / 1000
+    per step; inter-spike intervals geometric (fraction of one-step
+    intervals = p)."""
+    (sf, rf), (sr, rr), _ = _poisson_run()
+    p = 20.0 * 0.1 / 1000.0
+    n_trials = 10000 * 10000
+    assert abs(sf.size - n_trials * p) < 5 * np.sqrt(n_trials * p * (1 - p))
+    for lo, hi, rate in ((0, 500, 5.0), (500, 1000, 50.0)):
+        k = int(((rr >= lo) & (rr < hi)).sum())
+        q = rate * 1e-4
+        trials = 500 * 10000
+        assert abs(k - trials * q) < 5 * np.sqrt(trials * q * (1 - q)), (rate, k)
+    # ISIs of the flat population: P(ISI = 1 step) = p
+    order = np.lexsort((sf, rf))
+    s_sorted, r_sorted = sf[order], rf[order]
+    same = r_sorted[1:] == r_sorted[:-1]
+    isi = np.diff(s_sorted)[same]
+    frac1 = np.mean(isi == 1)
+    assert abs(frac1 - p) < 5 * np.sqrt(p * (1 - p) / isi.size)
+
+
+@pytest.mark.gpu
+def test_poisson_reproducible_across_engines_and_seeds():
+    a = _poisson_run("grid", seed=3, steps=2000)
+    b = _poisson_run("grid", seed=3, steps=2000)
+    c = _poisson_run("local", seed=3, steps=2000)
+    d = _poisson_run("grid", seed=4, steps=2000)
+    for x, y in ((a, b), (a, c)):
+        assert np.array_equal(x[0][0], y[0][0]) and np.array_equal(x[0][1], y[0][1])
+        assert np.array_equal(x[1][0], y[1][0]) and np.array_equal(x[1][1], y[1][1])
+    assert c[2] == "cluster"
+    assert not (a[0][0].size == d[0][0].size and np.array_equal(a[0][1], d[0][1]))
