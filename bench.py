@@ -694,6 +694,68 @@ def delays_study(reps=3):
     return rows
 
 
+def poisson_study(n=1_000_000, steps=1000, rate=20.0):
+    """n Poisson neurons at `rate` Hz (dt = 0.1 ms, spike monitor on): device
+    time per step (median of three runs of `steps` steps, CUDA events on the
+    network's stream, CUDA graphs), neuron updates per second, the bytes a
+    step must move (rates read, p written, spike bitmap and monitor words) as
+    a fraction of the measured HBM peak, the spike count against its
+    binomial expectation, and the oracle's C restatement (same draws) on one
+    host core over a sample."""
+    import torch
+    import annarchy_b200 as ann
+    from oracle import oracle as O
+    peak, kind = peaks()
+    rows = []
+    for prec in ("float", "double"):
+        net = ann.Network(dt=0.1, seed=42)
+        net.config(precision=prec, engine="grid", graph_steps=50)
+        pop = net.create(ann.PoissonPopulation(n, rates=rate))
+        mon = net.monitor(pop, "spike")
+        net.compile()
+        nat, be = net._backend.native, net._backend
+        stream = torch.cuda.ExternalStream(nat.stream())
+        net.simulate_steps(100)
+        mon.get("spike")
+        runs = []
+        for _ in range(3):
+            t0 = nat.get_time()
+            starts = be.begin_chunk(t0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            nat.run(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            be.end_chunk(t0, steps, starts)
+            s, _ = mon.spike_arrays()
+            mon.get("spike")
+            runs.append((e0.elapsed_time(e1), s.size))
+        runs.sort()
+        ms, spikes = runs[1]
+        wb = 8 if prec == "double" else 4
+        bytes_step = n * (2 * wb + 2 / 8)          # rates in, p out, bitmap + monitor bit
+        p = rate * 0.1 / 1000.0
+        row = {"precision": prec, "neurons": n, "us_per_step": ms * 1e3 / steps,
+               "neuron_steps_per_s": n * steps / (ms * 1e-3),
+               "gbs": bytes_step * steps / (ms * 1e-3) / 1e9,
+               "hbm_frac": bytes_step * steps / (ms * 1e-3) / 1e9 / peak, "peak_source": kind,
+               "spikes": int(spikes), "expected": n * steps * p,
+               "z_score": (spikes - n * steps * p) / np.sqrt(n * steps * p * (1 - p))}
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+        net.close()
+    # oracle on one core: 100k neurons x 200 steps
+    t0 = time.perf_counter()
+    O.poisson_run(np.full(100_000, rate), 0.1, np.array([1, 2], np.uint32), 0, 200)
+    cpu_s = time.perf_counter() - t0
+    row = {"oracle_neuron_steps_per_s_1core": 100_000 * 200 / cpu_s,
+           "sample": "100k neurons x 200 steps, double, one host core"}
+    rows.append(row)
+    print(json.dumps(row), flush=True)
+    return rows
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -761,6 +823,8 @@ def main():
                          "sizes (comma separated, e.g. 64,128,256)")
     ap.add_argument("--batched-steps", type=int, default=5000,
                     help="time steps of the batched-instance study")
+    ap.add_argument("--poisson", action="store_true",
+                    help="Poisson input study (1M neurons at 20 Hz)")
     ap.add_argument("--delays", action="store_true",
                     help="synaptic-delay study on the 4000-neuron network")
     ap.add_argument("--formats", default="",
@@ -781,6 +845,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         delays_study()
+        return
+    if args.poisson:
+        import torch
+        torch.cuda.set_device(0)
+        poisson_study()
         return
     if args.spmv:
         import torch

@@ -368,3 +368,52 @@ void orc_csr_rowsum(int n_rows, const int64_t* row_ptr, const int* col, const do
     sum[i] = accumulate ? sum[i] + s : s;
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Poisson populations (ANNarchy/inputs/PoissonPopulation.py:100-202)        */
+/* ------------------------------------------------------------------------ */
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): the backend's generator
+ * for random distributions in equations; counter (index, step low, step
+ * high, stream), key (seed0, seed1). */
+static void orc_philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n1 = (uint32_t)p1;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1, n3 = (uint32_t)p0;
+    c[0] = n0;
+    c[1] = n1;
+    c[2] = n2;
+    c[3] = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+/* Simulates `steps` steps of n Poisson neurons (no refractory period) in
+ * double precision: every step p = 1000 * u / dt with u the 53-bit uniform
+ * of draw (seed, stream, t, i), spike when p < rates[i]. Spikes are
+ * appended to (spike_t, spike_i) up to max_spikes; returns the total. */
+int64_t orc_poisson_run(int n, const double* rates, double dt, const uint32_t* seed, uint32_t stream,
+                        int64_t t0, int steps, int32_t* spike_t, int32_t* spike_i, int64_t max_spikes) {
+  int64_t total = 0;
+  for (int s = 0; s < steps; ++s) {
+    const int64_t t = t0 + s;
+    for (int i = 0; i < n; ++i) {
+      uint32_t c[4] = {(uint32_t)i, (uint32_t)t, (uint32_t)((uint64_t)t >> 32), stream};
+      orc_philox(c, seed[0], seed[1]);
+      const double u = (double)(((uint64_t)(c[0] >> 6) << 27) | (c[1] >> 5)) * (1.0 / 9007199254740992.0);
+      const double rand_0 = 0.0 + (1.0 - 0.0) * u;
+      const double p = 1000.0 * rand_0 / dt;
+      if (p < rates[i]) {
+        if (total < max_spikes) {
+          spike_t[total] = (int32_t)t;
+          spike_i[total] = i;
+        }
+        ++total;
+      }
+    }
+  }
+  return total;
+}

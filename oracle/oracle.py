@@ -215,3 +215,20 @@ def csr_rowsum(m: sp.csr_matrix, x: np.ndarray) -> np.ndarray:
     out = np.zeros(m.shape[0])
     lib().orc_csr_rowsum(C.c_int(m.shape[0]), _p(rp), _p(col), _p(w), _p(x), _p(out), C.c_int(0))
     return out
+
+
+def poisson_run(rates, dt: float, seed, stream: int, steps: int, t0: int = 0, max_spikes: int | None = None):
+    """Spike raster (steps, ranks) of Poisson neurons in double precision with
+    the backend's Philox draws (orc_poisson_run)."""
+    rates = np.ascontiguousarray(rates, dtype=np.float64)
+    seed = np.ascontiguousarray(seed, dtype=np.uint32)
+    cap = int(max_spikes if max_spikes is not None else max(1024, 2 * rates.size * steps * float(rates.max()) * dt / 1000 + 1024))
+    st = np.zeros(cap, dtype=np.int32)
+    si = np.zeros(cap, dtype=np.int32)
+    lib().orc_poisson_run.restype = C.c_int64
+    total = lib().orc_poisson_run(C.c_int(rates.size), _p(rates), C.c_double(dt), _p(seed),
+                                  C.c_uint32(stream), C.c_int64(t0), C.c_int(steps), _p(st), _p(si),
+                                  C.c_int64(cap))
+    if total > cap:
+        raise RuntimeError(f"spike buffer too small ({total} > {cap})")
+    return st[:total].copy(), si[:total].copy()

@@ -8,6 +8,7 @@ import pytest
 
 import annarchy_b200 as ann
 from annarchy_b200.parser.text import ParserError
+from oracle import oracle as orc
 from oracle import philox
 
 
@@ -55,7 +56,41 @@ def test_poisson_population_forms():
         ann.PoissonPopulation(10, target="exc")
 
 
+def test_oracle_poisson_matches_host_philox():
+    """The C oracle's Poisson step (double) equals the numpy restatement of
+    the same draws: p = 1000 * u / dt < rates."""
+    seed = np.array([12345, 678], dtype=np.uint32)
+    rates = np.linspace(1.0, 200.0, 300)
+    s, i = orc.poisson_run(rates, 0.1, seed, 7, 50, t0=3)
+    ws, wi = [], []
+    for t in range(3, 53):
+        u = philox.uniform(seed, 7, t, np.arange(300), True)
+        hit = np.nonzero(1000.0 * (0.0 + (1.0 - 0.0) * u) / 0.1 < rates)[0]
+        ws.append(np.full(hit.size, t))
+        wi.append(hit)
+    assert np.array_equal(s, np.concatenate(ws)) and np.array_equal(i, np.concatenate(wi))
+
+
 # ---------------------------------------------------------------- GPU
+@pytest.mark.gpu
+def test_poisson_double_equals_oracle():
+    """Double precision: the device raster of a PoissonPopulation with
+    per-neuron rates equals the oracle's, spike for spike."""
+    net = ann.Network(dt=0.1, seed=21)
+    net.config(precision="double", engine="grid")
+    rates = np.linspace(1.0, 100.0, 5000)
+    pop = net.create(ann.PoissonPopulation(5000, rates=rates))
+    mon = net.monitor(pop, "spike")
+    net.compile()
+    net.simulate_steps(2000)
+    s, r = mon.spike_arrays()
+    seed = net._backend.native.read("rng_seed")
+    os_, oi = orc.poisson_run(rates, 0.1, seed, (pop.id << 8) | 0, 2000)
+    assert s.size > 1000
+    assert np.array_equal(s, os_) and np.array_equal(r, oi)
+    net.close()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["double", "float"])
 def test_device_draws_match_host_philox(precision):
