@@ -477,7 +477,8 @@ class CompiledNetwork:
         nat.create(f"proj{k}__w", self._w(w))
         for prm in proj.desc["parameters"] + proj.desc["variables"]:
             if prm["locality"] == "global":
-                nat.create(f"proj{k}__{prm['name']}", np.array([prm["init"]], dtype=self.real))
+                value = proj._global_values.get(prm["name"], prm["init"])
+                nat.create(f"proj{k}__{prm['name']}", np.array([value], dtype=self.real))
         if proj.synapse_type.type == "rate":
             fmt = "csr" if proj._delay_steps is not None else self._rate_format(proj, lay)
             lay["format"] = fmt

@@ -182,6 +182,19 @@ class Network:
     def set_time(self, t: float):
         self.set_current_step(int(round(t / self.dt)))
 
+    def save(self, filename: str, populations: bool = True, projections: bool = True):
+        """Network state into a file in the reference's layout
+        (ANNarchy/core/IO.py:398-431): .npz, .gz, .mat (not loadable) or pickle."""
+        from .io import network_description, save_data
+        save_data(filename, network_description(self, populations, projections))
+
+    def load(self, filename: str, populations: bool = True, projections: bool = True,
+             pickle_encoding: str | None = None):
+        """State saved by save() (or by the reference's save()); before
+        compile() it also gives the projections their connectivity."""
+        from .io import load_data, load_network
+        load_network(self, load_data(filename, pickle_encoding), populations, projections)
+
     def reset(self, populations: bool = True, projections: bool = False, synapses: bool = False,
               monitors: bool = True, reseed_rng: bool = True):
         """Back to the state after compile() (ANNarchy/core/Network.py:628-675):

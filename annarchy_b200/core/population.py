@@ -155,6 +155,17 @@ class Population:
                 if attributes is None or p["name"] in attributes:
                     self._host[p["name"]] = self._initial(p)
 
+    def save(self, filename: str):
+        """Every parameter and variable into a file (.npz, .gz, .mat or
+        pickle), in the reference's layout (Population.py:1000-1066)."""
+        from .io import population_data, save_data
+        save_data(filename, population_data(self))
+
+    def load(self, filename: str, pickle_encoding: str | None = None):
+        """Attributes from a file saved by save() (or by the reference)."""
+        from .io import load_data, load_population_data
+        load_population_data(self, load_data(filename, pickle_encoding))
+
     def set_refractory(self, value):
         self._refractory_ms = draw(value, (self.size,), self._rng())
         self._has_refractory = self._has_refractory or bool(np.any(self._refractory_ms > 0))

@@ -74,6 +74,7 @@ class Projection:
         self.uniform_delay = 1          # steps; -1 when the delays are per synapse
         self.max_delay = 1              # steps
         self._delay_steps = None        # per synapse (CSR order) for non-uniform delays
+        self._global_values: dict[str, float] = {}   # global parameters set before compile()
 
     # -- properties -------------------------------------------------------------
     @property
@@ -345,7 +346,7 @@ class Projection:
         if name in glob:
             if self.net is not None and self.net._compiled:
                 return float(self.net._backend.read_projection_attribute(self, name)[0])
-            return float(glob[name]["init"])
+            return float(self._global_values.get(name, glob[name]["init"]))
         if self.net is not None and self.net._compiled:
             flat_v = self.net._backend.read_projection_attribute(self, name)
         elif name == "w":
@@ -361,7 +362,16 @@ class Projection:
         return [a for a in np.split(flat_v, np.cumsum(lengths)[:-1])]
 
     def set(self, values: dict):
+        glob = {p["name"] for p in self.desc["parameters"] + self.desc["variables"]
+                if p["locality"] == "global"}
         for name, value in values.items():
+            if name in glob:
+                value = float(np.asarray(value).reshape(-1)[0])
+                if self.net is not None and self.net._compiled:
+                    self.net._backend.write_projection_attribute(self, name, np.array([value]))
+                else:
+                    self._global_values[name] = value
+                continue
             nnz = self.nb_synapses
             if isinstance(value, list):
                 value = np.concatenate([np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in value])
@@ -438,6 +448,21 @@ class Projection:
             self.max_delay = int(steps.max())
         else:
             self.net._backend.write_delays(self, steps)
+
+    # -- save / load (ANNarchy/core/Projection.py:1731-1950) ---------------------------
+    def save(self, filename: str):
+        """Connectivity, delays and synaptic attributes into a file (.npz,
+        .gz, .mat or pickle), in the reference's layout."""
+        from .io import projection_data, save_data
+        save_data(filename, projection_data(self))
+
+    def load(self, filename: str, pickle_encoding: str | None = None):
+        """Before compile(): connectivity, weights and delays from a file
+        saved by save() (or by the reference); after compile(): attributes
+        and delays of the same connectivity."""
+        from .io import load_data, load_projection_data
+        load_projection_data(self, load_data(filename, pickle_encoding))
+        return self
 
     def dendrite_sizes(self):
         lengths = np.diff(self._csr.indptr)

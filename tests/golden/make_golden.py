@@ -151,6 +151,49 @@ def case_coba(name, seed, n, p, steps, v_every, stdp=False):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+def case_io(name):
+    """A state file written by the reference's Network.save(): an STDP
+    network (plastic E->E, I->all with a uniform 0.5 ms delay) after 50 steps
+    (io_ref_state.npz), and the values to expect when it is loaded
+    (io_ref_meta.npz)."""
+    import numpy as np
+    import ANNarchy as ann
+    from annarchy_b200 import workloads as wl
+    cn = wl.coba_net(seed=3, n=200, p=0.1)
+    net = ann.Network(dt=cn.dt, seed=1)
+    net.config(num_threads=1)
+    P = net.create(cn.n, _coba_neuron(ann, cn.params))
+    Pe, Pi = P[: cn.n_exc], P[cn.n_exc:]
+    ee = net.connect(Pe, Pe, "exc", synapse=ann.STDP(**wl.STDP_PARAMS))
+    ee.from_sparse(wl.to_from_sparse(wl.stdp_matrix(cn, 3, 0.1)), storage_format="csr")
+    ci = net.connect(Pi, P, "inh")
+    ci.from_sparse(wl.to_from_sparse(cn.w_inh), delays=0.5, storage_format="csr")
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    P.v = cn.v0
+    net.simulate(50 * cn.dt)
+    net.save(os.path.join(HERE, "io_ref_state.npz"))
+    meta = dict(v=np.asarray(P.v), w_ee=np.concatenate([np.asarray(d, dtype=np.float64) for d in ee.w]),
+                x_ee=np.concatenate([np.asarray(d, dtype=np.float64) for d in ee.x]))
+    # the other direction: a file written by this backend's save() (same
+    # network, halved weights, other potentials) loaded by the reference
+    import annarchy_b200 as b2
+    ours = b2.Network(dt=cn.dt, seed=1)
+    Q = ours.create(cn.n, wl.coba_neuron(cn.params))
+    oee = ours.connect(Q[: cn.n_exc], Q[: cn.n_exc], "exc", synapse=b2.STDP(**wl.STDP_PARAMS))
+    oee.from_sparse(wl.to_from_sparse(wl.stdp_matrix(cn, 3, 0.1) * 0.5))
+    oci = ours.connect(Q[cn.n_exc:], Q, "inh")
+    oci.from_sparse(wl.to_from_sparse(cn.w_inh), delays=0.5)
+    Q.v = np.linspace(-70.0, -40.0, cn.n)
+    path = os.path.join(WORK, "ours_state.npz")
+    ours.save(path)
+    net.load(path)
+    w_loaded = np.concatenate([np.asarray(d, dtype=np.float64) for d in ee.w])
+    w_ours = np.concatenate([np.asarray(d, dtype=np.float64) for d in oee.get("w")])
+    meta["reference_loaded_ours"] = bool(np.array_equal(w_loaded, w_ours) and
+                                         np.array_equal(np.asarray(P.v), Q.v))
+    np.savez_compressed(os.path.join(HERE, "io_ref_meta.npz"), **meta)
+
+
 def case_parser(name):
     """Description dicts of the reference parser for a set of models."""
     import ANNarchy as ann
@@ -204,6 +247,7 @@ CASES = {
     "coba_small": (case_coba, dict(seed=7, n=400, p=0.05, steps=2000, v_every=50)),
     "coba_c2": (case_coba, dict(seed=42, n=4000, p=0.02, steps=10000, v_every=0)),
     "stdp_small": (case_coba, dict(seed=11, n=400, p=0.05, steps=2000, v_every=0, stdp=True)),
+    "io": (case_io, {}),
 }
 
 
