@@ -12,7 +12,7 @@ the ANNarchy neural simulator.
     spikes = m.get("spike")
 """
 from .core.models import IF_cond_exp, LeakyIntegrator, Neuron, STDP, Synapse
-from .core.inputs import PoissonPopulation
+from .core.inputs import PoissonPopulation, TimedArray
 from .core.monitor import Monitor
 from .core.network import Network
 from .core.population import Population, PopulationView
@@ -25,5 +25,5 @@ float64 = "double"
 __version__ = "0.1.0"
 
 __all__ = ["Network", "Neuron", "Synapse", "Population", "PopulationView", "Projection",
-           "Monitor", "PoissonPopulation", "Uniform", "Normal", "LogNormal", "Exponential", "DiscreteUniform",
+           "Monitor", "PoissonPopulation", "TimedArray", "Uniform", "Normal", "LogNormal", "Exponential", "DiscreteUniform",
            "RandomDistribution", "LeakyIntegrator", "IF_cond_exp", "STDP", "float32", "float64"]

@@ -348,6 +348,8 @@ class CompiledNetwork:
             nat.create(f"pop{pop.id}__{name}", np.asarray(arr, dtype=dt).reshape(-1))
         for name in compensated_vars(pop, self.exact, self.net._config):
             nat.create(f"pop{pop.id}__kc_{name}", np.zeros(pop.size, dtype=self.real))
+        if hasattr(pop, "_ta_schedule_ms"):
+            self.write_timed_array(pop)
         R = self.slots.get(pop.id, 1)
         if pop.neuron_type.type == "rate" and R > 1:
             # rates of the last R steps (slot t % R holds step t), filled with
@@ -443,6 +445,18 @@ class CompiledNetwork:
         ring = np.zeros((R, S), dtype=self.real)
         ring[:, :pop.size] = np.asarray(r, dtype=self.real).reshape(-1)
         return ring.reshape(-1)
+
+    def write_timed_array(self, pop):
+        """Buffer (blocks x N), schedule (steps) and [t0, period, blocks] of a
+        TimedArray population."""
+        nat, k = self.native, pop.id
+        sched, per = pop.steps()
+        rates = pop._ta_rates if pop._ta_rates is not None else np.zeros((0, pop.size))
+        nb = len(sched)
+        nat.create(f"pop{k}__ta_buf", np.asarray(rates[:nb], dtype=self.real).reshape(-1)
+                   if nb else np.zeros(1, dtype=self.real))
+        nat.create(f"pop{k}__ta_sched", np.asarray(sched if nb else [0], dtype=np.int32))
+        nat.create(f"pop{k}__ta_meta", np.array([pop._ta_t0, per, nb], dtype=np.int64))
 
     def delay_capacity(self, proj) -> int:
         """Largest delay (steps) the pre-synaptic history kept since compile()

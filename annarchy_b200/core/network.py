@@ -66,12 +66,15 @@ class Network:
             self._config[key] = val
         return self
 
-    def create(self, geometry, neuron=None, name: str | None = None, **kw) -> Population:
+    def create(self, geometry=None, neuron=None, name: str | None = None, population=None,
+               **kw) -> Population:
         """A population of `neuron`, or (as the reference's
         net.create(PoissonPopulation(...))) a population object built outside
         the network, which then joins it."""
         if self._compiled:
             raise RuntimeError("the network is already compiled")
+        if population is not None:
+            geometry = population
         if isinstance(geometry, Population):
             pop = geometry
             if pop.net is not None and pop.net is not self:

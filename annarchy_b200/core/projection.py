@@ -429,7 +429,7 @@ class Projection:
                                  f"compile(); give the largest delay before compile()")
             self.uniform_delay = d
             self.max_delay = max(self.max_delay, d) if not compiled else self.max_delay
-            if compiled:
+            if compiled and self.max_delay > 1:      # without history the delay stays one step
                 self.net._backend.write_delays(self, np.array([d], dtype=np.int32))
             return
         if not isinstance(value, (list, np.ndarray)):

@@ -506,6 +506,36 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
 }}
 """
 
+    def timed_array_kernel(self, pop) -> str:
+        """TimedArray update (ANNarchy/inputs/TimedArray.py, update_variables):
+        internal time tau = t - t0 (modulo the period when positive); when tau
+        equals schedule[b], r = buffer[b]; otherwise r keeps its value. The
+        schedule is increasing, so b is found by bisection."""
+        k = pop.id
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_timed() {{
+    const long long t = *{self.ptr('t')};
+    const long long* anb_meta = {self.ptr(f'pop{k}__ta_meta')};
+    long long tau = t - anb_meta[0];
+    const long long period = anb_meta[1];
+    const int nb = (int)anb_meta[2];
+    if (tau < 0 || nb == 0) return;
+    if (period > 0) tau %= period;
+    const int* __restrict__ sched = {self.ptr(f'pop{k}__ta_sched')};
+    int lo = 0, hi = nb - 1, b = -1;
+    while (lo <= hi) {{
+      const int mid = (lo + hi) >> 1;
+      const long long s = sched[mid];
+      if (s == tau) {{ b = mid; break; }}
+      if (s < tau) lo = mid + 1; else hi = mid - 1;
+    }}
+    if (b < 0) return;
+    const {self.real}* __restrict__ buf = {self.ptr(f'pop{k}__ta_buf')} + (size_t)b * {pop.size};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < {pop.size}; i += gridDim.x * blockDim.x)
+      {self.ptr(f'pop{k}__r')}[i] = buf[i];
+}}
+"""
+
     def delay_kernel(self, pop) -> str:
         """This step's rates into the history ring of a population without
         an update of its own (the reference's update_delay)."""
@@ -916,7 +946,13 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
                 group = 1 if self.atomic_psp(proj) else 0
                 plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0, group))
         for pop in net.populations:
-            if self.has_update(pop):
+            if hasattr(pop, "_ta_schedule_ms"):
+                kernels.append(self.timed_array_kernel(pop))
+                plan.append((f"pop{pop.id}_timed", grid_for(pop.size), BLOCK, 0))
+                if self.slots(pop) > 1:
+                    kernels.append(self.delay_kernel(pop))
+                    plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))
+            elif self.has_update(pop):
                 kernels.append(self.pop_kernel(pop))
                 plan.append((f"pop{pop.id}_step", grid_for(pop.size), BLOCK, 0))
             elif pop.neuron_type.type == "rate" and self.slots(pop) > 1:

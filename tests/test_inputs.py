@@ -165,3 +165,74 @@ def test_poisson_reproducible_across_engines_and_seeds():
         assert np.array_equal(x[1][0], y[1][0]) and np.array_equal(x[1][1], y[1][1])
     assert c[2] == "cluster"
     assert not (a[0][0].size == d[0][0].size and np.array_equal(a[0][1], d[0][1]))
+
+
+# ---------------------------------------------------------------- TimedArray
+def test_timed_array_schedule_steps():
+    net = ann.Network(dt=0.5)
+    a = net.create(ann.TimedArray(rates=np.eye(4)))
+    b = net.create(ann.TimedArray(rates=np.eye(4), schedule=2.0, period=10.0))
+    c = net.create(ann.TimedArray(geometry=4))
+    c.update(np.eye(4), schedule=[1.0, 2.0, 5.0])
+    assert a.steps() == ([0, 1, 2, 3], -1)
+    assert b.steps() == ([0, 4, 8, 12], 20)
+    assert c.steps() == ([2, 4, 10], -1) and c.rates.shape == (3, 4)
+    assert a.schedule == [0.0, 0.5, 1.0, 1.5]
+    with pytest.raises(ValueError):
+        c.update(np.eye(4), schedule=[2.0, 1.0])
+    with pytest.raises(ValueError):
+        c.update(np.ones((2, 5)))
+
+
+def _timed_net(late: bool):
+    inputs = np.eye(10)
+    net = ann.Network(dt=1.0)
+    if late:
+        pops = [net.create(population=ann.TimedArray(geometry=10)) for _ in range(4)]
+        pops[0].update(rates=inputs)
+        pops[1].update(rates=inputs, schedule=10.0)
+        pops[2].update(rates=inputs, period=10.0)
+        pops[3].update(rates=inputs, schedule=2.0, period=20.0)
+    else:
+        pops = [net.create(population=ann.TimedArray(rates=inputs)),
+                net.create(population=ann.TimedArray(rates=inputs, schedule=10.0)),
+                net.create(population=ann.TimedArray(rates=inputs, period=10.0)),
+                net.create(population=ann.TimedArray(rates=inputs, schedule=2.0, period=20.0))]
+    out = net.create(10, ann.Neuron(equations="r = sum(exc)\nr2 = sum(exc2)\nr3 = sum(exc3)\nr4 = sum(exc4)"))
+    for p, tgt in zip(pops, ("exc", "exc2", "exc3", "exc4")):
+        net.connect(p, out, tgt).one_to_one(1.0)
+    net.compile()
+    return net, out, pops
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("late", [False, True])
+def test_timed_array_known_answers(late):
+    """tests_python/Interface/test_TimedArray.py (read as text): outputs after
+    11, 12, 21, 12 and 25 ms for the four schedule/period combinations, with
+    the arrays given at construction or set later with update()."""
+    net, out, pops = _timed_net(late)
+    e = np.eye(10)
+    net.reset()
+    net.simulate(11)
+    np.testing.assert_allclose(out.r, e[9])
+    net.reset()
+    net.simulate(12)
+    np.testing.assert_allclose(out.r, e[9])
+    net.reset()
+    net.simulate(11)
+    net.simulate(10)
+    np.testing.assert_allclose(out.r2, e[1])
+    net.reset()
+    net.simulate(12)
+    np.testing.assert_allclose(out.r3, e[0])
+    net.reset()
+    net.simulate(25)
+    np.testing.assert_allclose(out.r4, e[1])
+    # update with reset: the new buffer restarts at the next step
+    net.reset()
+    net.simulate(5)
+    pops[0].update(rates=2 * np.eye(10), reset=True)
+    net.simulate(3)
+    np.testing.assert_allclose(out.r, 2 * e[1])
+    net.close()
