@@ -24,6 +24,7 @@
 #include <memory>
 #include <string>
 #include <vector>
+#include <algorithm>
 
 #include "../../include/annarchy_b200.h"
 
@@ -1010,6 +1011,22 @@ __global__ void anb_flush_read(const uint4* __restrict__ p, size_t n, unsigned* 
 }
 }  // namespace
 
+// Streaming read of n 16-byte words, four loads in flight per thread, no
+// reuse (evict-first loads): the cold-read floor of a kernel that must read
+// that many bytes once.
+__global__ void anb_stream_read_kernel(const uint4* __restrict__ p, size_t n, unsigned* sink) {
+  unsigned acc = 0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    const uint4 a = __ldcs(p + i), b = __ldcs(p + i + stride), c = __ldcs(p + i + 2 * stride),
+                d = __ldcs(p + i + 3 * stride);
+    acc ^= a.x ^ b.y ^ c.z ^ d.w;
+  }
+  for (; i < n; i += stride) acc ^= __ldcs(p + i).x;
+  if (acc == 0x9e3779b9u) *sink = acc;
+}
+
 int anb_flush_l2(anb_net* net) {
   if (!net) return fail(ANB_ERR_ARG, "net is NULL");
   int rc = ensure_device(net);
@@ -1032,6 +1049,42 @@ int anb_flush_l2(anb_net* net) {
       reinterpret_cast<const uint4*>(net->flush_buf), net->flush_bytes / 16,
       reinterpret_cast<unsigned*>(static_cast<char*>(net->flush_buf) + net->flush_bytes));
   ANB_CUDA(cudaGetLastError());
+  return ANB_OK;
+}
+
+int anb_stream_read(anb_net* net, size_t bytes, int reps, double* ms_median) {
+  if (!net || !ms_median || bytes < 16 || reps < 1 || reps > 64) return fail(ANB_ERR_ARG, "bad arguments");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  void* buf = nullptr;
+  const size_t n = bytes / 16;
+  if (cudaMalloc(&buf, n * 16 + 16) != cudaSuccess) return fail(ANB_ERR_ALLOC, "stream buffer");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<float> ts;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  cudaError_t e = cudaMemsetAsync(buf, 0x33, n * 16 + 16, net->stream);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+    rc = anb_flush_l2(net);
+    if (rc) break;
+    cudaEventRecord(e0, net->stream);
+    anb_stream_read_kernel<<<sms * 8, 256, 0, net->stream>>>(
+        reinterpret_cast<const uint4*>(buf), n, reinterpret_cast<unsigned*>(static_cast<char*>(buf) + n * 16));
+    cudaEventRecord(e1, net->stream);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    ts.push_back(ms);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ANB_ERR_CUDA, std::string("stream read: ") + cudaGetErrorString(e));
+  std::sort(ts.begin(), ts.end());
+  *ms_median = ts[ts.size() / 2];
   return ANB_OK;
 }
 

@@ -48,6 +48,7 @@ SIGNATURES = {
     "anb_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "anb_bsr_tc_pack_x": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "anb_bsr_spmm_tc_shape": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "anb_stream_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
     "anb_array_copy_strided": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_size_t, C.c_char_p,
                                          C.c_size_t, C.c_size_t, C.c_size_t]),
     "anb_plan_add_concurrent": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint, C.c_int]),
@@ -278,6 +279,12 @@ class NativeNet:
     def free(self, name: str):
         check("anb_array_free", self.lib.anb_array_free(self.h, name.encode()))
         self.arrays.pop(name, None)
+
+    def stream_read_ms(self, nbytes: int, reps: int = 5) -> float:
+        """Median cold streaming-read time (ms) of `nbytes` (anb_stream_read)."""
+        out = C.c_double(0.0)
+        check("anb_stream_read", self.lib.anb_stream_read(self.h, int(nbytes), reps, C.byref(out)))
+        return out.value
 
     def copy_strided(self, dst, dst_offset, dst_stride, src, src_offset, src_stride, count):
         """Device copy of `count` 4-byte elements between arrays (byte offsets

@@ -114,9 +114,12 @@ def algorithmic_bytes(m: sp.csr_matrix, weight_bytes: int) -> float:
 
 
 def measure(m: sp.csr_matrix, sched: dict, precision: str = "float",
-            weight_dtype: str = "float32", reps: int = 5, seed: int = 0):
-    """Device time (ms, median of `reps` cold-L2 repetitions) of the weighted
-    sum of matrix m (post, pre) stored with schedule `sched`."""
+            weight_dtype: str = "float32", reps: int = 5, seed: int = 0, flush: bool = True):
+    """Device time (ms, median of `reps` repetitions) of the weighted sum of
+    matrix m (post, pre) stored with schedule `sched`: with a clean L2 flush
+    before each repetition (cold), or back to back (`flush=False`: the steady
+    state of a running simulation, where a matrix smaller than the L2 stays
+    there)."""
     from . import Network, Neuron
     n_post, n_pre = m.shape
     net = Network(dt=1.0, seed=seed)
@@ -132,7 +135,8 @@ def measure(m: sp.csr_matrix, sched: dict, precision: str = "float",
     net.simulate_steps(1)
     times = []
     for _ in range(reps):
-        nat.flush_l2()
+        if flush:
+            nat.flush_l2()
         nat.kernel_timing(True)
         net.simulate_steps(1)
         nat.synchronize()

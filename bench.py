@@ -266,30 +266,25 @@ def accuracy_study(seeds=range(42, 50)):
 
 
 def stream_read_us(nbytes, reps=5):
-    """Device time of a plain read of `nbytes` (torch sum of a float tensor)
-    after a clean L2 flush (reading 384 MB): the floor any kernel that must
-    read that many cold bytes meets, kernel launch and DRAM ramp included."""
-    import torch
-    x = torch.ones(max(1, int(nbytes) // 4), device="cuda")
-    flush = torch.ones((384 << 20) // 4, device="cuda")
-    ts = []
-    for _ in range(reps):
-        flush.sum()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        x.sum()
-        e1.record()
-        torch.cuda.synchronize()
-        ts.append(e0.elapsed_time(e1) * 1e3)
-    del x, flush
-    return float(sorted(ts)[len(ts) // 2])
+    """Device time of a plain streaming read of `nbytes` after a clean L2
+    flush (anb_stream_read: 16-byte evict-first loads, four in flight per
+    thread, 8 CTAs per SM): the floor any kernel that must read that many cold
+    bytes meets, kernel launch and DRAM ramp included."""
+    from annarchy_b200.runtime.lib import NativeNet
+    nat = NativeNet(0)
+    nat.initialize(1.0)
+    try:
+        return float(nat.stream_read_ms(int(nbytes), reps) * 1e3)
+    finally:
+        nat.close()
 
 
 def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
     """Rate-coded weighted sums of the 100k-neuron recurrent matrices in every
     feasible storage format: cold-L2 kernel time and achieved algorithmic
-    bandwidth as a fraction of the measured HBM peak."""
+    bandwidth as a fraction of the measured HBM peak; for the best schedule
+    also the steady state (back-to-back sums, matrices under 126 MB staying
+    in L2)."""
     from annarchy_b200 import tuning, workloads as wl
     peak, kind = peaks()
     out = {"peak_gbs": peak, "peak_source": kind, "results": {}}
@@ -311,9 +306,14 @@ def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
                 sel = S.default_model().choose(m) if S.default_model() else None
             except Exception:       # selector unavailable: reported as None
                 sel = None
+            # steady state of the best schedule: back-to-back sums, no flush
+            best_sched = next(sc for sc in scheds if tuning.schedule_name(sc) == best)
+            warm_ms = tuning.measure(m, best_sched, "float", dt, reps, flush=False)
             out["results"][f"{st}/{dt}"] = {
                 "nnz": int(m.nnz), "mean_row": float(rl.mean()), "max_row": int(rl.max()),
                 "algorithmic_mb": ab / 1e6, "best": best,
+                "best_steady_state": {"ms": warm_ms, "gbs": ab / (warm_ms * 1e-3) / 1e9,
+                                      "frac_of_hbm_peak": ab / (warm_ms * 1e-3) / 1e9 / peak},
                 "heuristic": tuning.heuristic(m), "selector": sel,
                 "stream_floor_us": floor_us,
                 "schedules": {k: {"ms": v, "gbs": ab / (v * 1e-3) / 1e9,
@@ -756,6 +756,55 @@ def poisson_study(n=1_000_000, steps=1000, rate=20.0):
     return rows
 
 
+def rate_study(reps=3):
+    """The reference's CPU-runnable configuration: 1000 constant inputs ->
+    4000 leaky integrators (tau dr/dt + r = sum(exc), rectified), input and
+    recurrent CSR projections (p = 0.1 / 0.02, ~720k synapses), dt = 1 ms,
+    1000 steps. Per precision: time per step (grid engine, CUDA graphs, device
+    synchronised on both sides; median of `reps`), GSynOps/s (synapses x steps
+    / time), the final rates against the double oracle (bit-exact in double,
+    norm-wise relative error in float), and the oracle on one host core and on
+    all of them."""
+    import torch
+    from annarchy_b200 import workloads as wl
+    from oracle import oracle as O
+    rn = wl.rate_net()
+    rows = []
+    ref, _ = O.rate_run(rn)
+    for prec in ("double", "float"):
+        net, pop, mon = wl.build_rate_network(rn, prec, record=False)
+        net.compile()
+        nat = net._backend.native
+        ts = []
+        for _ in range(reps + 1):
+            net.reset()
+            pop.reset()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            nat.run(rn.steps)
+            nat.synchronize()
+            ts.append(time.perf_counter() - t0)
+        ms = sorted(ts[1:])[len(ts[1:]) // 2] * 1e3
+        r = pop.r
+        row = {"precision": prec, "us_per_step": ms * 1e3 / rn.steps,
+               "gsynops": rn.nnz * rn.steps / (ms * 1e-3) / 1e9,
+               "rel_err_final": float(np.linalg.norm(r - ref) / np.linalg.norm(ref))}
+        if prec == "double":
+            row["bit_exact"] = bool(np.array_equal(r, ref))
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+        net.close()
+    for threads in (1, os.cpu_count() or 1):
+        t0 = time.perf_counter()
+        O.rate_run(rn, threads=threads)
+        cpu = time.perf_counter() - t0
+        row = {"oracle_threads": threads, "us_per_step": cpu * 1e6 / rn.steps,
+               "gsynops": rn.nnz * rn.steps / cpu / 1e9}
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+    return rows
+
+
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     from oracle import oracle as O
     out_deg = cn.out_degree()
@@ -823,6 +872,8 @@ def main():
                          "sizes (comma separated, e.g. 64,128,256)")
     ap.add_argument("--batched-steps", type=int, default=5000,
                     help="time steps of the batched-instance study")
+    ap.add_argument("--rate", action="store_true",
+                    help="rate-coded 1000 -> 4000 network study (the CPU-runnable configuration)")
     ap.add_argument("--poisson", action="store_true",
                     help="Poisson input study (1M neurons at 20 Hz)")
     ap.add_argument("--delays", action="store_true",
@@ -850,6 +901,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         poisson_study()
+        return
+    if args.rate:
+        import torch
+        torch.cuda.set_device(0)
+        rate_study()
         return
     if args.spmv:
         import torch

@@ -249,6 +249,11 @@ int anb_bsr_spmm_simt(const int* block_row_ptr, const int* block_col, const uint
  * starts with a cold cache holding no dirty lines; used between timed
  * repetitions. */
 int anb_flush_l2(anb_net* net);
+/* Cold-read floor: median device time (ms, CUDA events) over `reps` (1-64)
+ * repetitions of a streaming read of `bytes` from a fresh buffer, each after
+ * anb_flush_l2 (a measuring stick for kernels that must read that many bytes
+ * once). No counterpart in the reference. */
+int anb_stream_read(anb_net* net, size_t bytes, int reps, double* ms_median);
 int anb_kernel_timing(anb_net* net, int enable);
 int anb_kernel_time_count(anb_net* net, int* count);
 int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len,
