@@ -59,6 +59,10 @@ class CompiledNetwork:
         self.engine = None
         self.module = None
         self.slots: dict[int, int] = {}    # history ring length (steps) per population
+        # sharding by post neurons: (rank, world) and the owned slice per population
+        self.shard = net._config.get("shard")
+        self.owned: dict[int, tuple[int, int]] = {}
+        self._exchange = None
 
     # --------------------------------------------------------------- helpers
     def _w(self, w: np.ndarray) -> np.ndarray:
@@ -108,8 +112,11 @@ class CompiledNetwork:
             self.slots[pop.id] = max([1] + [int(p.max_delay) for p in net.projections
                                            if p.pre_pop is pop])
         self.engine = self._choose_engine()
-        # fast grid engine: per-step spike lists drive the event kernels
-        self.spike_lists = (not self.exact and self.engine == "grid")
+        # fast grid engine: per-step spike lists drive the event kernels (a
+        # sharded network transmits from the exchanged bitmaps instead)
+        self.spike_lists = (not self.exact and self.engine == "grid" and not self.shard)
+        if self.shard:
+            self._setup_shard()
         for pop in net.populations:
             self._create_population(pop)
         for proj in net.projections:
@@ -170,8 +177,41 @@ class CompiledNetwork:
             return
         raise RuntimeError(f"no cluster configuration fits this network ({last_err})")
 
+    def _setup_shard(self):
+        from .shard import Exchange, owned_range
+        rank, world = (int(x) for x in self.shard)
+        if not 0 <= rank < world:
+            raise ValueError(f"shard {self.shard}: rank must lie in [0, world)")
+        net = self.net
+        if any(p.neuron_type.type != "spike" for p in net.populations):
+            raise NotImplementedError("sharded networks are spiking networks")
+        if any(p.max_delay > 1 for p in net.projections):
+            raise NotImplementedError("sharded networks transmit without synaptic delays")
+        for pop in net.populations:
+            self.owned[pop.id] = owned_range(pop.size, rank, world)
+        if not isinstance(self.native, DryNative):
+            self._exchange = Exchange(rank, world, net._config.get("shard_group"))
+
+    def _local_rows(self, proj, post_rank, row_ptr, cols, w):
+        """The rows of the owned post neurons (sharded networks) and the mask
+        of their synapses in CSR order."""
+        keep_syn = np.ones(cols.size, dtype=bool)
+        if not self.shard:
+            return post_rank, row_ptr, cols, w, keep_syn
+        lo, hi = self.owned[proj.post_pop.id]
+        rows = (post_rank >= lo) & (post_rank < hi)
+        lengths = np.diff(row_ptr)
+        keep_syn = np.repeat(rows, lengths)
+        new_ptr = np.zeros(int(rows.sum()) + 1, dtype=row_ptr.dtype)
+        np.cumsum(lengths[rows], out=new_ptr[1:])
+        return post_rank[rows], new_ptr, cols[keep_syn], w[keep_syn], keep_syn
+
     def _choose_engine(self) -> str:
         want = self.net._config.get("engine", "auto")
+        if self.net._config.get("shard"):
+            if want == "local":
+                raise NotImplementedError("sharded networks run on the grid engine")
+            return "grid"
         ok, why = self._local_possible()
         if want == "local":
             if not ok:
@@ -382,12 +422,19 @@ class CompiledNetwork:
         if proj.synapse_type.type != "spike":
             raise NotImplementedError("device connectors are implemented for spiking projections")
         npost = len(proj.post_ranks_view)
+        post0, row0 = int(proj.post_ranks_view[0]), 0
+        if self.shard:                    # the owned rows of this projection
+            lo, hi = self.owned[proj.post_pop.id]
+            a, b = max(lo, post0), min(hi, post0 + npost)
+            if b <= a:
+                raise NotImplementedError("every rank must own at least one row of each projection")
+            row0, post0, npost = a - post0, a, b - a
         pre_lo, pre_hi = int(proj.pre_ranks[0]), int(proj.pre_ranks[-1]) + 1
         plastic = proj.plastic
         wdt = np.float64 if self.exact else (np.float32 if plastic else self.wdtype)
-        nat.connect_fixed_number_pre(f"proj{k}", npost, int(proj.post_ranks_view[0]), pre_lo, pre_hi,
+        nat.connect_fixed_number_pre(f"proj{k}", npost, post0, pre_lo, pre_hi,
                                      d["number"], d["seed"], d["wkind"], d["a"], d["b"], wdt,
-                                     d["exclude_self"])
+                                     d["exclude_self"], row_offset=row0)
         nnz = npost * d["number"]
         lay = {"rows": npost, "nnz": nnz, "idx_t": "int", "format": "csr", "device": True,
                "w0": pre_lo // 32, "w1": (pre_hi - 1) // 32 + 1}
@@ -401,8 +448,7 @@ class CompiledNetwork:
         lay["post_chunks"] = max(1, -(-d["number"] // 32))
         if plastic and self.spike_lists:
             row_of = np.full(proj.post_pop.size, -1, dtype=np.int32)
-            base = int(proj.post_ranks_view[0])
-            row_of[base:base + npost] = np.arange(npost, dtype=np.int32)
+            row_of[post0:post0 + npost] = np.arange(npost, dtype=np.int32)
             nat.create(f"proj{k}__row_of", row_of)
         if self.exact or plastic:
             lay["grid"] = grid_for(npost * 32)
@@ -481,6 +527,7 @@ class CompiledNetwork:
         if proj._csr is None:
             raise RuntimeError(f"projection {proj.name} has no connectivity (call a connector)")
         post_rank, row_ptr, cols, w = proj.csr_population_ranks()
+        post_rank, row_ptr, cols, w, keep_syn = self._local_rows(proj, post_rank, row_ptr, cols, w)
         rows = int(post_rank.size)
         nnz = int(cols.size)
         idx_t = "int" if nnz < 2**31 - 1 else "long long"
@@ -535,7 +582,8 @@ class CompiledNetwork:
                 nat.create(f"proj{k}__row_of", row_of)
             # warp per post row: exact order, per-synapse delays, and plastic
             # delayed projections (the spike lists hold only the last step)
-            gather = self.exact or proj._delay_steps is not None or (proj.plastic and proj.max_delay > 1)
+            gather = self.exact or proj._delay_steps is not None or (
+                proj.plastic and (proj.max_delay > 1 or not self.spike_lists))
             if gather:
                 lay["grid"] = grid_for(rows * 32)
             elif proj.plastic:
@@ -544,15 +592,16 @@ class CompiledNetwork:
                 lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
             if proj.plastic:
                 nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
+                host = {name: np.asarray(arr)[keep_syn] for name, arr in proj._host_attr.items()}
                 if self._trace_dtype(proj) is not None:
                     # w and the traces in one record per synapse (float32)
                     nat.free(f"proj{k}__w")
-                    nat.create(f"proj{k}__tr", self._trace_init(proj, nnz, {**proj._host_attr, "w": w}))
+                    nat.create(f"proj{k}__tr", self._trace_init(proj, nnz, {**host, "w": w}))
                 else:
                     if self.wdtype is not np.float64 and not self.exact:
                         # plastic weights stay float32 (they are updated every event)
                         nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
-                    for name, arr in proj._host_attr.items():
+                    for name, arr in host.items():
                         nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
                     nat.create(f"proj{k}___last_event", np.full(nnz, -10000, dtype=np.int64))
         self.layout[k] = lay
@@ -582,6 +631,8 @@ class CompiledNetwork:
         nat.create(f"mon{m}__start", np.array([mon._start_step], dtype=np.int64))
         if "spike" in mon.variables:
             nat.create_empty(f"mon{m}__spk", np.uint32, (cap_steps, words))
+            if self.shard:                # only the owned words are ever written
+                nat.fill(f"mon{m}__spk", np.uint32(0))
         if mon.ranks is not None:
             nat.create(f"mon{m}__ranks", np.asarray(mon.ranks, dtype=np.int32))
         for v in mon.variables:
@@ -603,11 +654,33 @@ class CompiledNetwork:
         while left > 0:
             n = min(left, cap)
             starts = self.begin_chunk(t)
-            nat.run(n)
+            if self.shard:
+                for s in range(n):            # one step, then the spike exchange
+                    nat.run(1)
+                    self._exchange_spikes(t + s)
+            else:
+                nat.run(n)
             nat.synchronize()
             self.end_chunk(t, n, starts)
             t += n
             left -= n
+
+    def _exchange_spikes(self, t):
+        """Every rank's bitmap words of step t into every rank's bitmap."""
+        from .shard import chunk_words
+        rank, world = (int(x) for x in self.shard)
+        for pop in self.net.populations:
+            words = (pop.size + 31) // 32
+            c = chunk_words(pop.size, world)
+            slot = t % self.slots.get(pop.id, 1)
+            name = f"pop{pop.id}__spk"
+            first = min(words, c * rank)
+            local = np.zeros(c, dtype=np.uint32)
+            cnt = min(words, first + c) - first
+            if cnt > 0:
+                local[:cnt] = self.native.read(name, count=cnt, offset=slot * words + first)
+            full = self._exchange.all_gather(local)[:words]
+            self.native.write(name, full, offset_bytes=slot * words * 4)
 
     def begin_chunk(self, t):
         """Point every monitor's device ring at step t (a chunk of at most

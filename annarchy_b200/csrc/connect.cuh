@@ -42,7 +42,8 @@ __device__ __forceinline__ unsigned short anb_from_double<unsigned short>(double
 }
 
 template <typename W>
-__global__ void anb_fixed_number_pre_kernel(int n_post, int post_base, int pre_lo, int pre_hi,
+__global__ void anb_fixed_number_pre_kernel(int n_post, int post_base, long long row_offset,
+                                            int pre_lo, int pre_hi,
                                             int number, unsigned long long seed, int wkind,
                                             double a, double b, int exclude_self,
                                             int* __restrict__ post_rank, int* __restrict__ row_ptr,
@@ -52,20 +53,21 @@ __global__ void anb_fixed_number_pre_kernel(int n_post, int post_base, int pre_l
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const long long row = e / number;
+    const long long grow = row_offset + row;                  // row of the whole projection
     const int k = (int)(e - row * number);
     const int s0 = pre_lo + (int)floor(k * width);
     int s1 = pre_lo + (int)floor((k + 1) * width);
     if (s1 <= s0) s1 = s0 + 1;
-    int pre = s0 + (int)(anb_u01(seed, row, k, 0) * (s1 - s0));
+    int pre = s0 + (int)(anb_u01(seed, grow, k, 0) * (s1 - s0));
     if (pre >= s1) pre = s1 - 1;
     const int post = post_base + (int)row;
     if (exclude_self && pre == post) pre = (pre + 1 < s1) ? pre + 1 : (pre - 1 >= s0 ? pre - 1 : pre);
     col[e] = pre;
     double v = a;
     if (wkind == 1) {
-      v = a + (b - a) * anb_u01(seed, row, k, 1);
+      v = a + (b - a) * anb_u01(seed, grow, k, 1);
     } else if (wkind == 2) {                                // Box-Muller
-      const double u1 = 1.0 - anb_u01(seed, row, k, 1), u2 = anb_u01(seed, row, k, 2);
+      const double u1 = 1.0 - anb_u01(seed, grow, k, 1), u2 = anb_u01(seed, grow, k, 2);
       v = a + b * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
     }
     w[e] = anb_from_double<W>(v);
@@ -203,7 +205,15 @@ int anb_connect_fixed_number_pre(anb_net* net, const char* prefix, int n_post, i
                                  int pre_lo, int pre_hi, int number, uint64_t seed,
                                  int weight_kind, double a, double b, int weight_bytes,
                                  int exclude_self) {
-  if (!net || !prefix) return fail(ANB_ERR_ARG, "NULL argument");
+  return anb_connect_fixed_number_pre_rows(net, prefix, n_post, post_base, 0, pre_lo, pre_hi, number,
+                                           seed, weight_kind, a, b, weight_bytes, exclude_self);
+}
+
+int anb_connect_fixed_number_pre_rows(anb_net* net, const char* prefix, int n_post, int post_base,
+                                      long long row_offset, int pre_lo, int pre_hi, int number,
+                                      uint64_t seed, int weight_kind, double a, double b,
+                                      int weight_bytes, int exclude_self) {
+  if (!net || !prefix || row_offset < 0) return fail(ANB_ERR_ARG, "NULL argument or negative row offset");
   if (n_post <= 0 || number <= 0 || pre_hi - pre_lo < number || weight_kind < 0 || weight_kind > 2)
     return fail(ANB_ERR_ARG, "bad fixed_number_pre arguments");
   const long long nnz = (long long)n_post * number;
@@ -224,15 +234,15 @@ int anb_connect_fixed_number_pre(anb_net* net, const char* prefix, int n_post, i
   const unsigned g = grid_of(nnz);
   if (weight_bytes == 8)
     anb_fixed_number_pre_kernel<double><<<g, 256, 0, net->stream>>>(
-        n_post, post_base, pre_lo, pre_hi, number, seed, weight_kind, a, b, exclude_self, pr, rp, cl,
+        n_post, post_base, row_offset, pre_lo, pre_hi, number, seed, weight_kind, a, b, exclude_self, pr, rp, cl,
         (double*)w);
   else if (weight_bytes == 4)
     anb_fixed_number_pre_kernel<float><<<g, 256, 0, net->stream>>>(
-        n_post, post_base, pre_lo, pre_hi, number, seed, weight_kind, a, b, exclude_self, pr, rp, cl,
+        n_post, post_base, row_offset, pre_lo, pre_hi, number, seed, weight_kind, a, b, exclude_self, pr, rp, cl,
         (float*)w);
   else
     anb_fixed_number_pre_kernel<unsigned short><<<g, 256, 0, net->stream>>>(
-        n_post, post_base, pre_lo, pre_hi, number, seed, weight_kind, a, b, exclude_self, pr, rp, cl,
+        n_post, post_base, row_offset, pre_lo, pre_hi, number, seed, weight_kind, a, b, exclude_self, pr, rp, cl,
         (unsigned short*)w);
   ANB_CUDA(cudaGetLastError());
   ANB_CUDA(cudaStreamSynchronize(net->stream));

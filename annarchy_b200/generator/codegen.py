@@ -471,10 +471,14 @@ class CodeGenerator:
         }}{ballot}
       }}
     }}"""
+        first = 0
         if local_engine:
             loop = "for (int anb_base = 0; anb_base < anb_n; anb_base += blockDim.x)"
         else:
-            loop = ("for (int anb_base = blockIdx.x * blockDim.x; anb_base < anb_n; "
+            # a sharded network updates the owned slice [first, anb_n) only
+            if grid_path and pop.id in getattr(self.c, "owned", {}):
+                first, size = self.c.owned[pop.id]
+            loop = (f"for (int anb_base = {first} + blockIdx.x * blockDim.x; anb_base < anb_n; "
                     "anb_base += gridDim.x * blockDim.x)")
         return f"""
     {{  // population {pop.name}: update{' and spike gather' if spiking else ''}
@@ -954,7 +958,8 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
                     plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))
             elif self.has_update(pop):
                 kernels.append(self.pop_kernel(pop))
-                plan.append((f"pop{pop.id}_step", grid_for(pop.size), BLOCK, 0))
+                lo, hi = getattr(self.c, "owned", {}).get(pop.id, (0, pop.size))
+                plan.append((f"pop{pop.id}_step", grid_for(max(1, hi - lo)), BLOCK, 0))
             elif pop.neuron_type.type == "rate" and self.slots(pop) > 1:
                 kernels.append(self.delay_kernel(pop))
                 plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))

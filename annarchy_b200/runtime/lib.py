@@ -42,6 +42,9 @@ SIGNATURES = {
     "anb_connect_fixed_number_pre": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int,
                                                C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_double,
                                                C.c_double, C.c_int, C.c_int]),
+    "anb_connect_fixed_number_pre_rows": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_longlong,
+                                                    C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
+                                                    C.c_double, C.c_double, C.c_int, C.c_int]),
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
@@ -298,12 +301,12 @@ class NativeNet:
                                                        v.ctypes.data_as(C.c_void_p), v.nbytes))
 
     def connect_fixed_number_pre(self, prefix, n_post, post_base, pre_lo, pre_hi, number, seed,
-                                 weight_kind, a, b, weight_dtype, exclude_self):
+                                 weight_kind, a, b, weight_dtype, exclude_self, row_offset: int = 0):
         wb = {np.dtype(np.float64): 8, np.dtype(np.float32): 4, np.dtype(np.uint16): 2}[
             np.dtype(weight_dtype)]
-        check("anb_connect_fixed_number_pre", self.lib.anb_connect_fixed_number_pre(
-            self.h, prefix.encode(), n_post, post_base, pre_lo, pre_hi, number, seed, weight_kind,
-            float(a), float(b), wb, 1 if exclude_self else 0))
+        check("anb_connect_fixed_number_pre_rows", self.lib.anb_connect_fixed_number_pre_rows(
+            self.h, prefix.encode(), n_post, post_base, int(row_offset), pre_lo, pre_hi, number, seed,
+            weight_kind, float(a), float(b), wb, 1 if exclude_self else 0))
         nnz = n_post * number
         self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n_post,))
         self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))
@@ -410,7 +413,7 @@ class DryNative:
         pass
 
     def connect_fixed_number_pre(self, prefix, n_post, post_base, pre_lo, pre_hi, number, seed,
-                                 weight_kind, a, b, weight_dtype, exclude_self):
+                                 weight_kind, a, b, weight_dtype, exclude_self, row_offset: int = 0):
         nnz = n_post * number
         self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n_post,))
         self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))

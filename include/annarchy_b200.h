@@ -123,6 +123,15 @@ int anb_connect_fixed_number_pre(anb_net* net, const char* prefix, int n_post, i
                                  int pre_lo, int pre_hi, int number, uint64_t seed,
                                  int weight_kind, double a, double b, int weight_bytes,
                                  int exclude_self);
+/* As anb_connect_fixed_number_pre for rows row_offset .. row_offset + n_post
+ * - 1 of a projection whose rows start at post rank post_base - row_offset:
+ * the same synapses the whole projection would get for those rows (the
+ * random draws are keyed by the projection's row), so a rank can build its
+ * share of rows alone. No counterpart in the reference. */
+int anb_connect_fixed_number_pre_rows(anb_net* net, const char* prefix, int n_post, int post_base,
+                                      long long row_offset, int pre_lo, int pre_hi, int number,
+                                      uint64_t seed, int weight_kind, double a, double b,
+                                      int weight_bytes, int exclude_self);
 
 /* Pre-major view of a projection's CSR arrays (the reference's CSRC,
  * ANNarchy/include/CSRCMatrix.hpp:164-222): "<prefix>__col_ptr" over the n_pre
