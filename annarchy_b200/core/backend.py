@@ -388,6 +388,9 @@ class CompiledNetwork:
             nat.create(f"pop{pop.id}__{name}", np.asarray(arr, dtype=dt).reshape(-1))
         for name in compensated_vars(pop, self.exact, self.net._config):
             nat.create(f"pop{pop.id}__kc_{name}", np.zeros(pop.size, dtype=self.real))
+        if pop.neuron_type.type == "rate":
+            for t in pop.targets:         # the last step's weighted sums (Population.sum)
+                nat.create(f"pop{pop.id}___last_sum_{t}", np.zeros(pop.size, dtype=self.real))
         if hasattr(pop, "_ta_schedule_ms"):
             self.write_timed_array(pop)
         R = self.slots.get(pop.id, 1)
@@ -766,6 +769,7 @@ class CompiledNetwork:
             nat.fill(f"pop{k}__kc_{name}", self.real(0))
         for t in pop.targets if pop.neuron_type.type == "rate" else []:
             nat.fill(f"pop{k}___sum_{t}", self.real(0))
+            nat.fill(f"pop{k}___last_sum_{t}", self.real(0))
         R = self.slots.get(k, 1)
         if pop.neuron_type.type == "rate" and R > 1:
             nat.write(f"pop{k}___delayed_r", self._ring_of(pop, self.read_population_attribute(pop, "r")))

@@ -155,6 +155,18 @@ class Population:
                 if attributes is None or p["name"] in attributes:
                     self._host[p["name"]] = self._initial(p)
 
+    def sum(self, target: str):
+        """Weighted sum of the inputs on `target` computed in the last step
+        (rate-coded populations; ANNarchy/core/Population.py, sum)."""
+        if self.neuron_type.type != "rate":
+            raise NotImplementedError("sum(target) is available for rate-coded populations")
+        if target not in self.targets:
+            raise ValueError(f"population {self.name!r} has no target {target!r}")
+        if not self._compiled():
+            return np.zeros(self.geometry if len(self.geometry) > 1 else self.size)
+        arr = self.net._backend.native.read(f"pop{self.id}___last_sum_{target}").astype(np.float64)
+        return arr.reshape(self.geometry) if len(self.geometry) > 1 else arr
+
     def save(self, filename: str):
         """Every parameter and variable into a file (.npz, .gz, .mat or
         pickle), in the reference's layout (Population.py:1000-1066)."""

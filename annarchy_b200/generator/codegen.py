@@ -354,6 +354,7 @@ class CodeGenerator:
             def gsrc(name):
                 return self.ptr(f"pop{k}__{name}")
 
+        grid_path = not smem and cluster is None and not local_engine
         loads, stores = [], []
         sidx = "anb_q" if cluster is not None else "anb_i"
         for name in names:
@@ -380,6 +381,9 @@ class CodeGenerator:
                 src = gsrc("_sum_" + t)
                 loads.append(f"const {self.real} _sum_{t} = {src}[anb_i];")
                 stores.append(f"{src}[anb_i] = ({self.real})0;")
+                if grid_path:
+                    # kept for Population.sum(target) (the sums are consumed here)
+                    stores.append(f"{gsrc('_last_sum_' + t)}[anb_i] = _sum_{t};")
         spike_code = ""
         if spiking:
             rr_src = smem["refractory_remaining"] if smem else gsrc("refractory_remaining")
@@ -411,7 +415,6 @@ class CodeGenerator:
           {gsrc('last_spike')}[anb_i] = t;
           {refr_set}
         }}"""
-        grid_path = not smem and cluster is None and not local_engine
         if spiking and ballot_hook is None:
             spk_dst = smem.get("spk") if smem else (self.spk_at(pop, "t") if grid_path else gsrc("spk"))
         else:
