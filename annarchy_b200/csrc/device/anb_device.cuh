@@ -570,18 +570,16 @@ __device__ __forceinline__ void anb_rate_coo_atomic(int nnz, const int* __restri
   }
 }
 
-// ---- panelled CSR (fast mode) -------------------------------------------------------
+// ---- panelled sliced ELL (fast mode) ------------------------------------------------
 // The pre-synaptic columns are cut into panels of at most `panel_width`
-// neurons; each panel is a CSR over all rows with 16-bit column indices
-// relative to the panel. One CTA owns rows [r0, r1) of one panel: it copies
-// the panel's rates into shared memory with bulk (TMA) copies, then streams
-// the contiguous synapse range of its rows in aligned 8-synapse chunks (one
-// 16-byte index load and 32 or 16 bytes of weights per thread and chunk), so
-// the gathers hit shared memory and every load of the matrix is a full
-// 16-byte vector. The first row of every chunk comes from a per-chunk table;
-// row boundaries inside a chunk from the CTA's row pointers staged in shared
-// memory. Partial row sums are added in shared memory, then into the global
-// sums (atomically when the projection has several panels).
+// neurons (16-bit column indices relative to the panel). Within a panel the
+// rows are sorted by their number of synapses there and cut into slices of 32
+// rows stored as steps of 32 elements, one per row: a header step naming the
+// rows, then element k of every row at step k + 1. A CTA copies its panel's
+// rates into shared memory with bulk (TMA) copies; each warp then streams a
+// contiguous range of steps, one row per lane, loading the next chunk of U
+// steps while it sums the current one, and adds its partial sum to the row's
+// global sum where a slice (or its range) ends.
 
 // Issue bulk copies of `bytes` (a multiple of 16, both addresses 16-byte
 // aligned) from global memory into this CTA's shared memory, completing on
@@ -636,93 +634,82 @@ __device__ __forceinline__ void anb_w8(const anb_bf16* w, float* o) {
   }
 }
 
-// cta_tab[4 * blockIdx.x ...] = (panel, r0, r1, first entry of the CTA in
-// crow); row_ptr: n_panels x (n_rows + 1) absolute offsets into col/w (both
-// padded by at least 8 entries past the last synapse); crow: for each chunk
-// of the CTA, the row (relative to r0) of its first synapse in the CTA's
-// range. Dynamic shared memory: panel_width floats, then max_rows + 1 ints of
-// row pointers and max_rows floats of row sums.
-template <typename W>
-__device__ __forceinline__ void anb_rate_pcsr(const int* __restrict__ cta_tab,
-                                              const int* __restrict__ row_ptr, int n_rows,
-                                              const unsigned short* __restrict__ crow,
+// Sum index of a header entry (column c, weight slot read as wv): the entry
+// stores v = index + 1 (0 for a padding lane) as column 0xF000 | (v >> 16)
+// and the weight slot's bits v (32-bit weights) or v & 0xffff (bfloat16).
+__device__ __forceinline__ int anb_pc_row(unsigned c, float wv, const float*) {
+  return __float_as_int(wv) - 1;
+}
+__device__ __forceinline__ int anb_pc_row(unsigned c, float wv, const anb_bf16*) {
+  return (int)(((c & 0xfffu) << 16) | (__float_as_uint(wv) >> 16)) - 1;
+}
+
+// cta_panel[blockIdx.x]: the CTA's panel; warp_tab[3 * (blockIdx.x * warps
+// + warp) ...] = (first step, end step, header step of the slice holding the
+// first step); col / w: 32 entries per step, columns from 0xF000 on marking
+// header steps. Dynamic shared memory: panel_width floats.
+template <typename W, int U>
+__device__ __forceinline__ void anb_rate_pcsr(const int* __restrict__ cta_panel,
+                                              const int* __restrict__ warp_tab,
                                               const unsigned short* __restrict__ col,
                                               const W* __restrict__ w,
                                               const float* __restrict__ x, int n_pre,
-                                              int panel_width, int max_rows,
-                                              const int* __restrict__ post_rank,
-                                              float* __restrict__ sum, int atomic, int* err) {
+                                              int panel_width, float* __restrict__ sum, int* err) {
   extern __shared__ __align__(16) unsigned char anb_pc_smem[];
   __shared__ __align__(8) unsigned long long anb_pc_mbar;
   float* xs = reinterpret_cast<float*>(anb_pc_smem);
-  int* rps = reinterpret_cast<int*>(anb_pc_smem + 4 * panel_width);
-  float* acc = reinterpret_cast<float*>(rps + max_rows + 1);
-  const int* tab = cta_tab + 4 * blockIdx.x;
-  const int p = tab[0], r0 = tab[1], r1 = tab[2], cr0 = tab[3];
-  const int nr = r1 - r0;
+  const int p = cta_panel[blockIdx.x];
   const int c0 = p * panel_width;
   const int cw = min(panel_width, n_pre - c0);
   const int cw4 = cw & ~3;
-  const int* __restrict__ rp = row_ptr + (long long)p * (n_rows + 1) + r0;
-  const int beg = rp[0], end = rp[nr];
   if (threadIdx.x == 0 && cw4 > 0) anb_bulk_issue(xs, x + c0, 4u * (unsigned)cw4, &anb_pc_mbar);
-  for (int q = threadIdx.x; q <= nr; q += blockDim.x) rps[q] = rp[q];
-  for (int q = threadIdx.x; q < nr; q += blockDim.x) acc[q] = 0.f;
   for (int q = cw4 + threadIdx.x; q < cw; q += blockDim.x) xs[q] = x[c0 + q];
-  const int a0 = beg & ~7;
-  // first chunk of this thread, loaded while the panel copy is in flight
-  int j0 = a0 + 8 * (int)threadIdx.x;
-  uint4 cv = make_uint4(0u, 0u, 0u, 0u);
-  float wv[8];
-  int row = 0;
-  if (j0 < end) {
-    cv = anb_ls_u4(reinterpret_cast<const uint4*>(col + j0));
-    anb_w8(w + j0, wv);
-    row = crow[cr0 + (j0 - a0) / 8];
-  }
-  __syncthreads();                                   // mbarrier, rps, acc published
-  if (cw4 > 0) anb_bulk_wait(&anb_pc_mbar, err);
-  while (j0 < end) {
-    // next chunk of this thread in flight while this one is summed
-    const int jn = j0 + 8 * (int)blockDim.x;
-    uint4 cn = make_uint4(0u, 0u, 0u, 0u);
-    float wn[8];
-    int rown = 0;
-    if (jn < end) {
-      cn = anb_ls_u4(reinterpret_cast<const uint4*>(col + jn));
-      anb_w8(w + jn, wn);
-      rown = crow[cr0 + (jn - a0) / 8];
-    }
-    const anb_u32 cq[4] = {cv.x, cv.y, cv.z, cv.w};
-    int nxt = rps[row + 1];                          // start of the next row
-    float s = 0.f;
+  const int lane = threadIdx.x & 31;
+  const int* wt = warp_tab + 3 * (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+  const int sb = wt[0], se = wt[1], hd = wt[2];
+  const unsigned short* cp = col + 32ll * sb + lane;
+  const W* wp = w + 32ll * sb + lane;
+  unsigned short ca[U], cb[U];
+  float wa[U], wb[U];
+  // the U steps from step j (zeros past the range)
+  auto load = [&](unsigned short (&c)[U], float (&wv)[U], const int j) {
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int j = j0 + e;
-      if (j < beg || j >= end) continue;
-      if (j >= nxt) {                                // the chunk enters the next row(s)
-        atomicAdd(&acc[row], s);
-        s = 0.f;
-        do { ++row; nxt = rps[row + 1]; } while (j >= nxt);
+    for (int u = 0; u < U; ++u) {
+      const bool in = j + u < se;
+      const long long o = 32ll * (j - sb + u);
+      c[u] = in ? anb_ls_h(cp + o) : (unsigned short)0;
+      wv[u] = in ? anb_w1(wp + o) : 0.f;
+    }
+  };
+  float acc = 0.f;
+  int cur = -1;                                      // sum index of the lane's current row
+  auto consume = [&](const unsigned short (&c)[U], const float (&wv)[U], const int j) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (j + u < se) {
+        if (c[u] >= 0xf000u) {                       // header: the previous slice ends
+          if (cur >= 0) atomicAdd(&sum[cur], acc);
+          acc = 0.f;
+          cur = anb_pc_row(c[u], wv[u], w);
+        } else {
+          acc += xs[c[u]] * wv[u];
+        }
       }
-      const unsigned c = (e & 1) ? (cq[e >> 1] >> 16) : (cq[e >> 1] & 0xffffu);
-      s += xs[c] * wv[e];
     }
-    atomicAdd(&acc[row], s);
-    j0 = jn;
-    cv = cn;
-    row = rown;
-#pragma unroll
-    for (int e = 0; e < 8; ++e) wv[e] = wn[e];
+  };
+  if (sb < se) {                                     // in flight during the panel copy
+    load(ca, wa, sb);
+    if (hd < sb) cur = anb_pc_row(anb_ls_h(col + 32ll * hd + lane), anb_w1(w + 32ll * hd + lane), w);
   }
-  __syncthreads();
-  for (int q = threadIdx.x; q < nr; q += blockDim.x) {
-    if (rps[q + 1] > rps[q]) {
-      const int post = post_rank ? post_rank[r0 + q] : r0 + q;
-      if (atomic) atomicAdd(&sum[post], acc[q]);
-      else sum[post] += acc[q];
-    }
+  __syncthreads();                                   // mbarrier and tail rates published
+  if (cw4 > 0) anb_bulk_wait(&anb_pc_mbar, err);
+  for (int j = sb; j < se; j += 2 * U) {
+    load(cb, wb, j + U);
+    consume(ca, wa, j);
+    load(ca, wa, j + 2 * U);
+    consume(cb, wb, j + U);
   }
+  if (cur >= 0) atomicAdd(&sum[cur], acc);
 }
 
 // ---- event-driven transmission -----------------------------------------------------

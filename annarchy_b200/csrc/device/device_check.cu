@@ -35,13 +35,13 @@ extern "C" __global__ void check_spike_scatter(const anb_u32* spk, const int* cp
                                                const anb_bf16* w, float* g) {
   anb_spike_scatter<float, anb_bf16>(0, 128, spk, cp, pi, w, g);
 }
-extern "C" __global__ void __launch_bounds__(1024, 2) check_rate_pcsr_f32(
-    const int* tab, const int* rp, int rows, const unsigned short* cr, const unsigned short* c, const float* w,
-    const float* x, int n_pre, int pw, int mr, const int* pr, float* s, int* err) {
-  anb_rate_pcsr<float>(tab, rp, rows, cr, c, w, x, n_pre, pw, mr, pr, s, 1, err);
+extern "C" __global__ void __launch_bounds__(384, 3) check_rate_pcsr_f32(
+    const int* cp, const int* wt, const unsigned short* c, const float* w, const float* x, int n_pre,
+    int pw, float* s, int* err) {
+  anb_rate_pcsr<float, 5>(cp, wt, c, w, x, n_pre, pw, s, err);
 }
-extern "C" __global__ void __launch_bounds__(1024, 2) check_rate_pcsr_bf16(
-    const int* tab, const int* rp, int rows, const unsigned short* cr, const unsigned short* c, const anb_bf16* w,
-    const float* x, int n_pre, int pw, int mr, const int* pr, float* s, int* err) {
-  anb_rate_pcsr<anb_bf16>(tab, rp, rows, cr, c, w, x, n_pre, pw, mr, pr, s, 1, err);
+extern "C" __global__ void __launch_bounds__(384, 3) check_rate_pcsr_bf16(
+    const int* cp, const int* wt, const unsigned short* c, const anb_bf16* w, const float* x, int n_pre,
+    int pw, float* s, int* err) {
+  anb_rate_pcsr<anb_bf16, 5>(cp, wt, c, w, x, n_pre, pw, s, err);
 }

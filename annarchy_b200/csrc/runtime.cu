@@ -846,7 +846,9 @@ static int resolve(anb_net* net, const char* kernel, unsigned grid, unsigned blo
   l.smem = smem;
   CUresult r = g_drv.moduleGetFunction(&l.fn, net->module, kernel);
   if (r != CUDA_SUCCESS) return fail(ANB_ERR_ARG, std::string("kernel not found: ") + kernel);
-  if (smem > 48 * 1024)
+  // the 48 KB default covers static and dynamic shared memory together:
+  // opt in whenever the dynamic part comes near it
+  if (smem > 32 * 1024)
     ANB_CU(g_drv.funcSetAttribute(l.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
   *out = l;
   return ANB_OK;

@@ -592,14 +592,13 @@ extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
                     f"{p('post_rank')}, {sum_});")
             return kern(name, call), [(name, grid_for(lay["rows"]), BLOCK, 0)]
         if fmt == "pcsr" and not self.exact:
-            pw, mr = lay["panel_width"], lay["pc_max_rows"]
-            smem = 4 * pw + 4 * (mr + 1) + 4 * mr
-            call = (f"anb_rate_pcsr<{W}>({p('pc_cta')}, {p('pc_row_ptr')}, {lay['rows']}, "
-                    f"{p('pc_crow')}, {p('pc_col')}, {p('pc_w')}, {pre_r}, {proj.pre_pop.size}, {pw}, {mr}, "
-                    f"{p('post_rank')}, {sum_}, {1 if lay['n_panels'] > 1 else 0}, {self.ptr('err')});")
+            pw = lay["panel_width"]
+            call = (f"anb_rate_pcsr<{W}, {lay['pc_unroll']}>({p('pc_cta')}, {p('pc_warp')}, "
+                    f"{p('pc_col')}, {p('pc_w')}, {pre_r}, "
+                    f"{proj.pre_pop.size}, {pw}, {sum_}, {self.ptr('err')});")
             B = lay["pc_block"]
             return (kern(name, call, B, lay["pc_resident"]),
-                    [(name, lay["pc_ctas"], B, smem)])
+                    [(name, lay["pc_ctas"], B, 4 * pw)])
         if fmt in ("csr", "pcsr"):       # pcsr in double precision: CSR order
             if self.exact:
                 call = (f"anb_rate_csr_scalar<double, double, {lay['idx_t']}>({lay['rows']}, "

@@ -126,78 +126,126 @@ def hyb_width(row_ptr) -> int:
     return int(np.argmax(counts))
 
 
-PCSR_MAX_ROWS = 4096
+PCSR_HEADER = 0xF000       # column values from here on mark a slice's header step
 
 
-def pcsr_arrays(row_ptr, cols, w, n_pre, panel_width=16384, ctas=296, max_rows=PCSR_MAX_ROWS):
-    """Panelled CSR. Returns dict(row_ptr (n_panels x (rows+1), int32,
-    absolute offsets), col (uint16, relative to the panel), w (float64,
-    reordered), cta_tab ((n_cta, 4) int32: panel, first row, end row, first
-    entry in crow), crow (uint16: for each aligned 8-synapse chunk
-    overlapping a CTA's synapse range, the row of its first synapse in the
-    range, relative to the CTA's first row), n_panels, panel_width).
-    Synapse arrays are padded by 8 zero entries past a multiple of 8. Each
-    panel gets CTAs in proportion to its synapses, and a CTA's rows are cut
-    where the cumulative synapse count crosses the panel's per-CTA share
-    (and after max_rows rows, at most 65535)."""
+def pcsr_arrays(row_ptr, cols, w, n_pre, post_rank=None, panel_width=16384, ctas=444,
+                warps=16):
+    """Panelled sliced ELL (the backend's single-precision schedule).
+
+    The pre-synaptic columns are cut into panels of `panel_width` neurons
+    (16-bit column indices relative to the panel, below PCSR_HEADER). Within
+    a panel the rows that have synapses there are sorted by their count there
+    (longest first) and cut into slices of 32 rows. A slice is stored as
+    steps of 32 elements, one per row: a header step naming the rows, then
+    element k of every row at step k + 1 (column 0 and weight 0 past a row's
+    end). The header's entry for lane l holds v = post_rank[row] + 1 (0 for a
+    padding lane): its column is PCSR_HEADER | (v >> 16), its weight slot
+    the bits of v (32-bit weights) or of v & 0xffff (16-bit weights). The
+    steps of all panels form one array. Every panel gets CTAs in proportion
+    to its steps, every CTA an equal range of the panel's steps and every
+    warp of it an equal part of that range, wherever slices begin or end.
+
+    Returns dict(col uint16 and w float64 (32 per step; header weights 0),
+    header (step indices of the headers), header_val (int64, 32 per header:
+    v), cta_panel (int32 per CTA), warp_tab ((CTAs x warps, 3) int32: first
+    step, end step, header step of the slice holding the first step),
+    n_panels, panel_width, n_steps, padded (stored elements)).
+    """
     row_ptr = np.asarray(row_ptr, dtype=np.int64)
     cols = np.asarray(cols, dtype=np.int64)
+    w = np.asarray(w, dtype=np.float64)
     n_rows = row_ptr.size - 1
-    panel_width = int(max(32, min(panel_width, 65536)) // 32 * 32)
-    max_rows = int(min(max_rows, 65535))
+    post = np.arange(n_rows) if post_rank is None else np.asarray(post_rank, dtype=np.int64)
+    panel_width = int(max(32, min(panel_width, PCSR_HEADER)) // 32 * 32)
     n_panels = max(1, -(-int(n_pre) // panel_width))
     rows_of = np.repeat(np.arange(n_rows, dtype=np.int64), np.diff(row_ptr))
-    panel = (cols // panel_width).astype(np.uint16)
-    # CSR order is row-major with ascending columns: a stable sort by panel
-    # gives panel, then row, then column
+    panel = cols // panel_width
+    # (panel, row) segments in CSR order: a stable sort by panel keeps the
+    # rows and their ascending columns
     order = np.argsort(panel, kind="stable")
-    counts = np.bincount(panel.astype(np.int64) * n_rows + rows_of,
+    counts = np.bincount(panel[order] * n_rows + rows_of[order],
                          minlength=n_panels * n_rows).reshape(n_panels, n_rows)
-    rp = np.zeros((n_panels, n_rows + 1), dtype=np.int64)
-    flat = np.cumsum(counts.reshape(-1))
-    starts = np.concatenate([[0], flat])            # start of (panel, row) segments
+    seg_start = np.concatenate([[0], np.cumsum(counts.reshape(-1))])
+    col_sorted = cols[order] - panel[order] * panel_width
+    w_sorted = w[order]
+    col_parts, w_parts, val_parts, head_parts, panel_steps = [], [], [], [], []
+    step0 = 0
     for p_ in range(n_panels):
-        rp[p_] = starts[p_ * n_rows: (p_ + 1) * n_rows + 1]
-    nnz = cols.size
-    pad = (-nnz) % 8 + 8
-    col16 = np.zeros(nnz + pad, dtype=np.uint16)
-    col16[:nnz] = (cols[order] - panel[order].astype(np.int64) * panel_width).astype(np.uint16)
-    wv = np.zeros(nnz + pad, dtype=np.float64)
-    wv[:nnz] = np.asarray(w, dtype=np.float64)[order]
-    per_panel = counts.sum(axis=1)
-    tab = []
-    for p_ in range(n_panels):
-        if per_panel[p_] == 0:
+        cnt = counts[p_]
+        rows = np.nonzero(cnt)[0]
+        if rows.size == 0:
+            panel_steps.append(0)
             continue
-        share = max(1, int(round(ctas * per_panel[p_] / max(nnz, 1))))
-        target = per_panel[p_] / share
-        cum = np.cumsum(counts[p_])
-        r0 = 0
-        while r0 < n_rows:
-            # next cut: where the panel's cumulative count reaches the next share
-            done = cum[r0 - 1] if r0 else 0
-            r1 = int(np.searchsorted(cum, done + target, side="left")) + 1
-            r1 = max(r0 + 1, min(r1, r0 + max_rows, n_rows))
-            if cum[r1 - 1] > done:
-                tab.append((p_, r0, r1))
-            r0 = r1
-    # per CTA: the row (relative to its first row) of the first synapse of
-    # each aligned 8-synapse chunk that overlaps its synapse range
-    full, crow = [], []
+        rows = rows[np.argsort(-cnt[rows], kind="stable")]          # longest first
+        ns = -(-rows.size // 32)
+        lane_rows = np.full(ns * 32, -1, dtype=np.int64)
+        lane_rows[:rows.size] = rows
+        lane_rows = lane_rows.reshape(ns, 32)
+        lens = np.where(lane_rows >= 0, cnt[np.maximum(lane_rows, 0)], 0)   # (ns, 32)
+        slen = lens.max(axis=1) + 1                                  # header + elements
+        head = np.concatenate([[0], np.cumsum(slen)[:-1]])
+        n = int(slen.sum())
+        s_idx = np.repeat(np.arange(ns), slen)
+        k_idx = np.arange(n) - np.repeat(head, slen) - 1             # -1 on headers
+        valid = (k_idx[:, None] >= 0) & (k_idx[:, None] < lens[s_idx])
+        src = seg_start[p_ * n_rows + np.maximum(lane_rows[s_idx], 0)] + k_idx[:, None]
+        cpad = np.zeros((n, 32), dtype=np.int64)
+        wpad = np.zeros((n, 32), dtype=np.float64)
+        cpad[valid] = col_sorted[src[valid]]
+        wpad[valid] = w_sorted[src[valid]]
+        val = np.where(lane_rows >= 0, post[np.maximum(lane_rows, 0)] + 1, 0)   # (ns, 32)
+        cpad[head] = PCSR_HEADER | (val >> 16)
+        col_parts.append(cpad.reshape(-1))
+        w_parts.append(wpad.reshape(-1))
+        val_parts.append(val.reshape(-1))
+        head_parts.append(step0 + head)
+        panel_steps.append(n)
+        step0 += n
+    n_steps = step0
+    cat = lambda parts, dt: (np.concatenate(parts) if parts else np.zeros(0)).astype(dt)
+    col16 = cat(col_parts, np.uint16)
+    wv = cat(w_parts, np.float64)
+    header = cat(head_parts, np.int64)
+    # CTAs: per panel in proportion to its steps; warps: equal parts of a CTA
+    cta_panel, wtab = [], []
     base = 0
-    for p_, r0, r1 in tab:
-        seg = rp[p_, r0:r1 + 1]
-        beg, end = int(seg[0]), int(seg[-1])
-        a0 = beg & ~7
-        first = np.maximum(np.arange(a0, end, 8, dtype=np.int64), beg)
-        crow.append((np.searchsorted(seg, first, side="right") - 1).astype(np.uint16))
-        full.append((p_, r0, r1, base))
-        base += first.size
-    cta_tab = np.asarray(full, dtype=np.int64).reshape(-1, 4).astype(np.int32)
-    crow = np.concatenate(crow) if crow else np.zeros(0, np.uint16)
-    return {"row_ptr": rp.astype(np.int32).reshape(-1), "col": col16, "w": wv, "cta_tab": cta_tab,
-            "crow": np.concatenate([crow, np.zeros(8, np.uint16)]),
-            "n_panels": n_panels, "panel_width": panel_width}
+    for p_, n in enumerate(panel_steps):
+        if n == 0:
+            continue
+        k = max(1, int(round(ctas * n / max(n_steps, 1))))
+        edges = base + (n * np.arange(k + 1)) // k
+        for a, b in zip(edges[:-1], edges[1:]):
+            cta_panel.append(p_)
+            we = a + ((b - a) * np.arange(warps + 1)) // warps
+            wtab.append(np.stack([we[:-1], we[1:]], axis=1))
+        base += n
+    if not cta_panel:                                # no synapses: one idle CTA
+        cta_panel = [0]
+        wtab = [np.zeros((warps, 2), dtype=np.int64)]
+    wtab = np.concatenate(wtab)
+    at = np.maximum(np.searchsorted(header, wtab[:, 0], side="right") - 1, 0)
+    first_head = header[at] if header.size else np.zeros_like(at)
+    warp_tab = np.concatenate([wtab, first_head[:, None]], axis=1).astype(np.int32)
+    return {"col": np.concatenate([col16, np.zeros(8, np.uint16)]),
+            "w": np.concatenate([wv, np.zeros(8)]),
+            "header": header, "header_val": cat(val_parts, np.int64),
+            "cta_panel": np.asarray(cta_panel, dtype=np.int32), "warp_tab": warp_tab,
+            "n_panels": n_panels, "panel_width": panel_width, "n_steps": int(n_steps),
+            "padded": int(col16.size)}
+
+
+def pcsr_weights(d, W):
+    """The weight array of a pcsr layout in the device type (W converts
+    float64 weights to float32 or to bfloat16 bits), headers filled in."""
+    out = np.array(W(d["w"]))
+    idx = (32 * d["header"][:, None] + np.arange(32)[None, :]).reshape(-1)
+    v = d["header_val"]
+    if out.dtype == np.uint16:
+        out[idx] = (v & 0xFFFF).astype(np.uint16)
+    else:
+        out.view(np.uint32)[idx] = v.astype(np.uint32)
+    return out
 
 
 def bsr_arrays(post_rank, row_ptr, cols, w, n_pre, tile):
@@ -310,21 +358,24 @@ def create_format_arrays(compiled, proj, fmt, post_rank, row_ptr, cols, w, lay):
             return
         cfg = proj.net._config
         pw = int(cfg.get("pcsr_panel", 16384))
-        mr = int(cfg.get("pcsr_rows", PCSR_MAX_ROWS))
         sms = int(cfg.get("sm_count", 148))
-        d = pcsr_arrays(row_ptr, cols, w, proj.pre_pop.size, panel_width=pw,
-                        ctas=int(cfg.get("pcsr_ctas", 2 * sms)), max_rows=mr)
-        nat.create(f"proj{k}__pc_row_ptr", d["row_ptr"])
+        block = int(cfg.get("pcsr_block", 384))
+        pw = max(32, min(pw, PCSR_HEADER)) // 32 * 32
+        resident = max(1, min(2048 // block, (228 * 1024) // (4 * pw + 1024 + 64)))
+        # steps per chunk (two chunks in flight): what the launch's registers allow
+        regs = 65536 // (block * resident) // 8 * 8
+        unroll = int(cfg.get("pcsr_unroll", max(2, min(16, (regs - 26) // 6))))
+        d = pcsr_arrays(row_ptr, cols, w, proj.pre_pop.size, post_rank=post_rank, panel_width=pw,
+                        ctas=int(cfg.get("pcsr_ctas", resident * sms)), warps=block // 32)
+        if d["padded"] >= 2 ** 31 - 64 or post_rank.size and int(np.max(post_rank)) >= 2 ** 28 - 2:
+            raise ValueError(f"{proj.name}: too many synapses or neurons for the pcsr format")
         nat.create(f"proj{k}__pc_col", d["col"])
-        nat.create(f"proj{k}__pc_w", W(d["w"]))
-        nat.create(f"proj{k}__pc_cta", d["cta_tab"].reshape(-1))
-        nat.create(f"proj{k}__pc_crow", d["crow"])
-        block = int(cfg.get("pcsr_block", 1024))
-        smem = 4 * d["panel_width"] + 8 * mr + 4
-        resident = max(1, min(2048 // block, (228 * 1024) // (smem + 1024)))
+        nat.create(f"proj{k}__pc_w", pcsr_weights(d, W))
+        nat.create(f"proj{k}__pc_cta", d["cta_panel"])
+        nat.create(f"proj{k}__pc_warp", d["warp_tab"].reshape(-1))
         lay.update(n_panels=d["n_panels"], panel_width=d["panel_width"],
-                   pc_ctas=int(d["cta_tab"].shape[0]), pc_max_rows=mr, pc_block=block,
-                   pc_resident=resident)
+                   pc_ctas=int(d["cta_panel"].size), pc_block=block, pc_resident=resident,
+                   pc_unroll=unroll)
     else:
         raise ValueError(f"unknown format {fmt!r}")
 
