@@ -23,10 +23,11 @@ then the tail of a row (the reference's HYB differs from CSR the same way).
 This backend adds one schedule of its own, without a counterpart among the
 reference's containers:
 
-* PCSR  (panelled CSR, single precision only): the pre-synaptic columns cut
-        into panels that fit in one CTA's shared memory, one CSR per panel
-        with 16-bit column indices, and a table assigning each CTA a row
-        range of one panel with about the same number of synapses. In double
+* PCSR  (panelled sliced ELL, single precision only): the pre-synaptic
+        columns cut into panels that fit in one CTA's shared memory (16-bit
+        column indices), the rows of each panel sorted by length and stored
+        in 32-row column-major slices, each behind a header step naming its
+        rows; CTAs and warps take equal step ranges (pcsr_arrays). In double
         precision a PCSR projection is summed as CSR (ascending pre rank).
 """
 from __future__ import annotations
