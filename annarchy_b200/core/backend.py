@@ -418,7 +418,8 @@ class CompiledNetwork:
         return names
 
     def _create_device_projection(self, proj):
-        """Fixed in-degree projection generated on the device."""
+        """Fixed in-degree or fixed-probability projection generated on the
+        device."""
         nat = self.native
         k = proj.id
         d = proj._device_conn
@@ -435,10 +436,22 @@ class CompiledNetwork:
         pre_lo, pre_hi = int(proj.pre_ranks[0]), int(proj.pre_ranks[-1]) + 1
         plastic = proj.plastic
         wdt = np.float64 if self.exact else (np.float32 if plastic else self.wdtype)
-        nat.connect_fixed_number_pre(f"proj{k}", npost, post0, pre_lo, pre_hi,
-                                     d["number"], d["seed"], d["wkind"], d["a"], d["b"], wdt,
-                                     d["exclude_self"], row_offset=row0)
-        nnz = npost * d["number"]
+        if d["kind"] == "fixed_number_pre":
+            nat.connect_fixed_number_pre(f"proj{k}", npost, post0, pre_lo, pre_hi,
+                                         d["number"], d["seed"], d["wkind"], d["a"], d["b"], wdt,
+                                         d["exclude_self"], row_offset=row0)
+            nnz = npost * d["number"]
+            lengths = np.full(npost, d["number"], dtype=np.int64)
+        else:
+            nnz = nat.connect_fixed_probability(f"proj{k}", npost, post0, pre_lo, pre_hi,
+                                                d["probability"], d["seed"], d["wkind"], d["a"],
+                                                d["b"], wdt, d["exclude_self"], row_offset=row0)
+            if isinstance(nat, DryNative):          # the expected in-degree
+                lengths = np.full(npost, -(-nnz // npost), dtype=np.int64)
+            else:
+                lengths = np.diff(nat.read(f"proj{k}__row_ptr").astype(np.int64))
+        proj._nnz = nnz
+        proj._device_lengths = lengths
         lay = {"rows": npost, "nnz": nnz, "idx_t": "int", "format": "csr", "device": True,
                "w0": pre_lo // 32, "w1": (pre_hi - 1) // 32 + 1}
         for prm in proj.desc["parameters"] + proj.desc["variables"]:
@@ -448,7 +461,7 @@ class CompiledNetwork:
             nat.csr_to_csc(f"proj{k}", proj.pre_pop.size, with_weights=not plastic)
         mean_fan = nnz / max(1, pre_hi - pre_lo)
         lay["chunks"] = max(1, -(-int(1.25 * mean_fan) // 32))
-        lay["post_chunks"] = max(1, -(-d["number"] // 32))
+        lay["post_chunks"] = max(1, -(-int(lengths.max() if lengths.size else 1) // 32))
         if plastic and self.spike_lists:
             row_of = np.full(proj.post_pop.size, -1, dtype=np.int32)
             row_of[post0:post0 + npost] = np.arange(npost, dtype=np.int32)

@@ -225,9 +225,23 @@ class Projection:
                           force_multiple_weights=False, storage_format=None, storage_order=None):
         """Each (post, pre) pair is connected independently with the given
         probability (per-post Bernoulli masks, as in the reference's
-        ANNarchy/cython_ext/Connector.pyx:306-345)."""
+        ANNarchy/cython_ext/Connector.pyx:306-345). Large projections (more
+        than 2e7 expected synapses, or device_connectors=True) are generated
+        on the device at compile() by geometric skipping
+        (anb_connect_fixed_probability_rows)."""
         rng = self._rng()
         npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
+        if 0.0 < probability <= 1.0 and self._device_ok(int(npost * npre * probability)):
+            self._device_conn = dict(kind="fixed_probability", probability=float(probability),
+                                     **self._device_weights(weights, delays),
+                                     seed=int(rng.integers(0, 2**63 - 1)),
+                                     exclude_self=(not allow_self_connections
+                                                   and self.pre_pop is self.post_pop))
+            self._nnz = int(round(npost * npre * probability))        # until compile()
+            self.connector_name = "Random (device)"
+            if storage_format is not None:
+                self._storage_format = storage_format
+            return self
         rows_l, cols_l = [], []
         for r0 in range(0, npost, 4096):
             r1 = min(npost, r0 + 4096)
@@ -253,6 +267,23 @@ class Projection:
             return True
         return mode == "auto" and nnz > 20_000_000 and contiguous
 
+    def _device_weights(self, weights, delays) -> dict:
+        """Weight law of a device connector: constant (wkind 0), Uniform (1)
+        or unbounded Normal (2); no synaptic delays."""
+        from .random import Normal, Uniform
+        if np.ndim(weights) == 0 and not hasattr(weights, "get_values"):
+            wk, a, b = 0, float(weights), 0.0
+        elif isinstance(weights, Uniform):
+            wk, a, b = 1, weights.min, weights.max
+        elif isinstance(weights, Normal) and weights.min is None and weights.max is None:
+            wk, a, b = 2, weights.mu, weights.sigma
+        else:
+            raise NotImplementedError("device connectors take constant, Uniform or Normal weights")
+        if not (np.ndim(delays) == 0 and not hasattr(delays, "get_values")
+                and round(float(delays or 0.0) / self._dt()) <= 1):
+            raise NotImplementedError("device connectors take no synaptic delays")
+        return dict(wkind=wk, a=a, b=b)
+
     def fixed_number_pre(self, number, weights, delays=0.0, allow_self_connections=False,
                          force_multiple_weights=False, storage_format=None, storage_order=None):
         """Every post neuron receives exactly `number` distinct pre neurons.
@@ -263,19 +294,8 @@ class Projection:
         rng = self._rng()
         npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
         if self._device_ok(npost * int(number)):
-            from .random import Normal, Uniform
-            if np.ndim(weights) == 0 and not hasattr(weights, "get_values"):
-                wk, a, b = 0, float(weights), 0.0
-            elif isinstance(weights, Uniform):
-                wk, a, b = 1, weights.min, weights.max
-            elif isinstance(weights, Normal) and weights.min is None and weights.max is None:
-                wk, a, b = 2, weights.mu, weights.sigma
-            else:
-                raise NotImplementedError("device connectors take constant, Uniform or Normal weights")
-            if not (np.ndim(delays) == 0 and not hasattr(delays, "get_values")
-                    and round(float(delays or 0.0) / self._dt()) <= 1):
-                raise NotImplementedError("device connectors take no synaptic delays")
-            self._device_conn = dict(kind="fixed_number_pre", number=int(number), wkind=wk, a=a, b=b,
+            self._device_conn = dict(kind="fixed_number_pre", number=int(number),
+                                     **self._device_weights(weights, delays),
                                      seed=int(rng.integers(0, 2**63 - 1)),
                                      exclude_self=(not allow_self_connections
                                                    and self.pre_pop is self.post_pop))
@@ -356,7 +376,10 @@ class Projection:
         if flat:
             return flat_v
         if getattr(self, "_device_conn", None):
-            return np.split(flat_v, len(self.post_ranks_view))
+            lengths = getattr(self, "_device_lengths", None)
+            if lengths is None:
+                return np.split(flat_v, len(self.post_ranks_view))
+            return np.split(flat_v, np.cumsum(lengths)[:-1])
         lengths = np.diff(self._csr.indptr)
         lengths = lengths[lengths > 0]
         return [a for a in np.split(flat_v, np.cumsum(lengths)[:-1])]

@@ -45,6 +45,10 @@ SIGNATURES = {
     "anb_connect_fixed_number_pre_rows": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_longlong,
                                                     C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
                                                     C.c_double, C.c_double, C.c_int, C.c_int]),
+    "anb_connect_fixed_probability_rows": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int,
+                                                     C.c_longlong, C.c_int, C.c_int, C.c_double,
+                                                     C.c_uint64, C.c_int, C.c_double, C.c_double,
+                                                     C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
@@ -313,6 +317,23 @@ class NativeNet:
         self.arrays[prefix + "__col"] = (np.dtype(np.int32), (nnz,))
         self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (nnz,))
 
+    def connect_fixed_probability(self, prefix, n_post, post_base, pre_lo, pre_hi, probability,
+                                  seed, weight_kind, a, b, weight_dtype, exclude_self,
+                                  row_offset: int = 0) -> int:
+        """Device-generated fixed-probability rows; returns the number of synapses."""
+        wb = {np.dtype(np.float64): 8, np.dtype(np.float32): 4, np.dtype(np.uint16): 2}[
+            np.dtype(weight_dtype)]
+        nnz = C.c_longlong(0)
+        check("anb_connect_fixed_probability_rows", self.lib.anb_connect_fixed_probability_rows(
+            self.h, prefix.encode(), n_post, post_base, int(row_offset), pre_lo, pre_hi,
+            float(probability), seed, weight_kind, float(a), float(b), wb,
+            1 if exclude_self else 0, C.byref(nnz)))
+        self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n_post,))
+        self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))
+        self.arrays[prefix + "__col"] = (np.dtype(np.int32), (nnz.value,))
+        self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (nnz.value,))
+        return int(nnz.value)
+
     def csr_to_csc(self, prefix, n_pre, with_weights):
         check("anb_csr_to_csc", self.lib.anb_csr_to_csc(self.h, prefix.encode(), n_pre,
                                                        1 if with_weights else 0))
@@ -419,6 +440,16 @@ class DryNative:
         self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))
         self.arrays[prefix + "__col"] = (np.dtype(np.int32), (nnz,))
         self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (nnz,))
+
+    def connect_fixed_probability(self, prefix, n_post, post_base, pre_lo, pre_hi, probability,
+                                  seed, weight_kind, a, b, weight_dtype, exclude_self,
+                                  row_offset: int = 0) -> int:
+        nnz = int(round(n_post * (pre_hi - pre_lo) * probability))     # the expected count
+        self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n_post,))
+        self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n_post + 1,))
+        self.arrays[prefix + "__col"] = (np.dtype(np.int32), (nnz,))
+        self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (nnz,))
+        return nnz
 
     def csr_to_csc(self, prefix, n_pre, with_weights):
         nnz = self.arrays[prefix + "__col"][1][0]

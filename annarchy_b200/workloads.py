@@ -413,9 +413,10 @@ class LargeNet:
 
 
 def build_large_network(ln: LargeNet, precision: str = "double", stdp: bool = True,
-                        record: bool = True, **config):
+                        record: bool = True, connector: str = "fixed_number_pre", **config):
     """Returns (net, pop, monitor, projections); connectivity is generated on
-    the device at compile()."""
+    the device at compile(): fixed in-degrees, or (connector
+    "fixed_probability") independent pairs with the same mean in-degrees."""
     from . import STDP, Network, Uniform
     net = Network(dt=ln.dt, seed=ln.seed)
     # float: Kahan compensation of v only (the conductances only decay)
@@ -426,9 +427,15 @@ def build_large_network(ln: LargeNet, precision: str = "double", stdp: bool = Tr
     P = net.create(ln.n, coba_neuron(params))
     Pe, Pi = P[: ln.n_exc], P[ln.n_exc:]
     syn = STDP(**STDP_PARAMS) if stdp else None
-    ee = net.connect(Pe, Pe, "exc", synapse=syn).fixed_number_pre(ln.fan_e, ln.w_exc)
-    ei = net.connect(Pe, Pi, "exc").fixed_number_pre(ln.fan_e, ln.w_exc)
-    ie = net.connect(Pi, P, "inh").fixed_number_pre(ln.fan_i, ln.w_inh)
+    if connector == "fixed_probability":
+        pe, pi = ln.fan_e / ln.n_exc, ln.fan_i / (ln.n - ln.n_exc)
+        ee = net.connect(Pe, Pe, "exc", synapse=syn).fixed_probability(pe, ln.w_exc)
+        ei = net.connect(Pe, Pi, "exc").fixed_probability(pe, ln.w_exc)
+        ie = net.connect(Pi, P, "inh").fixed_probability(pi, ln.w_inh)
+    else:
+        ee = net.connect(Pe, Pe, "exc", synapse=syn).fixed_number_pre(ln.fan_e, ln.w_exc)
+        ei = net.connect(Pe, Pi, "exc").fixed_number_pre(ln.fan_e, ln.w_exc)
+        ie = net.connect(Pi, P, "inh").fixed_number_pre(ln.fan_i, ln.w_inh)
     mon = net.monitor(P, "spike") if record else None
     P.v = np.random.default_rng(ln.seed).uniform(-60.0, -50.0, ln.n)
     return net, P, mon, (ee, ei, ie)

@@ -133,6 +133,21 @@ int anb_connect_fixed_number_pre_rows(anb_net* net, const char* prefix, int n_po
                                       uint64_t seed, int weight_kind, double a, double b,
                                       int weight_bytes, int exclude_self);
 
+/* Fixed-probability projection generated on the device (replaces the host
+ * construction of ANNarchy/core/ConnectorMethods.py:262-330 and
+ * ANNarchy/cython_ext/Connector.pyx:306-345, which build per-post Bernoulli
+ * masks as lists of lists): every pair (post_base + row, pre) with pre in
+ * [pre_lo, pre_hi) is connected with probability 0 < probability <= 1,
+ * sampled by geometric skipping keyed by (seed, row_offset + row), pre ranks
+ * ascending per row; exclude_self drops pre == post. Creates the arrays of
+ * anb_connect_fixed_number_pre (post_rank, row_ptr, col, w) and stores the
+ * number of synapses in *nnz_out. */
+int anb_connect_fixed_probability_rows(anb_net* net, const char* prefix, int n_post, int post_base,
+                                       long long row_offset, int pre_lo, int pre_hi,
+                                       double probability, uint64_t seed, int weight_kind, double a,
+                                       double b, int weight_bytes, int exclude_self,
+                                       long long* nnz_out);
+
 /* Pre-major view of a projection's CSR arrays (the reference's CSRC,
  * ANNarchy/include/CSRCMatrix.hpp:164-222): "<prefix>__col_ptr" over the n_pre
  * neurons of the pre population, "__post_idx" (post rank of each slot),
