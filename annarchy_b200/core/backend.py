@@ -22,6 +22,7 @@ import numpy as np
 from ..generator import formats as F
 from ..generator.codegen import CodeGenerator, compensated_vars, grid_for, trace_layout
 from ..runtime.lib import DryNative, NativeNet
+from .monitor import array_name
 
 BF16 = np.uint16
 MAX_MONITOR_BYTES = 256 << 20
@@ -653,7 +654,7 @@ class CompiledNetwork:
             nat.create(f"mon{m}__ranks", np.asarray(mon.ranks, dtype=np.int32))
         for v in mon.variables:
             if v != "spike":
-                nat.create_empty(f"mon{m}__{v}", np.float64, (lay["cap_var"], n))
+                nat.create_empty(f"mon{m}__{array_name(v)}", np.float64, (lay["cap_var"], n))
         self.mon_layout[m] = lay
 
     # ------------------------------------------------------------------- run
@@ -708,6 +709,7 @@ class CompiledNetwork:
             starts[mon.id] = first
             self.native.write(f"mon{mon.id}__t0", np.array([t], dtype=np.int64))
             self.native.write(f"mon{mon.id}__t0v", np.array([first], dtype=np.int64))
+            self.native.write(f"mon{mon.id}__start", np.array([mon._start_step], dtype=np.int64))
             self.native.write(f"mon{mon.id}__on", np.array([1 if mon._recording else 0],
                                                            dtype=np.int32))
         return starts
@@ -740,7 +742,7 @@ class CompiledNetwork:
                 if v == "spike":
                     continue
                 out = np.empty((nrec, lay["n"]), dtype=np.float64)
-                nat.read_into(f"mon{mon.id}__{v}", out)
+                nat.read_into(f"mon{mon.id}__{array_name(v)}", out)
                 mon._append_values(v, out, rec_steps)
 
     # ------------------------------------------------------------ attributes

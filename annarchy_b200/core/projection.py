@@ -221,6 +221,109 @@ class Projection:
         m = sp.csr_matrix((w, (rows, rows)), shape=(len(self.post_ranks_view), len(self.pre_ranks)))
         return self._store(m, "One-to-One", storage_format, delays)
 
+    # -- distance-based patterns ------------------------------------------------
+    @staticmethod
+    def _pattern_coords(geometry) -> np.ndarray:
+        """(size, dim) normalized coordinates of every rank as the reference's
+        pattern connectors compute them (ANNarchy/cython_ext/Connector.pyx:
+        464-489 with Coordinates.pyx:122-199): 1-D rank / (size - 1) in
+        double; 2-D and 3-D row-major indices / (extent - 1) rounded to
+        float32 (0 along an extent of 1); more dimensions in double."""
+        geometry = tuple(int(g) for g in np.atleast_1d(geometry))
+        size = int(np.prod(geometry))
+        ranks = np.arange(size)
+        if len(geometry) == 1:
+            if size < 2:
+                raise ValueError("distance-based patterns need more than one neuron along a 1-D "
+                                 "geometry")
+            return (ranks / float(size - 1))[:, None]
+        idx = np.stack(np.unravel_index(ranks, geometry), axis=1).astype(np.float64)
+        if len(geometry) > 3:
+            if min(geometry) < 2:
+                raise ValueError("distance-based patterns need extents above 1 beyond 3-D")
+            return idx / (np.asarray(geometry, dtype=np.float64) - 1.0)
+        den = np.asarray([g - 1.0 if g > 1 else 1.0 for g in geometry])
+        out = (idx / den).astype(np.float32).astype(np.float64)
+        out[:, np.asarray(geometry) <= 1] = 0.0
+        return out
+
+    def _pattern(self, kind: str, weight_of, limit_of, delays, allow_self_connections,
+                 storage_format, name):
+        """Rows of a distance-based pattern: every (post, pre) pair whose
+        float32 value passes the limit, pre ranks ascending. The squared
+        distance accumulates in float32 over the pre population's
+        dimensions, each term in double (Coordinates.pyx:10-48)."""
+        from .population import PopulationView
+        if isinstance(self.pre, PopulationView) or isinstance(self.post, PopulationView):
+            raise ValueError(f"{kind} connector is only possible on whole populations, "
+                             "not PopulationViews")
+        if self.pre_pop is not self.post_pop:
+            allow_self_connections = True
+        pre_c = self._pattern_coords(self.pre_pop.geometry)
+        post_c = self._pattern_coords(self.post_pop.geometry)
+        dim = pre_c.shape[1]
+        if post_c.shape[1] < dim:
+            raise ValueError(f"{kind} connector: the post-synaptic geometry has fewer dimensions "
+                             "than the pre-synaptic one")
+        npost, npre = post_c.shape[0], pre_c.shape[0]
+        rows_l, cols_l, w_l = [], [], []
+        block = max(1, 4_000_000 // max(npre, 1))
+        for r0 in range(0, npost, block):
+            r1 = min(npost, r0 + block)
+            if dim == 1:
+                d = ((pre_c[None, :, 0] - post_c[r0:r1, None, 0]) ** 2).astype(np.float32)
+            else:
+                d = np.zeros((r1 - r0, npre), dtype=np.float32)
+                for k in range(dim):
+                    term = (pre_c[None, :, k] - post_c[r0:r1, None, k]) ** 2
+                    d = (d.astype(np.float64) + term).astype(np.float32)
+            value = weight_of(d.astype(np.float64)).astype(np.float32)
+            keep = limit_of(value.astype(np.float64))
+            if not allow_self_connections:           # the same population: pre rank == post rank
+                rr = np.arange(r0, min(r1, npre))
+                keep[rr - r0, rr] = False
+            rows, cols = np.nonzero(keep)
+            rows_l.append(rows + r0)
+            cols_l.append(cols)
+            w_l.append(value[rows, cols].astype(np.float64))
+        rows = np.concatenate(rows_l)
+        cols = np.concatenate(cols_l)
+        m = sp.csr_matrix((np.concatenate(w_l), (rows, cols)), shape=(npost, npre))
+        return self._store(m, name, storage_format, delays)
+
+    def gaussian(self, amp, sigma, delays=0.0, limit=0.01, allow_self_connections=False,
+                 storage_format=None):
+        """Gaussian pattern (ANNarchy/core/ConnectorMethods.py:144-198,
+        cython_ext/Connector.pyx:433-502): post neuron i receives pre neuron
+        j with weight amp * exp(-d2 / (2 sigma^2)), d2 the squared distance of
+        their normalized coordinates, when that weight exceeds limit * amp;
+        amp and sigma in float32, the weight rounded to float32."""
+        a32, s32 = np.float32(amp), np.float32(sigma)
+        den = 2.0 * float(np.float32(s32 * s32))
+        a = float(a32)
+        return self._pattern("Gaussian", lambda d: a * np.exp(-d / den),
+                             lambda v: v > float(limit) * a, delays, allow_self_connections,
+                             storage_format, "Gaussian")
+
+    connect_gaussian = gaussian
+
+    def dog(self, amp_pos, sigma_pos, amp_neg, sigma_neg, delays=0.0, limit=0.01,
+            allow_self_connections=False, storage_format=None):
+        """Difference-of-Gaussians pattern (ANNarchy/core/ConnectorMethods.py:
+        201-260, cython_ext/Connector.pyx:504-575): weight amp_pos *
+        exp(-d2 / (2 sigma_pos^2)) - amp_neg * exp(-d2 / (2 sigma_neg^2)),
+        kept when |weight| exceeds limit * |amp_pos - amp_neg| (the
+        difference taken in float32)."""
+        ap, an = float(np.float32(amp_pos)), float(np.float32(amp_neg))
+        sp_, sn = np.float32(sigma_pos), np.float32(sigma_neg)
+        dp, dn = 2.0 * float(np.float32(sp_ * sp_)), 2.0 * float(np.float32(sn * sn))
+        span = abs(float(np.float32(np.float32(amp_pos) - np.float32(amp_neg))))
+        return self._pattern("DoG", lambda d: ap * np.exp(-d / dp) - an * np.exp(-d / dn),
+                             lambda v: np.abs(v) > float(limit) * span, delays,
+                             allow_self_connections, storage_format, "Difference-of-Gaussian")
+
+    connect_dog = dog
+
     def fixed_probability(self, probability, weights, delays=0.0, allow_self_connections=False,
                           force_multiple_weights=False, storage_format=None, storage_order=None):
         """Each (post, pre) pair is connected independently with the given

@@ -39,6 +39,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from ..core.monitor import array_name
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEVICE_HEADER = os.path.join(os.path.dirname(HERE), "csrc", "device", "anb_device.cuh")
 
@@ -917,13 +919,13 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
         for var in mon.variables:
             if var == "spike":
                 continue
-            src = self.ptr(f"pop{mon.population.id}__{var}")
+            src = self.ptr(f"pop{mon.population.id}__{array_name(var)}")
             ranks = self.ptr(f"mon{m}__ranks") if mon.ranks is not None else "nullptr"
             parts.append(f"""
     if (anb_on && ((t - {self.ptr(f'mon{m}__start')}[0]) % {mon.period_steps} == {mon.period_offset_steps % mon.period_steps})) {{
       const long long anb_slot = (t - {self.ptr(f'mon{m}__t0v')}[0]) / {mon.period_steps};
       if (anb_slot >= 0 && anb_slot < {lay['cap_var']})
-        anb_record({src}, {ranks}, {lay['n']}, {self.ptr(f'mon{m}__{var}')}, anb_slot);
+        anb_record({src}, {ranks}, {lay['n']}, {self.ptr(f'mon{m}__{array_name(var)}')}, anb_slot);
       else if (blockIdx.x == 0 && threadIdx.x == 0)
         anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
     }}""")

@@ -238,6 +238,92 @@ def _digest_desc(d):
     return keep
 
 
+def case_connect_patterns(name):
+    """Gaussian and difference-of-Gaussians connectivity built by the
+    reference's connector code (ANNarchy/cython_ext/Connector.pyx:433-575)
+    for 1-, 2- and 3-D geometries: per pattern the post ranks, the pre ranks
+    and weights of every dendrite (concatenated) and the dendrite sizes."""
+    import numpy as np
+    import ANNarchy as ann
+    from ANNarchy.cython_ext.Connector import dog, gaussian
+    net = ann.Network(dt=0.1, seed=1)
+    neuron = ann.Neuron(parameters="r = 0.0")
+    pats = {
+        "g2_self": ("gaussian", (12, 10), None, dict(amp=1.0, sigma=0.3, limit=0.01)),
+        "g2_map": ("gaussian", (15, 9), (8, 6), dict(amp=2.5, sigma=0.2, limit=0.05)),
+        "g1": ("gaussian", (40,), (30,), dict(amp=1.0, sigma=0.1, limit=0.01)),
+        "g3_self": ("gaussian", (5, 4, 3), None, dict(amp=0.7, sigma=0.35, limit=0.02)),
+        "dog2_self": ("dog", (12, 10), None, dict(amp_pos=1.0, sigma_pos=0.2, amp_neg=0.5,
+                                                  sigma_neg=0.5, limit=0.01)),
+        "dog2_map": ("dog", (10, 10), (7, 9), dict(amp_pos=1.5, sigma_pos=0.15, amp_neg=1.0,
+                                                   sigma_neg=0.3, limit=0.02)),
+    }
+    out = {}
+    for key, (kind, g_pre, g_post, kw) in pats.items():
+        pre = net.create(g_pre, neuron)
+        post = pre if g_post is None else net.create(g_post, neuron)
+        allow = g_post is not None
+        if kind == "gaussian":
+            lil = gaussian(pre, post, kw["amp"], kw["sigma"], 0.0, kw["limit"], allow, "lil", "post_to_pre")
+        else:
+            lil = dog(pre, post, kw["amp_pos"], kw["sigma_pos"], kw["amp_neg"], kw["sigma_neg"], 0.0,
+                      kw["limit"], allow, "lil", "post_to_pre")
+        out[key + "__post"] = np.asarray(list(lil.post_rank), dtype=np.int64)
+        out[key + "__sizes"] = np.asarray([len(r) for r in lil.pre_rank], dtype=np.int64)
+        out[key + "__pre"] = np.concatenate([np.asarray(r, dtype=np.int64) for r in lil.pre_rank])
+        out[key + "__w"] = np.concatenate([np.asarray(w, dtype=np.float64) for w in lil.w])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def spike_dict_fixture(seed=5, n=40, steps=2000):
+    """A seeded raster (dict rank -> ascending steps, some neurons silent)
+    for the spike-analysis fixtures."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = {}
+    for k in range(n):
+        rate = 0.0 if k % 7 == 3 else rng.uniform(0.001, 0.05)
+        steps_k = np.nonzero(rng.random(steps) < rate)[0] + 200
+        out[k] = [int(t) for t in steps_k]
+    return out
+
+
+def case_spike_analysis(name):
+    """The reference's spike-analysis functions (ANNarchy/core/Monitor.py:
+    1091-1330, cython_ext/Transformations.pyx:23-108) on a seeded raster at
+    dt = 0.1 ms."""
+    import numpy as np
+    import ANNarchy as ann
+    from ANNarchy.core import Monitor as M
+    import ANNarchy.cython_ext.Transformations as T
+    ann.setup(dt=0.1)
+    spikes = spike_dict_fixture()
+    out = {"ranks": np.asarray(list(spikes), dtype=np.int64),
+           "sizes": np.asarray([len(v) for v in spikes.values()], dtype=np.int64),
+           "steps": np.concatenate([np.asarray(v, dtype=np.int64) for v in spikes.values()])}
+    t, r = M.raster_plot(spikes, dt=0.1)
+    out["raster_t"], out["raster_r"] = t, r
+    out["hist_dt"] = M.histogram(spikes, dt=0.1)
+    out["hist_05"] = M.histogram(spikes, bins=0.5, dt=0.1)
+    out["hist_pn"] = M.histogram(spikes, bins=1.0, per_neuron=True, dt=0.1)
+    out["hist_win"] = M.histogram(spikes, bins=0.5, recording_window=(100, 2400), dt=0.1)
+    out["isi"] = np.asarray(M.inter_spike_interval(spikes, dt=0.1))
+    isi_pn = M.inter_spike_interval(spikes, ranks=[1, 2, 5, 9], per_neuron=True, dt=0.1)
+    out["isi_pn_keys"] = np.asarray(sorted(isi_pn), dtype=np.int64)
+    out["isi_pn_vals"] = np.concatenate([np.asarray(isi_pn[k]) for k in sorted(isi_pn)])
+    out["cv"] = np.asarray(M.coefficient_of_variation(spikes, dt=0.1))
+    out["cv_ranks"] = np.asarray(M.coefficient_of_variation(spikes, ranks=[0, 4, 8, 12], dt=0.1))
+    out["mean_fr"] = np.float64(M.mean_fr(spikes, dt=0.1))
+    out["mean_fr_dur"] = np.float64(M.mean_fr(spikes, duration=2500, dt=0.1))
+    for smooth in (0.0, 5.0):
+        for start, stop in ((0, 2300), (150, 2250)):
+            key = f"{int(smooth)}_{start}"
+            out["srate_" + key] = T.smoothed_rate({"data": spikes, "start": start, "stop": stop}, smooth)
+            out["prate_" + key] = T.population_rate({"data": spikes, "start": start, "stop": stop},
+                                                    smooth)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -248,6 +334,8 @@ CASES = {
     "coba_c2": (case_coba, dict(seed=42, n=4000, p=0.02, steps=10000, v_every=0)),
     "stdp_small": (case_coba, dict(seed=11, n=400, p=0.05, steps=2000, v_every=0, stdp=True)),
     "io": (case_io, {}),
+    "connect_patterns": (case_connect_patterns, {}),
+    "spike_analysis": (case_spike_analysis, {}),
 }
 
 
