@@ -135,6 +135,8 @@ class CompiledNetwork:
             mod = gen.local_module()
         else:
             nat.create("tickc", np.zeros(1, dtype=np.uint32))
+            if any(getattr(p, "stop_condition", None) for p in net.populations):
+                nat.create("stop_flags", np.full(len(net.populations), -1, dtype=np.int64))
             mod = gen.grid_module()
         self.module = mod
         nat.load_module(mod.source, mod.options)
@@ -143,6 +145,8 @@ class CompiledNetwork:
         else:
             nat.plan(mod.plan)
             nat.set_graph_steps(int(net._config.get("graph_steps", 32)))
+            for pop_id, kernel, grid, block, mode_all in mod.stops:
+                nat.set_stop_kernel(pop_id, kernel, grid, block, mode_all)
 
     def _build_cluster(self):
         """Fast spiking engine on one thread-block cluster: the smallest
@@ -214,6 +218,8 @@ class CompiledNetwork:
                 raise NotImplementedError("sharded networks run on the grid engine")
             return "grid"
         ok, why = self._local_possible()
+        if any(getattr(p, "stop_condition", None) for p in self.net.populations):
+            ok, why = False, "stop conditions"
         if want == "local":
             if not ok:
                 raise NotImplementedError("local engine not possible: " + why)
@@ -662,6 +668,33 @@ class CompiledNetwork:
         if not self.mon_layout:
             return 1 << 30
         return min(l["cap_steps"] for l in self.mon_layout.values())
+
+    def run_until(self, nsteps: int, pops, or_and: bool) -> int:
+        """At most nsteps steps, ending after the first step at which the
+        stop conditions of `pops` hold (all of them, or any); monitors are
+        drained per chunk as in run(). Returns the steps run."""
+        if self.shard:
+            raise NotImplementedError("simulate_until() is not supported for sharded networks")
+        if self.engine == "local":
+            if any(getattr(p, "stop_condition", None) for p in self.net.populations):
+                raise NotImplementedError("stop conditions need the grid engine")
+            self.run(nsteps)
+            return int(nsteps)
+        nat = self.native
+        t = nat.get_time()
+        left, total = int(nsteps), 0
+        cap = self.chunk_steps()
+        while left > 0:
+            n = min(left, cap)
+            starts = self.begin_chunk(t)
+            done, stopped = nat.run_until(n, [p.id for p in pops], or_and)
+            self.end_chunk(t, done, starts)
+            t += done
+            total += done
+            left -= done
+            if stopped or done < n:
+                break
+        return total
 
     def run(self, nsteps: int):
         nat = self.native

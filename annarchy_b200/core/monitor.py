@@ -30,9 +30,17 @@ _SUM = re.compile(r"^sum\((\w+)\)$")
 
 
 def array_name(var: str) -> str:
-    """Device array suffix of a recorded variable ('sum(exc)' -> '_sum_exc')."""
+    """Suffix of the recording buffer of a variable ('sum(exc)' -> '_sum_exc')."""
     m = _SUM.match(var)
     return f"_sum_{m.group(1)}" if m else var
+
+
+def source_name(var: str) -> str:
+    """Population array a variable is recorded from: the weighted sums of the
+    step just finished are kept in '_last_sum_<target>' (the update kernel
+    consumes and clears '_sum_<target>')."""
+    m = _SUM.match(var)
+    return f"_last_sum_{m.group(1)}" if m else var
 
 
 class Monitor:

@@ -67,7 +67,7 @@ class Network:
         return self
 
     def create(self, geometry=None, neuron=None, name: str | None = None, population=None,
-               **kw) -> Population:
+               stop_condition: str | None = None, **kw) -> Population:
         """A population of `neuron`, or (as the reference's
         net.create(PoissonPopulation(...))) a population object built outside
         the network, which then joins it."""
@@ -86,7 +86,10 @@ class Network:
         else:
             if neuron is None:
                 raise TypeError("create() needs a neuron type")
-            pop = Population(geometry, neuron, name=name, net=self, pop_id=len(self.populations))
+            pop = Population(geometry, neuron, name=name, net=self, pop_id=len(self.populations),
+                             stop_condition=stop_condition)
+        if stop_condition is not None and isinstance(geometry, Population):
+            object.__setattr__(pop, "stop_condition", stop_condition)
         self.populations.append(pop)
         return pop
 
@@ -155,6 +158,25 @@ class Network:
         if measure_time:
             print(f"Simulating {duration / 1000.0} seconds of the network took "
                   f"{time.time() - t0} seconds.")
+
+    def simulate_until(self, max_duration: float, population, operator: str = "and",
+                       measure_time: bool = False) -> float:
+        """Simulate at most max_duration ms and stop after the first step at
+        which the stop conditions of `population` (one or a list) hold: all
+        of them (operator "and") or any ("or") (ANNarchy/core/Simulate.py:
+        174-242, Network.simulate_until). Returns the simulated duration in
+        ms."""
+        if not self._compiled:
+            raise RuntimeError("simulate_until(): the network is not compiled yet")
+        import math
+        n = int(math.ceil(float(max_duration) / self.dt))
+        pops = population if isinstance(population, (list, tuple)) else [population]
+        t0 = time.time()
+        done = self._backend.run_until(n, list(pops), operator == "and")
+        if measure_time:
+            print(f"Simulating {done * self.dt / 1000.0} seconds of the network took "
+                  f"{time.time() - t0} seconds.")
+        return done * self.dt
 
     def simulate_steps(self, nsteps: int):
         if not self._compiled:

@@ -31,6 +31,7 @@ class Population:
         self.neuron_type = neuron
         self.net = net
         self.id = pop_id
+        self.stop_condition = stop_condition
         self.name = name or f"pop{pop_id}"
         self.desc = neuron.desc
         self.targets = list(self.desc["targets"])

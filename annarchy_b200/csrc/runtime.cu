@@ -152,6 +152,15 @@ struct anb_net {
   int64_t dec_rows_cap = 0;
   int* dec_out = nullptr;
   int64_t dec_out_cap = 0;
+  // stop conditions of populations (anb_run_until): the kernel of population
+  // `pop` writes the device step into stop_flags[pop] when a neuron satisfies
+  // the condition ("any") or when one fails it ("all")
+  struct Stop {
+    int pop;
+    Launch l;
+    int all;
+  };
+  std::vector<Stop> stops;
 };
 
 namespace {
@@ -584,6 +593,7 @@ int anb_module_load(anb_net* net, const char* source, const char* options) {
   ANB_CUDA(cudaStreamSynchronize(net->stream));
   drop_graph(net);
   net->plan.clear();
+  net->stops.clear();
   net->has_local = false;
   if (net->module) {
     g_drv.moduleUnload(net->module);
@@ -968,6 +978,74 @@ int anb_run(anb_net* net, int64_t nsteps) {
 }
 
 int anb_step(anb_net* net) { return anb_run(net, 1); }
+
+int anb_set_stop_kernel(anb_net* net, int pop, const char* kernel, unsigned grid, unsigned block,
+                        int all_mode) {
+  Launch l;
+  int rc = resolve(net, kernel, grid, block, 0, &l);
+  if (rc) return rc;
+  if (pop < 0) return fail(ANB_ERR_ARG, "negative population id");
+  Array* f = find(net, "stop_flags");
+  if (!f || f->bytes < (size_t)(pop + 1) * 8) return fail(ANB_ERR_STATE, "stop_flags array missing or short");
+  for (auto& st : net->stops)
+    if (st.pop == pop) {
+      st.l = l;
+      st.all = all_mode ? 1 : 0;
+      return ANB_OK;
+    }
+  net->stops.push_back({pop, l, all_mode ? 1 : 0});
+  return ANB_OK;
+}
+
+int anb_run_until(anb_net* net, int64_t steps, const int* populations, int n_populations, int or_and,
+                  int64_t* done, int* stopped) {
+  if (!net || !done || !stopped || (n_populations > 0 && !populations))
+    return fail(ANB_ERR_ARG, "NULL argument");
+  if (steps < 0 || n_populations < 0) return fail(ANB_ERR_ARG, "negative count");
+  *done = 0;
+  *stopped = 0;
+  if (net->stops.empty()) {                // no stop condition in the network: plain run
+    int rc = anb_run(net, steps);
+    if (rc) return rc;
+    *done = steps;
+    return ANB_OK;
+  }
+  if (net->has_local) return fail(ANB_ERR_STATE, "stop conditions need the grid engine");
+  Array* f = find(net, "stop_flags");
+  if (!f) return fail(ANB_ERR_STATE, "stop_flags array missing");
+  std::vector<const anb_net::Stop*> checked;
+  for (int i = 0; i < n_populations; ++i)
+    for (const auto& st : net->stops)
+      if (st.pop == populations[i]) checked.push_back(&st);
+  std::vector<long long> flags(f->bytes / 8);
+  for (int64_t n = 0; n < steps; ++n) {
+    int rc = anb_run(net, 1);
+    if (rc) return rc;
+    ++*done;
+    bool stop = or_and != 0;
+    if (!checked.empty()) {
+      for (const auto* st : checked) {
+        rc = launch(net, st->l, nullptr);
+        if (rc) return rc;
+      }
+      ANB_CUDA(cudaMemcpyAsync(flags.data(), f->ptr, flags.size() * 8, cudaMemcpyDeviceToHost,
+                               net->stream));
+      ANB_CUDA(cudaStreamSynchronize(net->stream));
+      for (const auto* st : checked) {
+        const bool marked = flags[st->pop] == (long long)net->t;
+        const bool cond = st->all ? !marked : marked;
+        stop = or_and ? (stop && cond) : (stop || cond);
+      }
+    }
+    // as in the reference, a list of populations without any stop condition
+    // ends an "and" run after one step
+    if (stop && n_populations > 0) {
+      *stopped = 1;
+      break;
+    }
+  }
+  return ANB_OK;
+}
 
 int anb_synchronize(anb_net* net) {
   if (!net) return fail(ANB_ERR_ARG, "net is NULL");

@@ -39,7 +39,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ..core.monitor import array_name
+from ..core.monitor import array_name, source_name
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEVICE_HEADER = os.path.join(os.path.dirname(HERE), "csrc", "device", "anb_device.cuh")
@@ -107,6 +107,7 @@ class Module:
     plan: list = field(default_factory=list)           # [(kernel, grid, block, smem)]
     local: tuple | None = None                         # (kernel, grid, block, smem)
     kernels: list = field(default_factory=list)
+    stops: list = field(default_factory=list)          # [(pop id, kernel, grid, block, all)]
 
 
 class CodeGenerator:
@@ -515,6 +516,51 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
 }}
 """
 
+    def stop_kernel(self, pop) -> tuple[str, bool]:
+        """Stop condition of a population for simulate_until (the reference
+        compiles it as PopStruct::stop_condition(),
+        ANNarchy/generator/Population/CUDAGenerator.py:836-917, parsed by
+        ANNarchy/parser/Extraction.py:927-947): "<condition> : any" (the
+        default) holds when a neuron satisfies it, ": all" when every neuron
+        does; "spiked" tests the spikes of the step just finished. The kernel
+        writes the device step into stop_flags[pop] when a neuron satisfies
+        the condition (any) or fails it (all). Returns (source, all)."""
+        from ..parser.equation import Statement
+        eq, _, flags = pop.stop_condition.partition(":")
+        mode_all = "all" in flags.split()
+        k = pop.id
+        eq = eq.strip()
+        if eq.replace(" ", "") == "spiked":
+            loads = ""
+            cond = f"(({self.spk_at(pop, '(t - 1)')}[anb_i >> 5] >> (anb_i & 31)) & 1u) != 0u"
+        else:
+            code = self.typed(self.fill(Statement("stop_cond", eq, pop.desc).parse()))
+            names = [n for n in self._locals(pop) if re.search(rf"\b{re.escape(n)}\b", code)]
+            loads = " ".join(
+                f"const {'int' if pop._ctype.get(n) in ('int', 'bool') else self.real} {n} = "
+                f"{self.ptr(f'pop{k}__{n}')}[anb_i];" for n in names)
+            cond = code
+        test = f"!({cond})" if mode_all else f"({cond})"
+        dt_t = "double" if self.exact else "float"
+        preamble = self._globals_preamble(pop, lambda n: self.ptr(f"pop{k}__{n}"))
+        src = f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
+    const long long t = *{self.ptr('t')};
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    (void)dt;
+    {preamble}
+    bool anb_hit = false;
+    for (int anb_i = blockIdx.x * blockDim.x + threadIdx.x; anb_i < {pop.size};
+         anb_i += gridDim.x * blockDim.x) {{
+      {loads}
+      if ({test}) anb_hit = true;
+    }}
+    if (__ballot_sync(0xffffffffu, anb_hit) != 0u && (threadIdx.x & 31) == 0)
+      atomicMax({self.ptr('stop_flags')} + {k}, t);
+}}
+"""
+        return src, mode_all
+
     def timed_array_kernel(self, pop) -> str:
         """TimedArray update (ANNarchy/inputs/TimedArray.py, update_variables):
         internal time tau = t - t0 (modulo the period when positive); when tau
@@ -919,7 +965,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
         for var in mon.variables:
             if var == "spike":
                 continue
-            src = self.ptr(f"pop{mon.population.id}__{array_name(var)}")
+            src = self.ptr(f"pop{mon.population.id}__{source_name(var)}")
             ranks = self.ptr(f"mon{m}__ranks") if mon.ranks is not None else "nullptr"
             parts.append(f"""
     if (anb_on && ((t - {self.ptr(f'mon{m}__start')}[0]) % {mon.period_steps} == {mon.period_offset_steps % mon.period_steps})) {{
@@ -1004,8 +1050,14 @@ extern "C" __global__ void anb_tick() {
 """)
             plan.append(("anb_tick", 1, 32, 0))
         kernels = self._append_epilogue(kernels, plan[-1][0], epilogue)
+        stops = []
+        for pop in net.populations:
+            if getattr(pop, "stop_condition", None):
+                code, mode_all = self.stop_kernel(pop)
+                kernels.append(code)
+                stops.append((pop.id, f"pop{pop.id}_stop", grid_for(pop.size), BLOCK, mode_all))
         return Module(self.assemble(kernels), self.options(), "grid", plan=plan,
-                      kernels=[p[0] for p in plan])
+                      kernels=[p[0] for p in plan], stops=stops)
 
     @staticmethod
     def _append_epilogue(kernels: list, name: str, code: str) -> list:

@@ -50,6 +50,9 @@ SIGNATURES = {
                                                      C.c_uint64, C.c_int, C.c_double, C.c_double,
                                                      C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
+    "anb_set_stop_kernel": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_uint, C.c_uint, C.c_int]),
+    "anb_run_until": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.c_int, C.c_int,
+                                C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
     "anb_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -372,6 +375,19 @@ class NativeNet:
     def run(self, steps: int):
         check("anb_run", self.lib.anb_run(self.h, int(steps)))
 
+    def set_stop_kernel(self, pop: int, kernel: str, grid: int, block: int, all_mode: bool):
+        check("anb_set_stop_kernel", self.lib.anb_set_stop_kernel(
+            self.h, int(pop), kernel.encode(), int(grid), int(block), 1 if all_mode else 0))
+
+    def run_until(self, steps: int, populations, or_and: bool) -> tuple[int, bool]:
+        """(steps run, whether the stop conditions ended the run)."""
+        pops = (C.c_int * max(1, len(populations)))(*[int(p) for p in populations])
+        done, stopped = C.c_int64(0), C.c_int(0)
+        check("anb_run_until", self.lib.anb_run_until(self.h, int(steps), pops, len(populations),
+                                                      1 if or_and else 0, C.byref(done),
+                                                      C.byref(stopped)))
+        return int(done.value), bool(stopped.value)
+
     def synchronize(self):
         check("anb_synchronize", self.lib.anb_synchronize(self.h))
 
@@ -467,6 +483,9 @@ class DryNative:
 
     def set_local_kernel(self, *a):
         self.local = a
+
+    def set_stop_kernel(self, *a):
+        pass
 
     def set_graph_steps(self, steps):
         pass

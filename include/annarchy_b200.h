@@ -202,6 +202,28 @@ int anb_set_graph_steps(anb_net* net, int steps);
  * anb_synchronize waits and reports device-side errors. */
 int anb_run(anb_net* net, int64_t nsteps);
 int anb_step(anb_net* net);
+
+/* Stop condition of population `pop` for anb_run_until: `kernel` (no
+ * parameters, launched with grid x block after a step) writes the device step
+ * into the int64 array "stop_flags"[pop] when a neuron satisfies the
+ * condition (all_mode 0: the condition holds if any neuron does) or when a
+ * neuron fails it (all_mode 1: it holds if none fails). No counterpart in the
+ * reference, whose populations compile a stop_condition() method
+ * (ANNarchy/generator/Population/CUDAGenerator.py:836-917). */
+int anb_set_stop_kernel(anb_net* net, int pop, const char* kernel, unsigned grid, unsigned block,
+                        int all_mode);
+
+/* Runs at most `steps` steps and stops after the first step at which the
+ * stop conditions of the listed populations hold: all of them (or_and != 0)
+ * or any (or_and == 0); populations without a condition are skipped, and a
+ * non-empty list with none ends an "and" run after one step. Without any stop
+ * condition in the network it runs all steps. *done receives the steps run,
+ * *stopped 1 when the conditions ended the run. Replaces the reference's
+ * run_until(steps, populations, or_and) -> steps run
+ * (ANNarchy/generator/Template/OpenMPBaseTemplate.py:95,367-374;
+ * CUDABaseTemplate.py:648-680, SimCore/CUDAGenerator.py:478-493). */
+int anb_run_until(anb_net* net, int64_t steps, const int* populations, int n_populations, int or_and,
+                  int64_t* done, int* stopped);
 int anb_synchronize(anb_net* net);
 
 /* Device-side error word: 0, or the code a kernel wrote when a bounded wait
