@@ -478,7 +478,7 @@ class CompiledNetwork:
         else:
             lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
         if plastic:
-            nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
+            nat.create(f"proj{k}__flags", np.array(proj._learn_flags, dtype=np.int32))
             if self._trace_dtype(proj) is not None:
                 dt = self._trace_dtype(proj)
                 nat.create_empty(f"proj{k}__tr", np.uint32, (nnz * dt.itemsize // 4,))
@@ -564,7 +564,23 @@ class CompiledNetwork:
                 value = proj._global_values.get(prm["name"], prm["init"])
                 nat.create(f"proj{k}__{prm['name']}", np.array([value], dtype=self.real))
         if proj.synapse_type.type == "rate":
-            fmt = "csr" if proj._delay_steps is not None else self._rate_format(proj, lay)
+            learning = CodeGenerator.rate_learning(proj)
+            if learning:
+                # the update kernel walks the CSR rows and writes the weights in place
+                if proj._storage_format not in ("csr", "auto"):
+                    raise NotImplementedError(f"{proj.name}: rate-coded projections with synaptic "
+                                              "equations use the csr format in this backend")
+                if proj.max_delay > 1:
+                    raise NotImplementedError(f"{proj.name}: rate-coded learning with synaptic "
+                                              "delays is not supported by this backend")
+                if not self.exact:
+                    nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
+                for name, arr in proj._host_attr.items():
+                    nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real)[keep_syn])
+                for name, arr in proj._host_semi.items():
+                    nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
+                nat.create(f"proj{k}__flags", np.array(proj._learn_flags, dtype=np.int32))
+            fmt = "csr" if (proj._delay_steps is not None or learning) else self._rate_format(proj, lay)
             lay["format"] = fmt
             if fmt != "csr":
                 F.create_format_arrays(self, proj, fmt, post_rank, row_ptr, cols, w, lay)
@@ -614,7 +630,7 @@ class CompiledNetwork:
             else:
                 lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
             if proj.plastic:
-                nat.create(f"proj{k}__flags", np.array([1], dtype=np.int32))
+                nat.create(f"proj{k}__flags", np.array(proj._learn_flags, dtype=np.int32))
                 host = {name: np.asarray(arr)[keep_syn] for name, arr in proj._host_attr.items()}
                 if self._trace_dtype(proj) is not None:
                     # w and the traces in one record per synapse (float32)

@@ -159,6 +159,17 @@ class Network:
             print(f"Simulating {duration / 1000.0} seconds of the network took "
                   f"{time.time() - t0} seconds.")
 
+    def enable_learning(self, projections=None, period: float | None = None,
+                        offset: float | None = None):
+        """Learning on for the given projections (default: all)."""
+        for proj in projections or self.projections:
+            proj.enable_learning(period=period, offset=offset)
+
+    def disable_learning(self, projections=None):
+        """Learning off for the given projections (default: all)."""
+        for proj in projections or self.projections:
+            proj.disable_learning()
+
     def simulate_until(self, max_duration: float, population, operator: str = "and",
                        measure_time: bool = False) -> float:
         """Simulate at most max_duration ms and stop after the first step at

@@ -75,6 +75,9 @@ class Projection:
         self.max_delay = 1              # steps
         self._delay_steps = None        # per synapse (CSR order) for non-uniform delays
         self._global_values: dict[str, float] = {}   # global parameters set before compile()
+        self._host_semi: dict[str, np.ndarray] = {}  # post-synaptic (per dendrite) attributes
+        # learning switches on the device: plasticity, update, period, offset (steps)
+        self._learn_flags = [1, 1, 1, 0]
 
     # -- properties -------------------------------------------------------------
     @property
@@ -153,10 +156,13 @@ class Projection:
             if storage_format not in FORMATS:
                 raise ValueError(f"unknown storage format {storage_format!r}")
             self._storage_format = storage_format
+        n_dend = int(np.count_nonzero(np.diff(m.indptr)))
         for v in self.desc["variables"] + self.desc["parameters"]:
+            init = v["init"] if not isinstance(v["init"], str) else 0.0
             if v["locality"] == "local" and v["name"] != "w":
-                init = v["init"] if not isinstance(v["init"], str) else 0.0
                 self._host_attr[v["name"]] = np.full(m.nnz, float(init))
+            elif v["locality"] == "semiglobal":
+                self._host_semi[v["name"]] = np.full(n_dend, float(init))
         return self
 
     def _weights(self, weights, nnz):
@@ -457,11 +463,76 @@ class Projection:
         cols = self.pre_ranks[m.indices].astype(np.int32)
         return post_ranks, row_ptr, cols, np.asarray(m.data, dtype=np.float64)
 
+    # -- learning switches (ANNarchy/core/Projection.py:1440-1509) ----------------------
+    def _write_flags(self):
+        if self.net is not None and self.net._compiled:
+            nat = self.net._backend.native
+            if f"proj{self.id}__flags" in nat.arrays:
+                nat.write(f"proj{self.id}__flags", np.array(self._learn_flags, dtype=np.int32))
+
+    @property
+    def plasticity(self) -> bool:
+        """Whether the weights change (the other synaptic variables still update)."""
+        return bool(self._learn_flags[0])
+
+    @plasticity.setter
+    def plasticity(self, value: bool):
+        self._learn_flags[0] = 1 if value else 0
+        self._write_flags()
+
+    @property
+    def update(self) -> bool:
+        """Whether the continuous synaptic equations run."""
+        return bool(self._learn_flags[1])
+
+    @update.setter
+    def update(self, value: bool):
+        self._learn_flags[1] = 1 if value else 0
+        self._write_flags()
+
+    def enable_learning(self, period: float | None = None, offset: float | None = None):
+        """Learning on: the synaptic equations run every `period` ms (default
+        every step), at the steps t with (t - offset) % period == 0,
+        integrating over the period; weights change again."""
+        if period is not None and offset is not None and offset >= period:
+            raise ValueError("enable_learning(): the offset must be smaller than the period")
+        if period is None and offset is not None:
+            raise ValueError("enable_learning(): if you define an offset, you have to define a "
+                             "period")
+        dt = self._dt()
+        steps = int(period / dt) if period is not None else 1
+        if period is None:
+            period = dt
+        if offset is not None:
+            # the reference takes the time of its default network
+            # (Global.get_time(), Projection.py:1481), which networks created
+            # with Network() never advance: the offset counts from step 0
+            rel = 0.0 % period + offset
+            off = int(int(rel % period) / dt)
+        else:
+            off = 0
+        self._learn_flags = [1, 1, max(1, steps), off]
+        self._write_flags()
+
+    def disable_learning(self, update=None):
+        """Rate-coded: the synaptic equations stop (weights included);
+        spiking: the weights stop changing, the other variables still
+        update."""
+        if self.synapse_type.type == "rate":
+            self._learn_flags[1] = 0
+        else:
+            self._learn_flags[0] = 0
+        self._write_flags()
+
     # -- attributes --------------------------------------------------------------------------
     def _attr_names(self):
         return ["w"] + list(self._host_attr)
 
     def get(self, name: str, flat: bool = False):
+        if name in self._host_semi:                 # one value per dendrite
+            if self.net is not None and self.net._compiled:
+                return self.net._backend.read_projection_attribute(self, name)
+            return self._host_semi[name].copy()
         if name not in self._attr_names() and name not in {p["name"] for p in self.desc["parameters"]}:
             raise AttributeError(f"projection {self.name!r} has no attribute {name!r}")
         glob = {p["name"]: p for p in self.desc["parameters"] + self.desc["variables"]
@@ -498,6 +569,12 @@ class Projection:
                 else:
                     self._global_values[name] = value
                 continue
+            if name in self._host_semi:
+                arr = draw(value, self._host_semi[name].shape, self._rng())
+                self._host_semi[name] = np.asarray(arr, dtype=np.float64)
+                if self.net is not None and self.net._compiled:
+                    self.net._backend.write_projection_attribute(self, name, self._host_semi[name])
+                continue
             nnz = self.nb_synapses
             if isinstance(value, list):
                 value = np.concatenate([np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in value])
@@ -516,7 +593,9 @@ class Projection:
             raise AttributeError(name)
         desc = self.__dict__.get("desc")
         if desc is not None and (name == "w" or name in self.__dict__.get("_host_attr", {}) or
-                                 name in {p["name"] for p in desc["parameters"]}):
+                                 name in self.__dict__.get("_host_semi", {}) or
+                                 name in {p["name"] for p in desc["parameters"] + desc["variables"]
+                                          if p["locality"] == "global"}):
             return self.get(name)
         raise AttributeError(name)
 
@@ -524,7 +603,8 @@ class Projection:
         desc = self.__dict__.get("desc")
         if desc is not None and (self.__dict__.get("_csr") is not None or
                                  self.__dict__.get("_device_conn")) and (
-                name == "w" or name in self.__dict__.get("_host_attr", {})):
+                name == "w" or name in self.__dict__.get("_host_attr", {}) or
+                name in self.__dict__.get("_host_semi", {})):
             self.set({name: value})
             return
         object.__setattr__(self, name, value)

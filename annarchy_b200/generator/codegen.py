@@ -561,6 +561,166 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
 """
         return src, mode_all
 
+    # ------------------------------------------------- rate-coded learning
+    @staticmethod
+    def rate_learning(proj) -> bool:
+        """A rate-coded projection whose synapse has continuous equations
+        (the reference's update_synapse)."""
+        if proj.synapse_type.type != "rate":
+            return False
+        return any(v.get("cpp") and v.get("method") != "event-driven"
+                   for v in proj.desc["variables"])
+
+    def _syn_block(self, proj, locality: str) -> str:
+        """The equations of one locality in the reference's order
+        (ANNarchy/generator/Utils.py:17-210): consecutive ODEs as one block
+        (all increments, then the switches with their bounds), other
+        statements with their bounds; the weight's update only while
+        plasticity is on."""
+        desc = proj.desc
+        blocks, is_ode = [], False
+        for v in desc["variables"]:
+            if not v.get("cpp") or v.get("method") == "event-driven" or v["name"] not in desc[locality]:
+                continue
+            if v.get("switch"):
+                if is_ode and blocks:
+                    blocks[-1][1].append(v)
+                else:
+                    blocks.append(("ode", [v]))
+                is_ode = True
+            else:
+                if not is_ode and blocks:
+                    blocks[-1][1].append(v)
+                else:
+                    blocks.append(("non-ode", [v]))
+                is_ode = False
+        idx = {"local": "%(local_index)s", "semiglobal": "%(semiglobal_index)s", "global": ""}[locality]
+
+        def bounds(v):
+            out = ""
+            for b, val in v.get("bounds", {}).items():
+                if b in ("min", "max"):
+                    op = "<" if b == "min" else ">"
+                    out += f"if({v['name']}{idx} {op} {val}) {v['name']}{idx} = {val};\n"
+            return out
+
+        code = []
+        for kind, vs in blocks:
+            if kind == "ode":
+                for v in vs:
+                    cpp = v["cpp"] if isinstance(v["cpp"], str) else "\n".join(v["cpp"])
+                    code.append(cpp)
+                for v in vs:
+                    body = v["switch"] + "\n" + bounds(v)
+                    code.append(f"if (anb_plastic) {{ {body} }}" if v["name"] == "w" else body)
+            else:
+                for v in vs:
+                    body = v["cpp"] + "\n" + bounds(v)
+                    code.append(f"if (anb_plastic) {{ {body} }}" if v["name"] == "w" else body)
+        text = "\n".join(code)
+        # updates every `period` steps integrate over period * dt (as the reference's _dt)
+        return re.sub(r"(?<![\w.])dt(?!\w)", "anb_dt", text)
+
+    def rate_update_kernels(self, proj) -> list:
+        """Continuous update of the synaptic variables of a rate-coded
+        projection after the neuron updates of the step
+        (ANNarchy/generator/Projection/SingleThreadGenerator.py:1575-1700,
+        OpenMP/CSR.py:833-865): when learning is on and (t - offset) is a
+        multiple of the period, the global equations once, then per dendrite
+        (a warp) its semiglobal equations (lane 0) followed by the local
+        equations of its synapses (one lane each). Returns [(source, plan
+        entry)]."""
+        k = proj.id
+        a, b = proj.pre_pop, proj.post_pop
+        lay = self.c.layout[k]
+        desc = proj.desc
+        for v in desc["variables"]:
+            if v.get("cpp") and v.get("method") not in ("explicit", "event-driven", None) \
+                    and v.get("switch"):
+                raise NotImplementedError(f"{proj.name}: synaptic variable {v['name']!r} uses the "
+                                          f"{v['method']!r} method; rate-coded synapses support "
+                                          "explicit Euler in this backend")
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        dt_t = "double" if self.exact else "float"
+        # no early return: the step counter's epilogue may follow these kernels
+        head = f"""    const long long t = *{self.ptr('t')};
+    const int* anb_fl = {p('flags')};
+    const int anb_plastic = anb_fl[0];
+    const bool anb_go = anb_fl[1] && (t - anb_fl[3]) % anb_fl[2] == 0;
+    const {dt_t} anb_dt = ({dt_t})(*{self.ptr('dt')}) * anb_fl[2];
+"""
+        glob_all = [q for q in desc["parameters"] + desc["variables"] if q["locality"] == "global"]
+        glob_eq = self._syn_block(proj, "global")
+        out = []
+
+        def refs(code):
+            decl = []
+            for prefix, pop in (("anb_pre_", a), ("anb_post_", b)):
+                for n in sorted(set(re.findall(prefix + r"(\w+)\[", code))):
+                    if n not in pop._host:
+                        raise NotImplementedError(f"{proj.name}: {prefix[4:-1]}.{n} is not an attribute "
+                                                  f"of {pop.name}")
+                    ct = "int" if pop._ctype.get(n) in ("int", "bool") else self.real
+                    decl.append(f"const {ct}* __restrict__ {prefix}{n} = "
+                                f"{self.ptr(f'pop{pop.id}__{n}')};")
+            return "\n    ".join(decl)
+
+        if glob_eq.strip():
+            code = self.typed(self.fill(glob_eq, post_prefix="anb_post_", post_index="[0]"))
+            names = {q["name"] for q in desc["variables"] if q["locality"] == "global" and q.get("cpp")}
+            loads = "\n    ".join(f"{self.real} {q['name']} = {p(q['name'])}[0];" for q in glob_all)
+            stores = "\n    ".join(f"{p(n)}[0] = {n};" for n in sorted(names))
+            src = f"""
+extern "C" __global__ void __launch_bounds__(32) proj{k}_update_global() {{
+{head}    if (anb_go && threadIdx.x == 0) {{
+    {loads}
+    {refs(code)}
+    {code}
+    {stores}
+    }}
+}}
+"""
+            out.append((src, (f"proj{k}_update_global", 1, 32, 0)))
+        semi_eq = self.typed(self.fill(self._syn_block(proj, "semiglobal"), semi="[anb_row]",
+                                       post_prefix="anb_post_", post_index="[anb_post]"))
+        loc_eq = self.typed(self.fill(self._syn_block(proj, "local"), local="[j]", semi="[anb_row]",
+                                      pre_prefix="anb_pre_", pre_index="[anb_col[j]]",
+                                      post_prefix="anb_post_", post_index="[anb_post]"))
+        if not (semi_eq.strip() or loc_eq.strip()):
+            return out
+        gvals = "\n    ".join(f"const {self.real} {q['name']} = {p(q['name'])}[0];" for q in glob_all)
+        arrays = []
+        for q in desc["variables"] + desc["parameters"]:
+            if q["locality"] in ("local", "semiglobal"):
+                arrays.append(f"{self.real}* __restrict__ {q['name']} = {p(q['name'])};")
+        if "w" not in {q["name"] for q in desc["variables"] + desc["parameters"]}:
+            arrays.append(f"{self.real}* __restrict__ w = {p('w')};")
+        rp_t = lay["idx_t"]
+        src = f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_update() {{
+{head}    {gvals}
+    {chr(10).join('    ' + x for x in arrays).strip()}
+    {refs(semi_eq + loc_eq)}
+    const int* __restrict__ anb_col = {p('col')};
+    const {rp_t}* __restrict__ anb_rp = {p('row_ptr')};
+    const int anb_lane = threadIdx.x & 31;
+    for (int anb_row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_go && anb_row < {lay['rows']};
+         anb_row += (gridDim.x * blockDim.x) >> 5) {{
+      const int anb_post = {p('post_rank')}[anb_row];
+      if (anb_lane == 0) {{
+        {semi_eq}
+      }}
+      __syncwarp();
+      for ({rp_t} j = anb_rp[anb_row] + anb_lane; j < anb_rp[anb_row + 1]; j += 32) {{
+        {loc_eq}
+      }}
+      __syncwarp();
+    }}
+}}
+"""
+        out.append((src, (f"proj{k}_update", grid_for(lay["rows"] * 32), BLOCK, 0)))
+        return out
+
     def timed_array_kernel(self, pop) -> str:
         """TimedArray update (ANNarchy/inputs/TimedArray.py, update_variables):
         internal time tau = t - t0 (modulo the period when positive); when tau
@@ -620,7 +780,8 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_delay() {{
         sum_ = self.ptr(f"pop{proj.post_pop.id}___sum_{proj.target}")
         fmt = lay["format"]
         p = lambda n: self.ptr(f"proj{k}__{n}")
-        W = self.c.wctype
+        # learning projections keep float32 weights (updated every step)
+        W = "float" if (self.rate_learning(proj) and not self.exact) else self.c.wctype
         name = f"proj{k}_psp"
         tdecl = f"const long long t = *{self.ptr('t')};\n    " if self.delayed(proj) else ""
 
@@ -1014,6 +1175,11 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
                 kernels.append(self.delay_kernel(pop))
                 plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))
         for proj in net.projections:
+            if self.rate_learning(proj):
+                for src, entry in self.rate_update_kernels(proj):
+                    kernels.append(src)
+                    plan.append(entry)
+        for proj in net.projections:
             if proj.synapse_type.type == "spike" and proj.desc.get("post_spike"):
                 kernels.append(self.post_event_kernel(proj))
                 plan.append((f"proj{proj.id}_post_event",
@@ -1043,7 +1209,10 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
       }}
     }}
 """
-        if not plan or [p[0] for p in plan].count(plan[-1][0]) > 1 or (len(plan[-1]) > 4 and plan[-1][4]):
+        last_src = next((kk for kk in kernels if f" {plan[-1][0]}()" in kk), "") if plan else ""
+        if not plan or [p[0] for p in plan].count(plan[-1][0]) > 1 or (len(plan[-1]) > 4 and plan[-1][4]) \
+                or re.search(r"\breturn\b", last_src):
+            # (a kernel that may return early cannot carry the step counter's epilogue)
             kernels.append("""
 extern "C" __global__ void anb_tick() {
 }

@@ -324,6 +324,58 @@ def case_spike_analysis(name):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+LEARN_SYNAPSE = dict(
+    parameters="eta = 0.02 : projection\ntau_alpha = 20.0 : projection",
+    equations="""
+        tau_alpha * dalpha/dt + alpha = pos(post.r - 0.5) : postsynaptic
+        dbeta/dt = -0.01 * beta : projection, init=1.0
+        dw/dt = eta * beta * pre.r * post.r - alpha * post.r^2 * w : min=0.0
+    """)
+
+
+def learning_inputs(seed=9, n_in=30, n_out=20):
+    """Rates of the input population and the (pre, post) weight matrix of the
+    rate-coded learning case."""
+    import numpy as np
+    from annarchy_b200 import workloads as wl
+    rng = np.random.default_rng(seed)
+    r_in = rng.uniform(0.0, 1.0, n_in)
+    w = wl.bernoulli_csr(rng, n_out, n_in, 0.4, lambda k: rng.uniform(0.0, 0.3, k))
+    return r_in, w
+
+
+def case_rate_learning(name, steps=200):
+    """A rate-coded network whose synapses learn (semiglobal, local and
+    global equations; min bound on w), one projection updating every step and
+    one every 3 steps from an offset (enable_learning(period, offset))."""
+    import numpy as np
+    import ANNarchy as ann
+    from annarchy_b200 import workloads as wl
+    r_in, w = learning_inputs()
+    net = ann.Network(dt=1.0, seed=1)
+    net.config(num_threads=1)
+    inp = net.create(r_in.size, ann.Neuron(parameters="r = 0.0"))
+    out = net.create(w.shape[0], ann.Neuron(parameters="tau = 10.0",
+                                            equations="tau * dr/dt + r = sum(exc) + sum(mod)"))
+    syn = ann.Synapse(**LEARN_SYNAPSE)
+    p1 = net.connect(inp, out, "exc", synapse=syn)
+    p1.from_sparse(wl.to_from_sparse(w), storage_format="csr")
+    p2 = net.connect(inp, out, "mod", synapse=syn)
+    p2.from_sparse(wl.to_from_sparse(w * 0.5), storage_format="csr")
+    m = net.monitor(out, "r")
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    inp.r = r_in
+    net.simulate(7.0)
+    p2.enable_learning(period=3.0, offset=1.0)
+    net.simulate((steps - 7) * 1.0)
+    out_d = dict(r=np.asarray(m.get("r")),
+                 w1=np.concatenate([np.asarray(d, dtype=np.float64) for d in p1.w]),
+                 w2=np.concatenate([np.asarray(d, dtype=np.float64) for d in p2.w]),
+                 alpha1=np.asarray(p1.alpha, dtype=np.float64), alpha2=np.asarray(p2.alpha, dtype=np.float64),
+                 beta1=np.float64(p1.beta), beta2=np.float64(p2.beta), steps=np.int64(steps))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out_d)
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -336,6 +388,7 @@ CASES = {
     "io": (case_io, {}),
     "connect_patterns": (case_connect_patterns, {}),
     "spike_analysis": (case_spike_analysis, {}),
+    "rate_learning": (case_rate_learning, {}),
 }
 
 
