@@ -159,6 +159,51 @@ class Network:
             print(f"Simulating {duration / 1000.0} seconds of the network took "
                   f"{time.time() - t0} seconds.")
 
+    # -- accessors (ANNarchy/core/Network.py) -------------------------------------------
+    def get_population(self, name: str) -> Population:
+        for pop in self.populations:
+            if pop.name == name:
+                return pop
+        raise ValueError(f"get_population(): no population named {name!r}")
+
+    def get_projection(self, name: str) -> Projection:
+        for proj in self.projections:
+            if proj.name == name:
+                return proj
+        raise ValueError(f"get_projection(): no projection named {name!r}")
+
+    def get_monitor(self, name: str) -> Monitor:
+        for mon in self.monitors:
+            if mon.name == name:
+                return mon
+        raise ValueError(f"get_monitor(): no monitor named {name!r}")
+
+    def get_populations(self) -> list:
+        return list(self.populations)
+
+    def get_projections(self, post=None, pre=None, target=None, suppress_error: bool = False) -> list:
+        """Projections, optionally only those onto `post`, from `pre` or with
+        `target`."""
+        res = [p for p in self.projections
+               if (post is None or p.post_pop is _pop_of(post))
+               and (pre is None or p.pre_pop is _pop_of(pre))
+               and (target is None or p.target == target)]
+        if not res and not suppress_error and (post is not None or pre is not None or target is not None):
+            raise ValueError("get_projections(): no matching projection")
+        return res
+
+    def get_monitors(self) -> list:
+        return list(self.monitors)
+
+    @property
+    def time(self) -> float:
+        """Current simulated time in ms."""
+        return self.get_time()
+
+    @time.setter
+    def time(self, value: float):
+        self.set_time(value)
+
     def enable_learning(self, projections=None, period: float | None = None,
                         offset: float | None = None):
         """Learning on for the given projections (default: all)."""
@@ -283,3 +328,7 @@ class Network:
             self.close()
         except Exception:
             pass
+
+
+def _pop_of(obj):
+    return obj.population if hasattr(obj, "population") and not isinstance(obj, Population) else obj

@@ -179,6 +179,44 @@ class Population:
         from .io import load_data, load_population_data
         load_population_data(self, load_data(filename, pickle_encoding))
 
+    # -- coordinates (ANNarchy/core/Population.py:915-1000) ---------------------------
+    def rank_from_coordinates(self, coord) -> int:
+        """Rank of the neuron at `coord` (row-major)."""
+        coord = tuple(int(c) for c in np.atleast_1d(coord))
+        if len(coord) != len(self.geometry) or any(not 0 <= c < g for c, g in zip(coord, self.geometry)):
+            raise ValueError(f"rank_from_coordinates(): there is no neuron of coordinates {coord} "
+                             f"in the population {self.name} {self.geometry}")
+        return int(np.ravel_multi_index(coord, self.geometry))
+
+    def coordinates_from_rank(self, rank: int) -> tuple:
+        """Coordinates of neuron `rank` (row-major)."""
+        if not 0 <= int(rank) < self.size:
+            raise ValueError(f"the given rank {rank} is larger than the size of the population "
+                             f"{self.size}")
+        c = np.unravel_index(int(rank), self.geometry)
+        return tuple(int(x) for x in c)
+
+    def normalized_coordinates_from_rank(self, rank: int, norm: float = 1.0) -> tuple:
+        """Coordinates mapped to [0, 1]^d. Up to three dimensions the
+        reference rounds them to float32 and ignores `norm`
+        (cython_ext/Coordinates.pyx:122-176); beyond, norm * c / (extent - 1)."""
+        coord = self.coordinates_from_rank(rank)
+        if len(self.geometry) <= 3:
+            return tuple(float(np.float32(c / (g - 1))) if g > 1 else 0.0
+                         for c, g in zip(coord, self.geometry))
+        return tuple(norm * float(c) / float(g - 1) if g > 1 else 0.0
+                     for c, g in zip(coord, self.geometry))
+
+    @property
+    def dimension(self) -> int:
+        return len(self.geometry)
+
+    @property
+    def refractory(self):
+        """Refractory period in ms (a value, or one per neuron when they differ)."""
+        r = self._refractory_ms
+        return float(r[0]) if r.size and np.all(r == r[0]) else r.copy()
+
     def set_refractory(self, value):
         self._refractory_ms = draw(value, (self.size,), self._rng())
         self._has_refractory = self._has_refractory or bool(np.any(self._refractory_ms > 0))

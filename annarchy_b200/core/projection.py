@@ -671,8 +671,168 @@ class Projection:
         return self
 
     def dendrite_sizes(self):
+        if getattr(self, "_device_conn", None):
+            lengths = getattr(self, "_device_lengths", None)
+            return np.asarray(lengths if lengths is not None else [], dtype=np.int64)
         lengths = np.diff(self._csr.indptr)
         return lengths[lengths > 0]
+
+    # -- dendrites and matrices (ANNarchy/core/Projection.py:841-1016, 1515-1730) --------
+    def nb_synapses_per_dendrite(self) -> list:
+        """Synapses of every dendrite (post neuron with synapses)."""
+        return [int(x) for x in self.dendrite_sizes()]
+
+    def _pre_ranks_of(self) -> list:
+        """Pre-synaptic ranks of every dendrite."""
+        m = self._csr
+        rows = np.nonzero(np.diff(m.indptr) > 0)[0]
+        return [self.pre_ranks[m.indices[m.indptr[r]:m.indptr[r + 1]]].tolist() for r in rows]
+
+    def dendrites(self):
+        """The dendrites in ascending post rank."""
+        for idx, n in enumerate(self.post_ranks):
+            yield Dendrite(self, n, idx)
+
+    def __iter__(self):
+        return self.dendrites()
+
+    def dendrite(self, post):
+        """The dendrite of a post-synaptic neuron (rank or coordinates)."""
+        rank = int(post) if np.ndim(post) == 0 else self.post_pop.rank_from_coordinates(post)
+        ranks = self.post_ranks
+        if rank not in ranks:
+            raise ValueError(f"the neuron of rank {rank} has no dendrite in this projection")
+        return Dendrite(self, rank, ranks.index(rank))
+
+    def __getitem__(self, *args):
+        return self.dendrite(args[0] if len(args) == 1 else args)
+
+    def synapse(self, pre: int, post: int):
+        """The synapse between two neurons (an IndividualSynapse), or None."""
+        if np.ndim(pre) != 0 or np.ndim(post) != 0:
+            raise ValueError("Projection.synapse() only accepts ranks for the pre and post neurons")
+        return self.dendrite(post).synapse(pre)
+
+    def connectivity_matrix(self, fill: float = 0.0) -> np.ndarray:
+        """Dense (post, pre) matrix of the weights over the whole populations,
+        `fill` where there is no synapse."""
+        res = np.ones((self.post_pop.size, self.pre_pop.size)) * fill
+        w = self.get("w")
+        for idx, (rank, pre) in enumerate(zip(self.post_ranks, self._pre_ranks_of())):
+            res[rank, pre] = w[idx]
+        return res
+
+    def receptive_fields(self, variable: str = "w", in_post_geometry: bool = True) -> np.ndarray:
+        """All receptive fields of a projection between 2-D populations, tiled
+        in the post-synaptic geometry (or a square grid), with a zero first
+        row as the reference builds it."""
+        import math
+        if in_post_geometry:
+            x_size, y_size = self.post_pop.geometry[1], self.post_pop.geometry[0]
+        else:
+            x_size = int(math.floor(math.sqrt(self.post_pop.size)))
+            y_size = int(math.ceil(math.sqrt(self.post_pop.size)))
+        ranks = self.post_ranks
+        pre = self._pre_ranks_of()
+        vals = self.get(variable)
+        geo = self.pre_pop.geometry
+
+        def rf(post_rank):
+            if post_rank not in ranks:
+                return np.zeros(geo)
+            i = ranks.index(post_rank)
+            res = np.zeros(self.pre_pop.size)
+            if len(res) == len(pre[i]):
+                res[pre[i]] = vals[i]
+            return res.reshape(geo)
+
+        res = np.zeros((1, x_size * geo[1]))
+        for y in range(y_size):
+            row = np.concatenate([rf(self.post_pop.rank_from_coordinates((y, x))) for x in range(x_size)],
+                                 axis=1)
+            res = np.concatenate((res, row))
+        return res
+
+    def save_connectivity(self, filename: str):
+        """Ranks, weights and delays in the reference's connectivity file
+        layout (.npz, .gz, .mat or pickle), loadable with from_file()."""
+        import os
+        import pickle
+        path = os.path.dirname(filename)
+        if path and not os.path.isdir(path):
+            os.makedirs(path)
+        delay = self.delay
+        data = {"name": self.name, "post_ranks": self.post_ranks,
+                "pre_ranks": np.array(self._pre_ranks_of(), dtype=object),
+                "w": np.array(self.get("w"), dtype=object),
+                "delay": np.array(delay, dtype=object) if isinstance(delay, list) else delay,
+                "max_delay": self.max_delay, "uniform_delay": self.uniform_delay,
+                "size": self.size, "nb_synapses": self.nb_synapses}
+        ext = os.path.splitext(filename)[1]
+        if ext == ".gz":
+            import gzip
+            with gzip.open(filename, mode="wb") as f:
+                pickle.dump(data, f, protocol=pickle.HIGHEST_PROTOCOL)
+        elif ext == ".npz":
+            np.savez_compressed(filename, **data)
+        elif ext == ".mat":
+            import scipy.io as sio
+            sio.savemat(filename, {k: (0 if v is None else v) for k, v in data.items()})
+        else:
+            with open(filename, mode="wb") as f:
+                pickle.dump(data, f, protocol=pickle.HIGHEST_PROTOCOL)
+
+    def from_file(self, filename: str, pickle_encoding=None, storage_format=None,
+                  storage_order=None):
+        """Connectivity, weights and delays saved by save_connectivity()
+        (ANNarchy/core/ConnectorMethods.py:799-890)."""
+        import gzip
+        import pickle
+        if filename.endswith(".npz"):
+            raw = np.load(filename, allow_pickle=True, **({} if pickle_encoding is None
+                                                          else {"encoding": pickle_encoding}))
+            data = {k: (raw[k].item() if raw[k].dtype == object and raw[k].ndim == 0 else raw[k])
+                    for k in raw.files}
+        else:
+            opener = gzip.open if filename.endswith(".gz") else open
+            with opener(filename, mode="rb") as f:
+                data = pickle.load(f, **({} if pickle_encoding is None else {"encoding": pickle_encoding}))
+        post = [int(r) for r in np.asarray(data["post_ranks"]).ravel()]
+        pre = [list(map(int, r)) for r in data["pre_ranks"]]
+        w_raw = data["w"]
+        if np.ndim(w_raw) == 0 or (isinstance(w_raw, np.ndarray) and w_raw.size == 1
+                                   and w_raw.dtype != object):
+            w = [np.full(len(p), float(np.asarray(w_raw).ravel()[0])) for p in pre]
+        else:
+            w = [np.atleast_1d(np.asarray(x, dtype=np.float64)) for x in w_raw]
+        pos_post = {int(r): i for i, r in enumerate(self.post_ranks_view)}
+        pos_pre = {int(r): i for i, r in enumerate(self.pre_ranks)}
+        rows = np.concatenate([np.full(len(p), pos_post[r]) for r, p in zip(post, pre)]) if pre else []
+        cols = np.concatenate([[pos_pre[c] for c in p] for p in pre]).astype(np.int64) if pre else []
+        m = sp.csr_matrix((np.concatenate(w) if w else [], (rows, cols)),
+                          shape=(len(self.post_ranks_view), len(self.pre_ranks)))
+        delay = data.get("delay")
+        if isinstance(delay, np.ndarray) and delay.dtype == object and delay.ndim > 0:
+            dm = sp.csr_matrix((np.concatenate([np.atleast_1d(np.asarray(x, dtype=np.float64))
+                                                for x in delay]), (rows, cols)), shape=m.shape)
+            return self._store(m, "From File", storage_format, None, dm)
+        d = 0.0 if delay is None else float(np.asarray(delay).ravel()[0])
+        return self._store(m, "From File", storage_format, d)
+
+    connect_from_file = from_file
+
+    def reset(self, attributes=-1, synapses: bool = False):
+        """Synaptic variables (not the weights) back to their initial values
+        (ANNarchy/core/Projection.py:841-880)."""
+        if synapses:
+            raise NotImplementedError("Projection.reset(synapses=True) is not supported by this "
+                                      "backend")
+        if self.net is not None and self.net._compiled:
+            self.net._backend.reset_projection(self)
+        for name in list(self._host_semi):
+            init = next((v["init"] for v in self.desc["variables"] if v["name"] == name), 0.0)
+            if not isinstance(init, str):
+                self.set({name: float(init)})
 
     @property
     def post_ranks(self):
@@ -681,3 +841,74 @@ class Projection:
     def __repr__(self):
         return (f"Projection({self.name!r}, {self.pre_pop.name}->{self.post_pop.name}, "
                 f"target={self.target!r}, {self.nb_synapses} synapses, {self._storage_format})")
+
+
+class IndividualSynapse:
+    """One synapse of a dendrite: its attributes by name."""
+
+    def __init__(self, dendrite, pre: int):
+        object.__setattr__(self, "dendrite", dendrite)
+        object.__setattr__(self, "pre", int(pre))
+        object.__setattr__(self, "idx", dendrite.pre_ranks.index(int(pre)))
+
+    def __getattr__(self, name):
+        return self.dendrite.get(name)[self.idx]
+
+    def __setattr__(self, name, value):
+        vals = np.asarray(self.dendrite.get(name), dtype=np.float64).copy()
+        vals[self.idx] = value
+        self.dendrite.set({name: vals})
+
+
+class Dendrite:
+    """The synapses of one post-synaptic neuron (ANNarchy/core/Dendrite.py):
+    `pre_ranks`, `size`, attributes by name."""
+
+    def __init__(self, proj, post_rank: int, idx: int):
+        object.__setattr__(self, "proj", proj)
+        object.__setattr__(self, "post_rank", int(post_rank))
+        object.__setattr__(self, "idx", int(idx))
+        object.__setattr__(self, "pre_ranks", proj._pre_ranks_of()[idx])
+
+    @property
+    def size(self) -> int:
+        return len(self.pre_ranks)
+
+    def __len__(self):
+        return self.size
+
+    def get(self, name: str):
+        if name in self.proj._host_semi:
+            return self.proj.get(name)[self.idx]
+        v = self.proj.get(name)
+        return v[self.idx] if isinstance(v, list) else v
+
+    def set(self, values: dict):
+        for name, value in values.items():
+            if name in self.proj._host_semi:
+                allv = np.asarray(self.proj.get(name), dtype=np.float64).copy()
+                allv[self.idx] = float(value)
+                self.proj.set({name: allv})
+                continue
+            rows = self.proj.get(name)
+            rows[self.idx] = np.broadcast_to(np.asarray(value, dtype=np.float64), (self.size,)).copy()
+            self.proj.set({name: rows})
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        return self.get(name)
+
+    def __setattr__(self, name, value):
+        self.set({name: value})
+
+    def synapse(self, pos: int):
+        if int(pos) not in self.pre_ranks:
+            return None
+        return IndividualSynapse(self, pos)
+
+    def receptive_field(self, variable: str = "w", fill: float = 0.0) -> np.ndarray:
+        """The values over the pre-synaptic geometry (`fill` elsewhere)."""
+        res = np.ones(self.proj.pre_pop.size) * fill
+        res[self.pre_ranks] = self.get(variable)
+        return res.reshape(self.proj.pre_pop.geometry)

@@ -376,6 +376,27 @@ def case_rate_learning(name, steps=200):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out_d)
 
 
+def case_connectivity_file(name):
+    """A connectivity file written by the reference's
+    Projection.save_connectivity() (ragged dendrites, a uniform delay), its
+    dense connectivity matrix and receptive fields."""
+    import numpy as np
+    import ANNarchy as ann
+    from annarchy_b200 import workloads as wl
+    rng = np.random.default_rng(17)
+    w = wl.bernoulli_csr(rng, 12, 15, 0.3, lambda k: rng.uniform(0.1, 1.0, k))
+    net = ann.Network(dt=0.5, seed=1)
+    net.config(num_threads=1)
+    a = net.create((3, 5), ann.Neuron(parameters="r = 0.0"))
+    b = net.create((4, 3), ann.Neuron(equations="r = sum(exc)"))
+    p = net.connect(a, b, "exc")
+    p.from_sparse(wl.to_from_sparse(w), delays=1.5, storage_format="lil")
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    p.save_connectivity(os.path.join(HERE, "connectivity_ref.npz"))
+    np.savez_compressed(os.path.join(HERE, name + "_meta.npz"), matrix=p.connectivity_matrix(),
+                        rf=p.receptive_fields())
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -389,6 +410,7 @@ CASES = {
     "connect_patterns": (case_connect_patterns, {}),
     "spike_analysis": (case_spike_analysis, {}),
     "rate_learning": (case_rate_learning, {}),
+    "connectivity_file": (case_connectivity_file, {}),
 }
 
 
