@@ -140,6 +140,7 @@ class CompiledNetwork:
             mod = gen.grid_module()
         self.module = mod
         nat.load_module(mod.source, mod.options)
+        self.write_constants()
         if mod.local is not None:
             nat.set_local_kernel(*mod.local)
         else:
@@ -173,6 +174,7 @@ class CompiledNetwork:
             mod = gen.cluster_module()
             try:
                 self.native.load_module(mod.source, mod.options)
+                self.write_constants()
                 self.native.set_local_kernel(*mod.local)
             except BackendError as exc:
                 last_err = exc
@@ -684,6 +686,11 @@ class CompiledNetwork:
         if not self.mon_layout:
             return 1 << 30
         return min(l["cap_steps"] for l in self.mon_layout.values())
+
+    def write_constants(self):
+        """The network constants' values into the loaded module."""
+        for name, c in self.net._constants.items():
+            self.native.set_constant(name, c.value)
 
     def run_until(self, nsteps: int, pops, or_and: bool) -> int:
         """At most nsteps steps, ending after the first step at which the

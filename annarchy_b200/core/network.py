@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import math
 import time
+import weakref
 
 import numpy as np
 
@@ -43,6 +44,11 @@ class Network:
         self._compiled = False
         self._backend = None
         self._t_python = 0
+        # constants usable in equations: the global ones, then this network's
+        self._constants: dict[str, Constant] = {}
+        for c in GLOBAL_CONSTANTS.values():
+            self._constants[c.name] = Constant(c.name, c.value, net=self)
+        _LIVE.add(self)
 
     # ----------------------------------------------------------- construction
     def config(self, **kwargs):
@@ -158,6 +164,21 @@ class Network:
         if measure_time:
             print(f"Simulating {duration / 1000.0} seconds of the network took "
                   f"{time.time() - t0} seconds.")
+
+    # -- constants (ANNarchy/core/Network.py:482-510, core/Constant.py) -------------------
+    def constant(self, name: str, value: float) -> "Constant":
+        """A constant usable by name in every equation of this network."""
+        if self._compiled:
+            raise RuntimeError("constants must be added before compile() in this backend")
+        c = Constant(name, value, net=self)
+        self._constants[name] = c
+        return c
+
+    def get_constant(self, name: str) -> "Constant":
+        return self._constants[name]
+
+    def get_constants(self) -> list:
+        return list(self._constants.values())
 
     # -- accessors (ANNarchy/core/Network.py) -------------------------------------------
     def get_population(self, name: str) -> Population:
@@ -332,3 +353,46 @@ class Network:
 
 def _pop_of(obj):
     return obj.population if hasattr(obj, "population") and not isinstance(obj, Population) else obj
+
+
+GLOBAL_CONSTANTS: dict[str, "Constant"] = {}
+
+
+class Constant(float):
+    """A named value usable in the equations of every neuron and synapse
+    (ANNarchy/core/Constant.py): `Constant(name, value)` at the module level
+    is seen by the networks created afterwards, `net.constant(name, value)`
+    by one network. An attribute of the same name hides it. `set()` changes
+    the value, also after compile(); a constant built from others keeps the
+    value it had."""
+
+    def __new__(cls, name: str, value: float, net=None):
+        return float.__new__(cls, value)
+
+    def __init__(self, name: str, value: float, net=None):
+        self.name = name
+        self.value = float(value)
+        self.net = net
+        if net is None:
+            GLOBAL_CONSTANTS[name] = self
+
+    def set(self, value: float):
+        """New value (for the networks created from a global constant: in each)."""
+        self.value = float(value)
+        nets = [self.net] if self.net is not None else [n for n in _LIVE if name_in(n, self.name)]
+        for n in nets:
+            c = n._constants.get(self.name)
+            if c is not None and c is not self:
+                c.value = float(value)
+            if n._compiled:
+                n._backend.native.set_constant(self.name, float(value))
+
+    def __repr__(self):
+        return f"Constant({self.name!r}, {self.value})"
+
+
+def name_in(net, name: str) -> bool:
+    return name in getattr(net, "_constants", {})
+
+
+_LIVE = weakref.WeakSet()             # networks that see the global constants

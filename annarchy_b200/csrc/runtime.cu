@@ -604,6 +604,27 @@ int anb_module_load(anb_net* net, const char* source, const char* options) {
   return bind(net);
 }
 
+int anb_module_set_constant(anb_net* net, const char* name, double value) {
+  if (!net || !name) return fail(ANB_ERR_ARG, "NULL argument");
+  if (!net->module) return fail(ANB_ERR_STATE, "no module loaded");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  CUdeviceptr dptr = 0;
+  size_t sz = 0;
+  CUresult r = g_drv.moduleGetGlobal(&dptr, &sz, net->module, name);
+  if (r != CUDA_SUCCESS) return fail(ANB_ERR_ARG, std::string("no constant named ") + name);
+  if (sz == 8) {
+    ANB_CUDA(cudaMemcpyAsync((void*)dptr, &value, 8, cudaMemcpyHostToDevice, net->stream));
+  } else if (sz == 4) {
+    const float f = (float)value;
+    ANB_CUDA(cudaMemcpyAsync((void*)dptr, &f, 4, cudaMemcpyHostToDevice, net->stream));
+  } else {
+    return fail(ANB_ERR_ARG, std::string(name) + " is not a float or double constant");
+  }
+  ANB_CUDA(cudaStreamSynchronize(net->stream));
+  return ANB_OK;
+}
+
 int anb_nvrtc_compile(const char* source, const char* options, char* log, size_t log_len,
                       size_t* cubin_bytes) {
   if (!source) return fail(ANB_ERR_ARG, "source is NULL");

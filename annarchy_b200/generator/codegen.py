@@ -1614,6 +1614,9 @@ anb_cluster_run(long long t0, int nsteps) {{
         self.ptr("dt")
         self.ptr("err")
         decl = "\n".join(f"__constant__ {ct}* anb_p_{name};" for name, ct in sorted(self.decls.items()))
+        # network constants usable in every equation (set through anb_module_set_constant);
+        # an attribute of the same name hides them, as in the reference
+        consts = "".join(f"__constant__ {self.real} {c};\n" for c in sorted(self.net._constants))
         types = "".join(self.types[k] for k in sorted(self.types))
         return (f"// generated by annarchy_b200 for network {self.net.id}\n{header}\n"
-                f"typedef {self.real} real;\n{types}{decl}\n" + "".join(kernels))
+                f"typedef {self.real} real;\n{types}{consts}{decl}\n" + "".join(kernels))

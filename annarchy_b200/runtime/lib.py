@@ -51,6 +51,7 @@ SIGNATURES = {
                                                      C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
     "anb_csr_to_csc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
     "anb_set_stop_kernel": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_uint, C.c_uint, C.c_int]),
+    "anb_module_set_constant": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double]),
     "anb_run_until": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.c_int, C.c_int,
                                 C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     "anb_nvrtc_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t,
@@ -375,6 +376,10 @@ class NativeNet:
     def run(self, steps: int):
         check("anb_run", self.lib.anb_run(self.h, int(steps)))
 
+    def set_constant(self, name: str, value: float):
+        check("anb_module_set_constant", self.lib.anb_module_set_constant(self.h, name.encode(),
+                                                                        float(value)))
+
     def set_stop_kernel(self, pop: int, kernel: str, grid: int, block: int, all_mode: bool):
         check("anb_set_stop_kernel", self.lib.anb_set_stop_kernel(
             self.h, int(pop), kernel.encode(), int(grid), int(block), 1 if all_mode else 0))
@@ -483,6 +488,9 @@ class DryNative:
 
     def set_local_kernel(self, *a):
         self.local = a
+
+    def set_constant(self, *a):
+        pass
 
     def set_stop_kernel(self, *a):
         pass

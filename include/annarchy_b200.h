@@ -163,6 +163,12 @@ int anb_csr_to_csc(anb_net* net, const char* prefix, int n_pre, int with_weights
  * (ANNarchy/generator/Compiler.py:496-596). */
 int anb_module_load(anb_net* net, const char* source, const char* options);
 
+/* Value of a module-scope constant of the loaded module (a float or double
+ * `__constant__` variable named `name`, written in its own precision).
+ * Replaces the generated module's set_<constant>(double)
+ * (ANNarchy/generator/NanoBind/BaseTemplate.py:1-45, core/Constant.py). */
+int anb_module_set_constant(anb_net* net, const char* name, double value);
+
 /* Compile-only check of a generated module (no device needed): NVRTC for
  * sm_100a; the compiler log is copied into `log` (may be NULL) and the cubin
  * size into *cubin_bytes. */
