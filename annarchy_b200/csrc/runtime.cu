@@ -612,7 +612,8 @@ int anb_module_set_constant(anb_net* net, const char* name, double value) {
   CUdeviceptr dptr = 0;
   size_t sz = 0;
   CUresult r = g_drv.moduleGetGlobal(&dptr, &sz, net->module, name);
-  if (r != CUDA_SUCCESS) return fail(ANB_ERR_ARG, std::string("no constant named ") + name);
+  if (r == CUDA_ERROR_NOT_FOUND) return ANB_OK;  // declared but used by no kernel: removed
+  if (r != CUDA_SUCCESS) return fail(ANB_ERR_ARG, std::string("constant ") + name + " not accessible");
   if (sz == 8) {
     ANB_CUDA(cudaMemcpyAsync((void*)dptr, &value, 8, cudaMemcpyHostToDevice, net->stream));
   } else if (sz == 4) {

@@ -164,7 +164,9 @@ int anb_csr_to_csc(anb_net* net, const char* prefix, int n_pre, int with_weights
 int anb_module_load(anb_net* net, const char* source, const char* options);
 
 /* Value of a module-scope constant of the loaded module (a float or double
- * `__constant__` variable named `name`, written in its own precision).
+ * `__constant__` variable named `name`, written in its own precision; a
+ * constant no kernel uses may be absent from the module, which is not an
+ * error).
  * Replaces the generated module's set_<constant>(double)
  * (ANNarchy/generator/NanoBind/BaseTemplate.py:1-45, core/Constant.py). */
 int anb_module_set_constant(anb_net* net, const char* name, double value);

@@ -29,11 +29,15 @@ def test_constants_compile_and_shadow():
 
 
 def test_global_constants_reach_new_networks():
+    from annarchy_b200.core.network import GLOBAL_CONSTANTS
     g = Constant("anb_test_gain", 3.0)
-    net = Network(dt=1.0)
-    assert net.get_constant("anb_test_gain").value == 3.0
-    g.set(4.0)
-    assert net.get_constant("anb_test_gain").value == 4.0
+    try:
+        net = Network(dt=1.0)
+        assert net.get_constant("anb_test_gain").value == 3.0
+        g.set(4.0)
+        assert net.get_constant("anb_test_gain").value == 4.0
+    finally:
+        GLOBAL_CONSTANTS.pop("anb_test_gain", None)
 
 
 @pytest.mark.gpu
