@@ -533,10 +533,11 @@ class Projection:
             if self.net is not None and self.net._compiled:
                 return self.net._backend.read_projection_attribute(self, name)
             return self._host_semi[name].copy()
-        if name not in self._attr_names() and name not in {p["name"] for p in self.desc["parameters"]}:
-            raise AttributeError(f"projection {self.name!r} has no attribute {name!r}")
         glob = {p["name"]: p for p in self.desc["parameters"] + self.desc["variables"]
                 if p["locality"] == "global"}
+        if name not in self._attr_names() and name not in glob and \
+                name not in {p["name"] for p in self.desc["parameters"]}:
+            raise AttributeError(f"projection {self.name!r} has no attribute {name!r}")
         if name in glob:
             if self.net is not None and self.net._compiled:
                 return float(self.net._backend.read_projection_attribute(self, name)[0])
@@ -604,7 +605,9 @@ class Projection:
         if desc is not None and (self.__dict__.get("_csr") is not None or
                                  self.__dict__.get("_device_conn")) and (
                 name == "w" or name in self.__dict__.get("_host_attr", {}) or
-                name in self.__dict__.get("_host_semi", {})):
+                name in self.__dict__.get("_host_semi", {}) or
+                name in {p["name"] for p in desc["parameters"] + desc["variables"]
+                         if p["locality"] == "global"}):
             self.set({name: value})
             return
         object.__setattr__(self, name, value)

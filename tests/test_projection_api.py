@@ -72,3 +72,17 @@ def test_coordinates_and_accessors():
     assert net.get_population("B") is b and net.get_projection(p.name) is p
     assert net.get_projections(post=b) == [p] and net.get_projections(pre=b, suppress_error=True) == []
     assert net.time == 0.0
+
+
+def test_global_synaptic_attributes():
+    """Projection-level parameters and variables read and assign through
+    get/set (before compile they are kept for the device arrays)."""
+    from annarchy_b200 import Synapse
+    net, a, b = _net()
+    syn = Synapse(parameters="eta = 0.02 : projection",
+                  equations="dbeta/dt = -beta : projection, init=1.0\ndw/dt = eta * beta")
+    p = net.connect(a, b, "exc", synapse=syn).all_to_all(0.5)
+    assert p.beta == 1.0 and p.eta == 0.02
+    p.beta = 0.25
+    p.eta = 0.5
+    assert "beta" not in p.__dict__ and p.beta == 0.25 and p.get("eta") == 0.5
