@@ -207,6 +207,20 @@ class Population:
         return tuple(norm * float(c) / float(g - 1) if g > 1 else 0.0
                      for c, g in zip(coord, self.geometry))
 
+    def enable(self):
+        """Not supported: populations are always updated in this backend."""
+        raise NotImplementedError("Population.enable()/disable() are not supported by this backend")
+
+    def disable(self):
+        """Not supported: populations are always updated in this backend."""
+        raise NotImplementedError("Population.enable()/disable() are not supported by this backend")
+
+    def compute_firing_rate(self, window: float):
+        """Not supported (record spikes with a monitor and use its
+        population_rate() or smoothed_rate())."""
+        raise NotImplementedError("Population.compute_firing_rate() is not supported by this "
+                                  "backend; record spikes and use Monitor.smoothed_rate()")
+
     @property
     def dimension(self) -> int:
         return len(self.geometry)
