@@ -127,6 +127,8 @@ def projection_data(proj) -> dict:
     for name in desc["attributes"]:
         if name in glob:
             desc[name] = proj.get(name)
+        elif name in proj._host_semi:                     # one value per dendrite
+            desc[name] = np.asarray(proj.get(name), dtype=np.float64)
         elif name in proj._attr_names():
             desc[name] = _per_dendrite([np.asarray(v) for v in proj.get(name)])
     return desc
@@ -169,6 +171,8 @@ def load_projection_data(proj, desc: dict):
             continue
         if v["locality"] == "global":
             proj.set({name: float(np.asarray(desc[name]).reshape(-1)[0])})
+        elif name in proj._host_semi:
+            proj.set({name: np.asarray(desc[name], dtype=np.float64).reshape(-1)})
         elif name in proj._attr_names():
             proj.set({name: [np.atleast_1d(np.asarray(x, dtype=np.float64)) for x in desc[name]]})
 

@@ -86,3 +86,21 @@ def test_global_synaptic_attributes():
     p.beta = 0.25
     p.eta = 0.5
     assert "beta" not in p.__dict__ and p.beta == 0.25 and p.get("eta") == 0.5
+
+
+def test_save_load_semiglobal(tmp_path):
+    """Per-dendrite (post-synaptic) variables are saved as one value per
+    dendrite and loaded back."""
+    from annarchy_b200 import Synapse
+    syn = Synapse(parameters="eta = 0.02 : projection",
+                  equations=["dalpha/dt = -alpha : postsynaptic", "dw/dt = eta * alpha"])
+    net, a, b = _net()
+    p = net.connect(a, b, "exc", synapse=syn).all_to_all(0.5)
+    p.alpha = np.arange(12.0)
+    path = str(tmp_path / "p.npz")
+    p.save(path)
+    net2, a2, b2 = _net()
+    q = net2.connect(a2, b2, "exc", synapse=syn).all_to_all(0.1)
+    q.load(path)
+    np.testing.assert_array_equal(q.alpha, np.arange(12.0))
+    np.testing.assert_array_equal(q.get("w", flat=True), np.full(180, 0.5))
