@@ -14,7 +14,7 @@ the ANNarchy neural simulator.
 from .core.models import IF_cond_exp, LeakyIntegrator, Neuron, STDP, Synapse
 from .core.inputs import PoissonPopulation, TimedArray
 from .core.monitor import Monitor
-from .core.network import Constant, Network
+from .core.network import Constant, Network, every
 from .core.population import Population, PopulationView
 from .core.projection import Projection
 from .core.random import (DiscreteUniform, Exponential, LogNormal, Normal, RandomDistribution,
@@ -27,4 +27,4 @@ __version__ = "0.1.0"
 __all__ = ["Network", "Neuron", "Synapse", "Population", "PopulationView", "Projection",
            "Monitor", "PoissonPopulation", "TimedArray", "Uniform", "Normal", "LogNormal", "Exponential", "DiscreteUniform",
            "RandomDistribution", "LeakyIntegrator", "IF_cond_exp", "STDP", "float32", "float64",
-           "Constant"]
+           "Constant", "every"]

@@ -49,6 +49,8 @@ class Network:
         for c in GLOBAL_CONSTANTS.values():
             self._constants[c.name] = Constant(c.name, c.value, net=self)
         _LIVE.add(self)
+        self._callbacks: list = []            # `every` decorators (Simulate.py:352-446)
+        self._callbacks_enabled = True
 
     # ----------------------------------------------------------- construction
     def config(self, **kwargs):
@@ -155,12 +157,15 @@ class Network:
     def _steps(self, duration: float) -> int:
         return int(math.ceil(float(duration) / self.dt))
 
-    def simulate(self, duration: float, measure_time: bool = False):
+    def simulate(self, duration: float, measure_time: bool = False, callbacks: bool = True):
         if not self._compiled:
             raise RuntimeError("simulate(): the network is not compiled yet")
         n = self._steps(duration)
         t0 = time.time()
-        self._backend.run(n)
+        if callbacks and self._callbacks_enabled and self._callbacks:
+            self._simulate_with_callbacks(duration)
+        else:
+            self._backend.run(n)
         if measure_time:
             print(f"Simulating {duration / 1000.0} seconds of the network took "
                   f"{time.time() - t0} seconds.")
@@ -254,6 +259,43 @@ class Network:
             print(f"Simulating {done * self.dt / 1000.0} seconds of the network took "
                   f"{time.time() - t0} seconds.")
         return done * self.dt
+
+    # -- callbacks (ANNarchy/core/Simulate.py:314-446) -------------------------------
+    def callback_times(self, t_start: int, duration: float) -> list:
+        """(step, callback, n) of every call during a simulation of
+        `duration` ms from step t_start, in time order (declaration order at
+        equal steps)."""
+        length = int(duration / self.dt)
+        times = []
+        for c in self._callbacks:
+            period = int(c.period / self.dt)
+            offset = int(c.offset / self.dt) % period
+            wait = int(c.wait / self.dt)
+            for n, m in enumerate(range(t_start + wait + offset, t_start + length, period)):
+                times.append((m, c, n))
+        return sorted(times, key=lambda x: x[0])
+
+    def _simulate_with_callbacks(self, duration: float):
+        t_start = self.current_step
+        length = int(duration / self.dt)
+        for step, cb, n in self.callback_times(t_start, duration):
+            if step != self.current_step:
+                self._backend.run(step - self.current_step)
+            cb.func(n)
+        if self.current_step < t_start + length:
+            self._backend.run(t_start + length - self.current_step)
+
+    def callbacks_enabled(self) -> bool:
+        return self._callbacks_enabled
+
+    def enable_callbacks(self):
+        self._callbacks_enabled = True
+
+    def disable_callbacks(self):
+        self._callbacks_enabled = False
+
+    def clear_all_callbacks(self):
+        self._callbacks.clear()
 
     def simulate_steps(self, nsteps: int):
         if not self._compiled:
@@ -396,3 +438,30 @@ def name_in(net, name: str) -> bool:
 
 
 _LIVE = weakref.WeakSet()             # networks that see the global constants
+
+
+class every:
+    """Decorator of a function called periodically during simulate()
+    (ANNarchy/core/Simulate.py:352-406): every `period` ms (at least dt),
+    `offset` ms into the period (negative: from its end), after `wait` ms,
+    counted from the start of each simulate() call; the function receives
+    the call count n.
+
+        @every(network=net, period=100.0, offset=-10.0)
+        def step_input(n):
+            pop.I = float(n) / 100.0
+    """
+
+    def __init__(self, network=None, period: float = 1.0, offset: float = 0.0, wait: float = 0.0):
+        if network is None:
+            raise ValueError("every(): pass the network (this backend has no default network)")
+        self.network = network
+        network._callbacks.append(self)
+        self.period = max(float(period), network.dt)
+        self.offset = min(float(offset), self.period)
+        self.wait = max(float(wait), 0.0)
+        self.func = None
+
+    def __call__(self, f):
+        self.func = f
+        return f
