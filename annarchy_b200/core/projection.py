@@ -202,6 +202,16 @@ class Projection:
             return self._store(m, "Connectivity matrix", storage_format, None, D.T if pre_post else D)
         return self._store(m, "Connectivity matrix", storage_format, delays)
 
+    def _drops_self(self, allow_self_connections: bool) -> bool:
+        """Whether a random connector leaves out the pairs with pre rank ==
+        post rank. The reference allows them as soon as pre and post are
+        different objects (ANNarchy/core/ConnectorMethods.py:283-284,
+        344-345, 410-411 compare the objects, not their populations): a view
+        connected to its own population keeps its self-synapses, and so do
+        two views of the same neurons made separately. all_to_all alone
+        compares the populations (ConnectorMethods.py:105-112)."""
+        return not allow_self_connections and self.pre is self.post
+
     def _self_mask(self, rows, cols):
         if self.pre_pop is not self.post_pop:
             return np.ones(rows.shape, dtype=bool)
@@ -344,8 +354,7 @@ class Projection:
             self._device_conn = dict(kind="fixed_probability", probability=float(probability),
                                      **self._device_weights(weights, delays),
                                      seed=int(rng.integers(0, 2**63 - 1)),
-                                     exclude_self=(not allow_self_connections
-                                                   and self.pre_pop is self.post_pop))
+                                     exclude_self=self._drops_self(allow_self_connections))
             self._nnz = int(round(npost * npre * probability))        # until compile()
             self.connector_name = "Random (device)"
             if storage_format is not None:
@@ -360,7 +369,7 @@ class Projection:
             cols_l.append(cc)
         rows = np.concatenate(rows_l) if rows_l else np.zeros(0, np.int64)
         cols = np.concatenate(cols_l) if cols_l else np.zeros(0, np.int64)
-        if not allow_self_connections:
+        if self._drops_self(allow_self_connections):
             keep = self._self_mask(rows, cols)
             rows, cols = rows[keep], cols[keep]
         w = self._weights(weights, rows.size)
@@ -406,21 +415,21 @@ class Projection:
             self._device_conn = dict(kind="fixed_number_pre", number=int(number),
                                      **self._device_weights(weights, delays),
                                      seed=int(rng.integers(0, 2**63 - 1)),
-                                     exclude_self=(not allow_self_connections
-                                                   and self.pre_pop is self.post_pop))
+                                     exclude_self=self._drops_self(allow_self_connections))
             self._nnz = npost * int(number)
             self.connector_name = "Random Convergent (device)"
             if storage_format is not None:
                 self._storage_format = storage_format
             return self
-        avail = npre - (0 if allow_self_connections or self.pre_pop is not self.post_pop else 1)
+        drop_self = self._drops_self(allow_self_connections)
+        avail = npre - (1 if drop_self else 0)
         if number > avail:
             raise ValueError("fixed_number_pre: number exceeds the available pre-synaptic neurons")
         cols = np.empty((npost, number), dtype=np.int64)
         for r0 in range(0, npost, 2048):
             r1 = min(npost, r0 + 2048)
             keys = rng.random((r1 - r0, npre), dtype=np.float32)
-            if not allow_self_connections and self.pre_pop is self.post_pop:
+            if drop_self:
                 pos = {int(r): k for k, r in enumerate(self.pre_ranks)}
                 for i in range(r0, r1):
                     k = pos.get(int(self.post_ranks_view[i]))
@@ -439,7 +448,7 @@ class Projection:
         rng = self._rng()
         npost, npre = len(self.post_ranks_view), len(self.pre_ranks)
         keys = rng.random((npre, npost))
-        if not allow_self_connections and self.pre_pop is self.post_pop:
+        if self._drops_self(allow_self_connections):
             for c in range(npre):
                 hit = np.nonzero(self.post_ranks_view == self.pre_ranks[c])[0]
                 keys[c, hit] = 2.0

@@ -1,18 +1,24 @@
 """Generate the golden fixtures in this folder by running the reference
 simulator (ANNarchy 5.0.3) itself, in its single-thread CPU build.
 
-Run from the repository root, in a container that has the reference sources
-at /root/reference, g++, cmake and the pybind11 wheel in /opt/wheelhouse:
+Run from the repository root, in a container that has the reference
+sources, g++, cmake and the pybind11 wheel in an offline wheelhouse:
 
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py coba_small # one case
 
-Set-up, done once under /tmp/anb_golden (nothing is written to the reference
-tree and no reference source enters this repository):
+Paths (environment variables, with their defaults):
 
-1. copy the reference sources to /tmp/anb_golden/src and build its Cython
-   extensions there (``setup.py build_ext --inplace``);
-2. install pybind11 from the offline wheelhouse into /tmp/anb_golden/pb;
+    ANB_REFERENCE    the reference's source tree (read only)   /root/reference
+    ANB_GOLDEN_WORK  scratch folder for the build and networks  /tmp/anb_golden
+    ANB_WHEELHOUSE   offline wheelhouse holding pybind11        /opt/wheelhouse
+
+Set-up, done once under the scratch folder (nothing is written to the
+reference tree and no reference source enters this repository):
+
+1. copy the reference sources to <work>/src and build its Cython extensions
+   there (``setup.py build_ext --inplace``);
+2. install pybind11 from the offline wheelhouse into <work>/pb;
 3. put ``refshim/`` on PYTHONPATH: an own ``nanobind`` stand-in whose CMake
    config builds the reference's generated wrapper as a pybind11 module, and
    empty ``h5py``/``matplotlib`` modules that the reference imports but these
@@ -35,8 +41,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
-WORK = "/tmp/anb_golden"
+REF = os.environ.get("ANB_REFERENCE", "/root/reference")
+WORK = os.environ.get("ANB_GOLDEN_WORK", "/tmp/anb_golden")
+WHEELHOUSE = os.environ.get("ANB_WHEELHOUSE", "/opt/wheelhouse")
 SRC = os.path.join(WORK, "src")
 PB = os.path.join(WORK, "pb")
 FLAGS = "-march=native -O3 -ffp-contract=off"
@@ -52,7 +59,7 @@ def setup_env() -> dict:
         open(os.path.join(SRC, ".built"), "w").close()
     if not os.path.isdir(os.path.join(PB, "pybind11")):
         subprocess.check_call([sys.executable, "-m", "pip", "install", "--no-index", "--quiet",
-                               "--find-links", "/opt/wheelhouse", "--target", PB, "pybind11"])
+                               "--find-links", WHEELHOUSE, "--target", PB, "pybind11"])
     env = dict(os.environ)
     env["PYTHONPATH"] = os.pathsep.join([SRC, os.path.join(HERE, "refshim"), PB, REPO])
     env["ANB_PYBIND11_INCLUDE"] = os.path.join(PB, "pybind11", "include")
@@ -199,7 +206,7 @@ def case_parser(name):
     import ANNarchy as ann
     from ANNarchy.parser.AnalyseNeuron import analyse_neuron
     from ANNarchy.parser.AnalyseSynapse import analyse_synapse
-    from annarchy_b200.parser.models_catalog import NEURONS, SYNAPSES
+    from models_catalog import NEURONS, SYNAPSES
     net = ann.Network(dt=0.1)
     res = {"neurons": {}, "synapses": {}}
     for key, spec in NEURONS.items():
@@ -397,6 +404,56 @@ def case_connectivity_file(name):
                         rf=p.receptive_fields())
 
 
+def case_self_connections(name):
+    """Which self-synapses the reference's random connectors keep. The
+    decision is made on the objects connected (ConnectorMethods.py:283-284,
+    344-345, 410-411): a view connected to its own population, or two views
+    of the same neurons made separately, keep pre == post pairs; the same
+    object on both sides drops them. Per case: the network seed, then the
+    LIL that the reference's connector builds from a generator seeded like
+    the network's (its post ranks, dendrite sizes and concatenated pre
+    ranks) for fixed_probability, and the number of pre == post pairs for
+    fixed_number_pre and fixed_number_post (whose draws differ from this
+    backend's, so only their self-pair rule is compared)."""
+    import numpy as np
+    import ANNarchy as ann
+    neuron = ann.Neuron(parameters="r = 0.0")
+    out = {}
+    cases = {
+        # key: (kind, seed, population size, pre slice, post slice, argument)
+        "fp_view_to_pop": ("fixed_probability", 3, 60, (40, 60), None, 0.3),
+        "fp_pop_to_view": ("fixed_probability", 4, 60, None, (10, 30), 0.3),
+        "fp_pop_to_pop": ("fixed_probability", 5, 60, None, None, 0.3),
+        "fp_same_view": ("fixed_probability", 6, 60, (0, 40), "same", 0.3),
+        "fp_two_views": ("fixed_probability", 7, 60, (0, 40), (0, 40), 0.3),
+        "fnpre_view_to_pop": ("fixed_number_pre", 8, 60, (40, 60), None, 10),
+        "fnpre_pop_to_pop": ("fixed_number_pre", 9, 60, None, None, 10),
+        "fnpost_view_to_pop": ("fixed_number_post", 10, 60, None, (40, 60), 10),
+        "fnpost_pop_to_pop": ("fixed_number_post", 11, 60, None, None, 10),
+    }
+    for key, (kind, seed, size, pre_sl, post_sl, arg) in cases.items():
+        net = ann.Network(dt=0.1, seed=seed)
+        pop = net.create(size, neuron)
+        pre = pop if pre_sl is None else pop[pre_sl[0]:pre_sl[1]]
+        if post_sl == "same":
+            post = pre
+        else:
+            post = pop if post_sl is None else pop[post_sl[0]:post_sl[1]]
+        proj = net.connect(pre, post, "exc")
+        getattr(proj, kind)(arg, 1.0)
+        lil = proj._connection_method(proj.pre, proj.post, np.random.default_rng(seed),
+                                      *proj._connection_args)
+        post_r = np.asarray(list(lil.post_rank), dtype=np.int64)
+        pre_r = [np.asarray(r, dtype=np.int64) for r in lil.pre_rank]
+        out[key + "__seed"] = np.int64(seed)
+        out[key + "__self_pairs"] = np.int64(sum(int(np.sum(r == p)) for p, r in zip(post_r, pre_r)))
+        if kind == "fixed_probability":
+            out[key + "__post"] = post_r
+            out[key + "__sizes"] = np.asarray([len(r) for r in pre_r], dtype=np.int64)
+            out[key + "__pre"] = np.concatenate(pre_r) if pre_r else np.zeros(0, np.int64)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -411,6 +468,7 @@ CASES = {
     "spike_analysis": (case_spike_analysis, {}),
     "rate_learning": (case_rate_learning, {}),
     "connectivity_file": (case_connectivity_file, {}),
+    "self_connections": (case_self_connections, {}),
 }
 
 

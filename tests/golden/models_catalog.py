@@ -5,7 +5,7 @@ ANNarchy/parser/AnalyseSynapse.py:34).
 Each entry is the keyword arguments of ``Neuron(...)`` / ``Synapse(...)``,
 valid for both this package and the reference.
 """
-from ..workloads import COBA_EQUATIONS, COBA_PARAMS, COBA_RESET, COBA_SPIKE, COBA_REFRACTORY
+from annarchy_b200.workloads import COBA_EQUATIONS, COBA_PARAMS, COBA_RESET, COBA_SPIKE, COBA_REFRACTORY
 
 NEURONS = {
     "input_rate": dict(parameters="r = 0.0"),

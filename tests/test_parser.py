@@ -2,13 +2,16 @@
 catalogue of models (tests/golden/parser_strings.json)."""
 import json
 import os
+import sys
 
 import pytest
 
 from annarchy_b200.core.models import Neuron, Synapse
 from annarchy_b200.parser.analysis import analyse_neuron, analyse_synapse
-from annarchy_b200.parser.models_catalog import NEURONS, SYNAPSES
 from annarchy_b200.parser.text import ParserError
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+from models_catalog import NEURONS, SYNAPSES  # noqa: E402
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "parser_strings.json")))
 
