@@ -7,22 +7,29 @@ I = 20 (the network as specified never fires), seed 42. One bench step =
 1 s of model time (10,000 time steps) from the seeded initial state, with
 the spike raster recorded on the device.
 
-  value      GSynOps/s of the fast path (float state and weights, network
-             state resident in the shared memory of one thread-block cluster),
-             device time (CUDA events)
+  value      GSynOps/s of the exact double-precision path (network state
+             resident in the shared memory of one thread-block cluster),
+             device time (CUDA events); its raster and potentials are
+             checked in the run against the reference's own output
+             (tests/golden/coba_c2.npz)
   e2e        the same through the public API: per step the initial state is
              copied from pinned host memory, the simulation runs, the spike
              raster is decoded on the device and read back as (step, rank)
              pairs, and Monitor.get() builds the per-neuron spike lists
              (wall clock)
+  fast_path  float state and weights on the same engine, with its firing-rate
+             error against the double path (one seed and eight seeds)
   fp64_path  the plain double-precision GPU path (bit-identical to the
-             reference; one kernel per phase, launched every step)
+             reference; one kernel per phase and step), with its CUDA graph
+             and launched step by step
 GSynOps = delivered synaptic events (sum over spikes of the out-degree of
 the spiking neuron, the reference's compute_delivered_spikes,
 ANNarchy/core/Utils.py:209-279) / second. RTF = simulated / wall time.
 
---impl reference runs the CPU oracle (the C restatement of the reference's
-OpenMP step) on all host cores instead.
+--impl reference runs the reference's own OpenMP build (baseline/_ref,
+compiled on this host) at 1 thread and at all cores and reports the faster;
+without it, the C restatement of that step (the oracle). --impl
+reference-cuda times the reference's own CUDA build on this GPU.
 """
 from __future__ import annotations
 
@@ -44,8 +51,9 @@ UNIT = "GSynOps/s"
 WORKLOAD = "coba_lif_4000_p0.02_dt0.1_10000steps_seed42"
 MODEL_STEPS = 10000
 # DRAM bytes (read + write) per launch of the bench's dominant kernel, from one
-# ncu capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum)
-NCU_TRAFFIC = {"anb_cluster_run": 1.193472e6}
+# ncu capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum),
+# keyed by (kernel, precision)
+NCU_TRAFFIC = {("anb_cluster_run", "float"): 1.193472e6}
 
 
 def dist_env():
@@ -165,11 +173,12 @@ def time_device(net, P, mon, cn, steps, warmup):
             kernel_launches[k] = kernel_launches.get(k, 0) + c
         launches += sum(c for _, c in kt.values())
         e, s = events_of(mon, out_deg)
+        last = mon.spike_arrays()
         mon.get("spike")
         events.append(e)
         spikes.append(s)
     return dict(ms=ms, events=events, spikes=spikes, launches=launches, kernel_ms=kernel_ms,
-                kernel_launches=kernel_launches)
+                kernel_launches=kernel_launches, raster=last, v=np.asarray(P.v))
 
 
 def time_graph_free(net, P, mon, cn, steps):
@@ -196,14 +205,15 @@ def time_graph_free(net, P, mon, cn, steps):
     return res
 
 
-def algorithmic_bytes(cn, spikes, events, wbytes, steps=MODEL_STEPS):
+def algorithmic_bytes(cn, spikes, events, wbytes, steps=MODEL_STEPS, sbytes=4):
     """HBM bytes one local-engine launch must move: per delivered event the
     post index (4 B) and the weight; per spike its two column pointers (8 B)
     and last_spike (8 B); per step the recorded bitmap (N/32 words); per
-    launch the state in and out (v, g_exc, g_inh, refractory counter)."""
+    launch the state in and out (v, g_exc, g_inh of sbytes each, refractory
+    counter and refractory period)."""
     n = cn.n
     words = (n + 31) // 32
-    return events * (4 + wbytes) + spikes * 16 + steps * words * 4 + 2 * n * (3 * 4 + 4 + 4)
+    return events * (4 + wbytes) + spikes * 16 + steps * words * 4 + 2 * n * (3 * sbytes + 4 + 4)
 
 
 def accuracy(cn):
@@ -428,6 +438,32 @@ def large_study(n=1_000_000, steps=1000):
     return out
 
 
+def large_profile(n, steps=3, warmup=30):
+    """A small case of the large plastic network for profiler captures: the
+    fast path only, each kernel launched on its own (no graph), `warmup`
+    steps and then `steps` steps, printing the per-kernel device times."""
+    import torch
+    from annarchy_b200 import workloads as wl
+    ln = wl.LargeNet(n=n, steps=steps)
+    net, P, mon, _ = wl.build_large_network(ln, "float", weight_dtype="bfloat16")
+    net.compile()
+    nat = net._backend.native
+    nat.kernel_timing(True)
+    net.simulate_steps(warmup)
+    nat.synchronize()
+    nat.kernel_timing(False)
+    nat.kernel_timing(True)
+    net.simulate_steps(steps)
+    nat.synchronize()
+    kt = nat.kernel_times()
+    nat.kernel_timing(False)
+    torch.cuda.synchronize()
+    print(json.dumps({"neurons": n, "synapses": ln.nnz, "steps": steps,
+                      "spikes": int(mon.spike_arrays()[1].size),
+                      "kernels_us": {k: t * 1e3 / c for k, (t, c) in kt.items()}}))
+    net.close()
+
+
 BATCH_VARIANTS = (("float", "bfloat16"), ("float", "float32"), ("double", None))
 
 
@@ -534,31 +570,38 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
     # no graph) on a sample of the instances, one after the other
     order = np.argsort([c.n for c in cns])
     pick = order[np.linspace(0, n_inst - 1, plain_sample).astype(int)]
-    tt, ev = 0.0, 0
-    for i in pick:
-        cn = cns[i]
-        net, P, mon = build_net(cn, "double", "grid", graph_steps=0)
-        net.simulate_steps(5)
-        mon.get("spike")
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        net.simulate_steps(plain_steps)
-        net._backend.native.synchronize()
-        tt += time.perf_counter() - t0
-        _, r_ = mon.spike_arrays()
-        ev += int(cn.out_degree()[r_].sum())
-        net.close()
-    # the plain path's step time hardly depends on the activity (one launch
-    # per phase), its events do: its GSynOps/s over the whole sweep is the
-    # sweep's events (as delivered by the batch) over n_inst x steps x the
-    # sampled time per instance-step
-    us_inst_step = tt * 1e6 / (plain_steps * len(pick))
     first = out[next(k for k in out if k.startswith("float") or k == "double")]
-    est = first["events"] / (n_inst * steps * us_inst_step * 1e-6) / 1e9
-    out["plain_fp64"] = {"gsynops": est, "us_per_instance_step": us_inst_step,
-                         "sampled_gsynops": ev / tt / 1e9,
+    plain = {}
+    for graph in (0, 32):
+        tt, ev = 0.0, 0
+        for i in pick:
+            cn = cns[i]
+            net, P, mon = build_net(cn, "double", "grid", graph_steps=graph)
+            net.simulate_steps(64)
+            mon.get("spike")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            net.simulate_steps(plain_steps)
+            net._backend.native.synchronize()
+            tt += time.perf_counter() - t0
+            _, r_ = mon.spike_arrays()
+            ev += int(cn.out_degree()[r_].sum())
+            net.close()
+        # the plain path's step time hardly depends on the activity (one launch
+        # per phase), its events do: its GSynOps/s over the whole sweep is the
+        # sweep's events (as delivered by the batch) over n_inst x steps x the
+        # sampled time per instance-step
+        us_inst_step = tt * 1e6 / (plain_steps * len(pick))
+        plain[graph] = (first["events"] / (n_inst * steps * us_inst_step * 1e-6) / 1e9,
+                        us_inst_step, ev / tt / 1e9)
+    out["plain_fp64"] = {"gsynops": plain[0][0], "us_per_instance_step": plain[0][1],
+                         "sampled_gsynops": plain[0][2],
+                         "graphed_gsynops": plain[32][0],
+                         "graphed_us_per_instance_step": plain[32][1],
                          "instances": [int(i) for i in pick], "steps": plain_steps}
     out["fast_vs_plain_fp64"] = out["float_bfloat16"]["gsynops"] / out["plain_fp64"]["gsynops"]
+    out["fast_vs_plain_fp64_graphed"] = (out["float_bfloat16"]["gsynops"]
+                                         / out["plain_fp64"]["graphed_gsynops"])
     if "double" in out:
         out["exact_batch_vs_plain_fp64"] = out["double"]["gsynops"] / out["plain_fp64"]["gsynops"]
     if verbose:
@@ -806,6 +849,8 @@ def rate_study(reps=3):
 
 
 def cpu_baseline_sample(cn, target_s=10.0, threads=1):
+    """The C restatement of the reference's step (oracle/anb_oracle.c) on
+    the same workload, repeated for about target_s seconds."""
     from oracle import oracle as O
     out_deg = cn.out_degree()
     t_total, events, reps = 0.0, 0, 0
@@ -818,35 +863,129 @@ def cpu_baseline_sample(cn, target_s=10.0, threads=1):
     return events / t_total / 1e9, reps, t_total
 
 
+def golden_c2():
+    """The raster the reference itself produced for this workload
+    (tests/golden/coba_c2.npz, made by tests/golden/make_golden.py)."""
+    d = np.load(os.path.join(ROOT, "tests", "golden", "coba_c2.npz"))
+    return d["spike_steps"], d["spike_idx"], d["v_final"]
+
+
+def _digest(a) -> str:
+    import hashlib
+    return hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def reference_cpu(steps, warmup, thread_counts):
+    """The reference's own OpenMP build (installed in baseline/_ref, compiled
+    on this host by oracle/ref_run.py) at each thread count: a list of
+    per-setting results, or (None, reason) when it cannot run here."""
+    from oracle import ref_run
+    why = ref_run.available()
+    if why:
+        return None, why
+    rows = []
+    for th in thread_counts:
+        try:
+            r = ref_run.run("coba", "openmp", th, steps, warmup, f"/tmp/anb_ref_run_{th}")
+        except Exception as e:          # noqa: BLE001 - reported, then the port is used
+            return None, f"reference build/run failed: {str(e)[-300:]}"
+        r["gsynops"] = sum(r["events"]) / sum(r["run_s"]) / 1e9
+        rows.append(r)
+    return rows, None
+
+
 def run_reference(args):
+    """Reference arm: the reference's own CPU implementation of the step on
+    this host's cores, at 1 thread and at all cores, the faster reported
+    (the 4000-neuron network is barrier-bound: more threads can be slower).
+    Falls back to the C restatement of that step (the oracle port) when the
+    reference cannot be built here."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from annarchy_b200 import workloads as wl
-    from oracle import oracle as O
     cn = wl.coba_net(seed=42)
-    threads = os.cpu_count() or 1
-    out_deg = cn.out_degree()
-    for _ in range(args.warmup):
-        O.coba_run(cn, threads=threads)
-    times, events = [], []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        res = O.coba_run(cn, threads=threads)
-        times.append(time.perf_counter() - t0)
-        events.append(int(out_deg[res["spike_idx"]].sum()))
-    val = sum(events) / sum(times) / 1e9
+    cores = os.cpu_count() or 1
+    counts = sorted({1, cores})
+    rows, why = reference_cpu(args.steps, args.warmup, counts)
+    g_steps, g_idx, _ = golden_c2()
+    if rows:
+        best = max(rows, key=lambda r: r["gsynops"])
+        val = best["gsynops"]
+        ms = 1e3 * sum(best["run_s"]) / len(best["run_s"])
+        kind, th = "reference", best["threads"]
+        sample = (f"{args.steps} timed runs of net.simulate(1000 ms) = 10,000 steps after "
+                  f"{args.warmup} warm-up runs; OpenMP build of the reference at "
+                  f"{', '.join(str(r['threads']) for r in rows)} threads, the faster kept")
+        detail = {f"threads_{r['threads']}": {"gsynops": r["gsynops"],
+                                               "ms_per_run": 1e3 * sum(r["run_s"]) / len(r["run_s"]),
+                                               "compile_s": r["compile_s"],
+                                               "raster_equals_fixture":
+                                                   r["raster_steps"] == _digest(g_steps)
+                                                   and r["raster_idx"] == _digest(g_idx)}
+                  for r in rows}
+    else:
+        from oracle import oracle as O
+        out_deg = cn.out_degree()
+        per = {}
+        for th in counts:
+            for _ in range(args.warmup):
+                O.coba_run(cn, threads=th)
+            times, events = [], []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                res = O.coba_run(cn, threads=th)
+                times.append(time.perf_counter() - t0)
+                events.append(int(out_deg[res["spike_idx"]].sum()))
+            per[th] = (sum(events) / sum(times) / 1e9, 1e3 * sum(times) / len(times))
+        th = max(per, key=lambda k: per[k][0])
+        val, ms = per[th]
+        kind = "port"
+        sample = (f"{args.steps} runs of 10,000 steps (1 s model time) of the C restatement at "
+                  f"{', '.join(map(str, counts))} threads, the faster kept ({why})")
+        detail = {f"threads_{k}": {"gsynops": v[0], "ms_per_run": v[1]} for k, v in per.items()}
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "neurons": cn.n, "synapses": cn.nnz,
                        "model_ms_per_step": MODEL_STEPS * cn.dt},
-            "rtf": (MODEL_STEPS * cn.dt / 1e3) / (sum(times) / len(times)),
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} runs of 10,000 steps (1 s model time)"},
+            "rtf": (MODEL_STEPS * cn.dt / 1e3) / (ms * 1e-3),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": th, "kind": kind,
+                             "sample": sample},
+            "runs": detail,
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def run_reference_cuda(args):
+    """The reference's own CUDA build (baseline/_ref, generated CUDA compiled
+    by nvcc for this GPU) on the spiking and the rate-coded workloads: wall
+    time of net.simulate() (the reference's step copies the spike count and
+    list to the host every step, so its device time is not separable)."""
+    from oracle import ref_run
+    why = ref_run.available()
+    if why:
+        print(json.dumps({"impl": "reference-cuda", "unavailable": why}))
+        return
+    g_steps, g_idx, _ = golden_c2()
+    for wl_name in ("coba", "rate"):
+        try:
+            r = ref_run.run(wl_name, "cuda", 1, args.steps, args.warmup, f"/tmp/anb_ref_cuda_{wl_name}")
+        except Exception as e:          # noqa: BLE001
+            print(json.dumps({"impl": "reference-cuda", "workload": wl_name,
+                              "unavailable": str(e)[-500:]}))
+            continue
+        ms = 1e3 * sum(r["run_s"]) / len(r["run_s"])
+        if wl_name == "coba":
+            r["gsynops"] = sum(r["events"]) / sum(r["run_s"]) / 1e9
+            r["raster_equals_fixture"] = (r["raster_steps"] == _digest(g_steps)
+                                          and r["raster_idx"] == _digest(g_idx))
+        else:
+            r["gsynops"] = r["synapses"] * r["time_steps"] / (ms * 1e-3) / 1e9
+        r["ms_per_run"] = ms
+        r["us_per_time_step"] = ms * 1e3 / r["time_steps"]
+        print(json.dumps({"impl": "reference-cuda", **r}), flush=True)
 
 
 def main():
@@ -863,6 +1002,9 @@ def main():
     ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
     ap.add_argument("--large", type=int, default=0,
                     help="the large plastic network with this many neurons (1000000 = 1e9 synapses)")
+    ap.add_argument("--large-profile", type=int, default=0,
+                    help="profiler case: the large network with this many neurons, fast path, "
+                         "kernels launched one by one")
     ap.add_argument("--batched", type=int, default=0,
                     help="batched-instance study with this many instances (256 = the sweep)")
     ap.add_argument("--spmv", default="",
@@ -886,6 +1028,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         large_study(args.large)
+        return
+    if args.large_profile:
+        import torch
+        torch.cuda.set_device(0)
+        large_profile(args.large_profile, steps=args.steps, warmup=args.warmup)
         return
     if args.spmm:
         import torch
@@ -934,6 +1081,9 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    if args.impl == "reference-cuda":
+        run_reference_cuda(args)
+        return
     if args.accuracy:
         import torch
         torch.cuda.set_device(0)
@@ -960,8 +1110,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from annarchy_b200 import workloads as wl
     cn = wl.coba_net(seed=42)
-    # fast path: float state and weights, cluster-resident local engine
-    net, P, mon = build_net(cn, "float", "local", "float32")
+    g_steps, g_idx, g_v = golden_c2()
+    peak, peak_kind = peaks()
+
+    # headline: the exact double path (cluster-resident local engine), whose
+    # raster and potentials equal the reference's bit for bit
+    net, P, mon = build_net(cn, "double", "local")
     with ClockSampler(local) as clk:
         if world > 1:
             torch.distributed.barrier()
@@ -976,60 +1130,94 @@ def main():
     ev_step = sum(dev["events"]) / len(dev["events"])
     value = world * ev_step / (ms_step * 1e-3) / 1e9
     rtf = (MODEL_STEPS * cn.dt / 1e3) / (ms_step * 1e-3)
+    s_last, i_last = dev["raster"]
+    bit_exact = bool(np.array_equal(s_last, g_steps) and np.array_equal(i_last, g_idx)
+                     and np.array_equal(dev["v"], g_v))
 
     # roofline of the dominant kernel
     kname = max(dev["kernel_ms"], key=dev["kernel_ms"].get)
     k_ms = dev["kernel_ms"][kname] / dev["kernel_launches"][kname]
     spikes_step = sum(dev["spikes"]) / len(dev["spikes"])
-    abytes = algorithmic_bytes(cn, spikes_step, ev_step, 4) * (
-        dev["kernel_launches"][kname] and 1)
-    peak, peak_kind = peaks()
+    abytes = algorithmic_bytes(cn, spikes_step, ev_step, 8, sbytes=8)
     achieved = abytes / (k_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(kname), "peak_source": peak_kind,
-            "algorithmic_bytes_per_launch": abytes, "launch_ms": k_ms}
+            "frac": achieved / peak, "traffic": NCU_TRAFFIC.get((kname, "double")),
+            "peak_source": peak_kind, "algorithmic_bytes_per_launch": abytes, "launch_ms": k_ms,
+            "note": "10,000 dependent time steps of 4000 neurons in one launch: bound by the "
+                    "per-step cluster barrier and on-chip latency, not by HBM"}
 
-    # end to end through the public API (pinned host inputs, raster read back)
-    out_deg = cn.out_degree()
-    v0_pin = torch.from_numpy(cn.v0.astype(np.float32)).pin_memory()
-    zeros_pin = torch.zeros(cn.n, dtype=torch.float32).pin_memory()
-    e2e_t, e2e_ev, e2e_sp = [], [], []
-    for it in range(args.warmup + args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        P.set({"v": v0_pin.numpy(), "g_exc": zeros_pin.numpy(), "g_inh": zeros_pin.numpy()})
-        net._backend.native.zero(f"pop{P.id}__refractory_remaining")
-        net.set_current_step(0)
-        net.simulate(MODEL_STEPS * cn.dt)
-        spikes = mon.get("spike")
-        t1 = time.perf_counter()
-        if it >= args.warmup:
-            e2e_t.append(t1 - t0)
-            e2e_ev.append(sum(out_deg[k] * len(v) for k, v in spikes.items()))
-            e2e_sp.append(sum(len(v) for v in spikes.values()))
-    e2e_val = world * (sum(e2e_ev) / len(e2e_ev)) / (sum(e2e_t) / len(e2e_t)) / 1e9
+    def e2e_run(net, P, mon, dtype):
+        """Per step through the public API: initial state from pinned host
+        memory, net.simulate(1 s), Monitor.get() of the spike raster (the
+        raster is decoded on the device; (step, rank) pairs cross the bus)."""
+        out_deg = cn.out_degree()
+        v0_pin = torch.from_numpy(cn.v0.astype(dtype)).pin_memory()
+        zeros_pin = torch.zeros(cn.n, dtype=torch.float64 if dtype == np.float64
+                                else torch.float32).pin_memory()
+        t_, ev_, sp_ = [], [], []
+        for it in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            P.set({"v": v0_pin.numpy(), "g_exc": zeros_pin.numpy(), "g_inh": zeros_pin.numpy()})
+            net._backend.native.zero(f"pop{P.id}__refractory_remaining")
+            net.set_current_step(0)
+            net.simulate(MODEL_STEPS * cn.dt)
+            spikes = mon.get("spike")
+            t1 = time.perf_counter()
+            if it >= args.warmup:
+                t_.append(t1 - t0)
+                ev_.append(sum(out_deg[k] * len(v) for k, v in spikes.items()))
+                sp_.append(sum(len(v) for v in spikes.values()))
+        sb = np.dtype(dtype).itemsize
+        return {"value": world * (sum(ev_) / len(ev_)) / (sum(t_) / len(t_)) / 1e9, "unit": UNIT,
+                "h2d_bytes_per_step": 3 * cn.n * sb + 8,
+                # (step, rank) int32 pairs and the spike count
+                "d2h_bytes_per_step": int(8 * sum(sp_) / len(sp_) + 8)}
+
+    e2e = e2e_run(net, P, mon, np.float64)
     net_engine = net.engine
     net.close()
 
-    # plain FP64 GPU path: one launch per phase per step, no graph
-    net64, P64, mon64 = build_net(cn, "double", "grid", graph_steps=0)
-    fp64 = time_graph_free(net64, P64, mon64, cn, max(2, args.steps // 2))
-    net64.close()
-    fp64_ms = sum(t for t, _ in fp64) / len(fp64)
-    fp64_val = (sum(e for _, e in fp64) / len(fp64)) / (fp64_ms * 1e-3) / 1e9
-    # exact double local engine (also bit-identical to the reference)
-    net64l, P64l, mon64l = build_net(cn, "double", "local")
-    d64 = time_device(net64l, P64l, mon64l, cn, max(2, args.steps // 2), 1)
-    net64l.close()
-    d64_ms = sum(d64["ms"]) / len(d64["ms"])
-    d64_val = (sum(d64["events"]) / len(d64["events"])) / (d64_ms * 1e-3) / 1e9
+    # fast path: float state and weights, same engine
+    net32, P32, mon32 = build_net(cn, "float", "local", "float32")
+    d32 = time_device(net32, P32, mon32, cn, args.steps, args.warmup)
+    e2e32 = e2e_run(net32, P32, mon32, np.float32)
+    net32.close()
+    ms32 = sum(d32["ms"]) / len(d32["ms"])
+    ev32 = sum(d32["events"]) / len(d32["events"])
+    k32 = max(d32["kernel_ms"], key=d32["kernel_ms"].get)
+    k32_ms = d32["kernel_ms"][k32] / d32["kernel_launches"][k32]
+    ab32 = algorithmic_bytes(cn, sum(d32["spikes"]) / len(d32["spikes"]), ev32, 4)
+    fast = {"value": world * ev32 / (ms32 * 1e-3) / 1e9, "ms_per_step": ms32, "dtype": "f32",
+            "engine": net_engine, "e2e": e2e32,
+            "roofline": {"kernel": k32, "achieved": ab32 / (k32_ms * 1e-3) / 1e9,
+                         "frac": ab32 / (k32_ms * 1e-3) / 1e9 / peak,
+                         "traffic": NCU_TRAFFIC.get((k32, "float"))}}
 
+    # plain FP64 GPU path (grid engine, one launch per phase and step), with
+    # and without its CUDA graph
+    plain = {}
+    for g in (32, 0):
+        net64, P64, mon64 = build_net(cn, "double", "grid", graph_steps=g)
+        r64 = time_graph_free(net64, P64, mon64, cn, max(2, args.steps // 2))
+        net64.close()
+        ms64 = sum(t for t, _ in r64) / len(r64)
+        plain[g] = ((sum(e for _, e in r64) / len(r64)) / (ms64 * 1e-3) / 1e9, ms64)
     acc = accuracy(cn) if rank == 0 else None
+    acc8 = accuracy_study() if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, reps, tt = cpu_baseline_sample(cn, 10.0, 1)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{reps} runs of the same 10,000-step workload ({tt:.1f} s, 1 thread)"}
+        rows, why = reference_cpu(2, 1, [1])
+        if rows:
+            r = rows[0]
+            cpu = {"value": r["gsynops"], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "2 runs of net.simulate(1000 ms) = 10,000 steps, OpenMP build of "
+                             "the reference (baseline/_ref) at 1 thread, after 1 warm-up run"}
+        else:
+            v, reps, tt = cpu_baseline_sample(cn, 10.0, 1)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"{reps} runs of the same 10,000-step workload ({tt:.1f} s, "
+                             f"1 thread; reference unavailable: {why})"}
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank != 0:
@@ -1047,30 +1235,36 @@ def main():
                    "instance_rtf": f["instance_rtf"], "ctas": f["ctas"],
                    "plain_fp64_gsynops": bs["plain_fp64"]["gsynops"],
                    "plain_fp64_us_per_instance_step": bs["plain_fp64"]["us_per_instance_step"],
+                   "plain_fp64_graphed_gsynops": bs["plain_fp64"].get("graphed_gsynops"),
                    "speedup_vs_plain_fp64": bs["fast_vs_plain_fp64"],
+                   "speedup_vs_plain_fp64_graphed": bs.get("fast_vs_plain_fp64_graphed"),
                    "roofline_frac": f["roofline"]["frac"], "clocks": f["clocks"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "neurons": cn.n, "synapses": cn.nnz,
                    "model_ms_per_step": MODEL_STEPS * cn.dt, "engine": net_engine,
-                   "l2": "working set (~4 MB) is L2-resident; no flush (latency-bound workload)",
+                   "precision": "double (bit-identical to the reference)",
+                   "l2": "working set (~6 MB) is L2-resident; no flush (latency-bound workload)",
                    "parallelism": f"replicas x{world}"},
         "rtf": rtf,
+        "bit_exact_vs_reference": {"ok": bit_exact, "checked": "raster and final v of the last "
+                                   "timed run against tests/golden/coba_c2.npz (the reference's "
+                                   "own output)"},
         "events_per_step": ev_step, "spikes_per_step": spikes_step,
-        "fp64_path": {"value": fp64_val, "ms_per_step": fp64_ms, "engine": "grid, no graph",
-                      "speedup_of_fast_path": value / world / fp64_val},
-        "fp64_local": {"value": d64_val, "ms_per_step": d64_ms, "bit_exact_vs_reference": True},
-        "accuracy_vs_fp64": acc,
+        "fast_path": fast,
+        "fp64_path": {"graphed": {"value": plain[32][0], "ms_per_step": plain[32][1],
+                                  "engine": "grid, CUDA graph of 32 steps"},
+                      "no_graph": {"value": plain[0][0], "ms_per_step": plain[0][1],
+                                   "engine": "grid, launched step by step"},
+                      "speedup_of_headline_vs_graphed": value / world / plain[32][0],
+                      "speedup_of_fast_path_vs_graphed": fast["value"] / world / plain[32][0]},
+        "accuracy_fast_vs_fp64": {"seed_42": acc, "seeds_42_49": acc8},
         "roofline": roof,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_val, "unit": UNIT,
-                "h2d_bytes_per_step": 3 * cn.n * 4 + cn.n * 4 + 8,
-                # the raster is decoded on the device: (step, rank) int32 pairs and
-                # the spike count cross the bus
-                "d2h_bytes_per_step": int(8 * sum(e2e_sp) / len(e2e_sp) + 8)},
+        "e2e": e2e,
         "gpu_launches": dev["launches"],
         "clocks": clk.summary(),
         "batched_sweep": batched,
