@@ -20,7 +20,8 @@ from __future__ import annotations
 import numpy as np
 
 from ..generator import formats as F
-from ..generator.codegen import CodeGenerator, compensated_vars, grid_for, trace_layout
+from ..generator.codegen import (CodeGenerator, compensated_vars, grid_for, list_grid,
+                                 trace_layout)
 from ..runtime.lib import DryNative, NativeNet
 from .monitor import array_name
 
@@ -107,7 +108,7 @@ class CompiledNetwork:
             key = net._rng.integers(0, 2**32, 2, dtype=np.uint64).astype(np.uint32)
         else:
             key = np.zeros(2, dtype=np.uint32)
-        nat.create("rng_seed", key)
+        nat.set_seed(int(key[0]) | (int(key[1]) << 32))
         # history kept per population: its outgoing projections' largest delay
         for pop in net.populations:
             self.slots[pop.id] = max([1] + [int(p.max_delay) for p in net.projections
@@ -475,7 +476,9 @@ class CompiledNetwork:
             row_of = np.full(proj.post_pop.size, -1, dtype=np.int32)
             row_of[post0:post0 + npost] = np.arange(npost, dtype=np.int32)
             nat.create(f"proj{k}__row_of", row_of)
-        if self.exact or plastic:
+        if self.spike_lists:
+            lay["grid"] = list_grid(pre_hi - pre_lo, lay["chunks"])
+        elif self.exact or plastic:
             lay["grid"] = grid_for(npost * 32)
         else:
             lay["grid"] = grid_for((lay["w1"] - lay["w0"]) * 32)
@@ -627,6 +630,8 @@ class CompiledNetwork:
                 proj.plastic and (proj.max_delay > 1 or not self.spike_lists))
             if gather:
                 lay["grid"] = grid_for(rows * 32)
+            elif self.spike_lists:
+                lay["grid"] = list_grid(len(proj.pre_ranks), lay["chunks"])
             elif proj.plastic:
                 lay["grid"] = grid_for(rows)
             else:
@@ -679,6 +684,7 @@ class CompiledNetwork:
         for v in mon.variables:
             if v != "spike":
                 nat.create_empty(f"mon{m}__{array_name(v)}", np.float64, (lay["cap_var"], n))
+                nat.record_declare(f"mon{m}__{array_name(v)}", n, 8, mon.period_steps)
         self.mon_layout[m] = lay
 
     # ------------------------------------------------------------------- run
@@ -844,6 +850,18 @@ class CompiledNetwork:
         R = self.slots.get(k, 1)
         if pop.neuron_type.type == "rate" and R > 1:
             nat.write(f"pop{k}___delayed_r", self._ring_of(pop, self.read_population_attribute(pop, "r")))
+        if pop.neuron_type.type == "spike":
+            nat.fill(f"pop{k}__spk", np.uint32(0))
+            nat.fill(f"pop{k}__refractory_remaining", np.int32(0))
+            nat.fill(f"pop{k}__last_spike", np.int64(-10000))
+            if f"pop{k}__spn" in nat.arrays:
+                nat.fill(f"pop{k}__spn", np.int32(0))
+
+    def reset_spike_state(self, pop):
+        """The spike part of the reference's PopStruct::reset(): no spikes
+        emitted, refractory counters cleared, no last spike."""
+        nat = self.native
+        k = pop.id
         if pop.neuron_type.type == "spike":
             nat.fill(f"pop{k}__spk", np.uint32(0))
             nat.fill(f"pop{k}__refractory_remaining", np.int32(0))

@@ -232,6 +232,7 @@ class Population:
         return float(r[0]) if r.size and np.all(r == r[0]) else r.copy()
 
     def set_refractory(self, value):
+        object.__setattr__(self, "_refractory_steps", None)
         self._refractory_ms = draw(value, (self.size,), self._rng())
         self._has_refractory = self._has_refractory or bool(np.any(self._refractory_ms > 0))
         if self._compiled():
@@ -239,8 +240,22 @@ class Population:
 
     @property
     def refractory_steps(self) -> np.ndarray:
+        steps = self.__dict__.get("_refractory_steps")
+        if steps is not None:
+            return steps
         dt = self.net.dt if self.net is not None else 1.0
         return (self._refractory_ms / dt).astype(np.int32)  # truncation, like int(x/dt)
+
+    def _set_refractory_steps(self, steps: np.ndarray):
+        """Refractory periods given in whole steps (as the reference's Python
+        layer hands them to its generated module, already truncated)."""
+        steps = np.broadcast_to(np.asarray(steps, dtype=np.int32), (self.size,)).copy()
+        dt = self.net.dt if self.net is not None else 1.0
+        object.__setattr__(self, "_refractory_steps", steps)
+        object.__setattr__(self, "_refractory_ms", steps * dt)
+        self._has_refractory = self._has_refractory or bool(np.any(steps > 0))
+        if self._compiled():
+            self.net._backend.write_refractory(self)
 
     # -- views ----------------------------------------------------------------
     def __getitem__(self, idx):

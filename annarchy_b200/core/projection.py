@@ -182,6 +182,55 @@ class Projection:
 
     connect_from_sparse = from_sparse
 
+    def _from_lil(self, post_ranks, pre_ranks, w, delays, requires_sorting: bool = False):
+        """Connectivity as the reference's generated module receives it
+        (init_from_lil, ANNarchy/generator/NanoBind/Projection.py:20-60;
+        built by ANNarchy/cython_ext/Connector.pyx:93-170): post population
+        ranks, per post the pre population ranks, weights (one value or one
+        per synapse) and delays in steps (one or one per synapse). Rows may
+        come unsorted when requires_sorting; pre ranks are sorted per row
+        with their weights and delays."""
+        post_ranks = [int(r) for r in post_ranks]
+        if len(pre_ranks) != len(post_ranks) or len(w) != len(post_ranks):
+            raise ValueError("init_from_lil: post_ranks, pre_ranks and w differ in length")
+        if requires_sorting:
+            order = sorted(range(len(post_ranks)), key=lambda i: post_ranks[i])
+        else:
+            order = range(len(post_ranks))
+        post_pos = {int(r): i for i, r in enumerate(self.post_ranks_view)}
+        pre_pos = {int(r): i for i, r in enumerate(self.pre_ranks)}
+        rows, cols, vals, dsteps = [], [], [], []
+        for i in order:
+            pr = np.asarray(pre_ranks[i], dtype=np.int64)
+            if post_ranks[i] not in post_pos:
+                raise ValueError(f"init_from_lil: post rank {post_ranks[i]} is not in the projection")
+            ww = np.asarray(w[i], dtype=np.float64)
+            ww = np.full(pr.size, float(ww.reshape(-1)[0])) if ww.size == 1 else ww
+            dd = np.asarray(delays[i] if delays is not None and len(delays) > i else [0],
+                            dtype=np.int64)
+            dd = np.full(pr.size, int(dd.reshape(-1)[0]) if dd.size else 0) if dd.size <= 1 else dd
+            if ww.size != pr.size or dd.size != pr.size:
+                raise ValueError(f"init_from_lil: row {i} has {pr.size} ranks, {ww.size} weights "
+                                 f"and {dd.size} delays")
+            try:
+                c = np.fromiter((pre_pos[int(r)] for r in pr), dtype=np.int64, count=pr.size)
+            except KeyError as e:
+                raise ValueError(f"init_from_lil: pre rank {e.args[0]} is not in the projection")
+            rows.append(np.full(pr.size, post_pos[post_ranks[i]], dtype=np.int64))
+            cols.append(c)
+            vals.append(ww)
+            dsteps.append(dd)
+        cat = (lambda a, dt: np.concatenate(a) if a else np.zeros(0, dt))
+        rows, cols = cat(rows, np.int64), cat(cols, np.int64)
+        vals, dsteps = cat(vals, np.float64), cat(dsteps, np.int64)
+        shape = (len(self.post_ranks_view), len(self.pre_ranks))
+        m = sp.csr_matrix((vals, (rows, cols)), shape=shape)
+        if dsteps.size and np.unique(dsteps).size > 1:
+            dm = sp.csr_matrix((dsteps * self._dt(), (rows, cols)), shape=shape)
+            return self._store(m, "From LIL", None, None, dm)
+        d = float(dsteps[0]) * self._dt() if dsteps.size else 0.0
+        return self._store(m, "From LIL", None, d)
+
     def from_matrix(self, weights, delays=0.0, pre_post=False, storage_format=None,
                     storage_order=None):
         """weights: dense (post, pre) array (or (pre, post) with pre_post=True);

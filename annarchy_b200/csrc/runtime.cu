@@ -161,6 +161,14 @@ struct anb_net {
     int all;
   };
   std::vector<Stop> stops;
+  // recorded state variables declared for anb_estimate_record_size
+  struct Record {
+    std::string ring;
+    int64_t values = 0;
+    int value_bytes = 8;
+    int64_t period = 1;
+  };
+  std::vector<Record> records;
 };
 
 namespace {
@@ -602,6 +610,134 @@ int anb_module_load(anb_net* net, const char* source, const char* options) {
   ANB_CU(g_drv.moduleLoadData(&net->module, cubin.data()));
   net->bindings_dirty = true;
   return bind(net);
+}
+
+// ---- entry points shaped like the reference module's set_seed,
+// estimate_record_size and proj<k>_wrapper.init_from_lil ----------------------------
+
+int anb_set_seed(anb_net* net, uint64_t seed, int num_sources, int use_seed_seq) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  if (num_sources < 0) return fail(ANB_ERR_ARG, "num_sources < 0");
+  (void)use_seed_seq;
+  const uint32_t key[2] = {(uint32_t)(seed & 0xffffffffull), (uint32_t)(seed >> 32)};
+  Array* a = find(net, "rng_seed");
+  if (a && a->bytes != sizeof(key)) return fail(ANB_ERR_ARG, "rng_seed has an unexpected size");
+  if (!a) {
+    int rc = anb_array_create(net, "rng_seed", sizeof(key));
+    if (rc) return rc;
+  }
+  return anb_array_write(net, "rng_seed", 0, key, sizeof(key));
+}
+
+int anb_record_declare(anb_net* net, const char* ring, int64_t values_per_record, int value_bytes,
+                       int64_t period_steps) {
+  if (!net || !ring) return fail(ANB_ERR_ARG, "NULL argument");
+  if (values_per_record < 0 || value_bytes <= 0 || period_steps <= 0)
+    return fail(ANB_ERR_ARG, "record sizes and period must be positive");
+  for (auto& r : net->records)
+    if (r.ring == ring) {
+      r.values = values_per_record;
+      r.value_bytes = value_bytes;
+      r.period = period_steps;
+      return ANB_OK;
+    }
+  anb_net::Record r;
+  r.ring = ring;
+  r.values = values_per_record;
+  r.value_bytes = value_bytes;
+  r.period = period_steps;
+  net->records.push_back(r);
+  return ANB_OK;
+}
+
+int anb_estimate_record_size(anb_net* net, int64_t nsteps, size_t* mib) {
+  if (!net || !mib) return fail(ANB_ERR_ARG, "NULL argument");
+  if (nsteps < 0) return fail(ANB_ERR_ARG, "nsteps < 0");
+  unsigned long long bytes = 0;
+  for (const auto& r : net->records)
+    bytes += (unsigned long long)(nsteps / r.period) * (unsigned long long)r.values *
+             (unsigned long long)r.value_bytes;
+  *mib = (size_t)(bytes >> 20);
+  return ANB_OK;
+}
+
+namespace {
+uint16_t to_bf16_rne(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x007fffffu)) return (uint16_t)((u >> 16) | 0x40u);
+  const uint32_t lsb = (u >> 16) & 1u;
+  return (uint16_t)((u + 0x7fffu + lsb) >> 16);
+}
+}  // namespace
+
+int anb_init_from_lil(anb_net* net, const char* prefix, int n_rows, const int* post_ranks,
+                      const int64_t* row_begin, const int* pre_ranks, const double* w,
+                      const int* delays, int requires_sorting, int weight_bytes, int64_t* nnz_out) {
+  if (!net || !prefix || n_rows < 0 || (n_rows > 0 && (!post_ranks || !row_begin)))
+    return fail(ANB_ERR_ARG, "NULL argument or negative row count");
+  if (weight_bytes != 8 && weight_bytes != 4 && weight_bytes != 2)
+    return fail(ANB_ERR_ARG, "weight_bytes must be 8, 4 or 2");
+  const int64_t nnz = n_rows ? row_begin[n_rows] : 0;
+  if (n_rows && row_begin[0] != 0) return fail(ANB_ERR_ARG, "row_begin[0] must be 0");
+  for (int r = 0; r < n_rows; ++r) {
+    if (row_begin[r + 1] < row_begin[r]) return fail(ANB_ERR_ARG, "row_begin is not ascending");
+    if (post_ranks[r] < 0) return fail(ANB_ERR_ARG, "negative post rank");
+  }
+  if (nnz > 0 && (!pre_ranks || !w)) return fail(ANB_ERR_ARG, "pre_ranks or w is NULL");
+  if (nnz >= (1ll << 31)) return fail(ANB_ERR_ARG, "more than 2^31 - 1 synapses");
+  for (int64_t j = 0; j < nnz; ++j)
+    if (pre_ranks[j] < 0) return fail(ANB_ERR_ARG, "negative pre rank");
+  // dendrites in ascending post rank when the caller asks for sorting (the
+  // reference's pairsort of init_matrix_from_lil), else in the given order
+  std::vector<int> order(n_rows);
+  for (int r = 0; r < n_rows; ++r) order[r] = r;
+  if (requires_sorting)
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return post_ranks[a] < post_ranks[b]; });
+  std::vector<int> post(n_rows), row_ptr(n_rows + 1), col(nnz), dly;
+  std::vector<unsigned char> wv((size_t)nnz * weight_bytes);
+  bool uniform_delay = true;
+  if (delays)
+    for (int64_t j = 1; j < nnz; ++j)
+      if (delays[j] != delays[0]) uniform_delay = false;
+  if (delays && !uniform_delay) dly.resize(nnz);
+  int64_t k = 0;
+  for (int i = 0; i < n_rows; ++i) {
+    const int r = order[i];
+    post[i] = post_ranks[r];
+    row_ptr[i] = (int)k;
+    for (int64_t j = row_begin[r]; j < row_begin[r + 1]; ++j, ++k) {
+      col[k] = pre_ranks[j];
+      if (weight_bytes == 8) {
+        std::memcpy(&wv[k * 8], &w[j], 8);
+      } else if (weight_bytes == 4) {
+        const float f = (float)w[j];
+        std::memcpy(&wv[k * 4], &f, 4);
+      } else {
+        const uint16_t h = to_bf16_rne((float)w[j]);
+        std::memcpy(&wv[k * 2], &h, 2);
+      }
+      if (!dly.empty()) dly[k] = delays[j];
+    }
+  }
+  row_ptr[n_rows] = (int)k;
+  const std::string p(prefix);
+  int rc = anb_array_create(net, (p + "__post_rank").c_str(), sizeof(int) * (size_t)n_rows);
+  if (!rc) rc = anb_array_write(net, (p + "__post_rank").c_str(), 0, post.data(), sizeof(int) * post.size());
+  if (!rc) rc = anb_array_create(net, (p + "__row_ptr").c_str(), sizeof(int) * row_ptr.size());
+  if (!rc) rc = anb_array_write(net, (p + "__row_ptr").c_str(), 0, row_ptr.data(), sizeof(int) * row_ptr.size());
+  if (!rc) rc = anb_array_create(net, (p + "__col").c_str(), sizeof(int) * (size_t)nnz);
+  if (!rc) rc = anb_array_write(net, (p + "__col").c_str(), 0, col.data(), sizeof(int) * col.size());
+  if (!rc) rc = anb_array_create(net, (p + "__w").c_str(), wv.size());
+  if (!rc) rc = anb_array_write(net, (p + "__w").c_str(), 0, wv.data(), wv.size());
+  if (!rc && !dly.empty()) {
+    rc = anb_array_create(net, (p + "__dly").c_str(), sizeof(int) * dly.size());
+    if (!rc) rc = anb_array_write(net, (p + "__dly").c_str(), 0, dly.data(), sizeof(int) * dly.size());
+  }
+  if (rc) return rc;
+  if (nnz_out) *nnz_out = nnz;
+  return ANB_OK;
 }
 
 int anb_module_set_constant(anb_net* net, const char* name, double value) {

@@ -93,6 +93,14 @@ def grid_for(n: int, block: int = BLOCK) -> int:
     return max(1, min(MAX_GRID, (n + block - 1) // block))
 
 
+def list_grid(n_pre: int, chunks: int, block: int = BLOCK) -> int:
+    """CTAs of a kernel whose warps take (spike, chunk of 32 synapses) work
+    items from a spike list: one warp per item while at most 1/64 of the
+    n_pre neurons spike in a step, and never more than one resident wave
+    (148 SMs x 8 CTAs); a busier step loops over the items."""
+    return max(1, min(148 * 8, -(-(n_pre * chunks * 32) // (64 * block))))
+
+
 def float_literals(code: str) -> str:
     """Suffix floating literals with f (single-precision modules), like the
     reference's float precision mode (ANNarchy/parser/Equation.py:172-197)."""
@@ -359,6 +367,7 @@ class CodeGenerator:
 
         grid_path = not smem and cluster is None and not local_engine
         loads, stores = [], []
+        hoist = []          # grid path: (ctype, variable, array) loaded for K neurons at once
         sidx = "anb_q" if cluster is not None else "anb_i"
         for name in names:
             ct = "int" if pop._ctype.get(name) in ("int", "bool") else self.real
@@ -366,6 +375,7 @@ class CodeGenerator:
             src = smem[name] if on_chip else gsrc(name)
             idx = sidx if on_chip else "anb_i"
             loads.append(f"{ct} {name} = {src}[{idx}];")
+            hoist.append((ct, name, src))
             if name in modified or (spiking and any(r["name"] == name for r in
                                                     pop.desc["spike"]["spike_reset"])):
                 stores.append(f"{src}[{idx}] = {name};")
@@ -378,11 +388,13 @@ class CodeGenerator:
             src = smem["kc_" + x] if on_chip else gsrc("kc_" + x)
             idx = sidx if on_chip else "anb_i"
             loads.append(f"{self.real} anb_kc_{x} = {src}[{idx}];")
+            hoist.append((self.real, f"anb_kc_{x}", src))
             stores.append(f"{src}[{idx}] = anb_kc_{x};")
         if pop.neuron_type.type == "rate":
             for t in pop.targets:
                 src = gsrc("_sum_" + t)
                 loads.append(f"const {self.real} _sum_{t} = {src}[anb_i];")
+                hoist.append((f"const {self.real}", f"_sum_{t}", src))
                 stores.append(f"{src}[anb_i] = ({self.real})0;")
                 if grid_path:
                     # kept for Population.sum(target) (the sums are consumed here)
@@ -399,6 +411,7 @@ class CodeGenerator:
                     resets += f"\n          anb_kc_{r['name']} = ({self.real})0;"
             if masked:
                 loads.append(f"int refractory_remaining = {rr_src}[{rr_idx}];")
+                hoist.append(("int", "refractory_remaining", rr_src))
                 loads.append("const int in_ref = (refractory_remaining > 0) ? 0 : 1;")
                 refr_dec = "refractory_remaining -= (1 - in_ref);"
                 guard = f"(in_ref != 0) && ({cond})"
@@ -478,6 +491,44 @@ class CodeGenerator:
       }}
     }}"""
         first = 0
+        K = self.neurons_per_thread(pop) if grid_path else 1
+        if grid_path and K > 1:
+            if pop.id in getattr(self.c, "owned", {}):
+                first, size = self.c.owned[pop.id]
+            derived = [ln for ln in loads if not any(ln == f"{ct} {nm} = {src}[anb_i];"
+                                                     for ct, nm, src in hoist)]
+            arrays = nl.join(f"{ct.replace('const ', '')} anb_h_{nm}[{K}];" for ct, nm, _ in hoist)
+            fetch = nl.join(f"  anb_h_{nm}[anb_k] = {src}[anb_j];" for _, nm, src in hoist)
+            unpack = nl.join(f"{ct} {nm} = anb_h_{nm}[anb_k];" for ct, nm, _ in hoist)
+            return f"""
+    {{  // population {pop.name}: update{' and spike gather' if spiking else ''}, {K} neurons per
+        // thread and pass with all their loads issued first
+      const int anb_n = {size if size is not None else pop.size};
+      for (int anb_base0 = {first} + blockIdx.x * blockDim.x * {K}; anb_base0 < anb_n;
+           anb_base0 += gridDim.x * blockDim.x * {K}) {{
+        {arrays}
+#pragma unroll
+        for (int anb_k = 0; anb_k < {K}; ++anb_k) {{
+          const int anb_j = anb_base0 + anb_k * blockDim.x + threadIdx.x;
+          if (anb_j < anb_n) {{
+          {fetch}
+          }}
+        }}
+#pragma unroll
+        for (int anb_k = 0; anb_k < {K}; ++anb_k) {{
+        const int anb_base = anb_base0 + anb_k * blockDim.x;
+        const int anb_i = anb_base + threadIdx.x;
+        bool anb_spiked = false;
+        if (anb_i < anb_n) {{
+        {unpack}
+        {nl.join(derived)}
+        {body.replace(chr(10), nl)}
+        {spike_code}
+        {nl.join(stores)}
+        }}{ballot}
+        }}
+      }}
+    }}"""
         if local_engine:
             loop = "for (int anb_base = 0; anb_base < anb_n; anb_base += blockDim.x)"
         else:
@@ -500,6 +551,13 @@ class CodeGenerator:
         }}{ballot}
       }}
     }}"""
+
+    @staticmethod
+    def neurons_per_thread(pop) -> int:
+        """Neurons one thread updates per pass of the grid engine's update
+        kernel: large populations issue the loads of several neurons before
+        computing any, so that enough bytes are in flight per thread."""
+        return 4 if pop.size >= (1 << 18) else (2 if pop.size >= (1 << 16) else 1)
 
     def pop_kernel(self, pop) -> str:
         preamble = self._globals_preamble(pop, lambda n: self.ptr(f"pop{pop.id}__{n}"))
@@ -1170,7 +1228,8 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
             elif self.has_update(pop):
                 kernels.append(self.pop_kernel(pop))
                 lo, hi = getattr(self.c, "owned", {}).get(pop.id, (0, pop.size))
-                plan.append((f"pop{pop.id}_step", grid_for(max(1, hi - lo)), BLOCK, 0))
+                K = self.neurons_per_thread(pop)
+                plan.append((f"pop{pop.id}_step", grid_for(max(1, -(-(hi - lo) // K))), BLOCK, 0))
             elif pop.neuron_type.type == "rate" and self.slots(pop) > 1:
                 kernels.append(self.delay_kernel(pop))
                 plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))
@@ -1182,8 +1241,10 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
         for proj in net.projections:
             if proj.synapse_type.type == "spike" and proj.desc.get("post_spike"):
                 kernels.append(self.post_event_kernel(proj))
-                plan.append((f"proj{proj.id}_post_event",
-                             grid_for(self.c.layout[proj.id]["rows"] * 32), BLOCK, 0))
+                lay = self.c.layout[proj.id]
+                grid = (list_grid(proj.post_pop.size, lay["post_chunks"])
+                        if (self.c.spike_lists and not self.exact) else grid_for(lay["rows"] * 32))
+                plan.append((f"proj{proj.id}_post_event", grid, BLOCK, 0))
         for mon in net.monitors:
             if any(v != "spike" for v in mon.variables):
                 # spikes are written by the update kernel of the population
@@ -1382,8 +1443,10 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
 
           1. deliver the spikes of step s-1 (replica of parity (s-1)&1) into
              the own neurons' conductances: fast mode with shared-memory
-             atomics, exact mode spike by spike in ascending pre rank with a
-             CTA barrier after each, which is the reference's per-post order;
+             atomics, exact mode by one warp per conductance array, its
+             projections in order and their spikes in ascending pre rank (a
+             warp barrier after each spike), which is the reference's
+             per-post order;
           2. update the own neurons and write the own bitmap words into the
              local replica of parity s&1 and into every other CTA's (DSMEM
              stores);
@@ -1429,6 +1492,7 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
                          f"{gspk}[(anb_base{k} >> 5) + q] = (nsteps & 1 ? {d['spk0']} : {d['spk1']})[(anb_base{k} >> 5) + q];")
         prop = []
         fast_groups: dict[int, list] = {}
+        exact_groups: dict[tuple, list] = {}
         for proj in net.projections:
             a, b = proj.pre_pop.id, proj.post_pop.id
             play = self.c.layout[proj.id]
@@ -1464,32 +1528,32 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
             deliver = (f"const int beg = {cp}[pre - {lo}], end = {cp}[pre - {lo} + 1];")
             spk = f"(anb_par ? {smem_ptrs[a]['spk0']} : {smem_ptrs[a]['spk1']})"
             if self.exact:
-                # every warp walks all nonzero words of the projection's range in
-                # ascending order (warp-uniform), one CTA barrier per spike
-                prop.append(f"""
-      {{  // {proj.name}: spikes in ascending pre rank, one CTA barrier per spike
-        const anb_u32* __restrict__ anb_spk = {spk};
-        for (int c = {play['w0']}; c < {play['w1']}; c += 32) {{
-          const anb_u32 anb_wv = (c + anb_lane < {play['w1']}) ? anb_spk[c + anb_lane] : 0u;
-          anb_u32 anb_nz = __ballot_sync(0xffffffffu, anb_wv != 0u);
-          while (anb_nz) {{
-            const int j = __ffs(anb_nz) - 1;
-            anb_nz &= anb_nz - 1;
-            anb_u32 m = __shfl_sync(0xffffffffu, anb_wv, j);
-            while (m) {{
-              const int b = __ffs(m) - 1;
-              m &= m - 1;
-              const int pre = ((c + j) << 5) + b;
-              {deliver}
-              if (end > beg) {{
-                for (int q = beg + threadIdx.x; q < end; q += blockDim.x)
+                # one warp per conductance array walks the nonzero words of the
+                # projection's range in ascending order; the lanes add one
+                # spike's synapses (distinct posts), then __syncwarp orders
+                # them before the next spike: per post, ascending pre rank
+                exact_groups.setdefault((b, proj.target), []).append(f"""
+        {{  // {proj.name}: spikes in ascending pre rank
+          const anb_u32* __restrict__ anb_spk = {spk};
+          for (int c = {play['w0']}; c < {play['w1']}; c += 32) {{
+            const anb_u32 anb_wv = (c + anb_lane < {play['w1']}) ? anb_spk[c + anb_lane] : 0u;
+            anb_u32 anb_nz = __ballot_sync(0xffffffffu, anb_wv != 0u);
+            while (anb_nz) {{
+              const int j = __ffs(anb_nz) - 1;
+              anb_nz &= anb_nz - 1;
+              anb_u32 m = __shfl_sync(0xffffffffu, anb_wv, j);
+              while (m) {{
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                const int pre = ((c + j) << 5) + b;
+                {deliver}
+                for (int q = beg + anb_lane; q < end; q += 32)
                   {g}[anb_s_pool_post[q]] += {w_src}[{w_idx}];
-                __syncthreads();
+                __syncwarp();
               }}
             }}
           }}
-        }}
-      }}""")
+        }}""")
             else:
                 fast_groups.setdefault(a, []).append(f"""
           if (pre >= {lo} && pre < {hi}) {{  // {proj.name}
@@ -1497,6 +1561,12 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
             for (int q = beg + anb_lane; q < end; q += 32)
               atomicAdd(&{g}[anb_s_pool_post[q]], anb_wf({w_src}[{w_idx}]));
           }}""")
+        if len(exact_groups) > lay["block"] // 32:
+            raise ValueError("more conductance arrays than warps in the cluster engine")
+        for gi, ((b, target), blocks) in enumerate(exact_groups.items()):
+            prop.append(f"""
+      if (anb_warp == {gi}) {{  // population {b}, g_{target}: projections in order{''.join(blocks)}
+      }}""")
         for a, blocks in fast_groups.items():
             pop_a = next(pp for pp in net.populations if pp.id == a)
             W = (pop_a.size + 31) // 32

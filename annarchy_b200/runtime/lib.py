@@ -95,6 +95,12 @@ SIGNATURES = {
                                 C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]),
     "anb_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_void_p]),
+    "anb_set_seed": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int]),
+    "anb_record_declare": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_int, C.c_int64]),
+    "anb_estimate_record_size": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_size_t)]),
+    "anb_init_from_lil": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                    C.POINTER(C.c_int64)]),
     "anb_mlp_noalloc_max_floats": (C.c_size_t, []),
     "anb_mlp_predict_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                           C.c_int, C.c_void_p, C.c_void_p]),
@@ -303,6 +309,48 @@ class NativeNet:
         check("anb_array_copy_strided", self.lib.anb_array_copy_strided(
             self.h, dst.encode(), dst_offset, dst_stride, src.encode(), src_offset, src_stride, count))
 
+    def set_seed(self, seed: int, num_sources: int = 1, use_seed_seq: bool = True):
+        """Key of the device's random draws (anb_set_seed)."""
+        check("anb_set_seed", self.lib.anb_set_seed(self.h, int(seed) & (2**64 - 1),
+                                                     int(num_sources), 1 if use_seed_seq else 0))
+
+    def record_declare(self, ring: str, values_per_record: int, value_bytes: int, period: int):
+        check("anb_record_declare", self.lib.anb_record_declare(
+            self.h, ring.encode(), int(values_per_record), int(value_bytes), int(period)))
+
+    def estimate_record_size(self, nsteps: int) -> int:
+        """MiB of the declared recorded variables after nsteps steps."""
+        out = C.c_size_t()
+        check("anb_estimate_record_size", self.lib.anb_estimate_record_size(
+            self.h, int(nsteps), C.byref(out)))
+        return int(out.value)
+
+    def init_from_lil(self, prefix: str, post_ranks, pre_ranks, w, delays=None,
+                      requires_sorting: bool = False, weight_bytes: int = 8) -> int:
+        """Upload LIL connectivity (lists per dendrite) as CSR arrays through
+        anb_init_from_lil; returns the synapse count."""
+        sizes = np.array([len(r) for r in pre_ranks], dtype=np.int64)
+        row_begin = np.zeros(len(sizes) + 1, dtype=np.int64)
+        np.cumsum(sizes, out=row_begin[1:])
+        post = np.ascontiguousarray(post_ranks, dtype=np.int32)
+        cat = (lambda a, dt: np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=dt) for x in a])
+                                                  if len(a) else np.zeros(0, dt)))
+        pre = cat(pre_ranks, np.int32)
+        ww = cat(w, np.float64)
+        dd = cat(delays, np.int32) if delays is not None else None
+        nnz = C.c_int64()
+        check("anb_init_from_lil", self.lib.anb_init_from_lil(
+            self.h, prefix.encode(), len(post), post.ctypes.data_as(C.c_void_p),
+            row_begin.ctypes.data_as(C.c_void_p), pre.ctypes.data_as(C.c_void_p),
+            ww.ctypes.data_as(C.c_void_p), dd.ctypes.data_as(C.c_void_p) if dd is not None else None,
+            1 if requires_sorting else 0, int(weight_bytes), C.byref(nnz)))
+        for name, dt, n in (("__post_rank", np.int32, len(post)), ("__row_ptr", np.int32, len(post) + 1),
+                            ("__col", np.int32, nnz.value)):
+            self.arrays[prefix + name] = (np.dtype(dt), (n,))
+        wdt = {8: np.float64, 4: np.float32, 2: np.uint16}[int(weight_bytes)]
+        self.arrays[prefix + "__w"] = (np.dtype(wdt), (nnz.value,))
+        return int(nnz.value)
+
     def fill(self, name: str, value):
         v = np.asarray(value)
         check("anb_array_fill", self.lib.anb_array_fill(self.h, name.encode(),
@@ -446,6 +494,12 @@ class DryNative:
         pass
 
     def fill(self, name, value):
+        pass
+
+    def set_seed(self, seed, num_sources=1, use_seed_seq=True):
+        self.arrays["rng_seed"] = (np.dtype(np.uint32), (2,))
+
+    def record_declare(self, *a):
         pass
 
     def free(self, name):

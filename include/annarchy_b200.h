@@ -133,6 +133,45 @@ int anb_connect_fixed_number_pre_rows(anb_net* net, const char* prefix, int n_po
                                       uint64_t seed, int weight_kind, double a, double b,
                                       int weight_bytes, int exclude_self);
 
+/* set_seed(long seed, int num_sources, bool use_seed_seq) of the generated
+ * module (ANNarchy/generator/NanoBind/BaseTemplate.py:16, called from
+ * ANNarchy/generator/Compiler.py:911-922 and ANNarchy/core/Network.py:673-685):
+ * the key of the device's counter-based random draws in equations becomes the
+ * two 32-bit halves of `seed` (array "rng_seed"). num_sources and
+ * use_seed_seq select the reference's per-thread std::mt19937 seeding and have
+ * no effect here (one counter-based stream per neuron and draw). */
+int anb_set_seed(anb_net* net, uint64_t seed, int num_sources, int use_seed_seq);
+
+/* Declare a recorded state variable: every `period_steps` steps one record of
+ * `values_per_record` values of `value_bytes` bytes (the device ring `ring`).
+ * Declaring a ring again updates it. Feeds anb_estimate_record_size. No
+ * counterpart in the reference (its recorders are compiled in). */
+int anb_record_declare(anb_net* net, const char* ring, int64_t values_per_record, int value_bytes,
+                       int64_t period_steps);
+
+/* estimate_record_size(int num_steps) of the generated module
+ * (ANNarchy/generator/Template/OpenMPBaseTemplate.py:204-211, called from
+ * ANNarchy/core/Simulate.py:275-300): MiB the declared recorded state
+ * variables take after nsteps more steps (spike records are not counted, as
+ * in the reference). */
+int anb_estimate_record_size(anb_net* net, int64_t nsteps, size_t* mib);
+
+/* proj<k>_wrapper.init_from_lil(post_ranks, pre_ranks, w, delays,
+ * requires_sorting) of the generated module
+ * (ANNarchy/generator/NanoBind/Projection.py:20-60, CSR container
+ * ANNarchy/include/CSRMatrix.hpp:142), with the list of lists flattened:
+ * dendrite r has post rank post_ranks[r] and the synapses row_begin[r] ..
+ * row_begin[r + 1] - 1 of pre_ranks, w (double) and delays (steps; NULL for
+ * none). Creates "<prefix>__post_rank", "__row_ptr", "__col" (int32) and
+ * "__w" (weight_bytes 8, 4 or 2 = bfloat16, rounded to nearest even), plus
+ * "__dly" (int32 per synapse) when the delays differ. requires_sorting orders
+ * the dendrites by post rank (stable); the synapses of a dendrite keep their
+ * order. Invalid input (descending row_begin, negative ranks) gives
+ * ANB_ERR_ARG and creates nothing. *nnz_out receives the synapse count. */
+int anb_init_from_lil(anb_net* net, const char* prefix, int n_rows, const int* post_ranks,
+                      const int64_t* row_begin, const int* pre_ranks, const double* w,
+                      const int* delays, int requires_sorting, int weight_bytes, int64_t* nnz_out);
+
 /* Fixed-probability projection generated on the device (replaces the host
  * construction of ANNarchy/core/ConnectorMethods.py:262-330 and
  * ANNarchy/cython_ext/Connector.pyx:306-345, which build per-post Bernoulli
