@@ -546,9 +546,32 @@ class CompiledNetwork:
         name = f"proj{proj.id}__dly" if proj._delay_steps is not None else f"proj{proj.id}__delay"
         self.native.write(name, np.asarray(steps, dtype=np.int32))
 
+    def _create_batched_tc(self, proj):
+        """A projection shared by the copies of a RateBatch: the per-copy
+        weights as 64 x 64 bfloat16 blocks in the layout of the tensor-core
+        product (one set for all copies), and the packed-rate scratch."""
+        from ..spmm import TILE, canonical_tiles
+        from ..generator.formats import bsr_arrays
+        nat = self.native
+        k = proj.id
+        batch, w = proj._batched
+        n_post, n_pre = w.shape
+        d = bsr_arrays(np.arange(n_post), w.indptr, w.indices, w.data, n_pre, TILE)
+        vals = d["values"].reshape(-1, TILE, TILE).transpose(0, 2, 1)      # [block][row][k]
+        n_bcols = -(-n_pre // TILE)
+        nat.create(f"proj{k}__brow", d["block_row_ptr"].astype(np.int32))
+        nat.create(f"proj{k}__bcol", d["block_col"].astype(np.int32))
+        nat.create(f"proj{k}__tiles", to_bf16(canonical_tiles(vals)))
+        nat.create_empty(f"proj{k}__xt", np.uint16, (n_bcols * batch * TILE,))
+        self.layout[k] = {"format": "bsr_tc", "rows": n_post, "nnz": int(w.nnz),
+                          "n_block_rows": int(d["n_block_rows"]), "n_blocks": int(d["n_blocks"]),
+                          "batch": batch, "n_pre": n_pre, "n_post": n_post}
+
     def _create_projection(self, proj):
         nat = self.native
         k = proj.id
+        if getattr(proj, "_batched", None) is not None:
+            return self._create_batched_tc(proj)
         if getattr(proj, "_device_conn", None):
             return self._create_device_projection(proj)
         self._create_delays(proj)

@@ -102,12 +102,20 @@ struct Array {
   size_t bytes = 0;
 };
 
+// Plan entries that are library operations rather than module kernels.
+enum { kOpKernel = 0, kOpBsrTc = 1 };
+
 struct Launch {
   std::string name;
   CUfunction fn = nullptr;
   unsigned grid = 1, block = 1, smem = 0;
   unsigned cluster = 1;  // CTAs per thread-block cluster (launch attribute)
   int group = 0;         // consecutive launches of one nonzero group may run concurrently
+  int op = kOpKernel;
+  // kOpBsrTc: arrays block_row_ptr, block_col, tiles, x, x_tiles, y and the
+  // sizes n_block_rows, batch, n_pre, n_post
+  std::string arr[6];
+  int iarg[4] = {0, 0, 0, 0};
 };
 
 struct TimedLaunch {
@@ -211,7 +219,30 @@ int bind(anb_net* net) {
   return ANB_OK;
 }
 
+// The batched block-sparse product of a plan entry: the rates x (batch x
+// n_pre, row-major) packed into bfloat16 tiles, then y (batch x n_post) +=
+// x W^T on the tensor cores; a bounded wait that gives up is reported in the
+// network's error word.
+int launch_bsr_tc(anb_net* net, const Launch& l, cudaStream_t st) {
+  void* p[6];
+  for (int i = 0; i < 6; ++i) {
+    Array* a = find(net, l.arr[i].c_str());
+    if (!a) return fail(ANB_ERR_STATE, l.name + ": array " + l.arr[i] + " is missing");
+    p[i] = a->ptr;
+  }
+  Array* err = find(net, "err");
+  int rc = anb_bsr_tc_pack_x((const float*)p[3], l.iarg[1], l.iarg[2], (uint16_t*)p[4], st);
+  if (rc == 0)
+    rc = anb_bsr_spmm_tc((const int*)p[0], (const int*)p[1], (const uint16_t*)p[2], l.iarg[0],
+                         (const uint16_t*)p[4], l.iarg[1], (float*)p[5], l.iarg[3],
+                         err ? (int*)err->ptr : nullptr, st);
+  if (rc == 2) return fail(ANB_ERR_ARG, l.name + ": the block product rejected its sizes");
+  if (rc != 0) return fail(ANB_ERR_CUDA, l.name + ": block product launch failed");
+  return ANB_OK;
+}
+
 int launch(anb_net* net, const Launch& l, void** params, cudaStream_t on = nullptr) {
+  if (l.op == kOpBsrTc) return launch_bsr_tc(net, l, on ? on : net->stream);
   if (l.cluster <= 1) {
     ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem,
                               (CUstream)(on ? on : net->stream), params, nullptr));
@@ -1034,6 +1065,43 @@ int anb_plan_add_concurrent(anb_net* net, const char* kernel, unsigned grid, uns
   if (rc) return rc;
   if (group < 0) return fail(ANB_ERR_ARG, "group must be >= 0");
   l.group = group;
+  drop_graph(net);
+  net->plan.push_back(l);
+  return ANB_OK;
+}
+
+int anb_plan_add_bsr_tc(anb_net* net, const char* prefix, const char* x_array,
+                        const char* y_array, int n_block_rows, int batch, int n_pre, int n_post,
+                        int group) {
+  if (!net || !prefix || !x_array || !y_array) return fail(ANB_ERR_ARG, "NULL argument");
+  if (batch < 16 || batch > 256 || batch % 16)
+    return fail(ANB_ERR_ARG, "batch must be a multiple of 16 between 16 and 256");
+  if (n_block_rows < 0 || n_pre <= 0 || n_post <= 0 || n_block_rows * 64 < n_post)
+    return fail(ANB_ERR_ARG, "inconsistent block-sparse sizes");
+  if (group < 0) return fail(ANB_ERR_ARG, "group must be >= 0");
+  Launch l;
+  l.name = std::string(prefix) + "_bsr_tc";
+  l.op = kOpBsrTc;
+  l.group = group;
+  const std::string p(prefix);
+  const std::string names[6] = {p + "__brow", p + "__bcol", p + "__tiles", x_array, p + "__xt",
+                                y_array};
+  const size_t n_bcols = (size_t)(n_pre + 63) / 64;
+  for (int i = 0; i < 6; ++i) {
+    Array* a = find(net, names[i].c_str());
+    if (!a) return fail(ANB_ERR_ARG, "unknown array " + names[i]);
+    l.arr[i] = names[i];
+  }
+  if (find(net, names[3].c_str())->bytes < sizeof(float) * (size_t)batch * n_pre)
+    return fail(ANB_ERR_ARG, names[3] + " holds fewer than batch x n_pre floats");
+  if (find(net, names[5].c_str())->bytes < sizeof(float) * (size_t)batch * n_post)
+    return fail(ANB_ERR_ARG, names[5] + " holds fewer than batch x n_post floats");
+  if (find(net, names[4].c_str())->bytes < 2 * n_bcols * (size_t)batch * 64)
+    return fail(ANB_ERR_ARG, names[4] + " is too small for the packed rates");
+  l.iarg[0] = n_block_rows;
+  l.iarg[1] = batch;
+  l.iarg[2] = n_pre;
+  l.iarg[3] = n_post;
   drop_graph(net);
   net->plan.push_back(l);
   return ANB_OK;

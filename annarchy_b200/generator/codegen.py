@@ -850,6 +850,14 @@ extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
     {tdecl}{body}
 }}
 """
+        if fmt == "bsr_tc":
+            # copies of the network sharing the weights: one tensor-core
+            # product for all of them (a library operation of the plan)
+            op = {"prefix": f"proj{k}", "x": f"pop{proj.pre_pop.id}__r",
+                  "y": f"pop{proj.post_pop.id}___sum_{proj.target}",
+                  "n_block_rows": lay["n_block_rows"], "batch": lay["batch"],
+                  "n_pre": lay["n_pre"], "n_post": lay["n_post"]}
+            return "", [(op, 0, 0, 0)]
         if proj._delay_steps is not None:
             # one delay per synapse: CSR rows read the rate ring per synapse
             a = proj.pre_pop

@@ -95,6 +95,8 @@ SIGNATURES = {
                                 C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]),
     "anb_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_void_p]),
+    "anb_plan_add_bsr_tc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
+                                      C.c_int, C.c_int, C.c_int, C.c_int]),
     "anb_set_seed": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int]),
     "anb_record_declare": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_int, C.c_int64]),
     "anb_estimate_record_size": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_size_t)]),
@@ -405,6 +407,13 @@ class NativeNet:
         """launches: (kernel, grid, block, shared bytes[, concurrency group])."""
         check("anb_plan_clear", self.lib.anb_plan_clear(self.h))
         for entry in launches:
+            if isinstance(entry[0], dict):          # a library operation
+                op = entry[0]
+                check("anb_plan_add_bsr_tc", self.lib.anb_plan_add_bsr_tc(
+                    self.h, op["prefix"].encode(), op["x"].encode(), op["y"].encode(),
+                    op["n_block_rows"], op["batch"], op["n_pre"], op["n_post"],
+                    entry[4] if len(entry) > 4 else 0))
+                continue
             name, grid, block, smem = entry[:4]
             group = entry[4] if len(entry) > 4 else 0
             check("anb_plan_add_concurrent", self.lib.anb_plan_add_concurrent(

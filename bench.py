@@ -609,6 +609,81 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
     return out
 
 
+def rate_batch_study(batches=(64, 128, 256), steps=200, reps=3):
+    """Copies of the 100k-neuron recurrent rate-coded network on the block
+    matrix (64x64 blocks at 2 % block density) run as one RateBatch (every
+    step: one tensor-core product for all copies, then the neuron update;
+    CUDA graph), against running the copies one after the other on the
+    single-network path (the same network, float state, bfloat16 weights in
+    the selector's format, and the plain double path). Device time (CUDA
+    events on the network's stream) per step; GSynOps/s = synapses x copies
+    / time."""
+    import torch
+    from annarchy_b200 import Network, Neuron, RateBatch, workloads as wl
+    m = wl.sweep_matrix("blocks")
+    n = m.shape[0]
+    neuron = Neuron(parameters="tau = 10.0", equations="tau*dr/dt + r = sum(exc) : min=0.0")
+    peak, kind = peaks()
+    out = {"matrix": "100k blocks 64x64, 2 %", "nnz": int(m.nnz), "steps": steps, "copies": {}}
+
+    def timed(net, nsteps):
+        nat = net._backend.native
+        st = torch.cuda.Stream()
+        nat.set_stream(st.cuda_stream)
+        net.simulate_steps(max(64, nsteps // 4))            # graphs built, warm
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            nat.run(nsteps)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        return best / nsteps
+
+    def single(precision, wd=None):
+        net = Network(dt=1.0, seed=1)
+        cfg = {"precision": precision, "engine": "grid"}
+        if wd:
+            cfg["weight_dtype"] = wd
+        net.config(**cfg)
+        pop = net.create(n, neuron)
+        net.connect(pop, pop, "exc").from_sparse(m.T.tocsr())
+        net.compile()
+        pop.r = np.random.default_rng(0).uniform(0, 1, n)
+        ms = timed(net, steps)
+        fmt = net._backend.layout[0]["format"]
+        net.close()
+        return ms, fmt
+
+    one_bf16, fmt = single("float", "bfloat16")
+    one_fp64, _ = single("double")
+    out["single_copy"] = {"float_bf16_us_per_step": one_bf16 * 1e3, "format": fmt,
+                          "fp64_us_per_step": one_fp64 * 1e3}
+    print(json.dumps(out["single_copy"]), flush=True)
+    for batch in batches:
+        tpl = Network(dt=1.0, seed=1)
+        pop = tpl.create(n, neuron)
+        tpl.connect(pop, pop, "exc").from_sparse(m.T.tocsr())
+        rb = RateBatch(tpl, batch)
+        rb.compile()
+        rb.set(pop, "r", np.random.default_rng(batch).uniform(0, 1, (batch, n)))
+        ms = timed(rb.net, steps)
+        lay = rb.net._backend.layout[0]
+        stored = lay["n_blocks"] * 64 * 64
+        res = {"us_per_step": ms * 1e3, "gsynops": m.nnz * batch / (ms * 1e-3) / 1e9,
+               "tflops_product": 2.0 * stored * batch / (ms * 1e-3) / 1e12,
+               "vs_sequential_float_bf16": one_bf16 * batch / ms,
+               "vs_sequential_fp64": one_fp64 * batch / ms,
+               "device_error": rb.net._backend.native.device_error()}
+        out["copies"][batch] = res
+        print(json.dumps({batch: res}), flush=True)
+        rb.close()
+    return out
+
+
 def wl_blocks_stored(m):
     """Stored entries of m in 64 x 64 blocks (every block with a nonzero)."""
     import scipy.sparse as sp
@@ -999,6 +1074,8 @@ def main():
                     help="skip the batched-instance summary in the default line")
     ap.add_argument("--fast-only", action="store_true",
                     help="time only the fast path (used for profiler captures)")
+    ap.add_argument("--only", default="", choices=("", "exact", "fast"),
+                    help="time only this path of the default workload (profiler captures)")
     ap.add_argument("--accuracy", action="store_true", help="multi-seed accuracy study only")
     ap.add_argument("--large", type=int, default=0,
                     help="the large plastic network with this many neurons (1000000 = 1e9 synapses)")
@@ -1012,6 +1089,9 @@ def main():
     ap.add_argument("--spmm", default="",
                     help="batched block-sparse products on the tensor cores for these batch "
                          "sizes (comma separated, e.g. 64,128,256)")
+    ap.add_argument("--rate-batch", default="",
+                    help="copies of the 100k block-matrix rate network as one RateBatch for these "
+                         "batch sizes (comma separated, e.g. 64,128,256)")
     ap.add_argument("--batched-steps", type=int, default=5000,
                     help="time steps of the batched-instance study")
     ap.add_argument("--rate", action="store_true",
@@ -1038,6 +1118,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         spmm_study(tuple(int(b) for b in args.spmm.split(",")))
+        return
+    if args.rate_batch:
+        import torch
+        torch.cuda.set_device(0)
+        rate_batch_study(tuple(int(b) for b in args.rate_batch.split(",")))
         return
     if args.delays:
         import torch
@@ -1089,12 +1174,15 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(accuracy_study()))
         return
-    if args.fast_only:
+    if args.fast_only or args.only:
         import torch
         torch.cuda.set_device(0)
         from annarchy_b200 import workloads as wl
         cn = wl.coba_net(seed=42)
-        net, P, mon = build_net(cn, "float", "local", "float32")
+        if args.only == "exact":
+            net, P, mon = build_net(cn, "double", "local")
+        else:
+            net, P, mon = build_net(cn, "float", "local", "float32")
         dev = time_device(net, P, mon, cn, args.steps, args.warmup)
         print(json.dumps({"ms_per_step": sum(dev["ms"]) / len(dev["ms"]),
                           "events_per_step": sum(dev["events"]) / len(dev["events"]),
@@ -1154,25 +1242,30 @@ def main():
         v0_pin = torch.from_numpy(cn.v0.astype(dtype)).pin_memory()
         zeros_pin = torch.zeros(cn.n, dtype=torch.float64 if dtype == np.float64
                                 else torch.float32).pin_memory()
-        t_, ev_, sp_ = [], [], []
+        t_, ev_, sp_, parts = [], [], [], []
         for it in range(args.warmup + args.steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             P.set({"v": v0_pin.numpy(), "g_exc": zeros_pin.numpy(), "g_inh": zeros_pin.numpy()})
             net._backend.native.zero(f"pop{P.id}__refractory_remaining")
             net.set_current_step(0)
+            ta = time.perf_counter()
             net.simulate(MODEL_STEPS * cn.dt)
+            tb = time.perf_counter()
             spikes = mon.get("spike")
             t1 = time.perf_counter()
             if it >= args.warmup:
                 t_.append(t1 - t0)
+                parts.append((ta - t0, tb - ta, t1 - tb))
                 ev_.append(sum(out_deg[k] * len(v) for k, v in spikes.items()))
                 sp_.append(sum(len(v) for v in spikes.values()))
         sb = np.dtype(dtype).itemsize
+        pm = np.mean(np.array(parts), axis=0) * 1e3
         return {"value": world * (sum(ev_) / len(ev_)) / (sum(t_) / len(t_)) / 1e9, "unit": UNIT,
                 "h2d_bytes_per_step": 3 * cn.n * sb + 8,
                 # (step, rank) int32 pairs and the spike count
-                "d2h_bytes_per_step": int(8 * sum(sp_) / len(sp_) + 8)}
+                "d2h_bytes_per_step": int(8 * sum(sp_) / len(sp_) + 8),
+                "ms_set_simulate_get": [round(float(x), 3) for x in pm]}
 
     e2e = e2e_run(net, P, mon, np.float64)
     net_engine = net.engine

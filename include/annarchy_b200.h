@@ -322,6 +322,19 @@ int anb_bsr_tc_pack_x(const float* x, int batch, int n_pre, uint16_t* x_tiles, v
 int anb_bsr_spmm_tc(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
                     int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
                     int* err, void* stream);
+/* Append to the step plan the batched weighted sums of one rate-coded
+ * projection shared by `batch` instances: per step the rates in array
+ * x_array (batch x n_pre float, row-major) are packed into bfloat16 tiles
+ * ("<prefix>__xt") and "<prefix>__brow", "__bcol", "__tiles" (the weights as
+ * 64 x 64 bfloat16 blocks, layout of anb_bsr_spmm_tc) add x W^T into y_array
+ * (batch x n_post float). Runs on the network's stream inside the step's
+ * CUDA graph; `group` as anb_plan_add_concurrent. Replaces, for a batch of
+ * network copies, the per-copy BSR weighted sum of
+ * ANNarchy/generator/Projection/CUDA/BSR.py:296-392. */
+int anb_plan_add_bsr_tc(anb_net* net, const char* prefix, const char* x_array,
+                        const char* y_array, int n_block_rows, int batch, int n_pre, int n_post,
+                        int group);
+
 /* Launch shape of anb_bsr_spmm_tc for this process: resident CTAs per SM
  * (1-4), shared-memory stages per CTA (2-12) and consecutive blocks of a row
  * per stage (1-8); 0 keeps the automatic choice (two stages; two blocks per
