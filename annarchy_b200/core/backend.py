@@ -138,7 +138,11 @@ class CompiledNetwork:
             nat.create("tickc", np.zeros(1, dtype=np.uint32))
             if any(getattr(p, "stop_condition", None) for p in net.populations):
                 nat.create("stop_flags", np.full(len(net.populations), -1, dtype=np.int64))
-            mod = gen.grid_module()
+            if self._persistent() and gen.persistent_ok():
+                nat.create("gbar", np.zeros(2, dtype=np.uint32))
+                mod = gen.persistent_module()
+            else:
+                mod = gen.grid_module()
         self.module = mod
         nat.load_module(mod.source, mod.options)
         self.write_constants()
@@ -149,6 +153,16 @@ class CompiledNetwork:
             nat.set_graph_steps(int(net._config.get("graph_steps", 32)))
             for pop_id, kernel, grid, block, mode_all in mod.stops:
                 nat.set_stop_kernel(pop_id, kernel, grid, block, mode_all)
+
+    def _persistent(self) -> bool:
+        """Run the grid engine's step as one persistent cooperative launch:
+        config persistent=True, or "auto" (the default) for networks with a
+        population of at least 32768 neurons (where the per-step launches of
+        the plan dominate the step)."""
+        mode = self.net._config.get("persistent", "auto")
+        if mode == "auto":
+            return max(p.size for p in self.net.populations) >= 32768
+        return bool(mode)
 
     def _build_cluster(self):
         """Fast spiking engine on one thread-block cluster: the smallest

@@ -648,6 +648,13 @@ __device__ __forceinline__ int anb_pc_row(unsigned c, float wv, const anb_bf16*)
 // + warp) ...] = (first step, end step, header step of the slice holding the
 // first step); col / w: 32 entries per step, columns from 0xF000 on marking
 // header steps. Dynamic shared memory: panel_width floats.
+// Weight of a pcsr entry as float (streaming load; the compiler folds the
+// constant step offsets of a chunk into the load addresses).
+__device__ __forceinline__ float anb_pc_w(const float* w) { return __ldcs(w); }
+__device__ __forceinline__ float anb_pc_w(const anb_bf16* w) {
+  return __uint_as_float((unsigned)__ldcs(reinterpret_cast<const unsigned short*>(w)) << 16);
+}
+
 template <typename W, int U>
 __device__ __forceinline__ void anb_rate_pcsr(const int* __restrict__ cta_panel,
                                               const int* __restrict__ warp_tab,
@@ -667,33 +674,42 @@ __device__ __forceinline__ void anb_rate_pcsr(const int* __restrict__ cta_panel,
   const int lane = threadIdx.x & 31;
   const int* wt = warp_tab + 3 * (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
   const int sb = wt[0], se = wt[1], hd = wt[2];
-  const unsigned short* cp = col + 32ll * sb + lane;
-  const W* wp = w + 32ll * sb + lane;
+  const unsigned short* __restrict__ cp = col + 32ll * sb + lane;
+  const W* __restrict__ wp = w + 32ll * sb + lane;
   unsigned short ca[U], cb[U];
   float wa[U], wb[U];
-  // the U steps from step j (zeros past the range)
+  // the U steps from step j: all of them (full) or those before se; a step
+  // past the range reads as a padding header (no row), which ends the lane's
+  // current row there; the range test is warp-uniform
   auto load = [&](unsigned short (&c)[U], float (&wv)[U], const int j) {
+    const unsigned short* cq = cp + 32 * (j - sb);
+    const W* wq = wp + 32 * (j - sb);
+    if (j + U <= se) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const bool in = j + u < se;
-      const long long o = 32ll * (j - sb + u);
-      c[u] = in ? anb_ls_h(cp + o) : (unsigned short)0;
-      wv[u] = in ? anb_w1(wp + o) : 0.f;
+      for (int u = 0; u < U; ++u) {
+        c[u] = __ldcs(cq + 32 * u);
+        wv[u] = anb_pc_w(wq + 32 * u);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool in = j + u < se;
+        c[u] = in ? __ldcs(cq + 32 * u) : (unsigned short)0xf000u;
+        wv[u] = in ? anb_pc_w(wq + 32 * u) : 0.f;
+      }
     }
   };
   float acc = 0.f;
   int cur = -1;                                      // sum index of the lane's current row
-  auto consume = [&](const unsigned short (&c)[U], const float (&wv)[U], const int j) {
+  auto consume = [&](const unsigned short (&c)[U], const float (&wv)[U]) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      if (j + u < se) {
-        if (c[u] >= 0xf000u) {                       // header: the previous slice ends
-          if (cur >= 0) atomicAdd(&sum[cur], acc);
-          acc = 0.f;
-          cur = anb_pc_row(c[u], wv[u], w);
-        } else {
-          acc += xs[c[u]] * wv[u];
-        }
+      if (c[u] >= 0xf000u) {                         // header: the previous slice ends
+        if (cur >= 0) atomicAdd(&sum[cur], acc);
+        acc = 0.f;
+        cur = anb_pc_row(c[u], wv[u], w);
+      } else {
+        acc = fmaf(xs[c[u]], wv[u], acc);
       }
     }
   };
@@ -705,9 +721,9 @@ __device__ __forceinline__ void anb_rate_pcsr(const int* __restrict__ cta_panel,
   if (cw4 > 0) anb_bulk_wait(&anb_pc_mbar, err);
   for (int j = sb; j < se; j += 2 * U) {
     load(cb, wb, j + U);
-    consume(ca, wa, j);
+    consume(ca, wa);
     load(ca, wa, j + 2 * U);
-    consume(cb, wb, j + U);
+    consume(cb, wb);
   }
   if (cur >= 0) atomicAdd(&sum[cur], acc);
 }
@@ -928,6 +944,46 @@ __device__ __forceinline__ void anb_spike_scatter_list(int lo, int hi, const int
     for (int q = col_ptr[pre] + c * 32 + lane; q < end; q += 32 * chunks)
       atomicAdd(&g[post_idx[q]], (R)anb_wf(w_pre[q]));
   }
+}
+
+// ---- grid-wide barrier of a cooperative persistent launch ----------------------------
+// bar[0] counts the CTAs that arrived, bar[1] is the generation. Every CTA
+// reads the generation before arriving; the last to arrive resets the count
+// and advances the generation, the others wait (bounded by a cycle budget of
+// about one second) until it changes. Returns false when this or any other
+// CTA gave up (err[0] holds ANB_DEVERR_BARRIER_TIMEOUT): the caller leaves its
+// loop. Other device errors (a full monitor ring) do not stop the run.
+#define ANB_GRID_WAIT_CYCLES (2000000000ll)
+__device__ __forceinline__ bool anb_grid_sync(unsigned* bar, int* err) {
+  __shared__ int anb_gs_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long c0 = clock64();
+      while (*gen == g) {
+        if (clock64() - c0 > ANB_GRID_WAIT_CYCLES ||
+            *(volatile int*)err == ANB_DEVERR_BARRIER_TIMEOUT) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+      if (!ok) atomicExch(err, ANB_DEVERR_BARRIER_TIMEOUT);
+    }
+    __threadfence();
+    anb_gs_ok = ok && *(volatile int*)err != ANB_DEVERR_BARRIER_TIMEOUT;
+  }
+  __syncthreads();
+  return anb_gs_ok != 0;
 }
 
 // ---- monitors ---------------------------------------------------------------------------

@@ -38,10 +38,10 @@ extern "C" __global__ void check_spike_scatter(const anb_u32* spk, const int* cp
 extern "C" __global__ void __launch_bounds__(384, 3) check_rate_pcsr_f32(
     const int* cp, const int* wt, const unsigned short* c, const float* w, const float* x, int n_pre,
     int pw, float* s, int* err) {
-  anb_rate_pcsr<float, 5>(cp, wt, c, w, x, n_pre, pw, s, err);
+  anb_rate_pcsr<float, 8>(cp, wt, c, w, x, n_pre, pw, s, err);
 }
 extern "C" __global__ void __launch_bounds__(384, 3) check_rate_pcsr_bf16(
     const int* cp, const int* wt, const unsigned short* c, const anb_bf16* w, const float* x, int n_pre,
     int pw, float* s, int* err) {
-  anb_rate_pcsr<anb_bf16, 5>(cp, wt, c, w, x, n_pre, pw, s, err);
+  anb_rate_pcsr<anb_bf16, 8>(cp, wt, c, w, x, n_pre, pw, s, err);
 }

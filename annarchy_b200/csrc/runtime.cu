@@ -46,6 +46,7 @@ struct Driver {
   decltype(&cuGetErrorString) getErrorString = nullptr;
   decltype(&cuLaunchKernelEx) launchKernelEx = nullptr;
   decltype(&cuOccupancyMaxActiveClusters) maxActiveClusters = nullptr;
+  decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) maxActiveBlocks = nullptr;
 };
 Driver g_drv;
 
@@ -70,7 +71,8 @@ bool load_driver() {
             entry("cuFuncSetAttribute", &g_drv.funcSetAttribute) &&
             entry("cuGetErrorString", &g_drv.getErrorString) &&
             entry("cuLaunchKernelEx", &g_drv.launchKernelEx) &&
-            entry("cuOccupancyMaxActiveClusters", &g_drv.maxActiveClusters);
+            entry("cuOccupancyMaxActiveClusters", &g_drv.maxActiveClusters) &&
+            entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", &g_drv.maxActiveBlocks);
   g_drv.loaded = ok;
   return ok;
 }
@@ -111,6 +113,7 @@ struct Launch {
   unsigned grid = 1, block = 1, smem = 0;
   unsigned cluster = 1;  // CTAs per thread-block cluster (launch attribute)
   int group = 0;         // consecutive launches of one nonzero group may run concurrently
+  bool cooperative = false;  // all CTAs resident at once (grid-wide barriers)
   int op = kOpKernel;
   // kOpBsrTc: arrays block_row_ptr, block_col, tiles, x, x_tiles, y and the
   // sizes n_block_rows, batch, n_pre, n_post
@@ -243,6 +246,26 @@ int launch_bsr_tc(anb_net* net, const Launch& l, cudaStream_t st) {
 
 int launch(anb_net* net, const Launch& l, void** params, cudaStream_t on = nullptr) {
   if (l.op == kOpBsrTc) return launch_bsr_tc(net, l, on ? on : net->stream);
+  if (l.cooperative) {
+    CUlaunchAttribute attr;
+    std::memset(&attr, 0, sizeof(attr));
+    attr.id = CU_LAUNCH_ATTRIBUTE_COOPERATIVE;
+    attr.value.cooperative = 1;
+    CUlaunchConfig cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDimX = l.grid;
+    cfg.gridDimY = 1;
+    cfg.gridDimZ = 1;
+    cfg.blockDimX = l.block;
+    cfg.blockDimY = 1;
+    cfg.blockDimZ = 1;
+    cfg.sharedMemBytes = l.smem;
+    cfg.hStream = (CUstream)(on ? on : net->stream);
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    ANB_CU(g_drv.launchKernelEx(&cfg, l.fn, params, nullptr));
+    return ANB_OK;
+  }
   if (l.cluster <= 1) {
     ANB_CU(g_drv.launchKernel(l.fn, l.grid, 1, 1, l.block, 1, 1, l.smem,
                               (CUstream)(on ? on : net->stream), params, nullptr));
@@ -1070,6 +1093,24 @@ int anb_plan_add_concurrent(anb_net* net, const char* kernel, unsigned grid, uns
   return ANB_OK;
 }
 
+int anb_set_local_kernel_cooperative(anb_net* net, const char* kernel, unsigned block,
+                                     unsigned shared_bytes, unsigned* grid_out) {
+  if (!net || !kernel) return fail(ANB_ERR_ARG, "NULL argument");
+  Launch l;
+  int rc = resolve(net, kernel, 1, block, shared_bytes, &l);
+  if (rc) return rc;
+  int per_sm = 0, sms = 0;
+  ANB_CU(g_drv.maxActiveBlocks(&per_sm, l.fn, (int)block, (size_t)shared_bytes));
+  ANB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device));
+  if (per_sm < 1) return fail(ANB_ERR_ARG, std::string(kernel) + ": no CTA fits on an SM");
+  l.grid = (unsigned)(per_sm * sms);
+  l.cooperative = true;
+  net->local = l;
+  net->has_local = true;
+  if (grid_out) *grid_out = l.grid;
+  return ANB_OK;
+}
+
 int anb_plan_add_bsr_tc(anb_net* net, const char* prefix, const char* x_array,
                         const char* y_array, int n_block_rows, int batch, int n_pre, int n_post,
                         int group) {
@@ -1174,6 +1215,12 @@ int anb_run(anb_net* net, int64_t nsteps) {
   rc = bind(net);
   if (rc) return rc;
   if (net->has_local) {
+    if (net->local.cooperative) {
+      // the grid barrier's counters start at zero (a run that gave up may
+      // have left a partial count)
+      Array* gb = find(net, "gbar");
+      if (gb) ANB_CUDA(cudaMemsetAsync(gb->ptr, 0, gb->bytes, net->stream));
+    }
     int64_t done = 0;
     while (done < nsteps) {
       long long t0 = (long long)(net->t + done);

@@ -1211,7 +1211,79 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
 """
 
     # ------------------------------------------------------------------ engines
+    def persistent_ok(self) -> bool:
+        """The grid engine's per-step kernels can run as phases of one
+        persistent launch: fast spiking networks whose kernels all walk their
+        work grid-stride (spike-list transmissions, updates, post events,
+        variable records) - no rate-coded projections (some formats need
+        their own grid), delays, timed arrays or stop conditions."""
+        net = self.net
+        if self.exact or not self.c.spike_lists or getattr(self.c, "shard", None):
+            return False
+        if any(p.synapse_type.type != "spike" for p in net.projections):
+            return False
+        if any(getattr(p, "stop_condition", None) or hasattr(p, "_ta_schedule_ms")
+               or p.neuron_type.type != "spike" or self.slots(p) > 1 for p in net.populations):
+            return False
+        return True
+
+    def persistent_module(self) -> Module:
+        """The grid engine's step as one cooperative persistent kernel
+        anb_grid_run(t0, nsteps): every kernel of the step plan becomes a
+        device function; per step the functions run in plan order, the
+        concurrent group of atomic transmissions as one phase, with a
+        grid-wide barrier after every phase (bounded: a CTA that waits about
+        a second reports ANB_DEVERR_BARRIER_TIMEOUT and every CTA leaves).
+        The reference launches each of these kernels every step and copies
+        the spike count to the host between them
+        (ANNarchy/generator/Template/CUDABaseTemplate.py:328-630)."""
+        kernels, plan = self._grid_parts()
+        t_ptr = self.ptr("t")
+        bodies = []
+        for src in kernels:
+            if not src.strip():
+                continue
+            src = re.sub(r'extern "C" __global__ void (?:__launch_bounds__\([^)]*\) )?(\w+)\(\) \{',
+                         r"__device__ __forceinline__ void \1_body(const long long anb_pt) {", src)
+            bodies.append(src.replace("*" + t_ptr, "anb_pt"))
+        phases, i = [], 0
+        while i < len(plan):
+            j = i + 1
+            if len(plan[i]) > 4 and plan[i][4]:
+                while j < len(plan) and len(plan[j]) > 4 and plan[j][4] == plan[i][4]:
+                    j += 1
+            phases.append([e[0] for e in plan[i:j]])
+            i = j
+        resets = "".join(f"\n        {self.ptr(f'pop{p.id}__spn')}[t & 1] = 0;"
+                         for p in self.net.populations if p.neuron_type.type == "spike")
+        steps = []
+        for ph in phases:
+            calls = "".join(f"\n      {name}_body(t);" for name in ph)
+            steps.append(f"""{calls}
+      if (!anb_grid_sync({self.ptr('gbar')}, {self.ptr('err')})) break;""")
+        src = f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) anb_grid_run(long long t0, int nsteps) {{
+    int anb_s = 0;
+    for (; anb_s < nsteps; ++anb_s) {{
+      const long long t = t0 + anb_s;
+      // this step's spike lists start empty (their parity was last read by
+      // the transmissions of step t - 1 and the post events of step t - 2)
+      if (blockIdx.x == 0 && threadIdx.x == 0) {{{resets}
+      }}{''.join(steps)}
+    }}
+    if (blockIdx.x == 0 && threadIdx.x == 0 && anb_s == nsteps) *{t_ptr} = t0 + nsteps;
+}}
+"""
+        return Module(self.assemble(bodies + [src]), self.options(), "grid",
+                      local=("anb_grid_run", 0, BLOCK, 0, -1), kernels=["anb_grid_run"])
+
     def grid_module(self) -> Module:
+        kernels, plan = self._grid_parts()
+        return self._grid_finish(kernels, plan)
+
+    def _grid_parts(self):
+        """Kernels and step plan of the grid engine (without the step
+        counter's epilogue)."""
         net = self.net
         kernels, plan = [], []
         for proj in net.projections:
@@ -1259,6 +1331,10 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
                 kernels.append(self.monitor_kernel(mon))
                 n = self.c.mon_layout[mon.id]["n"]
                 plan.append((f"mon{mon.id}_record", grid_for(max(n, 32)), BLOCK, 0))
+        return kernels, plan
+
+    def _grid_finish(self, kernels, plan) -> Module:
+        net = self.net
         resets = ""
         if self.c.spike_lists:
             for pop in net.populations:

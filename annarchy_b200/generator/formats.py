@@ -365,7 +365,7 @@ def create_format_arrays(compiled, proj, fmt, post_rank, row_ptr, cols, w, lay):
         resident = max(1, min(2048 // block, (228 * 1024) // (4 * pw + 1024 + 64)))
         # steps per chunk (two chunks in flight): what the launch's registers allow
         regs = 65536 // (block * resident) // 8 * 8
-        unroll = int(cfg.get("pcsr_unroll", max(2, min(16, (regs - 26) // 6))))
+        unroll = int(cfg.get("pcsr_unroll", max(2, min(16, (regs - 14) // 5))))
         d = pcsr_arrays(row_ptr, cols, w, proj.pre_pop.size, post_rank=post_rank, panel_width=pw,
                         ctas=int(cfg.get("pcsr_ctas", resident * sms)), warps=block // 32)
         if d["padded"] >= 2 ** 31 - 64 or post_rank.size and int(np.max(post_rank)) >= 2 ** 28 - 2:

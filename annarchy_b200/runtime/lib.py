@@ -95,6 +95,8 @@ SIGNATURES = {
                                 C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]),
     "anb_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_void_p]),
+    "anb_set_local_kernel_cooperative": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint,
+                                                   C.POINTER(C.c_uint)]),
     "anb_plan_add_bsr_tc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                       C.c_int, C.c_int, C.c_int, C.c_int]),
     "anb_set_seed": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int]),
@@ -420,6 +422,12 @@ class NativeNet:
                 self.h, name.encode(), grid, block, smem, group))
 
     def set_local_kernel(self, name, grid, block, smem, cluster: int = 1):
+        if cluster == -1:                       # cooperative: the runtime sizes the grid
+            g = C.c_uint()
+            check("anb_set_local_kernel_cooperative", self.lib.anb_set_local_kernel_cooperative(
+                self.h, name.encode(), block, smem, C.byref(g)))
+            self.local_grid = int(g.value)
+            return
         if cluster > 1:
             check("anb_set_local_kernel_ex", self.lib.anb_set_local_kernel_ex(
                 self.h, name.encode(), grid, block, smem, cluster))

@@ -322,6 +322,16 @@ int anb_bsr_tc_pack_x(const float* x, int batch, int n_pre, uint16_t* x_tiles, v
 int anb_bsr_spmm_tc(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
                     int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
                     int* err, void* stream);
+/* Use the module's persistent kernel `kernel(long long t0, int nsteps)` for
+ * every run: one cooperative launch (all CTAs resident, so the kernel may
+ * separate the phases of a step with grid-wide barriers, bounded waits that
+ * report ANB_DEVERR_BARRIER_TIMEOUT) of as many CTAs of `block` threads as
+ * fit on all SMs; *grid_out receives that number. The reference launches one
+ * kernel per phase and object every step and copies the spike count to the
+ * host in between (ANNarchy/generator/Template/CUDABaseTemplate.py:328-630). */
+int anb_set_local_kernel_cooperative(anb_net* net, const char* kernel, unsigned block,
+                                     unsigned shared_bytes, unsigned* grid_out);
+
 /* Append to the step plan the batched weighted sums of one rate-coded
  * projection shared by `batch` instances: per step the rates in array
  * x_array (batch x n_pre float, row-major) are packed into bfloat16 tiles
