@@ -425,7 +425,13 @@ class CompiledNetwork:
         if pop.neuron_type.type == "spike":
             n = pop.size
             # spike bitmaps of the last R steps (slot t % R holds step t)
-            nat.create(f"pop{pop.id}__spk", np.zeros(R * ((n + 31) // 32), dtype=np.uint32))
+            words = (n + 31) // 32
+            if self.shard:
+                # room for every rank's chunk of words: the all-gather writes
+                # world x chunk words in place
+                from .shard import chunk_words
+                words = max(words, chunk_words(n, int(self.shard[1])) * int(self.shard[1]))
+            nat.create(f"pop{pop.id}__spk", np.zeros(R * words, dtype=np.uint32))
             if self.spike_lists:
                 nat.create_empty(f"pop{pop.id}__spl", np.int32, (2 * n,))
                 nat.create(f"pop{pop.id}__spn", np.zeros(2, dtype=np.int32))
@@ -782,9 +788,16 @@ class CompiledNetwork:
             left -= n
 
     def _exchange_spikes(self, t):
-        """Every rank's bitmap words of step t into every rank's bitmap."""
+        """Every rank's bitmap words of step t into every rank's bitmap. Over
+        NCCL the bitmap is gathered in place in device memory, ordered on the
+        network's stream (no host copy); over gloo through the host."""
         from .shard import chunk_words
         rank, world = (int(x) for x in self.shard)
+        if self._exchange.device == "cuda":
+            for pop in self.net.populations:
+                c = chunk_words(pop.size, world)
+                self._exchange.all_gather_device(self.native, f"pop{pop.id}__spk", c)
+            return
         for pop in self.net.populations:
             words = (pop.size + 31) // 32
             c = chunk_words(pop.size, world)

@@ -39,6 +39,27 @@ class Exchange:
             raise RuntimeError("sharded networks need an initialised torch.distributed process group")
         self.device = "cuda" if backend == "nccl" else "cpu"
 
+    def all_gather_device(self, native, array: str, chunk: int):
+        """In-place all-gather of `chunk` 32-bit words per rank in the device
+        array `array` of the network (rank r's words at r * chunk): NCCL reads
+        this rank's chunk and writes the others' into the same buffer. The
+        collective waits for the work already queued on the network's stream
+        and the stream waits for it, so the next step's kernels see every
+        rank's spikes without a host synchronisation."""
+        import torch
+        ptr, nbytes = native.device_ptr(array), native.nbytes(array)
+        if nbytes < 4 * chunk * self.world:
+            raise RuntimeError(f"{array}: {nbytes} bytes cannot hold {self.world} chunks of {chunk} words")
+
+        class _View:                      # the array's memory seen by torch, no copy
+            __cuda_array_interface__ = {"shape": (chunk * self.world,), "typestr": "<i4",
+                                        "data": (ptr, False), "version": 3, "strides": None}
+        full = torch.as_tensor(_View(), device="cuda")
+        stream = torch.cuda.ExternalStream(native.stream())
+        with torch.cuda.stream(stream):
+            self.dist.all_gather_into_tensor(full, full[self.rank * chunk:(self.rank + 1) * chunk],
+                                             group=self.group)
+
     def all_gather(self, local: np.ndarray) -> np.ndarray:
         import torch
         t = torch.from_numpy(np.ascontiguousarray(local).view(np.int32)).to(self.device)

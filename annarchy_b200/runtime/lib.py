@@ -297,6 +297,13 @@ class NativeNet:
                                                        C.byref(n)))
         return p.value or 0
 
+    def nbytes(self, name: str) -> int:
+        p = C.c_void_p()
+        n = C.c_size_t()
+        check("anb_array_info", self.lib.anb_array_info(self.h, name.encode(), C.byref(p),
+                                                       C.byref(n)))
+        return int(n.value)
+
     def free(self, name: str):
         check("anb_array_free", self.lib.anb_array_free(self.h, name.encode()))
         self.arrays.pop(name, None)

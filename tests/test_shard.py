@@ -88,11 +88,14 @@ def test_shard_builds_local_rows():
     assert sum(rows) == np.count_nonzero(np.diff(cn.w_exc.indptr))
 
 
-def _coba_worker(rank, world, port, precision, steps, q):
+def _coba_worker(rank, world, port, precision, steps, q, backend="gloo"):
     import torch.distributed as dist
     from datetime import timedelta
     os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    if backend == "nccl":
+        import torch
+        torch.cuda.set_device(0)
+    dist.init_process_group(backend, rank=rank, world_size=world, timeout=timedelta(seconds=120))
     try:
         cn = wl.coba_net(seed=21, n=400, p=0.05, steps=steps)
         w_ee = wl.stdp_matrix(cn, 21, 0.05)
@@ -139,3 +142,30 @@ def test_sharded_coba_stdp_equals_oracle():
         _, _, v, lo, hi = res[r]
         assert np.array_equal(v, v_full[lo:hi])
         np.testing.assert_allclose(v, ref["v"][lo:hi], rtol=1e-9)
+
+
+def _nccl_worker(rank, world, port, q):
+    _coba_worker(rank, world, port, "double", 600, q, backend="nccl")
+
+
+@pytest.mark.gpu
+def test_sharded_exchange_in_device_memory_over_nccl():
+    """The exchange over NCCL gathers the bitmap words in place in device
+    memory, ordered on the network's stream (no host copy). One rank on the
+    one GPU of this machine (an NCCL group of one): the sharded path, its
+    padded bitmap and the in-place gather reproduce the unsharded run bit
+    for bit."""
+    steps = 600
+    res = _run_ranks(_nccl_worker, 1, ())
+    cn = wl.coba_net(seed=21, n=400, p=0.05, steps=steps)
+    w_ee = wl.stdp_matrix(cn, 21, 0.05)
+    net, P, mon = wl.build_coba_network(cn, "double", "grid", stdp_w_ee=w_ee)
+    net.compile()
+    net.simulate_steps(steps)
+    s1, i1 = mon.spike_arrays()
+    v_full = P.v.copy()
+    net.close()
+    s, i, v, lo, hi = res[0]
+    assert i1.size > 100
+    assert np.array_equal(s, s1) and np.array_equal(i, i1)
+    assert (lo, hi) == (0, 400) and np.array_equal(v, v_full)
