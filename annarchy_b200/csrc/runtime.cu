@@ -1332,8 +1332,19 @@ int anb_synchronize(anb_net* net) {
   int code = 0;
   rc = anb_device_error(net, &code);
   if (rc) return rc;
-  if (code) return fail(ANB_ERR_TIMEOUT, "device-side error code " + std::to_string(code));
-  return ANB_OK;
+  switch (code) {
+    case 0:
+      return ANB_OK;
+    case 1:  // ANB_DEVERR_BARRIER_TIMEOUT
+      return fail(ANB_ERR_TIMEOUT, "a bounded device-side wait gave up (barrier timeout, "
+                                   "device error code 1); clear it with anb_clear_device_error");
+    case 2:  // ANB_DEVERR_INDEX
+      return fail(ANB_ERR_STATE, "a kernel met an index out of range (device error code 2)");
+    case 3:  // ANB_DEVERR_MONITOR_OVERFLOW
+      return fail(ANB_ERR_STATE, "a monitor's device ring was full (device error code 3)");
+    default:
+      return fail(ANB_ERR_STATE, "device-side error code " + std::to_string(code));
+  }
 }
 
 int anb_device_error(anb_net* net, int* code) {

@@ -473,6 +473,9 @@ class NativeNet:
         check("anb_device_error", self.lib.anb_device_error(self.h, C.byref(c)))
         return c.value
 
+    def clear_device_error(self):
+        check("anb_clear_device_error", self.lib.anb_clear_device_error(self.h))
+
     # -- timing -----------------------------------------------------------------
     def flush_l2(self):
         check("anb_flush_l2", self.lib.anb_flush_l2(self.h))

@@ -316,15 +316,33 @@ def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
                 sel = S.default_model().choose(m) if S.default_model() else None
             except Exception:       # selector unavailable: reported as None
                 sel = None
+            # the selector's and the reference rule's choices are timed too (the
+            # large matrix's reduced schedule list may not hold them): their
+            # regret = their time / the best time
+            regret = {}
+            for who, choice in (("selector", sel), ("heuristic", {"format": tuning.heuristic(m)})):
+                if not choice:
+                    continue
+                name = tuning.schedule_name(choice)
+                if name not in table:
+                    try:
+                        table[name] = tuning.measure(m, choice, "float", dt, reps)
+                    except Exception as e:      # noqa: BLE001 - e.g. a format too large
+                        regret[who] = {"schedule": name, "error": str(e)[:200]}
+                        continue
+                regret[who] = {"schedule": name, "regret": table[name] / min(table.values())}
+            best = min(table, key=table.get)
             # steady state of the best schedule: back-to-back sums, no flush
-            best_sched = next(sc for sc in scheds if tuning.schedule_name(sc) == best)
+            best_sched = next((sc for sc in scheds if tuning.schedule_name(sc) == best),
+                              sel if sel and tuning.schedule_name(sel) == best
+                              else {"format": best})
             warm_ms = tuning.measure(m, best_sched, "float", dt, reps, flush=False)
             out["results"][f"{st}/{dt}"] = {
                 "nnz": int(m.nnz), "mean_row": float(rl.mean()), "max_row": int(rl.max()),
                 "algorithmic_mb": ab / 1e6, "best": best,
                 "best_steady_state": {"ms": warm_ms, "gbs": ab / (warm_ms * 1e-3) / 1e9,
                                       "frac_of_hbm_peak": ab / (warm_ms * 1e-3) / 1e9 / peak},
-                "heuristic": tuning.heuristic(m), "selector": sel,
+                "heuristic": tuning.heuristic(m), "selector": sel, "regret": regret,
                 "stream_floor_us": floor_us,
                 "schedules": {k: {"ms": v, "gbs": ab / (v * 1e-3) / 1e9,
                                   "frac": ab / (v * 1e-3) / 1e9 / peak,
