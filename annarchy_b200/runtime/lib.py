@@ -324,6 +324,7 @@ class NativeNet:
         """Key of the device's random draws (anb_set_seed)."""
         check("anb_set_seed", self.lib.anb_set_seed(self.h, int(seed) & (2**64 - 1),
                                                      int(num_sources), 1 if use_seed_seq else 0))
+        self.arrays["rng_seed"] = (np.dtype(np.uint32), (2,))
 
     def record_declare(self, ring: str, values_per_record: int, value_bytes: int, period: int):
         check("anb_record_declare", self.lib.anb_record_declare(

@@ -75,7 +75,6 @@ def test_set_seed_and_estimate_record_size():
     nat = L.NativeNet(0)
     try:
         nat.set_seed(0x0123456789ABCDEF, 4, True)
-        nat.arrays["rng_seed"] = (np.dtype(np.uint32), (2,))
         assert nat.read("rng_seed").tolist() == [0x89ABCDEF, 0x01234567]
         nat.record_declare("mon0__v", 1000, 8, 1)
         nat.record_declare("mon1__r", 4000, 8, 10)
