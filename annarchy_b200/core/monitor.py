@@ -217,7 +217,7 @@ class Monitor:
         steps = s[order].tolist()
         lo, hi = offs[:-1].tolist(), offs[1:].tolist()
         if self.ranks is None:
-            d = {k: steps[a:b] for k, (a, b) in enumerate(zip(lo, hi))}
+            d = dict(zip(range(size), map(steps.__getitem__, map(slice, lo, hi))))
         else:
             d = {int(k): steps[lo[int(k)]:hi[int(k)]] for k in self.ranks}
         if not keep:
