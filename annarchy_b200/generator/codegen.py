@@ -46,6 +46,7 @@ DEVICE_HEADER = os.path.join(os.path.dirname(HERE), "csrc", "device", "anb_devic
 
 BLOCK = 256
 MAX_GRID = 148 * 16
+PERSISTENT_BLOCK = 1024
 
 CTYPE_OF = {np.dtype(np.float64): "double", np.dtype(np.float32): "float",
             np.dtype(np.int32): "int", np.dtype(np.int64): "long long",
@@ -1261,8 +1262,10 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
             calls = "".join(f"\n      {name}_body(t);" for name in ph)
             steps.append(f"""{calls}
       if (!anb_grid_sync({self.ptr('gbar')}, {self.ptr('err')})) break;""")
+        # one CTA of PERSISTENT_BLOCK threads per SM: few CTAs arrive at each
+        # grid barrier (the arrivals serialise on one counter)
         src = f"""
-extern "C" __global__ void __launch_bounds__({BLOCK}) anb_grid_run(long long t0, int nsteps) {{
+extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run(long long t0, int nsteps) {{
     int anb_s = 0;
     for (; anb_s < nsteps; ++anb_s) {{
       const long long t = t0 + anb_s;
@@ -1275,7 +1278,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) anb_grid_run(long long t0,
 }}
 """
         return Module(self.assemble(bodies + [src]), self.options(), "grid",
-                      local=("anb_grid_run", 0, BLOCK, 0, -1), kernels=["anb_grid_run"])
+                      local=("anb_grid_run", 0, PERSISTENT_BLOCK, 0, -1), kernels=["anb_grid_run"])
 
     def grid_module(self) -> Module:
         kernels, plan = self._grid_parts()
