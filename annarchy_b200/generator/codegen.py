@@ -1003,9 +1003,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     def _packed(self, proj):
         return trace_layout(proj, self.exact)
 
-    def _pack_body(self, proj, body: str, idx: str = "j") -> str:
-        """Per-synapse statements on the packed record: load it once, use
-        its fields, store it back."""
+    def _pack_fields(self, proj, body: str, idx: str = "j") -> str:
+        """Per-synapse statements rewritten onto the fields of the packed
+        record `anb_s` (unchanged when the projection keeps separate arrays)."""
         lay = self._packed(proj)
         if lay is None:
             return body
@@ -1013,8 +1013,113 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
         body = body.replace(f"_last_event[{idx}] = t;", "anb_s._last_event = (int)t;")
         for n in names + ["_last_event"]:
             body = re.sub(rf"\b{re.escape(n)}\[{idx}\]", f"anb_s.{n}", body)
-        return (f"anb_tr{proj.id} anb_s = anb_tr[{idx}];\n          {body}\n"
+        return body
+
+    def _pack_body(self, proj, body: str, idx: str = "j") -> str:
+        """Per-synapse statements on the packed record: load it once, use
+        its fields, store it back."""
+        if self._packed(proj) is None:
+            return body
+        return (f"anb_tr{proj.id} anb_s = anb_tr[{idx}];\n          {self._pack_fields(proj, body, idx)}\n"
                 f"          anb_tr[{idx}] = anb_s;")
+
+    def _stdp_statements(self, proj):
+        """(pre-spike statements, post-spike statements) of a plastic spiking
+        projection, per synapse j: the event-driven decays (to t - 1 on the
+        pre side, as the reference's transmission of the previous step's
+        spikes; to t on the post side), then the synapse's own statements."""
+        pre = self._event_driven(proj, "j", "t-1")
+        for v in proj.desc["pre_spike"]:
+            code = self.fill(v["cpp"], local="[j]")
+            if v["name"] == "w" and proj.desc["plasticity"]:
+                code = f"if (anb_plastic) {{ {code} }}"
+            pre.append(self.typed(code))
+        post = self._event_driven(proj, "j", "t")
+        for v in proj.desc["post_spike"]:
+            code = self.fill(v["cpp"], local="[j]")
+            if v["name"] == "w":
+                code = f"if (anb_plastic) {{ {code} }}"
+            post.append(self.typed(code))
+        return "\n          ".join(pre), "\n          ".join(post)
+
+    def fused_stdp_functions(self, proj) -> str:
+        """Device functions of the persistent engine for a plastic projection
+        with post-spike statements, which let the post events of step t - 1
+        run in the same phase as the transmission of step t's spikes (one
+        grid barrier less per step):
+
+        * proj<k>_psp_fused_body(t, fused): the transmission of the spikes of
+          t - 1 (pre-spike statements, g += w); with `fused`, a synapse whose
+          post neuron also spiked at t - 1 first gets its post event of t - 1
+          (the reference's order: post events end step t - 1, transmissions
+          open step t), in the same thread, on the same loaded record;
+        * proj<k>_post_prev_body(t): the post events of the spikes of t - 1
+          (at time t - 1), skipping the synapses whose pre neuron spiked at
+          t - 1 (done by the transmission above)."""
+        k = proj.id
+        lay = self.c.layout[proj.id]
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        a, b = proj.pre_pop.id, proj.post_pop.id
+        pre_stmts, post_stmts = self._stdp_statements(proj)
+        packed = self._packed(proj) is not None
+        load = f"anb_tr{k} anb_s = anb_tr[j];" if packed else ""
+        store = "anb_tr[j] = anb_s;" if packed else ""
+        g = self.ptr(f"pop{b}__g_{proj.target}")
+        pre_bits, post_bits = self.ptr(f"pop{a}__spk"), self.ptr(f"pop{b}__spk")
+        ch, pch = lay["chunks"], lay["post_chunks"]
+        head = f"""
+    const float dt = (float)(*{self.ptr('dt')});
+    const int anb_plastic = {p('flags')}[0];
+    {self._syn_globals(proj)}
+    {self._syn_arrays(proj)}"""
+        return f"""
+__device__ __forceinline__ void proj{k}_psp_fused_body(const long long anb_pt, const int anb_fused) {{
+    const long long t = anb_pt;{head}
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int* __restrict__ anb_list = {self.ptr(f'pop{a}__spl')} + ((t - 1) & 1) * (long long){proj.pre_pop.size};
+    const long long anb_items = (long long){self.ptr(f'pop{a}__spn')}[(t - 1) & 1] * {ch};
+    for (long long anb_it = warp; anb_it < anb_items; anb_it += nwarps) {{
+      const int anb_pre = anb_list[anb_it / {ch}];
+      if (anb_pre < {lay['w0'] * 32} || anb_pre >= {lay['w1'] * 32}) continue;
+      const int anb_c = (int)(anb_it % {ch});
+      const int anb_end = {p('col_ptr')}[anb_pre + 1];
+      for (int anb_k = {p('col_ptr')}[anb_pre] + anb_c * 32 + lane; anb_k < anb_end;
+           anb_k += 32 * {ch}) {{
+        const int j = {p('inv_idx')}[anb_k];
+        const int anb_post = {p('post_idx')}[anb_k];
+        float sum = 0.f;
+        {load}
+        if (anb_fused && anb_bit({post_bits}, anb_post)) {{
+          const long long t = anb_pt - 1;
+          {self._pack_fields(proj, post_stmts)}
+        }}
+        {self._pack_fields(proj, pre_stmts)}
+        {store}
+        atomicAdd(&{g}[anb_post], sum);
+      }}
+    }}
+}}
+
+__device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt) {{
+    const long long t = anb_pt - 1;{head}
+    const int anb_lane = threadIdx.x & 31;
+    const int* __restrict__ anb_list = {self.ptr(f'pop{b}__spl')} + (t & 1) * (long long){proj.post_pop.size};
+    const long long anb_items = (long long){self.ptr(f'pop{b}__spn')}[t & 1] * {pch};
+    for (long long anb_it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_it < anb_items;
+         anb_it += (gridDim.x * blockDim.x) >> 5) {{
+      const int anb_row = {p('row_of')}[anb_list[anb_it / {pch}]];
+      if (anb_row < 0) continue;
+      const int anb_c = (int)(anb_it % {pch});
+      const int anb_end = {p('row_ptr')}[anb_row + 1];
+      for (int j = {p('row_ptr')}[anb_row] + anb_c * 32 + anb_lane; j < anb_end; j += 32 * {pch}) {{
+        if (anb_bit({pre_bits}, {p('col')}[j])) continue;   // done with the transmission
+        {self._pack_body(proj, post_stmts)}
+      }}
+    }}
+}}
+"""
 
     def _syn_arrays(self, proj):
         lay = self._packed(proj)
@@ -1240,6 +1345,14 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
         (ANNarchy/generator/Template/CUDABaseTemplate.py:328-630)."""
         kernels, plan = self._grid_parts()
         t_ptr = self.ptr("t")
+        # plastic projections with post events: those run with the next
+        # step's transmissions (fused_stdp_functions), the last step's after
+        # the loop
+        fused = [p for p in self.net.projections
+                 if p.synapse_type.type == "spike" and p.desc.get("post_spike")]
+        fused_ids = {p.id for p in fused}
+        plan = [e for e in plan if not (e[0].endswith("_post_event") and
+                                       int(e[0][4:e[0].index("_")]) in fused_ids)]
         bodies = []
         for src in kernels:
             if not src.strip():
@@ -1257,11 +1370,21 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
             i = j
         resets = "".join(f"\n        {self.ptr(f'pop{p.id}__spn')}[t & 1] = 0;"
                          for p in self.net.populations if p.neuron_type.type == "spike")
+        def call(name):
+            if name.endswith("_psp") and int(name[4:name.index("_")]) in fused_ids:
+                k = name[4:name.index("_")]
+                return (f"\n      proj{k}_psp_fused_body(t, anb_s > 0);"
+                        f"\n      if (anb_s > 0) proj{k}_post_prev_body(t);")
+            return f"\n      {name}_body(t);"
         steps = []
         for ph in phases:
-            calls = "".join(f"\n      {name}_body(t);" for name in ph)
+            calls = "".join(call(name) for name in ph)
             steps.append(f"""{calls}
       if (!anb_grid_sync({self.ptr('gbar')}, {self.ptr('err')})) break;""")
+        bodies += [self.fused_stdp_functions(p) for p in fused]
+        # the post events of the last step (the next launch starts unfused):
+        # proj<k>_post_event_body, converted with the plan's other kernels
+        tail = "".join(f"\n      proj{p.id}_post_event_body(t0 + nsteps - 1);" for p in fused)
         # one CTA of PERSISTENT_BLOCK threads per SM: few CTAs arrive at each
         # grid barrier (the arrivals serialise on one counter)
         src = f"""
@@ -1273,6 +1396,8 @@ extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run
       // the transmissions of step t - 1 and the post events of step t - 2)
       if (blockIdx.x == 0 && threadIdx.x == 0) {{{resets}
       }}{''.join(steps)}
+    }}
+    if (anb_s == nsteps && nsteps > 0) {{{tail}
     }}
     if (blockIdx.x == 0 && threadIdx.x == 0 && anb_s == nsteps) *{t_ptr} = t0 + nsteps;
 }}
