@@ -10,9 +10,8 @@ Instances never exchange data, so the only barriers are the CTA's own:
 
     for every step:
         deliver the spikes of the previous step of every own instance
-        (fast: shared-memory atomics; exact: one warp per instance and
-        conductance array, spike by spike in ascending pre rank with a warp
-        barrier per spike, the reference's per-post order)
+        (fast: shared-memory atomics; exact: spike by spike in ascending pre
+        rank with one CTA barrier per spike, the reference's per-post order)
         __syncthreads
         update every own instance's neurons, spike bitmap words by ballot
         (and into the spike monitor ring)
@@ -95,13 +94,10 @@ class BatchGenerator(CodeGenerator):
         {nl.join(body)}
       }}"""
 
-    def _delivery_exact_warp(self, proj) -> str:
-        """Exact mode, one warp: the projection's spikes of this instance in
-        ascending pre rank; per spike the lanes add its synapses (distinct
-        post neurons), then a warp barrier. The warp owns the instance's
-        conductance array of this target, so every post neuron adds its inputs
-        in the reference's order (ANNarchy/generator/Projection/OpenMP/
-        CSR.py:870-902) without CTA barriers."""
+    def _delivery_exact(self, proj) -> str:
+        """Exact mode: the spikes of the projection in ascending pre rank, one
+        CTA barrier after each, so every post neuron adds its inputs in the
+        reference's order (ANNarchy/generator/Projection/OpenMP/CSR.py:870-902)."""
         k = proj.id
         a, b = proj.pre_pop.id, proj.post_pop.id
         spk_col = self.b.array_index[(a, "spk")]
@@ -110,30 +106,26 @@ class BatchGenerator(CodeGenerator):
         cp = self.ptr(f"proj{k}__col_ptr")
         post, w = self.ptr(f"proj{k}__post"), self.ptr(f"proj{k}__w")
         return f"""
-          {{  // {proj.name}: spikes in ascending pre rank
-            const anb_u32* __restrict__ anb_spk = reinterpret_cast<const anb_u32*>(anb_smem + anb_so[{spk_col}]);
-            real* __restrict__ anb_g = reinterpret_cast<real*>(anb_smem + anb_so[{g_col}]);
-            const int anb_w0 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si];
-            const int anb_w1 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si + 1];
-            const {it}* __restrict__ anb_cp = {cp} + {self.ptr(f'proj{k}__bcpoff')}[anb_si];
-            for (int c = anb_w0; c < anb_w1; c += 32) {{
-              const anb_u32 anb_wv = (c + anb_lane < anb_w1) ? anb_spk[c + anb_lane] : 0u;
-              anb_u32 anb_nz = __ballot_sync(0xffffffffu, anb_wv != 0u);
-              while (anb_nz) {{
-                const int j = __ffs(anb_nz) - 1;
-                anb_nz &= anb_nz - 1;
-                anb_u32 m = __shfl_sync(0xffffffffu, anb_wv, j);
-                while (m) {{
-                  const int pre = ((c + j) << 5) + __ffs(m) - 1;
-                  m &= m - 1;
-                  const {it} beg = anb_cp[pre], end = anb_cp[pre + 1];
-                  for ({it} q = beg + anb_lane; q < end; q += 32)
-                    anb_g[{post}[q]] += {w}[q];
-                  __syncwarp();
-                }}
-              }}
+      {{  // {proj.name}: spikes in ascending pre rank, one CTA barrier per spike
+        const anb_u32* __restrict__ anb_spk = reinterpret_cast<const anb_u32*>(anb_smem + anb_so[{spk_col}]);
+        real* __restrict__ anb_g = reinterpret_cast<real*>(anb_smem + anb_so[{g_col}]);
+        const int anb_w0 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si];
+        const int anb_w1 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si + 1];
+        const {it}* __restrict__ anb_cp = {cp} + {self.ptr(f'proj{k}__bcpoff')}[anb_si];
+        for (int word = anb_w0; word < anb_w1; ++word) {{
+          anb_u32 m = anb_spk[word];
+          while (m) {{
+            const int pre = (word << 5) + __ffs(m) - 1;
+            m &= m - 1;
+            const {it} beg = anb_cp[pre], end = anb_cp[pre + 1];
+            if (end > beg) {{
+              for ({it} q = beg + threadIdx.x; q < end; q += blockDim.x)
+                anb_g[{post}[q]] += {w}[q];
+              __syncthreads();
             }}
-          }}"""
+          }}
+        }}
+      }}"""
 
     def _delivery_list(self, spk_pops) -> str:
         """Fast mode. The spikes of the previous step of every instance of the
@@ -320,22 +312,8 @@ class BatchGenerator(CodeGenerator):
         store = "".join(self._copy(p, False) for p in pops)
         spk_pops = [p for p in pops if any(pr.pre_pop is p for pr in net.projections)]
         if self.exact:
-            # one warp per (instance, conductance array): instances and
-            # targets never share an array, so they deliver in parallel
-            groups: dict[tuple, list] = {}
-            for pr in net.projections:
-                groups.setdefault((pr.post_pop.id, pr.target), []).append(pr)
-            NG = len(groups)
-            branches = "".join(
-                f"\n        {'if' if gi == 0 else 'else if'} (anb_gi == {gi}) {{"
-                + "".join(self._delivery_exact_warp(pr) for pr in prs) + "\n        }"
-                for gi, prs in enumerate(groups.values()))
-            deliver = f"""for (int anb_pair = anb_warp; anb_pair < (anb_se - anb_sb) * {NG};
-           anb_pair += anb_nwarps) {{
-        const int anb_si = anb_sb + anb_pair / {NG};
-        const int anb_gi = anb_pair % {NG};
-        {header}{branches}
-      }}"""
+            deliver = (f"for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{\n        {header}"
+                       + "".join(self._delivery_exact(pr) for pr in net.projections) + "\n      }")
         elif spk_pops:
             deliver = self._delivery_list(spk_pops)
         else:
