@@ -986,30 +986,6 @@ __device__ __forceinline__ bool anb_grid_sync(unsigned* bar, int* err) {
   return anb_gs_ok != 0;
 }
 
-// anb_spike_scatter_list on the CTAs [0, gx) of a partition of the grid (this
-// CTA is number bx of it): the persistent engine runs concurrent
-// transmissions on disjoint sets of CTAs.
-template <typename R, typename W>
-__device__ __forceinline__ void anb_spike_scatter_list_part(int bx, int gx, int lo, int hi,
-                                                            const int* __restrict__ list,
-                                                            int count, int chunks,
-                                                            const int* __restrict__ col_ptr,
-                                                            const int* __restrict__ post_idx,
-                                                            const W* __restrict__ w_pre,
-                                                            R* __restrict__ g) {
-  const int lane = threadIdx.x & 31;
-  const long long items = (long long)count * chunks;
-  for (long long it = ((long long)bx * blockDim.x + threadIdx.x) >> 5; it < items;
-       it += ((long long)gx * blockDim.x) >> 5) {
-    const int pre = list[it / chunks];
-    if (pre < lo || pre >= hi) continue;
-    const int c = (int)(it % chunks);
-    const int end = col_ptr[pre + 1];
-    for (int q = col_ptr[pre] + c * 32 + lane; q < end; q += 32 * chunks)
-      atomicAdd(&g[post_idx[q]], (R)anb_wf(w_pre[q]));
-  }
-}
-
 // ---- monitors ---------------------------------------------------------------------------
 
 // Copy n values (converted to double) into slot `slot` of a ring of `cap` slots.

@@ -1073,12 +1073,11 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     {self._syn_globals(proj)}
     {self._syn_arrays(proj)}"""
         return f"""
-__device__ __forceinline__ void proj{k}_psp_fused_body(const long long anb_pt, const int anb_fused,
-                                                      const int anb_bx, const int anb_gx) {{
+__device__ __forceinline__ void proj{k}_psp_fused_body(const long long anb_pt, const int anb_fused) {{
     const long long t = anb_pt;{head}
     const int lane = threadIdx.x & 31;
-    const int warp = (anb_bx * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (anb_gx * blockDim.x) >> 5;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int* __restrict__ anb_list = {self.ptr(f'pop{a}__spl')} + ((t - 1) & 1) * (long long){proj.pre_pop.size};
     const long long anb_items = (long long){self.ptr(f'pop{a}__spn')}[(t - 1) & 1] * {ch};
     for (long long anb_it = warp; anb_it < anb_items; anb_it += nwarps) {{
@@ -1103,14 +1102,13 @@ __device__ __forceinline__ void proj{k}_psp_fused_body(const long long anb_pt, c
     }}
 }}
 
-__device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt, const int anb_bx,
-                                                     const int anb_gx) {{
+__device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt) {{
     const long long t = anb_pt - 1;{head}
     const int anb_lane = threadIdx.x & 31;
     const int* __restrict__ anb_list = {self.ptr(f'pop{b}__spl')} + (t & 1) * (long long){proj.post_pop.size};
     const long long anb_items = (long long){self.ptr(f'pop{b}__spn')}[t & 1] * {pch};
-    for (long long anb_it = (anb_bx * blockDim.x + threadIdx.x) >> 5; anb_it < anb_items;
-         anb_it += (anb_gx * blockDim.x) >> 5) {{
+    for (long long anb_it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_it < anb_items;
+         anb_it += (gridDim.x * blockDim.x) >> 5) {{
       const int anb_row = {p('row_of')}[anb_list[anb_it / {pch}]];
       if (anb_row < 0) continue;
       const int anb_c = (int)(anb_it % {pch});
@@ -1359,16 +1357,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
         for src in kernels:
             if not src.strip():
                 continue
-            # every body runs on CTAs [0, anb_gx) of a partition of the grid,
-            # this CTA being number anb_bx
             src = re.sub(r'extern "C" __global__ void (?:__launch_bounds__\([^)]*\) )?(\w+)\(\) \{',
-                         r"__device__ __forceinline__ void \1_body(const long long anb_pt, "
-                         r"const int anb_bx, const int anb_gx) {", src)
-            src = (src.replace("*" + t_ptr, "anb_pt").replace("blockIdx.x", "anb_bx")
-                   .replace("gridDim.x", "anb_gx")
-                   .replace("anb_spike_scatter_list<", "anb_spike_scatter_list_part<"))
-            src = re.sub(r"anb_spike_scatter_list_part<([^>]*)>\(", r"anb_spike_scatter_list_part<\1>(anb_bx, anb_gx, ", src)
-            bodies.append(src)
+                         r"__device__ __forceinline__ void \1_body(const long long anb_pt) {", src)
+            bodies.append(src.replace("*" + t_ptr, "anb_pt"))
         phases, i = [], 0
         while i < len(plan):
             j = i + 1
@@ -1379,54 +1370,21 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
             i = j
         resets = "".join(f"\n        {self.ptr(f'pop{p.id}__spn')}[t & 1] = 0;"
                          for p in self.net.populations if p.neuron_type.type == "spike")
-        def call(name, bx, gx):
+        def call(name):
             if name.endswith("_psp") and int(name[4:name.index("_")]) in fused_ids:
                 k = name[4:name.index("_")]
-                return (f"{{ proj{k}_psp_fused_body(t, anb_s > 0, {bx}, {gx}); "
-                        f"if (anb_s > 0) proj{k}_post_prev_body(t, {bx}, {gx}); }}")
-            return f"{{ {name}_body(t, {bx}, {gx}); }}"
-
-        def weight(name):
-            # expected work of a body: the chunks per spike of its items
-            if name.endswith("_psp"):
-                k = int(name[4:name.index("_")])
-                lay = self.c.layout[k]
-                return lay.get("chunks", 1) + (lay.get("post_chunks", 0) if k in fused_ids else 0)
-            return 1
+                return (f"\n      proj{k}_psp_fused_body(t, anb_s > 0);"
+                        f"\n      if (anb_s > 0) proj{k}_post_prev_body(t);")
+            return f"\n      {name}_body(t);"
         steps = []
         for ph in phases:
-            if len(ph) == 1:
-                calls = "\n      " + call(ph[0], "blockIdx.x", "gridDim.x")
-            else:
-                # concurrent bodies on disjoint sets of CTAs, in proportion
-                # to their expected work (as the graph runs them as parallel
-                # branches)
-                ws = [weight(n) for n in ph]
-                tot = sum(ws)
-                cuts, acc = [], 0
-                for w_ in ws[:-1]:
-                    acc += w_
-                    cuts.append(acc)
-                lines = ["\n      {", "\n        const int anb_g = (int)gridDim.x, anb_b = (int)blockIdx.x;"]
-                for i, c in enumerate(cuts):
-                    lines.append(f"\n        const int anb_c{i} = max({i + 1}, min(anb_g - {len(ph) - 1 - i}, "
-                                 f"(int)((long long)anb_g * {c} / {tot})));")
-                bounds = ["0"] + [f"anb_c{i}" for i in range(len(cuts))] + ["anb_g"]
-                for i, name in enumerate(ph):
-                    lo, hi = bounds[i], bounds[i + 1]
-                    kw = "if" if i == 0 else "else if"
-                    cond = f"anb_b < {hi}" if i < len(ph) - 1 else ""
-                    head = f"{kw} ({cond})" if cond else "else"
-                    lines.append(f"\n        {head} {call(name, f'anb_b - {lo}', f'{hi} - {lo}')}")
-                lines.append("\n      }")
-                calls = "".join(lines)
+            calls = "".join(call(name) for name in ph)
             steps.append(f"""{calls}
       if (!anb_grid_sync({self.ptr('gbar')}, {self.ptr('err')})) break;""")
         bodies += [self.fused_stdp_functions(p) for p in fused]
         # the post events of the last step (the next launch starts unfused):
         # proj<k>_post_event_body, converted with the plan's other kernels
-        tail = "".join(f"\n      proj{p.id}_post_event_body(t0 + nsteps - 1, blockIdx.x, gridDim.x);"
-                       for p in fused)
+        tail = "".join(f"\n      proj{p.id}_post_event_body(t0 + nsteps - 1);" for p in fused)
         # one CTA of PERSISTENT_BLOCK threads per SM: few CTAs arrive at each
         # grid barrier (the arrivals serialise on one counter)
         src = f"""
