@@ -155,14 +155,11 @@ class CompiledNetwork:
                 nat.set_stop_kernel(pop_id, kernel, grid, block, mode_all)
 
     def _persistent(self) -> bool:
-        """Run the grid engine's step as one persistent cooperative launch:
-        config persistent=True, or "auto" (the default) for networks with a
-        population of at least 32768 neurons (where the per-step launches of
-        the plan dominate the step)."""
-        mode = self.net._config.get("persistent", "auto")
-        if mode == "auto":
-            return max(p.size for p in self.net.populations) >= 32768
-        return bool(mode)
+        """Run the grid engine's step as one persistent cooperative launch
+        (config persistent=True). Off by default: on the 1e9-synapse network
+        it measured 26.9 us per step against 26.8 us for the graph of
+        launches, and 17.4 against 16.1 us on its 200k-neuron version."""
+        return bool(self.net._config.get("persistent", False))
 
     def _build_cluster(self):
         """Fast spiking engine on one thread-block cluster: the smallest
@@ -453,6 +450,32 @@ class CompiledNetwork:
         nat = self.native
         k = proj.id
         d = proj._device_conn
+        if d["kind"] == "pattern":
+            wdt0 = np.float64 if (self.exact or proj.synapse_type.type != "spike" or proj.plastic
+                                  or self.shard) else self.wdtype
+            nnz = nat.connect_distance_pattern(f"proj{k}", d["pkind"], d["post_c"], d["pre_c"],
+                                               d["a_pos"], d["den_pos"], d["a_neg"], d["den_neg"],
+                                               d["threshold"], d["exclude_self"], wdt0)
+            if (proj.synapse_type.type != "spike" or proj.plastic or self.shard
+                    or isinstance(nat, DryNative)):
+                # the CSR comes back for the host path (storage formats, plastic
+                # records, sharding)
+                npost, npre = len(proj.post_ranks_view), len(proj.pre_ranks)
+                if isinstance(nat, DryNative):
+                    rp, col, w = np.zeros(npost + 1, np.int64), np.zeros(0, np.int64), np.zeros(0)
+                else:
+                    rp = nat.read(f"proj{k}__row_ptr").astype(np.int64)
+                    col = nat.read(f"proj{k}__col").astype(np.int64)
+                    w = nat.read(f"proj{k}__w").astype(np.float64)
+                for suffix in ("__post_rank", "__row_ptr", "__col", "__w"):
+                    nat.free(f"proj{k}{suffix}")
+                proj._device_conn = None
+                import scipy.sparse as sp
+                proj._store(sp.csr_matrix((w, col, rp), shape=(npost, npre)), d["name"],
+                            d["storage_format"], d["delays"])
+                return self._create_projection(proj)
+            return self._finish_device_projection(proj, nnz, np.diff(
+                nat.read(f"proj{k}__row_ptr").astype(np.int64)))
         if proj.synapse_type.type != "spike":
             raise NotImplementedError("device connectors are implemented for spiking projections")
         npost = len(proj.post_ranks_view)
@@ -480,6 +503,21 @@ class CompiledNetwork:
                 lengths = np.full(npost, -(-nnz // npost), dtype=np.int64)
             else:
                 lengths = np.diff(nat.read(f"proj{k}__row_ptr").astype(np.int64))
+        return self._finish_device_projection(proj, nnz, lengths)
+
+    def _finish_device_projection(self, proj, nnz, lengths):
+        """Layout of a projection whose CSR arrays the device built: the
+        column view, the spike-list chunks and the launch sizes."""
+        nat = self.native
+        k = proj.id
+        npost = len(proj.post_ranks_view)
+        post0, row0 = int(proj.post_ranks_view[0]), 0
+        if self.shard:
+            lo, hi = self.owned[proj.post_pop.id]
+            a, b = max(lo, post0), min(hi, post0 + npost)
+            row0, post0, npost = a - post0, a, b - a
+        pre_lo, pre_hi = int(proj.pre_ranks[0]), int(proj.pre_ranks[-1]) + 1
+        plastic = proj.plastic
         proj._nnz = nnz
         proj._device_lengths = lengths
         lay = {"rows": npost, "nnz": nnz, "idx_t": "int", "format": "csr", "device": True,

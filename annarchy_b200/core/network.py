@@ -11,9 +11,9 @@ Configuration (``Network.config``):
   weight_dtype "float32" or "bfloat16" storage of static weights (float mode).
   engine       "auto" | "grid" | "local" (see annarchy_b200.generator.codegen).
   graph_steps  steps captured per CUDA graph in the grid engine.
-  persistent   "auto" (default) | True | False: run the grid engine's step as
-               one cooperative persistent kernel with grid-wide barriers
-               (fast spiking networks; "auto" from 32768 neurons on).
+  persistent   True | False (default): run the grid engine's step as one
+               cooperative persistent kernel with grid-wide barriers (fast
+               spiking networks).
   device       CUDA device index.
 """
 from __future__ import annotations

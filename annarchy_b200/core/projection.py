@@ -331,6 +331,18 @@ class Projection:
             raise ValueError(f"{kind} connector: the post-synaptic geometry has fewer dimensions "
                              "than the pre-synaptic one")
         npost, npre = post_c.shape[0], pre_c.shape[0]
+        if self._device_ok(npost * npre // 10):
+            # generated on the device at compile() (anb_connect_distance_pattern)
+            self._device_delays(delays)
+            self._device_conn = dict(kind="pattern", pattern=kind, post_c=post_c, pre_c=pre_c,
+                                     exclude_self=not allow_self_connections, name=name,
+                                     storage_format=storage_format, delays=delays,
+                                     **self._pattern_params)
+            self._nnz = 0                                  # known after compile()
+            self.connector_name = name + " (device)"
+            if storage_format is not None:
+                self._storage_format = storage_format
+            return self
         rows_l, cols_l, w_l = [], [], []
         block = max(1, 4_000_000 // max(npre, 1))
         for r0 in range(0, npost, block):
@@ -366,6 +378,8 @@ class Projection:
         a32, s32 = np.float32(amp), np.float32(sigma)
         den = 2.0 * float(np.float32(s32 * s32))
         a = float(a32)
+        self._pattern_params = dict(pkind=0, a_pos=a, den_pos=den, a_neg=0.0, den_neg=1.0,
+                                    threshold=float(limit) * a)
         return self._pattern("Gaussian", lambda d: a * np.exp(-d / den),
                              lambda v: v > float(limit) * a, delays, allow_self_connections,
                              storage_format, "Gaussian")
@@ -383,6 +397,8 @@ class Projection:
         sp_, sn = np.float32(sigma_pos), np.float32(sigma_neg)
         dp, dn = 2.0 * float(np.float32(sp_ * sp_)), 2.0 * float(np.float32(sn * sn))
         span = abs(float(np.float32(np.float32(amp_pos) - np.float32(amp_neg))))
+        self._pattern_params = dict(pkind=1, a_pos=ap, den_pos=dp, a_neg=an, den_neg=dn,
+                                    threshold=float(limit) * span)
         return self._pattern("DoG", lambda d: ap * np.exp(-d / dp) - an * np.exp(-d / dn),
                              lambda v: np.abs(v) > float(limit) * span, delays,
                              allow_self_connections, storage_format, "Difference-of-Gaussian")
@@ -433,6 +449,12 @@ class Projection:
                 raise NotImplementedError("device connectors need contiguous pre and post ranks")
             return True
         return mode == "auto" and nnz > 20_000_000 and contiguous
+
+    def _device_delays(self, delays):
+        """Device connectors take no synaptic delays (one step at most)."""
+        if not (np.ndim(delays) == 0 and not hasattr(delays, "get_values")
+                and round(float(delays or 0.0) / self._dt()) <= 1):
+            raise NotImplementedError("device connectors take no synaptic delays")
 
     def _device_weights(self, weights, delays) -> dict:
         """Weight law of a device connector: constant (wkind 0), Uniform (1)

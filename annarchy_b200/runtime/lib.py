@@ -95,6 +95,10 @@ SIGNATURES = {
                                 C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]),
     "anb_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_void_p]),
+    "anb_connect_distance_pattern": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p,
+                                               C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_double,
+                                               C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                               C.POINTER(C.c_longlong)]),
     "anb_set_local_kernel_cooperative": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint,
                                                    C.POINTER(C.c_uint)]),
     "anb_plan_add_bsr_tc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
@@ -320,6 +324,27 @@ class NativeNet:
         check("anb_array_copy_strided", self.lib.anb_array_copy_strided(
             self.h, dst.encode(), dst_offset, dst_stride, src.encode(), src_offset, src_stride, count))
 
+    def connect_distance_pattern(self, prefix: str, kind: int, post_coords, pre_coords,
+                                 a_pos: float, den_pos: float, a_neg: float, den_neg: float,
+                                 threshold: float, exclude_self: bool, weight_dtype) -> int:
+        """Gaussian (kind 0) or difference-of-Gaussians (kind 1) pattern built
+        on the device (anb_connect_distance_pattern); returns the synapse count."""
+        qc = np.ascontiguousarray(post_coords, dtype=np.float64)
+        pc = np.ascontiguousarray(pre_coords, dtype=np.float64)
+        wb = np.dtype(weight_dtype).itemsize
+        nnz = C.c_longlong()
+        check("anb_connect_distance_pattern", self.lib.anb_connect_distance_pattern(
+            self.h, prefix.encode(), int(kind), qc.shape[0], qc.ctypes.data_as(C.c_void_p),
+            pc.shape[0], pc.ctypes.data_as(C.c_void_p), qc.shape[1], float(a_pos), float(den_pos),
+            float(a_neg), float(den_neg), float(threshold), 1 if exclude_self else 0, wb,
+            C.byref(nnz)))
+        n = nnz.value
+        for name, dt, count in (("__post_rank", np.int32, qc.shape[0]),
+                                ("__row_ptr", np.int32, qc.shape[0] + 1), ("__col", np.int32, n)):
+            self.arrays[prefix + name] = (np.dtype(dt), (count,))
+        self.arrays[prefix + "__w"] = (np.dtype(weight_dtype), (n,))
+        return int(n)
+
     def set_seed(self, seed: int, num_sources: int = 1, use_seed_seq: bool = True):
         """Key of the device's random draws (anb_set_seed)."""
         check("anb_set_seed", self.lib.anb_set_seed(self.h, int(seed) & (2**64 - 1),
@@ -526,6 +551,14 @@ class DryNative:
 
     def set_seed(self, seed, num_sources=1, use_seed_seq=True):
         self.arrays["rng_seed"] = (np.dtype(np.uint32), (2,))
+
+    def connect_distance_pattern(self, prefix, kind, post_coords, pre_coords, *a):
+        n = len(post_coords)
+        self.arrays[prefix + "__post_rank"] = (np.dtype(np.int32), (n,))
+        self.arrays[prefix + "__row_ptr"] = (np.dtype(np.int32), (n + 1,))
+        self.arrays[prefix + "__col"] = (np.dtype(np.int32), (0,))
+        self.arrays[prefix + "__w"] = (np.dtype(np.float64), (0,))
+        return 0
 
     def record_declare(self, *a):
         pass

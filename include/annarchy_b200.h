@@ -133,6 +133,25 @@ int anb_connect_fixed_number_pre_rows(anb_net* net, const char* prefix, int n_po
                                       uint64_t seed, int weight_kind, double a, double b,
                                       int weight_bytes, int exclude_self);
 
+/* Distance-based pattern generated on the device (replaces the host
+ * construction of ANNarchy/core/ConnectorMethods.py:144-260 and
+ * ANNarchy/cython_ext/Connector.pyx:433-575, a Python loop over all pairs):
+ * post neuron r (coordinates post_coords[r * dim ..], normalized as the
+ * reference's pattern connectors normalize them) receives pre neuron j
+ * (pre_coords[j * dim ..]) with the value amp * exp(-d / den) (kind 0,
+ * gaussian: a_pos, den_pos) or a_pos * exp(-d / den_pos) - a_neg * exp(-d /
+ * den_neg) (kind 1, difference of Gaussians), d the squared distance summed
+ * in float over the dimensions (each term in double), the value rounded to
+ * float; the pair is kept when the value (kind 1: its magnitude) exceeds
+ * threshold; exclude_self drops j == r. Pre ranks ascend per row. Creates the
+ * arrays of anb_connect_fixed_number_pre (post_rank, row_ptr, col, w with
+ * weight_bytes 8, 4 or 2) and stores the synapse count in *nnz_out. */
+int anb_connect_distance_pattern(anb_net* net, const char* prefix, int kind, int n_post,
+                                 const double* post_coords, int n_pre, const double* pre_coords,
+                                 int dim, double a_pos, double den_pos, double a_neg,
+                                 double den_neg, double threshold, int exclude_self,
+                                 int weight_bytes, long long* nnz_out);
+
 /* set_seed(long seed, int num_sources, bool use_seed_seq) of the generated
  * module (ANNarchy/generator/NanoBind/BaseTemplate.py:16, called from
  * ANNarchy/generator/Compiler.py:911-922 and ANNarchy/core/Network.py:673-685):
