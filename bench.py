@@ -631,9 +631,10 @@ def batched_study(n_inst=256, steps=5000, plain_sample=8, plain_steps=500, oracl
                          "graphed_gsynops": plain[32][0],
                          "graphed_us_per_instance_step": plain[32][1],
                          "instances": [int(i) for i in pick], "steps": plain_steps}
-    out["fast_vs_plain_fp64"] = out["float_bfloat16"]["gsynops"] / out["plain_fp64"]["gsynops"]
-    out["fast_vs_plain_fp64_graphed"] = (out["float_bfloat16"]["gsynops"]
-                                         / out["plain_fp64"]["graphed_gsynops"])
+    fast = next(k for k in ("float_bfloat16", "float_float32") if k in out)
+    out["fast_key"] = fast
+    out["fast_vs_plain_fp64"] = out[fast]["gsynops"] / out["plain_fp64"]["gsynops"]
+    out["fast_vs_plain_fp64_graphed"] = out[fast]["gsynops"] / out["plain_fp64"]["graphed_gsynops"]
     if "double" in out:
         out["exact_batch_vs_plain_fp64"] = out["double"]["gsynops"] / out["plain_fp64"]["gsynops"]
     if verbose:
@@ -1351,11 +1352,15 @@ def main():
     # launch): fast path only, plain FP64 single-instance path on a sample
     batched = None
     if not args.no_batched:
-        bs = batched_study(256, steps=5000, plain_sample=4, plain_steps=300, oracle_check=0,
-                           variants=(("float", "bfloat16"),), verbose=False)
-        f = bs["float_bfloat16"]
+        bs = batched_study(256, steps=5000, plain_sample=4, plain_steps=300, oracle_check=256,
+                           variants=(("float", "float32"), ("double", None)), verbose=False)
+        f = bs["float_float32"]
         batched = {"workload": "256 COBA instances, N~U{1000..8000}, p=0.02, 5000 steps, "
-                               "float state / bfloat16 weights",
+                               "float state / float32 weights",
+                   "rate_err_per_instance_vs_fp64": f.get("rate_err_per_instance", {}).get("mean"),
+                   "rate_err_total_vs_fp64": f.get("rate_err_total"),
+                   "fp64_batch_every_instance_bit_exact_vs_oracle":
+                       bs["double"].get("oracle_bit_exact", {}).get("ok"),
                    "gsynops": f["gsynops"], "us_per_step": f["us_per_step"],
                    "instance_rtf": f["instance_rtf"], "ctas": f["ctas"],
                    "plain_fp64_gsynops": bs["plain_fp64"]["gsynops"],
