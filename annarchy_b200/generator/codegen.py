@@ -1740,48 +1740,13 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
             deliver = (f"const int beg = {cp}[pre - {lo}], end = {cp}[pre - {lo} + 1];")
             spk = f"(anb_par ? {smem_ptrs[a]['spk0']} : {smem_ptrs[a]['spk1']})"
             if self.exact:
-                # one warp per conductance array: it collects the projection's
-                # spikes in ascending pre rank, up to 32 at a time (one per
-                # lane), then delivers them one after the other; a spike's
-                # synapses (distinct posts) go to the lanes, and the next
-                # spike's post indices and weights are loaded before the
-                # current spike's additions, so only the read-modify-write of
-                # the conductances and a warp barrier stay on the chain. Per
-                # post neuron the additions keep ascending pre rank, the
-                # reference's order.
-                wq = (lambda q: w_src + "[" + w_idx.replace("q", q) + "]") if not palette else (
-                    lambda q: f"{w_src}[anb_s_pool_w[{q}]]")
-                rct = "double"
-                rnd = f"""
-              {{  // deliver the collected spikes (lanes < anb_ns hold them)
-                int anb_bb = 0, anb_ee = 0;
-                if (anb_lane < anb_ns) {{ anb_bb = {cp}[anb_mypre - {lo}]; anb_ee = {cp}[anb_mypre - {lo} + 1]; }}
-                int anb_b0 = __shfl_sync(0xffffffffu, anb_bb, 0), anb_e0 = __shfl_sync(0xffffffffu, anb_ee, 0);
-                bool anb_v0 = anb_b0 + anb_lane < anb_e0;
-                int anb_p0 = anb_v0 ? (int)anb_s_pool_post[anb_b0 + anb_lane] : 0;
-                {rct} anb_w0 = anb_v0 ? ({rct}){wq("anb_b0 + anb_lane")} : ({rct})0;
-                for (int anb_i = 0; anb_i < anb_ns; ++anb_i) {{
-                  int anb_b1 = 0, anb_e1 = 0, anb_p1 = 0;
-                  {rct} anb_w1 = ({rct})0;
-                  bool anb_v1 = false;
-                  if (anb_i + 1 < anb_ns) {{
-                    anb_b1 = __shfl_sync(0xffffffffu, anb_bb, anb_i + 1);
-                    anb_e1 = __shfl_sync(0xffffffffu, anb_ee, anb_i + 1);
-                    anb_v1 = anb_b1 + anb_lane < anb_e1;
-                    if (anb_v1) {{ anb_p1 = anb_s_pool_post[anb_b1 + anb_lane]; anb_w1 = {wq("anb_b1 + anb_lane")}; }}
-                  }}
-                  if (anb_v0) {g}[anb_p0] += anb_w0;
-                  for (int q = anb_b0 + 32 + anb_lane; q < anb_e0; q += 32)
-                    {g}[anb_s_pool_post[q]] += {wq("q")};
-                  __syncwarp();
-                  anb_b0 = anb_b1; anb_e0 = anb_e1; anb_p0 = anb_p1; anb_w0 = anb_w1; anb_v0 = anb_v1;
-                }}
-                anb_ns = 0;
-              }}"""
+                # one warp per conductance array walks the nonzero words of the
+                # projection's range in ascending order; the lanes add one
+                # spike's synapses (distinct posts), then __syncwarp orders
+                # them before the next spike: per post, ascending pre rank
                 exact_groups.setdefault((b, proj.target), []).append(f"""
         {{  // {proj.name}: spikes in ascending pre rank
           const anb_u32* __restrict__ anb_spk = {spk};
-          int anb_ns = 0, anb_mypre = 0;
           for (int c = {play['w0']}; c < {play['w1']}; c += 32) {{
             const anb_u32 anb_wv = (c + anb_lane < {play['w1']}) ? anb_spk[c + anb_lane] : 0u;
             anb_u32 anb_nz = __ballot_sync(0xffffffffu, anb_wv != 0u);
@@ -1790,14 +1755,16 @@ extern "C" __global__ void __launch_bounds__({block}, 1) anb_local_run(long long
               anb_nz &= anb_nz - 1;
               anb_u32 m = __shfl_sync(0xffffffffu, anb_wv, j);
               while (m) {{
-                const int pre = ((c + j) << 5) + __ffs(m) - 1;
+                const int b = __ffs(m) - 1;
                 m &= m - 1;
-                if (anb_lane == anb_ns) anb_mypre = pre;
-                if (++anb_ns == 32) {rnd}
+                const int pre = ((c + j) << 5) + b;
+                {deliver}
+                for (int q = beg + anb_lane; q < end; q += 32)
+                  {g}[anb_s_pool_post[q]] += {w_src}[{w_idx}];
+                __syncwarp();
               }}
             }}
           }}
-          if (anb_ns > 0) {rnd}
         }}""")
             else:
                 fast_groups.setdefault(a, []).append(f"""
