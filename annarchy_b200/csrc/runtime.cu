@@ -1452,6 +1452,104 @@ int anb_stream_read(anb_net* net, size_t bytes, int reps, double* ms_median) {
   return ANB_OK;
 }
 
+// Tile-fill floor: every CTA streams `copies / gridDim.x` tiles of
+// `tile_bytes`, picked pseudo-randomly from `n_tiles` tiles of an L2-resident
+// buffer, into a ring of `stages` shared-memory stages with bulk copies
+// completing on one mbarrier per stage (one thread issues and waits): the
+// floor of a kernel that stages such tiles from L2 through shared memory.
+// Every wait is bounded; a timeout is reported in `err`.
+__global__ void anb_tile_fill_kernel(const unsigned char* __restrict__ src, int n_tiles,
+                                     unsigned tile_bytes, int copies, int stages, int* err,
+                                     unsigned* sink) {
+  extern __shared__ __align__(128) unsigned char anb_tf_smem[];
+  __shared__ __align__(8) unsigned long long full[16];
+  if (threadIdx.x != 0) return;
+  for (int q = 0; q < stages; ++q)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&full[q]))
+                 : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  auto wait = [&](int q, unsigned parity) {
+    const unsigned mb = (unsigned)__cvta_generic_to_shared(&full[q]);
+    unsigned done = 0;
+    for (int it = 0; it < (1 << 24) && !done; ++it)
+      asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                   : "=r"(done) : "r"(mb), "r"(parity) : "memory");
+    if (!done) atomicExch(err, 1);
+    return done != 0;
+  };
+  unsigned acc = 0;
+  int k = 0;
+  for (int i = blockIdx.x; i < copies; i += gridDim.x, ++k) {
+    const int q = k % stages;
+    if (k >= stages) {
+      if (!wait(q, (unsigned)(k / stages - 1) & 1u)) return;
+      acc += anb_tf_smem[(size_t)q * tile_bytes];
+    }
+    const unsigned mb = (unsigned)__cvta_generic_to_shared(&full[q]);
+    const unsigned t = (unsigned)(((unsigned long long)i * 2654435761ull) % (unsigned)n_tiles);
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }"
+                 ::"r"(mb), "r"(tile_bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"((unsigned)__cvta_generic_to_shared(anb_tf_smem + (size_t)q * tile_bytes)),
+                 "l"(src + (size_t)t * tile_bytes), "r"(tile_bytes), "r"(mb)
+                 : "memory");
+  }
+  for (int d = 0; d < (k < stages ? k : stages); ++d) {
+    const int kq = k - 1 - d;
+    if (!wait(kq % stages, (unsigned)(kq / stages) & 1u)) return;
+    acc += anb_tf_smem[(size_t)(kq % stages) * tile_bytes];
+  }
+  if (acc == 0x9e3779b9u) *sink = acc;
+}
+
+int anb_tile_fill(anb_net* net, int n_tiles, int tile_bytes, int copies, int ctas_per_sm, int stages,
+                  int reps, double* ms_median) {
+  if (!net || !ms_median || n_tiles < 1 || tile_bytes < 16 || tile_bytes % 16 || tile_bytes > (64 << 10) ||
+      copies < 1 || ctas_per_sm < 1 || ctas_per_sm > 8 || stages < 1 || stages > 16 || reps < 1 || reps > 64 ||
+      (size_t)stages * tile_bytes > (200u << 10))
+    return fail(ANB_ERR_ARG, "bad arguments");
+  int rc = ensure_device(net);
+  if (rc) return rc;
+  const size_t bytes = (size_t)n_tiles * tile_bytes;
+  void* buf = nullptr;
+  if (cudaMalloc(&buf, bytes + 64) != cudaSuccess) return fail(ANB_ERR_ALLOC, "tile buffer");
+  int* err = reinterpret_cast<int*>(static_cast<char*>(buf) + bytes);
+  unsigned* sink = reinterpret_cast<unsigned*>(static_cast<char*>(buf) + bytes + 16);
+  const size_t smem = (size_t)stages * tile_bytes;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<float> ts;
+  cudaError_t e = cudaMemsetAsync(buf, 0x33, bytes + 64, net->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 4, net->stream);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(anb_tile_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  const int grid = sms * ctas_per_sm;
+  // one untimed pass brings the tiles into L2
+  for (int r = 0; r <= reps && e == cudaSuccess; ++r) {
+    cudaEventRecord(e0, net->stream);
+    anb_tile_fill_kernel<<<grid, 32, smem, net->stream>>>(static_cast<const unsigned char*>(buf), n_tiles,
+                                                         (unsigned)tile_bytes, copies, stages, err, sink);
+    cudaEventRecord(e1, net->stream);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0) ts.push_back(ms);
+  }
+  int h_err = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, 4, cudaMemcpyDeviceToHost);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(ANB_ERR_CUDA, std::string("tile fill: ") + cudaGetErrorString(e));
+  if (h_err) return fail(ANB_ERR_TIMEOUT, "tile fill: a bulk-copy wait timed out");
+  std::sort(ts.begin(), ts.end());
+  *ms_median = ts[ts.size() / 2];
+  return ANB_OK;
+}
+
 int anb_kernel_timing(anb_net* net, int enable) {
   if (!net) return fail(ANB_ERR_ARG, "net is NULL");
   int rc = ensure_device(net);

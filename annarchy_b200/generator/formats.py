@@ -360,9 +360,14 @@ def create_format_arrays(compiled, proj, fmt, post_rank, row_ptr, cols, w, lay):
         cfg = proj.net._config
         pw = int(cfg.get("pcsr_panel", 16384))
         sms = int(cfg.get("sm_count", 148))
-        block = int(cfg.get("pcsr_block", 384))
+        # two CTAs of 512 threads per SM (64 registers a thread: 10 steps per
+        # chunk): on the 100k-neuron uniform, local and power-law matrices
+        # 23.0 / 27.8 / 24.6 us against 23.7 / 34.3 / 28.7 us with three CTAs
+        # of 384 threads (cold L2, float32 weights)
+        block = int(cfg.get("pcsr_block", 512))
         pw = max(32, min(pw, PCSR_HEADER)) // 32 * 32
-        resident = max(1, min(2048 // block, (228 * 1024) // (4 * pw + 1024 + 64)))
+        resident = max(1, min(2048 // block, (228 * 1024) // (4 * pw + 1024 + 64), 2))
+        resident = int(cfg.get("pcsr_resident", resident))
         # steps per chunk (two chunks in flight): what the launch's registers allow
         regs = 65536 // (block * resident) // 8 * 8
         unroll = int(cfg.get("pcsr_unroll", max(2, min(16, (regs - 14) // 5))))

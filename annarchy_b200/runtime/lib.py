@@ -59,7 +59,10 @@ SIGNATURES = {
     "anb_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "anb_bsr_tc_pack_x": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "anb_bsr_spmm_tc_shape": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "anb_bsr_spmm_tc_prefetch": (C.c_int, [C.c_int]),
     "anb_stream_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
+    "anb_tile_fill": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.POINTER(C.c_double)]),
     "anb_array_copy_strided": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_size_t, C.c_char_p,
                                          C.c_size_t, C.c_size_t, C.c_size_t]),
     "anb_plan_add_concurrent": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint, C.c_int]),
@@ -316,6 +319,16 @@ class NativeNet:
         """Median cold streaming-read time (ms) of `nbytes` (anb_stream_read)."""
         out = C.c_double(0.0)
         check("anb_stream_read", self.lib.anb_stream_read(self.h, int(nbytes), reps, C.byref(out)))
+        return out.value
+
+    def tile_fill_ms(self, n_tiles: int, tile_bytes: int, copies: int, ctas_per_sm: int = 2,
+                     stages: int = 3, reps: int = 5) -> float:
+        """Median time (ms) of `copies` bulk copies of L2-resident tiles into
+        shared memory (anb_tile_fill)."""
+        out = C.c_double(0.0)
+        check("anb_tile_fill", self.lib.anb_tile_fill(self.h, int(n_tiles), int(tile_bytes), int(copies),
+                                                      int(ctas_per_sm), int(stages), int(reps),
+                                                      C.byref(out)))
         return out.value
 
     def copy_strided(self, dst, dst_offset, dst_stride, src, src_offset, src_stride, count):

@@ -56,6 +56,13 @@ def tc_shape(ctas_per_sm: int = 0, stages: int = 0, group: int = 0):
         raise ValueError(f"launch shape ({ctas_per_sm}, {stages}, {group}) out of range")
 
 
+def tc_prefetch(blocks: int = 4):
+    """L2 prefetch distance (blocks) of the tensor-core product's weight
+    tiles for this process; see anb_bsr_spmm_tc_prefetch."""
+    if L.load().anb_bsr_spmm_tc_prefetch(int(blocks)) != 0:
+        raise ValueError(f"prefetch distance {blocks} out of range (0-64)")
+
+
 class BlockSparseBatch:
     """Weights w (scipy sparse, n_post x n_pre) as 64 x 64 bfloat16 blocks on
     device `device`; calls compute y[b] = w @ x[b] for `batch` rate vectors

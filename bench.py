@@ -789,6 +789,13 @@ def spmm_study(batches=(64, 128, 256), reps=5):
                         "hbm_frac": wbytes / (ms * 1e-3) / 1e9 / peak}
         if "simt" in res:
             res["tc_speedup"] = res["simt"]["us"] / res["tc"]["us"]
+        # floor of the rate tiles' way from L2 into shared memory: one bulk copy
+        # of a batch x 64 bfloat16 tile per stored block (two CTAs per SM,
+        # three stages each), no products
+        fill = bsb.nat.tile_fill_ms(bsb.n_bcols, batch * 128, bsb.n_blocks, 2,
+                                    max(1, min(16, (96 << 10) // (batch * 128))), reps)
+        res["x_fill_floor_us"] = fill * 1e3
+        res["tc"]["of_x_fill_floor"] = fill / (res["tc"]["us"] * 1e-3)
         out["results"][batch] = res
         print(json.dumps({batch: res}), flush=True)
         bsb.close()

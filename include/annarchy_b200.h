@@ -374,6 +374,12 @@ int anb_plan_add_bsr_tc(anb_net* net, const char* prefix, const char* x_array,
  * columns per SM). Returns 0 or 2. For tuning; no counterpart in the
  * reference. */
 int anb_bsr_spmm_tc_shape(int ctas_per_sm, int stages, int group);
+
+/* L2 prefetch distance of anb_bsr_spmm_tc for this process: while copying a
+ * block, each CTA keeps the weight tiles of its next `blocks` blocks (0-64;
+ * 0 = none, default 4) on their way from HBM into L2 with bulk prefetches.
+ * Returns 0 or 2. For tuning; no counterpart in the reference. */
+int anb_bsr_spmm_tc_prefetch(int blocks);
 int anb_bsr_spmm_simt(const int* block_row_ptr, const int* block_col, const uint16_t* a_tiles,
                       int n_block_rows, const uint16_t* x_tiles, int batch, float* y, int n_post,
                       void* stream);
@@ -389,6 +395,16 @@ int anb_flush_l2(anb_net* net);
  * anb_flush_l2 (a measuring stick for kernels that must read that many bytes
  * once). No counterpart in the reference. */
 int anb_stream_read(anb_net* net, size_t bytes, int reps, double* ms_median);
+/* Tile-fill floor: median device time (ms) over `reps` (1-64) launches of
+ * `ctas_per_sm` (1-8) CTAs per SM that together copy `copies` tiles of
+ * `tile_bytes` (16-65536, a multiple of 16), picked pseudo-randomly from
+ * `n_tiles` tiles of an L2-resident buffer, into `stages` (1-16, at most
+ * 200 KB in all) shared-memory stages per CTA with bulk copies (after one
+ * untimed launch that brings the tiles into L2): the floor of a kernel that
+ * stages such tiles through shared memory. No counterpart in the
+ * reference. */
+int anb_tile_fill(anb_net* net, int n_tiles, int tile_bytes, int copies, int ctas_per_sm, int stages,
+                  int reps, double* ms_median);
 int anb_kernel_timing(anb_net* net, int enable);
 int anb_kernel_time_count(anb_net* net, int* count);
 int anb_kernel_time_get(anb_net* net, int index, char* name, size_t name_len,
