@@ -1452,24 +1452,25 @@ int anb_stream_read(anb_net* net, size_t bytes, int reps, double* ms_median) {
   return ANB_OK;
 }
 
-// Tile-fill floor: every CTA streams `copies / gridDim.x` tiles of
+// Tile-fill floor: every CTA streams its share of `copies` tiles of
 // `tile_bytes`, picked pseudo-randomly from `n_tiles` tiles of an L2-resident
-// buffer, into a ring of `stages` shared-memory stages with bulk copies
-// completing on one mbarrier per stage (one thread issues and waits): the
-// floor of a kernel that stages such tiles from L2 through shared memory.
-// Every wait is bounded; a timeout is reported in `err`.
+// buffer, into `stages` shared-memory stages with bulk copies completing on
+// one mbarrier per stage. Lane 0 of warp w issues the copies of stage w (one
+// thread's bulk copies are served one after another, so every stage has its
+// own issuing thread): the floor of a kernel that stages such tiles from L2
+// through shared memory. Every wait is bounded; a timeout is reported in
+// `err`.
 __global__ void anb_tile_fill_kernel(const unsigned char* __restrict__ src, int n_tiles,
                                      unsigned tile_bytes, int copies, int stages, int* err,
                                      unsigned* sink) {
   extern __shared__ __align__(128) unsigned char anb_tf_smem[];
   __shared__ __align__(8) unsigned long long full[16];
-  if (threadIdx.x != 0) return;
-  for (int q = 0; q < stages; ++q)
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&full[q]))
-                 : "memory");
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) != 0 || w >= stages) return;
+  const unsigned mb = (unsigned)__cvta_generic_to_shared(&full[w]);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  auto wait = [&](int q, unsigned parity) {
-    const unsigned mb = (unsigned)__cvta_generic_to_shared(&full[q]);
+  auto wait = [&](unsigned parity) {
     unsigned done = 0;
     for (int it = 0; it < (1 << 24) && !done; ++it)
       asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -1477,27 +1478,26 @@ __global__ void anb_tile_fill_kernel(const unsigned char* __restrict__ src, int 
     if (!done) atomicExch(err, 1);
     return done != 0;
   };
+  unsigned char* dst = anb_tf_smem + (size_t)w * tile_bytes;
   unsigned acc = 0;
-  int k = 0;
-  for (int i = blockIdx.x; i < copies; i += gridDim.x, ++k) {
-    const int q = k % stages;
-    if (k >= stages) {
-      if (!wait(q, (unsigned)(k / stages - 1) & 1u)) return;
-      acc += anb_tf_smem[(size_t)q * tile_bytes];
+  int k = 0;                                   // uses of this stage
+  for (long long i = blockIdx.x + (long long)w * gridDim.x; i < copies;
+       i += (long long)stages * gridDim.x, ++k) {
+    if (k > 0) {
+      if (!wait((unsigned)(k - 1) & 1u)) return;
+      acc += dst[0];
     }
-    const unsigned mb = (unsigned)__cvta_generic_to_shared(&full[q]);
     const unsigned t = (unsigned)(((unsigned long long)i * 2654435761ull) % (unsigned)n_tiles);
     asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }"
                  ::"r"(mb), "r"(tile_bytes) : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"((unsigned)__cvta_generic_to_shared(anb_tf_smem + (size_t)q * tile_bytes)),
-                 "l"(src + (size_t)t * tile_bytes), "r"(tile_bytes), "r"(mb)
+                 ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src + (size_t)t * tile_bytes),
+                 "r"(tile_bytes), "r"(mb)
                  : "memory");
   }
-  for (int d = 0; d < (k < stages ? k : stages); ++d) {
-    const int kq = k - 1 - d;
-    if (!wait(kq % stages, (unsigned)(kq / stages) & 1u)) return;
-    acc += anb_tf_smem[(size_t)(kq % stages) * tile_bytes];
+  if (k > 0) {
+    if (!wait((unsigned)(k - 1) & 1u)) return;
+    acc += dst[0];
   }
   if (acc == 0x9e3779b9u) *sink = acc;
 }
@@ -1530,7 +1530,7 @@ int anb_tile_fill(anb_net* net, int n_tiles, int tile_bytes, int copies, int cta
   // one untimed pass brings the tiles into L2
   for (int r = 0; r <= reps && e == cudaSuccess; ++r) {
     cudaEventRecord(e0, net->stream);
-    anb_tile_fill_kernel<<<grid, 32, smem, net->stream>>>(static_cast<const unsigned char*>(buf), n_tiles,
+    anb_tile_fill_kernel<<<grid, 32 * stages, smem, net->stream>>>(static_cast<const unsigned char*>(buf), n_tiles,
                                                          (unsigned)tile_bytes, copies, stages, err, sink);
     cudaEventRecord(e1, net->stream);
     e = cudaEventSynchronize(e1);

@@ -196,3 +196,10 @@ def heuristic(m: sp.csr_matrix, plastic: bool = False) -> str:
     if mean <= 128:
         return "ellr" if plastic else "sell_1"
     return "csr"
+
+
+def heuristic_schedule(m: sp.csr_matrix, plastic: bool = False) -> dict:
+    """The reference's choice (heuristic) as a schedule: its GPU SELL has no
+    row sorting (sell_sigma = 1)."""
+    name = heuristic(m, plastic)
+    return {"format": "sell", "sell_sigma": 1} if name == "sell_1" else {"format": name}

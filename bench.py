@@ -320,7 +320,7 @@ def format_study(structures, dtypes=("float32", "bfloat16"), reps=5):
             # large matrix's reduced schedule list may not hold them): their
             # regret = their time / the best time
             regret = {}
-            for who, choice in (("selector", sel), ("heuristic", {"format": tuning.heuristic(m)})):
+            for who, choice in (("selector", sel), ("heuristic", tuning.heuristic_schedule(m))):
                 if not choice:
                     continue
                 name = tuning.schedule_name(choice)

@@ -399,9 +399,10 @@ int anb_stream_read(anb_net* net, size_t bytes, int reps, double* ms_median);
  * `ctas_per_sm` (1-8) CTAs per SM that together copy `copies` tiles of
  * `tile_bytes` (16-65536, a multiple of 16), picked pseudo-randomly from
  * `n_tiles` tiles of an L2-resident buffer, into `stages` (1-16, at most
- * 200 KB in all) shared-memory stages per CTA with bulk copies (after one
- * untimed launch that brings the tiles into L2): the floor of a kernel that
- * stages such tiles through shared memory. No counterpart in the
+ * 200 KB in all) shared-memory stages per CTA with bulk copies, each stage
+ * with its own issuing thread (after one untimed launch that brings the
+ * tiles into L2): the floor of a kernel that stages such tiles through
+ * shared memory. No counterpart in the
  * reference. */
 int anb_tile_fill(anb_net* net, int n_tiles, int tile_bytes, int copies, int ctas_per_sm, int stages,
                   int reps, double* ms_median);

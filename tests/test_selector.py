@@ -62,6 +62,9 @@ def test_heuristic_is_the_reference_rule():
     assert tuning.heuristic(short) == "sell_1"
     assert tuning.heuristic(short, plastic=True) == "ellr"
     assert tuning.heuristic(long_rows) == "csr"
+    assert tuning.heuristic_schedule(short) == {"format": "sell", "sell_sigma": 1}
+    assert tuning.schedule_name(tuning.heuristic_schedule(short)) == "sell_1"
+    assert tuning.heuristic_schedule(long_rows) == {"format": "csr"}
 
 
 @pytest.mark.gpu
