@@ -20,7 +20,7 @@ from __future__ import annotations
 import numpy as np
 
 from ..generator import formats as F
-from ..generator.codegen import (CodeGenerator, compensated_vars, grid_for, list_grid,
+from ..generator.codegen import (CodeGenerator, compensated_vars, global_equations, grid_for, list_grid,
                                  trace_layout)
 from ..runtime.lib import DryNative, NativeNet
 from .monitor import array_name
@@ -92,7 +92,8 @@ class CompiledNetwork:
             if host is not None and n in host:
                 rec[n] = host[n]
             else:
-                init = next((v["init"] for v in proj.desc["variables"] if v["name"] == n), 0.0)
+                init = next((v["init"] for v in proj.desc["variables"] + proj.desc["parameters"]
+                             if v["name"] == n), 0.0)
                 rec[n] = float(init) if not isinstance(init, str) else 0.0
         rec["_last_event"] = -10000
         return rec.view(np.uint32).reshape(-1)
@@ -254,6 +255,8 @@ class CompiledNetwork:
             return False, "device-generated connectivity"
         if any(v != "spike" for m in net.monitors for v in m.variables):
             return False, "variable monitors"
+        if any(global_equations(p) for p in net.populations):
+            return False, "population-level variables with equations"
         smem = self._local_smem_bytes()
         if smem > LOCAL_SMEM_LIMIT:
             return False, f"state needs {smem} bytes of shared memory"
@@ -435,14 +438,14 @@ class CompiledNetwork:
             nat.create(f"pop{pop.id}__refractory", pop.refractory_steps.astype(np.int32))
             nat.create(f"pop{pop.id}__refractory_remaining", np.zeros(n, dtype=np.int32))
             nat.create(f"pop{pop.id}__last_spike", np.full(n, -10000, dtype=np.int64))
+        if global_equations(pop):
+            # ticket of the update kernel's last CTA, which stores the new
+            # values of the population-level variables
+            nat.create(f"pop{pop.id}__gtick", np.zeros(1, dtype=np.uint32))
 
     def _syn_local_names(self, proj):
-        names = [v["name"] for v in proj.desc["variables"]
-                 if v["locality"] == "local" and v["name"] != "w"]
-        for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
-            if v["name"] not in names and v["name"] not in ("w", "g_target"):
-                names.append(v["name"])
-        return names
+        from ..generator.codegen import syn_local_names
+        return syn_local_names(proj)[1:]
 
     def _create_device_projection(self, proj):
         """Fixed in-degree or fixed-probability projection generated on the
@@ -551,7 +554,11 @@ class CompiledNetwork:
                 nat.free(f"proj{k}__w")
             else:
                 for name in self._syn_local_names(proj):
+                    init = next((v["init"] for v in proj.desc["variables"] + proj.desc["parameters"]
+                                 if v["name"] == name), 0.0)
                     nat.create_empty(f"proj{k}__{name}", self.real, (nnz,))
+                    nat.fill(f"proj{k}__{name}",
+                             np.dtype(self.real).type(float(init) if not isinstance(init, str) else 0.0))
                 nat.create_empty(f"proj{k}___last_event", np.int64, (nnz,))
                 nat.fill(f"proj{k}___last_event", np.int64(-10000))
         self.layout[k] = lay

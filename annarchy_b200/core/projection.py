@@ -61,7 +61,15 @@ class Projection:
             raise TypeError("a rate-coded synapse needs a rate-coded pre-synaptic population")
         if self.post_pop.neuron_type.type == "spike" and synapse.type == "spike":
             if target not in self.post_pop.targets:
-                raise ValueError(f"target {target!r} is not used by the post-synaptic neuron")
+                # a conductance the neuron only assigns (`g_exc = 0`) is not
+                # found by the target extraction (ANNarchy/parser/
+                # Extraction.py:686-702 wants a character before `g_`); the
+                # projection adds its target to the population's, as the
+                # reference's does (ANNarchy/core/Projection.py:105-110)
+                if self.post_pop._locality.get("g_" + str(target)) == "local":
+                    self.post_pop.targets.append(target)
+                else:
+                    raise ValueError(f"target {target!r} is not used by the post-synaptic neuron")
         self.pre_ranks = _ranks(pre)
         self.post_ranks_view = _ranks(post)
         self._csr: sp.csr_matrix | None = None   # (n_post_view, n_pre_view), view-relative
@@ -95,7 +103,17 @@ class Projection:
 
     @property
     def plastic(self) -> bool:
-        return bool(self.desc.get("plasticity")) or bool(self.desc.get("post_spike"))
+        """Whether the synapses keep per-synapse state updated by events: the
+        weight changes, post-spike statements, or pre-spike statements that
+        do more than `g_target += w` (short-term plasticity's x and u, a
+        transmission scaled by a synaptic variable)."""
+        d = self.desc
+        if d.get("plasticity") or d.get("post_spike"):
+            return True
+        for v in d.get("pre_spike", []):
+            if v["name"] != "g_target" or v["eq"].replace(" ", "") != "g_target+=w":
+                return True
+        return False
 
     @property
     def storage_format(self) -> str:
@@ -771,13 +789,14 @@ class Projection:
         rows = np.nonzero(np.diff(m.indptr) > 0)[0]
         return [self.pre_ranks[m.indices[m.indptr[r]:m.indptr[r + 1]]].tolist() for r in rows]
 
+    @property
     def dendrites(self):
-        """The dendrites in ascending post rank."""
-        for idx, n in enumerate(self.post_ranks):
-            yield Dendrite(self, n, idx)
+        """The dendrites in ascending post rank (an iterator, a property as in
+        ANNarchy/core/Projection.py:954-970)."""
+        return (Dendrite(self, n, idx) for idx, n in enumerate(self.post_ranks))
 
     def __iter__(self):
-        return self.dendrites()
+        return self.dendrites
 
     def dendrite(self, post):
         """The dendrite of a post-synaptic neuron (rank or coordinates)."""

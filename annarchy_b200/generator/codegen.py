@@ -72,6 +72,26 @@ def compensated_vars(pop, exact: bool, config: dict) -> list:
     return names if comp is True else [n for n in names if n in comp]
 
 
+def global_equations(pop) -> list:
+    """The population-level (global) variables of a population's neuron that
+    have an equation, in declaration order."""
+    glob = set(pop.desc.get("global", []) or [])
+    return [v for v in pop.desc["variables"]
+            if v["name"] in glob and v.get("cpp") and v.get("method") != "event-driven"]
+
+
+def syn_local_names(proj) -> list:
+    """Per-synapse arrays of a plastic spiking projection: w, the other local
+    variables, the local parameters (one value per synapse, as the
+    reference stores them) and what the pre/post-spike statements assign."""
+    names = ["w"] + [v["name"] for v in proj.desc["variables"] + proj.desc["parameters"]
+                     if v["locality"] == "local" and v["name"] != "w"]
+    for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
+        if v["name"] not in names and v["name"] not in ("w", "g_target"):
+            names.append(v["name"])
+    return names
+
+
 def trace_layout(proj, exact: bool):
     """Fast-mode plastic spiking projections keep their per-synapse state
     (w, the other local variables, the last event step) packed in one record
@@ -80,11 +100,7 @@ def trace_layout(proj, exact: bool):
     record bytes) or None when the variables stay separate arrays."""
     if exact or not proj.plastic or proj.synapse_type.type != "spike":
         return None
-    names = ["w"] + [v["name"] for v in proj.desc["variables"]
-                     if v["locality"] == "local" and v["name"] != "w"]
-    for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
-        if v["name"] not in names and v["name"] not in ("w", "g_target"):
-            names.append(v["name"])
+    names = syn_local_names(proj)
     nbytes = 4 * (len(names) + 1)
     nbytes = 8 if nbytes <= 8 else -(-nbytes // 16) * 16
     return names, nbytes
@@ -204,8 +220,7 @@ class CodeGenerator:
             if v.get("cpp", "") == "" or v.get("method") == "event-driven":
                 continue
             if v["name"] not in local:
-                raise NotImplementedError(f"global variable {v['name']!r} with an equation is "
-                                          "not supported by this backend")
+                continue            # population-level: _global_update
             if v.get("switch"):
                 if is_ode:
                     blocks[-1][1].append(v)
@@ -225,6 +240,7 @@ class CodeGenerator:
             for b, val in v.get("bounds", {}).items():
                 if b in ("min", "max"):
                     op = "<" if b == "min" else ">"
+                    val = self.fill(str(val))
                     out.append(f"if ({v['name']} {op} {val}) {v['name']} = {val};")
             return out
 
@@ -272,10 +288,12 @@ class CodeGenerator:
 
     def _globals_preamble(self, pop, src) -> str:
         out = []
+        evolving = {v["name"] for v in global_equations(pop)}
         for p in pop.desc["parameters"] + pop.desc["variables"]:
             if p["locality"] == "global":
                 ct = "int" if p.get("ctype") in ("int", "bool") else self.real
-                out.append(f"const {ct} {p['name']} = {src(p['name'])}[0];")
+                const = "" if p["name"] in evolving else "const "
+                out.append(f"{const}{ct} {p['name']} = {src(p['name'])}[0];")
         for n in self._reciprocals(pop):
             out.append(f"const {self.real} anb_inv_{n} = ({self.real})1 / {n};")
         for v in pop.desc["variables"]:
@@ -288,13 +306,16 @@ class CodeGenerator:
                 "LogNormal": "anb_draw_lognormal", "Exponential": "anb_draw_exponential",
                 "DiscreteUniform": "anb_draw_discrete_uniform"}
 
-    def _random_draws(self, pop) -> str:
+    def _random_draws(self, pop, which: str = "all") -> str:
         """This step's draws of the random distributions in the neuron's
         equations: Philox4x32-10 keyed by the network's seed, counter (neuron,
         step, population and distribution); one draw per neuron, or one per
-        population (same counter in every thread) for a global variable."""
+        population (same counter in every thread) for a global variable.
+        `which`: "all", "local" or "global" draws."""
         out = []
         for k, rd in enumerate(pop.desc.get("random_distributions", [])):
+            if which != "all" and (rd["locality"] == "local") != (which == "local"):
+                continue
             idx = "(unsigned)anb_i" if rd["locality"] == "local" else "0xFFFFFFFFu"
             args = ", ".join(f"({self.real})({self.typed(a)})" for a in rd["args"])
             out.append(f"const {self.real} {rd['name']} = {self._DRAW_FN[rd['dist']]}<{self.real}>("
@@ -333,6 +354,43 @@ class CodeGenerator:
                 out.append(f"const long long anb_mon_t0{m} = {self.ptr(f'mon{m}__t0')}[0];")
         return "\n    ".join(out)
 
+    def _global_update(self, pop) -> str:
+        """The population-level equations of step t, evaluated before the
+        neurons' (the reference's global step, ANNarchy/generator/Population/
+        CUDAGenerator.py: the global kernel launched before the local one) by
+        every thread on the same loaded values, so each has this step's
+        values without a grid barrier; consecutive ODEs form one block (all
+        increments, then the switches and bounds)."""
+        lines, group = [], []
+
+        def flush():
+            for v in group:
+                lines.append(self.typed(self.fill(v["cpp"])))
+            for v in group:
+                lines.append(self.typed(self.fill(v["switch"])))
+                lines.extend(self._bound_lines(v))
+            group.clear()
+
+        for v in global_equations(pop):
+            if v.get("switch"):
+                group.append(v)
+                continue
+            flush()
+            lines.append(self.typed(self.fill(v["cpp"])))
+            lines.extend(self._bound_lines(v))
+        flush()
+        draws = self._random_draws(pop, "global")
+        return "\n    ".join(([draws] if draws else []) + lines)
+
+    def _bound_lines(self, v) -> list:
+        out = []
+        for b, val in v.get("bounds", {}).items():
+            if b in ("min", "max"):
+                op = "<" if b == "min" else ">"
+                val = self.fill(str(val))
+                out.append(self.typed(f"if ({v['name']} {op} {val}) {v['name']} = {val};"))
+        return out
+
     def neuron_update(self, pop, *, local_engine=False, smem=None, cluster=None,
                       ballot_hook=None, size=None, gsrc=None, refractory=None) -> str:
         """Update (+ spike gather) of one population for step t.
@@ -349,9 +407,13 @@ class CodeGenerator:
         that replaces the per-neuron array."""
         spiking = pop.neuron_type.type == "spike"
         masked = spiking and pop._has_refractory
+        geq = bool(global_equations(pop))
+        if geq and (smem or cluster is not None or local_engine or size is not None):
+            raise NotImplementedError(f"{pop.name}: population-level variables with equations run "
+                                      "on the grid engine only")
         body, modified = self._neuron_body(pop, None, masked)
         body = self._use_reciprocals(pop, body)
-        draws = self._random_draws(pop)
+        draws = self._random_draws(pop, "local" if geq else "all")
         if draws:
             body = draws + "\n" + body
         # only the local attributes the update reads or writes are loaded
@@ -561,17 +623,34 @@ class CodeGenerator:
         return 4 if pop.size >= (1 << 18) else (2 if pop.size >= (1 << 16) else 1)
 
     def pop_kernel(self, pop) -> str:
-        preamble = self._globals_preamble(pop, lambda n: self.ptr(f"pop{pop.id}__{n}"))
+        k = pop.id
+        preamble = self._globals_preamble(pop, lambda n: self.ptr(f"pop{k}__{n}"))
         rp = self._fused_record_preamble(pop)
         if rp:
             preamble += "\n    " + rp
+        geq = global_equations(pop)
+        store = ""
+        if geq:
+            preamble += "\n    " + self._global_update(pop)
+            # the last CTA to finish (every other one has read the old values)
+            # stores the new ones
+            writes = " ".join(f"{self.ptr(f'pop{k}__{v['name']}')}[0] = {v['name']};" for v in geq)
+            store = f"""
+    __syncthreads();
+    if (threadIdx.x == 0) {{
+      __threadfence();
+      if (atomicAdd({self.ptr(f'pop{k}__gtick')}, 1u) == gridDim.x - 1) {{
+        *{self.ptr(f'pop{k}__gtick')} = 0u;
+        {writes}
+      }}
+    }}"""
         dt_t = "double" if self.exact else "float"
         return f"""
-extern "C" __global__ void __launch_bounds__({BLOCK}) pop{pop.id}_step() {{
+extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_step() {{
     const long long t = *{self.ptr('t')};
     const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
     {preamble}
-{self.neuron_update(pop)}
+{self.neuron_update(pop)}{store}
 }}
 """
 
@@ -1028,18 +1107,8 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
         projection, per synapse j: the event-driven decays (to t - 1 on the
         pre side, as the reference's transmission of the previous step's
         spikes; to t on the post side), then the synapse's own statements."""
-        pre = self._event_driven(proj, "j", "t-1")
-        for v in proj.desc["pre_spike"]:
-            code = self.fill(v["cpp"], local="[j]")
-            if v["name"] == "w" and proj.desc["plasticity"]:
-                code = f"if (anb_plastic) {{ {code} }}"
-            pre.append(self.typed(code))
-        post = self._event_driven(proj, "j", "t")
-        for v in proj.desc["post_spike"]:
-            code = self.fill(v["cpp"], local="[j]")
-            if v["name"] == "w":
-                code = f"if (anb_plastic) {{ {code} }}"
-            post.append(self.typed(code))
+        pre = self._event_driven(proj, "j", "t-1") + self.syn_spike_statements(proj, "pre_spike")
+        post = self._event_driven(proj, "j", "t") + self.syn_spike_statements(proj, "post_spike")
         return "\n          ".join(pre), "\n          ".join(post)
 
     def fused_stdp_functions(self, proj) -> str:
@@ -1090,7 +1159,7 @@ __device__ __forceinline__ void proj{k}_psp_fused_body(const long long anb_pt, c
         const int j = {p('inv_idx')}[anb_k];
         const int anb_post = {p('post_idx')}[anb_k];
         float sum = 0.f;
-        {load}
+        {self.syn_index_defs(pre_stmts + post_stmts, "anb_pre", "anb_post")}{load}
         if (anb_fused && anb_bit({post_bits}, anb_post)) {{
           const long long t = anb_pt - 1;
           {self._pack_fields(proj, post_stmts)}
@@ -1109,13 +1178,14 @@ __device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt) {
     const long long anb_items = (long long){self.ptr(f'pop{b}__spn')}[t & 1] * {pch};
     for (long long anb_it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_it < anb_items;
          anb_it += (gridDim.x * blockDim.x) >> 5) {{
-      const int anb_row = {p('row_of')}[anb_list[anb_it / {pch}]];
+      const int anb_spiker = anb_list[anb_it / {pch}];
+      const int anb_row = {p('row_of')}[anb_spiker];
       if (anb_row < 0) continue;
       const int anb_c = (int)(anb_it % {pch});
       const int anb_end = {p('row_ptr')}[anb_row + 1];
       for (int j = {p('row_ptr')}[anb_row] + anb_c * 32 + anb_lane; j < anb_end; j += 32 * {pch}) {{
         if (anb_bit({pre_bits}, {p('col')}[j])) continue;   // done with the transmission
-        {self._pack_body(proj, post_stmts)}
+        {self.syn_index_defs(post_stmts, f"{p('col')}[j]", "anb_spiker")}{self._pack_body(proj, post_stmts)}
       }}
     }}
 }}
@@ -1130,24 +1200,79 @@ __device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt) {
             fields += "".join(f" int anb_pad{i};" for i in range(pad))
             self.types[f"anb_tr{proj.id}"] = (f"struct __align__({min(nbytes, 16)}) anb_tr{proj.id} "
                                               f"{{ {fields} }};\n")
-            return (f"anb_tr{proj.id}* __restrict__ anb_tr = "
-                    f"reinterpret_cast<anb_tr{proj.id}*>({self.ptr(f'proj{proj.id}__tr')});")
-        names = ["w"] + [v["name"] for v in proj.desc["variables"]
-                         if v["locality"] == "local" and v["name"] != "w"]
-        for v in proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", []):
-            if v["name"] not in names and v["name"] != "g_target":
-                names.append(v["name"])
+            return "\n    ".join(
+                [f"anb_tr{proj.id}* __restrict__ anb_tr = "
+                 f"reinterpret_cast<anb_tr{proj.id}*>({self.ptr(f'proj{proj.id}__tr')});"]
+                + self._syn_neuron_refs(proj))
         decl = []
-        for n in names:
+        for n in syn_local_names(proj):
             decl.append(f"{self.real}* __restrict__ {n} = {self.ptr(f'proj{proj.id}__{n}')};")
         decl.append(f"long long* __restrict__ _last_event = {self.ptr(f'proj{proj.id}___last_event')};")
-        return "\n    ".join(decl)
+        return "\n    ".join(decl + self._syn_neuron_refs(proj))
+
+    def syn_fill(self, code: str, idx: str = "j") -> str:
+        """A per-synapse statement: synapse arrays at [idx], the pre- and
+        post-synaptic neurons' attributes (pre.x, post.x, t_pre, t_post) at
+        [anb_pi] and [anb_qi], which every kernel running these statements
+        defines for its synapse (syn_index_defs)."""
+        return self.fill(code, local=f"[{idx}]", pre_prefix="anb_pre_", pre_index="[anb_pi]",
+                         post_prefix="anb_post_", post_index="[anb_qi]")
+
+    def syn_spike_statements(self, proj, which: str) -> list:
+        """The pre_spike or post_spike statements of a spiking projection for
+        synapse j, each followed by its bounds (`w -= 1.0 : min=0.0`), the
+        weight's only while plasticity is on."""
+        out = []
+        for v in proj.desc[which]:
+            code = self.syn_fill(v["cpp"])
+            if v["name"] != "g_target":
+                idx = "[j]" if v["locality"] == "local" else "[0]"
+                for b, val in v.get("bounds", {}).items():
+                    if b in ("min", "max"):
+                        op = "<" if b == "min" else ">"
+                        val = self.syn_fill(str(val))
+                        code += f" if ({v['name']}{idx} {op} {val}) {v['name']}{idx} = {val};"
+            if v["name"] == "w" and (which == "post_spike" or proj.desc["plasticity"]):
+                code = f"if (anb_plastic) {{ {code} }}"
+            out.append(self.typed(code))
+        return out
+
+    def _syn_neuron_refs(self, proj) -> list:
+        """Pointers to the pre/post population arrays the projection's
+        per-synapse statements read (last_spike for t_pre / t_post)."""
+        code = " ".join(v.get("cpp", "") or "" for v in
+                        proj.desc.get("pre_spike", []) + proj.desc.get("post_spike", [])
+                        + [v for v in proj.desc["variables"] if v.get("method") == "event-driven"])
+        code = self.syn_fill(code) if code.strip() else ""
+        decl = []
+        for prefix, pop in (("anb_pre_", proj.pre_pop), ("anb_post_", proj.post_pop)):
+            for n in sorted(set(re.findall(prefix + r"(\w+)\[", code))):
+                if n == "last_spike":
+                    ct = "long long"
+                elif n in pop._host:
+                    ct = "int" if pop._ctype.get(n) in ("int", "bool") else self.real
+                else:
+                    raise NotImplementedError(f"{proj.name}: {prefix[4:-1]}.{n} is not an attribute "
+                                              f"of {pop.name}")
+                decl.append(f"const {ct}* __restrict__ {prefix}{n} = {self.ptr(f'pop{pop.id}__{n}')};")
+        return decl
+
+    @staticmethod
+    def syn_index_defs(body: str, pre: str, post: str) -> str:
+        """Definitions of anb_pi / anb_qi (pre and post neuron of the synapse)
+        for a body that uses them."""
+        out = ""
+        if "anb_pi]" in body:
+            out += f"const int anb_pi = {pre};\n          "
+        if "anb_qi]" in body:
+            out += f"const int anb_qi = {post};\n          "
+        return out
 
     def _event_driven(self, proj, idx, t_expr):
         out = []
         for v in proj.desc["variables"]:
             if v.get("method") == "event-driven":
-                code = self.fill(v["cpp"], local=f"[{idx}]")
+                code = self.syn_fill(v["cpp"], idx)
                 out.append(self.typed(code.replace("(t))", f"({t_expr}))")))
         out.append(f"_last_event[{idx}] = t;")
         return out
@@ -1155,12 +1280,7 @@ __device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt) {
     def plastic_psp_kernel(self, proj, lay, pre_spk, g) -> str:
         k = proj.id
         p = lambda n: self.ptr(f"proj{k}__{n}")
-        stmts = self._event_driven(proj, "j", "t-1")
-        for v in proj.desc["pre_spike"]:
-            code = self.fill(v["cpp"], local="[j]")
-            if v["name"] == "w" and proj.desc["plasticity"]:
-                code = f"if (anb_plastic) {{ {code} }}"
-            stmts.append(self.typed(code))
+        stmts = self._event_driven(proj, "j", "t-1") + self.syn_spike_statements(proj, "pre_spike")
         body = self._pack_body(proj, "\n          ".join(stmts))
         if self.exact or self.delayed(proj) or not self.c.spike_lists:
             # warp per post row; the spiking synapses of a row are processed in
@@ -1191,7 +1311,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
           const int anb_b = __ffs(anb_m) - 1;
           anb_m &= anb_m - 1;
           if (anb_lane == anb_b) {{
-            {body}
+            {self.syn_index_defs(body, f"{p('col')}[j]", "anb_post")}{body}
           }}
           sum = __shfl_sync(0xffffffffu, sum, anb_b);
         }}
@@ -1224,7 +1344,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
            anb_k += 32 * {lay['chunks']}) {{
         const int j = {p('inv_idx')}[anb_k];
         float sum = 0.f;
-        {body}
+        {self.syn_index_defs(body, "anb_pre", f"{p('post_idx')}[anb_k]")}{body}
         atomicAdd(&{g}[{p('post_idx')}[anb_k]], sum);
       }}
     }}
@@ -1236,12 +1356,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
         lay = self.c.layout[proj.id]
         p = lambda n: self.ptr(f"proj{k}__{n}")
         post_spk = self.spk_at(proj.post_pop, "t")
-        stmts = self._event_driven(proj, "j", "t")
-        for v in proj.desc["post_spike"]:
-            code = self.fill(v["cpp"], local="[j]")
-            if v["name"] == "w":
-                code = f"if (anb_plastic) {{ {code} }}"
-            stmts.append(self.typed(code))
+        stmts = self._event_driven(proj, "j", "t") + self.syn_spike_statements(proj, "post_spike")
         body = self._pack_body(proj, "\n        ".join(stmts))
         dt_t = "double" if self.exact else "float"
         if not self.exact and self.c.spike_lists:
@@ -1259,12 +1374,13 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
     const long long anb_items = (long long){self.ptr(f'pop{b}__spn')}[t & 1] * {ch};
     for (long long anb_it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; anb_it < anb_items;
          anb_it += (gridDim.x * blockDim.x) >> 5) {{
-      const int anb_row = {p('row_of')}[anb_list[anb_it / {ch}]];
+      const int anb_spiker = anb_list[anb_it / {ch}];
+      const int anb_row = {p('row_of')}[anb_spiker];
       if (anb_row < 0) continue;
       const int anb_c = (int)(anb_it % {ch});
       const int anb_end = {p('row_ptr')}[anb_row + 1];
       for (int j = {p('row_ptr')}[anb_row] + anb_c * 32 + anb_lane; j < anb_end; j += 32 * {ch}) {{
-        {body}
+        {self.syn_index_defs(body, f"{p('col')}[j]", "anb_spiker")}{body}
       }}
     }}
 }}
@@ -1282,21 +1398,39 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
       const int anb_post = {p('post_rank')}[anb_row];
       if (!anb_bit({post_spk}, anb_post)) continue;           // warp-uniform
       for (int j = {p('row_ptr')}[anb_row] + anb_lane; j < {p('row_ptr')}[anb_row + 1]; j += 32) {{
-        {body}
+        {self.syn_index_defs(body, f"{p('col')}[j]", "anb_post")}{body}
       }}
     }}
 }}
 """
 
     # --------------------------------------------------------------- monitors
-    def monitor_kernel(self, mon) -> str:
-        """Variable recording of one monitor (grid engine). Spike bitmaps are
-        written by the update kernel of the population."""
+    @staticmethod
+    def target_variables(mon) -> list:
+        """The conductances g_<target> a monitor of a spiking population
+        records: the reference records them right after the step's
+        transmissions, before the neurons' update (record_targets,
+        ANNarchy/generator/Template/OpenMPBaseTemplate.py:236-242 and
+        Monitor/MonitorGenerator.py:112-156); every other variable after the
+        update."""
+        pop = mon.population
+        if pop.neuron_type.type != "spike":
+            return []
+        names = {"g_" + t for t in pop.targets}
+        return [v for v in mon.variables if v in names]
+
+    def monitor_kernel(self, mon, targets: bool = False) -> str:
+        """Variable recording of one monitor (grid engine): the conductances
+        of the step's transmissions (`targets`, kernel mon<m>_record_targets,
+        launched before the updates) or the other variables (mon<m>_record,
+        after them). Spike bitmaps are written by the update kernel of the
+        population."""
         m = mon.id
         lay = self.c.mon_layout[m]
+        tv = self.target_variables(mon)
         parts = []
         for var in mon.variables:
-            if var == "spike":
+            if var == "spike" or (var in tv) != targets:
                 continue
             src = self.ptr(f"pop{mon.population.id}__{source_name(var)}")
             ranks = self.ptr(f"mon{m}__ranks") if mon.ranks is not None else "nullptr"
@@ -1309,7 +1443,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_post_event() {{
         anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
     }}""")
         return f"""
-extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
+extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record{'_targets' if targets else ''}() {{
     const long long t = *{self.ptr('t')};
     const int anb_on = {self.ptr(f'mon{m}__on')}[0];
     {''.join(parts)}
@@ -1329,7 +1463,8 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record() {{
         if any(p.synapse_type.type != "spike" for p in net.projections):
             return False
         if any(getattr(p, "stop_condition", None) or hasattr(p, "_ta_schedule_ms")
-               or p.neuron_type.type != "spike" or self.slots(p) > 1 for p in net.populations):
+               or p.neuron_type.type != "spike" or self.slots(p) > 1 or global_equations(p)
+               for p in net.populations):
             return False
         return True
 
@@ -1426,6 +1561,12 @@ extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run
                 # (one graph branch each); the gathers write g[post] in place
                 group = 1 if self.atomic_psp(proj) else 0
                 plan.append((f"proj{proj.id}_psp", lay["grid"], BLOCK, 0, group))
+        for mon in net.monitors:
+            if self.target_variables(mon):
+                # the conductances after the transmissions, before the updates
+                kernels.append(self.monitor_kernel(mon, targets=True))
+                n = self.c.mon_layout[mon.id]["n"]
+                plan.append((f"mon{mon.id}_record_targets", grid_for(max(n, 32)), BLOCK, 0))
         for pop in net.populations:
             if hasattr(pop, "_ta_schedule_ms"):
                 kernels.append(self.timed_array_kernel(pop))
@@ -1454,7 +1595,8 @@ extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run
                         if (self.c.spike_lists and not self.exact) else grid_for(lay["rows"] * 32))
                 plan.append((f"proj{proj.id}_post_event", grid, BLOCK, 0))
         for mon in net.monitors:
-            if any(v != "spike" for v in mon.variables):
+            tv = self.target_variables(mon)
+            if any(v != "spike" and v not in tv for v in mon.variables):
                 # spikes are written by the update kernel of the population
                 kernels.append(self.monitor_kernel(mon))
                 n = self.c.mon_layout[mon.id]["n"]

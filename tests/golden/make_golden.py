@@ -454,6 +454,59 @@ def case_self_connections(name):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+# Tsodyks-Markram short-term plasticity written out as a synapse description
+# (the same text is used by the tests): event-driven recovery x and
+# facilitation u, both updated at each pre-synaptic spike
+STP_PARAMETERS = """
+    tau_rec = 200.0 : projection
+    tau_facil = 50.0 : projection
+    U = 0.2
+"""
+STP_EQUATIONS = """
+    dx/dt = (1 - x)/tau_rec : init = 1.0, event-driven
+    du/dt = (U - u)/tau_facil : init = 0.2, event-driven
+"""
+STP_PRE_SPIKE = """
+    g_target += w * u * x
+    x *= (1 - u)
+    u += U * (1 - u)
+"""
+
+
+def case_stp(name, seed, n, p, steps, g_every):
+    """The COBA network with its excitatory projection through short-term
+    plasticity: raster, final state, the per-synapse x and u, and g_exc
+    recorded every g_every steps (the reference records conductances right
+    after the transmissions, before the neurons' update)."""
+    import numpy as np
+    import ANNarchy as ann
+    from annarchy_b200 import workloads as wl
+    cn = wl.coba_net(seed=seed, n=n, p=p, steps=steps)
+    net = ann.Network(dt=cn.dt, seed=seed)
+    net.config(num_threads=1)
+    P = net.create(n, _coba_neuron(ann, cn.params))
+    Pe, Pi = P[: cn.n_exc], P[cn.n_exc:]
+    stp = ann.Synapse(parameters=STP_PARAMETERS, equations=STP_EQUATIONS, pre_spike=STP_PRE_SPIKE)
+    ce = net.connect(Pe, P, "exc", synapse=stp)
+    ce.from_sparse(wl.to_from_sparse(cn.w_exc), storage_format="csr")
+    ci = net.connect(Pi, P, "inh")
+    ci.from_sparse(wl.to_from_sparse(cn.w_inh), storage_format="csr")
+    m = net.monitor(P, ["spike"])
+    mg = net.monitor(P, ["g_exc"], period=g_every * cn.dt)
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    P.v = cn.v0
+    net.simulate(steps * cn.dt)
+    s_steps, s_idx = _spikes_to_arrays(m.get("spike"))
+    out = dict(seed=seed, n=n, p=p, steps=steps, g_every=g_every,
+               digest_exc=wl.csr_digest(cn.w_exc), digest_inh=wl.csr_digest(cn.w_inh),
+               spike_steps=s_steps, spike_idx=s_idx, v_final=np.asarray(P.v),
+               g_exc_final=np.asarray(P.g_exc), g_inh_final=np.asarray(P.g_inh),
+               g_exc_trace=np.asarray(mg.get("g_exc")),
+               x_final=np.concatenate([np.asarray(d, dtype=np.float64) for d in ce.x]),
+               u_final=np.concatenate([np.asarray(d, dtype=np.float64) for d in ce.u]))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -469,6 +522,7 @@ CASES = {
     "rate_learning": (case_rate_learning, {}),
     "connectivity_file": (case_connectivity_file, {}),
     "self_connections": (case_self_connections, {}),
+    "stp_small": (case_stp, dict(seed=5, n=400, p=0.05, steps=2000, g_every=50)),
 }
 
 

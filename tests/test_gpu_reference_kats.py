@@ -1,0 +1,231 @@
+"""Known-answer cases of the reference's own test suite, run through this
+backend on the GPU with the values those tests expect:
+
+* spike transmission without delay, with a uniform and with per-synapse
+  delays (ANNarchy tests_python/SpikeSynapse/test_SpikingTransmission.py:
+  74-84, 154-175, 240-253): five pre-synaptic neurons spiking at t = 1 ms,
+  all-to-all onto two neurons whose g_exc is reset by their equation;
+* the spike condition, reset and refractory period
+  (tests_python/Neuron/test_SpikingNeuron.py:73-128);
+* local, global and mixed neuron updates and bounds
+  (tests_python/Neuron/test_NeuronUpdate.py:81-115);
+* pre- and post-spike weight updates with bounds
+  (tests_python/SpikeSynapse/test_SpikingSynapse.py:60-137) and the
+  time-dependent rule's compilation (:140-195);
+* rate-coded connectivity patterns (tests_python/RateSynapse/
+  test_RateTransmission.py:79-131).
+
+Every case runs in double (the reference's arithmetic) and in float
+precision; the expected values are small integers or tenths, exact in
+both."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from annarchy_b200 import Network, Neuron, Synapse, Uniform
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = ("double", "float")
+
+
+def _transmission_net(precision, connect):
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    emit = Neuron(spike="t==1")
+    recv = Neuron(equations="g_exc = 0", spike="g_exc>30")
+    pre = net.create(5, emit)
+    post = net.create(2, recv)
+    connect(net.connect(pre, post, "exc"))
+    mon = net.monitor(post, ["g_exc"])
+    net.compile()
+    return net, mon
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_spike_transmission_no_delay(precision):
+    net, mon = _transmission_net(precision, lambda p: p.all_to_all(weights=1.0))
+    net.simulate(5)
+    np.testing.assert_array_equal(mon.get("g_exc"),
+                                  [[0, 0], [0, 0], [5, 5], [0, 0], [0, 0]])
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_spike_transmission_uniform_delay(precision):
+    net, mon = _transmission_net(precision, lambda p: p.all_to_all(weights=1.0, delays=3.0))
+    net.simulate(6)
+    np.testing.assert_array_equal(mon.get("g_exc"),
+                                  [[0, 0], [0, 0], [0, 0], [0, 0], [5, 5], [0, 0]])
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_spike_transmission_nonuniform_delay(precision):
+    # delays per post neuron over the five pre neurons, as the reference's
+    # test sets them: post 0 gets 2 events at t = 2, 2 at t = 3, 1 at t = 4;
+    # post 1 gets 1, 2 and 2
+    d = np.array([[1.0, 2.0, 3.0, 2.0, 1.0], [3.0, 2.0, 1.0, 2.0, 3.0]])    # (post, pre)
+    w = sp.csr_matrix(np.ones((5, 2)))                                        # (pre, post)
+    net, mon = _transmission_net(
+        precision, lambda p: p.from_sparse(w, delays=sp.csr_matrix(d.T)))
+    net.simulate(5)
+    np.testing.assert_array_equal(mon.get("g_exc"),
+                                  [[0, 0], [0, 0], [2, 1], [2, 2], [1, 2]])
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_spike_condition_reset_refractory(precision):
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    plain = net.create(3, Neuron(equations="v = v + 1.0", spike="v == 3.0", reset="v = 1.0"))
+    refr = net.create(3, Neuron(parameters="Vt = 3.0", equations="v = v + 1.0",
+                                spike="v == Vt", reset="v = 1.0 ", refractory=3.0))
+    glob = net.create(3, Neuron(parameters="Vt = 3.0 : population", equations="v = v + 1.0",
+                                spike="v == Vt", reset="v = 1.0 "))
+    net.compile()
+    seen = {id(p): [float(np.asarray(p.v)[0])] for p in (plain, refr, glob)}
+    for _ in range(7):
+        net.simulate(1)
+        for p in (plain, refr, glob):
+            seen[id(p)].append(float(np.asarray(p.v)[0]))
+    assert seen[id(plain)][:6] == [0, 1, 2, 1, 2, 1]
+    assert seen[id(refr)] == [0, 1, 2, 1, 1, 1, 1, 2]
+    assert seen[id(glob)][:6] == [0, 1, 2, 1, 2, 1]
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_neuron_update_local_global_mixed_bounds(precision):
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    local = net.create(3, Neuron(equations="""
+        noise = Uniform(0,1)
+        r = t
+    """))
+    glob = net.create(3, Neuron(equations="""
+        noise = Uniform(0,1) : population
+        glob_r = t : population
+        r = t
+    """))
+    mixed = net.create(3, Neuron(parameters="glob_par = 1.0: population",
+                                 equations="r = t + glob_par"))
+    bound = net.create(3, Neuron(parameters="""
+        min_r=1.0: population
+        max_r=3.0: population
+    """, equations="r = t : min=min_r, max=max_r"))
+    mon = net.monitor(bound, "r")
+    net.compile()
+    net.simulate(5)
+    np.testing.assert_array_equal(np.asarray(local.r), [4.0, 4.0, 4.0])
+    np.testing.assert_array_equal(np.ravel(glob.glob_r), [4.0])
+    np.testing.assert_array_equal(np.asarray(mixed.r), [5.0, 5.0, 5.0])
+    np.testing.assert_array_equal(mon.get("r")[:, 0], [1, 1, 2, 3, 3])
+    net.close()
+
+
+def _every_step_spiking(net):
+    return net.create(3, Neuron(parameters="v = 1", equations="mp = g_exc", spike="v > 0"))
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_pre_spike_weight_update_with_bound(precision):
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    pop = _every_step_spiking(net)
+    syn = Synapse(parameters="g = 1.0", pre_spike="w -= 1.0 : min=0.0")
+    proj = net.connect(pop, pop, "exc", synapse=syn)
+    proj.all_to_all(5.0)
+    net.compile()
+    np.testing.assert_array_equal(proj.dendrite(0).w, [5.0, 5.0])
+    net.simulate(5)
+    np.testing.assert_array_equal(proj.dendrite(0).w, [1.0, 1.0])
+    net.simulate(5)
+    np.testing.assert_array_equal(proj.dendrite(0).w, [0.0, 0.0])
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_post_spike_weight_update_with_bound(precision):
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    pop = _every_step_spiking(net)
+    syn = Synapse(parameters="constant = 1.0", post_spike="w += 1.0 * constant : max=10.0")
+    proj = net.connect(pop, pop, "exc", synapse=syn)
+    proj.all_to_all(5.0)
+    net.compile()
+    np.testing.assert_array_equal(proj.dendrite(0).w, [5.0, 5.0])
+    net.simulate(5)
+    np.testing.assert_array_equal(proj.dendrite(0).w, [10.0, 10.0])
+    net.simulate(5)
+    np.testing.assert_array_equal(proj.dendrite(0).w, [10.0, 10.0])
+    net.close()
+
+
+def test_time_dependent_rule_compiles_and_runs():
+    # Izhikevich's (2003) regular-spiking neuron with a constant drive
+    izhikevich = Neuron(
+        parameters="""
+            a = 0.02
+            b = 0.2
+            c = -65.0
+            d = 8.0
+            I = 10.0
+        """,
+        equations="""
+            dv/dt = 0.04 * v^2 + 5.0 * v + 140.0 - u + I + g_exc : init = -65.0
+            du/dt = a * (b * v - u) : init = -13.0
+        """,
+        spike="v >= 30.0",
+        reset="""
+            v = c
+            u += d
+        """)
+    stdp = Synapse(
+        parameters="""
+            tau_pre = 10.0 : projection
+            tau_post = 10.0 : projection
+            cApre = 0.01 : projection
+            cApost = 0.0105 : projection
+            wmax = 0.01 : projection
+        """,
+        pre_spike="""
+            g_target += w
+            w = clip(w - cApost * exp((t_post - t)/tau_post) , 0.0 , wmax)
+        """,
+        post_spike="""
+            w = clip(w + cApre * exp((t_pre - t)/tau_pre) , 0.0 , wmax)
+        """)
+    net = Network(dt=1.0, seed=1)
+    pop = net.create(100, izhikevich)
+    net.connect(pop, pop, "exc", stdp).all_to_all(Uniform(-1.0, 1.0))
+    net.compile()
+    net.simulate(10)
+    assert net._backend.native.device_error() == 0
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_rate_transmission_patterns(precision):
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    pop1 = net.create((3, 3), Neuron(equations="r = 1"))
+    pop2 = net.create((3, 3), Neuron(equations="r = sum(exc)"))
+    one = net.connect(pop1, pop2, "exc")
+    one.one_to_one(weights=0.1)
+    a2a = net.connect(pop1, pop2, "exc")
+    a2a.all_to_all(weights=0.1)
+    fnp = net.connect(pop1, pop2, "exc")
+    fnp.fixed_number_pre(3, weights=0.1)
+    net.compile()
+    assert list(one.dendrite(3).pre_ranks) == [3]
+    np.testing.assert_allclose(one.dendrite(3).w, [0.1])
+    assert list(a2a.dendrite(3).pre_ranks) == list(range(9))
+    np.testing.assert_allclose(a2a.dendrite(3).w, np.ones(9) * 0.1)
+    assert [d.size for d in fnp.dendrites] == [3] * 9
+    # after one step every post neuron sums 1 (one-to-one) + 9 + 3 rates of
+    # 1.0 weighted by 0.1 (the rates of step 0 are the initial 0.0)
+    net.simulate(2)
+    np.testing.assert_allclose(np.ravel(pop2.r), 1.3, rtol=1e-6)
+    net.close()

@@ -56,7 +56,7 @@ def test_dendrites_and_synapses():
     syn.w = 5.0
     assert p.connectivity_matrix()[2, d.pre_ranks[1]] == 5.0
     assert p.synapse(int(np.nonzero(m[2] == 0)[0][0]), 2) is None
-    assert [x.post_rank for x in p.dendrites()] == p.post_ranks
+    assert [x.post_rank for x in p.dendrites] == p.post_ranks
     rf = d.receptive_field()
     assert rf.shape == (3, 5) and rf.ravel()[d.pre_ranks[0]] == d.w[0]
 
