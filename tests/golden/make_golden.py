@@ -454,25 +454,6 @@ def case_self_connections(name):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
-# Tsodyks-Markram short-term plasticity written out as a synapse description
-# (the same text is used by the tests): event-driven recovery x and
-# facilitation u, both updated at each pre-synaptic spike
-STP_PARAMETERS = """
-    tau_rec = 200.0 : projection
-    tau_facil = 50.0 : projection
-    U = 0.2
-"""
-STP_EQUATIONS = """
-    dx/dt = (1 - x)/tau_rec : init = 1.0, event-driven
-    du/dt = (U - u)/tau_facil : init = 0.2, event-driven
-"""
-STP_PRE_SPIKE = """
-    g_target += w * u * x
-    x *= (1 - u)
-    u += U * (1 - u)
-"""
-
-
 def case_stp(name, seed, n, p, steps, g_every):
     """The COBA network with its excitatory projection through short-term
     plasticity: raster, final state, the per-synapse x and u, and g_exc
@@ -481,6 +462,7 @@ def case_stp(name, seed, n, p, steps, g_every):
     import numpy as np
     import ANNarchy as ann
     from annarchy_b200 import workloads as wl
+    from stp_model import STP_EQUATIONS, STP_PARAMETERS, STP_PRE_SPIKE
     cn = wl.coba_net(seed=seed, n=n, p=p, steps=steps)
     net = ann.Network(dt=cn.dt, seed=seed)
     net.config(num_threads=1)
