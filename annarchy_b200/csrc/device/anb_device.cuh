@@ -32,10 +32,24 @@ typedef long long anb_i64;
 // (names as emitted by the reference parser: ANNarchy/parser/ParserTemplate.py)
 template <typename T> __device__ __forceinline__ T positive(T x) { return x > T(0) ? x : T(0); }
 template <typename T> __device__ __forceinline__ T negative(T x) { return x < T(0) ? x : T(0); }
-__device__ __forceinline__ double modulo(double a, double b) { return fmod(a, b); }
-__device__ __forceinline__ int modulo(int a, int b) { return a % b; }
-__device__ __forceinline__ double power(double a, double b) { return pow(a, b); }
-__device__ __forceinline__ float power(float a, float b) { return powf(a, b); }
+// modulo(a, b): the integer remainder of a and b truncated to 64-bit
+// integers (the reference's `long(a) % long(b)`)
+template <typename A, typename B>
+__device__ __forceinline__ long long modulo(A a, B b) { return (long long)a % (long long)b; }
+// power(x, a): x multiplied by itself, a converted to an unsigned integer
+// exponent (the reference's integer power, a - 1 multiplications in order);
+// an exponent of 0 gives x
+__device__ __forceinline__ double power(double x, unsigned int a) {
+  double r = x;
+  for (unsigned int i = 1; i < a; ++i) r *= x;
+  return r;
+}
+__device__ __forceinline__ float power(float x, unsigned int a) {
+  float r = x;
+  for (unsigned int i = 1; i < a; ++i) r *= x;
+  return r;
+}
+__device__ __forceinline__ double power(int x, unsigned int a) { return power((double)x, a); }
 #define clip(x, a, b) ((x) < (a) ? (a) : ((x) > (b) ? (b) : (x)))
 
 // ---- bfloat16 ---------------------------------------------------------------

@@ -229,3 +229,46 @@ def test_rate_transmission_patterns(precision):
     net.simulate(2)
     np.testing.assert_allclose(np.ravel(pop2.r), 1.3, rtol=1e-6)
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_builtin_functions(precision):
+    """modulo, power and clip (tests_python/Common/test_BuiltinFunctions.py:
+    52-104)."""
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    pop = net.create(1, Neuron(parameters="base = 2.0", equations="""
+        r = modulo(t,3)
+        pr = power(base,3)
+        clip_below = clip(-2, -1, 1)
+        clip_within = clip(0, -1, 1)
+        clip_above = clip(2, -1, 1)
+    """))
+    mon = net.monitor(pop, ["r", "pr", "clip_below", "clip_within", "clip_above"])
+    net.compile()
+    net.simulate(10)
+    got = mon.get()
+    np.testing.assert_array_equal(got["r"][:, 0], [0, 1, 2, 0, 1, 2, 0, 1, 2, 0])
+    np.testing.assert_array_equal(got["pr"][:, 0], [8.0] * 10)
+    np.testing.assert_array_equal(got["clip_below"][:, 0], [-1.0] * 10)
+    np.testing.assert_array_equal(got["clip_within"][:, 0], [0.0] * 10)
+    np.testing.assert_array_equal(got["clip_above"][:, 0], [1.0] * 10)
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_neuron_random_variables(precision):
+    """A local Uniform(0, 1) draws a different value per neuron, a
+    population-level one a single value (tests_python/Common/
+    test_RandomVariables.py:47-70)."""
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    loc = net.create(3, Neuron(equations="r = Uniform(0,1)"))
+    glob = net.create(3, Neuron(parameters="", equations="r = Uniform(0,1) : population"))
+    net.compile()
+    net.simulate(1)
+    r = np.asarray(loc.r)
+    assert np.all((r >= 0.0) & (r <= 1.0)) and not np.allclose(r, 0.0) and r.max() != r.min()
+    g = np.ravel(glob.r)
+    assert g.size == 1 and 0.0 < g[0] <= 1.0
+    net.close()

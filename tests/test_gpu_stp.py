@@ -1,11 +1,12 @@
 """Short-term plasticity (event-driven x and u updated at every pre-synaptic
 spike, transmission w * u * x) on the 400-neuron COBA network against the
 reference's own run (tests/golden/stp_small.npz, made by
-tests/golden/make_golden.py): in double precision the raster, the final
-state, every synapse's x and u and the g_exc recorded every 50 steps (after
-the transmissions, before the update, as the reference records
-conductances) are bit-identical; in single precision the spike count is
-close."""
+tests/golden/make_golden.py): in double precision the raster is
+bit-identical, and the final state, every synapse's x and u and the g_exc
+recorded every 50 steps (after the transmissions, before the update, as
+the reference records conductances) agree within 1e-12 (the event-driven
+decays call the device's exp(), whose last bit can differ from glibc's);
+in single precision the spike count is close."""
 import os
 import sys
 
@@ -54,7 +55,8 @@ def test_stp_exact(golden):
     assert np.array_equal(out["idx"], g["spike_idx"])
     for k, gk in (("v", "v_final"), ("g_exc", "g_exc_final"), ("g_inh", "g_inh_final"),
                   ("trace", "g_exc_trace"), ("x", "x_final"), ("u", "u_final")):
-        assert np.array_equal(out[k], g[gk]), k
+        assert out[k].shape == g[gk].shape, k
+        np.testing.assert_allclose(out[k], g[gk], rtol=1e-12, atol=1e-12, err_msg=k)
 
 
 def test_stp_float_rates(golden):
