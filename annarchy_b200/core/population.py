@@ -53,6 +53,16 @@ class Population:
         self._has_refractory = bool(refr)
         object.__setattr__(self, "_ready", True)
 
+    def _add_rate_target(self, target: str):
+        """A projection's target that the neuron's equations do not use: its
+        weighted sum array (zero until compile)."""
+        if target in self.targets:
+            return
+        self.targets.append(target)
+        self._host["_sum_" + target] = np.zeros(self.size)
+        self._locality["_sum_" + target] = "local"
+        self._ctype["_sum_" + target] = "double"
+
     # -- helpers --------------------------------------------------------------
     def _initial(self, p):
         init = p["init"]

@@ -59,6 +59,11 @@ class Projection:
             raise TypeError("a spiking synapse needs a spiking pre-synaptic population")
         if synapse.type == "rate" and pre_type != "rate":
             raise TypeError("a rate-coded synapse needs a rate-coded pre-synaptic population")
+        if self.post_pop.neuron_type.type == "rate" and target not in self.post_pop.targets:
+            # a rate-coded target the neuron does not sum: its weighted sum is
+            # still computed (ANNarchy/core/Projection.py:105-110 adds the
+            # target to the population's)
+            self.post_pop._add_rate_target(target)
         if self.post_pop.neuron_type.type == "spike" and synapse.type == "spike":
             if target not in self.post_pop.targets:
                 # a conductance the neuron only assigns (`g_exc = 0`) is not

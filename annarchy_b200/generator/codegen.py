@@ -773,11 +773,17 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
         lay = self.c.layout[k]
         desc = proj.desc
         for v in desc["variables"]:
-            if v.get("cpp") and v.get("method") not in ("explicit", "event-driven", None) \
-                    and v.get("switch"):
+            if v.get("cpp") and v.get("method") not in ("explicit", "exponential", "event-driven",
+                                                        None) and v.get("switch"):
                 raise NotImplementedError(f"{proj.name}: synaptic variable {v['name']!r} uses the "
                                           f"{v['method']!r} method; rate-coded synapses support "
-                                          "explicit Euler in this backend")
+                                          "explicit and exponential Euler in this backend")
+        # constants of the exponential method (the step's decay factor over
+        # the update period, the reference's __stepsize_<x>)
+        pre_loop = "\n    ".join(
+            self.typed("const double " + v["pre_loop"]["name"] + " = " + re.sub(
+                r"(?<![\w.])dt(?!\w)", "anb_dt", self.fill(v["pre_loop"]["value"])) + ";")
+            for v in desc["variables"] if v.get("pre_loop"))
         p = lambda n: self.ptr(f"proj{k}__{n}")
         dt_t = "double" if self.exact else "float"
         # no early return: the step counter's epilogue may follow these kernels
@@ -812,6 +818,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
 extern "C" __global__ void __launch_bounds__(32) proj{k}_update_global() {{
 {head}    if (anb_go && threadIdx.x == 0) {{
     {loads}
+    {pre_loop}
     {refs(code)}
     {code}
     {stores}
@@ -827,6 +834,8 @@ extern "C" __global__ void __launch_bounds__(32) proj{k}_update_global() {{
         if not (semi_eq.strip() or loc_eq.strip()):
             return out
         gvals = "\n    ".join(f"const {self.real} {q['name']} = {p(q['name'])}[0];" for q in glob_all)
+        if pre_loop:
+            gvals += "\n    " + pre_loop
         arrays = []
         for q in desc["variables"] + desc["parameters"]:
             if q["locality"] in ("local", "semiglobal"):

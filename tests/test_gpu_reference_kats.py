@@ -272,3 +272,75 @@ def test_neuron_random_variables(precision):
     g = np.ravel(glob.r)
     assert g.size == 1 and 0.0 < g[0] <= 1.0
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_rate_synapse_localities_psp_access_and_modified_psp(precision):
+    """Synaptic, postsynaptic and projection-level parameters; pre.sum(exc)
+    and post.sum(exc) in a synaptic equation; a modified psp
+    (tests_python/RateSynapse/test_RateSynapse.py:15-150, which only
+    compile them); here also run, with their values checked."""
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    n0 = Neuron(parameters="r = 0")
+    loc = net.connect(net.create(3, n0), net.create(1, n0), "exc", synapse=Synapse(parameters="""
+        a = 0.1
+        b = 0.1 : postsynaptic
+        c = 0.1 : projection
+    """))
+    loc.all_to_all(weights=1.0)
+    summing = Neuron(equations="r = sum(exc)")
+    syn = Synapse(equations="w = pre.sum(exc) + post.sum(exc)")
+    p1, p2 = net.create(1, summing), net.create(1, summing)
+    acc1 = net.connect(p1, p2, "exc", synapse=syn)
+    acc1.all_to_all(weights=1.0, force_multiple_weights=True)
+    net.connect(p2, p1, "exc", synapse=syn).all_to_all(weights=1.0, force_multiple_weights=True)
+    q1, q2 = net.create(1, summing), net.create(1, summing)
+    net.connect(q1, q2, "exc", synapse=Synapse(parameters="reversal = 1.0",
+                                                 psp="w*pos(reversal-pre.r)")).all_to_all(
+        weights=1.0, force_multiple_weights=True)
+    net.compile()
+    net.simulate(3)
+    np.testing.assert_allclose(loc.get("a", flat=True), [0.1] * 3, rtol=1e-7)
+    np.testing.assert_allclose(np.ravel(loc.get("b")), [0.1], rtol=1e-7)
+    np.testing.assert_allclose(loc.get("c"), 0.1, rtol=1e-7)
+    # nothing drives p1 / p2: all sums and weights become and stay 0
+    np.testing.assert_array_equal(acc1.get("w", flat=True), [0.0])
+    # q2 sums w * pos(1 - 0) = 1 from the second step on
+    np.testing.assert_array_equal(np.ravel(q2.r), [1.0])
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_rate_learning_rules_weighted_sums(precision):
+    """Hebbian, Oja and BCM learning projections with learning disabled: the
+    weighted sums of one step with a pre-synaptic rate of 1.0 equal the
+    weights (tests_python/RateSynapse/test_RateDefaultSynapseModels.py:
+    60-90; the three rules are written out here in their textbook form)."""
+    hebb = Synapse(parameters="eta = 0.01 : projection",
+                   equations="dw/dt = eta * pre.r * post.r : min=0.0, explicit")
+    oja = Synapse(parameters="""
+        eta = 0.01 : projection
+        alpha = 1.0 : projection
+    """, equations="dw/dt = eta * ( pre.r * post.r - alpha * post.r^2 * w ) : min=0.0, explicit")
+    bcm = Synapse(parameters="""
+        eta = 0.01 : projection
+        tau = 2000.0 : projection
+    """, equations="""
+        tau * dtheta/dt = post.r^2 - theta : postsynaptic, exponential
+        dw/dt = eta * post.r * (post.r - theta) * pre.r : min=0.0, explicit
+    """)
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    neuron = Neuron(equations="r=sum(Hebb)+sum(Oja)+sum(IBCM)")
+    inp, out = net.create(1, neuron), net.create(1, neuron)
+    for syn, target in ((hebb, "Hebb"), (oja, "Oja"), (bcm, "IBCM")):
+        net.connect(inp, out, target, synapse=syn).all_to_all(weights=0.1,
+                                                             force_multiple_weights=True)
+    net.compile()
+    net.disable_learning()
+    inp.r = 1.0
+    net.simulate(1)
+    for target in ("Hebb", "Oja", "IBCM"):
+        np.testing.assert_allclose(out.sum(target), 0.1, rtol=1e-7)
+    net.close()
