@@ -1007,10 +1007,24 @@ class CompiledNetwork:
         self.native.write(st, np.asarray(arr, dtype=dt.fields[name][0]).view(np.float32))
         self.native.copy_strided(f"proj{k}__tr", off, dt.itemsize, st, 0, 4, nnz)
 
+    def _host_only(self, proj, name) -> bool:
+        """A synaptic attribute no kernel uses (a parameter of a projection
+        without learning or events) has no device array: the host copy is
+        its value."""
+        return (f"proj{proj.id}__{name}" not in self.native.arrays
+                and not isinstance(self.native, DryNative))
+
     def read_projection_attribute(self, proj, name):
         dt = self._trace_dtype(proj)
         if dt is not None and name in dt.names[:-1]:
             return self._field_io(proj, name)
+        if self._host_only(proj, name):
+            if name in proj._host_semi:
+                return proj._host_semi[name].copy()
+            if name in proj._host_attr:
+                return proj._host_attr[name].copy()
+            glob = {p["name"]: p for p in proj.desc["parameters"] + proj.desc["variables"]}
+            return np.array([float(proj._global_values.get(name, glob[name]["init"]))])
         arr = self.native.read(f"proj{proj.id}__{name}")
         if arr.dtype == np.uint16:
             return from_bf16(arr)
@@ -1021,6 +1035,10 @@ class CompiledNetwork:
         tdt = self._trace_dtype(proj)
         if tdt is not None and name in tdt.names[:-1]:
             self._field_io(proj, name, arr)
+            return
+        if self._host_only(proj, name):
+            if name not in proj._host_semi and name not in proj._host_attr:
+                proj._global_values[name] = float(np.asarray(arr).reshape(-1)[0])
             return
         dtype, _ = self.native.arrays[f"proj{k}__{name}"]
         data = to_bf16(arr) if dtype == np.uint16 else np.asarray(arr, dtype=dtype)

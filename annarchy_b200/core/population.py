@@ -278,6 +278,21 @@ class Population:
     def __repr__(self):
         return f"Population({self.name!r}, size={self.size}, {self.neuron_type.type})"
 
+    def neuron(self, *coord) -> "IndividualNeuron":
+        """The neuron of the given rank or coordinates
+        (ANNarchy/core/Population.py:728-757)."""
+        if len(coord) == 1 and isinstance(coord[0], (int, np.integer)):
+            rank = int(coord[0])
+        else:
+            rank = self.rank_from_coordinates(coord[0] if len(coord) == 1 else tuple(coord))
+        if rank is None or not 0 <= rank < self.size:
+            raise IndexError(f"population {self.name!r} has no neuron {coord}")
+        return IndividualNeuron(self, rank)
+
+    def neurons(self):
+        """Every neuron of the population, in rank order."""
+        return (IndividualNeuron(self, r) for r in range(self.size))
+
     # spikes of the last step (spiking populations)
     @property
     def spiked(self):
@@ -326,3 +341,64 @@ class PopulationView:
 
     def __repr__(self):
         return f"PopulationView({self.population.name!r}, size={self.size})"
+
+    def __add__(self, other):
+        """The union of two views (or a view and a neuron) of the same
+        population, in ascending rank (ANNarchy/core/PopulationView.py:
+        320-332)."""
+        return _join(self, other)
+
+
+def _join(a, b):
+    pa = a.population if not isinstance(a, Population) else a
+    pb = b.population if not isinstance(b, Population) else b
+    if pa is not pb:
+        raise ValueError("can only add two PopulationViews of the same population")
+    ranks = lambda x: np.arange(x.size) if isinstance(x, Population) else np.asarray(x.ranks)
+    return PopulationView(pa, np.array(sorted(set(ranks(a).tolist()) | set(ranks(b).tolist()))))
+
+
+class IndividualNeuron:
+    """One neuron of a population: its attributes read and written by rank
+    (ANNarchy/core/Neuron.py:219-300)."""
+
+    def __init__(self, population: Population, rank: int):
+        object.__setattr__(self, "population", population)
+        object.__setattr__(self, "rank", int(rank))
+
+    @property
+    def ranks(self):
+        return np.array([self.rank], dtype=np.int64)
+
+    @property
+    def size(self):
+        return 1
+
+    @property
+    def id(self):
+        return self.population.id
+
+    @property
+    def neuron_type(self):
+        return self.population.neuron_type
+
+    @property
+    def net(self):
+        return self.population.net
+
+    def __getattr__(self, name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        val = self.population.get(name)
+        if np.ndim(val) == 0:
+            return val
+        return np.asarray(val).reshape(-1)[self.rank]
+
+    def __setattr__(self, name, value):
+        self.population._set_ranks(name, np.array([self.rank]), value)
+
+    def __add__(self, other):
+        return _join(self, other)
+
+    def __repr__(self):
+        return f"IndividualNeuron({self.population.name!r}, rank={self.rank})"
