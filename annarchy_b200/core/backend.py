@@ -658,6 +658,15 @@ class CompiledNetwork:
                 nat.create(f"proj{k}__{prm['name']}", np.array([value], dtype=self.real))
         if proj.synapse_type.type == "rate":
             learning = CodeGenerator.rate_learning(proj)
+            custom = CodeGenerator.custom_psp(proj)
+            if custom and not learning:
+                # the psp kernel reads the synapse's own attributes, real weights
+                if not self.exact:
+                    nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
+                for name, arr in proj._host_attr.items():
+                    nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real)[keep_syn])
+                for name, arr in proj._host_semi.items():
+                    nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
             if learning:
                 # the update kernel walks the CSR rows and writes the weights in place
                 if proj._storage_format not in ("csr", "auto"):
@@ -673,7 +682,8 @@ class CompiledNetwork:
                 for name, arr in proj._host_semi.items():
                     nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
                 nat.create(f"proj{k}__flags", np.array(proj._learn_flags, dtype=np.int32))
-            fmt = "csr" if (proj._delay_steps is not None or learning) else self._rate_format(proj, lay)
+            fmt = ("csr" if (proj._delay_steps is not None or learning or custom)
+                   else self._rate_format(proj, lay))
             lay["format"] = fmt
             if fmt != "csr":
                 F.create_format_arrays(self, proj, fmt, post_rank, row_ptr, cols, w, lay)
@@ -736,6 +746,8 @@ class CompiledNetwork:
                         # plastic weights stay float32 (they are updated every event)
                         nat.create(f"proj{k}__w", np.asarray(w, dtype=np.float32))
                     for name, arr in host.items():
+                        nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
+                    for name, arr in proj._host_semi.items():
                         nat.create(f"proj{k}__{name}", np.asarray(arr, dtype=self.real))
                     nat.create(f"proj{k}___last_event", np.full(nnz, -10000, dtype=np.int64))
         self.layout[k] = lay

@@ -53,6 +53,20 @@ class Population:
         self._has_refractory = bool(refr)
         object.__setattr__(self, "_ready", True)
 
+    def _add_spike_target(self, target: str):
+        """A projection's target that the spiking neuron's equations do not
+        mention: a conductance g_<target> that only the transmissions change
+        (the reference adds the target to the population,
+        ANNarchy/core/Projection.py:105-110, and declares g_<target>)."""
+        if target in self.targets:
+            return
+        self.targets.append(target)
+        name = "g_" + target
+        if name not in self._host:
+            self._host[name] = np.zeros(self.size)
+            self._locality[name] = "local"
+            self._ctype[name] = "double"
+
     def _add_rate_target(self, target: str):
         """A projection's target that the neuron's equations do not use: its
         weighted sum array (zero until compile)."""

@@ -68,13 +68,11 @@ class Projection:
             if target not in self.post_pop.targets:
                 # a conductance the neuron only assigns (`g_exc = 0`) is not
                 # found by the target extraction (ANNarchy/parser/
-                # Extraction.py:686-702 wants a character before `g_`); the
-                # projection adds its target to the population's, as the
-                # reference's does (ANNarchy/core/Projection.py:105-110)
-                if self.post_pop._locality.get("g_" + str(target)) == "local":
-                    self.post_pop.targets.append(target)
-                else:
-                    raise ValueError(f"target {target!r} is not used by the post-synaptic neuron")
+                # Extraction.py:686-702 wants a character before `g_`), or the
+                # neuron does not mention it: the projection adds its target
+                # to the population's, as the reference's does
+                # (ANNarchy/core/Projection.py:105-110)
+                self.post_pop._add_spike_target(target)
         self.pre_ranks = _ranks(pre)
         self.post_ranks_view = _ranks(post)
         self._csr: sp.csr_matrix | None = None   # (n_post_view, n_pre_view), view-relative
@@ -115,6 +113,8 @@ class Projection:
         d = self.desc
         if d.get("plasticity") or d.get("post_spike"):
             return True
+        if any(v.get("cpp") and v.get("method") != "event-driven" for v in d["variables"]):
+            return True                 # synaptic variables updated every step
         for v in d.get("pre_spike", []):
             if v["name"] != "g_target" or v["eq"].replace(" ", "") != "g_target+=w":
                 return True

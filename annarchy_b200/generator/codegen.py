@@ -100,6 +100,8 @@ def trace_layout(proj, exact: bool):
     record bytes) or None when the variables stay separate arrays."""
     if exact or not proj.plastic or proj.synapse_type.type != "spike":
         return None
+    if CodeGenerator.continuous_update(proj):
+        return None                 # the per-step update walks separate arrays
     names = syn_local_names(proj)
     nbytes = 4 * (len(names) + 1)
     nbytes = 8 if nbytes <= 8 else -(-nbytes // 16) * 16
@@ -701,6 +703,71 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
 
     # ------------------------------------------------- rate-coded learning
     @staticmethod
+    def custom_psp(proj) -> bool:
+        """A rate-coded synapse whose psp is not w * pre.r."""
+        if proj.synapse_type.type != "rate":
+            return False
+        eq = proj.desc.get("psp", {}).get("eq", "w*pre.r").replace(" ", "")
+        return eq not in ("w*pre.r", "pre.r*w")
+
+    def custom_psp_kernel(self, proj) -> str:
+        """Weighted sum with the synapse's own psp expression
+        (ANNarchy/generator/Projection/OpenMP/CSR.py:177-253 with the psp
+        code in place of w * pre.r): thread per post row, the terms added in
+        stored (ascending pre rank) order, then the row's sum added to the
+        target's sum."""
+        k = proj.id
+        lay = self.c.layout[k]
+        a, b = proj.pre_pop, proj.post_pop
+        desc = proj.desc
+        p = lambda n: self.ptr(f"proj{k}__{n}")
+        code = self.typed(self.fill(desc["psp"]["cpp"], local="[j]", semi="[anb_row]",
+                                    pre_prefix="anb_pre_", pre_index="[anb_col[j]]",
+                                    post_prefix="anb_post_", post_index="[anb_post]"))
+        expr = code.strip().rstrip(";")
+        decl = [f"const {self.real} {q['name']} = {p(q['name'])}[0];"
+                for q in desc["parameters"] + desc["variables"] if q["locality"] == "global"]
+        for q in desc["parameters"] + desc["variables"]:
+            if q["locality"] in ("local", "semiglobal") and q["name"] != "w":
+                decl.append(f"const {self.real}* __restrict__ {q['name']} = {p(q['name'])};")
+        decl.append(f"const {self.real}* __restrict__ w = {p('w')};")
+        for prefix, pop in (("anb_pre_", a), ("anb_post_", b)):
+            for n in sorted(set(re.findall(prefix + r"(\w+)\[", expr))):
+                if n not in pop._host:
+                    raise NotImplementedError(f"{proj.name}: {prefix[4:-1]}.{n} is not an attribute "
+                                              f"of {pop.name}")
+                ct = "int" if pop._ctype.get(n) in ("int", "bool") else self.real
+                decl.append(f"const {ct}* __restrict__ {prefix}{n} = {self.ptr(f'pop{pop.id}__{n}')};")
+        dt_t = "double" if self.exact else "float"
+        sum_ = self.ptr(f"pop{b.id}___sum_{proj.target}")
+        rp_t = lay["idx_t"]
+        nl = "\n    "
+        return f"""
+extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
+    const long long t = *{self.ptr('t')};
+    const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
+    (void)t; (void)dt;
+    {nl.join(decl)}
+    const int* __restrict__ anb_col = {p('col')};
+    const {rp_t}* __restrict__ anb_rp = {p('row_ptr')};
+    for (int anb_row = blockIdx.x * blockDim.x + threadIdx.x; anb_row < {lay['rows']};
+         anb_row += gridDim.x * blockDim.x) {{
+      const int anb_post = {p('post_rank')}[anb_row];
+      {self.real} anb_s = ({self.real})0;
+      for ({rp_t} j = anb_rp[anb_row]; j < anb_rp[anb_row + 1]; ++j) anb_s += {expr};
+      {sum_}[anb_post] += anb_s;
+    }}
+}}
+"""
+
+    @staticmethod
+    def continuous_update(proj) -> bool:
+        """Synaptic variables with equations evaluated every step (the
+        reference's update_synapse), rate-coded or spiking."""
+        return any(v.get("cpp") and v.get("method") != "event-driven"
+                   for v in proj.desc["variables"])
+
+    @staticmethod
     def rate_learning(proj) -> bool:
         """A rate-coded projection whose synapse has continuous equations
         (the reference's update_synapse)."""
@@ -772,6 +839,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
         a, b = proj.pre_pop, proj.post_pop
         lay = self.c.layout[k]
         desc = proj.desc
+        if getattr(proj, "_device_conn", None) or lay.get("device"):
+            raise NotImplementedError(f"{proj.name}: synaptic equations evaluated every step need "
+                                      "connectivity built on the host in this backend")
         for v in desc["variables"]:
             if v.get("cpp") and v.get("method") not in ("explicit", "exponential", "event-driven",
                                                         None) and v.get("switch"):
@@ -927,8 +997,9 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_delay() {{
         sum_ = self.ptr(f"pop{proj.post_pop.id}___sum_{proj.target}")
         fmt = lay["format"]
         p = lambda n: self.ptr(f"proj{k}__{n}")
-        # learning projections keep float32 weights (updated every step)
-        W = "float" if (self.rate_learning(proj) and not self.exact) else self.c.wctype
+        # learning and custom-psp projections keep float32 weights
+        W = ("float" if ((self.rate_learning(proj) or self.custom_psp(proj)) and not self.exact)
+             else self.c.wctype)
         name = f"proj{k}_psp"
         tdecl = f"const long long t = *{self.ptr('t')};\n    " if self.delayed(proj) else ""
 
@@ -939,6 +1010,11 @@ extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
     {tdecl}{body}
 }}
 """
+        if self.custom_psp(proj):
+            if self.delayed(proj):
+                raise NotImplementedError(f"{proj.name}: a custom psp with synaptic delays is not "
+                                          "supported by this backend")
+            return self.custom_psp_kernel(proj), [(name, grid_for(lay["rows"]), BLOCK, 0)]
         if fmt == "bsr_tc":
             # copies of the network sharing the weights: one tensor-core
             # product for all of them (a library operation of the plan)
@@ -1592,7 +1668,7 @@ extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run
                 kernels.append(self.delay_kernel(pop))
                 plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))
         for proj in net.projections:
-            if self.rate_learning(proj):
+            if self.continuous_update(proj):
                 for src, entry in self.rate_update_kernels(proj):
                     kernels.append(src)
                     plan.append(entry)

@@ -489,6 +489,38 @@ def case_stp(name, seed, n, p, steps, g_every):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+def case_spiking_continuous(name, steps=30):
+    """A spiking synapse with equations evaluated every step (decaying pre-
+    and post-traces set at pre- and post-synaptic spikes, w their sum), the
+    network of the reference's test_SpikingContinuousUpdate: the synapse's
+    w and traces after every step."""
+    import numpy as np
+    import ANNarchy as ann
+    net = ann.Network(dt=1.0, seed=1)
+    net.config(num_threads=1)
+    pre_n = ann.Neuron(equations="mp=t", spike="(modulo(t,3))")
+    post_n = ann.Neuron(equations="mp=t", spike="(modulo(t,5))")
+    syn = ann.Synapse(pre_spike="pre_trace=pre.mp : init=0.0",
+                      post_spike="post_trace=post.mp : init=0.0",
+                      equations="""
+                          post_trace = post_trace -1 : min=0.0
+                          pre_trace = pre_trace -1 : min=0.0
+                          w = post_trace + pre_trace
+                      """)
+    p0 = net.create(1, pre_n)
+    p1 = net.create(1, post_n)
+    proj = net.connect(p0, p1, "exc", syn)
+    proj.all_to_all(weights=0.0)
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    rows = []
+    for _ in range(steps):
+        net.simulate(1)
+        rows.append([float(np.ravel(proj.w)[0]), float(np.ravel(proj.pre_trace)[0]),
+                     float(np.ravel(proj.post_trace)[0])])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), steps=steps,
+                        w_pre_post=np.asarray(rows))
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -505,6 +537,7 @@ CASES = {
     "connectivity_file": (case_connectivity_file, {}),
     "self_connections": (case_self_connections, {}),
     "stp_small": (case_stp, dict(seed=5, n=400, p=0.05, steps=2000, g_every=50)),
+    "spiking_continuous": (case_spiking_continuous, {}),
 }
 
 

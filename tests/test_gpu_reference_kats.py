@@ -344,3 +344,54 @@ def test_rate_learning_rules_weighted_sums(precision):
     for target in ("Hebb", "Oja", "IBCM"):
         np.testing.assert_allclose(out.sum(target), 0.1, rtol=1e-7)
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_rate_continuous_update_of_all_localities(precision):
+    """Projection-level, postsynaptic and synaptic variables updated every
+    step (tests_python/RateSynapse/test_RateContinuousUpdate.py:15-55, which
+    runs one step): after step 0, w = 0 + 0.1 + 0.2."""
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    neuron = Neuron(parameters="r=1.0")
+    proj = net.connect(net.create(3, neuron), net.create(1, neuron), "exc", Synapse(equations="""
+        glob_var = 0.1 : projection
+        semi_glob_var = 0.2 : postsynaptic
+        w = t + glob_var + semi_glob_var
+    """))
+    proj.all_to_all(weights=0.0)
+    net.compile()
+    net.simulate(1)
+    np.testing.assert_allclose(proj.get("w", flat=True), [0.3] * 3, rtol=1e-7)
+    np.testing.assert_allclose(proj.get("glob_var"), 0.1, rtol=1e-7)
+    np.testing.assert_allclose(np.ravel(proj.get("semi_glob_var")), [0.2], rtol=1e-7)
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_spiking_synapse_with_equations_every_step(golden, precision):
+    """A spiking synapse whose traces are set at pre- and post-synaptic
+    spikes and decay every step, w their sum (the network of
+    tests_python/SpikeSynapse/test_SpikingContinuousUpdate.py:15-60): w and
+    both traces after every one of 30 steps equal the reference's run
+    (tests/golden/spiking_continuous.npz)."""
+    g = golden("spiking_continuous")["w_pre_post"]
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    pre = net.create(1, Neuron(equations="mp=t", spike="(modulo(t,3))"))
+    post = net.create(1, Neuron(equations="mp=t", spike="(modulo(t,5))"))
+    proj = net.connect(pre, post, "exc", Synapse(
+        pre_spike="pre_trace=pre.mp : init=0.0", post_spike="post_trace=post.mp : init=0.0",
+        equations="""
+            post_trace = post_trace -1 : min=0.0
+            pre_trace = pre_trace -1 : min=0.0
+            w = post_trace + pre_trace
+        """))
+    proj.all_to_all(weights=0.0)
+    net.compile()
+    rows = []
+    for _ in range(g.shape[0]):
+        net.simulate(1)
+        rows.append([proj.get(n, flat=True)[0] for n in ("w", "pre_trace", "post_trace")])
+    np.testing.assert_array_equal(np.asarray(rows), g)
+    net.close()
