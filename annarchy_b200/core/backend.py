@@ -105,7 +105,7 @@ class CompiledNetwork:
         nat.initialize(net.dt)
         # key of the random draws in equations (drawn from the network's seed,
         # only when some equation draws)
-        if any(p.desc.get("random_distributions") for p in net.populations):
+        if any(p.desc.get("random_distributions") for p in net.populations + net.projections):
             key = net._rng.integers(0, 2**32, 2, dtype=np.uint64).astype(np.uint32)
         else:
             key = np.zeros(2, dtype=np.uint32)

@@ -867,6 +867,20 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
         glob_eq = self._syn_block(proj, "global")
         out = []
 
+        def draws(locality, index):
+            """This step's draws of the synapse's random distributions of one
+            locality: Philox keyed by the network's seed, stream (projection,
+            distribution), step and index (synapse, dendrite or 0)."""
+            lines = []
+            for kk, rd in enumerate(desc.get("random_distributions", [])):
+                if rd["locality"] != locality:
+                    continue
+                args = ", ".join(f"({self.real})({self.typed(a)})" for a in rd["args"])
+                lines.append(f"const {self.real} {rd['name']} = {self._DRAW_FN[rd['dist']]}<{self.real}>("
+                             f"{self.ptr('rng_seed')}, {0x40000000 | (k << 8) | kk}u, t, "
+                             f"(unsigned)({index}), {args});")
+            return "\n        ".join(lines)
+
         def refs(code):
             decl = []
             for prefix, pop in (("anb_pre_", a), ("anb_post_", b)):
@@ -881,6 +895,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
 
         if glob_eq.strip():
             code = self.typed(self.fill(glob_eq, post_prefix="anb_post_", post_index="[0]"))
+            code = draws("global", "0") + "\n    " + code
             names = {q["name"] for q in desc["variables"] if q["locality"] == "global" and q.get("cpp")}
             loads = "\n    ".join(f"{self.real} {q['name']} = {p(q['name'])}[0];" for q in glob_all)
             stores = "\n    ".join(f"{p(n)}[0] = {n};" for n in sorted(names))
@@ -903,6 +918,10 @@ extern "C" __global__ void __launch_bounds__(32) proj{k}_update_global() {{
                                       post_prefix="anb_post_", post_index="[anb_post]"))
         if not (semi_eq.strip() or loc_eq.strip()):
             return out
+        if semi_eq.strip():
+            semi_eq = draws("semiglobal", "anb_row") + "\n        " + semi_eq
+        if loc_eq.strip():
+            loc_eq = draws("local", "j") + "\n        " + loc_eq
         gvals = "\n    ".join(f"const {self.real} {q['name']} = {p(q['name'])}[0];" for q in glob_all)
         if pre_loop:
             gvals += "\n    " + pre_loop

@@ -370,10 +370,17 @@ def analyse_synapse(synapse) -> dict:
                 desc["local"].append(var["name"])
                 desc["attributes"].append(var["name"])
     untouched_all = {}
+    randoms = []
+    desc["random_distributions"] = randoms
     for var in variables:
         eq = var.get("transformed_eq", var["eq"])
         if eq.strip() == "":
             continue
+        # per-step draws (one per synapse, dendrite or projection by the
+        # variable's locality)
+        rand_untouched = {}
+        eq = _extract_random(" " + eq + " ", var, randoms, rand_untouched)
+        untouched_all.update(rand_untouched)
         _unsupported(eq, var["name"])
         eq, untouched = _prepost(eq)
         for k, v in untouched.items():

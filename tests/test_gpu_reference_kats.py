@@ -395,3 +395,22 @@ def test_spiking_synapse_with_equations_every_step(golden, precision):
         rows.append([proj.get(n, flat=True)[0] for n in ("w", "pre_trace", "post_trace")])
     np.testing.assert_array_equal(np.asarray(rows), g)
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_synapse_random_variables(precision):
+    """A Normal(1.0, 0.001) draw per synapse and step in a synaptic equation
+    (tests_python/Common/test_RandomVariables.py:73-115): after one step the
+    weights lie within 10 sigma of 1.0 and differ."""
+    from annarchy_b200 import LeakyIntegrator
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    v = net.create(5, LeakyIntegrator())
+    proj = net.connect(v, v, "exc", synapse=Synapse(equations="w = Normal(1.0, 0.001)"))
+    proj.fixed_number_pre(number=1, weights=0.0)
+    net.compile()
+    net.simulate(1)
+    w = np.asarray(proj.get("w", flat=True))
+    np.testing.assert_allclose(w, 1.0, atol=0.01)
+    assert w.max() != w.min()
+    net.close()
