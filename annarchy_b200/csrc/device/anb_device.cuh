@@ -51,6 +51,7 @@ __device__ __forceinline__ float power(float x, unsigned int a) {
 }
 __device__ __forceinline__ double power(int x, unsigned int a) { return power((double)x, a); }
 #define clip(x, a, b) ((x) < (a) ? (a) : ((x) > (b) ? (b) : (x)))
+#define ite(a, b, c) ((a) ? (b) : (c))
 
 // ---- bfloat16 ---------------------------------------------------------------
 __device__ __forceinline__ float anb_bf16_to_f32(anb_bf16 h) {

@@ -8,14 +8,16 @@ The description has the same keys as the reference's
 ``pre_spike``/``post_spike``/``psp``. C strings keep the reference's index
 placeholders (``%(local_index)s`` ...); the code generator fills them.
 
-Random distributions inside neuron equations (``p = Uniform(0.0, 1.0)``)
-become per-step draws ``rand_<k>`` listed in ``random_distributions``, as the
-reference's parser extracts them (ANNarchy/parser/Extraction.py,
-extract_randomdist); the code generator draws them on the device.
+Random distributions inside neuron and synapse equations
+(``p = Uniform(0.0, 1.0)``) become per-step draws ``rand_<k>`` listed in
+``random_distributions``, as the reference's parser extracts them
+(ANNarchy/parser/Extraction.py, extract_randomdist); the code generator draws
+them on the device. If-then-else statements (``x = if c: a else: b``, nested)
+become C conditionals as in ANNarchy/parser/ITE.py; ``ite(c, a, b)`` is a
+function of the device header.
 
-Not supported by this backend (an error names them): if-then-else
-statements, global operations (``mean(r)``...), random distributions inside
-synapse equations, user functions, coupled implicit/midpoint/rk4 systems.
+Not supported by this backend (an error names them): global operations
+(``mean(r)``...), user functions, coupled implicit/midpoint/rk4 systems.
 """
 from __future__ import annotations
 
@@ -181,13 +183,89 @@ def _extract_random(eq, var, found, untouched):
 
 
 def _unsupported(eq, where):
-    if re.search(r"\bite\(|\bif\b.*\belse\b", eq):
-        raise ParserError(f"{where}: if-then-else statements are not supported by this backend")
     if re.search(r"\b(mean|min|max|norm1|norm2)\(", eq):
         raise ParserError(f"{where}: global operations are not supported by this backend")
     if re.search(r"\b(Uniform|Normal|LogNormal|Exponential|Gamma|Binomial|DiscreteUniform)\(", eq):
         raise ParserError(f"{where}: random distributions in equations are not supported by "
                           "this backend")
+
+
+def _extract_ite(eq, split=True):
+    """An if-then-else right-hand side (ANNarchy/parser/ITE.py:93-175):
+
+        x = if cond: a else: b          (branches may nest)
+
+    becomes `x = __conditional__0` and the nested [condition, then, else]
+    structure; (eq, []) when the statement has no conditional."""
+    if "if " not in eq:
+        return eq, []
+    left, right = eq.split("=", 1) if split else ("", eq)
+    n_then, n_else = right.count(":"), len(re.findall("else", right))
+    if n_then == 0:
+        raise ParserError(f"{eq}: conditional statements must define then and else values "
+                          "(var = if condition: a else: b)")
+    if not right.strip().startswith("if"):
+        raise ParserError(f"{eq}: the right term must directly start with an if statement")
+    if n_then != 2 * n_else:
+        raise ParserError(f"{eq}: conditional statements must use both : and else")
+    lines = []
+    for item in (x.strip() for x in right.split(":")):
+        if item.startswith("if "):
+            lines.append(item)
+        elif item.endswith("else"):
+            lines.append(item.split("else")[0].strip())
+            lines.append("else")
+        else:
+            lines.append(item)
+
+    def nest(rest):
+        out = []
+        while rest:
+            if rest[0].startswith("if"):
+                block = [rest.pop(0).split("if")[1], nest(rest)]
+                if rest and rest[0].startswith("else"):
+                    rest.pop(0)
+                    block.append(nest(rest))
+                out.append(block)
+            elif not rest[0].startswith("else"):
+                out.append(rest.pop(0))
+            else:
+                break
+        return out[0]
+
+    condition = nest(lines)
+    right = " __conditional__0 "
+    return (left + "=" + right if split else right), [condition]
+
+
+def _ite_statement(name, eq, conditions, desc, untouched, method="explicit", kind=None):
+    """The C code of a statement with conditionals (ANNarchy/parser/ITE.py:
+    13-90): the statement with its placeholders, each replaced by
+    (cond ? then : else), conditions parsed as conditions and branches as
+    expressions, nested branches recursively. Returns (code, Statement)."""
+    keys = list(untouched)
+
+    def branch(b):
+        if isinstance(b, list):
+            return conditional(b)
+        return Statement(name, b, desc, untouched=keys, kind="return").parse().split(";")[0]
+
+    def conditional(c):
+        cond = Statement(name, c[0], desc, untouched=keys, kind="cond").parse()
+        return "(" + cond + " ? " + branch(c[1]) + " : " + branch(c[2]) + ")"
+
+    st = Statement(name, eq, desc, untouched=keys + [f"__conditional__{i}" for i in
+                                                   range(len(conditions))],
+                   method=method, kind=kind)
+    code = st.parse()
+    for i, c in enumerate(conditions):
+        ite = conditional(c)
+        if isinstance(code, str):
+            code = code.replace(f"__conditional__{i}", ite)
+        else:
+            code = list(code)
+            code[1] = code[1].replace(f"__conditional__{i}", ite)
+    return code, st
 
 
 def _bound_code(name, value, desc, untouched):
@@ -257,8 +335,8 @@ def analyse_neuron(neuron) -> dict:
         for b in ("min", "max"):
             if b in var["bounds"]:
                 var["bounds"][b] = _bound_code(var["name"], var["bounds"][b], desc, untouched)
-        st = Statement(var["name"], eq, desc, untouched=untouched, method=method)
-        code = st.parse()
+        eq, conditions = _extract_ite(eq)
+        code, st = _ite_statement(var["name"], eq, conditions, desc, untouched, method)
         if isinstance(code, str):
             pre_loop, cpp, switch = {}, code, None
         else:
@@ -390,8 +468,8 @@ def analyse_synapse(synapse) -> dict:
             if b in var["bounds"]:
                 var["bounds"][b] = _bound_code(var["name"], var["bounds"][b], desc,
                                                list(untouched_all))
-        st = Statement(var["name"], eq, desc, untouched=list(untouched_all), method=method)
-        code = st.parse()
+        eq, conditions = _extract_ite(eq)
+        code, st = _ite_statement(var["name"], eq, conditions, desc, untouched_all, method)
         if isinstance(code, str):
             pre_loop, cpp, switch = {}, code, None
         else:
@@ -407,8 +485,8 @@ def analyse_synapse(synapse) -> dict:
         eq, untouched = _prepost(" " + desc["raw_psp"].strip() + " ")
         for k, v in untouched.items():
             untouched_all.setdefault(k, v)
-        st = Statement("psp", eq, desc, untouched=list(untouched_all), kind="return")
-        code = st.parse()
+        eq, conditions = _extract_ite(eq, split=False)
+        code, st = _ite_statement("psp", eq, conditions, desc, untouched_all, kind="return")
         for prev, new in sorted(untouched_all.items(), key=lambda kv: len(kv[0]), reverse=True):
             code = code.replace(prev, new)
         desc["psp"] = {"eq": desc["raw_psp"].strip(), "cpp": code}

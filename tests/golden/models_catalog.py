@@ -59,6 +59,25 @@ NEURONS = {
         """),
 }
 
+# if-then-else statements (the models of the reference's test_ITE.py)
+NEURONS.update({
+    "ite_simple": dict(equations="r = if (t is 1): 1.0 else: 0.0"),
+    "ite_nested": dict(parameters="state = 1.0", equations="""
+            r = if (t <= 5):
+                    0
+                else:
+                    if (t >= 7):
+                        2
+                    else:
+                        1
+        """),
+    "ite_ode": dict(equations="dr/dt = if t > 5: 1 else: 0"),
+    "ite_function": dict(equations="r = ite(t is 1, 1.0, 0.0)"),
+    "ite_function_nested": dict(parameters="state = 2.0",
+                                equations="r = ite(state >= 2, 2, ite(state == 1, 1, 0))"),
+    "ite_function_ode": dict(equations="dr/dt = ite((t > 5) and (t <20), 1, 0)"),
+})
+
 SYNAPSES = {
     "stdp": dict(parameters="""
             tau_plus = 16.8 : projection

@@ -18,11 +18,16 @@ backend on the GPU with the values those tests expect:
 Every case runs in double (the reference's arithmetic) and in float
 precision; the expected values are small integers or tenths, exact in
 both."""
+import os
+import sys
+
 import numpy as np
 import pytest
 import scipy.sparse as sp
 
 from annarchy_b200 import Network, Neuron, Synapse, Uniform
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 
 pytestmark = pytest.mark.gpu
 
@@ -413,4 +418,21 @@ def test_synapse_random_variables(precision):
     w = np.asarray(proj.get("w", flat=True))
     np.testing.assert_allclose(w, 1.0, atol=0.01)
     assert w.max() != w.min()
+    net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_if_then_else(precision):
+    """Conditional statements and the ite() function, nested and inside
+    ODEs (tests_python/Common/test_ITE.py:15-95): r after 10 steps."""
+    from models_catalog import NEURONS
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    keys = ("ite_simple", "ite_nested", "ite_ode", "ite_function", "ite_function_nested",
+            "ite_function_ode")
+    pops = [net.create(1, Neuron(**NEURONS[k])) for k in keys]
+    net.compile()
+    net.simulate(10)
+    np.testing.assert_array_equal([float(np.ravel(p.r)[0]) for p in pops],
+                                  [0.0, 2.0, 4.0, 0.0, 2.0, 4.0])
     net.close()

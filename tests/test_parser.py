@@ -52,8 +52,15 @@ def test_rate_neuron_needs_r():
         analyse_neuron(Neuron(parameters="tau = 10.0", equations="tau * dv/dt = -v"))
 
 
-def test_unsupported_constructs_rejected():
+def test_conditional_statement_errors():
+    """Malformed conditionals are refused as the reference refuses them
+    (ANNarchy/parser/ITE.py:150-170)."""
     with pytest.raises(ParserError):
-        analyse_neuron(Neuron(equations="r = ite(v > 0, 1.0, 0.0)\n dv/dt = -v"))
+        analyse_neuron(Neuron(equations="r = 1.0 + if t > 1: 1.0 else: 0.0"))
+    with pytest.raises(ParserError):
+        analyse_neuron(Neuron(equations="r = if t > 1: 1.0"))
+
+
+def test_unsupported_constructs_rejected():
     with pytest.raises(ParserError):
         analyse_neuron(Neuron(equations="r = mean(v)\n dv/dt = -v"))
