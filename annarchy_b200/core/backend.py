@@ -255,8 +255,8 @@ class CompiledNetwork:
             return False, "device-generated connectivity"
         if any(v != "spike" for m in net.monitors for v in m.variables):
             return False, "variable monitors"
-        if any(global_equations(p) for p in net.populations):
-            return False, "population-level variables with equations"
+        if any(global_equations(p) or p.desc.get("global_operations") for p in net.populations):
+            return False, "population-level variables with equations or global operations"
         smem = self._local_smem_bytes()
         if smem > LOCAL_SMEM_LIMIT:
             return False, f"state needs {smem} bytes of shared memory"

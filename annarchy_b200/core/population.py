@@ -43,6 +43,12 @@ class Population:
             self._ctype[p["name"]] = p.get("ctype", "double")
         for p in self.desc["parameters"] + self.desc["variables"]:
             self._host[p["name"]] = self._initial(p)
+        for op in self.desc.get("global_operations", []):
+            # the population-wide reduction of the previous step
+            name = "_" + op["function"] + "_" + op["variable"]
+            self._host[name] = np.float64(0.0)
+            self._locality[name] = "global"
+            self._ctype[name] = "double"
         if self.neuron_type.type == "rate":
             for t in self.targets:
                 self._host["_sum_" + t] = np.zeros(self.size)

@@ -296,6 +296,9 @@ class CodeGenerator:
                 ct = "int" if p.get("ctype") in ("int", "bool") else self.real
                 const = "" if p["name"] in evolving else "const "
                 out.append(f"{const}{ct} {p['name']} = {src(p['name'])}[0];")
+        for op in pop.desc.get("global_operations", []):
+            name = "_" + op["function"] + "_" + op["variable"]
+            out.append(f"const {self.real} {name} = {src(name)}[0];")
         for n in self._reciprocals(pop):
             out.append(f"const {self.real} anb_inv_{n} = ({self.real})1 / {n};")
         for v in pop.desc["variables"]:
@@ -653,6 +656,67 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_step() {{
     const {dt_t} dt = ({dt_t})(*{self.ptr('dt')});
     {preamble}
 {self.neuron_update(pop)}{store}
+}}
+"""
+
+    def globalops_kernel(self, pop) -> str:
+        """The population's reductions after this step's update
+        (ANNarchy/generator/Template/GlobalOperationTemplate.py): in double
+        precision one thread in index order as the reference (the sum starts
+        from element 0; mean = sum / n, norm2 = sqrt of the sum of squares);
+        in single precision one CTA's tree reduction."""
+        k = pop.id
+        n = pop.size
+        R = self.real
+        outs = []
+        for op in pop.desc["global_operations"]:
+            f, v = op["function"], op["variable"]
+            outs.append((f, self.ptr(f"pop{k}__{v}"), self.ptr(f"pop{k}___{f}_{v}")))
+        if self.exact:
+            body = []
+            for f, src, dst in outs:
+                first = {"norm1": f"fabs({src}[0])", "norm2": f"{src}[0] * {src}[0]"}.get(f, f"{src}[0]")
+                step = {"max": f"if ({src}[i] > s) s = {src}[i];",
+                        "min": f"if ({src}[i] < s) s = {src}[i];",
+                        "mean": f"s += {src}[i];",
+                        "norm1": f"s += fabs({src}[i]);",
+                        "norm2": f"s += {src}[i] * {src}[i];"}[f]
+                fin = {"mean": f"s / ({R}){n}", "norm2": "sqrt(s)"}.get(f, "s")
+                body.append(f"{{ {R} s = {first}; for (int i = 1; i < {n}; ++i) {{ {step} }} {dst}[0] = {fin}; }}")
+            code = "\n      ".join(body)
+            return f"""
+extern "C" __global__ void __launch_bounds__(32) pop{k}_globalops() {{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {{
+      {code}
+    }}
+}}
+"""
+        parts = []
+        for idx, (f, src, dst) in enumerate(outs):
+            init = {"max": "__int_as_float(0xff800000)",
+                    "min": "__int_as_float(0x7f800000)"}.get(f, "0.f")
+            acc = {"max": "fmaxf(s, x)", "min": "fminf(s, x)", "mean": "s + x",
+                   "norm1": "s + fabsf(x)", "norm2": "s + x * x"}[f]
+            comb = {"max": "fmaxf(s, o)", "min": "fminf(s, o)"}.get(f, "s + o")
+            fin = {"mean": f"s / (float){n}", "norm2": "sqrtf(s)"}.get(f, "s")
+            parts.append(f"""
+    {{
+      float s = {init};
+      for (int i = threadIdx.x; i < {n}; i += blockDim.x) {{ const float x = (float){src}[i]; s = {acc}; }}
+      for (int d = 16; d > 0; d >>= 1) {{ const float o = __shfl_xor_sync(0xffffffffu, s, d); s = {comb}; }}
+      if ((threadIdx.x & 31) == 0) anb_red[threadIdx.x >> 5] = s;
+      __syncthreads();
+      if (threadIdx.x < 32) {{
+        s = threadIdx.x < (blockDim.x >> 5) ? anb_red[threadIdx.x] : {init};
+        for (int d = 16; d > 0; d >>= 1) {{ const float o = __shfl_xor_sync(0xffffffffu, s, d); s = {comb}; }}
+        if (threadIdx.x == 0) {dst}[0] = {fin};
+      }}
+      __syncthreads();
+    }}""")
+        return f"""
+extern "C" __global__ void __launch_bounds__(1024) pop{k}_globalops() {{
+    __shared__ float anb_red[32];
+    if (blockIdx.x != 0) return;{''.join(parts)}
 }}
 """
 
@@ -1568,7 +1632,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record{'_targets' i
             return False
         if any(getattr(p, "stop_condition", None) or hasattr(p, "_ta_schedule_ms")
                or p.neuron_type.type != "spike" or self.slots(p) > 1 or global_equations(p)
-               for p in net.populations):
+               or p.desc.get("global_operations") for p in net.populations):
             return False
         return True
 
@@ -1683,6 +1747,9 @@ extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run
                 lo, hi = getattr(self.c, "owned", {}).get(pop.id, (0, pop.size))
                 K = self.neurons_per_thread(pop)
                 plan.append((f"pop{pop.id}_step", grid_for(max(1, -(-(hi - lo) // K))), BLOCK, 0))
+            if pop.desc.get("global_operations"):
+                kernels.append(self.globalops_kernel(pop))
+                plan.append((f"pop{pop.id}_globalops", 1, 32 if self.exact else 1024, 0))
             elif pop.neuron_type.type == "rate" and self.slots(pop) > 1:
                 kernels.append(self.delay_kernel(pop))
                 plan.append((f"pop{pop.id}_delay", grid_for(pop.size), BLOCK, 0))

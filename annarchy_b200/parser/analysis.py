@@ -182,9 +182,32 @@ def _extract_random(eq, var, found, untouched):
     return _RANDOM_RE.sub(repl, eq)
 
 
-def _unsupported(eq, where):
-    if re.search(r"\b(mean|min|max|norm1|norm2)\(", eq):
-        raise ParserError(f"{where}: global operations are not supported by this backend")
+GLOBAL_OPERATIONS = ("min", "max", "mean", "norm1", "norm2")
+
+
+def _extract_globalops(eq, desc, where):
+    """Population-wide reductions of a neuron's local variable in an
+    equation (``mean(r)``, ``max(v)``...; ANNarchy/parser/Extraction.py:
+    124-145): replaced by the scalar ``_<op>_<var>``, computed after every
+    step's update and listed in desc["global_operations"]."""
+    untouched = {}
+    for op in GLOBAL_OPERATIONS:
+        for _, var in re.findall(r"([^\w]*)" + op + r"\(([\s\w]*)\)", eq):
+            if var.strip() not in desc["local"]:
+                raise ParserError(f"{where}: there is no local attribute {var!r}")
+            new = "_" + op + "_" + var.strip()
+            eq = eq.replace(op + "(" + var + ")", new)
+            untouched[new] = new
+            item = {"function": op, "variable": var.strip()}
+            if item not in desc["global_operations"]:
+                desc["global_operations"].append(item)
+    return eq, untouched
+
+
+def _unsupported(eq, where, neuron=False):
+    if not neuron and re.search(r"\b(mean|min|max|norm1|norm2)\(", eq):
+        raise ParserError(f"{where}: global operations in synapses are not supported by this "
+                          "backend")
     if re.search(r"\b(Uniform|Normal|LogNormal|Exponential|Gamma|Binomial|DiscreteUniform)\(", eq):
         raise ParserError(f"{where}: random distributions in equations are not supported by "
                           "this backend")
@@ -320,13 +343,16 @@ def analyse_neuron(neuron) -> dict:
         desc["spike"] = _spike(desc)
     randoms = []
     desc["random_distributions"] = randoms
+    desc["global_operations"] = []
     for var in variables:
         eq = var.get("transformed_eq", var["eq"])
         if eq.strip() == "":
             continue
         untouched = {}
         eq = _extract_random(eq, var, randoms, untouched)
-        _unsupported(eq, var["name"])
+        eq, glob_untouched = _extract_globalops(eq, desc, var["name"])
+        untouched.update(glob_untouched)
+        _unsupported(eq, var["name"], neuron=True)
         for t in targets:
             eq = re.sub(r"(?P<pre>[^\w.])sum\(\)", r"\1sum(__all__)", eq)
             eq = re.sub(r"sum\(\s*" + t + r"\s*\)", "__sum_" + t + "__", eq)

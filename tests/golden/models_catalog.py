@@ -78,6 +78,15 @@ NEURONS.update({
     "ite_function_ode": dict(equations="dr/dt = ite((t > 5) and (t <20), 1, 0)"),
 })
 
+# population-wide reductions (the model of the reference's test_GlobalOperations.py)
+NEURONS["global_operations"] = dict(parameters="r=0", equations="""
+            mean_r = mean(r)
+            max_r = max(r)
+            min_r = min(r)
+            l1 = norm1(r)
+            l2 = norm2(r)
+        """)
+
 SYNAPSES = {
     "stdp": dict(parameters="""
             tau_plus = 16.8 : projection

@@ -436,3 +436,33 @@ def test_if_then_else(precision):
     np.testing.assert_array_equal([float(np.ravel(p.r)[0]) for p in pops],
                                   [0.0, 2.0, 4.0, 0.0, 2.0, 4.0])
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_global_operations(precision):
+    """mean, max, min, norm1 and norm2 of a population's variable, used in
+    the next step's equations (tests_python/Neuron/test_GlobalOperations.py:
+    15-150): six neurons with fixed rates, and 500 with random ones."""
+    from models_catalog import NEURONS
+    tol = 1e-12 if precision == "double" else 1e-6
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    small = net.create(6, Neuron(**NEURONS["global_operations"]))
+    large = net.create(500, Neuron(**NEURONS["global_operations"]))
+    net.compile()
+    small.r = [2.0, 1.0, 0.0, -5.0, -3.0, -1.0]
+    vals = np.random.default_rng(3).random(500)
+    large.r = vals
+    net.simulate(2)
+    np.testing.assert_allclose(np.asarray(small.mean_r), -1.0, rtol=tol, atol=tol)
+    np.testing.assert_allclose(np.asarray(small.max_r), 2.0, rtol=tol)
+    np.testing.assert_allclose(np.asarray(small.min_r), -5.0, rtol=tol)
+    np.testing.assert_allclose(np.asarray(small.l1), 12.0, rtol=tol)
+    np.testing.assert_allclose(np.asarray(small.l2), np.sqrt(40.0), rtol=tol)
+    np.testing.assert_allclose(np.asarray(large.mean_r), vals.mean(), rtol=tol * 10)
+    np.testing.assert_allclose(np.asarray(large.min_r), np.float32(vals.min()) if tol > 1e-9
+                               else vals.min(), rtol=tol)
+    np.testing.assert_allclose(np.asarray(large.max_r), np.float32(vals.max()) if tol > 1e-9
+                               else vals.max(), rtol=tol)
+    np.testing.assert_allclose(np.asarray(large.l2), np.linalg.norm(vals), rtol=tol * 10)
+    net.close()

@@ -62,5 +62,12 @@ def test_conditional_statement_errors():
 
 
 def test_unsupported_constructs_rejected():
+    # a reduction of something that is not a local attribute
     with pytest.raises(ParserError):
-        analyse_neuron(Neuron(equations="r = mean(v)\n dv/dt = -v"))
+        analyse_neuron(Neuron(equations="r = mean(w)\n dv/dt = -v"))
+    # coupled implicit systems
+    with pytest.raises(ParserError):
+        analyse_neuron(Neuron(equations="""
+            dv/dt = -v + u : implicit
+            du/dt = -u + v : implicit
+        """))
