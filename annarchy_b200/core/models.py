@@ -10,6 +10,9 @@ condition; a synapse is spiking when it has ``pre_spike`` or ``post_spike``.
 from __future__ import annotations
 
 import copy
+from dataclasses import dataclass
+
+from .random import RandomDistribution
 
 # analysed descriptions by defining strings: the equations of identical
 # models (e.g. the copies of a parameter sweep) are parsed once
@@ -21,6 +24,50 @@ def _cached(kind, key, analyse, model):
     if key not in _DESC_CACHE:
         _DESC_CACHE[key] = analyse(model)
     return copy.deepcopy(_DESC_CACHE[key])
+
+
+@dataclass
+class Parameter:
+    """A parameter of a neuron or synapse given as an object in the dict
+    form of `parameters` (ANNarchy/core/Attributes.py:11-48): its value (a
+    number or a random distribution drawn at creation), locality ('global',
+    the default of plain values, 'semiglobal' or 'local') and type."""
+    value: object
+    locality: str = "global"
+    type: object = "float"
+
+
+@dataclass
+class Variable:
+    """A variable of a neuron or synapse given as an object in the list form
+    of `equations` (ANNarchy/core/Attributes.py:51-130): its equation and
+    flags, written out as the equation line `eq : init=..., min=..., max=...,
+    method, type, locality`."""
+    equation: str
+    init: object = None
+    min: object = None
+    max: object = None
+    method: str | None = None
+    locality: str = "local"
+    type: object = "float"
+
+    def __str__(self):
+        flags = []
+        if self.init is not None:
+            flags.append(f"init={self.init!r}" if isinstance(self.init, RandomDistribution)
+                         else f"init={self.init}")
+        if self.min is not None:
+            flags.append(f"min={self.min}")
+        if self.max is not None:
+            flags.append(f"max={self.max}")
+        if self.method is not None:
+            flags.append(str(self.method))
+        kind = {float: "float", int: "int", bool: "bool"}.get(self.type, str(self.type))
+        if kind != "float":
+            flags.append(kind)
+        if self.locality != "local":
+            flags.append("postsynaptic" if self.locality == "semiglobal" else "population")
+        return self.equation + (" : " + ", ".join(flags) if flags else "")
 
 
 class Neuron:

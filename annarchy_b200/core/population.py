@@ -108,6 +108,16 @@ class Population:
         return list(self.desc["attributes"])
 
     @property
+    def parameters(self):
+        """Names of the neuron's parameters (Population.py, `parameters`)."""
+        return [p["name"] for p in self.desc["parameters"]]
+
+    @property
+    def variables(self):
+        """Names of the neuron's variables (Population.py, `variables`)."""
+        return [v["name"] for v in self.desc["variables"]]
+
+    @property
     def ranks(self):
         return np.arange(self.size)
 
@@ -289,6 +299,15 @@ class Population:
 
     # -- views ----------------------------------------------------------------
     def __getitem__(self, idx):
+        """A rank, a slice or a list of ranks gives a view; coordinates
+        without slices give that neuron; coordinates with slices give the
+        view of the neurons they cover, in row-major order
+        (ANNarchy/core/Population.py:782-890)."""
+        if isinstance(idx, tuple):
+            if not any(isinstance(i, slice) for i in idx):
+                return self.neuron(idx)
+            grid = np.arange(self.size).reshape(tuple(self.geometry))
+            return PopulationView(self, np.asarray(grid[idx]).reshape(-1))
         ranks = np.arange(self.size)[idx]
         return PopulationView(self, np.atleast_1d(ranks))
 

@@ -1009,10 +1009,24 @@ class Dendrite:
     def __setattr__(self, name, value):
         self.set({name: value})
 
-    def synapse(self, pos: int):
-        if int(pos) not in self.pre_ranks:
+    def synapse(self, pos):
+        """The synapse from the pre-synaptic neuron of this rank or these
+        coordinates (ANNarchy/core/Dendrite.py:69-87); None without one."""
+        rank = int(pos) if isinstance(pos, (int, np.integer)) else \
+            self.proj.pre_pop.rank_from_coordinates(tuple(pos))
+        if rank not in self.pre_ranks:
             return None
-        return IndividualSynapse(self, pos)
+        return IndividualSynapse(self, rank)
+
+    def synapses(self):
+        """The dendrite's synapses in ascending pre-synaptic rank."""
+        return (IndividualSynapse(self, n) for n in self.pre_ranks)
+
+    def __getitem__(self, *args):
+        return self.synapse(args[0] if len(args) == 1 else args)
+
+    def __iter__(self):
+        return self.synapses()
 
     def receptive_field(self, variable: str = "w", fill: float = 0.0) -> np.ndarray:
         """The values over the pre-synaptic geometry (`fill` elsewhere)."""
