@@ -16,7 +16,7 @@ from .core.inputs import PoissonPopulation, TimedArray
 from .core.monitor import Monitor
 from .core.network import Constant, Network, every
 from .core.population import Population, PopulationView
-from .core.projection import Projection
+from .core.projection import LILConnectivity, Projection
 from .core.rate_batch import RateBatch
 from .core.random import (DiscreteUniform, Exponential, LogNormal, Normal, RandomDistribution,
                           Uniform)
@@ -28,4 +28,4 @@ __version__ = "0.1.0"
 __all__ = ["Network", "Neuron", "Synapse", "Population", "PopulationView", "Projection",
            "Monitor", "PoissonPopulation", "TimedArray", "Uniform", "Normal", "LogNormal", "Exponential", "DiscreteUniform",
            "RandomDistribution", "LeakyIntegrator", "IF_cond_exp", "STDP", "float32", "float64",
-           "Constant", "every", "RateBatch", "Parameter", "Variable"]
+           "Constant", "every", "RateBatch", "Parameter", "Variable", "LILConnectivity"]

@@ -180,13 +180,42 @@ class Projection:
                 raise ValueError(f"unknown storage format {storage_format!r}")
             self._storage_format = storage_format
         n_dend = int(np.count_nonzero(np.diff(m.indptr)))
-        for v in self.desc["variables"] + self.desc["parameters"]:
-            init = v["init"] if not isinstance(v["init"], str) else 0.0
+        params = {q["name"]: q for q in self.desc["parameters"]}
+        # parameters first: a variable may take its initial value from one
+        for v in self.desc["parameters"] + self.desc["variables"]:
+            init = v["init"]
+            if isinstance(init, str):
+                src = params.get(init)
+                if src is None:
+                    raise ValueError(f"init value {init!r} of {v['name']} is not a parameter")
+                init = self._host_attr.get(init, self._host_semi.get(init, src["init"]))
             if v["locality"] == "local" and v["name"] != "w":
-                self._host_attr[v["name"]] = np.full(m.nnz, float(init))
+                self._host_attr[v["name"]] = np.broadcast_to(
+                    np.asarray(init, dtype=np.float64), (m.nnz,)).copy()
             elif v["locality"] == "semiglobal":
-                self._host_semi[v["name"]] = np.full(n_dend, float(init))
+                self._host_semi[v["name"]] = np.broadcast_to(
+                    np.asarray(init, dtype=np.float64), (n_dend,)).copy()
         return self
+
+    def from_function(self, method, storage_format=None, storage_order=None, **args):
+        """Connectivity returned by a user function method(pre, post, dt,
+        **args) as a LILConnectivity (ANNarchy/core/ConnectorMethods.py:
+        456-530)."""
+        syn = method(self.pre, self.post, self._dt(), **args)
+        if not isinstance(syn, LILConnectivity):
+            raise TypeError("the connection method must return a LILConnectivity")
+        syn.validate()
+        delays = ([[syn.uniform_delay]] * len(syn.post_rank) if syn.uniform_delay != -1
+                  else syn.delay)
+        self._from_lil(syn.post_rank, syn.pre_rank, syn.w, delays, syn.requires_sorting)
+        self.connector_name = "User-defined"
+        if storage_format is not None:
+            if storage_format not in FORMATS:
+                raise ValueError(f"unknown storage format {storage_format!r}")
+            self._storage_format = storage_format
+        return self
+
+    connect_with_func = from_function
 
     def _weights(self, weights, nnz):
         return draw(weights, (nnz,), self._rng())
@@ -948,6 +977,55 @@ class Projection:
     def __repr__(self):
         return (f"Projection({self.name!r}, {self.pre_pop.name}->{self.post_pop.name}, "
                 f"target={self.target!r}, {self.nb_synapses} synapses, {self._storage_format})")
+
+
+class LILConnectivity:
+    """Connectivity built row by row by a user function (the reference's
+    ANNarchy/cython_ext/Connector.pyx:93-170): add(post_rank, pre_ranks,
+    weights, delays) with one weight for all the row's synapses or one per
+    synapse, delays in ms (one or one per synapse) kept in steps."""
+
+    def __init__(self, dt: float = 1.0):
+        self.dt = float(dt)
+        self.post_rank, self.pre_rank, self.w, self.delay = [], [], [], []
+        self.max_delay = 0
+        self.uniform_delay = -1
+        self.size = 0
+        self.nb_synapses = 0
+        self.requires_sorting = False
+        self._last = -1
+
+    def add(self, rank, ranks, w, d):
+        rank, ranks = int(rank), [int(r) for r in ranks]
+        w = [float(x) for x in np.atleast_1d(w)]
+        d = [float(x) for x in np.atleast_1d(d)]
+        if rank < self._last:
+            self.requires_sorting = True
+        else:
+            self._last = rank
+        if not ranks:
+            return
+        self.post_rank.append(rank)
+        self.pre_rank.append(ranks)
+        self.w.append(w if (len(w) > 1 or len(ranks) == 1) else [w[0]] * len(ranks))
+        steps = [int(round(x / self.dt)) for x in d]
+        self.delay.append(steps)
+        self.max_delay = max(self.max_delay, int(round(max(d) / self.dt)))
+        if len(d) > 1:
+            self.uniform_delay = -1
+        else:
+            u = int(round(d[0] / self.dt))
+            self.uniform_delay = -1 if (self.uniform_delay != u and self.size > 0) else u
+        self.size += 1
+        self.nb_synapses += len(ranks)
+
+    push_back = add
+
+    def validate(self):
+        """Each row's pre-synaptic ranks are distinct."""
+        for rank, ranks in zip(self.post_rank, self.pre_rank):
+            if len(set(ranks)) != len(ranks):
+                raise ValueError(f"LILConnectivity: the dendrite of {rank} has duplicate synapses")
 
 
 class IndividualSynapse:

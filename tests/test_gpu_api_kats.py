@@ -144,3 +144,85 @@ def test_dendrites_of_a_learning_synapse():
     np.testing.assert_array_equal(proj.tau, new)
     np.testing.assert_array_equal(proj.dendrite(1).get("tau"), 7000.0)
     net.close()
+
+
+def _sparse_4x8():
+    from scipy import sparse
+    wm = sparse.lil_matrix((4, 8))
+    for i in range(8):
+        wm[1, i] = 0.2
+    for i in range(2, 6):
+        wm[3, i] = 0.5
+    return wm.T
+
+
+@pytest.mark.parametrize("modified", [False, True])
+def test_projection_access(modified):
+    """Weights, dendrites, size and post ranks of a from_sparse projection;
+    with a synapse holding local, postsynaptic and projection-level
+    parameters and a variable initialised from a parameter
+    (tests_python/RateSynapse/test_Projection.py:15-230)."""
+    net = Network(dt=1.0, seed=1)
+    simple = Neuron(parameters="r=0")
+    syn = Synapse(parameters="""
+        loc_var        = 5000.0
+        semi_glob_var  = 8.0    : postsynaptic
+        glob_var       = 8.0    : projection
+    """, equations="""
+        dx/dt = -x              : init = loc_var
+        dw/dt = -w
+    """) if modified else None
+    proj = net.connect(net.create(8, simple), net.create(4, simple), "exc", synapse=syn)
+    proj.from_sparse(_sparse_4x8())
+    net.compile()
+    np.testing.assert_allclose(proj.w[0], 0.2)
+    np.testing.assert_allclose(proj.w[1], 0.5)
+    np.testing.assert_allclose(proj.dendrite(1).w, 0.2)
+    np.testing.assert_allclose(proj.dendrite(3).w, 0.5)
+    assert proj.size == 2 and list(proj.post_ranks) == [1, 3]
+    if modified:
+        np.testing.assert_array_equal(proj.loc_var[0], 5000.0)
+        np.testing.assert_array_equal(proj.get("loc_var")[1], 5000.0)
+        np.testing.assert_array_equal(proj.x[0], 5000.0)
+        np.testing.assert_array_equal(proj.semi_glob_var, 8.0)
+        np.testing.assert_array_equal(proj.get("glob_var"), 8.0)
+    net.close()
+
+
+def test_custom_connectivity_from_function():
+    """Diagonal bands built by user functions returning a LILConnectivity,
+    without delay, with a uniform delay of 2 ms and with per-synapse delays
+    DiscreteUniform(1, 5) (tests_python/RateSynapse/
+    test_RateCustomConnectivity.py:15-200); the sums of the band through
+    the projection without delay are checked after two steps."""
+    from annarchy_b200 import DiscreteUniform, LILConnectivity
+
+    def band(pre, post, dt, weight, delay=None):
+        syn = LILConnectivity(dt=dt)
+        for post_rk in post.ranks:
+            ranks = [r for r in (post_rk - 1, post_rk, post_rk + 1) if r in pre.ranks]
+            if delay is None:
+                d = [0]
+            elif isinstance(delay, (int, float)):
+                d = [delay]
+            else:
+                d = delay.get_values(len(ranks))
+            syn.add(post_rk, ranks, [weight] * len(ranks), d)
+        return syn
+
+    net = Network(dt=1.0, seed=1)
+    pop1 = net.create(5, Neuron(equations="r = 1"))
+    pop2 = net.create(5, Neuron(equations="r = sum(exc)"))
+    p0 = net.connect(pre=pop1, post=pop2, target="exc")
+    p0.from_function(method=band, weight=0.1)
+    p1 = net.connect(pre=pop1, post=pop2, target="exc2")
+    p1.from_function(method=band, weight=0.1, delay=2)
+    p2 = net.connect(pre=pop1, post=pop2, target="exc3")
+    p2.from_function(method=band, weight=0.1, delay=DiscreteUniform(1, 5))
+    net.compile()
+    assert p0.delay == 1.0 and p1.delay == 2.0
+    assert [list(d.pre_ranks) for d in p0.dendrites] == [[0, 1], [0, 1, 2], [1, 2, 3], [2, 3, 4],
+                                                          [3, 4]]
+    net.simulate(2)
+    np.testing.assert_allclose(np.ravel(pop2.r), [0.2, 0.3, 0.3, 0.3, 0.2], rtol=1e-12)
+    net.close()
