@@ -11,7 +11,8 @@ the ANNarchy neural simulator.
     net.simulate(1000.0)
     spikes = m.get("spike")
 """
-from .core.models import IF_cond_exp, LeakyIntegrator, Neuron, Parameter, STDP, Synapse, Variable
+from .core.models import (IF_cond_exp, LeakyIntegrator, Neuron, Parameter, STDP, Synapse, Variable,
+                          add_function, functions)
 from .core.inputs import PoissonPopulation, TimedArray
 from .core.monitor import Monitor
 from .core.network import Constant, Network, every
@@ -28,4 +29,5 @@ __version__ = "0.1.0"
 __all__ = ["Network", "Neuron", "Synapse", "Population", "PopulationView", "Projection",
            "Monitor", "PoissonPopulation", "TimedArray", "Uniform", "Normal", "LogNormal", "Exponential", "DiscreteUniform",
            "RandomDistribution", "LeakyIntegrator", "IF_cond_exp", "STDP", "float32", "float64",
-           "Constant", "every", "RateBatch", "Parameter", "Variable", "LILConnectivity"]
+           "Constant", "every", "RateBatch", "Parameter", "Variable", "LILConnectivity",
+           "add_function", "functions"]

@@ -19,6 +19,30 @@ from .random import RandomDistribution
 _DESC_CACHE: dict = {}
 
 
+def _global_functions_key():
+    from ..parser.equation import GLOBAL_FUNCTIONS
+    return tuple(sorted((k, v["cpp"]) for k, v in GLOBAL_FUNCTIONS.items()))
+
+
+def add_function(function: str):
+    """Define a function usable in every neuron and synapse defined
+    afterwards, e.g. ``add_function("sigmoid(x) = 1.0 / (1.0 + exp(-x))")``
+    (ANNarchy/core/Global.py, add_function)."""
+    from ..parser.analysis import analyse_functions
+    from ..parser.equation import GLOBAL_FUNCTIONS
+    for f in analyse_functions(function):
+        GLOBAL_FUNCTIONS[f["name"]] = f
+
+
+def functions(name: str):
+    """A function defined by add_function, as a host callable on arrays."""
+    from ..parser.equation import GLOBAL_FUNCTIONS
+    from .functions import evaluator
+    if name not in GLOBAL_FUNCTIONS:
+        raise KeyError(f"no function {name!r} was added")
+    return evaluator(GLOBAL_FUNCTIONS[name])
+
+
 def _cached(kind, key, analyse, model):
     key = (kind, repr(key))
     if key not in _DESC_CACHE:
@@ -75,8 +99,6 @@ class Neuron:
                  axon_reset=None, refractory=None, functions=None, name="", description=""):
         if axon_spike or axon_reset:
             raise NotImplementedError("axonal spikes are not supported by this backend")
-        if functions:
-            raise NotImplementedError("user functions are not supported by this backend")
         self.parameters = parameters
         self.equations = equations
         self.spike = spike
@@ -93,7 +115,8 @@ class Neuron:
         if self._desc is None:
             from ..parser.analysis import analyse_neuron
             self._desc = _cached("neuron", (self.parameters, self.equations, self.spike,
-                                            self.reset, self.refractory, self.type),
+                                            self.reset, self.refractory, self.type,
+                                            self.functions, _global_functions_key()),
                                  analyse_neuron, self)
         return self._desc
 
@@ -107,8 +130,8 @@ class Synapse:
                  creating=None, name=None, description=None):
         if operation != "sum":
             raise NotImplementedError("only operation='sum' is supported by this backend")
-        if pre_axon_spike or functions or pruning or creating:
-            raise NotImplementedError("axonal spikes, functions and structural plasticity are "
+        if pre_axon_spike or pruning or creating:
+            raise NotImplementedError("axonal spikes and structural plasticity are "
                                       "not supported by this backend")
         self.parameters = parameters
         self.equations = equations
@@ -116,6 +139,7 @@ class Synapse:
         self.operation = operation
         self.pre_spike = pre_spike
         self.post_spike = post_spike
+        self.functions = functions
         self.type = "spike" if (pre_spike or post_spike) else "rate"
         self.name = name or ("Spiking synapse" if self.type == "spike" else "Rate-coded synapse")
         self.description = description
@@ -126,7 +150,8 @@ class Synapse:
         if self._desc is None:
             from ..parser.analysis import analyse_synapse
             self._desc = _cached("synapse", (self.parameters, self.equations, self.psp,
-                                             self.pre_spike, self.post_spike, self.type),
+                                             self.pre_spike, self.post_spike, self.type,
+                                             self.functions, _global_functions_key()),
                                  analyse_synapse, self)
         return self._desc
 

@@ -135,6 +135,9 @@ class Population:
         host = object.__getattribute__(self, "_host")
         if name in host:
             return self.get(name)
+        fn = _model_function(self.desc, name)
+        if fn is not None:
+            return fn
         raise AttributeError(f"population {self.name!r} has no attribute {name!r}")
 
     def __setattr__(self, name, value):
@@ -338,6 +341,15 @@ class Population:
         if not self._compiled():
             return np.array([], dtype=np.int64)
         return self.net._backend.read_spiked(self)
+
+
+def _model_function(desc, name):
+    """A model's own user function as a host callable, or None."""
+    funcs = {f["name"]: f for f in desc.get("functions", [])}
+    if name not in funcs:
+        return None
+    from .functions import evaluator
+    return evaluator(funcs[name], {k: v for k, v in funcs.items() if k != name})
 
 
 class PopulationView:

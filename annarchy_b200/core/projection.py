@@ -730,6 +730,11 @@ class Projection:
                                  name in {p["name"] for p in desc["parameters"] + desc["variables"]
                                           if p["locality"] == "global"}):
             return self.get(name)
+        if desc is not None:
+            from .population import _model_function
+            fn = _model_function(desc, name)
+            if fn is not None:
+                return fn
         raise AttributeError(name)
 
     def __setattr__(self, name, value):

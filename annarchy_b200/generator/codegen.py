@@ -2203,12 +2203,32 @@ anb_cluster_run(long long t0, int nsteps) {{
             opts.append("-I" + cuda_inc)
         return opts
 
+    def user_functions(self) -> str:
+        """Device functions of the user functions the network's models use
+        (global ones from add_function, then the models' own)."""
+        from ..parser.equation import GLOBAL_FUNCTIONS
+        funcs: dict = {}
+        for f in GLOBAL_FUNCTIONS.values():
+            funcs[f["name"]] = f
+        for obj in list(self.net.populations) + list(self.net.projections):
+            for f in obj.desc.get("functions", []):
+                if f["name"] in funcs and funcs[f["name"]]["cpp"] != f["cpp"]:
+                    raise ValueError(f"two different functions named {f['name']!r}")
+                funcs[f["name"]] = f
+        out = []
+        for f in funcs.values():
+            args = ", ".join(f"{self.real} {a}" for a in f["args"])
+            out.append(f"__device__ __forceinline__ {self.real} {f['name']}({args}) {{ "
+                       f"return {self.typed(f['cpp'])}; }}")
+        return ("\n" + "\n".join(out)) if out else ""
+
     def assemble(self, kernels: list) -> str:
         header = open(DEVICE_HEADER).read()
         self.ptr("t")
         self.ptr("dt")
         self.ptr("err")
         decl = "\n".join(f"__constant__ {ct}* anb_p_{name};" for name, ct in sorted(self.decls.items()))
+        decl += self.user_functions()
         # network constants usable in every equation (set through anb_module_set_constant);
         # an attribute of the same name hides them, as in the reference
         consts = "".join(f"__constant__ {self.real} {c};\n" for c in sorted(self.net._constants))

@@ -17,12 +17,13 @@ become C conditionals as in ANNarchy/parser/ITE.py; ``ite(c, a, b)`` is a
 function of the device header.
 
 Not supported by this backend (an error names them): global operations
-(``mean(r)``...), user functions, coupled implicit/midpoint/rk4 systems.
+(``mean(pre.r)`` in synapses), coupled implicit/midpoint/rk4 systems.
 """
 from __future__ import annotations
 
 import re
 
+from . import equation as _eq
 from .equation import BUILTIN_FUNCTIONS, Statement
 from .text import ParserError, equation_list, lhs_name, parse_flags, split_flags, statements
 
@@ -305,6 +306,48 @@ def _bound_code(name, value, desc, untouched):
 # neurons
 # ---------------------------------------------------------------------------
 
+def analyse_functions(text) -> list:
+    """User functions ``name(a, b) = expression`` (one per line, branches
+    with if/else allowed; ANNarchy/parser/Function.py and the reference's
+    add_function): the arguments are plain symbols, the body a C
+    expression; the description keeps what a host evaluator needs."""
+    out = []
+    if not text:
+        return out
+    empty = {"attributes": [], "local": [], "semiglobal": [], "global": []}
+    for line in (x.strip() for x in str(text).split("\n")):
+        if not line or line.startswith("#"):
+            continue
+        m = re.match(r"^(\w+)\s*\(([^()]*)\)\s*=(.*)$", line)
+        if not m:
+            raise ParserError("a function must be defined as name(arguments) = expression: " + line)
+        name, rhs = m.group(1), m.group(3).strip()
+        args = [a.strip() for a in m.group(2).split(",") if a.strip()]
+        eq, conditions = _extract_ite(rhs, split=False)
+        code, _ = _ite_statement(name, eq, conditions, empty, {a: a for a in args},
+                                 kind="return")
+        out.append({"name": name, "args": args, "cpp": code.strip().rstrip(";").strip(),
+                    "eq": eq, "conditions": conditions})
+    return out
+
+
+def _with_functions(analyse):
+    """Run a model's analysis with its own functions visible to the
+    parser; the description lists them under "functions"."""
+    def run(model):
+        funcs = analyse_functions(getattr(model, "functions", None))
+        token = _eq._SCOPE_FUNCTIONS.set(tuple(f["name"] for f in funcs))
+        try:
+            desc = analyse(model)
+        finally:
+            _eq._SCOPE_FUNCTIONS.reset(token)
+        desc["functions"] = funcs
+        return desc
+    run.__doc__ = analyse.__doc__
+    return run
+
+
+@_with_functions
 def analyse_neuron(neuron) -> dict:
     """Description dict of a neuron type (AnalyseNeuron.py:27-392)."""
     desc = {"object": "neuron", "type": neuron.type, "raw_parameters": neuron.parameters,
@@ -440,6 +483,7 @@ def _event_statements(raw):
     return out
 
 
+@_with_functions
 def analyse_synapse(synapse) -> dict:
     """Description dict of a synapse type (AnalyseSynapse.py:34-590)."""
     desc = {"object": "synapse", "type": synapse.type, "raw_parameters": synapse.parameters,

@@ -16,6 +16,7 @@ decay of synaptic traces (Equation.py:606-660).
 """
 from __future__ import annotations
 
+import contextvars
 import re
 
 import sympy as sp
@@ -55,6 +56,16 @@ C_FUNCTION_NAMES = {
     "modulo": "modulo", "fabs": "fabs", "clip": "clip", "ite": "ite", "power": "power",
     "isfinite": "isfinite", "isnan": "isnan",
 }
+
+
+# user functions visible to the statements being parsed: the global ones
+# (add_function) and those of the model under analysis
+GLOBAL_FUNCTIONS: dict = {}
+_SCOPE_FUNCTIONS = contextvars.ContextVar("anb_scope_functions", default=())
+
+
+def user_function_names() -> tuple:
+    return tuple(GLOBAL_FUNCTIONS) + tuple(_SCOPE_FUNCTIONS.get())
 
 
 def symbol_table(local, semiglobal, global_, untouched, functions=(), constants=()):
@@ -97,6 +108,7 @@ class Statement:
         self.desc = desc
         self.attributes = list(desc["attributes"])
         self.functions = dict(C_FUNCTION_NAMES)
+        functions = tuple(functions) + user_function_names()
         for f in functions:
             self.functions[f] = f
         self.table = symbol_table(desc["local"], desc["semiglobal"], desc["global"],

@@ -466,3 +466,30 @@ def test_global_operations(precision):
                                else vals.max(), rtol=tol)
     np.testing.assert_allclose(np.asarray(large.l2), np.linalg.norm(vals), rtol=tol * 10)
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_user_functions_in_equations(precision):
+    """A neuron's own function with nested branches and a global one from
+    add_function, evaluated in the update kernel (tests_python/Common/
+    test_CustomFunc.py): inputs -2, 0.5, 1.5 and 3 through one-to-one
+    weights of 1."""
+    from annarchy_b200 import add_function
+    add_function("glob_pos(x) = pos(x)")
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    inp = net.create(4, Neuron(parameters="r = 0.0"))
+    tf = net.create(4, Neuron(equations="r = transfer_function(sum(exc), 1.0)",
+                              functions="transfer_function(x, t) = if x > t: if x > 2*t : "
+                                        "(x - 2*t)^2 else: x - t else: 0."))
+    gp = net.create(4, Neuron(equations="r = glob_pos(sum(exc))"))
+    net.connect(inp, tf, "exc").one_to_one(1.0)
+    net.connect(inp, gp, "exc").one_to_one(1.0)
+    net.compile()
+    inp.r = [-2.0, 0.5, 1.5, 3.0]
+    net.simulate(1)
+    np.testing.assert_allclose(np.ravel(tf.r), [0.0, 0.0, 0.5, 1.0], rtol=1e-7)
+    np.testing.assert_allclose(np.ravel(gp.r), [0.0, 0.5, 1.5, 3.0], rtol=1e-7)
+    np.testing.assert_allclose(tf.transfer_function([-2.0, 0.5, 1.5, 3.0], [1.0] * 4),
+                               [0.0, 0.0, 0.5, 1.0])
+    net.close()
