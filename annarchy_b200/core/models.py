@@ -128,8 +128,8 @@ class Synapse:
     def __init__(self, parameters="", equations="", psp=None, operation="sum", pre_spike=None,
                  post_spike=None, pre_axon_spike=None, functions=None, pruning=None,
                  creating=None, name=None, description=None):
-        if operation != "sum":
-            raise NotImplementedError("only operation='sum' is supported by this backend")
+        if operation not in ("sum", "max", "min", "mean"):
+            raise ValueError(f"operation {operation!r}: sum, max, min or mean")
         if pre_axon_spike or pruning or creating:
             raise NotImplementedError("axonal spikes and structural plasticity are "
                                       "not supported by this backend")

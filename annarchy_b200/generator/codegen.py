@@ -768,18 +768,22 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
     # ------------------------------------------------- rate-coded learning
     @staticmethod
     def custom_psp(proj) -> bool:
-        """A rate-coded synapse whose psp is not w * pre.r."""
+        """A rate-coded synapse whose psp is not w * pre.r, or whose
+        operation over the synapses is not a sum."""
         if proj.synapse_type.type != "rate":
             return False
+        if getattr(proj.synapse_type, "operation", "sum") != "sum":
+            return True
         eq = proj.desc.get("psp", {}).get("eq", "w*pre.r").replace(" ", "")
         return eq not in ("w*pre.r", "pre.r*w")
 
     def custom_psp_kernel(self, proj) -> str:
-        """Weighted sum with the synapse's own psp expression
-        (ANNarchy/generator/Projection/OpenMP/CSR.py:177-253 with the psp
-        code in place of w * pre.r): thread per post row, the terms added in
-        stored (ascending pre rank) order, then the row's sum added to the
-        target's sum."""
+        """Weighted sum with the synapse's own psp expression and operation
+        (ANNarchy/generator/Projection/OpenMP/CSR.py:177-253): thread per
+        post row over its synapses in stored (ascending pre rank) order -
+        the terms added (sum), their largest or smallest starting from the
+        first synapse's (max, min), or their sum over the row's synapse
+        count (mean) - then added to the target's sum."""
         k = proj.id
         lay = self.c.layout[k]
         a, b = proj.pre_pop, proj.post_pop
@@ -806,6 +810,20 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
         sum_ = self.ptr(f"pop{b.id}___sum_{proj.target}")
         rp_t = lay["idx_t"]
         nl = "\n    "
+        op = getattr(proj.synapse_type, "operation", "sum")
+        beg, end = "anb_rp[anb_row]", "anb_rp[anb_row + 1]"
+        if op in ("max", "min"):
+            cmp = ">" if op == "max" else "<"
+            reduce = (f"{self.real} anb_s = ({self.real})0;\n      if ({beg} < {end}) {{\n"
+                      f"        {{ const {rp_t} j = {beg}; anb_s = {expr}; }}\n"
+                      f"        for ({rp_t} j = {beg} + 1; j < {end}; ++j) {{\n"
+                      f"          const {self.real} anb_v = {expr};\n"
+                      f"          if (anb_v {cmp} anb_s) anb_s = anb_v;\n        }}\n      }}")
+        else:
+            reduce = (f"{self.real} anb_s = ({self.real})0;\n"
+                      f"      for ({rp_t} j = {beg}; j < {end}; ++j) anb_s += {expr};")
+            if op == "mean":
+                reduce += f"\n      if ({end} > {beg}) anb_s /= ({self.real})({end} - {beg});"
         return f"""
 extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     const long long t = *{self.ptr('t')};
@@ -817,8 +835,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
     for (int anb_row = blockIdx.x * blockDim.x + threadIdx.x; anb_row < {lay['rows']};
          anb_row += gridDim.x * blockDim.x) {{
       const int anb_post = {p('post_rank')}[anb_row];
-      {self.real} anb_s = ({self.real})0;
-      for ({rp_t} j = anb_rp[anb_row]; j < anb_rp[anb_row + 1]; ++j) anb_s += {expr};
+      {reduce}
       {sum_}[anb_post] += anb_s;
     }}
 }}

@@ -493,3 +493,26 @@ def test_user_functions_in_equations(precision):
     np.testing.assert_allclose(tf.transfer_function([-2.0, 0.5, 1.5, 3.0], [1.0] * 4),
                                [0.0, 0.0, 0.5, 1.0])
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_rate_synapse_operations(precision):
+    """max, min and mean instead of the sum over a row's synapses
+    (tests_python/RateSynapse/test_RateDelays.py:405-520, weights 1.0): the
+    three sums equal the largest, smallest and mean pre-synaptic rate."""
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    inp = net.create((3, 3), Neuron(parameters="r=0.0"))
+    out = net.create(4, Neuron(equations="r = sum(p1) + sum(p2)"))
+    for target, op in (("p1", "max"), ("p2", "min"), ("p3", "mean")):
+        net.connect(inp, out, target, synapse=Synapse(psp="pre.r * w", operation=op)).all_to_all(
+            weights=1.0)
+    net.compile()
+    pre_r = np.random.default_rng(5).random((3, 3))
+    inp.r = pre_r
+    net.simulate(1)
+    tol = 1e-12 if precision == "double" else 1e-6
+    np.testing.assert_allclose(out.sum("p1"), pre_r.max(), rtol=tol)
+    np.testing.assert_allclose(out.sum("p2"), pre_r.min(), rtol=tol)
+    np.testing.assert_allclose(out.sum("p3"), pre_r.mean(), rtol=tol)
+    net.close()
