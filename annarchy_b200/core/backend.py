@@ -255,7 +255,7 @@ class CompiledNetwork:
             return False, "device-generated connectivity"
         if any(v != "spike" for m in net.monitors for v in m.variables):
             return False, "variable monitors"
-        if any(global_equations(p) or p.desc.get("global_operations") for p in net.populations):
+        if any(global_equations(p) or p._globalops for p in net.populations):
             return False, "population-level variables with equations or global operations"
         smem = self._local_smem_bytes()
         if smem > LOCAL_SMEM_LIMIT:

@@ -43,12 +43,9 @@ class Population:
             self._ctype[p["name"]] = p.get("ctype", "double")
         for p in self.desc["parameters"] + self.desc["variables"]:
             self._host[p["name"]] = self._initial(p)
+        self._globalops = []
         for op in self.desc.get("global_operations", []):
-            # the population-wide reduction of the previous step
-            name = "_" + op["function"] + "_" + op["variable"]
-            self._host[name] = np.float64(0.0)
-            self._locality[name] = "global"
-            self._ctype[name] = "double"
+            self._add_globalop(op)
         if self.neuron_type.type == "rate":
             for t in self.targets:
                 self._host["_sum_" + t] = np.zeros(self.size)
@@ -58,6 +55,20 @@ class Population:
         self._refractory_ms = np.full(self.size, float(refr or 0.0))
         self._has_refractory = bool(refr)
         object.__setattr__(self, "_ready", True)
+
+    def _add_globalop(self, op: dict):
+        """A population-wide reduction (the previous step's value) that the
+        neuron's or a projection's equations use: `_<op>_<variable>`."""
+        if op["variable"] not in self.desc["local"]:
+            raise ValueError(f"{op['function']}({op['variable']}): {op['variable']!r} is not a "
+                             f"local attribute of {self.name!r}")
+        if op in self._globalops:
+            return
+        self._globalops.append(dict(op))
+        name = "_" + op["function"] + "_" + op["variable"]
+        self._host[name] = np.float64(0.0)
+        self._locality[name] = "global"
+        self._ctype[name] = "double"
 
     def _add_spike_target(self, target: str):
         """A projection's target that the spiking neuron's equations do not

@@ -59,6 +59,10 @@ class Projection:
             raise TypeError("a spiking synapse needs a spiking pre-synaptic population")
         if synapse.type == "rate" and pre_type != "rate":
             raise TypeError("a rate-coded synapse needs a rate-coded pre-synaptic population")
+        # reductions of the pre/post populations used by the synapse
+        for side, pop in (("pre", self.pre_pop), ("post", self.post_pop)):
+            for op in self.desc.get(side + "_global_operations", []):
+                pop._add_globalop(op)
         if self.post_pop.neuron_type.type == "rate" and target not in self.post_pop.targets:
             # a rate-coded target the neuron does not sum: its weighted sum is
             # still computed (ANNarchy/core/Projection.py:105-110 adds the

@@ -296,7 +296,7 @@ class CodeGenerator:
                 ct = "int" if p.get("ctype") in ("int", "bool") else self.real
                 const = "" if p["name"] in evolving else "const "
                 out.append(f"{const}{ct} {p['name']} = {src(p['name'])}[0];")
-        for op in pop.desc.get("global_operations", []):
+        for op in pop._globalops:
             name = "_" + op["function"] + "_" + op["variable"]
             out.append(f"const {self.real} {name} = {src(name)}[0];")
         for n in self._reciprocals(pop):
@@ -669,7 +669,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_step() {{
         n = pop.size
         R = self.real
         outs = []
-        for op in pop.desc["global_operations"]:
+        for op in pop._globalops:
             f, v = op["function"], op["variable"]
             outs.append((f, self.ptr(f"pop{k}__{v}"), self.ptr(f"pop{k}___{f}_{v}")))
         if self.exact:
@@ -806,6 +806,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) pop{k}_stop() {{
                                               f"of {pop.name}")
                 ct = "int" if pop._ctype.get(n) in ("int", "bool") else self.real
                 decl.append(f"const {ct}* __restrict__ {prefix}{n} = {self.ptr(f'pop{pop.id}__{n}')};")
+        decl += self._globalop_refs(proj, expr)
         dt_t = "double" if self.exact else "float"
         sum_ = self.ptr(f"pop{b.id}___sum_{proj.target}")
         rp_t = lay["idx_t"]
@@ -972,7 +973,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) proj{k}_psp() {{
                     ct = "int" if pop._ctype.get(n) in ("int", "bool") else self.real
                     decl.append(f"const {ct}* __restrict__ {prefix}{n} = "
                                 f"{self.ptr(f'pop{pop.id}__{n}')};")
-            return "\n    ".join(decl)
+            return "\n    ".join(decl + self._globalop_refs(proj, code))
 
         if glob_eq.strip():
             code = self.typed(self.fill(glob_eq, post_prefix="anb_post_", post_index="[0]"))
@@ -1440,6 +1441,17 @@ __device__ __forceinline__ void proj{k}_post_prev_body(const long long anb_pt) {
                     raise NotImplementedError(f"{proj.name}: {prefix[4:-1]}.{n} is not an attribute "
                                               f"of {pop.name}")
                 decl.append(f"const {ct}* __restrict__ {prefix}{n} = {self.ptr(f'pop{pop.id}__{n}')};")
+        return decl + self._globalop_refs(proj, code)
+
+    def _globalop_refs(self, proj, code: str) -> list:
+        """Scalars of the pre/post populations' reductions a synaptic
+        statement reads (`anb_pre__mean_r`: the value after the previous
+        step)."""
+        decl = []
+        for prefix, pop in (("anb_pre_", proj.pre_pop), ("anb_post_", proj.post_pop)):
+            for n in sorted(set(re.findall(prefix + r"_(\w+)\b(?!\s*\[)", code))):
+                if "_" + n in pop._host and pop._locality.get("_" + n) == "global":
+                    decl.append(f"const {self.real} {prefix}_{n} = {self.ptr(f'pop{pop.id}___{n}')}[0];")
         return decl
 
     @staticmethod
@@ -1649,7 +1661,7 @@ extern "C" __global__ void __launch_bounds__({BLOCK}) mon{m}_record{'_targets' i
             return False
         if any(getattr(p, "stop_condition", None) or hasattr(p, "_ta_schedule_ms")
                or p.neuron_type.type != "spike" or self.slots(p) > 1 or global_equations(p)
-               or p.desc.get("global_operations") for p in net.populations):
+               or p._globalops for p in net.populations):
             return False
         return True
 
@@ -1764,7 +1776,7 @@ extern "C" __global__ void __launch_bounds__({PERSISTENT_BLOCK}, 1) anb_grid_run
                 lo, hi = getattr(self.c, "owned", {}).get(pop.id, (0, pop.size))
                 K = self.neurons_per_thread(pop)
                 plan.append((f"pop{pop.id}_step", grid_for(max(1, -(-(hi - lo) // K))), BLOCK, 0))
-            if pop.desc.get("global_operations"):
+            if pop._globalops:
                 kernels.append(self.globalops_kernel(pop))
                 plan.append((f"pop{pop.id}_globalops", 1, 32 if self.exact else 1024, 0))
             elif pop.neuron_type.type == "rate" and self.slots(pop) > 1:

@@ -205,6 +205,26 @@ def _extract_globalops(eq, desc, where):
     return eq, untouched
 
 
+def _extract_globalops_synapse(eq, desc, where):
+    """Reductions of the pre- or post-synaptic population in a synaptic
+    equation (``mean(pre.r)``, ``max(post.v)``; ANNarchy/parser/
+    Extraction.py:148-190): replaced by that population's scalar
+    `%(pre_prefix)s_<op>_<var>` and listed in desc["pre_global_operations"] /
+    desc["post_global_operations"]."""
+    untouched = {}
+    for op in GLOBAL_OPERATIONS:
+        for side in ("pre", "post"):
+            for var in re.findall(r"(?<![\w.])" + op + r"\(\s*" + side + r"\.([\w]+)\s*\)", eq):
+                new = "__" + side + "_" + op + "_" + var
+                eq = re.sub(op + r"\(\s*" + side + r"\." + var + r"\s*\)", new, eq)
+                untouched[new] = "%(" + side + "_prefix)s_" + op + "_" + var
+                item = {"function": op, "variable": var}
+                lst = desc.setdefault(side + "_global_operations", [])
+                if item not in lst:
+                    lst.append(item)
+    return eq, untouched
+
+
 def _unsupported(eq, where, neuron=False):
     if not neuron and re.search(r"\b(mean|min|max|norm1|norm2)\(", eq):
         raise ParserError(f"{where}: global operations in synapses are not supported by this "
@@ -529,6 +549,8 @@ def analyse_synapse(synapse) -> dict:
         rand_untouched = {}
         eq = _extract_random(" " + eq + " ", var, randoms, rand_untouched)
         untouched_all.update(rand_untouched)
+        eq, glob_untouched = _extract_globalops_synapse(eq, desc, var["name"])
+        untouched_all.update(glob_untouched)
         _unsupported(eq, var["name"])
         eq, untouched = _prepost(eq)
         for k, v in untouched.items():
@@ -552,7 +574,10 @@ def analyse_synapse(synapse) -> dict:
         if method in ("implicit", "semiimplicit", "midpoint", "rk4") and switch is not None:
             raise ParserError(f"{var['name']}: method {method!r} is not supported by this backend")
     if "raw_psp" in desc:
-        eq, untouched = _prepost(" " + desc["raw_psp"].strip() + " ")
+        eq, glob_untouched = _extract_globalops_synapse(" " + desc["raw_psp"].strip() + " ", desc,
+                                                        "psp")
+        untouched_all.update(glob_untouched)
+        eq, untouched = _prepost(eq)
         for k, v in untouched.items():
             untouched_all.setdefault(k, v)
         eq, conditions = _extract_ite(eq, split=False)

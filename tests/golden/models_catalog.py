@@ -111,3 +111,9 @@ SYNAPSES = {
         """),
     "spike_default": dict(pre_spike="g_target += w"),
 }
+
+# reductions of the pre- and post-synaptic populations in a learning rule
+# (the covariance synapse of the reference's test_RateDelays.py)
+SYNAPSES["covariance"] = dict(parameters="tau = 5000.0", equations="""
+            tau * dw/dt = (pre.r - mean(pre.r) ) * (post.r - mean(post.r) )
+        """)

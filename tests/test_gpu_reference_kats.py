@@ -516,3 +516,29 @@ def test_rate_synapse_operations(precision):
     np.testing.assert_allclose(out.sum("p2"), pre_r.min(), rtol=tol)
     np.testing.assert_allclose(out.sum("p3"), pre_r.mean(), rtol=tol)
     net.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_covariance_rule_with_population_means(precision):
+    """mean(pre.r) and mean(post.r) in a learning rule (the covariance
+    synapse of tests_python/RateSynapse/test_RateDelays.py:530-570, compiled
+    there; here run): the means are those after the previous step (0 in
+    step 0), so after two steps w = 1 + dt/tau * (pre.r * post.r
+    + (pre.r - mean pre) * (post.r - mean post))."""
+    from models_catalog import SYNAPSES
+    net = Network(dt=1.0, seed=1)
+    net.config(precision=precision)
+    neuron = Neuron(parameters="r=0")
+    pre = net.create(6, neuron)
+    post = net.create(2, neuron)
+    proj = net.connect(pre, post, "exc", synapse=Synapse(**SYNAPSES["covariance"]))
+    proj.all_to_all(weights=1.0)
+    net.compile()
+    pr = np.random.default_rng(9).random(6)
+    po = np.array([1.0, 3.0])
+    pre.r, post.r = pr, po
+    net.simulate(2)
+    w = np.asarray(proj.get("w", flat=True)).reshape(2, 6)
+    expected = 1.0 + (np.outer(po, pr) + np.outer(po - po.mean(), pr - pr.mean())) / 5000.0
+    np.testing.assert_allclose(w, expected, rtol=1e-12 if precision == "double" else 1e-6)
+    net.close()
