@@ -53,7 +53,7 @@ MODEL_STEPS = 10000
 # DRAM bytes (read + write) per launch of the bench's dominant kernel, from one
 # ncu capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum),
 # keyed by (kernel, precision)
-NCU_TRAFFIC = {("anb_cluster_run", "float"): 1.193472e6, ("anb_cluster_run", "double"): 1.563008e6}
+NCU_TRAFFIC = {("anb_cluster_run", "float"): 1.193472e6, ("anb_cluster_run", "double"): 1.602304e6}
 
 
 def dist_env():
