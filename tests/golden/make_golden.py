@@ -521,6 +521,32 @@ def case_spiking_continuous(name, steps=30):
                         w_pre_post=np.asarray(rows))
 
 
+def case_covariance(name, steps=3):
+    """The covariance rule with the pre/post population means
+    (models_catalog "covariance"): six pre neurons with random rates, two
+    post neurons with rates 1 and 3, weights after each step."""
+    import numpy as np
+    import ANNarchy as ann
+    from models_catalog import SYNAPSES
+    net = ann.Network(dt=1.0, seed=1)
+    net.config(num_threads=1)
+    neuron = ann.Neuron(parameters="r=0")
+    pre = net.create(6, neuron)
+    post = net.create(2, neuron)
+    proj = net.connect(pre, post, "exc", synapse=ann.Synapse(**SYNAPSES["covariance"]))
+    proj.all_to_all(weights=1.0)
+    net.compile(directory=os.path.join(WORK, "net_" + name), compiler_flags=FLAGS, silent=True)
+    pr = np.random.default_rng(9).random(6)
+    pre.r = pr
+    post.r = np.array([1.0, 3.0])
+    ws = []
+    for _ in range(steps):
+        net.simulate(1)
+        ws.append(np.array([np.asarray(d, dtype=np.float64) for d in proj.w]))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), pre_r=pr, post_r=np.array([1.0, 3.0]),
+                        w=np.asarray(ws))
+
+
 CASES = {
     "parser_strings": (case_parser, dict()),
     "rate_small": (case_rate, dict(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100,
@@ -538,6 +564,7 @@ CASES = {
     "self_connections": (case_self_connections, {}),
     "stp_small": (case_stp, dict(seed=5, n=400, p=0.05, steps=2000, g_every=50)),
     "spiking_continuous": (case_spiking_continuous, {}),
+    "covariance": (case_covariance, {}),
 }
 
 

@@ -519,13 +519,16 @@ def test_rate_synapse_operations(precision):
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
-def test_covariance_rule_with_population_means(precision):
+def test_covariance_rule_with_population_means(golden, precision):
     """mean(pre.r) and mean(post.r) in a learning rule (the covariance
     synapse of tests_python/RateSynapse/test_RateDelays.py:530-570, compiled
-    there; here run): the means are those after the previous step (0 in
-    step 0), so after two steps w = 1 + dt/tau * (pre.r * post.r
-    + (pre.r - mean pre) * (post.r - mean post))."""
+    there; here run): weights after each of three steps against the
+    reference's own run of the same network (tests/golden/covariance.npz,
+    made by make_golden.py). The means already hold the rates set before
+    the first step, so each step adds dt/tau * (pre.r - mean pre) *
+    (post.r - mean post)."""
     from models_catalog import SYNAPSES
+    gold = golden("covariance")
     net = Network(dt=1.0, seed=1)
     net.config(precision=precision)
     neuron = Neuron(parameters="r=0")
@@ -534,11 +537,9 @@ def test_covariance_rule_with_population_means(precision):
     proj = net.connect(pre, post, "exc", synapse=Synapse(**SYNAPSES["covariance"]))
     proj.all_to_all(weights=1.0)
     net.compile()
-    pr = np.random.default_rng(9).random(6)
-    po = np.array([1.0, 3.0])
-    pre.r, post.r = pr, po
-    net.simulate(2)
-    w = np.asarray(proj.get("w", flat=True)).reshape(2, 6)
-    expected = 1.0 + (np.outer(po, pr) + np.outer(po - po.mean(), pr - pr.mean())) / 5000.0
-    np.testing.assert_allclose(w, expected, rtol=1e-12 if precision == "double" else 1e-6)
+    pre.r, post.r = gold["pre_r"], gold["post_r"]
+    for step in range(gold["w"].shape[0]):
+        net.simulate(1)
+        w = np.asarray(proj.get("w", flat=True)).reshape(2, 6)
+        np.testing.assert_allclose(w, gold["w"][step], rtol=1e-12 if precision == "double" else 1e-6)
     net.close()
