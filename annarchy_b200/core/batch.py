@@ -23,8 +23,8 @@ import re
 
 import numpy as np
 
-from ..runtime.lib import NativeNet, DryNative, device_sm_count
-from ..generator.codegen import compensated_vars
+from ..runtime.lib import NativeNet, DryNative, bank_interleave, device_sm_count
+from ..generator.codegen import compensated_vars, global_equations
 from .backend import BF16, MAX_MONITOR_BYTES, to_bf16
 
 # opt-in dynamic shared memory of one CTA on sm_100 (227 KB)
@@ -171,6 +171,9 @@ class Batch:
         for p in self.net.populations:
             if p.desc.get("random_distributions"):
                 raise NotImplementedError("batched instances draw no random numbers in equations")
+            if global_equations(p) or p._globalops:
+                raise NotImplementedError("batched instances evaluate no population-level "
+                                          "equations or global operations")
 
     # -------------------------------------------------------------- layout
     def _smem_arrays(self, pop):
@@ -186,7 +189,10 @@ class Batch:
             if p["locality"] == "local" and p["name"] in used:
                 ct = "int" if p.get("ctype") in ("int", "bool") else ("double" if self.exact else "float")
                 out.append((p["name"], ct))
-        out.append(("refractory_remaining", "int"))
+        # the refractory counter in 16 bits when every period fits
+        j = self.net.populations.index(pop)
+        rmax = max(int(np.max(n.populations[j].refractory_steps, initial=0)) for n in self.networks)
+        out.append(("refractory_remaining", "short" if rmax < 32768 else "int"))
         for name in compensated_vars(pop, self.exact, self.comp_config(pop)):
             out.append(("kc_" + name, "float"))
         out.append(("spk", "anb_u32"))
@@ -198,9 +204,33 @@ class Batch:
         names = [v["name"] for v in pop.desc["variables"] if not v["name"].startswith("g_")]
         return {"compensate": names}
 
+    def header_layout(self):
+        """The per-slot quantities that a launch copies once into shared
+        memory (so that no step reads them from global memory): 64-bit
+        offsets, global parameter values and 32-bit entries, each a list of
+        (key, global array, index within the slot's row of that array).
+        Returns (longs, reals, ints, bytes per slot)."""
+        longs, reals, ints = [], [], []
+        for pop in self.net.populations:
+            k = pop.id
+            longs += [(f"goff{k}", f"pop{k}__bgoff", 1, 0), (f"woff{k}", f"pop{k}__bwoff", 1, 0)]
+            ints += [(f"n{k}", f"pop{k}__bn", 1, 0), (f"refr{k}", f"pop{k}__brefr", 1, 0)]
+            for p in pop.desc["parameters"] + pop.desc["variables"]:
+                if p["locality"] == "global":
+                    entry = (f"p{k}_{p['name']}", f"pop{k}__{p['name']}", 1, 0)
+                    (ints if p.get("ctype") in ("int", "bool") else reals).append(entry)
+        for proj in self.net.projections:
+            k = proj.id
+            longs.append((f"cp{k}", f"proj{k}__bcpoff", 1, 0))
+            ints += [(f"wr{k}_0", f"proj{k}__bwr", 2, 0), (f"wr{k}_1", f"proj{k}__bwr", 2, 1)]
+        ints += [(f"so{c}", "bt__soff", self.n_arrays, c) for c in range(self.n_arrays)]
+        rs = 8 if self.exact else 4
+        nbytes = -(-(8 * len(longs) + rs * len(reals) + 4 * len(ints)) // 16) * 16
+        return longs, reals, ints, nbytes
+
     @staticmethod
     def _csize(ct):
-        return {"double": 8, "float": 4, "int": 4, "anb_u32": 4}[ct]
+        return {"double": 8, "float": 4, "int": 4, "short": 2, "anb_u32": 4}[ct]
 
     def _instance_bytes(self, net):
         """Shared-memory byte offsets of every array of one instance."""
@@ -255,9 +285,20 @@ class Batch:
                 self.array_index[(pop.id, name)] = len(self.array_index)
         self.n_arrays = len(self.array_index)
         inst = [self._instance_bytes(n) for n in nets]
-        sizes = [b for _, b in inst]
-        # fast mode keeps room for the delivery scratch (at least 512 list entries)
-        limit = SMEM_LIMIT - (0 if self.exact else 4 * (32 + 512))
+        # every instance also takes one header slot at the start of its CTA's
+        # shared memory
+        self.header_bytes = self.header_layout()[3]
+        sizes = [b + self.header_bytes for _, b in inst]
+        # synapse indices in 32 bits while every projection's concatenation fits
+        tot = max([sum(n.projections[j].nb_synapses for n in nets)
+                   for j in range(len(self.net.projections))] or [0])
+        self.idx_t = "int" if tot + 8 < 2**31 - 1 else "long long"
+        # fast mode keeps room for the delivery scratch: 32 warp sums, the
+        # list counter, then at least 512 list entries, each with its
+        # synapse range in every projection
+        isz = 4 if self.idx_t == "int" else 8
+        self.entry_bytes = 4 + 2 * isz * len(self.net.projections)
+        limit = SMEM_LIMIT - (0 if self.exact else 4 * 36 + 512 * self.entry_bytes + 16)
         if max(sizes) > limit:
             i = int(np.argmax(sizes))
             raise ValueError(f"instance {i} needs {sizes[i]} bytes of shared memory "
@@ -277,23 +318,26 @@ class Batch:
         self.n_cta = n_cta
         self.cta_load = np.bincount(where, weights=costs, minlength=n_cta)
         nat.create("bt__cta", cta)
-        # shared-memory offsets: the instances of a CTA one after the other
+        # shared-memory offsets: the header slots of the CTA's instances, then
+        # the instances' arrays one after the other
         soff = np.empty((len(nets), self.n_arrays), dtype=np.int64)
         for c in range(n_cta):
-            base = 0
+            base = (cta[c + 1] - cta[c]) * self.header_bytes
             for s in range(cta[c], cta[c + 1]):
                 i = order[s]
                 soff[s] = np.asarray(inst[i][0], dtype=np.int64) + base
-                base += sizes[i]
+                base += inst[i][1]
         assert soff.max() < SMEM_LIMIT
         nat.create("bt__soff", soff.astype(np.int32))
-        self.native_soff, self.cta, self.inst_bytes = soff, cta, sizes
-        # state of the CTA's instances, then (fast mode) the delivery scratch:
-        # 32 warp sums and a spike list of list_cap entries
+        self.native_soff, self.cta, self.inst_bytes = soff, cta, [b for _, b in inst]
+        self.max_slots = int(np.diff(cta).max())
+        # state of the CTA's instances, then (fast mode) the delivery scratch
+        # with a list of list_cap entries (a multiple of 4)
         self.smem_state = -(-int(max(np.bincount(where, weights=sizes, minlength=n_cta))) // 16) * 16
-        self.list_cap = 0 if self.exact else int(min(1024, (SMEM_LIMIT - self.smem_state) // 4 - 32))
+        free = SMEM_LIMIT - self.smem_state - 4 * 36
+        self.list_cap = 0 if self.exact else int(min(1024, free // self.entry_bytes) // 4 * 4)
         assert self.exact or self.list_cap >= 512
-        self.smem = self.smem_state + (0 if self.exact else 4 * (32 + self.list_cap))
+        self.smem = self.smem_state + (0 if self.exact else 4 * 36 + self.list_cap * self.entry_bytes)
         words = np.array([sum((p.size + 31) // 32 for p in n.populations) for n in nets])
         cta_words = np.bincount(where, weights=words, minlength=n_cta)
         if cta_words.max() > 1024:
@@ -381,14 +425,20 @@ class Batch:
                 base += int(csc.nnz)
                 cbase += npre + 1
             self.fan_out[k] = fan
-            total = base
-            self.idx_t = "int" if total < 2**31 - 1 else "long long"
+            assert self.idx_t == "long long" or base + 8 < 2**31 - 1
             it = np.int32 if self.idx_t == "int" else np.int64
             nat.create(f"proj{k}__col_ptr", np.concatenate(cps).astype(it))
             nat.create(f"proj{k}__bcpoff", np.asarray(cpoff, dtype=np.int64))
             nat.create(f"proj{k}__bwr", np.asarray(wr, dtype=np.int32).reshape(-1))
             post = np.concatenate(posts) if posts else np.zeros(0, np.int64)
             w = np.concatenate(ws) if ws else np.zeros(0)
+            if not self.exact and base:
+                # fast mode adds a spike's synapses with shared-memory atomics
+                # in any order: deal each row's synapses over the warp's atomic
+                # instructions by bank
+                row_ptr = np.concatenate([c[:-1] for c in cps] + [np.array([base])])
+                perm = bank_interleave(row_ptr, post)
+                post, w = post[perm], w[perm]
             # the fast delivery reads aligned groups of 4 synapses: pad the
             # arrays so that the last group stays inside them
             pad = (-post.size) % 4 + 4
@@ -405,8 +455,6 @@ class Batch:
                 wd = self.wdtype
                 nat.create(f"proj{k}__w", to_bf16(w) if wd is BF16 else np.asarray(w, dtype=wd))
                 self.packed[k] = False
-        if not self.net.projections:
-            self.idx_t = "int"
 
     def _create_monitors(self, order):
         nat = self.native

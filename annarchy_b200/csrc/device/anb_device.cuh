@@ -285,6 +285,12 @@ __device__ __forceinline__ anb_u32 anb_ls_u(const anb_u32* p) {
   return v;
 }
 
+// Bulk prefetch of a byte range of global memory into L2; the address and
+// the size are multiples of 16 bytes and the range lies inside one array.
+__device__ __forceinline__ void anb_prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
+}
+
 // Four consecutive weights widened to float (16-byte or 8-byte load).
 __device__ __forceinline__ float4 anb_w4(const float* w) { return anb_ls_f4(reinterpret_cast<const float4*>(w)); }
 __device__ __forceinline__ float4 anb_w4(const anb_bf16* w) {

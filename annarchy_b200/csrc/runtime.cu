@@ -1010,6 +1010,39 @@ int anb_monitor_decode(anb_net* net, const char* array, int64_t steps, int64_t w
   return ANB_OK;
 }
 
+int anb_bank_interleave(const int64_t* row_ptr, int64_t n_rows, const int32_t* post, int64_t* perm) {
+  if (n_rows < 0 || (n_rows > 0 && (!row_ptr || !post || !perm)))
+    return fail(ANB_ERR_ARG, "anb_bank_interleave: invalid arguments");
+  for (int64_t r = 0; r < n_rows; ++r)
+    if (row_ptr[r + 1] < row_ptr[r]) return fail(ANB_ERR_ARG, "anb_bank_interleave: row pointers decrease");
+  std::vector<int64_t> by_bank, slots;
+  for (int64_t r = 0; r < n_rows; ++r) {
+    const int64_t b = row_ptr[r], e = row_ptr[r + 1];
+    const int64_t n = e - b;
+    if (n == 0) continue;
+    // the row's synapses by bank (post rank mod 32), stable within a bank
+    int64_t start[33] = {0};
+    for (int64_t q = b; q < e; ++q) ++start[(post[q] & 31) + 1];
+    for (int k = 0; k < 32; ++k) start[k + 1] += start[k];
+    by_bank.assign((size_t)n, 0);
+    for (int64_t q = b; q < e; ++q) by_bank[(size_t)start[post[q] & 31]++] = q;
+    // positions in the order lane, block, component: one aligned group of 4
+    // positions per lane, 32 lanes per 128-position block; the positions of
+    // one block with the same component are one warp's atomic instruction
+    slots.clear();
+    const int64_t base = b & ~(int64_t)3;
+    const int64_t blocks = (e - base + 127) / 128;
+    for (int64_t l = 0; l < 32; ++l)
+      for (int64_t blk = 0; blk < blocks; ++blk)
+        for (int64_t c = 0; c < 4; ++c) {
+          const int64_t q = base + blk * 128 + 4 * l + c;
+          if (q >= b && q < e) slots.push_back(q);
+        }
+    for (int64_t j = 0; j < n; ++j) perm[slots[(size_t)j] - row_ptr[0]] = by_bank[(size_t)j];
+  }
+  return ANB_OK;
+}
+
 int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
                           int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity) {
   int64_t k = 0;

@@ -21,6 +21,9 @@ Per-instance quantities come from small tables indexed by the instance's
 slot (its position in the packed order): population sizes, offsets into the
 concatenated global arrays, the shared-memory offset of every state array,
 global parameter values and the word range of each projection's pre ranks.
+A launch copies each slot's row of these tables once into a header at the
+start of the CTA's shared memory, so that the steps read none of them from
+global memory.
 
 The per-step semantics are the single-network ones of the reference's
 generated core (ANNarchy/generator/Template/OpenMPBaseTemplate.py:131-484),
@@ -28,6 +31,8 @@ repeated per instance; the reference runs such sweeps as separate processes
 (Network.parallel_run, ANNarchy/core/Network.py:751-900).
 """
 from __future__ import annotations
+
+import numpy as np
 
 from .codegen import CodeGenerator, Module
 
@@ -49,6 +54,41 @@ class BatchGenerator(CodeGenerator):
         from .codegen import compensated_vars
         return compensated_vars(pop, self.exact, self.b.comp_config(pop))
 
+    def _hptr(self, key, slot="anb_si") -> str:
+        """Pointer to the shared-memory copy of a per-slot quantity (the
+        header slots sit at the start of the CTA's shared memory)."""
+        if not hasattr(self, "_hpos"):
+            longs, reals, ints, self._hbytes = self.b.header_layout()
+            self._hpos, off = {}, 0
+            for entries, ct, size in ((longs, "long long", 8), (reals, self.real, 8 if self.exact else 4),
+                                      (ints, "int", 4)):
+                for e in entries:
+                    self._hpos[e[0]] = (ct, off)
+                    off += size
+        ct, off = self._hpos[key]
+        return f"reinterpret_cast<const {ct}*>(anb_smem + ({slot} - anb_sb) * {self._hbytes} + {off})"
+
+    def _hx(self, key, slot="anb_si") -> str:
+        return f"{self._hptr(key, slot)}[0]"
+
+    def _header_fill(self) -> str:
+        """One thread per slot of the CTA copies the slot's row of every
+        per-slot table into the slot's header."""
+        longs, reals, ints, _ = self.b.header_layout()
+        self._hptr(longs[0][0] if longs else ints[0][0])
+        lines = []
+        for key, arr, stride, col in longs + reals + ints:
+            ct, _ = self._hpos[key]
+            idx = "anb_si" if stride == 1 else f"anb_si * {stride} + {col}"
+            dst = self._hptr(key).replace("const ", "", 1)
+            lines.append(f"{dst}[0] = {self.ptr(arr)}[{idx}];")
+        nl = "\n      "
+        return f"""
+    for (int anb_si = anb_sb + threadIdx.x; anb_si < anb_se; anb_si += blockDim.x) {{
+      {nl.join(lines)}
+    }}
+    __syncthreads();"""
+
     def _pop_gsrc(self, k):
         return lambda name: f"({self.ptr(f'pop{k}__{name}')} + anb_goff{k})"
 
@@ -63,12 +103,12 @@ class BatchGenerator(CodeGenerator):
         return lines, d
 
     def _instance_header(self, pops) -> str:
-        out = [f"const int* __restrict__ anb_so = {self.ptr('bt__soff')} + anb_si * {self.b.n_arrays};"]
+        out = [f"const int* __restrict__ anb_so = {self._hptr('so0')};"]
         for pop in pops:
             k = pop.id
-            out.append(f"const int anb_n{k} = {self.ptr(f'pop{k}__bn')}[anb_si];")
-            out.append(f"const long long anb_goff{k} = {self.ptr(f'pop{k}__bgoff')}[anb_si];")
-            out.append(f"const long long anb_woff{k} = {self.ptr(f'pop{k}__bwoff')}[anb_si];")
+            out.append(f"const int anb_n{k} = {self._hx(f'n{k}')};")
+            out.append(f"const long long anb_goff{k} = {self._hx(f'goff{k}')};")
+            out.append(f"const long long anb_woff{k} = {self._hx(f'woff{k}')};")
             out.append(f"(void)anb_n{k}; (void)anb_goff{k}; (void)anb_woff{k};")
         return "\n      ".join(out)
 
@@ -109,9 +149,9 @@ class BatchGenerator(CodeGenerator):
       {{  // {proj.name}: spikes in ascending pre rank, one CTA barrier per spike
         const anb_u32* __restrict__ anb_spk = reinterpret_cast<const anb_u32*>(anb_smem + anb_so[{spk_col}]);
         real* __restrict__ anb_g = reinterpret_cast<real*>(anb_smem + anb_so[{g_col}]);
-        const int anb_w0 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si];
-        const int anb_w1 = {self.ptr(f'proj{k}__bwr')}[2 * anb_si + 1];
-        const {it}* __restrict__ anb_cp = {cp} + {self.ptr(f'proj{k}__bcpoff')}[anb_si];
+        const int anb_w0 = {self._hx(f'wr{k}_0')};
+        const int anb_w1 = {self._hx(f'wr{k}_1')};
+        const {it}* __restrict__ anb_cp = {cp} + {self._hx(f'cp{k}')};
         for (int word = anb_w0; word < anb_w1; ++word) {{
           anb_u32 m = anb_spk[word];
           while (m) {{
@@ -127,30 +167,102 @@ class BatchGenerator(CodeGenerator):
         }}
       }}"""
 
+    def _scratch(self, spk_pops) -> str:
+        """Fast-mode scratch after the instances' state: 32 warp sums, the
+        spike-list counter, the list, and per projection the list entries'
+        synapse ranges (begin, end)."""
+        it = self.b.idx_t
+        cap = self.b.list_cap
+        lines = [f"int* __restrict__ anb_scan = reinterpret_cast<int*>(anb_smem + {self.b.smem_state});",
+                 "int* __restrict__ anb_lcnt = anb_scan + 32;",
+                 "int* __restrict__ anb_list = anb_scan + 36;"]
+        off = self.b.smem_state + 4 * (36 + cap)
+        for proj in self.net.projections:
+            if proj.pre_pop not in spk_pops:
+                continue
+            k = proj.id
+            for end in ("b", "e"):
+                lines.append(f"{it}* __restrict__ anb_l{end}{k} = reinterpret_cast<{it}*>(anb_smem + {off});")
+                off += cap * (8 if it == "long long" else 4)
+        assert off <= self.b.smem, (off, self.b.smem)
+        return "\n    ".join(lines)
+
+    def _append_spikes(self, pop, spk_pops) -> str:
+        """Fast mode, inside the update's ballot: the warp's spikes are
+        appended to the CTA's list for the next step's delivery, each with its
+        synapse range in every projection leaving the population (the column
+        pointers are read here, where their latency hides behind the other
+        warps' updates), and the range's synapse words are prefetched into L2."""
+        if self.exact or pop not in spk_pops:
+            return ""
+        pi = spk_pops.index(pop)
+        P = len(spk_pops)
+        cap = self.b.list_cap
+        it = self.b.idx_t
+        per = []
+        for proj in self.net.projections:
+            if proj.pre_pop is not pop:
+                continue
+            k = proj.id
+            cp = f"({self.ptr(f'proj{k}__col_ptr')} + {self._hx(f'cp{k}')})"
+            if self.b.packed.get(k):
+                pref = [(self.ptr(f"proj{k}__syn"), 4)]
+            else:
+                pref = [(self.ptr(f"proj{k}__post"), 4)]
+                wsize = {np.float64: 8, np.float32: 4}.get(self.b.wdtype, 2)
+                pref.append((self.ptr(f"proj{k}__w"), wsize))
+            pf = []
+            for arr, size in pref:
+                # aligned to 16 bytes on both ends; the arrays are padded so
+                # that the rounded end stays inside them
+                g = 16 // size if size < 16 else 1
+                pf.append(f"anb_prefetch_l2({arr} + (anb_b & ~({it}){g - 1}), "
+                          f"(unsigned)((((anb_e + {g - 1}) & ~({it}){g - 1}) - (anb_b & ~({it}){g - 1})) * {size}));")
+            per.append(f"""
+              {{
+                const {it} anb_b = {cp}[anb_i], anb_e = {cp}[anb_i + 1];
+                anb_lb{k}[anb_q] = anb_b;
+                anb_le{k}[anb_q] = anb_e;
+                if (anb_e > anb_b) {{ {' '.join(pf)} }}
+              }}""")
+        return f"""
+        if (anb_m) {{
+          int anb_q0 = 0;
+          if ((threadIdx.x & 31) == 0) anb_q0 = atomicAdd(anb_lcnt, __popc(anb_m));
+          anb_q0 = __shfl_sync(0xffffffffu, anb_q0, 0);
+          if (anb_spiked) {{
+            const int anb_q = anb_q0 + __popc(anb_m & ((1u << (threadIdx.x & 31)) - 1u));
+            if (anb_q < {cap}) {{
+              anb_list[anb_q] = (((anb_si - anb_sb) * {P} + {pi}) << 16) | anb_i;{''.join(per)}
+            }}
+          }}
+        }}"""
+
     def _delivery_list(self, spk_pops) -> str:
-        """Fast mode. The spikes of the previous step of every instance of the
-        CTA are gathered into one list in shared memory (each thread holds one
-        bitmap word; a CTA prefix sum of the popcounts gives every spike its
-        slot), LIST_CAP entries per round. Warp w then delivers entries
-        4w..4w+3 (+128 per pass): the four spikes' synapse ranges are read as
-        aligned 4-synapse groups (16-byte loads), lane l taking group l of
-        each, all four loads in flight before the shared-memory atomics. A
-        burst of spikes in one instance is spread over all warps of the CTA."""
+        """Fast mode. The previous step's update appended every spike of the
+        CTA's instances to a list in shared memory with its synapse ranges;
+        when more spikes came than the list holds (or at the first step of a
+        launch) the list is rebuilt from the spike bitmaps instead (each
+        thread holds one bitmap word; a CTA prefix sum of the popcounts gives
+        every spike its slot), LIST_CAP entries per round. Warp w then
+        delivers entries 4w..4w+3 (+128 per pass): the four spikes' synapse
+        ranges are read as aligned 4-synapse groups (16-byte loads), lane l
+        taking group l of each, all four loads in flight before the
+        shared-memory atomics. A burst of spikes in one instance is spread
+        over all warps of the CTA."""
         P = len(spk_pops)
         it = self.b.idx_t
         cap = self.b.list_cap
-        NA = self.b.n_arrays
-        so_tab = self.ptr("bt__soff")
         find = []
         for pi, pop in enumerate(spk_pops):
             k = pop.id
             col = self.b.array_index[(k, "spk")]
             find.append(f"""
           {{
-            const int anb_W = ({self.ptr(f'pop{k}__bn')}[anb_si] + 31) >> 5;
+            const int anb_W = ({self._hx(f'n{k}')} + 31) >> 5;
             const int anb_r = (int)threadIdx.x - anb_base;
             if (anb_r >= 0 && anb_r < anb_W) {{
-              anb_lw = reinterpret_cast<const anb_u32*>(anb_smem + {so_tab}[anb_si * {NA} + {col}])[anb_r];
+              anb_lw = reinterpret_cast<const anb_u32*>(anb_smem + {self._hx(f'so{col}')})[anb_r];
               anb_lpair = (anb_si - anb_sb) * {P} + {pi};
               anb_lword = anb_r;
             }}
@@ -184,10 +296,15 @@ class BatchGenerator(CodeGenerator):
            {it} anb_bq1 = 0, anb_eq1 = 0;
            int anb_go1 = 0;
            if (anb_ent >= 0 && anb_epop == {pi}) {{
-             const {it}* __restrict__ anb_cp = {self.ptr(f'proj{k}__col_ptr')} + {self.ptr(f'proj{k}__bcpoff')}[anb_eslot];
-             anb_bq1 = anb_cp[anb_rank];
-             anb_eq1 = anb_cp[anb_rank + 1];
-             anb_go1 = {so_tab}[anb_eslot * {NA} + {g_col}];
+             if (anb_fromlist) {{
+               anb_bq1 = anb_lb{k}[anb_e0 + anb_lane];
+               anb_eq1 = anb_le{k}[anb_e0 + anb_lane];
+             }} else {{
+               const {it}* __restrict__ anb_cp = {self.ptr(f'proj{k}__col_ptr')} + {self._hx(f'cp{k}', 'anb_eslot')};
+               anb_bq1 = anb_cp[anb_rank];
+               anb_eq1 = anb_cp[anb_rank + 1];
+             }}
+             anb_go1 = {self._hx(f'so{g_col}', 'anb_eslot')};
            }}
            for (int anb_sub = 0; anb_sub < 4; anb_sub += {U}) {{
             {it} anb_bq[{U}], anb_eq[{U}];
@@ -222,17 +339,21 @@ class BatchGenerator(CodeGenerator):
           }}""")
         return f"""
       {{  // delivery: CTA-wide list of the previous step's spikes
+        const int anb_cnt = *anb_lcnt;
+        const bool anb_fromlist = anb_cnt <= {cap};
+        __syncthreads();  // every thread has read the counter
+        if (threadIdx.x == 0) *anb_lcnt = 0;
         anb_u32 anb_lw = 0u;
         int anb_lpair = 0, anb_lword = 0;
-        {{
+        int anb_total = anb_cnt, anb_excl = 0;
+        if (!anb_fromlist) {{
           int anb_base = 0;
           for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{{''.join(find)}
           }}
+          anb_excl = anb_block_exclusive_scan(__popc(anb_lw), anb_scan, &anb_total);
         }}
-        int anb_total;
-        const int anb_excl = anb_block_exclusive_scan(__popc(anb_lw), anb_scan, &anb_total);
         for (int anb_r0 = 0; anb_r0 < anb_total; anb_r0 += {cap}) {{
-          {{
+          if (!anb_fromlist) {{
             int k = anb_excl;
             anb_u32 m = anb_lw;
             while (m) {{
@@ -242,8 +363,8 @@ class BatchGenerator(CodeGenerator):
                 anb_list[k - anb_r0] = (anb_lpair << 16) | ((anb_lword << 5) + b);
               ++k;
             }}
+            __syncthreads();
           }}
-          __syncthreads();
           const int anb_nl = min({cap}, anb_total - anb_r0);
           for (int anb_e0 = anb_warp * 4; anb_e0 < anb_nl; anb_e0 += anb_nwarps * 4) {{
             const int anb_ent = (anb_lane < 4 && anb_e0 + anb_lane < anb_nl) ? anb_list[anb_e0 + anb_lane] : -1;
@@ -256,6 +377,10 @@ class BatchGenerator(CodeGenerator):
           __syncthreads();
         }}
       }}"""
+
+    def _spk_pops(self) -> list:
+        """Populations with outgoing projections (their spikes are delivered)."""
+        return [p for p in self.net.populations if any(pr.pre_pop is p for pr in self.net.projections)]
 
     def _update(self, pop) -> str:
         k = pop.id
@@ -278,10 +403,10 @@ class BatchGenerator(CodeGenerator):
         const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
         if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {{
           {d['spk']}[anb_i >> 5] = anb_m;{recs}
-        }}
+        }}{self._append_spikes(pop, self._spk_pops())}
       }}"""
-        globals_ = self._globals_preamble(pop, lambda n: f"({self.ptr(f'pop{k}__{n}')} + anb_si)")
-        globals_ += f"\n    const int anb_refr{k} = {self.ptr(f'pop{k}__brefr')}[anb_si];"
+        globals_ = self._globals_preamble(pop, lambda n: self._hptr(f"p{k}_{n}"))
+        globals_ += f"\n    const int anb_refr{k} = {self._hx(f'refr{k}')};"
         # a refractory period shared by all neurons of the instance comes from
         # the slot table (no global load in the spike branch)
         refr = (f"(anb_refr{k} >= 0 ? anb_refr{k} : "
@@ -310,7 +435,7 @@ class BatchGenerator(CodeGenerator):
         header = self._instance_header(pops)
         load = "".join(self._copy(p, True) for p in pops)
         store = "".join(self._copy(p, False) for p in pops)
-        spk_pops = [p for p in pops if any(pr.pre_pop is p for pr in net.projections)]
+        spk_pops = self._spk_pops()
         if self.exact:
             deliver = (f"for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{\n        {header}"
                        + "".join(self._delivery_exact(pr) for pr in net.projections) + "\n      }")
@@ -320,9 +445,11 @@ class BatchGenerator(CodeGenerator):
             deliver = ""
         update = "".join(self._update(p) for p in pops)
         dt_t = "double" if self.exact else "float"
-        scratch = "" if self.exact else f"""// scratch after the instances' state: 32 warp sums, then the spike list
-    int* __restrict__ anb_scan = reinterpret_cast<int*>(anb_smem + {self.b.smem_state});
-    int* __restrict__ anb_list = anb_scan + 32;"""
+        scratch = "" if self.exact or not spk_pops else self._scratch(spk_pops)
+        if scratch:
+            # no list at the first step of a launch: the delivery rebuilds it
+            # from the spike bitmaps
+            scratch += f"\n    if (threadIdx.x == 0) *anb_lcnt = {self.b.list_cap} + 1;"
         src = f"""
 extern "C" __global__ void __launch_bounds__({BATCH_BLOCK}, 1)
 anb_batch_run(long long t0, int nsteps) {{
@@ -336,6 +463,7 @@ anb_batch_run(long long t0, int nsteps) {{
     const int anb_se = {self.ptr('bt__cta')}[blockIdx.x + 1];
     {scratch}
     {mon_pre}
+    {self._header_fill()}
     for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{
       {header}
       {load}

@@ -72,6 +72,7 @@ SIGNATURES = {
                                     C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "anb_monitor_decode": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_int64, C.c_int64,
                                      C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
+    "anb_bank_interleave": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "anb_bitmap_decode": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p,
                                       C.c_void_p, C.c_int64]),
     "anb_plan_clear": (C.c_int, [C.c_void_p]),
@@ -181,6 +182,22 @@ def nvrtc_compile(source: str, options: list[str]) -> tuple[int, str]:
     check("anb_nvrtc_compile", load().anb_nvrtc_compile(source.encode(), "\n".join(options).encode(),
                                                         log, len(log), C.byref(n)))
     return n.value, log.value.decode(errors="replace")
+
+
+def bank_interleave(row_ptr: np.ndarray, post: np.ndarray) -> np.ndarray:
+    """Permutation of the positions row_ptr[0]..row_ptr[-1]-1 that deals each
+    row's synapses, by bank of their post rank, over the warp's atomic
+    instructions (anb_bank_interleave)."""
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    post = np.ascontiguousarray(post, dtype=np.int32)
+    n = int(row_ptr[-1] - row_ptr[0]) if row_ptr.size else 0
+    perm = np.arange(row_ptr[0] if row_ptr.size else 0, (row_ptr[0] if row_ptr.size else 0) + n,
+                     dtype=np.int64)
+    if n:
+        check("anb_bank_interleave", load().anb_bank_interleave(
+            row_ptr.ctypes.data_as(C.c_void_p), row_ptr.size - 1, post.ctypes.data_as(C.c_void_p),
+            perm.ctypes.data_as(C.c_void_p)))
+    return perm
 
 
 def bitmap_decode(buf: np.ndarray, n: int):

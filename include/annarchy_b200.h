@@ -317,6 +317,20 @@ int anb_monitor_decode(anb_net* net, const char* array, int64_t steps, int64_t w
 int64_t anb_bitmap_decode(const uint32_t* words, int64_t steps, int64_t words_per_step,
                           int64_t n, int64_t* out_steps, int64_t* out_ranks, int64_t capacity);
 
+/* Host-side reordering of a pre-major synapse list for the batched engine's
+ * fast delivery, where lane l of a warp adds the synapses of the aligned group
+ * of 4 positions 4l..4l+3 of each 128-position block, one shared-memory atomic
+ * instruction per block and component. Within each row r (positions
+ * row_ptr[r] .. row_ptr[r+1]-1), the synapses ordered by bank (post rank mod
+ * 32) are dealt over those instructions in turn, so that an instruction's
+ * atomics fall into distinct banks where the row allows it. Writes
+ * perm[q - row_ptr[0]] = the position whose synapse goes to position q. The
+ * order of additions within a row is free in this mode (float atomics); the
+ * reference delivers a spike's synapses in stored order
+ * (ANNarchy/generator/Projection/OpenMP/CSR.py:870-902), which only the exact
+ * mode keeps. Host memory only. */
+int anb_bank_interleave(const int64_t* row_ptr, int64_t n_rows, const int32_t* post, int64_t* perm);
+
 /* ---- batched weighted sums on the tensor cores --------------------------
  * Y[b][post] += sum_pre W[post][pre] * X[b][pre] for `batch` instances that
  * share a block-sparse weight matrix of dense 64 x 64 bfloat16 tiles (the

@@ -31,6 +31,37 @@ def test_skip_generator_matches_bernoulli_density():
     assert abs(rows.mean() - 40) < 1 and rows.std() < 10
 
 
+def _atomic_sets(row_ptr, post):
+    """Bank multiplicity of every atomic instruction of the fast delivery:
+    positions of one row in the same aligned 128-position block with the
+    same index mod 4."""
+    worst = []
+    for b, e in zip(row_ptr[:-1], row_ptr[1:]):
+        q = np.arange(b, e)
+        rel = q - (b & ~3)
+        sets = (rel // 128) * 4 + rel % 4
+        for s in np.unique(sets):
+            worst.append(np.bincount(post[q[sets == s]] % 32).max())
+    return np.array(worst)
+
+
+def test_bank_interleave_permutes_rows_and_spreads_banks():
+    rng = np.random.default_rng(3)
+    lens = rng.integers(0, 400, 60)
+    lens[:3] = (0, 1, 5)
+    row_ptr = np.zeros(61, dtype=np.int64)
+    np.cumsum(lens, out=row_ptr[1:])
+    post = np.concatenate([np.sort(rng.choice(8000, n, replace=False)) for n in lens]).astype(np.int32)
+    perm = L.bank_interleave(row_ptr, post)
+    # a permutation within every row
+    for b, e in zip(row_ptr[:-1], row_ptr[1:]):
+        assert sorted(perm[b:e].tolist()) == list(range(b, e))
+    before, after = _atomic_sets(row_ptr, post), _atomic_sets(row_ptr, post[perm])
+    assert after.sum() < 0.7 * before.sum() and after.mean() < 2.0
+    with pytest.raises(L.BackendError):
+        L.bank_interleave(np.array([0, 5, 3]), np.zeros(5, dtype=np.int32))
+
+
 @pytest.mark.parametrize("prec,wd", [("float", "bfloat16"), ("float", "float32"), ("double", None)])
 def test_batch_module_compiles(prec, wd):
     cns = _cns([300, 1000, 2500, 777, 4000, 8000], 10)
