@@ -174,7 +174,7 @@ class BatchGenerator(CodeGenerator):
         it = self.b.idx_t
         cap = self.b.list_cap
         lines = [f"int* __restrict__ anb_scan = reinterpret_cast<int*>(anb_smem + {self.b.smem_state});",
-                 "int* __restrict__ anb_lcnt = anb_scan + 32;",
+                 "int* __restrict__ anb_lcnt = anb_scan + 32;  // by step parity",
                  "int* __restrict__ anb_list = anb_scan + 36;"]
         off = self.b.smem_state + 4 * (36 + cap)
         for proj in self.net.projections:
@@ -228,7 +228,7 @@ class BatchGenerator(CodeGenerator):
         return f"""
         if (anb_m) {{
           int anb_q0 = 0;
-          if ((threadIdx.x & 31) == 0) anb_q0 = atomicAdd(anb_lcnt, __popc(anb_m));
+          if ((threadIdx.x & 31) == 0) anb_q0 = atomicAdd(anb_lcnt + (t & 1), __popc(anb_m));
           anb_q0 = __shfl_sync(0xffffffffu, anb_q0, 0);
           if (anb_spiked) {{
             const int anb_q = anb_q0 + __popc(anb_m & ((1u << (threadIdx.x & 31)) - 1u));
@@ -339,10 +339,11 @@ class BatchGenerator(CodeGenerator):
           }}""")
         return f"""
       {{  // delivery: CTA-wide list of the previous step's spikes
-        const int anb_cnt = *anb_lcnt;
+        // the previous step's counter; this step's update counts into the
+        // other one (last read by the previous step's delivery)
+        const int anb_cnt = anb_lcnt[(t - 1) & 1];
         const bool anb_fromlist = anb_cnt <= {cap};
-        __syncthreads();  // every thread has read the counter
-        if (threadIdx.x == 0) *anb_lcnt = 0;
+        if (threadIdx.x == 0) anb_lcnt[t & 1] = 0;
         anb_u32 anb_lw = 0u;
         int anb_lpair = 0, anb_lword = 0;
         int anb_total = anb_cnt, anb_excl = 0;
@@ -374,7 +375,8 @@ class BatchGenerator(CodeGenerator):
             const int anb_epop = anb_ent >= 0 ? anb_pair % {P} : -1;
             (void)anb_rank; (void)anb_eslot;{''.join(projs)}
           }}
-          __syncthreads();
+          // before the next round's list (the step's own barrier follows the last)
+          if (anb_r0 + {cap} < anb_total) __syncthreads();
         }}
       }}"""
 
@@ -382,28 +384,40 @@ class BatchGenerator(CodeGenerator):
         """Populations with outgoing projections (their spikes are delivered)."""
         return [p for p in self.net.populations if any(pr.pre_pop is p for pr in self.net.projections)]
 
+    def _record(self) -> str:
+        """Spike monitors, after the update's barrier: the step's bitmap words
+        of every instance of the CTA copied from shared memory into the
+        monitor's ring, one thread per word."""
+        out = []
+        for mon in self.net.monitors:
+            if "spike" not in mon.variables:
+                continue
+            m, k = mon.id, mon.population.id
+            col = self.b.array_index[(k, "spk")]
+            out.append(f"""
+      if (anb_mon_on{m}) {{  // spike monitor {m}
+        const long long anb_slot = t - anb_mon_t0{m};
+        if (anb_slot >= 0 && anb_slot < {self.b.mon_cap[m]}) {{
+          for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{
+            const int anb_W = ({self._hx(f'n{k}')} + 31) >> 5;
+            const anb_u32* __restrict__ anb_w = reinterpret_cast<const anb_u32*>(anb_smem + {self._hx(f'so{col}')});
+            anb_u32* __restrict__ anb_dst = {self.ptr(f'mon{m}__spk')} + anb_slot * {self.b.total_words[k]}LL + {self._hx(f'woff{k}')};
+            for (int q = threadIdx.x; q < anb_W; q += blockDim.x) anb_dst[q] = anb_w[q];
+          }}
+        }} else if (threadIdx.x == 0) {{
+          anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
+        }}
+      }}""")
+        return "".join(out)
+
     def _update(self, pop) -> str:
         k = pop.id
         lines, d = self._smem_ptrs(pop)
-        recs = ""
-        for mon in self.net.monitors:
-            if mon.population is not pop or "spike" not in mon.variables:
-                continue
-            m = mon.id
-            recs += f"""
-          if (anb_mon_on{m}) {{
-            const long long anb_slot = t - anb_mon_t0{m};
-            if (anb_slot >= 0 && anb_slot < {self.b.mon_cap[m]})
-              {self.ptr(f'mon{m}__spk')}[anb_slot * {self.b.total_words[k]}LL + anb_woff{k} + (anb_i >> 5)] = anb_m;
-            else
-              anb_report({self.ptr('err')}, ANB_DEVERR_MONITOR_OVERFLOW);
-          }}"""
         hook = f"""
       {{
         const anb_u32 anb_m = __ballot_sync(0xffffffffu, anb_spiked);
-        if ((threadIdx.x & 31) == 0 && anb_i < anb_n) {{
-          {d['spk']}[anb_i >> 5] = anb_m;{recs}
-        }}{self._append_spikes(pop, self._spk_pops())}
+        if ((threadIdx.x & 31) == 0 && anb_i < anb_n)
+          {d['spk']}[anb_i >> 5] = anb_m;{self._append_spikes(pop, self._spk_pops())}
       }}"""
         globals_ = self._globals_preamble(pop, lambda n: self._hptr(f"p{k}_{n}"))
         globals_ += f"\n    const int anb_refr{k} = {self._hx(f'refr{k}')};"
@@ -449,7 +463,7 @@ class BatchGenerator(CodeGenerator):
         if scratch:
             # no list at the first step of a launch: the delivery rebuilds it
             # from the spike bitmaps
-            scratch += f"\n    if (threadIdx.x == 0) *anb_lcnt = {self.b.list_cap} + 1;"
+            scratch += f"\n    if (threadIdx.x == 0) anb_lcnt[0] = anb_lcnt[1] = {self.b.list_cap} + 1;"
         src = f"""
 extern "C" __global__ void __launch_bounds__({BATCH_BLOCK}, 1)
 anb_batch_run(long long t0, int nsteps) {{
@@ -477,7 +491,7 @@ anb_batch_run(long long t0, int nsteps) {{
         {header}
         {update}
       }}
-      __syncthreads();
+      __syncthreads();{self._record()}
     }}
     for (int anb_si = anb_sb; anb_si < anb_se; ++anb_si) {{
       {header}
