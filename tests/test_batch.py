@@ -196,3 +196,38 @@ def test_batch_reset_reproduces_run():
         s1, r1 = m[2].spike_arrays()
         assert np.array_equal(s0, s1) and np.array_equal(r0, r1)
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wd", ["float32", "bfloat16"])
+@pytest.mark.parametrize("first_spikes", [(300, 100, 0), (6000, 100, 1500)])
+def test_fast_batch_delivers_one_step_of_spikes(wd, first_spikes):
+    """The fast delivery of one step's spikes, checked synapse by synapse:
+    neurons 0..k-1 of each instance start above threshold and spike at
+    step 0; after step 1 every conductance is the sum of the weights of those
+    spikes, decayed once. 400 spikes in the CTA take the list the update
+    appended them to; 7600 overflow it and are delivered from the spike
+    bitmaps in rounds."""
+    from annarchy_b200.core.backend import from_bf16, to_bf16
+    cns = _cns([6000, 2500, 1500], 10)
+    for cn, k in zip(cns, first_spikes):
+        cn.v0 = np.full(cn.n, -60.0)
+        cn.v0[:k] = -40.0
+    b, members = wl.build_batch(cns, "float", wd, ctas=1)
+    b.compile()
+    assert b.n_cta == 1
+    b.simulate_steps(2)
+    for cn, k, (net, P, mon) in zip(cns, first_spikes, members):
+        spiked = np.zeros(cn.n)
+        spiked[:k] = 1.0
+        steps, ranks = mon.spike_arrays()
+        assert ranks[steps == 0].tolist() == list(range(k))
+        we, wi = cn.w_exc.copy(), cn.w_inh.copy()
+        if wd == "bfloat16":
+            we.data, wi.data = from_bf16(to_bf16(we.data)), from_bf16(to_bf16(wi.data))
+        for g, w, pre, tau in ((P.g_exc, we, spiked[:cn.n_exc], cn.params["tau_exc"]),
+                               (P.g_inh, wi, spiked[cn.n_exc:], cn.params["tau_inh"])):
+            s = w @ pre
+            expected = s - 0.1 * s / tau
+            np.testing.assert_allclose(np.asarray(g), expected, rtol=2e-6, atol=1e-6)
+    b.close()
