@@ -93,6 +93,43 @@ __device__ __forceinline__ void anb_rate_csr_scalar(int n_rows, const I* __restr
   }
 }
 
+// Warp per row, the same sum in the same order as anb_rate_csr_scalar: the
+// lanes form 32 products pre_r[col[j]] * w[j] at a time (coalesced index and
+// weight loads, all gathers in flight, the next 32 loading while these are
+// added), then every lane adds them one by one in stored order, as the
+// reference's sequential loop does (ANNarchy/generator/Projection/OpenMP/
+// CSR.py:177-253); no addition is reordered, so the result is the scalar
+// kernel's bit for bit.
+template <typename R, typename W, typename I>
+__device__ __forceinline__ void anb_rate_csr_ordered(int n_rows, const I* __restrict__ row_ptr,
+                                                     const int* __restrict__ col,
+                                                     const W* __restrict__ w,
+                                                     const R* __restrict__ pre_r,
+                                                     const int* __restrict__ post_rank,
+                                                     R* __restrict__ sum) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); row < n_rows; row += nwarps) {
+    const I beg = row_ptr[row], end = row_ptr[row + 1];
+    R s = R(0);
+    I j = beg + lane;
+    R p = j < end ? pre_r[col[j]] * (R)w[j] : R(0);
+    for (I j0 = beg; j0 < end; j0 += 32) {
+      const I jn = j0 + 32 + lane;
+      const R pn = jn < end ? pre_r[col[jn]] * (R)w[jn] : R(0);
+      if (end - j0 >= 32) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) s += __shfl_sync(0xffffffffu, p, k);
+      } else {
+        const int cnt = (int)(end - j0);
+        for (int k = 0; k < cnt; ++k) s += __shfl_sync(0xffffffffu, p, k);
+      }
+      p = pn;
+    }
+    if (lane == 0) sum[post_rank ? post_rank[row] : row] += s;
+  }
+}
+
 // ---- random numbers in equations --------------------------------------------------------
 // Counter-based generator Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror,
 // D. E. Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11): ten

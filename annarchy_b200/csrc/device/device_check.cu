@@ -8,6 +8,7 @@
 extern "C" __global__ void check_rate_csr_scalar(int n, const int* rp, const int* c, const double* w,
                                                  const double* r, const int* pr, double* s) {
   anb_rate_csr_scalar<double, double, int>(n, rp, c, w, r, pr, s);
+  anb_rate_csr_ordered<double, double, int>(n, rp, c, w, r, pr, s);
 }
 extern "C" __global__ void check_rate_csr_vector_f32(int n, const int* rp, const int* c, const float* w,
                                                      const float* r, const int* pr, float* s) {

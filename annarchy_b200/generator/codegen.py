@@ -1142,9 +1142,10 @@ extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
                     [(name, lay["pc_ctas"], B, 4 * pw)])
         if fmt in ("csr", "pcsr"):       # pcsr in double precision: CSR order
             if self.exact:
-                call = (f"anb_rate_csr_scalar<double, double, {lay['idx_t']}>({lay['rows']}, "
+                # warp per row, additions in stored order
+                call = (f"anb_rate_csr_ordered<double, double, {lay['idx_t']}>({lay['rows']}, "
                         f"{p('row_ptr')}, {p('col')}, {p('w')}, {pre_r}, {p('post_rank')}, {sum_});")
-                return kern(name, call), [(name, lay["grid"], BLOCK, 0)]
+                return kern(name, call), [(name, grid_for(lay["rows"] * 32), BLOCK, 0)]
             G = lay["vgroup"]
             if lay.get("heavy", 0):
                 light = (f"anb_rate_csr_vec<{G}, {W}>({lay['light']}, {p('rows_light')}, {p('row_ptr')}, "
