@@ -221,6 +221,36 @@ __device__ __forceinline__ int anb_ring_slot(long long s, int slots) {
 // t - delay; slots x n_pre values). The reference's non-uniform delays read
 // pre.r from its queue entry delay - 1 (ANNarchy/generator/Projection/
 // SingleThreadGenerator.py, _computesum_rate with max_delay > 1).
+// The same sum with a warp per row (products gathered 32 at a time, added
+// one by one in stored order, as anb_rate_csr_ordered).
+template <typename R, typename W, typename I>
+__device__ __forceinline__ void anb_rate_csr_delayed_ordered(int n_rows, const I* __restrict__ row_ptr,
+                                                             const int* __restrict__ col,
+                                                             const W* __restrict__ w,
+                                                             const int* __restrict__ dly,
+                                                             const R* __restrict__ ring, int n_pre,
+                                                             int slots, long long t,
+                                                             const int* __restrict__ post_rank,
+                                                             R* __restrict__ sum) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); row < n_rows; row += nwarps) {
+    const I beg = row_ptr[row], end = row_ptr[row + 1];
+    R s = R(0);
+    I j = beg + lane;
+    R p = j < end ? ring[(size_t)anb_ring_slot(t - dly[j], slots) * n_pre + col[j]] * (R)w[j] : R(0);
+    for (I j0 = beg; j0 < end; j0 += 32) {
+      const I jn = j0 + 32 + lane;
+      const R pn = jn < end ? ring[(size_t)anb_ring_slot(t - dly[jn], slots) * n_pre + col[jn]] * (R)w[jn]
+                            : R(0);
+      const int cnt = end - j0 >= 32 ? 32 : (int)(end - j0);
+      for (int k = 0; k < cnt; ++k) s += __shfl_sync(0xffffffffu, p, k);
+      p = pn;
+    }
+    if (lane == 0) sum[post_rank ? post_rank[row] : row] += s;
+  }
+}
+
 template <typename R, typename W, typename I>
 __device__ __forceinline__ void anb_rate_csr_delayed(int n_rows, const I* __restrict__ row_ptr,
                                                      const int* __restrict__ col,

@@ -10,6 +10,14 @@ extern "C" __global__ void check_rate_csr_scalar(int n, const int* rp, const int
   anb_rate_csr_scalar<double, double, int>(n, rp, c, w, r, pr, s);
   anb_rate_csr_ordered<double, double, int>(n, rp, c, w, r, pr, s);
 }
+extern "C" __global__ void check_rate_csr_delayed(int n, const int* rp, const int* c, const double* w,
+                                                  const int* d, const double* ring, int n_pre, int slots,
+                                                  long long t, const int* pr, double* s) {
+  anb_rate_csr_delayed_ordered<double, double, int>(n, rp, c, w, d, ring, n_pre, slots, t, pr, s);
+  anb_rate_csr_delayed_ordered<float, float, int>(n, rp, c, reinterpret_cast<const float*>(w), d,
+                                                  reinterpret_cast<const float*>(ring), n_pre, slots, t, pr,
+                                                  reinterpret_cast<float*>(s));
+}
 extern "C" __global__ void check_rate_csr_vector_f32(int n, const int* rp, const int* c, const float* w,
                                                      const float* r, const int* pr, float* s) {
   anb_rate_csr_vector<8, float, int>(n, rp, c, w, r, pr, s, 10000);

@@ -1127,11 +1127,11 @@ extern "C" __global__ void __launch_bounds__({bounds}) {nm}() {{
         if proj._delay_steps is not None:
             # one delay per synapse: CSR rows read the rate ring per synapse
             a = proj.pre_pop
-            call = (f"anb_rate_csr_delayed<{self.real}, {W}, {lay['idx_t']}>({lay['rows']}, "
+            call = (f"anb_rate_csr_delayed_ordered<{self.real}, {W}, {lay['idx_t']}>({lay['rows']}, "
                     f"{p('row_ptr')}, {p('col')}, {p('w')}, {p('dly')}, "
                     f"{self.ptr(f'pop{a.id}___delayed_r')}, {self.c.ring_stride(a)}, {self.slots(a)}, t, "
                     f"{p('post_rank')}, {sum_});")
-            return kern(name, call), [(name, grid_for(lay["rows"]), BLOCK, 0)]
+            return kern(name, call), [(name, grid_for(lay["rows"] * 32), BLOCK, 0)]
         if fmt == "pcsr" and not self.exact:
             pw = lay["panel_width"]
             call = (f"anb_rate_pcsr<{W}, {lay['pc_unroll']}>({p('pc_cta')}, {p('pc_warp')}, "
