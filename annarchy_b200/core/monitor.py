@@ -20,6 +20,7 @@ their float32 step size in the rate transformations.
 from __future__ import annotations
 
 import copy
+import gc
 import re
 
 import numpy as np
@@ -213,13 +214,22 @@ class Monitor:
         counts = np.bincount(r, minlength=size)
         offs = np.zeros(size + 1, dtype=np.int64)
         np.cumsum(counts, out=offs[1:])
-        # one conversion to Python ints, then list slices per neuron
-        steps = s[order].tolist()
-        lo, hi = offs[:-1].tolist(), offs[1:].tolist()
-        if self.ranks is None:
-            d = dict(zip(range(size), map(steps.__getitem__, map(slice, lo, hi))))
-        else:
-            d = {int(k): steps[lo[int(k)]:hi[int(k)]] for k in self.ranks}
+        # one conversion to Python ints, then list slices per neuron; the
+        # collector stays off meanwhile (thousands of new lists, no cycles: in
+        # a process holding many objects its passes would cost more than the
+        # construction)
+        was_enabled = gc.isenabled()
+        gc.disable()
+        try:
+            steps = s[order].tolist()
+            lo, hi = offs[:-1].tolist(), offs[1:].tolist()
+            if self.ranks is None:
+                d = dict(zip(range(size), map(steps.__getitem__, map(slice, lo, hi))))
+            else:
+                d = {int(k): steps[lo[int(k)]:hi[int(k)]] for k in self.ranks}
+        finally:
+            if was_enabled:
+                gc.enable()
         if not keep:
             self._spike_steps, self._spike_ranks = [], []
         return d
