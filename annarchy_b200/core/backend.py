@@ -152,6 +152,7 @@ class CompiledNetwork:
         else:
             nat.plan(mod.plan)
             nat.set_graph_steps(int(net._config.get("graph_steps", 32)))
+            nat.set_pdl(bool(net._config.get("pdl", True)))
             for pop_id, kernel, grid, block, mode_all in mod.stops:
                 nat.set_stop_kernel(pop_id, kernel, grid, block, mode_all)
 

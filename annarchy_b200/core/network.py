@@ -11,6 +11,9 @@ Configuration (``Network.config``):
   weight_dtype "float32" or "bfloat16" storage of static weights (float mode).
   engine       "auto" | "grid" | "local" (see annarchy_b200.generator.codegen).
   graph_steps  steps captured per CUDA graph in the grid engine.
+  pdl          True (default) | False: launch the grid engine's step kernels
+               with programmatic dependent launch (each may be scheduled
+               while its predecessor runs and waits for it on the device).
   persistent   True | False (default): run the grid engine's step as one
                cooperative persistent kernel with grid-wide barriers (fast
                spiking networks).

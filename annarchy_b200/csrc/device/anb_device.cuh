@@ -68,6 +68,16 @@ __device__ __forceinline__ bool anb_bit(const anb_u32* bits, int i) {
   return (bits[i >> 5] >> (i & 31)) & 1u;
 }
 
+// Start of every kernel of the grid engine's plan, which may be launched
+// while the previous kernel of the stream still runs (programmatic dependent
+// launch): wait until that kernel has finished and its writes are visible,
+// then allow the next kernel to be scheduled. Outside such a launch both
+// return at once.
+__device__ __forceinline__ void anb_pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void anb_report(int* err, int code) {
   if (err) atomicCAS(err, 0, code);
 }

@@ -145,6 +145,10 @@ struct anb_net {
   Launch local;
   bool has_local = false;
   int graph_steps = 32;
+  // plan kernels launched with programmatic stream serialization (each
+  // generated kernel waits for its predecessor with griddepcontrol.wait)
+  bool pdl = true;
+  bool pdl_prev = false;   // the last plan operation was a kernel on the main stream
   cudaGraphExec_t graph = nullptr;
   double dt = 1.0;
   int64_t t = 0;
@@ -244,13 +248,35 @@ int launch_bsr_tc(anb_net* net, const Launch& l, cudaStream_t st) {
   return ANB_OK;
 }
 
-int launch(anb_net* net, const Launch& l, void** params, cudaStream_t on = nullptr) {
+int launch(anb_net* net, const Launch& l, void** params, cudaStream_t on = nullptr, bool pdl = false) {
   if (l.op == kOpBsrTc) return launch_bsr_tc(net, l, on ? on : net->stream);
   if (l.cooperative) {
     CUlaunchAttribute attr;
     std::memset(&attr, 0, sizeof(attr));
     attr.id = CU_LAUNCH_ATTRIBUTE_COOPERATIVE;
     attr.value.cooperative = 1;
+    CUlaunchConfig cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDimX = l.grid;
+    cfg.gridDimY = 1;
+    cfg.gridDimZ = 1;
+    cfg.blockDimX = l.block;
+    cfg.blockDimY = 1;
+    cfg.blockDimZ = 1;
+    cfg.sharedMemBytes = l.smem;
+    cfg.hStream = (CUstream)(on ? on : net->stream);
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    ANB_CU(g_drv.launchKernelEx(&cfg, l.fn, params, nullptr));
+    return ANB_OK;
+  }
+  if (l.cluster <= 1 && pdl) {
+    // may be scheduled while the stream's previous kernel still runs; the
+    // kernel's griddepcontrol.wait orders its reads after that kernel
+    CUlaunchAttribute attr;
+    std::memset(&attr, 0, sizeof(attr));
+    attr.id = CU_LAUNCH_ATTRIBUTE_PROGRAMMATIC_STREAM_SERIALIZATION;
+    attr.value.programmaticStreamSerializationAllowed = 1;
     CUlaunchConfig cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDimX = l.grid;
@@ -355,11 +381,16 @@ int run_plan_once(anb_net* net) {
     if (l.group != 0 && !net->timing)
       while (j < n && net->plan[j].group == l.group) ++j;
     if (j - i == 1) {
-      int rc = net->timing ? timed_launch(net, l, nullptr) : launch(net, l, nullptr);
+      // programmatic only after a kernel of the main stream (not after the
+      // join of parallel branches or a library operation)
+      const bool pdl = net->pdl && net->pdl_prev && !net->timing && l.op != kOpBsrTc && l.cluster <= 1;
+      int rc = net->timing ? timed_launch(net, l, nullptr) : launch(net, l, nullptr, nullptr, pdl);
       if (rc != ANB_OK) return rc;
+      net->pdl_prev = l.op != kOpBsrTc && l.cluster <= 1 && !l.cooperative;
       i = j;
       continue;
     }
+    net->pdl_prev = false;
     int rc = ensure_side(net, j - i - 1);
     if (rc != ANB_OK) return rc;
     ANB_CUDA(cudaEventRecord(net->fork_ev, net->stream));
@@ -373,6 +404,7 @@ int run_plan_once(anb_net* net) {
     rc = launch(net, l, nullptr);
     if (rc != ANB_OK) return rc;
     for (size_t q = i + 1; q < j; ++q) ANB_CUDA(cudaStreamWaitEvent(net->stream, net->side_ev[q - i - 1], 0));
+    net->pdl_prev = false;
     i = j;
   }
   return ANB_OK;
@@ -382,6 +414,7 @@ int build_graph(anb_net* net) {
   if (net->graph) return ANB_OK;
   cudaGraph_t g = nullptr;
   ANB_CUDA(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+  net->pdl_prev = false;
   int rc = ANB_OK;
   for (int s = 0; s < net->graph_steps && rc == ANB_OK; ++s) rc = run_plan_once(net);
   cudaError_t e = cudaStreamEndCapture(net->stream, &g);
@@ -1228,6 +1261,14 @@ int anb_set_local_kernel_ex(anb_net* net, const char* kernel, unsigned grid, uns
   }
   net->local = l;
   net->has_local = true;
+  return ANB_OK;
+}
+
+int anb_set_pdl(anb_net* net, int on) {
+  if (!net) return fail(ANB_ERR_ARG, "net is NULL");
+  drop_graph(net);
+  net->pdl = on != 0;
+  net->pdl_prev = false;
   return ANB_OK;
 }
 

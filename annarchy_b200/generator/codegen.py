@@ -1841,6 +1841,10 @@ extern "C" __global__ void anb_tick() {
                 code, mode_all = self.stop_kernel(pop)
                 kernels.append(code)
                 stops.append((pop.id, f"pop{pop.id}_stop", grid_for(pop.size), BLOCK, mode_all))
+        # every kernel first waits for its predecessor on the stream (the plan
+        # is launched with programmatic dependent launch)
+        kernels = [re.sub(r'(extern "C" __global__ void (?:__launch_bounds__\([^)]*\) )?\w+\(\) \{)',
+                          r"\1\n    anb_pdl_enter();", src) for src in kernels]
         return Module(self.assemble(kernels), self.options(), "grid", plan=plan,
                       kernels=[p[0] for p in plan], stops=stops)
 

@@ -81,6 +81,7 @@ SIGNATURES = {
     "anb_set_local_kernel_ex": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint, C.c_uint, C.c_uint,
                                           C.c_uint]),
     "anb_set_graph_steps": (C.c_int, [C.c_void_p, C.c_int]),
+    "anb_set_pdl": (C.c_int, [C.c_void_p, C.c_int]),
     "anb_run": (C.c_int, [C.c_void_p, C.c_int64]),
     "anb_step": (C.c_int, [C.c_void_p]),
     "anb_synchronize": (C.c_int, [C.c_void_p]),
@@ -501,6 +502,9 @@ class NativeNet:
     def set_graph_steps(self, steps: int):
         check("anb_set_graph_steps", self.lib.anb_set_graph_steps(self.h, steps))
 
+    def set_pdl(self, on: bool):
+        check("anb_set_pdl", self.lib.anb_set_pdl(self.h, 1 if on else 0))
+
     def run(self, steps: int):
         check("anb_run", self.lib.anb_run(self.h, int(steps)))
 
@@ -641,6 +645,9 @@ class DryNative:
         pass
 
     def set_graph_steps(self, steps):
+        pass
+
+    def set_pdl(self, on):
         pass
 
     def close(self):

@@ -262,6 +262,16 @@ int anb_set_local_kernel_ex(anb_net* net, const char* kernel, unsigned grid, uns
 /* Steps per captured CUDA graph in the grid engine (0 = no graph). */
 int anb_set_graph_steps(anb_net* net, int steps);
 
+/* Programmatic dependent launch of the grid engine's plan (on by default):
+ * a kernel that follows another kernel on the network's stream may be
+ * scheduled while that one still runs and waits for it on the device
+ * (griddepcontrol.wait at its start), which hides the launch latency between
+ * the step's dependent kernels. The reference launches each kernel after the
+ * previous one returns (ANNarchy/generator/Template/CUDABaseTemplate.py:
+ * 328-630). Every kernel of a module run this way must begin with that wait;
+ * the generated ones do. */
+int anb_set_pdl(anb_net* net, int on);
+
 /* run(int) and step() of the generated module
  * (ANNarchy/generator/Template/CUDABaseTemplate.py:328-630, called from
  * ANNarchy/core/Simulate.py:76-87). Returns after the work is queued;
