@@ -390,7 +390,6 @@ int run_plan_once(anb_net* net) {
       i = j;
       continue;
     }
-    net->pdl_prev = false;
     int rc = ensure_side(net, j - i - 1);
     if (rc != ANB_OK) return rc;
     ANB_CUDA(cudaEventRecord(net->fork_ev, net->stream));
@@ -401,7 +400,10 @@ int run_plan_once(anb_net* net) {
       if (rc != ANB_OK) return rc;
       ANB_CUDA(cudaEventRecord(net->side_ev[q - i - 1], st));
     }
-    rc = launch(net, l, nullptr);
+    // the branch on the main stream may start early like a single launch; the
+    // side branches wait for the fork event (the previous kernel's end)
+    const bool pdl = net->pdl && net->pdl_prev && l.op != kOpBsrTc && l.cluster <= 1;
+    rc = launch(net, l, nullptr, nullptr, pdl);
     if (rc != ANB_OK) return rc;
     for (size_t q = i + 1; q < j; ++q) ANB_CUDA(cudaStreamWaitEvent(net->stream, net->side_ev[q - i - 1], 0));
     net->pdl_prev = false;
