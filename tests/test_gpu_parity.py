@@ -92,6 +92,38 @@ def test_coba_small_exact(golden, engine):
     out["net"].close()
 
 
+@pytest.mark.parametrize("graph_steps", [32, 0])
+@pytest.mark.parametrize("pdl", [True, False])
+def test_coba_small_exact_launch_modes(golden, graph_steps, pdl):
+    """The grid engine's plan replayed as CUDA graphs or launched step by
+    step, with and without programmatic dependent launch: the reference's
+    raster and final state bit for bit in every mode."""
+    g = golden("coba_small")
+    cn = wl.coba_net(seed=7, n=400, p=0.05, steps=2000)
+    out = run_coba(cn, 2000, engine="grid", graph_steps=graph_steps, pdl=pdl)
+    assert np.array_equal(out["steps"], g["spike_steps"])
+    assert np.array_equal(out["idx"], g["spike_idx"])
+    for k in ("v", "g_exc", "g_inh"):
+        assert np.array_equal(out[k], g[k + "_final"]), k
+    out["net"].close()
+
+
+def test_rate_c1_float_launch_modes():
+    """The float rate net with and without programmatic dependent launch,
+    CUDA graphs and step-by-step launches: the same final rates (the float
+    sums here add in a fixed order)."""
+    rn = wl.rate_net(seed=7, n_in=100, n_out=200, p_in=0.1, p_rec=0.05, steps=100)
+    outs = []
+    for graph_steps, pdl in ((32, True), (32, False), (0, True)):
+        net, pop, _ = wl.build_rate_network(rn, "float", record=False, graph_steps=graph_steps, pdl=pdl)
+        net.compile()
+        net.simulate_steps(100)
+        outs.append(np.asarray(pop.r).copy())
+        net.close()
+    for r in outs[1:]:
+        assert np.array_equal(r, outs[0])
+
+
 def test_coba_c2_exact(golden):
     g = golden("coba_c2")
     cn = wl.coba_net(seed=42)
